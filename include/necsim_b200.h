@@ -1,0 +1,228 @@
+/*
+ * necsim_b200.h -- C ABI of the B200 (sm_100a) backend for necsim-rust's
+ * Independent coalescence algorithm.
+ *
+ * The backend is a drop-in for the reference's `algorithm: CUDA(...)` /
+ * `Independent(...)` path: it takes a scenario (NonSpatial,
+ * SpatiallyImplicit, AlmostInfinite with Normal dispersal,
+ * SpatiallyExplicit with uniform turnover), a seeded WyHash RNG and the
+ * algorithm arguments, simulates every lineage on the GPU and hands the
+ * events to reporters in the reference's reporting order.
+ *
+ * Conventions: every entry point returns 0 on success and a negative
+ * NECSIM_E_* code on failure (never aborts or throws across the ABI); the
+ * message of the last failure on a context is returned by
+ * necsim_gpu_last_error().  All pointers are host pointers owned by the
+ * caller; the backend copies what it needs.  A context is used by one host
+ * thread at a time.
+ */
+#ifndef NECSIM_B200_H
+#define NECSIM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NECSIM_B200_ABI_VERSION 1
+
+/* ---- error codes ---- */
+#define NECSIM_OK 0
+#define NECSIM_E_INVALID_ARGUMENT (-1)   /* bad scenario / argument values     */
+#define NECSIM_E_CUDA (-2)               /* a CUDA runtime call failed          */
+#define NECSIM_E_OUT_OF_MEMORY (-3)      /* device or host allocation failed    */
+#define NECSIM_E_DEVICE_CHECK (-4)       /* a device-side bound check tripped   */
+#define NECSIM_E_TIMEOUT (-5)            /* a bounded device wait gave up       */
+#define NECSIM_E_DISPERSAL_MAP (-6)      /* dispersal map breaks the contract   */
+#define NECSIM_E_EMPTY_HABITAT (-7)      /* habitat map has no habitable cell   */
+#define NECSIM_E_UNSUPPORTED (-8)        /* valid in the reference, not here    */
+#define NECSIM_E_CALLBACK (-9)           /* a reporter callback asked to stop   */
+#define NECSIM_E_TOO_LARGE (-10)         /* exceeds a documented size limit     */
+
+/* ---- scenarios ---- */
+enum necsim_scenario_kind {
+    NECSIM_NON_SPATIAL = 0,            /* rustcoalescence/scenarios/src/non_spatial.rs               */
+    NECSIM_SPATIALLY_IMPLICIT = 1,     /* rustcoalescence/scenarios/src/spatially_implicit.rs        */
+    NECSIM_ALMOST_INFINITE_NORMAL = 2, /* rustcoalescence/scenarios/src/almost_infinite/normal.rs    */
+    NECSIM_SPATIALLY_EXPLICIT = 3,     /* rustcoalescence/scenarios/src/spatially_explicit/turnover/uniform.rs */
+};
+
+/* Replaces the reference's `ScenarioCogs` as produced by `Scenario::new`
+ * (rustcoalescence/scenarios/src/lib.rs:39-109) plus the
+ * `speciation_probability_per_generation` argument. */
+typedef struct necsim_scenario {
+    int32_t kind;                    /* enum necsim_scenario_kind */
+    uint32_t reserved0;
+    double speciation_probability;   /* (0, 1] per generation */
+    double turnover_rate;            /* uniform turnover lambda, reference default 0.5 */
+    uint32_t width, height, deme;    /* NonSpatial area + deme; SI local area + deme;
+                                        SpatiallyExplicit habitat map size */
+    uint32_t meta_width, meta_height, meta_deme; /* SI metacommunity */
+    double migration_probability;    /* SI migration probability per generation */
+    double sigma;                    /* AlmostInfinite Normal dispersal sigma */
+    uint32_t centre_x, centre_y, radius, reserved1; /* AlmostInfinite Circle sample */
+    const uint32_t *habitat;         /* SpatiallyExplicit: width*height u32, row-major */
+    const double *dispersal;         /* SpatiallyExplicit: (w*h) x (w*h) f64, row-major */
+} necsim_scenario;
+
+/* Replaces `CudaArguments` / `IndependentArguments`
+ * (rustcoalescence/algorithms/cuda/src/arguments.rs:61-138,
+ *  rustcoalescence/algorithms/independent/src/arguments.rs:79-146).
+ * Zero fields take the documented defaults. */
+typedef struct necsim_args {
+    double delta_t;            /* Poisson re-priming interval; default 2.0 (Independent) */
+    uint64_t step_slice;       /* expected events per lineage between dedup passes; default 10 */
+    uint64_t min_round_events; /* a round runs at least this many expected events in total
+                                  (widens rounds when few lineages are left); default 2^20 */
+    uint32_t block_size;       /* threads per block of the step kernel; 0 = autotuned */
+    uint32_t grid_size;        /* blocks of the step kernel; 0 = autotuned */
+    uint32_t dedup_factor_pct; /* dedup hash table load: slots = next_pow2(n*pct/100); default 200 */
+    uint32_t schedule;         /* 0 = plain (unsorted) kernel, 1 = learned lifetime buckets */
+    int32_t report_dispersal;  /* reporters consume dispersal events (ReportDispersal) */
+    int32_t device;            /* CUDA device ordinal; default 0 */
+    uint32_t rounds_per_graph; /* rounds captured per CUDA graph launch; 0 = default (16) */
+    uint32_t reserved;
+} necsim_args;
+
+/* ---- events and lineages (reference layouts) ---- */
+/* SpeciationEvent (necsim/core/src/event.rs:57-66), 40 bytes */
+typedef struct necsim_speciation_event {
+    uint64_t global_lineage_reference;
+    double prior_time;
+    double event_time;
+    uint32_t x, y, index, pad;
+} necsim_speciation_event;
+
+/* DispersalEvent (necsim/core/src/event.rs:74-82) without the interaction
+ * (always LineageInteraction::Maybe on the Independent path), 56 bytes */
+typedef struct necsim_dispersal_event {
+    uint64_t global_lineage_reference;
+    double prior_time;
+    double event_time;
+    uint32_t x, y, index;
+    uint32_t target_x, target_y, target_index;
+    uint32_t pad, pad2;
+} necsim_dispersal_event;
+
+/* Lineage (necsim/core/src/lineage.rs:91-106), 32 bytes */
+typedef struct necsim_lineage {
+    uint64_t global_reference;
+    double last_event_time;
+    uint32_t x, y, index, pad;
+} necsim_lineage;
+
+/* Reporter sink, replaces `Reporter::report_speciation` /
+ * `report_dispersal` (necsim/core/src/reporter/mod.rs:22-58).  Events are
+ * delivered in batches, each batch in the reference's PackedEvent order
+ * (event.rs:256-280), batches in increasing time.  A callback returning
+ * non-zero stops the delivery with NECSIM_E_CALLBACK. */
+typedef struct necsim_reporter {
+    void *user;
+    int (*report_speciation)(void *user, const necsim_speciation_event *events, uint64_t n);
+    int (*report_dispersal)(void *user, const necsim_dispersal_event *events, uint64_t n);
+} necsim_reporter;
+
+/* Replaces `SimulationOutcome` (rustcoalescence/algorithms/src/result.rs):
+ * Done{time, steps} or Paused{time, steps, lineages, rng}. */
+typedef struct necsim_outcome {
+    int32_t paused;            /* 0 = Done, 1 = Paused (remaining lineages available) */
+    int32_t pad;
+    double time;               /* time of the last executed event */
+    uint64_t steps;            /* executed events (lineage steps) */
+    uint64_t n_initial;        /* lineages simulated */
+    uint64_t n_remaining;      /* lineages left when paused */
+    uint64_t n_speciation;     /* speciation events reported (with duplicates) */
+    uint64_t biodiversity;     /* BiodiversityReporter count of distinct species */
+    uint64_t n_dispersal;      /* dispersal events reported */
+    uint64_t n_rounds;         /* synchronised rounds executed */
+    uint64_t n_dedup;          /* duplicate lineages removed */
+    uint64_t n_launches;       /* kernels launched by this call */
+    double kernel_ms;          /* device time of the step kernel (CUDA events) */
+    double total_ms;           /* device time of the whole simulation (CUDA events) */
+} necsim_outcome;
+
+typedef struct necsim_ctx necsim_ctx;
+
+/* Create a context: validates the scenario, builds the dispersal tables
+ * (SpatiallyExplicit: packed separable alias, packed_separable_alias/mod.rs:64-203),
+ * uploads them to the device and enumerates the origin lineages
+ * (OriginPreSampler::all(), origin_sampler/*.rs).  Replaces the set-up half of
+ * `Algorithm::initialise_and_simulate` (rustcoalescence/algorithms/src/lib.rs:81-93). */
+int necsim_gpu_create(const necsim_scenario *scenario, const necsim_args *args,
+                      necsim_ctx **out_ctx);
+/* On failure *out_ctx may still receive a context that only carries the
+ * error message (necsim_gpu_last_error); destroy it with necsim_gpu_destroy. */
+
+/* Simulate all origin lineages of the context's scenario to completion or
+ * until `pause_before` (< 0: no pause).  `wyhash_seed` is the WyHash seed
+ * word (necsim/impls/no-std/src/cogs/rng/wyhash.rs:41-49); use
+ * necsim_seed_from_u64() for the reference's `rng: Seed(u64)`.
+ * Replaces `Algorithm::initialise_and_simulate` (algorithms/src/lib.rs:81-93). */
+int necsim_gpu_simulate(necsim_ctx *ctx, uint64_t wyhash_seed, double pause_before,
+                        const necsim_reporter *reporter, necsim_outcome *outcome);
+
+/* Simulate caller-provided lineages (resume), with min_event_time =
+ * resume_time.  Replaces `Algorithm::resume_and_simulate`
+ * (algorithms/src/lib.rs:95-107). */
+int necsim_gpu_simulate_lineages(necsim_ctx *ctx, const necsim_lineage *lineages, uint64_t n,
+                                 double resume_time, uint64_t wyhash_seed, double pause_before,
+                                 const necsim_reporter *reporter, necsim_outcome *outcome);
+
+/* Lineages left after a paused simulation (SimulationOutcome::Paused.lineages),
+ * in ascending global reference order.  *n_out receives the count; at most
+ * `cap` are written. */
+int necsim_gpu_remaining_lineages(necsim_ctx *ctx, necsim_lineage *out, uint64_t cap,
+                                  uint64_t *n_out);
+
+/* Batched sweep: simulate `n_sims` independent simulations (scenarios may
+ * differ in every parameter, seeds per simulation) in one persistent launch
+ * per round.  No reference counterpart as a single call: it replaces
+ * `n_sims` calls of `Algorithm::initialise_and_simulate`.  outcomes[s]
+ * receives simulation s's outcome; reporters may be NULL or an array of
+ * n_sims sinks. */
+int necsim_gpu_simulate_batch(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds,
+                              uint32_t n_sims, const necsim_args *args, double pause_before,
+                              const necsim_reporter *reporters, necsim_outcome *outcomes,
+                              char *error, size_t error_cap);
+
+const char *necsim_gpu_last_error(const necsim_ctx *ctx);
+void necsim_gpu_destroy(necsim_ctx *ctx);
+
+/* SeedableRng::seed_from_u64 (necsim/core/src/cogs/rng.rs:33-63) followed by
+ * WyHash::from_seed (wyhash.rs:41-49): the WyHash seed word for `Seed(seed)`. */
+uint64_t necsim_seed_from_u64(uint64_t seed);
+
+/* ABI version, for bindings to check. */
+int necsim_abi_version(void);
+
+/* ---- host-side table construction (no GPU needed) ---- */
+/* One cell of the SpatiallyExplicit device tables, 32 bytes: the habitat
+ * injection prefix (habitat/in_memory.rs:143-163), the self-dispersal
+ * probability and non-self event (SeparableAliasSelfDispersal) and the
+ * cell's alias range (AliasSamplerRange), packed_separable_alias/mod.rs:22-42. */
+typedef struct necsim_cell_record {
+    uint64_t injection;
+    double self_dispersal;
+    uint32_t atom_start, atom_count, habitat, non_self_event;
+} necsim_cell_record;
+
+/* AliasMethodSamplerAtom (alias/packed.rs:10-15) with u32 events, 16 bytes. */
+typedef struct necsim_alias_atom {
+    double u;
+    uint32_t e, k;
+} necsim_alias_atom;
+
+/* Builds the tables InMemoryPackedSeparableAliasDispersalSampler::new
+ * (packed_separable_alias/mod.rs:64-203) builds, into caller buffers:
+ * `cells` needs width*height records, `atoms` up to `atom_cap` atoms;
+ * *n_atoms receives the atom count (call with atoms == NULL to size). */
+int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cells,
+                        necsim_alias_atom *atoms, uint64_t atom_cap, uint64_t *n_atoms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NECSIM_B200_H */

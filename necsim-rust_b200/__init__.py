@@ -1,0 +1,475 @@
+"""necsim-rust B200 backend: the Independent coalescence algorithm on sm_100a.
+
+Python mirror of the reference's `rustcoalescence simulate` interface for
+this path (RON arguments ``speciation``, ``sample``, ``rng``, ``scenario``,
+``algorithm``, ``pause``, ``reporters``; docs/simulate.ron), calling the
+C ABI in ``include/necsim_b200.h`` through ctypes.  The CUDA library must be
+built (``build.py``); there is no CPU fallback: importing this package on a
+machine without the library raises, and simulating without a GPU fails with
+the CUDA error the library reports.
+"""
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import build as _build
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = _build.LIB
+
+NON_SPATIAL = 0
+SPATIALLY_IMPLICIT = 1
+ALMOST_INFINITE_NORMAL = 2
+SPATIALLY_EXPLICIT = 3
+
+ERRORS = {
+    -1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "device bound check",
+    -5: "device wait timeout", -6: "dispersal map contract violated", -7: "empty habitat map",
+    -8: "unsupported", -9: "reporter stopped delivery", -10: "too large",
+}
+
+
+class NecsimError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "error"), code, message))
+        self.code = code
+
+
+# ---------------------------------------------------------------------------
+# ctypes mirror of include/necsim_b200.h
+# ---------------------------------------------------------------------------
+class CScenario(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32), ("reserved0", ctypes.c_uint32),
+        ("speciation_probability", ctypes.c_double), ("turnover_rate", ctypes.c_double),
+        ("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("deme", ctypes.c_uint32),
+        ("meta_width", ctypes.c_uint32), ("meta_height", ctypes.c_uint32),
+        ("meta_deme", ctypes.c_uint32),
+        ("migration_probability", ctypes.c_double), ("sigma", ctypes.c_double),
+        ("centre_x", ctypes.c_uint32), ("centre_y", ctypes.c_uint32),
+        ("radius", ctypes.c_uint32), ("reserved1", ctypes.c_uint32),
+        ("habitat", ctypes.POINTER(ctypes.c_uint32)),
+        ("dispersal", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class CArgs(ctypes.Structure):
+    _fields_ = [
+        ("delta_t", ctypes.c_double), ("step_slice", ctypes.c_uint64),
+        ("min_round_events", ctypes.c_uint64), ("block_size", ctypes.c_uint32),
+        ("grid_size", ctypes.c_uint32), ("dedup_factor_pct", ctypes.c_uint32),
+        ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class COutcome(ctypes.Structure):
+    _fields_ = [
+        ("paused", ctypes.c_int32), ("pad", ctypes.c_int32), ("time", ctypes.c_double),
+        ("steps", ctypes.c_uint64), ("n_initial", ctypes.c_uint64),
+        ("n_remaining", ctypes.c_uint64), ("n_speciation", ctypes.c_uint64),
+        ("biodiversity", ctypes.c_uint64), ("n_dispersal", ctypes.c_uint64),
+        ("n_rounds", ctypes.c_uint64), ("n_dedup", ctypes.c_uint64),
+        ("n_launches", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+SPECIATION_DTYPE = np.dtype(
+    [("gref", "<u8"), ("prior_time", "<f8"), ("event_time", "<f8"),
+     ("x", "<u4"), ("y", "<u4"), ("index", "<u4"), ("pad", "<u4")])
+DISPERSAL_DTYPE = np.dtype(
+    [("gref", "<u8"), ("prior_time", "<f8"), ("event_time", "<f8"),
+     ("x", "<u4"), ("y", "<u4"), ("index", "<u4"),
+     ("tx", "<u4"), ("ty", "<u4"), ("tindex", "<u4"), ("pad", "<u4"), ("pad2", "<u4")])
+LINEAGE_DTYPE = np.dtype(
+    [("gref", "<u8"), ("last_event_time", "<f8"),
+     ("x", "<u4"), ("y", "<u4"), ("index", "<u4"), ("pad", "<u4")])
+CELL_DTYPE = np.dtype(
+    [("injection", "<u8"), ("self_dispersal", "<f8"), ("atom_start", "<u4"),
+     ("atom_count", "<u4"), ("habitat", "<u4"), ("non_self_event", "<u4")])
+ATOM_DTYPE = np.dtype([("u", "<f8"), ("e", "<u4"), ("k", "<u4")])
+
+_SPEC_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64)
+_DISP_CB = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64)
+
+
+class CReporter(ctypes.Structure):
+    _fields_ = [("user", ctypes.c_void_p), ("report_speciation", _SPEC_CB),
+                ("report_dispersal", _DISP_CB)]
+
+
+SYMBOLS = [
+    "necsim_abi_version", "necsim_seed_from_u64", "necsim_gpu_create", "necsim_gpu_simulate",
+    "necsim_gpu_simulate_lineages", "necsim_gpu_remaining_lineages",
+    "necsim_gpu_simulate_batch", "necsim_gpu_last_error", "necsim_gpu_destroy",
+    "necsim_build_tables",
+]
+
+_lib = None
+
+
+def lib():
+    """Loads the CUDA backend library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libnecsim_b200.so is not built: run `python necsim-rust_b200/build.py` "
+                          "(there is no CPU fallback)")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    u64 = ctypes.c_uint64
+    L.necsim_abi_version.restype = ctypes.c_int
+    L.necsim_seed_from_u64.argtypes = [u64]
+    L.necsim_seed_from_u64.restype = u64
+    L.necsim_gpu_create.argtypes = [P(CScenario), P(CArgs), P(vp)]
+    L.necsim_gpu_create.restype = ctypes.c_int
+    L.necsim_gpu_simulate.argtypes = [vp, u64, ctypes.c_double, P(CReporter), P(COutcome)]
+    L.necsim_gpu_simulate.restype = ctypes.c_int
+    L.necsim_gpu_simulate_lineages.argtypes = [vp, vp, u64, ctypes.c_double, u64,
+                                               ctypes.c_double, P(CReporter), P(COutcome)]
+    L.necsim_gpu_simulate_lineages.restype = ctypes.c_int
+    L.necsim_gpu_remaining_lineages.argtypes = [vp, vp, u64, P(u64)]
+    L.necsim_gpu_remaining_lineages.restype = ctypes.c_int
+    L.necsim_gpu_simulate_batch.argtypes = [P(CScenario), P(u64), ctypes.c_uint32, P(CArgs),
+                                            ctypes.c_double, vp, P(COutcome), ctypes.c_char_p,
+                                            ctypes.c_size_t]
+    L.necsim_gpu_simulate_batch.restype = ctypes.c_int
+    L.necsim_gpu_last_error.argtypes = [vp]
+    L.necsim_gpu_last_error.restype = ctypes.c_char_p
+    L.necsim_gpu_destroy.argtypes = [vp]
+    L.necsim_gpu_destroy.restype = None
+    L.necsim_build_tables.argtypes = [P(CScenario), vp, vp, u64, P(u64)]
+    L.necsim_build_tables.restype = ctypes.c_int
+    if L.necsim_abi_version() != 1:
+        raise ImportError("libnecsim_b200.so ABI version mismatch")
+    _lib = L
+    return L
+
+
+# ---------------------------------------------------------------------------
+# Reference-shaped configuration (docs/simulate.ron)
+# ---------------------------------------------------------------------------
+@dataclass
+class NonSpatial:
+    """`NonSpatial(area: (w, h), deme: d)` (scenarios/src/non_spatial.rs)."""
+    area: Tuple[int, int]
+    deme: int
+
+
+@dataclass
+class SpatiallyImplicit:
+    """`SpatiallyImplicit(local_area, local_deme, meta_area, meta_deme, migration)`
+    (scenarios/src/spatially_implicit.rs)."""
+    local_area: Tuple[int, int]
+    local_deme: int
+    meta_area: Tuple[int, int]
+    meta_deme: int
+    migration: float
+
+
+@dataclass
+class Circle:
+    """`Circle(centre: (x, y), radius: r)` sample (almost_infinite/mod.rs:92-107)."""
+    radius: int
+    centre: Tuple[int, int] = (0xFFFFFFFF // 2, 0xFFFFFFFF // 2)
+
+
+@dataclass
+class Normal:
+    """`Normal(sigma: s)` dispersal (almost_infinite/normal.rs)."""
+    sigma: float
+
+
+@dataclass
+class AlmostInfinite:
+    """`AlmostInfinite(sample: Circle(..), dispersal: Normal(..))`."""
+    sample: Circle
+    dispersal: Normal
+
+
+@dataclass
+class SpatiallyExplicit:
+    """`SpatiallyExplicit(habitat, dispersal, turnover)` with in-memory maps
+    (spatially_explicit/turnover/uniform.rs): habitat u32 [h, w], dispersal
+    f64 [h*w, h*w]."""
+    habitat: np.ndarray
+    dispersal: np.ndarray
+    turnover: float = 0.5
+
+
+@dataclass
+class CUDA:
+    """`CUDA(...)` algorithm arguments (algorithms/cuda/src/arguments.rs) for
+    this backend; defaults follow the Independent algorithm's where results
+    depend on them (delta_t 2.0)."""
+    delta_t: float = 2.0
+    step_slice: int = 10
+    block_size: int = 0
+    grid_size: int = 0
+    min_round_events: int = 1 << 20
+    dedup_factor_pct: int = 200
+    schedule: str = "plain"   # or "learned"
+    device: int = 0
+    rounds_per_graph: int = 16
+
+
+Independent = CUDA
+
+
+@dataclass
+class Outcome:
+    paused: bool
+    time: float
+    steps: int
+    n_initial: int
+    n_remaining: int
+    n_speciation: int
+    biodiversity: int
+    n_rounds: int
+    n_dedup: int
+    n_launches: int
+    kernel_ms: float
+    total_ms: float
+    speciation: Optional[np.ndarray] = None
+    remaining: Optional[np.ndarray] = None
+
+
+def seed_from_u64(seed: int) -> int:
+    """WyHash seed word of `rng: Seed(seed)` (core/src/cogs/rng.rs:33-63)."""
+    return int(lib().necsim_seed_from_u64(seed))
+
+
+def _scenario_struct(scenario, speciation: float):
+    c = CScenario()
+    c.speciation_probability = speciation
+    c.turnover_rate = 0.5
+    keep = []
+    if isinstance(scenario, NonSpatial):
+        c.kind = NON_SPATIAL
+        c.width, c.height = scenario.area
+        c.deme = scenario.deme
+    elif isinstance(scenario, SpatiallyImplicit):
+        c.kind = SPATIALLY_IMPLICIT
+        c.width, c.height = scenario.local_area
+        c.deme = scenario.local_deme
+        c.meta_width, c.meta_height = scenario.meta_area
+        c.meta_deme = scenario.meta_deme
+        c.migration_probability = scenario.migration
+    elif isinstance(scenario, AlmostInfinite):
+        c.kind = ALMOST_INFINITE_NORMAL
+        c.sigma = scenario.dispersal.sigma
+        c.centre_x, c.centre_y = scenario.sample.centre
+        c.radius = scenario.sample.radius
+    elif isinstance(scenario, SpatiallyExplicit):
+        c.kind = SPATIALLY_EXPLICIT
+        h = np.ascontiguousarray(scenario.habitat, dtype=np.uint32)
+        d = np.ascontiguousarray(scenario.dispersal, dtype=np.float64)
+        if h.ndim != 2 or d.shape != (h.size, h.size):
+            raise ValueError("habitat must be [h, w] and dispersal [h*w, h*w]")
+        c.height, c.width = h.shape
+        c.turnover_rate = scenario.turnover
+        c.habitat = h.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        c.dispersal = d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        keep += [h, d]
+    else:
+        raise TypeError("unknown scenario %r" % (scenario,))
+    c._keep = keep
+    return c
+
+
+def _args_struct(algorithm: CUDA):
+    a = CArgs()
+    a.delta_t = algorithm.delta_t
+    a.step_slice = algorithm.step_slice
+    a.min_round_events = algorithm.min_round_events
+    a.block_size = algorithm.block_size
+    a.grid_size = algorithm.grid_size
+    a.dedup_factor_pct = algorithm.dedup_factor_pct
+    a.schedule = 1 if algorithm.schedule == "learned" else 0
+    a.report_dispersal = 0
+    a.device = algorithm.device
+    a.rounds_per_graph = algorithm.rounds_per_graph
+    return a
+
+
+class _Collector:
+    """Reporter sink gathering speciation events (in delivery order)."""
+
+    def __init__(self):
+        self.chunks = []
+
+        def on_spec(user, ptr, n):
+            buf = (ctypes.c_char * (n * SPECIATION_DTYPE.itemsize)).from_address(ptr)
+            self.chunks.append(np.frombuffer(bytes(buf), dtype=SPECIATION_DTYPE))
+            return 0
+
+        def on_disp(user, ptr, n):
+            return 0
+
+        self._spec = _SPEC_CB(on_spec)
+        self._disp = _DISP_CB(on_disp)
+        self.struct = CReporter(None, self._spec, self._disp)
+
+    def events(self):
+        if not self.chunks:
+            return np.zeros(0, dtype=SPECIATION_DTYPE)
+        return np.concatenate(self.chunks)
+
+
+def _outcome(o: COutcome, spec=None, remaining=None) -> Outcome:
+    return Outcome(bool(o.paused), o.time, o.steps, o.n_initial, o.n_remaining, o.n_speciation,
+                   o.biodiversity, o.n_rounds, o.n_dedup, o.n_launches, o.kernel_ms, o.total_ms,
+                   spec, remaining)
+
+
+class Simulation:
+    """A scenario bound to the GPU (tables uploaded once), simulated per seed.
+
+    Mirrors `Algorithm::initialise_and_simulate` / `resume_and_simulate`
+    (rustcoalescence/algorithms/src/lib.rs:81-107)."""
+
+    def __init__(self, scenario, speciation: float, algorithm: Optional[CUDA] = None):
+        self.algorithm = algorithm or CUDA()
+        L = lib()
+        self._scenario = _scenario_struct(scenario, speciation)
+        self._args = _args_struct(self.algorithm)
+        ctx = ctypes.c_void_p()
+        rc = L.necsim_gpu_create(ctypes.byref(self._scenario), ctypes.byref(self._args),
+                                 ctypes.byref(ctx))
+        self._ctx = ctx
+        if rc != 0:
+            msg = L.necsim_gpu_last_error(ctx).decode() if ctx.value else ""
+            self.close()
+            raise NecsimError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_ctx", None) is not None and self._ctx.value:
+            lib().necsim_gpu_destroy(self._ctx)
+        self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc):
+        if rc != 0:
+            raise NecsimError(rc, lib().necsim_gpu_last_error(self._ctx).decode())
+
+    def _remaining(self):
+        L = lib()
+        n = ctypes.c_uint64(0)
+        self._check(L.necsim_gpu_remaining_lineages(self._ctx, None, 0, ctypes.byref(n)))
+        out = np.zeros(max(n.value, 1), dtype=LINEAGE_DTYPE)
+        self._check(L.necsim_gpu_remaining_lineages(self._ctx, out.ctypes.data, n.value,
+                                                    ctypes.byref(n)))
+        return out[:n.value]
+
+    def simulate(self, seed: int, pause_before: Optional[float] = None, collect: bool = True,
+                 wyhash_seed: Optional[int] = None) -> Outcome:
+        """Simulates every origin lineage; `seed` is the RON `rng: Seed(seed)`."""
+        L = lib()
+        ws = seed_from_u64(seed) if wyhash_seed is None else wyhash_seed
+        col = _Collector() if collect else None
+        out = COutcome()
+        pb = -1.0 if pause_before is None else float(pause_before)
+        rc = L.necsim_gpu_simulate(self._ctx, ws, pb, ctypes.byref(col.struct) if col else None,
+                                   ctypes.byref(out))
+        self._check(rc)
+        return _outcome(out, col.events() if col else None,
+                        self._remaining() if out.paused else None)
+
+    def resume(self, lineages: np.ndarray, resume_time: float, seed: int,
+               pause_before: Optional[float] = None, collect: bool = True,
+               wyhash_seed: Optional[int] = None) -> Outcome:
+        """Simulates the given lineages from `resume_time` (resume_and_simulate)."""
+        L = lib()
+        ws = seed_from_u64(seed) if wyhash_seed is None else wyhash_seed
+        lins = np.ascontiguousarray(lineages, dtype=LINEAGE_DTYPE)
+        col = _Collector() if collect else None
+        out = COutcome()
+        pb = -1.0 if pause_before is None else float(pause_before)
+        rc = L.necsim_gpu_simulate_lineages(self._ctx, lins.ctypes.data, len(lins), resume_time,
+                                            ws, pb, ctypes.byref(col.struct) if col else None,
+                                            ctypes.byref(out))
+        self._check(rc)
+        return _outcome(out, col.events() if col else None,
+                        self._remaining() if out.paused else None)
+
+
+def simulate(speciation: float, scenario, seed: int, algorithm: Optional[CUDA] = None,
+             pause_before: Optional[float] = None, collect: bool = True) -> Outcome:
+    """One-shot `rustcoalescence simulate` equivalent for this backend."""
+    with Simulation(scenario, speciation, algorithm) as sim:
+        return sim.simulate(seed, pause_before=pause_before, collect=collect)
+
+
+def simulate_batch(scenarios: Sequence, speciations: Sequence[float], seeds: Sequence[int],
+                   algorithm: Optional[CUDA] = None, pause_before: Optional[float] = None,
+                   collect: bool = False) -> List[Outcome]:
+    """Runs many independent simulations (one scenario kind) in one batched
+    launch per round; returns one Outcome per simulation."""
+    L = lib()
+    n = len(scenarios)
+    structs = (CScenario * n)()
+    keep = []
+    for j, (sc, nu) in enumerate(zip(scenarios, speciations)):
+        c = _scenario_struct(sc, nu)
+        keep.append(c)
+        structs[j] = c
+    seeds_arr = (ctypes.c_uint64 * n)(*[seed_from_u64(s) for s in seeds])
+    outs = (COutcome * n)()
+    cols = [_Collector() for _ in range(n)] if collect else None
+    reps = None
+    if collect:
+        reps = (CReporter * n)(*[c.struct for c in cols])
+    args = _args_struct(algorithm or CUDA())
+    err = ctypes.create_string_buffer(512)
+    pb = -1.0 if pause_before is None else float(pause_before)
+    rc = L.necsim_gpu_simulate_batch(structs, seeds_arr, n, ctypes.byref(args), pb,
+                                     ctypes.cast(reps, ctypes.c_void_p) if reps else None,
+                                     outs, err, 512)
+    if rc != 0:
+        raise NecsimError(rc, err.value.decode())
+    return [_outcome(outs[j], cols[j].events() if cols else None) for j in range(n)]
+
+
+def build_tables(scenario: SpatiallyExplicit):
+    """Host-side SpatiallyExplicit tables (cells, atoms) as numpy arrays."""
+    L = lib()
+    c = _scenario_struct(scenario, 0.5)
+    n_atoms = ctypes.c_uint64(0)
+    rc = L.necsim_build_tables(ctypes.byref(c), None, None, 0, ctypes.byref(n_atoms))
+    if rc != 0:
+        raise NecsimError(rc, "table build failed")
+    cells = np.zeros(c.width * c.height, dtype=CELL_DTYPE)
+    atoms = np.zeros(max(n_atoms.value, 1), dtype=ATOM_DTYPE)
+    rc = L.necsim_build_tables(ctypes.byref(c), cells.ctypes.data, atoms.ctypes.data,
+                               n_atoms.value, ctypes.byref(n_atoms))
+    if rc != 0:
+        raise NecsimError(rc, "table build failed")
+    return cells, atoms[:n_atoms.value]
+
+
+def distinct_speciation_set(events: np.ndarray) -> np.ndarray:
+    """Sorted unique (event_time bits, x, y, index) rows: the species identities
+    (SpeciesIdentity::from_speciation, plugins/species/src/identity.rs:41)."""
+    if len(events) == 0:
+        return np.zeros((0, 4), dtype=np.uint64)
+    k = np.stack([events["event_time"].view(np.uint64), events["x"].astype(np.uint64),
+                  events["y"].astype(np.uint64), events["index"].astype(np.uint64)], axis=1)
+    return np.unique(k, axis=0)

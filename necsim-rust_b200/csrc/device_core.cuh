@@ -1,0 +1,198 @@
+// device_core.cuh -- per-lineage arithmetic of the Independent algorithm on
+// sm_100a: WyHash priming/sampling, the Poisson event-time sampler, the
+// speciation test, the four dispersal samplers and the coalescence index.
+//
+// Every f64 expression is evaluated as one IEEE-754 round-to-nearest
+// operation per source operator in the reference's order (the file is
+// compiled with --fmad=false so no multiply-add is contracted), and every
+// integer operation wraps like Rust's, so a lineage's trajectory is the
+// reference's bit for bit.
+#pragma once
+
+#include <cstdint>
+
+#include "layout.h"
+
+namespace necsim {
+
+// necsim/impls/no-std/src/cogs/rng/wyhash.rs:9-12
+constexpr uint64_t kWyP0 = 0xa0761d6478bd642fULL;
+constexpr uint64_t kWyP1 = 0xe7037ed1a0b428dbULL;
+constexpr uint64_t kWyP2 = 0x8ebc6af09c88c6e3ULL;
+constexpr uint64_t kWyP5 = 0xeb44accab455d165ULL;
+// wyhash.rs:99-119 SeaHash diffusion multiplier
+constexpr uint64_t kSeaHashK = 0x6eed0e9da4d94a4fULL;
+// event_time_sampler/poisson.rs:10: 2^64 / phi
+constexpr uint64_t kInvPhi = 0x9e3779b97f4a7c15ULL;
+// core::f64::consts::TAU
+constexpr double kTau = 6.283185307179586;
+
+// wyhash.rs:85-96: 64x64 -> 128 multiply, low and high halves xor-folded
+__device__ __forceinline__ uint64_t wymum(uint64_t a, uint64_t b) {
+    const uint64_t lo = a * b;
+    const uint64_t hi = __umul64hi(a, b);
+    return (a ^ lo) ^ (b ^ hi);
+}
+
+// wyhash.rs:99-119
+__device__ __forceinline__ uint64_t seahash_diffuse(uint64_t x) {
+    x *= kSeaHashK;
+    const uint64_t a = x >> 32;
+    const uint64_t b = x >> 60;
+    x ^= a >> b;
+    x *= kSeaHashK;
+    return x;
+}
+
+__device__ __forceinline__ uint64_t swap_halves(uint64_t v) { return (v << 32) | (v >> 32); }
+
+struct Rng {
+    uint64_t seed;
+    uint64_t state;
+
+    // wyhash.rs:68-80 PrimeableRng::prime_with
+    __device__ __forceinline__ void prime(uint64_t location_index, uint64_t time_index) {
+        const uint64_t l = seahash_diffuse(location_index);
+        const uint64_t t = seahash_diffuse(time_index);
+        const uint64_t h = wymum(swap_halves(l) ^ (seed ^ kWyP0), swap_halves(t) ^ kWyP2);
+        state = wymum(h, 16ULL ^ kWyP5);
+    }
+
+    // wyhash.rs:53-63 RngCore::sample_u64
+    __device__ __forceinline__ uint64_t next_u64() {
+        state += kWyP0;
+        return seahash_diffuse(wymum(state ^ kWyP1, state));
+    }
+
+    // necsim/core/src/cogs/rng.rs:75-82 -- [0, 1)
+    __device__ __forceinline__ double closed_open() {
+        return __dmul_rn(__ull2double_rn(next_u64() >> 11), 0x1.0p-53);
+    }
+
+    // rng.rs:84-93 -- (0, 1]
+    __device__ __forceinline__ double open_closed() {
+        return __dmul_rn(__ull2double_rn((next_u64() >> 11) + 1ULL), 0x1.0p-53);
+    }
+};
+
+// Rust `f64 as u64` for the non-negative finite values these call sites see
+// (floor of a product of a unit sample and a table length, or of t / dt);
+// saturates like Rust above range.
+__device__ __forceinline__ uint64_t f64_to_u64(double v) {
+    if (!(v > 0.0)) return 0;
+    if (v >= 18446744073709551616.0) return ~0ULL;
+    return __double2ull_rz(v);
+}
+__device__ __forceinline__ uint32_t f64_to_u32(double v) {
+    if (!(v > 0.0)) return 0;
+    if (v >= 4294967296.0) return 0xffffffffu;
+    return __double2uint_rz(v);
+}
+__device__ __forceinline__ int64_t f64_to_i64(double v) {
+    if (v != v) return 0;
+    if (v >= 9223372036854775808.0) return INT64_MAX;
+    if (v < -9223372036854775808.0) return INT64_MIN;
+    return __double2ll_rz(v);
+}
+
+// rng.rs:133-145 RngSampler::sample_index_u64
+__device__ __forceinline__ uint64_t sample_index_u64(Rng &g, uint64_t length) {
+    const uint64_t index = f64_to_u64(floor(__dmul_rn(g.closed_open(), __ull2double_rn(length))));
+    return index < length - 1 ? index : length - 1;
+}
+
+// necsim/core/bond/src/positive_f64.rs:103-113 PositiveF64::max_after
+__device__ __forceinline__ double max_after(double before, double value) {
+    if (value > before || before != before) return value;
+    if (isinf(before)) return before;
+    return __longlong_as_double(__double_as_longlong(before) + 1);
+}
+
+// event_time_sampler/poisson.rs:30-109: the next event time strictly after
+// `time` at the location with injection `inj`.  Leaves `g` primed with
+// (inj, reprime) exactly as the reference leaves its RNG, and returns the
+// re-prime time index in `reprime`.  `p0 = exp(-lambda * delta_t)` is a
+// per-run constant computed on the host with the system libm (the
+// reference's IntrinsicsMathsCore); p0 == 0 is rejected at set-up.
+__device__ __forceinline__ double poisson_next_event_time(Rng &g, uint64_t inj, double time,
+                                                          double delta_t, double lambda_dt,
+                                                          double p0, uint64_t &reprime) {
+    uint64_t time_step = f64_to_u64(floor(__ddiv_rn(time, delta_t)));
+    double best;
+    uint32_t best_k;
+    for (;;) {
+        g.prime(inj, time_step);
+        // Devroye's sequential inversion of Poisson(lambda * delta_t)
+        uint32_t n_events = 0;
+        double prod = p0;
+        double acc = p0;
+        const double u = g.closed_open();
+        while (u > acc && prod > 0.0) {
+            n_events += 1;
+            prod = __dmul_rn(prod, __ddiv_rn(lambda_dt, __uint2double_rn(n_events)));
+            acc = __dadd_rn(acc, prod);
+        }
+        bool found = false;
+        best = 0.0;
+        best_k = 0;
+        const double step_start = __ull2double_rn(time_step);
+        for (uint32_t k = 0; k < n_events; ++k) {
+            const double et = __dmul_rn(__dadd_rn(step_start, g.closed_open()), delta_t);
+            if (et > time && (!found || best > et)) {
+                best = et;
+                best_k = k;
+                found = true;
+            }
+        }
+        if (found) break;
+        time_step += 1;
+    }
+    reprime = time_step + kInvPhi * (uint64_t)(best_k + 1);
+    g.prime(inj, reprime);
+    return best;
+}
+
+// habitat/almost_infinite.rs:100-114 clamp_round_dispersal of a Box-Muller
+// draw (rng.rs:180-197; almost_infinite_normal.rs:58-68).  The transcendental
+// calls are CUDA's double-precision log/sin/cos; their results only pass
+// through round(), whose outcome equals the reference's (glibc) except when
+// the displacement lies within a few ulp of a half-integer.
+__device__ __forceinline__ void normal_dispersal(Rng &g, double sigma, uint32_t x, uint32_t y,
+                                                 uint32_t &tx, uint32_t &ty) {
+    const double u0 = g.open_closed();
+    const double u1 = g.closed_open();
+    const double r = __dsqrt_rn(__dmul_rn(-2.0, log(u0)));
+    const double theta = __dmul_rn(-kTau, u1);
+    const double z0 = __dmul_rn(r, sin(theta));
+    const double z1 = __dmul_rn(r, cos(theta));
+    const double dx = __dadd_rn(__dmul_rn(z0, sigma), 0.0);
+    const double dy = __dadd_rn(__dmul_rn(z1, sigma), 0.0);
+    const int64_t wrap = (int64_t)1 << 32;
+    const int64_t nx = ((int64_t)x + f64_to_i64(round(dx))) % wrap;
+    const int64_t ny = ((int64_t)y + f64_to_i64(round(dy))) % wrap;
+    tx = (uint32_t)((nx + wrap) % wrap);
+    ty = (uint32_t)((ny + wrap) % wrap);
+}
+
+// dispersal_sampler/non_spatial.rs:42-66 over an extent (ox, oy, w, h)
+__device__ __forceinline__ void non_spatial_dispersal(Rng &g, uint32_t ox, uint32_t oy, uint64_t w,
+                                                      uint64_t h, uint32_t &tx, uint32_t &ty) {
+    const uint64_t idx = sample_index_u64(g, w * h);
+    tx = ox + (uint32_t)(idx % w);
+    ty = oy + (uint32_t)(idx / w);
+}
+
+// landscape/extent.rs:44-49 LandscapeExtent::contains for the SI local
+// extent, whose origin is (0, 0)
+__device__ __forceinline__ bool in_local(const SimParams &p, uint32_t x, uint32_t y) {
+    return x <= p.width - 1 && y <= p.height - 1;
+}
+
+// habitat/non_spatial.rs:88-105 map_indexed_location_to_u64_injective
+__device__ __forceinline__ uint64_t non_spatial_injection(uint32_t ox, uint32_t oy, uint64_t w,
+                                                          uint32_t deme, uint32_t x, uint32_t y,
+                                                          uint32_t i) {
+    return ((uint64_t)(y - oy) * w + (uint64_t)(x - ox)) * (uint64_t)deme + (uint64_t)i;
+}
+
+}  // namespace necsim

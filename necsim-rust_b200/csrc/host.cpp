@@ -1,0 +1,1017 @@
+// host.cpp -- C ABI of the B200 backend: scenario set-up, dispersal tables,
+// origin lineages, the round loop (captured in CUDA graphs) and event
+// delivery to the reporters.  See include/necsim_b200.h for the contract.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/necsim_b200.h"
+#include "kernels.h"
+#include "layout.h"
+#include "tables.h"
+
+using namespace necsim;
+
+namespace {
+
+struct CudaFailure {
+    cudaError_t err;
+    const char *what;
+};
+
+#define CK(call)                                                   \
+    do {                                                           \
+        cudaError_t e_ = (call);                                   \
+        if (e_ != cudaSuccess) throw CudaFailure{e_, #call};       \
+    } while (0)
+
+struct ApiError {
+    int code;
+    std::string msg;
+};
+
+[[noreturn]] void fail(int code, const std::string &msg) { throw ApiError{code, msg}; }
+
+template <typename T>
+T *dev_alloc(size_t n) {
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(NECSIM_E_OUT_OF_MEMORY, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed");
+    }
+    if (e != cudaSuccess) throw CudaFailure{e, "cudaMalloc"};
+    return static_cast<T *>(p);
+}
+
+// SeedableRng::seed_from_u64 (necsim/core/src/cogs/rng.rs:33-63): PCG32
+// output words fill the 8 seed bytes little-endian; WyHash::from_seed
+// (wyhash.rs:41-49) reads them as one little-endian u64.
+uint64_t seed_from_u64(uint64_t state) {
+    uint64_t seed = 0;
+    for (int word = 0; word < 2; ++word) {
+        state = state * 6364136223846793005ULL + 11634580027462260723ULL;
+        const uint32_t xorshifted = (uint32_t)(((state >> 18) ^ state) >> 27);
+        const uint32_t rot = (uint32_t)(state >> 59);
+        const uint32_t out = (xorshifted >> rot) | (xorshifted << ((32u - rot) & 31u));
+        seed |= (uint64_t)out << (32 * word);
+    }
+    return seed;
+}
+
+// One simulation's host-side description.
+struct SimHost {
+    necsim_scenario sc;
+    uint64_t seed;
+    uint64_t n_origins;
+    uint64_t lineage_offset;  // first slot in the batch's lineage arrays
+    double start_time;        // min last event time of its lineages
+    double start_max;         // max last event time of its lineages
+    SimParams params;
+};
+
+void validate(const necsim_scenario &sc) {
+    if (!(sc.speciation_probability > 0.0) || !(sc.speciation_probability <= 1.0))
+        fail(NECSIM_E_INVALID_ARGUMENT, "speciation_probability must be in (0, 1]");
+    if (!(sc.turnover_rate > 0.0) || !std::isfinite(sc.turnover_rate))
+        fail(NECSIM_E_INVALID_ARGUMENT, "turnover_rate must be positive");
+    switch (sc.kind) {
+    case NECSIM_NON_SPATIAL:
+        if (!sc.width || !sc.height || !sc.deme) fail(NECSIM_E_INVALID_ARGUMENT, "NonSpatial area and deme must be >= 1");
+        break;
+    case NECSIM_SPATIALLY_IMPLICIT:
+        if (!sc.width || !sc.height || !sc.deme || !sc.meta_width || !sc.meta_height || !sc.meta_deme)
+            fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyImplicit areas and demes must be >= 1");
+        if (!(sc.migration_probability > 0.0) || !(sc.migration_probability <= 1.0))
+            fail(NECSIM_E_INVALID_ARGUMENT, "migration probability must be in (0, 1]");
+        break;
+    case NECSIM_ALMOST_INFINITE_NORMAL:
+        if (!(sc.sigma >= 0.0) || !std::isfinite(sc.sigma)) fail(NECSIM_E_INVALID_ARGUMENT, "sigma must be >= 0");
+        if (sc.radius > 65535) fail(NECSIM_E_INVALID_ARGUMENT, "circle radius is a u16");
+        break;
+    case NECSIM_SPATIALLY_EXPLICIT:
+        if (!sc.width || !sc.height || !sc.habitat || !sc.dispersal)
+            fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyExplicit needs habitat and dispersal maps");
+        break;
+    default:
+        fail(NECSIM_E_INVALID_ARGUMENT, "unknown scenario kind");
+    }
+}
+
+// Number of origin lineages of the scenario (OriginPreSampler::all()).
+uint64_t count_origins(const necsim_scenario &sc) {
+    switch (sc.kind) {
+    case NECSIM_NON_SPATIAL:
+    case NECSIM_SPATIALLY_IMPLICIT:
+        return (uint64_t)sc.width * sc.height * sc.deme;
+    case NECSIM_ALMOST_INFINITE_NORMAL: {
+        const int64_t r = sc.radius;
+        uint64_t n = 0;
+        for (int64_t dy = -r; dy <= r; ++dy)
+            for (int64_t dx = -r; dx <= r; ++dx)
+                if ((uint64_t)(dx * dx + dy * dy) <= (uint64_t)(r * r)) ++n;
+        return n;
+    }
+    default: {
+        uint64_t n = 0;
+        const uint64_t cells = (uint64_t)sc.width * sc.height;
+        for (uint64_t c = 0; c < cells; ++c) n += sc.habitat[c];
+        return n;
+    }
+    }
+}
+
+SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64_t wy_seed) {
+    SimParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.seed = wy_seed;
+    p.nu = sc.speciation_probability;
+    p.lambda = sc.turnover_rate;
+    p.delta_t = args.delta_t;
+    p.lambda_dt = p.lambda * p.delta_t;  // poisson.rs:40
+    p.p0 = std::exp(-p.lambda_dt);       // poisson.rs:42, system libm like IntrinsicsMathsCore
+    p.migration = sc.migration_probability;
+    p.sigma = sc.sigma;
+    p.width = sc.width;
+    p.height = sc.height;
+    p.deme = sc.deme;
+    if (sc.kind == NECSIM_SPATIALLY_IMPLICIT) {
+        // habitat/spatially_implicit.rs:45-49: meta origin (inv(w), inv(h))
+        p.meta_ox = 0xffffffffu - (sc.meta_width - 1);
+        p.meta_oy = 0xffffffffu - (sc.meta_height - 1);
+        p.meta_width = sc.meta_width;
+        p.meta_height = sc.meta_height;
+        p.meta_deme = sc.meta_deme;
+    }
+    p.step_slice = args.step_slice;
+    p.min_round_events = args.min_round_events;
+    p.pause_before = -1.0;
+    return p;
+}
+
+necsim_args with_defaults(const necsim_args *in) {
+    necsim_args a;
+    std::memset(&a, 0, sizeof(a));
+    if (in) a = *in;
+    if (!(a.delta_t > 0.0)) a.delta_t = 2.0;
+    if (a.step_slice == 0) a.step_slice = 10;
+    if (a.min_round_events == 0) a.min_round_events = 1ULL << 20;
+    if (a.dedup_factor_pct == 0) a.dedup_factor_pct = 200;
+    if (a.dedup_factor_pct < 110) a.dedup_factor_pct = 110;
+    if (a.rounds_per_graph == 0) a.rounds_per_graph = 16;
+    if (a.rounds_per_graph % 2) a.rounds_per_graph += 1;
+    return a;
+}
+
+// ---- device buffers of one (batched) simulation ----
+struct DeviceLineages {
+    LineageSoA soa{};
+    uint8_t *state = nullptr;
+    void alloc(uint64_t n) {
+        soa.x = dev_alloc<uint32_t>(n);
+        soa.y = dev_alloc<uint32_t>(n);
+        soa.idx = dev_alloc<uint32_t>(n);
+        soa.sim = dev_alloc<uint32_t>(n);
+        soa.last = dev_alloc<double>(n);
+        soa.next = dev_alloc<double>(n);
+        soa.reprime = dev_alloc<uint64_t>(n);
+        soa.gref = dev_alloc<uint64_t>(n);
+        soa.steps = dev_alloc<uint64_t>(n);
+        soa.has_next = dev_alloc<uint8_t>(n);
+        state = dev_alloc<uint8_t>(n);
+    }
+    void release() {
+        void *ptrs[] = {soa.x, soa.y, soa.idx, soa.sim, soa.last, soa.next, soa.reprime,
+                        soa.gref, soa.steps, soa.has_next, state};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        soa = LineageSoA{};
+        state = nullptr;
+    }
+};
+
+struct Control {  // small device scalars
+    unsigned long long n_cur, out_count, work, mask, n_spec_total, n_disp_total, steps_total;
+    unsigned int n_active;
+    uint32_t status;
+};
+
+struct Engine {
+    int device = 0;
+    int kind = 0;
+    necsim_args args{};
+    cudaStream_t stream = nullptr;
+    int n_sms = 148;
+
+    std::vector<SimHost> sims;
+    uint64_t n_total = 0;  // lineage slots
+
+    // SpatiallyExplicit tables (shared by all simulations of a batch only if
+    // they share the map; a batch of SE simulations gets one table set each)
+    std::vector<CellRecord *> d_cells;
+    std::vector<AliasAtom *> d_atoms;
+
+    DeviceLineages A, B;
+    uint32_t *owner = nullptr, *slot = nullptr;
+    unsigned long long *min_gref = nullptr;
+    unsigned long long table_size = 0;
+    SimParams *d_params = nullptr;
+    SimCounters *d_counters = nullptr;
+    Control *d_ctl = nullptr;
+    DevSpeciationEvent *d_spec = nullptr;
+    uint64_t spec_cap = 0;
+    DevDispersalEvent *d_disp = nullptr;
+    uint64_t disp_cap = 0;
+    Control *h_ctl = nullptr;  // pinned
+
+    unsigned step_grid = 0, step_block = 0;
+    unsigned aux_grid = 0, aux_block = 256;
+
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<cudaEvent_t> ev_start, ev_end;
+    cudaEvent_t ev_total0 = nullptr, ev_total1 = nullptr;
+    bool timing_in_graph = true;
+
+    ~Engine() { release(); }
+
+    void release() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        for (auto e : ev_start) cudaEventDestroy(e);
+        for (auto e : ev_end) cudaEventDestroy(e);
+        ev_start.clear();
+        ev_end.clear();
+        if (ev_total0) cudaEventDestroy(ev_total0);
+        if (ev_total1) cudaEventDestroy(ev_total1);
+        ev_total0 = ev_total1 = nullptr;
+        A.release();
+        B.release();
+        void *ptrs[] = {owner, slot, min_gref, d_params, d_counters, d_ctl, d_spec, d_disp};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        owner = slot = nullptr;
+        min_gref = nullptr;
+        d_params = nullptr;
+        d_counters = nullptr;
+        d_ctl = nullptr;
+        d_spec = nullptr;
+        d_disp = nullptr;
+        for (auto p : d_cells)
+            if (p) cudaFree(p);
+        for (auto p : d_atoms)
+            if (p) cudaFree(p);
+        d_cells.clear();
+        d_atoms.clear();
+        if (h_ctl) cudaFreeHost(h_ctl);
+        h_ctl = nullptr;
+        if (stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+    }
+};
+
+// ---- SpatiallyExplicit tables ----
+void upload_tables(Engine &E, SimHost &s) {
+    HostTables t;
+    int rc = build_spatially_explicit_tables(s.sc, t);
+    if (rc == 1) fail(NECSIM_E_EMPTY_HABITAT, "habitat map has no habitable cell");
+    if (rc == 2) fail(NECSIM_E_DISPERSAL_MAP, "dispersal map violates the in-memory dispersal contract");
+    if (rc == 3) fail(NECSIM_E_TOO_LARGE, "more than 2^32 alias atoms");
+    if (rc) fail(NECSIM_E_INVALID_ARGUMENT, "table build failed");
+    CellRecord *dc = dev_alloc<CellRecord>(t.cells.size());
+    AliasAtom *da = dev_alloc<AliasAtom>(t.atoms.size());
+    E.d_cells.push_back(dc);
+    E.d_atoms.push_back(da);
+    CK(cudaMemcpyAsync(dc, t.cells.data(), t.cells.size() * sizeof(CellRecord), cudaMemcpyHostToDevice, E.stream));
+    if (!t.atoms.empty())
+        CK(cudaMemcpyAsync(da, t.atoms.data(), t.atoms.size() * sizeof(AliasAtom), cudaMemcpyHostToDevice, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+    s.params.cells = dc;
+    s.params.atoms = da;
+    s.params.n_cells = t.cells.size();
+    s.params.n_atoms = t.atoms.size();
+}
+
+void setup_engine(Engine &E, const necsim_args &args) {
+    E.args = args;
+    E.device = args.device;
+    CK(cudaSetDevice(E.device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, E.device));
+    E.n_sms = prop.multiProcessorCount;
+    CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&E.ev_total0));
+    CK(cudaEventCreate(&E.ev_total1));
+    void *h = nullptr;
+    CK(cudaMallocHost(&h, sizeof(Control)));
+    E.h_ctl = static_cast<Control *>(h);
+}
+
+void choose_launch(Engine &E) {
+    unsigned block = E.args.block_size ? E.args.block_size : 128;
+    if (block > (unsigned)kStepBlockMax) block = kStepBlockMax;
+    block = std::max(32u, block / 32 * 32);
+    int per_sm = 0;
+    CK(step_kernel_occupancy(E.kind, (int)block, &per_sm));
+    if (per_sm < 1) per_sm = 1;
+    E.step_block = block;
+    E.step_grid = E.args.grid_size ? E.args.grid_size : (unsigned)(per_sm * E.n_sms);
+    E.aux_block = 256;
+    E.aux_grid = (unsigned)(E.n_sms * 8);
+}
+
+void alloc_run_buffers(Engine &E) {
+    const uint64_t n = E.n_total;
+    E.A.alloc(n);
+    E.B.alloc(n);
+    unsigned long long want = (n * E.args.dedup_factor_pct + 99) / 100;
+    if (want < 2) want = 2;
+    unsigned long long size = 1;
+    while (size < want) size <<= 1;
+    E.table_size = size;
+    E.owner = dev_alloc<uint32_t>(size);
+    E.min_gref = dev_alloc<unsigned long long>(size);
+    E.slot = dev_alloc<uint32_t>(n);
+    CK(cudaMemsetAsync(E.owner, 0xff, size * sizeof(uint32_t), E.stream));
+    CK(cudaMemsetAsync(E.min_gref, 0xff, size * sizeof(unsigned long long), E.stream));
+    E.d_params = dev_alloc<SimParams>(E.sims.size());
+    E.d_counters = dev_alloc<SimCounters>(E.sims.size());
+    E.d_ctl = dev_alloc<Control>(1);
+    E.spec_cap = n;
+    E.d_spec = dev_alloc<DevSpeciationEvent>(n);
+}
+
+// Builds the origin lineages of every simulation on the host, in the
+// reference's origin-sampler order, and uploads them as structure of arrays.
+void upload_origins(Engine &E, const std::vector<std::vector<necsim_lineage>> *given) {
+    const uint64_t n = E.n_total;
+    std::vector<uint32_t> x(n), y(n), idx(n), sim(n);
+    std::vector<double> last(n);
+    std::vector<uint64_t> gref(n);
+    for (size_t s = 0; s < E.sims.size(); ++s) {
+        SimHost &sh = E.sims[s];
+        uint64_t o = sh.lineage_offset;
+        double tmin = 0.0, tmax = 0.0;
+        bool first = true;
+        auto push = [&](uint32_t xx, uint32_t yy, uint32_t ii, uint64_t g, double t) {
+            x[o] = xx;
+            y[o] = yy;
+            idx[o] = ii;
+            sim[o] = (uint32_t)s;
+            last[o] = t;
+            gref[o] = g;
+            ++o;
+            if (first || t < tmin) tmin = t;
+            if (first || t > tmax) tmax = t;
+            first = false;
+        };
+        const necsim_scenario &sc = sh.sc;
+        if (given) {
+            for (const necsim_lineage &l : (*given)[s]) push(l.x, l.y, l.index, l.global_reference, l.last_event_time);
+        } else if (sc.kind == NECSIM_NON_SPATIAL || sc.kind == NECSIM_SPATIALLY_IMPLICIT) {
+            // origin_sampler/non_spatial.rs:89-112 over landscape/extent.rs:80-100
+            // (SI samples only its local community, origin_sampler/spatially_implicit.rs)
+            uint64_t g = 0;
+            for (uint32_t yy = 0; yy < sc.height; ++yy)
+                for (uint32_t xx = 0; xx < sc.width; ++xx)
+                    for (uint32_t ii = 0; ii < sc.deme; ++ii) push(xx, yy, ii, g++, 0.0);
+        } else if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL) {
+            // origin_sampler/singleton_demes/circle.rs:36-70, 100-140
+            const uint32_t r = sc.radius;
+            const uint64_t d = (uint64_t)r * 2 + 1;
+            const uint32_t ox = sc.centre_x - r, oy = sc.centre_y - r;
+            const uint64_t r2 = (uint64_t)r * r;
+            for (uint64_t yy = 0; yy < d; ++yy)
+                for (uint64_t xx = 0; xx < d; ++xx) {
+                    const uint32_t px = ox + (uint32_t)xx, py = oy + (uint32_t)yy;
+                    const uint64_t dx = std::min<uint32_t>(px - sc.centre_x, sc.centre_x - px);
+                    const uint64_t dy = std::min<uint32_t>(py - sc.centre_y, sc.centre_y - py);
+                    if (dx * dx + dy * dy <= r2) push(px, py, 0, ((uint64_t)py << 32) | px, 0.0);
+                }
+        } else {
+            // origin_sampler/in_memory.rs:89-119; gref = prefix(cell) + index
+            uint64_t g = 0;
+            for (uint32_t yy = 0; yy < sc.height; ++yy)
+                for (uint32_t xx = 0; xx < sc.width; ++xx) {
+                    const uint32_t h = sc.habitat[(uint64_t)yy * sc.width + xx];
+                    for (uint32_t ii = 0; ii < h; ++ii) push(xx, yy, ii, g++, 0.0);
+                }
+        }
+        if (o != sh.lineage_offset + sh.n_origins) fail(NECSIM_E_INVALID_ARGUMENT, "origin count mismatch");
+        sh.start_time = tmin;
+        sh.start_max = tmax;
+    }
+    LineageSoA &d = E.A.soa;
+    CK(cudaMemcpyAsync(d.x, x.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.y, y.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.idx, idx.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.sim, sim.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.last, last.data(), n * 8, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.gref, gref.data(), n * 8, cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemsetAsync(d.steps, 0, n * 8, E.stream));
+    CK(cudaMemsetAsync(d.has_next, 0, n, E.stream));
+    CK(cudaMemsetAsync(d.next, 0, n * 8, E.stream));
+    CK(cudaMemsetAsync(d.reprime, 0, n * 8, E.stream));
+    CK(cudaMemsetAsync(E.A.state, 0, n, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+}
+
+StepArgs make_step_args(Engine &E, DeviceLineages &in) {
+    StepArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.in = in.soa;
+    a.state = in.state;
+    a.order = nullptr;
+    a.n_cur = &E.d_ctl->n_cur;
+    a.work = &E.d_ctl->work;
+    a.params = E.d_params;
+    a.counters = E.d_counters;
+    a.spec = E.d_spec;
+    a.n_spec_total = &E.d_ctl->n_spec_total;
+    a.spec_cap = E.spec_cap;
+    a.disp = E.d_disp;
+    a.n_disp_total = &E.d_ctl->n_disp_total;
+    a.disp_cap = E.disp_cap;
+    a.report_dispersal = E.args.report_dispersal ? 1 : 0;
+    a.status = &E.d_ctl->status;
+    a.steps_total = &E.d_ctl->steps_total;
+    return a;
+}
+
+DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
+    DedupArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.in = in.soa;
+    a.out = out.soa;
+    a.state = in.state;
+    a.state_out = out.state;
+    a.n_cur = &E.d_ctl->n_cur;
+    a.mask = &E.d_ctl->mask;
+    a.owner = E.owner;
+    a.min_gref = E.min_gref;
+    a.slot = E.slot;
+    a.out_count = &E.d_ctl->out_count;
+    a.counters = E.d_counters;
+    a.status = &E.d_ctl->status;
+    return a;
+}
+
+ScheduleArgs make_schedule_args(Engine &E) {
+    ScheduleArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.params = E.d_params;
+    a.counters = E.d_counters;
+    a.n_sims = (uint32_t)E.sims.size();
+    a.dedup_pct = E.args.dedup_factor_pct;
+    a.n_cur = &E.d_ctl->n_cur;
+    a.out_count = &E.d_ctl->out_count;
+    a.work = &E.d_ctl->work;
+    a.mask = &E.d_ctl->mask;
+    a.table_size = E.table_size;
+    a.n_active = &E.d_ctl->n_active;
+    return a;
+}
+
+// Enqueues `rounds` rounds (even) on the stream; with `events`, records a
+// timing event pair around every step kernel.
+void enqueue_rounds(Engine &E, unsigned rounds, bool events, bool external) {
+    for (unsigned r = 0; r < rounds; ++r) {
+        DeviceLineages &in = (r % 2 == 0) ? E.A : E.B;
+        DeviceLineages &out = (r % 2 == 0) ? E.B : E.A;
+        if (events) {
+            if (external)
+                CK(cudaEventRecordWithFlags(E.ev_start[r], E.stream, cudaEventRecordExternal));
+            else
+                CK(cudaEventRecord(E.ev_start[r], E.stream));
+        }
+        CK(launch_step(E.kind, make_step_args(E, in), E.step_grid, E.step_block, E.stream));
+        if (events) {
+            if (external)
+                CK(cudaEventRecordWithFlags(E.ev_end[r], E.stream, cudaEventRecordExternal));
+            else
+                CK(cudaEventRecord(E.ev_end[r], E.stream));
+        }
+        CK(launch_dedup(make_dedup_args(E, in, out), E.aux_grid, E.aux_block, E.stream));
+        CK(launch_schedule(make_schedule_args(E), E.stream));
+    }
+}
+
+void build_graph(Engine &E) {
+    const unsigned rounds = E.args.rounds_per_graph;
+    E.ev_start.resize(rounds);
+    E.ev_end.resize(rounds);
+    for (unsigned r = 0; r < rounds; ++r) {
+        CK(cudaEventCreate(&E.ev_start[r]));
+        CK(cudaEventCreate(&E.ev_end[r]));
+    }
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        enqueue_rounds(E, rounds, true, true);
+    } catch (...) {
+        cudaStreamEndCapture(E.stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        throw;
+    }
+    CK(cudaStreamEndCapture(E.stream, &graph));
+    cudaError_t e = cudaGraphInstantiate(&E.graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) throw CudaFailure{e, "cudaGraphInstantiate"};
+}
+
+struct RunResult {
+    double kernel_ms = 0.0;
+    double total_ms = 0.0;
+    uint64_t launches = 0;
+    uint64_t rounds_launched = 0;
+};
+
+// The round loop: initial schedule, then graphs of `rounds_per_graph` rounds
+// until no simulation is active.
+RunResult run_rounds(Engine &E) {
+    RunResult rr;
+    const unsigned rounds = E.args.rounds_per_graph;
+    // initial control state
+    Control c;
+    std::memset(&c, 0, sizeof(c));
+    c.out_count = E.n_total;
+    CK(cudaMemcpyAsync(E.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, E.stream));
+    std::vector<SimParams> ps(E.sims.size());
+    std::vector<SimCounters> cs(E.sims.size());
+    for (size_t s = 0; s < E.sims.size(); ++s) {
+        ps[s] = E.sims[s].params;
+        ps[s].horizon = E.sims[s].start_time;
+        ps[s].active = 0;
+        std::memset(&cs[s], 0, sizeof(SimCounters));
+        cs[s].n_live_next = E.sims[s].n_origins;
+        // max over the initial last event times (monolithic/mod.rs:121-126)
+        double t0 = E.sims[s].start_time;
+        cs[s].max_time_bits = 0;
+        (void)t0;
+    }
+    CK(cudaMemcpyAsync(E.d_params, ps.data(), ps.size() * sizeof(SimParams), cudaMemcpyHostToDevice, E.stream));
+    CK(cudaMemcpyAsync(E.d_counters, cs.data(), cs.size() * sizeof(SimCounters), cudaMemcpyHostToDevice, E.stream));
+    CK(cudaEventRecord(E.ev_total0, E.stream));
+    CK(launch_schedule(make_schedule_args(E), E.stream));
+    rr.launches += 1;
+    CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+    uint64_t graph_launches = 0;
+    while (E.h_ctl->n_active > 0) {
+        // every round advances each active simulation's horizon by at least
+        // step_slice / lambda, so this bound is never reached by a valid run
+        if (++graph_launches > (1ULL << 26) / rounds)
+            fail(NECSIM_E_TIMEOUT, "round limit reached");
+        if (E.graph_exec && E.timing_in_graph) {
+            CK(cudaGraphLaunch(E.graph_exec, E.stream));
+        } else {
+            enqueue_rounds(E, rounds, true, false);
+        }
+        rr.launches += (uint64_t)rounds * 5;
+        rr.rounds_launched += rounds;
+        CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
+        CK(cudaStreamSynchronize(E.stream));
+        for (unsigned r = 0; r < rounds; ++r) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, E.ev_start[r], E.ev_end[r]) == cudaSuccess) rr.kernel_ms += ms;
+        }
+        if (E.h_ctl->status & ~kErrDedupFull) break;
+    }
+    CK(cudaEventRecord(E.ev_total1, E.stream));
+    CK(cudaEventSynchronize(E.ev_total1));
+    float tot = 0.f;
+    CK(cudaEventElapsedTime(&tot, E.ev_total0, E.ev_total1));
+    rr.total_ms = tot;
+    return rr;
+}
+
+inline uint64_t bits_of(double v) {
+    uint64_t b;
+    std::memcpy(&b, &v, 8);
+    return b;
+}
+
+// PackedEvent::cmp (necsim/core/src/event.rs:256-280) for speciation events
+// (target == origin), per simulation.
+bool spec_less(const DevSpeciationEvent &a, const DevSpeciationEvent &b) {
+    if (a.sim != b.sim) return a.sim < b.sim;
+    const uint64_t ta = bits_of(a.event_time), tb = bits_of(b.event_time);
+    if (ta != tb) return ta < tb;
+    if (a.x != b.x) return a.x < b.x;
+    if (a.y != b.y) return a.y < b.y;
+    if (a.idx != b.idx) return a.idx < b.idx;
+    const uint64_t pa = bits_of(a.prior_time), pb = bits_of(b.prior_time);
+    if (pa != pb) return pa < pb;
+    return a.gref < b.gref;
+}
+
+bool disp_less(const DevDispersalEvent &a, const DevDispersalEvent &b) {
+    if (a.sim != b.sim) return a.sim < b.sim;
+    const uint64_t ta = bits_of(a.event_time), tb = bits_of(b.event_time);
+    if (ta != tb) return ta < tb;
+    if (a.x != b.x) return a.x < b.x;
+    if (a.y != b.y) return a.y < b.y;
+    if (a.idx != b.idx) return a.idx < b.idx;
+    if (a.tx != b.tx) return a.tx < b.tx;
+    if (a.ty != b.ty) return a.ty < b.ty;
+    if (a.tidx != b.tidx) return a.tidx < b.tidx;
+    const uint64_t pa = bits_of(a.prior_time), pb = bits_of(b.prior_time);
+    if (pa != pb) return pa < pb;
+    return a.gref < b.gref;
+}
+
+struct Remaining {
+    std::vector<std::vector<necsim_lineage>> per_sim;
+};
+
+// Collects counters, surviving lineages and events after the rounds; fills
+// the outcomes and delivers events to the reporters.
+void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bool one_reporter,
+            necsim_outcome *outcomes, Remaining &rem) {
+    const size_t ns = E.sims.size();
+    std::vector<SimCounters> cs(ns);
+    CK(cudaMemcpy(cs.data(), E.d_counters, ns * sizeof(SimCounters), cudaMemcpyDeviceToHost));
+    Control c;
+    CK(cudaMemcpy(&c, E.d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    if (c.status & (kErrCellIndex | kErrAtomIndex | kErrEventOverflow | kErrDispersalOverflow))
+        fail(NECSIM_E_DEVICE_CHECK, "device bound check failed (status " + std::to_string(c.status) + ")");
+    // surviving lineages live in A after an even number of rounds
+    const uint64_t n = c.n_cur;
+    LineageSoA &d = E.A.soa;
+    std::vector<uint32_t> x(n), y(n), idx(n), sim(n);
+    std::vector<double> last(n);
+    std::vector<uint64_t> gref(n), steps(n);
+    if (n) {
+        CK(cudaMemcpy(x.data(), d.x, n * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(y.data(), d.y, n * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(idx.data(), d.idx, n * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(sim.data(), d.sim, n * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(last.data(), d.last, n * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gref.data(), d.gref, n * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(steps.data(), d.steps, n * 8, cudaMemcpyDeviceToHost));
+    }
+    rem.per_sim.assign(ns, {});
+    std::vector<uint64_t> extra_steps(ns, 0);
+    std::vector<double> extra_time(ns, 0.0);
+    for (uint64_t j = 0; j < n; ++j) {
+        const uint32_t s = sim[j];
+        extra_steps[s] += steps[j];
+        extra_time[s] = std::max(extra_time[s], last[j]);
+        necsim_lineage l;
+        l.global_reference = gref[j];
+        l.last_event_time = last[j];
+        l.x = x[j];
+        l.y = y[j];
+        l.index = idx[j];
+        l.pad = 0;
+        rem.per_sim[s].push_back(l);
+    }
+    for (auto &v : rem.per_sim)
+        std::sort(v.begin(), v.end(), [](const necsim_lineage &a, const necsim_lineage &b) {
+            return a.global_reference < b.global_reference;
+        });
+
+    const uint64_t n_spec = std::min<uint64_t>(c.n_spec_total, E.spec_cap);
+    std::vector<DevSpeciationEvent> ev(n_spec);
+    if (n_spec)
+        CK(cudaMemcpy(ev.data(), E.d_spec, n_spec * sizeof(DevSpeciationEvent), cudaMemcpyDeviceToHost));
+    std::sort(ev.begin(), ev.end(), spec_less);
+
+    size_t pos = 0;
+    for (size_t s = 0; s < ns; ++s) {
+        necsim_outcome &o = outcomes[s];
+        std::memset(&o, 0, sizeof(o));
+        double t;
+        uint64_t tb = cs[s].max_time_bits;
+        std::memcpy(&t, &tb, 8);
+        // max_time: initial last event times (monolithic/mod.rs:121-126), every
+        // executed event, and min_event_time once a lineage was simulated
+        // (active_lineage_sampler/independent/sampler.rs:64-66)
+        o.time = std::max(std::max(t, extra_time[s]), E.sims[s].start_max);
+        if (cs[s].n_rounds > 0 && E.sims[s].n_origins > 0)
+            o.time = std::max(o.time, E.sims[s].params.min_event_time);
+        o.steps = cs[s].steps + extra_steps[s];
+        o.n_initial = E.sims[s].n_origins;
+        o.n_remaining = rem.per_sim[s].size();
+        o.paused = o.n_remaining > 0 ? 1 : 0;
+        o.n_speciation = cs[s].n_speciation;
+        o.n_rounds = cs[s].n_rounds;
+        o.n_dedup = cs[s].n_dedup;
+        o.n_launches = rr.launches;
+        o.kernel_ms = rr.kernel_ms;
+        o.total_ms = rr.total_ms;
+        // deliver this simulation's events in PackedEvent order; count
+        // species like BiodiversityReporter (plugins/common/src/biodiversity.rs:32-45)
+        size_t end = pos;
+        while (end < ev.size() && ev[end].sim == s) ++end;
+        std::vector<necsim_speciation_event> out;
+        out.reserve(end - pos);
+        uint64_t species = 0;
+        for (size_t k = pos; k < end; ++k) {
+            const DevSpeciationEvent &e = ev[k];
+            if (k == pos || !(ev[k - 1].x == e.x && ev[k - 1].y == e.y && ev[k - 1].idx == e.idx &&
+                              ev[k - 1].event_time == e.event_time))
+                ++species;
+            necsim_speciation_event r;
+            r.global_lineage_reference = e.gref;
+            r.prior_time = e.prior_time;
+            r.event_time = e.event_time;
+            r.x = e.x;
+            r.y = e.y;
+            r.index = e.idx;
+            r.pad = 0;
+            out.push_back(r);
+        }
+        o.biodiversity = species;
+        const necsim_reporter *rep = reporters ? (one_reporter ? reporters : &reporters[s]) : nullptr;
+        if (rep && rep->report_speciation && !out.empty()) {
+            if (rep->report_speciation(rep->user, out.data(), out.size()) != 0)
+                fail(NECSIM_E_CALLBACK, "reporter stopped the delivery");
+        }
+        pos = end;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+struct necsim_ctx {
+    std::unique_ptr<Engine> engine;
+    necsim_scenario scenario{};
+    necsim_args args{};
+    std::vector<uint32_t> habitat;  // owned copies of the SE maps' habitat
+    std::string error;
+    Remaining remaining;
+    bool tables_ready = false;
+    SimParams table_params{};  // cells/atoms pointers of the uploaded tables
+};
+
+namespace {
+
+int report(necsim_ctx *ctx, char *buf, size_t cap, int code, const std::string &msg) {
+    if (ctx) ctx->error = msg;
+    if (buf && cap) {
+        std::snprintf(buf, cap, "%s", msg.c_str());
+    }
+    return code;
+}
+
+template <typename F>
+int guarded(necsim_ctx *ctx, char *buf, size_t cap, F &&f) {
+    try {
+        f();
+        if (ctx) ctx->error.clear();
+        return NECSIM_OK;
+    } catch (const ApiError &e) {
+        return report(ctx, buf, cap, e.code, e.msg);
+    } catch (const CudaFailure &e) {
+        return report(ctx, buf, cap, NECSIM_E_CUDA,
+                      std::string(e.what) + ": " + cudaGetErrorString(e.err));
+    } catch (const std::bad_alloc &) {
+        return report(ctx, buf, cap, NECSIM_E_OUT_OF_MEMORY, "host allocation failed");
+    } catch (...) {
+        return report(ctx, buf, cap, NECSIM_E_INVALID_ARGUMENT, "unexpected failure");
+    }
+}
+
+// Runs simulations (one or a batch) end to end on a fresh engine.
+void run_simulations(Engine &E, std::vector<SimHost> sims, const necsim_args &args,
+                     const std::vector<std::vector<necsim_lineage>> *given,
+                     const necsim_reporter *reporters, bool one_reporter, necsim_outcome *outcomes,
+                     Remaining &rem, const std::vector<SimParams> *prebuilt_tables) {
+    E.kind = sims.front().sc.kind;
+    for (auto &s : sims)
+        if (s.sc.kind != E.kind) fail(NECSIM_E_UNSUPPORTED, "a batch must share one scenario kind");
+    if (args.report_dispersal) fail(NECSIM_E_UNSUPPORTED, "dispersal reporting is not enabled in this build");
+    uint64_t off = 0;
+    for (auto &s : sims) {
+        s.lineage_offset = off;
+        off += s.n_origins;
+    }
+    if (off >= 0xffffffffULL) fail(NECSIM_E_TOO_LARGE, "more than 2^32 - 1 lineages");
+    E.sims = std::move(sims);
+    E.n_total = off;
+    for (size_t s = 0; s < E.sims.size(); ++s) {
+        SimHost &sh = E.sims[s];
+        if (sh.sc.kind == NECSIM_SPATIALLY_EXPLICIT) {
+            if (prebuilt_tables) {
+                sh.params.cells = (*prebuilt_tables)[s].cells;
+                sh.params.atoms = (*prebuilt_tables)[s].atoms;
+                sh.params.n_cells = (*prebuilt_tables)[s].n_cells;
+                sh.params.n_atoms = (*prebuilt_tables)[s].n_atoms;
+            } else {
+                upload_tables(E, sh);
+            }
+        }
+        if (!(sh.params.p0 > 0.0)) fail(NECSIM_E_UNSUPPORTED, "exp(-lambda * delta_t) underflows to 0");
+    }
+    choose_launch(E);
+    alloc_run_buffers(E);
+    upload_origins(E, given);
+    if (E.n_total > 0) build_graph(E);
+    RunResult rr;
+    if (E.n_total > 0) rr = run_rounds(E);
+    finish(E, rr, reporters, one_reporter, outcomes, rem);
+}
+
+}  // namespace
+
+extern "C" {
+
+int necsim_abi_version(void) { return NECSIM_B200_ABI_VERSION; }
+
+uint64_t necsim_seed_from_u64(uint64_t seed) { return seed_from_u64(seed); }
+
+int necsim_gpu_create(const necsim_scenario *scenario, const necsim_args *args, necsim_ctx **out_ctx) {
+    if (!scenario || !out_ctx) return NECSIM_E_INVALID_ARGUMENT;
+    *out_ctx = nullptr;
+    necsim_ctx *ctx = new (std::nothrow) necsim_ctx();
+    if (!ctx) return NECSIM_E_OUT_OF_MEMORY;
+    int rc = guarded(ctx, nullptr, 0, [&] {
+        validate(*scenario);
+        ctx->scenario = *scenario;
+        ctx->args = with_defaults(args);
+        if (scenario->kind == NECSIM_SPATIALLY_EXPLICIT) {
+            const uint64_t cells = (uint64_t)scenario->width * scenario->height;
+            ctx->habitat.assign(scenario->habitat, scenario->habitat + cells);
+            // tables are built and uploaded once per context
+            ctx->engine.reset(new Engine());
+            setup_engine(*ctx->engine, ctx->args);
+            SimHost sh;
+            std::memset(&sh, 0, sizeof(sh));
+            sh.sc = *scenario;
+            sh.params = base_params(*scenario, ctx->args, 0);
+            upload_tables(*ctx->engine, sh);
+            ctx->table_params = sh.params;
+            ctx->tables_ready = true;
+            ctx->scenario.habitat = ctx->habitat.data();
+            ctx->scenario.dispersal = nullptr;  // consumed by the table build
+        }
+    });
+    if (rc != NECSIM_OK) {
+        // keep the context so the caller can read the message, then fail
+        *out_ctx = ctx;
+        return rc;
+    }
+    *out_ctx = ctx;
+    return NECSIM_OK;
+}
+
+static int simulate_impl(necsim_ctx *ctx, const necsim_lineage *lineages, uint64_t n_lineages,
+                         bool resume, double resume_time, uint64_t wyhash_seed, double pause_before,
+                         const necsim_reporter *reporter, necsim_outcome *outcome) {
+    if (!ctx || !outcome) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(ctx, nullptr, 0, [&] {
+        // a fresh engine per simulation; SE tables are carried over
+        std::unique_ptr<Engine> tables_owner;
+        std::vector<SimParams> prebuilt;
+        Engine *E = new Engine();
+        std::unique_ptr<Engine> E_owner(E);
+        if (ctx->tables_ready) {
+            // move the table allocations into this run's engine, then back
+            Engine &T = *ctx->engine;
+            E->d_cells.swap(T.d_cells);
+            E->d_atoms.swap(T.d_atoms);
+            prebuilt.push_back(ctx->table_params);
+        }
+        struct Restore {
+            necsim_ctx *ctx;
+            Engine *E;
+            ~Restore() {
+                if (ctx->tables_ready) {
+                    ctx->engine->d_cells.swap(E->d_cells);
+                    ctx->engine->d_atoms.swap(E->d_atoms);
+                }
+            }
+        } restore{ctx, E};
+        setup_engine(*E, ctx->args);
+        SimHost sh;
+        std::memset(&sh, 0, sizeof(sh));
+        sh.sc = ctx->scenario;
+        sh.seed = wyhash_seed;
+        sh.params = base_params(ctx->scenario, ctx->args, wyhash_seed);
+        sh.params.pause_before = pause_before >= 0.0 ? pause_before : -1.0;
+        std::vector<std::vector<necsim_lineage>> given;
+        if (resume) {
+            sh.params.min_event_time = resume_time;
+            // independent/mod.rs:98-117: lineages outside the habitat are not simulated
+            std::vector<necsim_lineage> keep;
+            keep.reserve(n_lineages);
+            for (uint64_t j = 0; j < n_lineages; ++j) {
+                const necsim_lineage &l = lineages[j];
+                uint32_t h = 0;
+                const necsim_scenario &sc = ctx->scenario;
+                switch (sc.kind) {
+                case NECSIM_NON_SPATIAL:
+                    h = (l.x < sc.width && l.y < sc.height) ? sc.deme : 0;
+                    break;
+                case NECSIM_SPATIALLY_IMPLICIT: {
+                    const uint32_t mox = 0xffffffffu - (sc.meta_width - 1), moy = 0xffffffffu - (sc.meta_height - 1);
+                    if (l.x < sc.width && l.y < sc.height)
+                        h = sc.deme;
+                    else if (l.x >= mox && l.y >= moy)
+                        h = sc.meta_deme;
+                    break;
+                }
+                case NECSIM_ALMOST_INFINITE_NORMAL:
+                    h = 1;
+                    break;
+                default:
+                    h = (l.x < sc.width && l.y < sc.height) ? ctx->habitat[(uint64_t)l.y * sc.width + l.x] : 0;
+                    break;
+                }
+                if (h > 0 && l.index < h) keep.push_back(l);
+            }
+            sh.n_origins = keep.size();
+            given.push_back(std::move(keep));
+        } else {
+            sh.n_origins = count_origins(ctx->scenario);
+        }
+        std::vector<SimHost> sims{sh};
+        necsim_outcome o;
+        run_simulations(*E, sims, ctx->args, resume ? &given : nullptr, reporter, true, &o,
+                        ctx->remaining, ctx->tables_ready ? &prebuilt : nullptr);
+        *outcome = o;
+    });
+}
+
+int necsim_gpu_simulate(necsim_ctx *ctx, uint64_t wyhash_seed, double pause_before,
+                        const necsim_reporter *reporter, necsim_outcome *outcome) {
+    return simulate_impl(ctx, nullptr, 0, false, 0.0, wyhash_seed, pause_before, reporter, outcome);
+}
+
+int necsim_gpu_simulate_lineages(necsim_ctx *ctx, const necsim_lineage *lineages, uint64_t n,
+                                 double resume_time, uint64_t wyhash_seed, double pause_before,
+                                 const necsim_reporter *reporter, necsim_outcome *outcome) {
+    if (n && !lineages) return NECSIM_E_INVALID_ARGUMENT;
+    return simulate_impl(ctx, lineages, n, true, resume_time, wyhash_seed, pause_before, reporter, outcome);
+}
+
+int necsim_gpu_remaining_lineages(necsim_ctx *ctx, necsim_lineage *out, uint64_t cap, uint64_t *n_out) {
+    if (!ctx || !n_out) return NECSIM_E_INVALID_ARGUMENT;
+    const std::vector<necsim_lineage> *v = ctx->remaining.per_sim.empty() ? nullptr : &ctx->remaining.per_sim[0];
+    const uint64_t n = v ? v->size() : 0;
+    *n_out = n;
+    if (out)
+        for (uint64_t j = 0; j < n && j < cap; ++j) out[j] = (*v)[j];
+    return NECSIM_OK;
+}
+
+int necsim_gpu_simulate_batch(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds,
+                              uint32_t n_sims, const necsim_args *args_in, double pause_before,
+                              const necsim_reporter *reporters, necsim_outcome *outcomes, char *error,
+                              size_t error_cap) {
+    if (!scenarios || !wyhash_seeds || !outcomes || n_sims == 0) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, error, error_cap, [&] {
+        const necsim_args args = with_defaults(args_in);
+        std::vector<SimHost> sims(n_sims);
+        for (uint32_t s = 0; s < n_sims; ++s) {
+            validate(scenarios[s]);
+            SimHost &sh = sims[s];
+            std::memset(&sh, 0, sizeof(sh));
+            sh.sc = scenarios[s];
+            sh.seed = wyhash_seeds[s];
+            sh.params = base_params(scenarios[s], args, wyhash_seeds[s]);
+            sh.params.pause_before = pause_before >= 0.0 ? pause_before : -1.0;
+            sh.n_origins = count_origins(scenarios[s]);
+        }
+        Engine E;
+        setup_engine(E, args);
+        Remaining rem;
+        run_simulations(E, sims, args, nullptr, reporters, false, outcomes, rem, nullptr);
+    });
+}
+
+int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cells, necsim_alias_atom *atoms,
+                        uint64_t atom_cap, uint64_t *n_atoms) {
+    if (!scenario || !n_atoms || scenario->kind != NECSIM_SPATIALLY_EXPLICIT) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, nullptr, 0, [&] {
+        validate(*scenario);
+        HostTables t;
+        const int rc = build_spatially_explicit_tables(*scenario, t);
+        if (rc == 1) fail(NECSIM_E_EMPTY_HABITAT, "habitat map has no habitable cell");
+        if (rc == 2) fail(NECSIM_E_DISPERSAL_MAP, "dispersal map violates the in-memory dispersal contract");
+        if (rc == 3) fail(NECSIM_E_TOO_LARGE, "more than 2^32 alias atoms");
+        *n_atoms = t.atoms.size();
+        static_assert(sizeof(necsim_cell_record) == sizeof(CellRecord), "cell record layout");
+        static_assert(sizeof(necsim_alias_atom) == sizeof(AliasAtom), "alias atom layout");
+        if (cells) std::memcpy(cells, t.cells.data(), t.cells.size() * sizeof(CellRecord));
+        if (atoms) std::memcpy(atoms, t.atoms.data(), std::min<uint64_t>(atom_cap, t.atoms.size()) * sizeof(AliasAtom));
+    });
+}
+
+const char *necsim_gpu_last_error(const necsim_ctx *ctx) { return ctx ? ctx->error.c_str() : "null context"; }
+
+void necsim_gpu_destroy(necsim_ctx *ctx) { delete ctx; }
+
+}  // extern "C"

@@ -1,0 +1,66 @@
+// kernels.h -- launch arguments of the round kernels (host <-> device).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "layout.h"
+
+namespace necsim {
+
+constexpr int kStepBlockMax = 256;
+
+struct StepArgs {
+    LineageSoA in;                       // lineages of this round (updated in place)
+    uint8_t *state;                      // per slot: 0 alive, 1 speciated, 2 dropped
+    const uint32_t *order;               // queue order of slots (nullptr: identity)
+    const unsigned long long *n_cur;     // live lineages in `in`
+    unsigned long long *work;            // queue head (reset by the scheduler)
+    const SimParams *params;
+    SimCounters *counters;
+    DevSpeciationEvent *spec;
+    unsigned long long *n_spec_total;
+    uint64_t spec_cap;
+    DevDispersalEvent *disp;
+    unsigned long long *n_disp_total;
+    uint64_t disp_cap;
+    int report_dispersal;
+    uint32_t *status;
+    unsigned long long *steps_total;     // optional per-launch event count
+};
+
+struct DedupArgs {
+    LineageSoA in;
+    LineageSoA out;
+    const uint8_t *state;
+    uint8_t *state_out;
+    const unsigned long long *n_cur;
+    const unsigned long long *mask;      // table slots - 1 for this round
+    uint32_t *owner;                     // slot -> owning lineage (0xffffffff empty)
+    unsigned long long *min_gref;        // slot -> smallest global reference
+    uint32_t *slot;                      // lineage -> slot
+    unsigned long long *out_count;
+    SimCounters *counters;
+    uint32_t *status;
+};
+
+struct ScheduleArgs {
+    SimParams *params;
+    SimCounters *counters;
+    uint32_t n_sims;
+    uint32_t dedup_pct;
+    unsigned long long *n_cur;
+    unsigned long long *out_count;
+    unsigned long long *work;
+    unsigned long long *mask;
+    unsigned long long table_size;
+    unsigned int *n_active;
+};
+
+cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st);
+cudaError_t step_kernel_occupancy(int kind, int block, int *blocks_per_sm);
+cudaError_t launch_dedup(const DedupArgs &a, unsigned grid, unsigned block, cudaStream_t st);
+cudaError_t launch_schedule(const ScheduleArgs &a, cudaStream_t st);
+
+}  // namespace necsim

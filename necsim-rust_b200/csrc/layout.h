@@ -1,0 +1,123 @@
+// layout.h -- data layout shared by the host driver and the sm_100a kernels.
+//
+// HBM layout (one simulation or a batch of simulations of one scenario kind):
+//  * lineages: structure of arrays, double-buffered (round r reads A, writes
+//    the survivors to B), one slot per live lineage, coalesced per field;
+//  * SpatiallyExplicit tables: one 32-byte CellRecord per habitat cell (one
+//    DRAM sector: injection base, habitat, alias range, self-dispersal) and
+//    one 16-byte AliasAtom per alias bucket, so an event reads 2 sectors;
+//  * per-simulation SimParams (scenario scalars + the round horizon) and
+//    SimCounters (steps, time, event counts), indexed by the lineage's sim id;
+//  * dedup table: open-addressed slots (owner lineage, min global reference).
+#pragma once
+
+#include <cstdint>
+
+namespace necsim {
+
+enum Kind : int32_t {
+    kNonSpatial = 0,
+    kSpatiallyImplicit = 1,
+    kAlmostInfiniteNormal = 2,
+    kSpatiallyExplicit = 3,
+};
+
+// One habitat cell of a SpatiallyExplicit map, 32 bytes (one DRAM sector).
+// Restates InMemoryHabitat's u64 injection prefix (habitat/in_memory.rs:143-163),
+// the cell's habitat, AliasSamplerRange and SeparableAliasSelfDispersal
+// (dispersal_sampler/in_memory/packed_separable_alias/mod.rs:22-42).
+struct alignas(32) CellRecord {
+    uint64_t injection;      // prefix sum of habitat over preceding cells
+    double self_dispersal;   // probability of self-dispersal
+    uint32_t atom_start;     // first alias atom of the cell
+    uint32_t atom_count;     // number of alias atoms
+    uint32_t habitat;        // deme capacity
+    uint32_t non_self_event; // == own cell index iff self-dispersal is not in the atoms
+};
+static_assert(sizeof(CellRecord) == 32, "CellRecord must fill one sector");
+
+// AliasMethodSamplerAtom<usize> (alias/packed.rs:10-15) with u32 events, 16 bytes.
+struct alignas(16) AliasAtom {
+    double u;
+    uint32_t e;
+    uint32_t k;
+};
+static_assert(sizeof(AliasAtom) == 16, "AliasAtom must be 16 bytes");
+
+// Per-simulation scalars, read by every lineage of the simulation.
+struct SimParams {
+    uint64_t seed;            // WyHash seed word
+    double nu;                // speciation probability
+    double lambda;            // uniform turnover rate
+    double delta_t;
+    double lambda_dt;         // lambda * delta_t
+    double p0;                // exp(-lambda * delta_t), host libm
+    double migration;         // SI
+    double sigma;             // AlmostInfinite
+    double min_event_time;    // resume time (0 for a fresh start)
+    double pause_before;      // < 0: none
+    double horizon;           // current round's horizon (schedule kernel)
+    uint32_t width, height, deme;             // NS / SI local / SE map width
+    uint32_t meta_ox, meta_oy, meta_width, meta_height, meta_deme;
+    const CellRecord *cells;  // SE
+    const AliasAtom *atoms;   // SE
+    uint64_t n_cells;
+    uint64_t n_atoms;
+    uint64_t step_slice;
+    uint64_t min_round_events;
+    int32_t active;           // 1 while the simulation still advances
+    int32_t pad;
+};
+
+// Per-simulation counters (device), accumulated as lineages leave.
+struct SimCounters {
+    unsigned long long steps;          // events of removed lineages
+    unsigned long long max_time_bits;  // max event time (non-negative f64 bits)
+    unsigned long long n_speciation;
+    unsigned long long n_dedup;
+    unsigned long long n_rounds;
+    unsigned long long n_live;         // live lineages at the round start
+    unsigned long long n_live_next;    // survivors of the current round
+    unsigned long long n_dispersal;
+};
+
+// Lineage state, structure of arrays.
+struct LineageSoA {
+    uint32_t *x, *y, *idx, *sim;
+    double *last;        // last event time
+    double *next;        // peeked next event time (valid iff has_next)
+    uint64_t *reprime;   // time index the RNG is primed with after the peek
+    uint64_t *gref;      // global lineage reference
+    uint64_t *steps;     // events executed by this lineage
+    uint8_t *has_next;
+};
+
+// Speciation event record written by the kernel (SpeciationEvent plus the
+// simulation id), 40 bytes.
+struct DevSpeciationEvent {
+    uint64_t gref;
+    double prior_time;
+    double event_time;
+    uint32_t x, y, idx, sim;
+};
+
+// Dispersal event record (DispersalEvent payload plus simulation id), 56 bytes.
+struct DevDispersalEvent {
+    uint64_t gref;
+    double prior_time;
+    double event_time;
+    uint32_t x, y, idx;
+    uint32_t tx, ty, tidx;
+    uint32_t sim, pad;
+};
+
+// Device status word bits (set instead of trapping).
+enum : uint32_t {
+    kErrCellIndex = 1u << 0,     // a SpatiallyExplicit cell index out of range
+    kErrAtomIndex = 1u << 1,     // an alias atom index out of range
+    kErrEventOverflow = 1u << 2, // speciation event buffer full
+    kErrDedupFull = 1u << 3,     // dedup probe sequence exhausted
+    kErrDispersalOverflow = 1u << 4,
+};
+
+}  // namespace necsim
