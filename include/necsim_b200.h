@@ -221,6 +221,14 @@ typedef struct necsim_alias_atom {
 int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cells,
                         necsim_alias_atom *atoms, uint64_t atom_cap, uint64_t *n_atoms);
 
+/* The scenario's origin lineages in the reference's origin-sampler order
+ * (OriginPreSampler::all() through origin_sampler/{non_spatial,in_memory,
+ * spatially_implicit,singleton_demes/circle}.rs, Lineage::new gives the
+ * global reference = the location's u64 injection).  *n_out receives the
+ * count; at most `cap` are written (out may be NULL to size). */
+int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *out, uint64_t cap,
+                             uint64_t *n_out);
+
 #ifdef __cplusplus
 }
 #endif

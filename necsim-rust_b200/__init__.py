@@ -107,7 +107,7 @@ SYMBOLS = [
     "necsim_abi_version", "necsim_seed_from_u64", "necsim_gpu_create", "necsim_gpu_simulate",
     "necsim_gpu_simulate_lineages", "necsim_gpu_remaining_lineages",
     "necsim_gpu_simulate_batch", "necsim_gpu_last_error", "necsim_gpu_destroy",
-    "necsim_build_tables",
+    "necsim_build_tables", "necsim_enumerate_origins",
 ]
 
 _lib = None
@@ -147,6 +147,8 @@ def lib():
     L.necsim_gpu_destroy.restype = None
     L.necsim_build_tables.argtypes = [P(CScenario), vp, vp, u64, P(u64)]
     L.necsim_build_tables.restype = ctypes.c_int
+    L.necsim_enumerate_origins.argtypes = [P(CScenario), vp, u64, P(u64)]
+    L.necsim_enumerate_origins.restype = ctypes.c_int
     if L.necsim_abi_version() != 1:
         raise ImportError("libnecsim_b200.so ABI version mismatch")
     _lib = L
@@ -463,6 +465,21 @@ def build_tables(scenario: SpatiallyExplicit):
     if rc != 0:
         raise NecsimError(rc, "table build failed")
     return cells, atoms[:n_atoms.value]
+
+
+def enumerate_origins(scenario, speciation: float = 0.5) -> np.ndarray:
+    """The scenario's origin lineages in the reference's order (host only)."""
+    L = lib()
+    c = _scenario_struct(scenario, speciation)
+    n = ctypes.c_uint64(0)
+    rc = L.necsim_enumerate_origins(ctypes.byref(c), None, 0, ctypes.byref(n))
+    if rc != 0:
+        raise NecsimError(rc, "origin enumeration failed")
+    out = np.zeros(max(n.value, 1), dtype=LINEAGE_DTYPE)
+    rc = L.necsim_enumerate_origins(ctypes.byref(c), out.ctypes.data, n.value, ctypes.byref(n))
+    if rc != 0:
+        raise NecsimError(rc, "origin enumeration failed")
+    return out[:n.value]
 
 
 def distinct_speciation_set(events: np.ndarray) -> np.ndarray:

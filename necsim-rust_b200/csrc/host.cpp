@@ -349,6 +349,41 @@ void alloc_run_buffers(Engine &E) {
     E.d_spec = dev_alloc<DevSpeciationEvent>(n);
 }
 
+// Calls push(x, y, index, global_reference) for every origin lineage of the
+// scenario in the reference's origin-sampler order (OriginPreSampler::all()).
+template <typename F>
+void for_each_origin(const necsim_scenario &sc, F &&push) {
+    if (sc.kind == NECSIM_NON_SPATIAL || sc.kind == NECSIM_SPATIALLY_IMPLICIT) {
+        // origin_sampler/non_spatial.rs:89-112 over landscape/extent.rs:80-100
+        // (SI samples only its local community, origin_sampler/spatially_implicit.rs)
+        uint64_t g = 0;
+        for (uint32_t yy = 0; yy < sc.height; ++yy)
+            for (uint32_t xx = 0; xx < sc.width; ++xx)
+                for (uint32_t ii = 0; ii < sc.deme; ++ii) push(xx, yy, ii, g++);
+    } else if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL) {
+        // origin_sampler/singleton_demes/circle.rs:36-70, 100-140
+        const uint32_t r = sc.radius;
+        const uint64_t d = (uint64_t)r * 2 + 1;
+        const uint32_t ox = sc.centre_x - r, oy = sc.centre_y - r;
+        const uint64_t r2 = (uint64_t)r * r;
+        for (uint64_t yy = 0; yy < d; ++yy)
+            for (uint64_t xx = 0; xx < d; ++xx) {
+                const uint32_t px = ox + (uint32_t)xx, py = oy + (uint32_t)yy;
+                const uint64_t dx = std::min<uint32_t>(px - sc.centre_x, sc.centre_x - px);
+                const uint64_t dy = std::min<uint32_t>(py - sc.centre_y, sc.centre_y - py);
+                if (dx * dx + dy * dy <= r2) push(px, py, 0u, ((uint64_t)py << 32) | px);
+            }
+    } else {
+        // origin_sampler/in_memory.rs:89-119; global reference = prefix(cell) + index
+        uint64_t g = 0;
+        for (uint32_t yy = 0; yy < sc.height; ++yy)
+            for (uint32_t xx = 0; xx < sc.width; ++xx) {
+                const uint32_t h = sc.habitat[(uint64_t)yy * sc.width + xx];
+                for (uint32_t ii = 0; ii < h; ++ii) push(xx, yy, ii, g++);
+            }
+    }
+}
+
 // Builds the origin lineages of every simulation on the host, in the
 // reference's origin-sampler order, and uploads them as structure of arrays.
 void upload_origins(Engine &E, const std::vector<std::vector<necsim_lineage>> *given) {
@@ -376,34 +411,8 @@ void upload_origins(Engine &E, const std::vector<std::vector<necsim_lineage>> *g
         const necsim_scenario &sc = sh.sc;
         if (given) {
             for (const necsim_lineage &l : (*given)[s]) push(l.x, l.y, l.index, l.global_reference, l.last_event_time);
-        } else if (sc.kind == NECSIM_NON_SPATIAL || sc.kind == NECSIM_SPATIALLY_IMPLICIT) {
-            // origin_sampler/non_spatial.rs:89-112 over landscape/extent.rs:80-100
-            // (SI samples only its local community, origin_sampler/spatially_implicit.rs)
-            uint64_t g = 0;
-            for (uint32_t yy = 0; yy < sc.height; ++yy)
-                for (uint32_t xx = 0; xx < sc.width; ++xx)
-                    for (uint32_t ii = 0; ii < sc.deme; ++ii) push(xx, yy, ii, g++, 0.0);
-        } else if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL) {
-            // origin_sampler/singleton_demes/circle.rs:36-70, 100-140
-            const uint32_t r = sc.radius;
-            const uint64_t d = (uint64_t)r * 2 + 1;
-            const uint32_t ox = sc.centre_x - r, oy = sc.centre_y - r;
-            const uint64_t r2 = (uint64_t)r * r;
-            for (uint64_t yy = 0; yy < d; ++yy)
-                for (uint64_t xx = 0; xx < d; ++xx) {
-                    const uint32_t px = ox + (uint32_t)xx, py = oy + (uint32_t)yy;
-                    const uint64_t dx = std::min<uint32_t>(px - sc.centre_x, sc.centre_x - px);
-                    const uint64_t dy = std::min<uint32_t>(py - sc.centre_y, sc.centre_y - py);
-                    if (dx * dx + dy * dy <= r2) push(px, py, 0, ((uint64_t)py << 32) | px, 0.0);
-                }
         } else {
-            // origin_sampler/in_memory.rs:89-119; gref = prefix(cell) + index
-            uint64_t g = 0;
-            for (uint32_t yy = 0; yy < sc.height; ++yy)
-                for (uint32_t xx = 0; xx < sc.width; ++xx) {
-                    const uint32_t h = sc.habitat[(uint64_t)yy * sc.width + xx];
-                    for (uint32_t ii = 0; ii < h; ++ii) push(xx, yy, ii, g++, 0.0);
-                }
+            for_each_origin(sc, [&](uint32_t xx, uint32_t yy, uint32_t ii, uint64_t g) { push(xx, yy, ii, g, 0.0); });
         }
         if (o != sh.lineage_offset + sh.n_origins) fail(NECSIM_E_INVALID_ARGUMENT, "origin count mismatch");
         sh.start_time = tmin;
@@ -1007,6 +1016,27 @@ int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cel
         static_assert(sizeof(necsim_alias_atom) == sizeof(AliasAtom), "alias atom layout");
         if (cells) std::memcpy(cells, t.cells.data(), t.cells.size() * sizeof(CellRecord));
         if (atoms) std::memcpy(atoms, t.atoms.data(), std::min<uint64_t>(atom_cap, t.atoms.size()) * sizeof(AliasAtom));
+    });
+}
+
+int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *out, uint64_t cap,
+                             uint64_t *n_out) {
+    if (!scenario || !n_out) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, nullptr, 0, [&] {
+        validate(*scenario);
+        uint64_t n = 0;
+        for_each_origin(*scenario, [&](uint32_t x, uint32_t y, uint32_t i, uint64_t g) {
+            if (out && n < cap) {
+                out[n].global_reference = g;
+                out[n].last_event_time = 0.0;
+                out[n].x = x;
+                out[n].y = y;
+                out[n].index = i;
+                out[n].pad = 0;
+            }
+            ++n;
+        });
+        *n_out = n;
     });
 }
 

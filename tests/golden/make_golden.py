@@ -1,0 +1,300 @@
+"""Generates tests/golden/kat.json: known-answer vectors for the hot path.
+
+The values come from a pure-Python restatement of the reference's
+arithmetic, written independently of the C oracle, so that the oracle (and
+through it the GPU backend) is pinned by a second implementation:
+
+  * SeedableRng::seed_from_u64        necsim/core/src/cogs/rng.rs:33-63
+  * WyHash prime_with / sample_u64    necsim/impls/no-std/src/cogs/rng/wyhash.rs:53-119
+  * sample_uniform_closed_open        rng.rs:75-82
+  * PoissonEventTimeSampler           .../event_time_sampler/poisson.rs:30-109
+  * Box-Muller + clamp_round_dispersal  rng.rs:180-197, habitat/almost_infinite.rs:100-114
+  * LandscapeExtent iteration order   necsim/core/src/landscape/extent.rs:80-100, with the
+    reference's own test cases (extent.rs:110-160)
+  * full reference-schedule runs of tiny scenarios (monolithic/mod.rs:43-270)
+
+Run:  python tests/golden/make_golden.py
+"""
+import json
+import math
+import os
+import struct
+
+M64 = (1 << 64) - 1
+P0, P1, P2, P5 = 0xA0761D6478BD642F, 0xE7037ED1A0B428DB, 0x8EBC6AF09C88C6E3, 0xEB44ACCAB455D165
+K = 0x6EED0E9DA4D94A4F
+INV_PHI = 0x9E3779B97F4A7C15
+
+
+def seed_from_u64(state):
+    seed = b""
+    for _ in range(2):
+        state = (state * 6364136223846793005 + 11634580027462260723) & M64
+        xorshifted = (((state >> 18) ^ state) >> 27) & 0xFFFFFFFF
+        rot = state >> 59
+        x = ((xorshifted >> rot) | (xorshifted << ((32 - rot) % 32))) & 0xFFFFFFFF
+        seed += struct.pack("<I", x)
+    return struct.unpack("<Q", seed)[0]
+
+
+def diffuse(x):
+    x = (x * K) & M64
+    a, b = x >> 32, x >> 60
+    x ^= a >> b
+    return (x * K) & M64
+
+
+def wymum(a, b):
+    r = a * b
+    return (a ^ (r & M64)) ^ (b ^ (r >> 64))
+
+
+def rot32(v):
+    return ((v << 32) | (v >> 32)) & M64
+
+
+class Wy:
+    def __init__(self, seed):
+        self.seed = seed
+        self.state = seed
+
+    def prime(self, loc, t):
+        h = wymum(rot32(diffuse(loc)) ^ (self.seed ^ P0), rot32(diffuse(t)) ^ P2)
+        self.state = wymum(h, 16 ^ P5)
+
+    def u64(self):
+        self.state = (self.state + P0) & M64
+        return diffuse(wymum(self.state ^ P1, self.state))
+
+    def co(self):
+        return float(self.u64() >> 11) * 2.0 ** -53
+
+    def oc(self):
+        return float((self.u64() >> 11) + 1) * 2.0 ** -53
+
+
+def poisson_next(g, inj, t, lam, dt):
+    lam_dt = lam * dt
+    p0 = math.exp(-lam_dt)
+    ts = int(math.floor(t / dt))
+    while True:
+        g.prime(inj, ts)
+        n, prod, acc = 0, p0, p0
+        u = g.co()
+        while u > acc and prod > 0.0:
+            n += 1
+            prod *= lam_dt / float(n)
+            acc += prod
+        best = None
+        for k in range(n):
+            et = (float(ts) + g.co()) * dt
+            if et > t and (best is None or best[0] > et):
+                best = (et, k)
+        if best is not None:
+            break
+        ts += 1
+    reprime = (ts + INV_PHI * (best[1] + 1)) & M64
+    g.prime(inj, reprime)
+    return best[0], reprime
+
+
+def normal_dispersal(d0, d1, sigma, x, y):
+    u0 = float((d0 >> 11) + 1) * 2.0 ** -53
+    u1 = float(d1 >> 11) * 2.0 ** -53
+    r = math.sqrt(-2.0 * math.log(u0))
+    theta = -6.283185307179586 * u1
+    dx = (r * math.sin(theta)) * sigma + 0.0
+    dy = (r * math.cos(theta)) * sigma + 0.0
+
+    def rnd(v):  # f64::round: half away from zero (the subtraction below is exact)
+        a = abs(v)
+        f = math.floor(a)
+        r = int(f) + (1 if a - f >= 0.5 else 0)
+        return r if v >= 0 else -r
+
+    W = 1 << 32
+    return (x + rnd(dx)) % W, (y + rnd(dy)) % W
+
+
+def extent_iter(ox, oy, w, h):
+    """LandscapeExtent::iter (extent.rs:80-100) for width w and height h."""
+    out = []
+    for yy in range(h):
+        for xx in range(w):
+            out.append(((ox + xx) & 0xFFFFFFFF, (oy + yy) & 0xFFFFFFFF))
+    return out
+
+
+def circle_origins(cx, cy, r):
+    out = []
+    for (x, y) in extent_iter((cx - r) & 0xFFFFFFFF, (cy - r) & 0xFFFFFFFF, 2 * r + 1, 2 * r + 1):
+        dx = min((x - cx) & 0xFFFFFFFF, (cx - x) & 0xFFFFFFFF)
+        dy = min((y - cy) & 0xFFFFFFFF, (cy - y) & 0xFFFFFFFF)
+        if dx * dx + dy * dy <= r * r:
+            out.append((x, y))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Tiny end-to-end runs with the reference's Monolithic schedule (NonSpatial)
+# ---------------------------------------------------------------------------
+def fnv_sample(x, y, i, t, u):
+    h = 0xCBF29CE484222325
+    data = struct.pack("<IIIdd", x, y, i, t, u)
+    for b in data:
+        h ^= b
+        h = (h * 0x100000001B3) & M64
+    return h
+
+
+def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0,
+                             lam=0.5, dt=2.0):
+    g = Wy(seed_from_u64(seed))
+    lineages = []
+    for yy in range(h):
+        for xx in range(w):
+            for ii in range(deme):
+                lineages.append([((yy * w + xx) * deme + ii), 0.0, xx, yy, ii])
+    n = len(lineages)
+    slow = [(lin, lin[1]) for lin in lineages]
+    fast = []
+    es = max(int(n * event_slice), 1)
+    cap = int(n * dedup)
+    cache = [None] * cap
+    level = 0.0
+    steps = 0
+    max_time = 0.0
+    delivered = []
+    slow_ev = []
+
+    def inj(lin):
+        return ((lin[3] * w + lin[2]) * deme + lin[4])
+
+    while slow:
+        rate = 0.0
+        for _ in slow:
+            rate = rate + lam * nu
+        level = level + float(es) / rate
+        slow_ev.sort()
+        delivered += slow_ev
+        slow_ev = []
+        active = None
+        prev_next = None
+        prev_sample = None
+        while slow or active is not None:
+            nxt = None
+            while slow:
+                item = slow.pop(0)
+                if item[1] < level:
+                    nxt = item[0]
+                    break
+                fast.append(item)
+            prev_task, active = active, nxt
+            sample, prev_sample = prev_sample, None
+            if prev_task is not None and prev_next is not None:
+                dup = False
+                if sample is not None and cap > 0:
+                    idx = fnv_sample(*sample) % cap
+                    dup = cache[idx] == sample
+                    cache[idx] = sample
+                if not dup:
+                    (slow if prev_next < level else fast).append((prev_task, prev_next))
+            prev_next = None
+            if active is None:
+                continue
+            lin = active
+            k = 0
+            new_time = lin[1]
+            while True:
+                before = lin[1]
+                t, _ = poisson_next(g, inj(lin), before, lam, dt)
+                nt = t if t > before else struct.unpack("<d", struct.pack("<Q", struct.unpack("<Q", struct.pack("<d", before))[0] + 1))[0]
+                prev_next = nt
+                if k >= step_slice or nt >= level:
+                    break
+                new_time = nt
+                us = g.co()
+                if prev_sample is None or not (prev_sample[4] <= us):
+                    prev_sample = (lin[2], lin[3], lin[4], nt, us)
+                k += 1
+                if us < nu:
+                    slow_ev.append((nt, lin[2], lin[3], lin[4], lin[1], lin[0]))
+                    active = None
+                    break
+                idx = min(int(math.floor(g.co() * float(w * h))), w * h - 1)
+                tx, ty = idx % w, idx // w
+                ti = int(math.floor(g.co() * float(deme)))
+                lin = [lin[0], nt, tx, ty, ti]
+                active = lin
+            steps += k
+            max_time = max(max_time, new_time)
+        slow, fast = fast, []
+    slow_ev.sort()
+    delivered += slow_ev
+    species = 0
+    last = None
+    for e in delivered:
+        key = (e[0], e[1], e[2], e[3])
+        if key != last:
+            species += 1
+        last = key
+    return {"steps": steps, "time": max_time, "biodiversity": species,
+            "events": [[e[5], e[4], e[0], e[1], e[2], e[3]] for e in delivered]}
+
+
+def main():
+    kat = {}
+    kat["seed_from_u64"] = {str(s): seed_from_u64(s) for s in [0, 1, 7, 42, 2 ** 63 + 5, M64]}
+    kat["seahash_diffuse"] = {str(x): diffuse(x) for x in [0, 1, 12345, 2 ** 40 + 3, M64]}
+    kat["wymum"] = [[a, b, wymum(a, b)] for a, b in [(1, 2), (P0, P1), (M64, M64), (12345, 2 ** 63)]]
+    seqs = []
+    for seed, loc, t in [(seed_from_u64(42), 0, 0), (seed_from_u64(7), 123456, 17),
+                         (seed_from_u64(1), (5 << 32) | 9, 2 ** 63)]:
+        g = Wy(seed)
+        g.prime(loc, t)
+        seqs.append({"seed": seed, "location": loc, "time_index": t,
+                     "u64": [g.u64() for _ in range(8)]})
+    kat["wyhash_sequences"] = seqs
+    pois = []
+    for seed, inj, t in [(seed_from_u64(42), 0, 0.0), (seed_from_u64(42), 99, 3.5),
+                         (seed_from_u64(7), 2 ** 40, 1234.25), (seed_from_u64(1), 17, 1e6 + 0.5)]:
+        g = Wy(seed)
+        et, rp = poisson_next(g, inj, t, 0.5, 2.0)
+        pois.append({"seed": seed, "injection": inj, "time": t, "event_time": et,
+                     "event_time_bits": struct.unpack("<Q", struct.pack("<d", et))[0],
+                     "reprime": rp})
+    kat["poisson_next_event_time"] = pois
+    nd = []
+    g = Wy(seed_from_u64(3))
+    g.prime(1, 1)
+    for _ in range(64):
+        d0, d1 = g.u64(), g.u64()
+        for (x, y, sigma) in [(2 ** 31, 2 ** 31, 10.0), (0, 0, 3.5), (2 ** 32 - 1, 5, 100.0)]:
+            tx, ty = normal_dispersal(d0, d1, sigma, x, y)
+            nd.append([d0, d1, sigma, x, y, tx, ty])
+    kat["normal_dispersal"] = nd
+    m1, m2 = 0xFFFFFFFF, 0xFFFFFFFE
+    # the reference's own LandscapeExtent iteration tests (extent.rs:110-160)
+    kat["extent_iter"] = [
+        {"origin": [0, 0], "w": 1, "h": 1, "locations": extent_iter(0, 0, 1, 1)},
+        {"origin": [42, 24], "w": 4, "h": 2, "locations": extent_iter(42, 24, 4, 2)},
+        {"origin": [m2, m1], "w": 4, "h": 2, "locations": extent_iter(m2, m1, 4, 2)},
+    ]
+    kat["circle_origins"] = [
+        {"centre": [0, 0], "radius": 1, "locations": circle_origins(0, 0, 1)},
+        {"centre": [2 ** 31 - 1, 2 ** 31 - 1], "radius": 3,
+         "locations": circle_origins(2 ** 31 - 1, 2 ** 31 - 1, 3)},
+    ]
+    kat["nonspatial_runs"] = []
+    for (w, h, deme, nu, seed) in [(2, 2, 2, 0.05, 3), (4, 3, 2, 0.02, 42), (5, 5, 1, 0.1, 9)]:
+        r = nonspatial_reference_run(w, h, deme, nu, seed)
+        r.update({"width": w, "height": h, "deme": deme, "speciation": nu, "seed": seed})
+        kat["nonspatial_runs"].append(r)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kat.json")
+    with open(path, "w") as f:
+        json.dump(kat, f, indent=1)
+    print("wrote", path)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+"""GPU parity: the sm_100a backend against the oracle (marked gpu).
+
+Bit-exact contract:
+  * against the oracle's canonical schedule (the GPU's own schedule):
+    the full delivered speciation stream (global reference, prior time,
+    event time, origin), steps, time, rounds and dedup counts;
+  * against the oracle's reference schedule (the reference's Monolithic
+    Independent run): the species count and the sorted set of distinct
+    speciation events (event-time bits, x, y, index).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("gref", "prior_time", "event_time", "x", "y", "index")
+
+
+def same_stream(a, b):
+    if len(a) != len(b):
+        return False
+    for f in FIELDS:
+        x, y = a[f], b[f]
+        if x.dtype.kind == "f":
+            x, y = x.view(np.uint64), y.view(np.uint64)
+        if not np.array_equal(x, y):
+            return False
+    return True
+
+
+def run_gpu(nb, syn, desc, seed, algo=None, pause=None):
+    algo = algo or nb.CUDA()
+    with nb.Simulation(syn.to_scenario(desc), desc["speciation_probability"], algo) as sim:
+        return sim.simulate(seed, pause_before=pause)
+
+
+def check(nb, syn, oracle, desc, seed, algo=None, pause=None, reference=True):
+    algo = algo or nb.CUDA()
+    g = run_gpu(nb, syn, desc, seed, algo, pause)
+    c = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, step_slice=algo.step_slice,
+                        min_round_events=algo.min_round_events, pause_before=pause)
+    assert same_stream(g.speciation, c.speciation)
+    assert (g.steps, g.n_rounds, g.n_dedup, g.biodiversity) == (c.steps, c.n_rounds, c.n_dedup,
+                                                                 c.biodiversity)
+    assert np.float64(g.time).view(np.uint64) == np.float64(c.time).view(np.uint64)
+    assert g.paused == (c.status == 1) and g.n_remaining == c.n_remaining
+    if g.paused:
+        rem = np.sort(g.remaining, order="gref")
+        crem = np.sort(c.remaining, order="gref")
+        for f in ("gref", "x", "y", "index"):
+            assert np.array_equal(rem[f], crem[f])
+        assert np.array_equal(rem["last_event_time"].view(np.uint64),
+                              crem["last_event_time"].view(np.uint64))
+    if reference:
+        r = oracle.simulate(desc, seed, mode=oracle.MODE_REFERENCE, pause_before=pause)
+        assert g.biodiversity == r.biodiversity
+        assert np.array_equal(nb.distinct_speciation_set(g.speciation),
+                              oracle.distinct_speciation_set(r.speciation))
+    return g
+
+
+def se_desc(syn, w, h, nu, seed, maxv=20, sigma=2.0):
+    hab = syn.habitat_map(w, h, 0.15, maxv, seed)
+    return dict(kind=3, speciation_probability=nu, width=w, height=h, habitat=hab,
+                dispersal=syn.dispersal_map(hab, sigma))
+
+
+CASES = {
+    "ns_tiny": (dict(kind=0, speciation_probability=0.01, width=4, height=4, deme=2), 3),
+    "ns_deme1": (dict(kind=0, speciation_probability=0.005, width=30, height=20, deme=1), 11),
+    "ns_single": (dict(kind=0, speciation_probability=0.05, width=1, height=1, deme=1), 1),
+    "ns_nu_one": (dict(kind=0, speciation_probability=1.0, width=10, height=10, deme=3), 2),
+    "si": (dict(kind=1, speciation_probability=1e-3, width=1000, height=1, deme=1,
+                meta_width=100000, meta_height=1, meta_deme=1, migration_probability=0.1), 5),
+    "si_demes": (dict(kind=1, speciation_probability=5e-3, width=20, height=10, deme=3,
+                      meta_width=300, meta_height=7, meta_deme=2, migration_probability=0.3), 6),
+    "ai": (dict(kind=2, speciation_probability=1e-3, sigma=10.0, radius=30,
+                centre_x=0xFFFFFFFF // 2, centre_y=0xFFFFFFFF // 2), 7),
+    "ai_wrap": (dict(kind=2, speciation_probability=2e-3, sigma=3.0, radius=15, centre_x=2,
+                     centre_y=0xFFFFFFFF - 1), 8),
+    "ai_sigma0": (dict(kind=2, speciation_probability=0.01, sigma=0.0, radius=5, centre_x=100,
+                       centre_y=100), 9),
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_small_scenarios(nb, syn, oracle, name):
+    desc, seed = CASES[name]
+    check(nb, syn, oracle, desc, seed)
+
+
+@pytest.mark.parametrize("w,h,nu,seed", [(8, 8, 2e-3, 1), (16, 16, 1e-3, 2), (16, 8, 5e-3, 3)])
+def test_spatially_explicit_small(nb, syn, oracle, w, h, nu, seed):
+    check(nb, syn, oracle, se_desc(syn, w, h, nu, seed), seed)
+
+
+def test_config1_nonspatial_full(nb, syn, oracle):
+    desc, seed = syn.config1()
+    g = check(nb, syn, oracle, desc, seed)
+    assert g.n_initial == 100_000
+
+
+def test_config3_spatially_explicit_full(nb, syn, oracle):
+    desc, seed = syn.config3()
+    check(nb, syn, oracle, desc, seed)
+
+
+@pytest.mark.parametrize("algo_kw", [dict(min_round_events=1 << 12), dict(step_slice=3),
+                                     dict(block_size=64, grid_size=7), dict(rounds_per_graph=2),
+                                     dict(dedup_factor_pct=120)])
+def test_launch_and_schedule_parameters(nb, syn, oracle, algo_kw):
+    desc, seed = syn.config1()
+    check(nb, syn, oracle, desc, seed, algo=nb.CUDA(**algo_kw), reference=False)
+
+
+def test_launch_shape_does_not_change_output(nb, syn):
+    """Block/grid size and graph length only reorder work: identical streams."""
+    desc, seed = se_desc(syn, 16, 16, 1e-3, 4), 4
+    outs = [run_gpu(nb, syn, desc, seed, nb.CUDA(block_size=b, grid_size=g, rounds_per_graph=r))
+            for b, g, r in [(32, 1, 2), (128, 0, 16), (256, 3, 4)]]
+    for o in outs[1:]:
+        assert same_stream(o.speciation, outs[0].speciation)
+        assert o.steps == outs[0].steps
+
+
+@pytest.mark.parametrize("pause", [50.0, 500.0])
+def test_pause(nb, syn, oracle, pause):
+    desc, seed = syn.config1()
+    g = check(nb, syn, oracle, desc, seed, pause=pause)
+    assert g.paused and np.all(g.speciation["event_time"] < pause)
+
+
+def test_pause_resume_equals_straight_run(nb, syn):
+    desc, seed = CASES["ai"]
+    with nb.Simulation(syn.to_scenario(desc), desc["speciation_probability"]) as sim:
+        full = sim.simulate(seed)
+        first = sim.simulate(seed, pause_before=400.0)
+        rest = sim.resume(first.remaining, 400.0, seed)
+    both = np.unique(np.concatenate([nb.distinct_speciation_set(first.speciation),
+                                     nb.distinct_speciation_set(rest.speciation)]), axis=0)
+    assert np.array_equal(both, nb.distinct_speciation_set(full.speciation))
+
+
+def test_resume_matches_oracle(nb, syn, oracle):
+    desc, seed = CASES["si_demes"]
+    first = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, pause_before=100.0,
+                            min_round_events=1 << 20)
+    with nb.Simulation(syn.to_scenario(desc), desc["speciation_probability"]) as sim:
+        g = sim.resume(first.remaining, 100.0, seed)
+    c = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, lineages=first.remaining,
+                        resume_time=100.0, min_round_events=1 << 20)
+    assert same_stream(g.speciation, c.speciation)
+    assert g.steps == c.steps and g.time == c.time
+
+
+def test_batch_equals_single_runs(nb, syn):
+    sims = syn.config4(n_sims=6, max_local=3000)
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] * 100 for d, _ in sims]  # keep lifetimes short
+    seeds = [s for _, s in sims]
+    batch = nb.simulate_batch(scen, nus, seeds, collect=True)
+    for j in range(len(sims)):
+        single = nb.simulate(nus[j], scen[j], seeds[j])
+        assert same_stream(batch[j].speciation, single.speciation)
+        assert (batch[j].steps, batch[j].biodiversity, batch[j].n_rounds) == (
+            single.steps, single.biodiversity, single.n_rounds)

@@ -1,0 +1,81 @@
+"""The oracle against the known-answer vectors of tests/golden/kat.json
+(an independent pure-Python restatement, see make_golden.py) and the
+reference's own LandscapeExtent iteration tests (extent.rs:110-160)."""
+import numpy as np
+
+
+def test_seed_from_u64(oracle, kat):
+    for s, v in kat["seed_from_u64"].items():
+        assert oracle.seed_from_u64(int(s)) == v
+
+
+def test_seahash_and_wymum(oracle, kat):
+    L = oracle.lib()
+    for x, v in kat["seahash_diffuse"].items():
+        assert L.oracle_seahash_diffuse(int(x)) == v
+    for a, b, v in kat["wymum"]:
+        assert L.oracle_wymum(a, b) == v
+
+
+def test_wyhash_sequences(oracle, kat):
+    for case in kat["wyhash_sequences"]:
+        got = oracle.wyhash_sequence(case["seed"], case["location"], case["time_index"],
+                                     len(case["u64"]))
+        assert [int(v) for v in got] == case["u64"]
+
+
+def test_poisson_next_event_time(oracle, kat):
+    for case in kat["poisson_next_event_time"]:
+        t, rp = oracle.poisson_next_event_time(case["seed"], case["injection"], case["time"])
+        assert np.float64(t).view(np.uint64) == case["event_time_bits"]
+        assert rp == case["reprime"]
+        assert t > case["time"]
+
+
+def test_normal_dispersal(oracle, kat):
+    for d0, d1, sigma, x, y, tx, ty in kat["normal_dispersal"]:
+        assert oracle.normal_dispersal(d0, d1, sigma, x, y) == (tx, ty)
+
+
+def test_circle_origin_order(oracle, kat):
+    # the circle sampler walks a (possibly wrapping) LandscapeExtent
+    for case in kat["circle_origins"]:
+        desc = dict(kind=oracle.ALMOST_INFINITE_NORMAL, speciation_probability=0.1, sigma=1.0,
+                    centre_x=case["centre"][0], centre_y=case["centre"][1],
+                    radius=case["radius"])
+        o = oracle.enumerate_origins(desc)
+        assert [[int(a), int(b)] for a, b in zip(o["x"], o["y"])] == case["locations"]
+        assert list(o["gref"]) == [(y << 32) | x for x, y in case["locations"]]
+
+
+def test_extent_iteration_cases_present(kat):
+    # restated expectations of the reference's extent tests, incl. wrapping
+    m1, m2 = 0xFFFFFFFF, 0xFFFFFFFE
+    cases = kat["extent_iter"]
+    assert cases[0]["locations"] == [[0, 0]]
+    assert cases[1]["locations"][:5] == [[42, 24], [43, 24], [44, 24], [45, 24], [42, 25]]
+    assert cases[2]["locations"] == [[m2, m1], [m1, m1], [0, m1], [1, m1],
+                                     [m2, 0], [m1, 0], [0, 0], [1, 0]]
+
+
+def test_nonspatial_reference_runs(oracle, kat):
+    """Full reference-schedule runs of tiny NonSpatial scenarios: steps,
+    time, species and the delivered speciation stream."""
+    for case in kat["nonspatial_runs"]:
+        desc = dict(kind=oracle.NON_SPATIAL, speciation_probability=case["speciation"],
+                    width=case["width"], height=case["height"], deme=case["deme"])
+        r = oracle.simulate(desc, case["seed"], mode=oracle.MODE_REFERENCE)
+        assert r.steps == case["steps"]
+        assert r.time == case["time"]
+        assert r.biodiversity == case["biodiversity"]
+        got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
+                int(e["y"]), int(e["index"])] for e in r.speciation]
+        assert got == case["events"]
+
+
+def test_nonspatial_origin_order(oracle):
+    o = oracle.enumerate_origins(dict(kind=0, speciation_probability=0.1, width=3, height=2,
+                                      deme=2))
+    assert list(o["gref"]) == list(range(12))
+    assert list(zip(o["x"], o["y"], o["index"]))[:5] == [(0, 0, 0), (0, 0, 1), (1, 0, 0),
+                                                         (1, 0, 1), (2, 0, 0)]
