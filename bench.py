@@ -1,0 +1,350 @@
+"""Benchmark: events/sec of the B200 Independent-algorithm backend.
+
+Workload (default): the batched sweep of 256 SpatiallyImplicit simulations
+(local community J = floor(10^U(3,6)) cells of deme 1, metacommunity 1e7
+cells, migration U(0.01, 0.2), speciation 10^U(-6,-3), seeds 0..255) run
+to completion in one batched launch per round.  One step = one full batch.
+
+  value      events/sec with the origins resident in HBM (device time of the
+             whole batch measured with CUDA events by the library, max over
+             ranks), events = executed lineage steps
+  e2e        the same metric through the public C ABI call
+             necsim_gpu_simulate_batch with host buffers: scenario set-up,
+             host->device origin upload, simulation, device->host events
+  roofline   the step kernel's algorithmic bytes per launch / its average
+             launch time, against the measured HBM copy bandwidth
+  cpu_baseline  the CPU restatement of the reference's Independent
+             algorithm on a bounded sample of the same workload
+
+`--impl reference` times that CPU restatement alone (all host cores) and
+prints its line.  Multi-GPU (`--gpus N` under torchrun) runs N independent
+replicas of the batch (weak scaling, no data-path collective).
+"""
+import argparse
+import concurrent.futures
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "events/sec on 1 B200: learned-scheduled vs plain independent kernel, bit-exact"
+UNIT = "events/s"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="c4", choices=["c4", "c5", "c2", "c3", "c1"])
+    p.add_argument("--schedule", default="plain", choices=["plain", "learned"])
+    p.add_argument("--cpu-sample-pause", type=float, default=400.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+def workload(name):
+    """(description, list of (scenario dict, seed))"""
+    syn = importlib.import_module("necsim-rust_b200.synthetic")
+    if name == "c4":
+        return ("256 x SpatiallyImplicit sweep: J=floor(10^U(3,6)) deme 1, meta 1e7 deme 1, "
+                "migration U(0.01,0.2), speciation 10^U(-6,-3), seeds 0..255", syn.config4())
+    if name == "c5":
+        d, s = syn.config5()
+        return ("SpatiallyExplicit 128x128 habitat (0 w.p. 0.2 else U{1..500}), dense "
+                "16384^2 Gaussian sigma=4 dispersal, speciation 1e-6, seed %d" % s, [(d, s)])
+    if name == "c3":
+        d, s = syn.config3()
+        return ("SpatiallyExplicit 64x64 habitat, dense 4096^2 dispersal, speciation 1e-4, seed 1",
+                [(d, s)])
+    if name == "c2":
+        d, s = syn.config2()
+        return ("AlmostInfinite circle r=100, Normal sigma=10, speciation 1e-5, seed 7", [(d, s)])
+    d, s = syn.config1()
+    return ("NonSpatial 100x100 deme 10, speciation 1e-3, seed 42", [(d, s)])
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.torch = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as td
+            self.torch = torch
+            torch.cuda.set_device(self.local_rank)
+            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                  device_id=torch.device("cuda", self.local_rank))
+            self.td = td
+
+    def barrier(self):
+        if self.torch is not None:
+            self.td.barrier()
+
+    def max(self, v):
+        if self.torch is None:
+            return v
+        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device="cuda")
+        self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if self.torch is None:
+            return v
+        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device="cuda")
+        self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.torch is not None:
+            self.td.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement of the reference (bounded sample)
+# ---------------------------------------------------------------------------
+def cpu_sample(sims, pause, threads):
+    """Runs the reference-faithful CPU restatement on every simulation of the
+    workload up to time `pause` (a bounded sample), `threads` at a time.
+    Returns (events, seconds)."""
+    import oracle
+
+    def one(item):
+        d, seed = item
+        return oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause).steps
+
+    oracle.lib()
+    t0 = time.perf_counter()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as ex:
+        steps = sum(ex.map(one, sims))
+    return steps, time.perf_counter() - t0
+
+
+def cpu_sample_desc(name, pause, n):
+    return "%s: all %d simulation(s) advanced to t=%g (pause_before) with the reference schedule" % (
+        name, n, pause)
+
+
+def reference_arm(args, dist):
+    if dist.rank != 0:
+        dist.close()
+        return
+    desc, sims = workload(args.workload)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_sample(sims, args.cpu_sample_pause, threads)
+    ev, sec = 0, 0.0
+    for _ in range(args.steps):
+        e, s = cpu_sample(sims, args.cpu_sample_pause, threads)
+        ev += e
+        sec += s
+    value = ev / sec
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
+        "data": "synthetic", "config": {"workload": desc, "schedule": "reference Monolithic"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
+                                                   len(sims))},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    dist.close()
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    if args.impl == "reference":
+        return reference_arm(args, dist)
+
+    nb = importlib.import_module("necsim-rust_b200")
+    syn = importlib.import_module("necsim-rust_b200.synthetic")
+    desc, sims = workload(args.workload)
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] for d, _ in sims]
+    seeds = [s for _, s in sims]
+    algo = nb.CUDA(schedule=args.schedule, device=dist.local_rank if dist.world > 1 else 0)
+    se = sims[0][0]["kind"] == 3
+    kind = sims[0][0]["kind"]
+
+    batch = nb.Batch(scen, nus, seeds, algo)
+    for _ in range(args.warmup):
+        batch.run()
+
+    clocks = Clocks(dist.local_rank)
+    dist.barrier()
+    clocks.start()
+    steps = 0
+    dev_ms = 0.0
+    kernel_ms = 0.0
+    step_launches = 0
+    visits = 0
+    launches = 0
+    n_spec = 0
+    for _ in range(args.steps):
+        outs = batch.run()
+        o0 = outs[0]
+        steps += sum(o.steps for o in outs)
+        n_spec += sum(o.n_speciation for o in outs)
+        dev_ms += o0.total_ms          # device time of the whole batch (CUDA events)
+        kernel_ms += o0.kernel_ms      # step-kernel time (CUDA events around each launch)
+        step_launches += o0.n_step_launches
+        visits += o0.lineage_visits
+        launches += o0.n_launches
+    dist.barrier()
+    clk = clocks.stop()
+    batch.close()
+
+    # end to end through the public C ABI with host buffers
+    e2e_steps, e2e_sec, h2d, d2h = 0, 0.0, 0, 0
+    for _ in range(args.steps):
+        dist.barrier()
+        t0 = time.perf_counter()
+        outs = nb.simulate_batch(scen, nus, seeds, algo)
+        dt = time.perf_counter() - t0
+        e2e_sec += dist.max(dt)
+        e2e_steps += sum(o.steps for o in outs)
+        h2d += outs[0].h2d_bytes
+        d2h += outs[0].d2h_bytes
+
+    max_ms = dist.max(dev_ms)
+    total_steps = dist.sum(steps)
+    value = total_steps / (max_ms / 1e3)
+    e2e_value = dist.sum(e2e_steps) / e2e_sec
+
+    # roofline of the step kernel: algorithmic bytes = lineage state read and
+    # written per visit (4 u32 + 5 u64/f64 + 1 flag, 57 B each way), speciation
+    # events written (40 B) and, for SpatiallyExplicit, one 32-B cell record
+    # and one 32-B atom sector per event
+    state_bytes = 2 * 57
+    alg_bytes = visits * state_bytes + n_spec * 40 + (steps * 64 if se else 0)
+    avg_launch_ms = kernel_ms / max(step_launches, 1)
+    per_launch_bytes = alg_bytes / max(step_launches, 1)
+    achieved = per_launch_bytes / (avg_launch_ms / 1e3) / 1e9 if avg_launch_ms > 0 else 0.0
+    peak, peak_kind = load_peaks()
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "step_kernel_%s_traffic.json" % args.workload)
+    if os.path.exists(prof):
+        try:
+            with open(prof) as f:
+                t = json.load(f)
+            traffic = t["dram_bytes_per_lineage_visit"] * visits / max(step_launches, 1)
+        except Exception:
+            traffic = None
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
+        "data": "synthetic",
+        "config": {"workload": desc, "schedule": args.schedule, "kind": kind,
+                   "simulations": len(sims), "lineages": int(sum(o.n_initial for o in outs)),
+                   "l2": "inputs larger than L2 (lineage state %.2f GB)" % (
+                       sum(o.n_initial for o in outs) * 57 * 2 / 1e9),
+                   "parallelism": "replicas" if dist.world > 1 else "single"},
+        "events_per_step": steps / args.steps,
+        "clocks": clk,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                "d2h_bytes_per_step": d2h / args.steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                     "kernel": "step_kernel", "avg_launch_ms": avg_launch_ms,
+                     "launches": step_launches},
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads)
+        line["cpu_baseline"] = {"value": ev / sec, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
+                                                          len(sims))}
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -76,6 +76,7 @@ typedef struct necsim_args {
     uint64_t step_slice;       /* expected events per lineage between dedup passes; default 10 */
     uint64_t min_round_events; /* a round runs at least this many expected events in total
                                   (widens rounds when few lineages are left); default 2^20 */
+    uint64_t step_slice_max;   /* cap on expected events per lineage per round; default 1024 */
     uint32_t block_size;       /* threads per block of the step kernel; 0 = autotuned */
     uint32_t grid_size;        /* blocks of the step kernel; 0 = autotuned */
     uint32_t dedup_factor_pct; /* dedup hash table load: slots = next_pow2(n*pct/100); default 200 */
@@ -141,6 +142,10 @@ typedef struct necsim_outcome {
     uint64_t n_launches;       /* kernels launched by this call */
     double kernel_ms;          /* device time of the step kernel (CUDA events) */
     double total_ms;           /* device time of the whole simulation (CUDA events) */
+    uint64_t h2d_bytes;        /* host-to-device bytes copied by the call */
+    uint64_t d2h_bytes;        /* device-to-host bytes copied by the call */
+    uint64_t n_step_launches;  /* step-kernel launches (one per round) */
+    uint64_t lineage_visits;   /* lineage slots the step kernels processed */
 } necsim_outcome;
 
 typedef struct necsim_ctx necsim_ctx;
@@ -186,6 +191,24 @@ int necsim_gpu_simulate_batch(const necsim_scenario *scenarios, const uint64_t *
                               uint32_t n_sims, const necsim_args *args, double pause_before,
                               const necsim_reporter *reporters, necsim_outcome *outcomes,
                               char *error, size_t error_cap);
+
+/* Resident batch: the same batch as necsim_gpu_simulate_batch split into a
+ * set-up call (validation, tables, origin lineages uploaded once and kept
+ * in device memory, CUDA graph captured) and runs that restart from the
+ * resident origins with no host-to-device lineage copy.  Each run simulates
+ * every simulation from its origins with its seed; runs are identical.
+ * No reference counterpart: it is `n_sims` calls of
+ * `Algorithm::initialise_and_simulate` with the set-up hoisted out.
+ * On failure *out may still receive an object carrying the message
+ * (necsim_gpu_batch_last_error); destroy it with necsim_gpu_batch_destroy. */
+typedef struct necsim_batch necsim_batch;
+int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds,
+                            uint32_t n_sims, const necsim_args *args, double pause_before,
+                            necsim_batch **out);
+int necsim_gpu_batch_run(necsim_batch *batch, const necsim_reporter *reporters,
+                         necsim_outcome *outcomes);
+const char *necsim_gpu_batch_last_error(const necsim_batch *batch);
+void necsim_gpu_batch_destroy(necsim_batch *batch);
 
 const char *necsim_gpu_last_error(const necsim_ctx *ctx);
 void necsim_gpu_destroy(necsim_ctx *ctx);

@@ -59,7 +59,8 @@ class CScenario(ctypes.Structure):
 class CArgs(ctypes.Structure):
     _fields_ = [
         ("delta_t", ctypes.c_double), ("step_slice", ctypes.c_uint64),
-        ("min_round_events", ctypes.c_uint64), ("block_size", ctypes.c_uint32),
+        ("min_round_events", ctypes.c_uint64), ("step_slice_max", ctypes.c_uint64),
+        ("block_size", ctypes.c_uint32),
         ("grid_size", ctypes.c_uint32), ("dedup_factor_pct", ctypes.c_uint32),
         ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
@@ -75,7 +76,9 @@ class COutcome(ctypes.Structure):
         ("biodiversity", ctypes.c_uint64), ("n_dispersal", ctypes.c_uint64),
         ("n_rounds", ctypes.c_uint64), ("n_dedup", ctypes.c_uint64),
         ("n_launches", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
-        ("total_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64), ("n_step_launches", ctypes.c_uint64),
+        ("lineage_visits", ctypes.c_uint64),
     ]
 
 
@@ -107,7 +110,8 @@ SYMBOLS = [
     "necsim_abi_version", "necsim_seed_from_u64", "necsim_gpu_create", "necsim_gpu_simulate",
     "necsim_gpu_simulate_lineages", "necsim_gpu_remaining_lineages",
     "necsim_gpu_simulate_batch", "necsim_gpu_last_error", "necsim_gpu_destroy",
-    "necsim_build_tables", "necsim_enumerate_origins",
+    "necsim_build_tables", "necsim_enumerate_origins", "necsim_gpu_batch_create",
+    "necsim_gpu_batch_run", "necsim_gpu_batch_last_error", "necsim_gpu_batch_destroy",
 ]
 
 _lib = None
@@ -149,6 +153,15 @@ def lib():
     L.necsim_build_tables.restype = ctypes.c_int
     L.necsim_enumerate_origins.argtypes = [P(CScenario), vp, u64, P(u64)]
     L.necsim_enumerate_origins.restype = ctypes.c_int
+    L.necsim_gpu_batch_create.argtypes = [P(CScenario), P(u64), ctypes.c_uint32, P(CArgs),
+                                          ctypes.c_double, P(vp)]
+    L.necsim_gpu_batch_create.restype = ctypes.c_int
+    L.necsim_gpu_batch_run.argtypes = [vp, vp, P(COutcome)]
+    L.necsim_gpu_batch_run.restype = ctypes.c_int
+    L.necsim_gpu_batch_last_error.argtypes = [vp]
+    L.necsim_gpu_batch_last_error.restype = ctypes.c_char_p
+    L.necsim_gpu_batch_destroy.argtypes = [vp]
+    L.necsim_gpu_batch_destroy.restype = None
     if L.necsim_abi_version() != 1:
         raise ImportError("libnecsim_b200.so ABI version mismatch")
     _lib = L
@@ -216,6 +229,7 @@ class CUDA:
     block_size: int = 0
     grid_size: int = 0
     min_round_events: int = 1 << 20
+    step_slice_max: int = 1024
     dedup_factor_pct: int = 200
     schedule: str = "plain"   # or "learned"
     device: int = 0
@@ -239,6 +253,10 @@ class Outcome:
     n_launches: int
     kernel_ms: float
     total_ms: float
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
+    n_step_launches: int = 0
+    lineage_visits: int = 0
     speciation: Optional[np.ndarray] = None
     remaining: Optional[np.ndarray] = None
 
@@ -291,6 +309,7 @@ def _args_struct(algorithm: CUDA):
     a.delta_t = algorithm.delta_t
     a.step_slice = algorithm.step_slice
     a.min_round_events = algorithm.min_round_events
+    a.step_slice_max = algorithm.step_slice_max
     a.block_size = algorithm.block_size
     a.grid_size = algorithm.grid_size
     a.dedup_factor_pct = algorithm.dedup_factor_pct
@@ -328,7 +347,7 @@ class _Collector:
 def _outcome(o: COutcome, spec=None, remaining=None) -> Outcome:
     return Outcome(bool(o.paused), o.time, o.steps, o.n_initial, o.n_remaining, o.n_speciation,
                    o.biodiversity, o.n_rounds, o.n_dedup, o.n_launches, o.kernel_ms, o.total_ms,
-                   spec, remaining)
+                   o.h2d_bytes, o.d2h_bytes, o.n_step_launches, o.lineage_visits, spec, remaining)
 
 
 class Simulation:
@@ -448,6 +467,63 @@ def simulate_batch(scenarios: Sequence, speciations: Sequence[float], seeds: Seq
     if rc != 0:
         raise NecsimError(rc, err.value.decode())
     return [_outcome(outs[j], cols[j].events() if cols else None) for j in range(n)]
+
+
+class Batch:
+    """A resident batch of independent simulations (one scenario kind): the
+    set-up (tables, origins, CUDA graph) happens once, `run()` re-simulates
+    all of them from their origins on the device."""
+
+    def __init__(self, scenarios: Sequence, speciations: Sequence[float], seeds: Sequence[int],
+                 algorithm: Optional[CUDA] = None, pause_before: Optional[float] = None):
+        L = lib()
+        n = len(scenarios)
+        self.n = n
+        self._structs = (CScenario * n)()
+        self._keep = []
+        for j, (sc, nu) in enumerate(zip(scenarios, speciations)):
+            c = _scenario_struct(sc, nu)
+            self._keep.append(c)
+            self._structs[j] = c
+        self._seeds = (ctypes.c_uint64 * n)(*[seed_from_u64(s) for s in seeds])
+        self._args = _args_struct(algorithm or CUDA())
+        pb = -1.0 if pause_before is None else float(pause_before)
+        b = ctypes.c_void_p()
+        rc = L.necsim_gpu_batch_create(self._structs, self._seeds, n, ctypes.byref(self._args), pb,
+                                       ctypes.byref(b))
+        self._b = b
+        if rc != 0:
+            msg = L.necsim_gpu_batch_last_error(b).decode() if b.value else ""
+            self.close()
+            raise NecsimError(rc, msg)
+
+    def run(self, collect: bool = False) -> List[Outcome]:
+        L = lib()
+        outs = (COutcome * self.n)()
+        cols = [_Collector() for _ in range(self.n)] if collect else None
+        reps = (CReporter * self.n)(*[c.struct for c in cols]) if collect else None
+        rc = L.necsim_gpu_batch_run(self._b, ctypes.cast(reps, ctypes.c_void_p) if reps else None,
+                                    outs)
+        if rc != 0:
+            raise NecsimError(rc, L.necsim_gpu_batch_last_error(self._b).decode())
+        return [_outcome(outs[j], cols[j].events() if cols else None) for j in range(self.n)]
+
+    def close(self):
+        if getattr(self, "_b", None) is not None and self._b.value:
+            lib().necsim_gpu_batch_destroy(self._b)
+        self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def build_tables(scenario: SpatiallyExplicit):

@@ -75,6 +75,36 @@ struct Rng {
     }
 };
 
+// ---- counter form of the same generator ----
+// After prime_with the k-th sample_u64 (k = 1, 2, ...) only depends on the
+// primed state s0: state_k = s0 + k * P0 (wrapping).  Computing the samples
+// of one event from s0 independently, instead of one after the other, gives
+// the same values with the 64-bit multiply chains overlapped.
+
+// the location half of prime_with: rotate(diffuse(location)) ^ seed ^ P0
+__device__ __forceinline__ uint64_t location_term(uint64_t seed, uint64_t location_index) {
+    return swap_halves(seahash_diffuse(location_index)) ^ (seed ^ kWyP0);
+}
+
+// WyHash state after prime_with(location, time_index), from the location term
+__device__ __forceinline__ uint64_t primed_state(uint64_t loc_term, uint64_t time_index) {
+    const uint64_t h = wymum(loc_term, swap_halves(seahash_diffuse(time_index)) ^ kWyP2);
+    return wymum(h, 16ULL ^ kWyP5);
+}
+
+// the k-th sample_u64 after priming to s0
+__device__ __forceinline__ uint64_t draw_at(uint64_t s0, uint32_t k) {
+    const uint64_t s = s0 + (uint64_t)k * kWyP0;
+    return seahash_diffuse(wymum(s ^ kWyP1, s));
+}
+
+__device__ __forceinline__ double unit_closed_open(uint64_t v) {
+    return __dmul_rn(__ull2double_rn(v >> 11), 0x1.0p-53);
+}
+__device__ __forceinline__ double unit_open_closed(uint64_t v) {
+    return __dmul_rn(__ull2double_rn((v >> 11) + 1ULL), 0x1.0p-53);
+}
+
 // Rust `f64 as u64` for the non-negative finite values these call sites see
 // (floor of a product of a unit sample and a table length, or of t / dt);
 // saturates like Rust above range.
@@ -115,21 +145,28 @@ __device__ __forceinline__ double max_after(double before, double value) {
 // per-run constant computed on the host with the system libm (the
 // reference's IntrinsicsMathsCore); p0 == 0 is rejected at set-up.
 __device__ __forceinline__ double poisson_next_event_time(Rng &g, uint64_t inj, double time,
-                                                          double delta_t, double lambda_dt,
-                                                          double p0, uint64_t &reprime) {
-    uint64_t time_step = f64_to_u64(floor(__ddiv_rn(time, delta_t)));
+                                                          const SimParams &p, uint64_t &reprime) {
+    const double delta_t = p.delta_t;
+    // floor(time / delta_t); with a power-of-two delta_t the product with the
+    // exact reciprocal is the same correctly rounded quotient
+    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, delta_t);
+    uint64_t time_step = f64_to_u64(floor(q));
     double best;
     uint32_t best_k;
     for (;;) {
         g.prime(inj, time_step);
         // Devroye's sequential inversion of Poisson(lambda * delta_t)
         uint32_t n_events = 0;
-        double prod = p0;
-        double acc = p0;
+        double prod = p.p0;
+        double acc = p.p0;
         const double u = g.closed_open();
         while (u > acc && prod > 0.0) {
             n_events += 1;
-            prod = __dmul_rn(prod, __ddiv_rn(lambda_dt, __uint2double_rn(n_events)));
+            // lambda_dt / n: host-divided table for small n, same IEEE quotient
+            const double ratio = n_events <= (uint32_t)kPoissonTable
+                                     ? p.lambda_dt_over_k[n_events - 1]
+                                     : __ddiv_rn(p.lambda_dt, __uint2double_rn(n_events));
+            prod = __dmul_rn(prod, ratio);
             acc = __dadd_rn(acc, prod);
         }
         bool found = false;
@@ -150,6 +187,84 @@ __device__ __forceinline__ double poisson_next_event_time(Rng &g, uint64_t inj, 
     reprime = time_step + kInvPhi * (uint64_t)(best_k + 1);
     g.prime(inj, reprime);
     return best;
+}
+
+// One bucket of the Poisson sampler (poisson.rs:50-95) primed to s0: the
+// earliest event strictly after `time` (ties: lowest index), or -1.  The
+// Devroye uniform and the first two event-time uniforms are drawn up front.
+__device__ __forceinline__ int poisson_bucket(uint64_t s0, uint64_t time_step, double time,
+                                              const SimParams &p, double &best) {
+    const uint64_t d1 = draw_at(s0, 1);
+    const uint64_t d2 = draw_at(s0, 2);
+    const uint64_t d3 = draw_at(s0, 3);
+    // Devroye's loop on the constant acc_n sequence: the ranks passed are the
+    // leading thresholds below X (thresholds are non-decreasing, alive bits a
+    // prefix), so the count equals the loop's exit rank
+    const uint64_t X = d1 >> 11;
+    uint32_t n_events = 0;
+#pragma unroll
+    for (int n = 0; n < kPoissonThresholds; ++n) n_events += (X > p.poisson_threshold[n]) ? 1u : 0u;
+    const uint32_t alive = (uint32_t)__popc(p.poisson_alive);
+    if (alive < n_events) n_events = alive;
+    if (n_events == (uint32_t)kPoissonThresholds) {
+        // continue the reference loop beyond the tabulated ranks
+        const double u = unit_closed_open(d1);
+        double prod = p.poisson_prod_k;
+        double acc = p.poisson_acc_k;
+        while (u > acc && prod > 0.0) {
+            n_events += 1;
+            const double ratio = n_events <= (uint32_t)kPoissonTable
+                                     ? p.lambda_dt_over_k[n_events - 1]
+                                     : __ddiv_rn(p.lambda_dt, __uint2double_rn(n_events));
+            prod = __dmul_rn(prod, ratio);
+            acc = __dadd_rn(acc, prod);
+        }
+    }
+    if (n_events == 0) return -1;
+    // event times (t_s + u_k) * delta_t; non-negative doubles compare like
+    // their bit patterns
+    const double step_start = __ull2double_rn(time_step);
+    const long long time_bits = __double_as_longlong(time);
+    int best_k = -1;
+    long long best_bits = 0;
+    for (uint32_t k = 0; k < n_events; ++k) {
+        const uint64_t d = k == 0 ? d2 : (k == 1 ? d3 : draw_at(s0, k + 2));
+        const double et = __dmul_rn(__dadd_rn(step_start, unit_closed_open(d)), p.delta_t);
+        const long long eb = __double_as_longlong(et);
+        if (eb > time_bits && (best_k < 0 || best_bits > eb)) {
+            best_bits = eb;
+            best_k = (int)k;
+        }
+    }
+    best = __longlong_as_double(best_bits);
+    return best_k;
+}
+
+// poisson_next_event_time in counter form: buckets are primed two at a time
+// (the second speculatively) from the shared location term.  Returns the
+// event time, the re-prime time index and the re-primed state.
+__device__ __forceinline__ double poisson_next_event_time_ilp(uint64_t loc_term, double time,
+                                                              const SimParams &p,
+                                                              uint64_t &reprime,
+                                                              uint64_t &reprimed_state) {
+    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
+    uint64_t time_step = f64_to_u64(floor(q));
+    for (;;) {
+        const uint64_t s0 = primed_state(loc_term, time_step);
+        const uint64_t s1 = primed_state(loc_term, time_step + 1);
+        double best = 0.0;
+        int k = poisson_bucket(s0, time_step, time, p, best);
+        if (k < 0) {
+            time_step += 1;
+            k = poisson_bucket(s1, time_step, time, p, best);
+        }
+        if (k >= 0) {
+            reprime = time_step + kInvPhi * (uint64_t)(k + 1);
+            reprimed_state = primed_state(loc_term, reprime);
+            return best;
+        }
+        time_step += 1;
+    }
 }
 
 // habitat/almost_infinite.rs:100-114 clamp_round_dispersal of a Box-Muller
@@ -177,9 +292,72 @@ __device__ __forceinline__ void normal_dispersal(Rng &g, double sigma, uint32_t 
 // dispersal_sampler/non_spatial.rs:42-66 over an extent (ox, oy, w, h)
 __device__ __forceinline__ void non_spatial_dispersal(Rng &g, uint32_t ox, uint32_t oy, uint64_t w,
                                                       uint64_t h, uint32_t &tx, uint32_t &ty) {
-    const uint64_t idx = sample_index_u64(g, w * h);
-    tx = ox + (uint32_t)(idx % w);
-    ty = oy + (uint32_t)(idx / w);
+    const uint64_t n = w * h;
+    const uint64_t idx = sample_index_u64(g, n);
+    if (h == 1) {  // idx < w: quotient 0
+        tx = ox + (uint32_t)idx;
+        ty = oy;
+    } else if (n <= 0xffffffffULL) {  // 32-bit divide (same quotient)
+        const uint32_t i32 = (uint32_t)idx, w32 = (uint32_t)w;
+        const uint32_t q = i32 / w32;
+        tx = ox + (i32 - q * w32);
+        ty = oy + q;
+    } else {
+        tx = ox + (uint32_t)(idx % w);
+        ty = oy + (uint32_t)(idx / w);
+    }
+}
+
+// ---- the same samplers fed with pre-drawn samples ----
+
+// rng.rs:133-145 sample_index_u64 of one sample
+__device__ __forceinline__ uint64_t index_from_draw(uint64_t d, uint64_t length) {
+    const uint64_t index = f64_to_u64(floor(__dmul_rn(unit_closed_open(d), __ull2double_rn(length))));
+    return index < length - 1 ? index : length - 1;
+}
+
+// dispersal_sampler/non_spatial.rs:42-66
+__device__ __forceinline__ void non_spatial_dispersal_draw(uint64_t d, uint32_t ox, uint32_t oy,
+                                                           uint64_t w, uint64_t h, uint32_t &tx,
+                                                           uint32_t &ty) {
+    const uint64_t n = w * h;
+    const uint64_t idx = index_from_draw(d, n);
+    if (h == 1) {  // idx < w: quotient 0
+        tx = ox + (uint32_t)idx;
+        ty = oy;
+    } else if (n <= 0xffffffffULL) {  // 32-bit divide (same quotient)
+        const uint32_t i32 = (uint32_t)idx, w32 = (uint32_t)w;
+        const uint32_t q = i32 / w32;
+        tx = ox + (i32 - q * w32);
+        ty = oy + q;
+    } else {
+        tx = ox + (uint32_t)(idx % w);
+        ty = oy + (uint32_t)(idx / w);
+    }
+}
+
+// core/src/cogs/coalescence_sampler.rs:59-78: floor(u * habitat) as u32
+__device__ __forceinline__ uint32_t coalescence_index(uint64_t d, uint32_t habitat) {
+    return f64_to_u32(floor(__dmul_rn(unit_closed_open(d), __uint2double_rn(habitat))));
+}
+
+// rng.rs:180-197 + almost_infinite.rs:100-114 from the two Box-Muller samples
+__device__ __forceinline__ void normal_dispersal_draw(uint64_t d0, uint64_t d1, double sigma,
+                                                      uint32_t x, uint32_t y, uint32_t &tx,
+                                                      uint32_t &ty) {
+    const double u0 = unit_open_closed(d0);
+    const double u1 = unit_closed_open(d1);
+    const double r = __dsqrt_rn(__dmul_rn(-2.0, log(u0)));
+    const double theta = __dmul_rn(-kTau, u1);
+    const double z0 = __dmul_rn(r, sin(theta));
+    const double z1 = __dmul_rn(r, cos(theta));
+    const double dx = __dadd_rn(__dmul_rn(z0, sigma), 0.0);
+    const double dy = __dadd_rn(__dmul_rn(z1, sigma), 0.0);
+    const int64_t wrap = (int64_t)1 << 32;
+    const int64_t nx = ((int64_t)x + f64_to_i64(round(dx))) % wrap;
+    const int64_t ny = ((int64_t)y + f64_to_i64(round(dy))) % wrap;
+    tx = (uint32_t)((nx + wrap) % wrap);
+    ty = (uint32_t)((ny + wrap) % wrap);
 }
 
 // landscape/extent.rs:44-49 LandscapeExtent::contains for the SI local

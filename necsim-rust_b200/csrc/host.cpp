@@ -154,6 +154,31 @@ SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64
     }
     p.step_slice = args.step_slice;
     p.min_round_events = args.min_round_events;
+    p.step_slice_max = args.step_slice_max;
+    // floor(t / delta_t) is computed as floor(t * (1 / delta_t)) when delta_t
+    // is a power of two: both round the same exact quotient
+    int exp2 = 0;
+    const double mant = std::frexp(p.delta_t, &exp2);
+    p.inv_delta_t = (mant == 0.5) ? 1.0 / p.delta_t : 0.0;
+    // lambda * delta_t / k for the first Poisson ranks (poisson.rs:58),
+    // divided here with the same IEEE division the reference performs
+    for (int k = 1; k <= kPoissonTable; ++k) p.lambda_dt_over_k[k - 1] = p.lambda_dt / (double)k;
+    // the constant Devroye sequence (poisson.rs:51-65) as integer thresholds
+    {
+        double prod = p.p0, acc = p.p0;
+        p.poisson_alive = 0;
+        for (int n = 0; n < kPoissonThresholds; ++n) {
+            p.poisson_threshold[n] = (uint64_t)std::floor(std::ldexp(acc, 53));
+            if (prod > 0.0) p.poisson_alive |= 1u << n;
+            prod = prod * (p.lambda_dt / (double)(n + 1));
+            acc = acc + prod;
+        }
+        p.poisson_prod_k = prod;
+        p.poisson_acc_k = acc;
+    }
+    // u < c  <=>  X < ceil(c * 2^53) for the 53-bit integer X of the uniform
+    p.nu_threshold = (uint64_t)std::ceil(std::ldexp(sc.speciation_probability, 53));
+    p.migration_threshold = (uint64_t)std::ceil(std::ldexp(sc.migration_probability, 53));
     p.pause_before = -1.0;
     return p;
 }
@@ -165,6 +190,8 @@ necsim_args with_defaults(const necsim_args *in) {
     if (!(a.delta_t > 0.0)) a.delta_t = 2.0;
     if (a.step_slice == 0) a.step_slice = 10;
     if (a.min_round_events == 0) a.min_round_events = 1ULL << 20;
+    if (a.step_slice_max == 0) a.step_slice_max = 1024;
+    if (a.step_slice_max < a.step_slice) a.step_slice_max = a.step_slice;
     if (a.dedup_factor_pct == 0) a.dedup_factor_pct = 200;
     if (a.dedup_factor_pct < 110) a.dedup_factor_pct = 110;
     if (a.rounds_per_graph == 0) a.rounds_per_graph = 16;
@@ -200,7 +227,7 @@ struct DeviceLineages {
 };
 
 struct Control {  // small device scalars
-    unsigned long long n_cur, out_count, work, mask, n_spec_total, n_disp_total, steps_total;
+    unsigned long long n_cur, out_count, work, mask, n_spec_total, n_disp_total, steps_total, visits;
     unsigned int n_active;
     uint32_t status;
 };
@@ -221,6 +248,8 @@ struct Engine {
     std::vector<AliasAtom *> d_atoms;
 
     DeviceLineages A, B;
+    LineageSoA O{};  // resident origins (x, y, idx, sim, last, gref)
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;  // host<->device traffic of the current call
     uint32_t *owner = nullptr, *slot = nullptr;
     unsigned long long *min_gref = nullptr;
     unsigned long long table_size = 0;
@@ -255,6 +284,10 @@ struct Engine {
         ev_total0 = ev_total1 = nullptr;
         A.release();
         B.release();
+        void *optrs[] = {O.x, O.y, O.idx, O.sim, O.last, O.gref};
+        for (void *p : optrs)
+            if (p) cudaFree(p);
+        O = LineageSoA{};
         void *ptrs[] = {owner, slot, min_gref, d_params, d_counters, d_ctl, d_spec, d_disp};
         for (void *p : ptrs)
             if (p) cudaFree(p);
@@ -290,6 +323,7 @@ void upload_tables(Engine &E, SimHost &s) {
     AliasAtom *da = dev_alloc<AliasAtom>(t.atoms.size());
     E.d_cells.push_back(dc);
     E.d_atoms.push_back(da);
+    E.h2d_bytes += t.cells.size() * sizeof(CellRecord) + t.atoms.size() * sizeof(AliasAtom);
     CK(cudaMemcpyAsync(dc, t.cells.data(), t.cells.size() * sizeof(CellRecord), cudaMemcpyHostToDevice, E.stream));
     if (!t.atoms.empty())
         CK(cudaMemcpyAsync(da, t.atoms.data(), t.atoms.size() * sizeof(AliasAtom), cudaMemcpyHostToDevice, E.stream));
@@ -418,19 +452,40 @@ void upload_origins(Engine &E, const std::vector<std::vector<necsim_lineage>> *g
         sh.start_time = tmin;
         sh.start_max = tmax;
     }
-    LineageSoA &d = E.A.soa;
+    // resident copy of the origins: every run starts from it
+    LineageSoA &d = E.O;
+    d.x = dev_alloc<uint32_t>(n);
+    d.y = dev_alloc<uint32_t>(n);
+    d.idx = dev_alloc<uint32_t>(n);
+    d.sim = dev_alloc<uint32_t>(n);
+    d.last = dev_alloc<double>(n);
+    d.gref = dev_alloc<uint64_t>(n);
     CK(cudaMemcpyAsync(d.x, x.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
     CK(cudaMemcpyAsync(d.y, y.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
     CK(cudaMemcpyAsync(d.idx, idx.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
     CK(cudaMemcpyAsync(d.sim, sim.data(), n * 4, cudaMemcpyHostToDevice, E.stream));
     CK(cudaMemcpyAsync(d.last, last.data(), n * 8, cudaMemcpyHostToDevice, E.stream));
     CK(cudaMemcpyAsync(d.gref, gref.data(), n * 8, cudaMemcpyHostToDevice, E.stream));
+    E.h2d_bytes += n * (4 * 4 + 8 * 2);
+    CK(cudaStreamSynchronize(E.stream));
+}
+
+// Resets the working lineages to the resident origins (device to device).
+void reset_lineages(Engine &E) {
+    const uint64_t n = E.n_total;
+    LineageSoA &d = E.A.soa;
+    const LineageSoA &o = E.O;
+    CK(cudaMemcpyAsync(d.x, o.x, n * 4, cudaMemcpyDeviceToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.y, o.y, n * 4, cudaMemcpyDeviceToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.idx, o.idx, n * 4, cudaMemcpyDeviceToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.sim, o.sim, n * 4, cudaMemcpyDeviceToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.last, o.last, n * 8, cudaMemcpyDeviceToDevice, E.stream));
+    CK(cudaMemcpyAsync(d.gref, o.gref, n * 8, cudaMemcpyDeviceToDevice, E.stream));
     CK(cudaMemsetAsync(d.steps, 0, n * 8, E.stream));
     CK(cudaMemsetAsync(d.has_next, 0, n, E.stream));
     CK(cudaMemsetAsync(d.next, 0, n * 8, E.stream));
     CK(cudaMemsetAsync(d.reprime, 0, n * 8, E.stream));
     CK(cudaMemsetAsync(E.A.state, 0, n, E.stream));
-    CK(cudaStreamSynchronize(E.stream));
 }
 
 StepArgs make_step_args(Engine &E, DeviceLineages &in) {
@@ -452,6 +507,7 @@ StepArgs make_step_args(Engine &E, DeviceLineages &in) {
     a.report_dispersal = E.args.report_dispersal ? 1 : 0;
     a.status = &E.d_ctl->status;
     a.steps_total = &E.d_ctl->steps_total;
+    a.n_sims = (uint32_t)E.sims.size();
     return a;
 }
 
@@ -486,6 +542,7 @@ ScheduleArgs make_schedule_args(Engine &E) {
     a.mask = &E.d_ctl->mask;
     a.table_size = E.table_size;
     a.n_active = &E.d_ctl->n_active;
+    a.visits = &E.d_ctl->visits;
     return a;
 }
 
@@ -548,11 +605,14 @@ struct RunResult {
 RunResult run_rounds(Engine &E) {
     RunResult rr;
     const unsigned rounds = E.args.rounds_per_graph;
+    CK(cudaEventRecord(E.ev_total0, E.stream));
+    reset_lineages(E);
     // initial control state
     Control c;
     std::memset(&c, 0, sizeof(c));
     c.out_count = E.n_total;
     CK(cudaMemcpyAsync(E.d_ctl, &c, sizeof(c), cudaMemcpyHostToDevice, E.stream));
+    E.h2d_bytes += sizeof(c) + E.sims.size() * (sizeof(SimParams) + sizeof(SimCounters));
     std::vector<SimParams> ps(E.sims.size());
     std::vector<SimCounters> cs(E.sims.size());
     for (size_t s = 0; s < E.sims.size(); ++s) {
@@ -561,24 +621,28 @@ RunResult run_rounds(Engine &E) {
         ps[s].active = 0;
         std::memset(&cs[s], 0, sizeof(SimCounters));
         cs[s].n_live_next = E.sims[s].n_origins;
-        // max over the initial last event times (monolithic/mod.rs:121-126)
-        double t0 = E.sims[s].start_time;
-        cs[s].max_time_bits = 0;
-        (void)t0;
     }
     CK(cudaMemcpyAsync(E.d_params, ps.data(), ps.size() * sizeof(SimParams), cudaMemcpyHostToDevice, E.stream));
     CK(cudaMemcpyAsync(E.d_counters, cs.data(), cs.size() * sizeof(SimCounters), cudaMemcpyHostToDevice, E.stream));
-    CK(cudaEventRecord(E.ev_total0, E.stream));
     CK(launch_schedule(make_schedule_args(E), E.stream));
     rr.launches += 1;
     CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
     uint64_t graph_launches = 0;
+    uint64_t stalled = 0;
+    unsigned long long last_steps = ~0ULL, last_live = ~0ULL;
     while (E.h_ctl->n_active > 0) {
         // every round advances each active simulation's horizon by at least
-        // step_slice / lambda, so this bound is never reached by a valid run
-        if (++graph_launches > (1ULL << 26) / rounds)
-            fail(NECSIM_E_TIMEOUT, "round limit reached");
+        // step_slice / lambda, so each live lineage expects >= step_slice
+        // events per round: a valid run never reaches these bounds
+        if (++graph_launches > (1ULL << 26) / rounds) fail(NECSIM_E_TIMEOUT, "round limit reached");
+        if (E.h_ctl->steps_total == last_steps && E.h_ctl->n_cur == last_live) {
+            if (++stalled >= 64) fail(NECSIM_E_TIMEOUT, "no progress over 64 graph launches");
+        } else {
+            stalled = 0;
+        }
+        last_steps = E.h_ctl->steps_total;
+        last_live = E.h_ctl->n_cur;
         if (E.graph_exec && E.timing_in_graph) {
             CK(cudaGraphLaunch(E.graph_exec, E.stream));
         } else {
@@ -587,6 +651,7 @@ RunResult run_rounds(Engine &E) {
         rr.launches += (uint64_t)rounds * 5;
         rr.rounds_launched += rounds;
         CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
+        E.d2h_bytes += sizeof(Control);
         CK(cudaStreamSynchronize(E.stream));
         for (unsigned r = 0; r < rounds; ++r) {
             float ms = 0.f;
@@ -693,6 +758,8 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
     if (n_spec)
         CK(cudaMemcpy(ev.data(), E.d_spec, n_spec * sizeof(DevSpeciationEvent), cudaMemcpyDeviceToHost));
     std::sort(ev.begin(), ev.end(), spec_less);
+    E.d2h_bytes += ns * sizeof(SimCounters) + sizeof(Control) + n * (4 * 4 + 8 * 3) +
+                   n_spec * sizeof(DevSpeciationEvent);
 
     size_t pos = 0;
     for (size_t s = 0; s < ns; ++s) {
@@ -717,6 +784,10 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
         o.n_launches = rr.launches;
         o.kernel_ms = rr.kernel_ms;
         o.total_ms = rr.total_ms;
+        o.h2d_bytes = E.h2d_bytes;
+        o.d2h_bytes = E.d2h_bytes;
+        o.n_step_launches = rr.rounds_launched;
+        o.lineage_visits = c.visits;
         // deliver this simulation's events in PackedEvent order; count
         // species like BiodiversityReporter (plugins/common/src/biodiversity.rs:32-45)
         size_t end = pos;
@@ -794,10 +865,30 @@ int guarded(necsim_ctx *ctx, char *buf, size_t cap, F &&f) {
 }
 
 // Runs simulations (one or a batch) end to end on a fresh engine.
+void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &args,
+                    const std::vector<std::vector<necsim_lineage>> *given,
+                    const std::vector<SimParams> *prebuilt_tables);
+
+// Executes one run of a prepared engine: reset to the resident origins,
+// rounds, collection and delivery.
+void execute_engine(Engine &E, const necsim_reporter *reporters, bool one_reporter,
+                    necsim_outcome *outcomes, Remaining &rem) {
+    RunResult rr;
+    if (E.n_total > 0) rr = run_rounds(E);
+    finish(E, rr, reporters, one_reporter, outcomes, rem);
+}
+
 void run_simulations(Engine &E, std::vector<SimHost> sims, const necsim_args &args,
                      const std::vector<std::vector<necsim_lineage>> *given,
                      const necsim_reporter *reporters, bool one_reporter, necsim_outcome *outcomes,
                      Remaining &rem, const std::vector<SimParams> *prebuilt_tables) {
+    prepare_engine(E, std::move(sims), args, given, prebuilt_tables);
+    execute_engine(E, reporters, one_reporter, outcomes, rem);
+}
+
+void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &args,
+                    const std::vector<std::vector<necsim_lineage>> *given,
+                    const std::vector<SimParams> *prebuilt_tables) {
     E.kind = sims.front().sc.kind;
     for (auto &s : sims)
         if (s.sc.kind != E.kind) fail(NECSIM_E_UNSUPPORTED, "a batch must share one scenario kind");
@@ -828,9 +919,6 @@ void run_simulations(Engine &E, std::vector<SimHost> sims, const necsim_args &ar
     alloc_run_buffers(E);
     upload_origins(E, given);
     if (E.n_total > 0) build_graph(E);
-    RunResult rr;
-    if (E.n_total > 0) rr = run_rounds(E);
-    finish(E, rr, reporters, one_reporter, outcomes, rem);
 }
 
 }  // namespace
@@ -1000,6 +1088,62 @@ int necsim_gpu_simulate_batch(const necsim_scenario *scenarios, const uint64_t *
         run_simulations(E, sims, args, nullptr, reporters, false, outcomes, rem, nullptr);
     });
 }
+
+struct necsim_batch {
+    Engine engine;
+    std::string error;
+    Remaining rem;
+};
+
+static std::vector<SimHost> batch_sims(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds,
+                                       uint32_t n_sims, const necsim_args &args, double pause_before) {
+    std::vector<SimHost> sims(n_sims);
+    for (uint32_t s = 0; s < n_sims; ++s) {
+        validate(scenarios[s]);
+        SimHost &sh = sims[s];
+        std::memset(&sh, 0, sizeof(sh));
+        sh.sc = scenarios[s];
+        sh.seed = wyhash_seeds[s];
+        sh.params = base_params(scenarios[s], args, wyhash_seeds[s]);
+        sh.params.pause_before = pause_before >= 0.0 ? pause_before : -1.0;
+        sh.n_origins = count_origins(scenarios[s]);
+    }
+    return sims;
+}
+
+int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,
+                            const necsim_args *args_in, double pause_before, necsim_batch **out) {
+    if (!scenarios || !wyhash_seeds || !out || n_sims == 0) return NECSIM_E_INVALID_ARGUMENT;
+    *out = nullptr;
+    necsim_batch *b = new (std::nothrow) necsim_batch();
+    if (!b) return NECSIM_E_OUT_OF_MEMORY;
+    char msg[512] = {0};
+    const int rc = guarded(nullptr, msg, sizeof(msg), [&] {
+        const necsim_args args = with_defaults(args_in);
+        setup_engine(b->engine, args);
+        prepare_engine(b->engine, batch_sims(scenarios, wyhash_seeds, n_sims, args, pause_before), args,
+                       nullptr, nullptr);
+    });
+    b->error = msg;
+    *out = b;
+    return rc;
+}
+
+int necsim_gpu_batch_run(necsim_batch *b, const necsim_reporter *reporters, necsim_outcome *outcomes) {
+    if (!b || !outcomes) return NECSIM_E_INVALID_ARGUMENT;
+    char msg[512] = {0};
+    const int rc = guarded(nullptr, msg, sizeof(msg), [&] {
+        b->engine.h2d_bytes = 0;
+        b->engine.d2h_bytes = 0;
+        execute_engine(b->engine, reporters, false, outcomes, b->rem);
+    });
+    b->error = msg;
+    return rc;
+}
+
+const char *necsim_gpu_batch_last_error(const necsim_batch *b) { return b ? b->error.c_str() : "null batch"; }
+
+void necsim_gpu_batch_destroy(necsim_batch *b) { delete b; }
 
 int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cells, necsim_alias_atom *atoms,
                         uint64_t atom_cap, uint64_t *n_atoms) {

@@ -32,12 +32,12 @@ __device__ __forceinline__ unsigned long long f64_bits(double v) {
     return (unsigned long long)__double_as_longlong(v);
 }
 
-// Speciation probability at a location (speciation_probability/uniform.rs;
-// speciation_probability/spatially_implicit.rs:31-44).
+// ceil(speciation probability * 2^53) at a location
+// (speciation_probability/uniform.rs; speciation_probability/spatially_implicit.rs:31-44)
 template <int KIND>
-__device__ __forceinline__ double speciation_probability(const SimParams &p, uint32_t x, uint32_t y) {
-    if (KIND == kSpatiallyImplicit && in_local(p, x, y)) return 0.0;
-    return p.nu;
+__device__ __forceinline__ uint64_t speciation_threshold(const SimParams &p, uint32_t x, uint32_t y) {
+    if (KIND == kSpatiallyImplicit && in_local(p, x, y)) return 0;
+    return p.nu_threshold;
 }
 
 // Per-lane lineage registers.
@@ -74,19 +74,35 @@ __device__ __forceinline__ bool load_cell(const SimParams &p, uint32_t x, uint32
     return true;
 }
 
-// packed_separable_alias/dispersal.rs:16-77 and alias/packed.rs:135-163
-__device__ __forceinline__ bool spatially_explicit_dispersal(Rng &g, const SimParams &p, uint32_t x,
-                                                             uint32_t y, const CellRecord &rec,
-                                                             uint32_t &tx, uint32_t &ty,
-                                                             uint32_t *status) {
+// packed_separable_alias/dispersal.rs:16-77 and alias/packed.rs:135-163, fed
+// with the event's samples 2..4: the self-dispersal test (when taken) uses
+// the first, the alias draw the next; `d_coal` receives the sample after them.
+__device__ __forceinline__ bool spatially_explicit_dispersal_draw(
+    uint64_t e2, uint64_t e3, uint64_t e4, const SimParams &p, uint32_t x, uint32_t y,
+    const CellRecord &rec, uint32_t &tx, uint32_t &ty, uint64_t &d_coal, uint32_t *status) {
     const uint64_t cell = (uint64_t)y * p.width + (uint64_t)x;
     uint64_t target;
     const double sd = rec.self_dispersal;
+    bool use_alias;
+    uint64_t d_alias;
     if (sd == 1.0) {
+        use_alias = false;
+        d_alias = 0;
+        d_coal = e2;
+    } else if (sd == 0.0 || (uint64_t)rec.non_self_event != cell) {
+        use_alias = true;
+        d_alias = e2;
+        d_coal = e3;
+    } else {
+        use_alias = unit_closed_open(e2) >= sd;
+        d_alias = e3;
+        d_coal = use_alias ? e4 : e3;
+    }
+    if (!use_alias) {
         target = cell;
-    } else if (sd == 0.0 || (uint64_t)rec.non_self_event != cell || g.closed_open() >= sd) {
+    } else {
         const uint64_t len = rec.atom_count;
-        const double f = __dmul_rn(__dmul_rn(g.closed_open(), 1.0), __ull2double_rn(len));
+        const double f = __dmul_rn(__dmul_rn(unit_closed_open(d_alias), 1.0), __ull2double_rn(len));
         const uint64_t i = f64_to_u64(floor(f));
         const double frac = __dsub_rn(f, __ull2double_rn(i));
         const uint64_t at = (uint64_t)rec.atom_start + i;
@@ -96,11 +112,12 @@ __device__ __forceinline__ bool spatially_explicit_dispersal(Rng &g, const SimPa
         }
         const AliasAtom atom = p.atoms[at];
         target = (frac < atom.u) ? atom.e : atom.k;
-    } else {
-        target = cell;
     }
-    tx = (uint32_t)(target % p.width);
-    ty = (uint32_t)(target / p.width);
+    // cell indices are < 2^32 (one CellRecord per cell): 32-bit divide
+    const uint32_t t32 = (uint32_t)target, w32 = p.width;
+    const uint32_t q = t32 / w32;
+    tx = t32 - q * w32;
+    ty = q;
     return true;
 }
 
@@ -109,8 +126,17 @@ __device__ __forceinline__ bool spatially_explicit_dispersal(Rng &g, const SimPa
 // One lane per lineage at a time; a lane whose lineage reaches the horizon
 // (or speciates) takes the next lineage of the queue, so warps stay full
 // while lineages of very different event counts drain.
-template <int KIND>
+template <int KIND, bool SINGLE>
 __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
+    // one simulation: its parameters live in shared memory for the launch
+    __shared__ __align__(16) unsigned char params_smem[SINGLE ? sizeof(SimParams) : 16];
+    if (SINGLE) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(a.params);
+        uint4 *dst = reinterpret_cast<uint4 *>(params_smem);
+        for (unsigned w = threadIdx.x; w < sizeof(SimParams) / 16; w += blockDim.x) dst[w] = src[w];
+        __syncthreads();
+    }
+    const SimParams *P = SINGLE ? reinterpret_cast<const SimParams *>(params_smem) : a.params;
     const uint64_t n = *a.n_cur;
     const unsigned lane_id = threadIdx.x & 31u;
     const unsigned lanemask_lt = (1u << lane_id) - 1u;
@@ -131,7 +157,7 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
                 if (k < n) {
                     const uint32_t slot = a.order ? a.order[k] : (uint32_t)k;
                     const uint32_t s = a.in.sim[slot];
-                    const SimParams &p = a.params[s];
+                    const SimParams &p = P[SINGLE ? 0 : s];
                     if (p.active) {
                         l.slot = slot;
                         l.s = s;
@@ -158,21 +184,21 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         if (!__any_sync(kFull, have)) break;
         if (!have) continue;
 
-        const SimParams &p = a.params[l.s];
-        const uint64_t inj = lane_injection<KIND>(l, p);
+        const SimParams &p = P[SINGLE ? 0 : l.s];
+        const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+        uint64_t rs;  // WyHash state re-primed for the event
         if (!l.has_next) {
             // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
             // (active_lineage_sampler/independent/sampler.rs:69-116)
             const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
-            const double t = poisson_next_event_time(l.g, inj, before, p.delta_t, p.lambda_dt, p.p0,
-                                                     l.reprime);
+            const double t = poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
             l.next = max_after(before, t);
             l.has_next = true;
         } else {
-            l.g.prime(inj, l.reprime);
+            rs = primed_state(loc_term, l.reprime);
         }
 
-        if (l.next >= l.horizon) {
+        if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) {  // non-negative
             // early stop: keep the peeked time for the next round
             a.in.x[l.slot] = l.x;
             a.in.y[l.slot] = l.y;
@@ -190,8 +216,14 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         // (event_sampler/independent.rs:112-222)
         l.steps += 1;
         local_steps += 1;
-        const double us = l.g.closed_open();
-        if (us < speciation_probability<KIND>(p, l.x, l.y)) {
+        // the event's samples 1..4 after the re-prime, drawn up front; which
+        // of them the dispersal and coalescence use depends on the branch
+        const uint64_t e1 = draw_at(rs, 1);
+        const uint64_t e2 = draw_at(rs, 2);
+        const uint64_t e3 = draw_at(rs, 3);
+        const uint64_t e4 = (KIND == kNonSpatial) ? 0 : draw_at(rs, 4);
+        // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
+        if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
             const unsigned long long e = atomicAdd(a.n_spec_total, 1ULL);
             if (e < a.spec_cap) {
                 DevSpeciationEvent ev;
@@ -217,35 +249,34 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
 
         uint32_t tx, ty, ti;
         if (KIND == kNonSpatial) {
-            non_spatial_dispersal(l.g, 0, 0, p.width, p.height, tx, ty);
-            ti = f64_to_u32(floor(__dmul_rn(l.g.closed_open(), __uint2double_rn(p.deme))));
+            non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, tx, ty);
+            ti = coalescence_index(e3, p.deme);
         } else if (KIND == kSpatiallyImplicit) {
             // dispersal_sampler/spatially_implicit.rs:58-86
-            bool to_meta;
-            if (in_local(p, l.x, l.y)) {
-                to_meta = l.g.closed_open() < p.migration;
-            } else {
-                to_meta = true;
-            }
+            const bool local = in_local(p, l.x, l.y);
+            const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
+            const uint64_t d_index = local ? e3 : e2;
+            const uint64_t d_coal = local ? e4 : e3;
             if (to_meta)
-                non_spatial_dispersal(l.g, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
+                non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
             else
-                non_spatial_dispersal(l.g, 0, 0, p.width, p.height, tx, ty);
+                non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, tx, ty);
             // habitat/spatially_implicit.rs:95-103: local extent first
-            const uint32_t cap = in_local(p, tx, ty) ? p.deme : p.meta_deme;
-            ti = f64_to_u32(floor(__dmul_rn(l.g.closed_open(), __uint2double_rn(cap))));
+            ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
         } else if (KIND == kAlmostInfiniteNormal) {
-            normal_dispersal(l.g, p.sigma, l.x, l.y, tx, ty);
-            (void)l.g.closed_open();  // CoalescenceRngSample::new draws, singleton demes -> 0
+            // sample e4 is CoalescenceRngSample::new's draw; singleton demes -> index 0
+            normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
             ti = 0;
         } else {
-            if (!spatially_explicit_dispersal(l.g, p, l.x, l.y, l.rec, tx, ty, a.status) ||
+            uint64_t d_coal;
+            if (!spatially_explicit_dispersal_draw(e2, e3, e4, p, l.x, l.y, l.rec, tx, ty, d_coal,
+                                                   a.status) ||
                 !load_cell(p, tx, ty, l.rec, a.status)) {
                 a.state[l.slot] = 2;  // dropped by a failed bound check
                 have = false;
                 continue;
             }
-            ti = f64_to_u32(floor(__dmul_rn(l.g.closed_open(), __uint2double_rn(l.rec.habitat))));
+            ti = coalescence_index(d_coal, l.rec.habitat);
         }
         if (a.report_dispersal) {
             const unsigned long long e = atomicAdd(a.n_disp_total, 1ULL);
@@ -386,7 +417,7 @@ __global__ void dedup_clear_kernel(DedupArgs a) {
 }
 
 // Picks each simulation's next horizon from its live count:
-// H' = min(H + max(step_slice, ceil(min_round_events / n)) / lambda, pause).
+// H' = min(H + clamp(ceil(min_round_events / n), step_slice, step_slice_max) / lambda, pause).
 __global__ void schedule_kernel(ScheduleArgs a) {
     __shared__ unsigned int active_sum;
     if (threadIdx.x == 0) active_sum = 0;
@@ -402,6 +433,7 @@ __global__ void schedule_kernel(ScheduleArgs a) {
         if (live > 0 && !paused) {
             const unsigned long long step_slice = p.step_slice ? p.step_slice : 1ULL;
             unsigned long long per = (p.min_round_events + live - 1) / live;
+            if (p.step_slice_max && per > p.step_slice_max) per = p.step_slice_max;
             if (per < step_slice) per = step_slice;
             double h = __dadd_rn(p.horizon, __ddiv_rn(__ull2double_rn(per), p.lambda));
             if (p.pause_before >= 0.0 && p.pause_before < h) h = p.pause_before;
@@ -417,6 +449,7 @@ __global__ void schedule_kernel(ScheduleArgs a) {
     __syncthreads();
     if (threadIdx.x == 0) {
         *a.n_active = active_sum;
+        if (active_sum > 0) *a.visits += *a.out_count;
         const unsigned long long n = *a.out_count;
         *a.n_cur = n;
         *a.out_count = 0;
@@ -433,7 +466,10 @@ __global__ void schedule_kernel(ScheduleArgs a) {
 // ---- host-side launchers ----
 template <int KIND>
 static cudaError_t launch_step_t(const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st) {
-    step_kernel<KIND><<<grid, block, 0, st>>>(a);
+    if (a.n_sims == 1)
+        step_kernel<KIND, true><<<grid, block, 0, st>>>(a);
+    else
+        step_kernel<KIND, false><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -450,13 +486,13 @@ cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned blo
 cudaError_t step_kernel_occupancy(int kind, int block, int *blocks_per_sm) {
     switch (kind) {
     case kNonSpatial:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kNonSpatial>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kNonSpatial, false>, block, 0);
     case kSpatiallyImplicit:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kSpatiallyImplicit>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kSpatiallyImplicit, false>, block, 0);
     case kAlmostInfiniteNormal:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kAlmostInfiniteNormal>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kAlmostInfiniteNormal, false>, block, 0);
     case kSpatiallyExplicit:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kSpatiallyExplicit>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kSpatiallyExplicit, false>, block, 0);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -28,6 +28,7 @@ struct StepArgs {
     int report_dispersal;
     uint32_t *status;
     unsigned long long *steps_total;     // optional per-launch event count
+    uint32_t n_sims;                     // simulations in `params`
 };
 
 struct DedupArgs {
@@ -56,6 +57,7 @@ struct ScheduleArgs {
     unsigned long long *mask;
     unsigned long long table_size;
     unsigned int *n_active;
+    unsigned long long *visits;          // lineages the scheduled rounds process
 };
 
 cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st);

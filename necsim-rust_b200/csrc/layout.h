@@ -44,8 +44,27 @@ struct alignas(16) AliasAtom {
 };
 static_assert(sizeof(AliasAtom) == 16, "AliasAtom must be 16 bytes");
 
+constexpr int kPoissonTable = 16;
+constexpr int kPoissonThresholds = 8;
+
 // Per-simulation scalars, read by every lineage of the simulation.
-struct SimParams {
+//
+// Comparisons of a uniform u = X * 2^-53 (X the 53-bit integer of a draw)
+// with a constant c are done on integers: u > c  <=>  X > floor(c * 2^53) and
+// u < c  <=>  X < ceil(c * 2^53), both exact (scaling by 2^53 is exact).
+struct alignas(16) SimParams {
+    double lambda_dt_over_k[kPoissonTable];  // lambda_dt / k, k = 1..16
+    // Devroye's loop (poisson.rs:51-65) visits the constant sequence
+    // acc_n = acc_{n-1} + prod_n, prod_n = prod_{n-1} * (lambda_dt / n); the
+    // draw continues past rank n iff X > poisson_threshold[n] (and prod_n > 0)
+    uint64_t poisson_threshold[kPoissonThresholds];  // floor(acc_n * 2^53)
+    uint32_t poisson_alive;   // bit n: prod_n > 0
+    uint32_t pad0;
+    double poisson_prod_k;    // prod_n and acc_n at n = kPoissonThresholds
+    double poisson_acc_k;
+    uint64_t nu_threshold;    // ceil(nu * 2^53): speciation iff X < this
+    uint64_t migration_threshold;  // ceil(migration * 2^53)
+    double inv_delta_t;       // 1 / delta_t if delta_t is a power of two, else 0
     uint64_t seed;            // WyHash seed word
     double nu;                // speciation probability
     double lambda;            // uniform turnover rate
@@ -65,9 +84,13 @@ struct SimParams {
     uint64_t n_atoms;
     uint64_t step_slice;
     uint64_t min_round_events;
+    uint64_t step_slice_max;
     int32_t active;           // 1 while the simulation still advances
     int32_t pad;
 };
+
+// the step kernel copies one SimParams into shared memory in 16-byte words
+static_assert(sizeof(SimParams) % 16 == 0, "SimParams must be whole 16-byte words");
 
 // Per-simulation counters (device), accumulated as lineages leave.
 struct SimCounters {

@@ -764,7 +764,7 @@ static int64_t enumerate_origins(const oracle_scenario *sc, const sim_t *s, line
 }
 
 int64_t oracle_count_origins(const oracle_scenario *sc) {
-    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1};
+    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1, 0};
     sim_t s;
     oracle_scenario tmp = *sc;
     int rc;
@@ -781,7 +781,7 @@ int64_t oracle_count_origins(const oracle_scenario *sc) {
 }
 
 int64_t oracle_enumerate_origins(const oracle_scenario *sc, oracle_lineage *out, uint64_t cap) {
-    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1};
+    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1, 0};
     sim_t s;
     int rc;
     if (sc->kind == ORACLE_SPATIALLY_EXPLICIT) {
@@ -1264,8 +1264,10 @@ static int simulate_canonical(sim_t *s, const oracle_args *args, lineage_t *lins
     int has_pause = pause_before >= 0.0;
     uint64_t step_slice = args->step_slice ? args->step_slice : 1;
     while (n > 0 && (!has_pause || horizon < pause_before)) {
-        /* events per lineage this round: max(step_slice, ceil(min_round_events / n)) */
+        /* events per lineage this round:
+         * clamp(ceil(min_round_events / n), step_slice, max(step_slice, step_slice_max)) */
         uint64_t per = (args->min_round_events + n - 1) / n;
+        if (args->step_slice_max && per > args->step_slice_max) per = args->step_slice_max;
         if (per < step_slice) per = step_slice;
         double next_horizon = horizon + (double)per / s->lambda;
         if (has_pause && pause_before < next_horizon) next_horizon = pause_before;

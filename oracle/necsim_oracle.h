@@ -59,6 +59,7 @@ typedef struct oracle_args {
     int32_t mode;               /* ORACLE_MODE_* */
     uint32_t partition_rank;    /* IsolatedIndividuals partition (size 1 = monolithic) */
     uint32_t partition_size;
+    uint64_t step_slice_max;    /* canonical schedule: cap on events per lineage per round (0: none) */
 } oracle_args;
 
 typedef struct oracle_speciation_event {   /* SpeciationEvent, 40 bytes */

@@ -55,6 +55,7 @@ class OracleArgs(ctypes.Structure):
         ("mode", ctypes.c_int32),
         ("partition_rank", ctypes.c_uint32),
         ("partition_size", ctypes.c_uint32),
+        ("step_slice_max", ctypes.c_uint64),
     ]
 
 
@@ -195,7 +196,7 @@ def make_scenario(desc):
 
 def make_args(mode=MODE_REFERENCE, delta_t=2.0, step_slice=10, dedup_factor=1.0,
               event_slice_factor=2.0, min_round_events=0, report_dispersal=False,
-              partition=(0, 1)):
+              partition=(0, 1), step_slice_max=0):
     a = OracleArgs()
     a.delta_t = delta_t
     a.step_slice = step_slice
@@ -206,6 +207,7 @@ def make_args(mode=MODE_REFERENCE, delta_t=2.0, step_slice=10, dedup_factor=1.0,
     a.mode = mode
     a.partition_rank = partition[0]
     a.partition_size = partition[1]
+    a.step_slice_max = step_slice_max
     return a
 
 

@@ -38,7 +38,8 @@ def check(nb, syn, oracle, desc, seed, algo=None, pause=None, reference=True):
     algo = algo or nb.CUDA()
     g = run_gpu(nb, syn, desc, seed, algo, pause)
     c = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, step_slice=algo.step_slice,
-                        min_round_events=algo.min_round_events, pause_before=pause)
+                        min_round_events=algo.min_round_events, pause_before=pause,
+                        step_slice_max=algo.step_slice_max)
     assert same_stream(g.speciation, c.speciation)
     assert (g.steps, g.n_rounds, g.n_dedup, g.biodiversity) == (c.steps, c.n_rounds, c.n_dedup,
                                                                  c.biodiversity)
@@ -144,7 +145,7 @@ def test_pause_resume_equals_straight_run(nb, syn):
 def test_resume_matches_oracle(nb, syn, oracle):
     desc, seed = CASES["si_demes"]
     first = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, pause_before=100.0,
-                            min_round_events=1 << 20)
+                            min_round_events=1 << 20, step_slice_max=1024)
     with nb.Simulation(syn.to_scenario(desc), desc["speciation_probability"]) as sim:
         g = sim.resume(first.remaining, 100.0, seed)
     c = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, lineages=first.remaining,
