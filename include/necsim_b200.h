@@ -210,6 +210,38 @@ int necsim_gpu_batch_run(necsim_batch *batch, const necsim_reporter *reporters,
 const char *necsim_gpu_batch_last_error(const necsim_batch *batch);
 void necsim_gpu_batch_destroy(necsim_batch *batch);
 
+/* ---- allocation-free round ----
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory themselves or through us (a host whose allocator owns the GPU, a
+ * plugin handed a fixed arena, a service that forbids cudaMalloc/cudaFree
+ * and the device synchronisation they can cause after start-up): one round
+ * -- every lineage advanced through all its events before `horizon`, then
+ * lineages in identical state merged into the one with the smallest global
+ * reference -- computed in a working area that lives in the library as a
+ * static device array (about 9.5 MB per GPU, kept until the process exits).
+ *
+ * d_lineages (n entries), d_out (n entries) and d_events (events_cap
+ * entries) are DEVICE pointers owned by the caller; n may not exceed
+ * NECSIM_NOALLOC_MAX_LINEAGES (NECSIM_E_TOO_LARGE otherwise).  Scenario
+ * kinds without tables only (NonSpatial, SpatiallyImplicit, AlmostInfinite);
+ * SpatiallyExplicit returns NECSIM_E_UNSUPPORTED.  resume_time is the
+ * min_event_time of the lineages.  Surviving lineages and speciation events
+ * are written in no particular order; *n_out, *n_events and *steps (events
+ * executed) are set on return.  Work is queued on `stream` (a cudaStream_t,
+ * NULL = default stream) and the call waits for it.
+ *
+ * The first call on a device looks up the device address of the working
+ * area; make that first call before capturing any stream into a CUDA graph.
+ * Every call shares the one working area and clears it before use, so calls
+ * whose GPU work overlaps (other streams or host threads) race. */
+#define NECSIM_NOALLOC_MAX_LINEAGES 65536
+int necsim_gpu_round_noalloc(const necsim_scenario *scenario, const necsim_args *args,
+                             uint64_t wyhash_seed, const necsim_lineage *d_lineages, uint64_t n,
+                             double resume_time, double horizon, necsim_lineage *d_out,
+                             uint64_t *n_out, necsim_speciation_event *d_events,
+                             uint64_t events_cap, uint64_t *n_events, uint64_t *steps,
+                             void *stream);
+
 const char *necsim_gpu_last_error(const necsim_ctx *ctx);
 void necsim_gpu_destroy(necsim_ctx *ctx);
 

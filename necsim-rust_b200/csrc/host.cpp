@@ -1189,3 +1189,13 @@ const char *necsim_gpu_last_error(const necsim_ctx *ctx) { return ctx ? ctx->err
 void necsim_gpu_destroy(necsim_ctx *ctx) { delete ctx; }
 
 }  // extern "C"
+
+// Per-simulation parameters for callers outside this file (the
+// allocation-free round in noalloc.cu): the same values base_params gives
+// the engine, with the defaults of with_defaults.
+namespace necsim {
+SimParams host_sim_params(const necsim_scenario &sc, const necsim_args *args, uint64_t wyhash_seed) {
+    const necsim_args a = with_defaults(args);
+    return base_params(sc, a, wyhash_seed);
+}
+}  // namespace necsim
