@@ -44,10 +44,12 @@ def parse():
     p.add_argument("--steps", type=int, default=2)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="c4", choices=["c4", "c5", "c2", "c3", "c1"])
+    p.add_argument("--workload", default="c4", choices=["c4", "c4-small", "c5", "c2", "c3", "c1"])
     p.add_argument("--schedule", default="plain", choices=["plain", "learned"])
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--pause", type=float, default=None,
+                   help="pause_before of every simulation (default: run to completion)")
     return p.parse_args()
 
 
@@ -60,6 +62,10 @@ def workload(name):
     if name == "c4":
         return ("256 x SpatiallyImplicit sweep: J=floor(10^U(3,6)) deme 1, meta 1e7 deme 1, "
                 "migration U(0.01,0.2), speciation 10^U(-6,-3), seeds 0..255", syn.config4())
+    if name == "c4-small":
+        # every 16th simulation of the sweep: the profiling-sized case
+        return ("16 of the 256 SpatiallyImplicit sweep simulations (every 16th)",
+                syn.config4()[::16])
     if name == "c5":
         d, s = syn.config5()
         return ("SpatiallyExplicit 128x128 habitat (0 w.p. 0.2 else U{1..500}), dense "
@@ -249,7 +255,7 @@ def main():
     se = sims[0][0]["kind"] == 3
     kind = sims[0][0]["kind"]
 
-    batch = nb.Batch(scen, nus, seeds, algo)
+    batch = nb.Batch(scen, nus, seeds, algo, pause_before=args.pause)
     for _ in range(args.warmup):
         batch.run()
 
@@ -282,7 +288,7 @@ def main():
     for _ in range(args.steps):
         dist.barrier()
         t0 = time.perf_counter()
-        outs = nb.simulate_batch(scen, nus, seeds, algo)
+        outs = nb.simulate_batch(scen, nus, seeds, algo, pause_before=args.pause)
         dt = time.perf_counter() - t0
         e2e_sec += dist.max(dt)
         e2e_steps += sum(o.steps for o in outs)
@@ -320,6 +326,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
         "data": "synthetic",
         "config": {"workload": desc, "schedule": args.schedule, "kind": kind,
+                   "pause_before": args.pause,
                    "simulations": len(sims), "lineages": int(sum(o.n_initial for o in outs)),
                    "l2": "inputs larger than L2 (lineage state %.2f GB)" % (
                        sum(o.n_initial for o in outs) * 57 * 2 / 1e9),

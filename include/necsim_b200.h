@@ -84,7 +84,8 @@ typedef struct necsim_args {
     int32_t report_dispersal;  /* reporters consume dispersal events (ReportDispersal) */
     int32_t device;            /* CUDA device ordinal; default 0 */
     uint32_t rounds_per_graph; /* rounds captured per CUDA graph launch; 0 = default (16) */
-    uint32_t reserved;
+    uint32_t resident_off;     /* 1: keep small simulations in the global rounds instead of
+                                  the per-simulation resident kernel (same results) */
 } necsim_args;
 
 /* ---- events and lineages (reference layouts) ---- */
@@ -146,6 +147,8 @@ typedef struct necsim_outcome {
     uint64_t d2h_bytes;        /* device-to-host bytes copied by the call */
     uint64_t n_step_launches;  /* step-kernel launches (one per round) */
     uint64_t lineage_visits;   /* lineage slots the step kernels processed */
+    double resident_ms;        /* device time of the per-simulation resident kernel (CUDA
+                                  events; overlaps the global rounds) */
 } necsim_outcome;
 
 typedef struct necsim_ctx necsim_ctx;

@@ -64,7 +64,7 @@ class CArgs(ctypes.Structure):
         ("grid_size", ctypes.c_uint32), ("dedup_factor_pct", ctypes.c_uint32),
         ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("resident_off", ctypes.c_uint32),
     ]
 
 
@@ -78,7 +78,7 @@ class COutcome(ctypes.Structure):
         ("n_launches", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_uint64),
         ("d2h_bytes", ctypes.c_uint64), ("n_step_launches", ctypes.c_uint64),
-        ("lineage_visits", ctypes.c_uint64),
+        ("lineage_visits", ctypes.c_uint64), ("resident_ms", ctypes.c_double),
     ]
 
 
@@ -234,6 +234,7 @@ class CUDA:
     schedule: str = "plain"   # or "learned"
     device: int = 0
     rounds_per_graph: int = 16
+    resident: bool = True     # small simulations run in the per-simulation resident kernel
 
 
 Independent = CUDA
@@ -257,6 +258,7 @@ class Outcome:
     d2h_bytes: int = 0
     n_step_launches: int = 0
     lineage_visits: int = 0
+    resident_ms: float = 0.0
     speciation: Optional[np.ndarray] = None
     remaining: Optional[np.ndarray] = None
 
@@ -317,6 +319,7 @@ def _args_struct(algorithm: CUDA):
     a.report_dispersal = 0
     a.device = algorithm.device
     a.rounds_per_graph = algorithm.rounds_per_graph
+    a.resident_off = 0 if algorithm.resident else 1
     return a
 
 
@@ -347,7 +350,8 @@ class _Collector:
 def _outcome(o: COutcome, spec=None, remaining=None) -> Outcome:
     return Outcome(bool(o.paused), o.time, o.steps, o.n_initial, o.n_remaining, o.n_speciation,
                    o.biodiversity, o.n_rounds, o.n_dedup, o.n_launches, o.kernel_ms, o.total_ms,
-                   o.h2d_bytes, o.d2h_bytes, o.n_step_launches, o.lineage_visits, spec, remaining)
+                   o.h2d_bytes, o.d2h_bytes, o.n_step_launches, o.lineage_visits, o.resident_ms,
+                   spec, remaining)
 
 
 class Simulation:

@@ -189,23 +189,46 @@ __device__ __forceinline__ double poisson_next_event_time(Rng &g, uint64_t inj, 
     return best;
 }
 
+// Devroye's Poisson(lambda * delta_t) count (poisson.rs:51-65) from the
+// bucket's first sample d1: the loop passes rank n while
+// X > floor(acc_n * 2^53) and prod_n > 0, continued in f64 beyond the
+// tabulated ranks.
+__device__ __forceinline__ uint32_t poisson_count(uint64_t d1, const SimParams &p) {
+    const uint64_t X = d1 >> 11;
+    const uint32_t alive = (uint32_t)__popc(p.poisson_alive);
+    const uint32_t limit = alive < (uint32_t)kPoissonThresholds ? alive : (uint32_t)kPoissonThresholds;
+    uint32_t n_events = 0;
+    while (n_events < limit && X > p.poisson_threshold[n_events]) ++n_events;
+    if (n_events == (uint32_t)kPoissonThresholds) {
+        const double u = unit_closed_open(d1);
+        double prod = p.poisson_prod_k;
+        double acc = p.poisson_acc_k;
+        while (u > acc && prod > 0.0) {
+            n_events += 1;
+            const double ratio = n_events <= (uint32_t)kPoissonTable
+                                     ? p.lambda_dt_over_k[n_events - 1]
+                                     : __ddiv_rn(p.lambda_dt, __uint2double_rn(n_events));
+            prod = __dmul_rn(prod, ratio);
+            acc = __dadd_rn(acc, prod);
+        }
+    }
+    return n_events;
+}
+
 // One bucket of the Poisson sampler (poisson.rs:50-95) primed to s0: the
 // earliest event strictly after `time` (ties: lowest index), or -1.  The
 // Devroye uniform and the first two event-time uniforms are drawn up front.
 __device__ __forceinline__ int poisson_bucket(uint64_t s0, uint64_t time_step, double time,
                                               const SimParams &p, double &best) {
     const uint64_t d1 = draw_at(s0, 1);
-    const uint64_t d2 = draw_at(s0, 2);
-    const uint64_t d3 = draw_at(s0, 3);
-    // Devroye's loop on the constant acc_n sequence: the ranks passed are the
-    // leading thresholds below X (thresholds are non-decreasing, alive bits a
-    // prefix), so the count equals the loop's exit rank
+    // Devroye's loop on the constant acc_n sequence: it passes rank n while
+    // X > floor(acc_n * 2^53) and prod_n > 0 (thresholds are non-decreasing,
+    // alive bits a prefix)
     const uint64_t X = d1 >> 11;
-    uint32_t n_events = 0;
-#pragma unroll
-    for (int n = 0; n < kPoissonThresholds; ++n) n_events += (X > p.poisson_threshold[n]) ? 1u : 0u;
     const uint32_t alive = (uint32_t)__popc(p.poisson_alive);
-    if (alive < n_events) n_events = alive;
+    const uint32_t limit = alive < (uint32_t)kPoissonThresholds ? alive : (uint32_t)kPoissonThresholds;
+    uint32_t n_events = 0;
+    while (n_events < limit && X > p.poisson_threshold[n_events]) ++n_events;
     if (n_events == (uint32_t)kPoissonThresholds) {
         // continue the reference loop beyond the tabulated ranks
         const double u = unit_closed_open(d1);
@@ -228,7 +251,7 @@ __device__ __forceinline__ int poisson_bucket(uint64_t s0, uint64_t time_step, d
     int best_k = -1;
     long long best_bits = 0;
     for (uint32_t k = 0; k < n_events; ++k) {
-        const uint64_t d = k == 0 ? d2 : (k == 1 ? d3 : draw_at(s0, k + 2));
+        const uint64_t d = draw_at(s0, k + 2);
         const double et = __dmul_rn(__dadd_rn(step_start, unit_closed_open(d)), p.delta_t);
         const long long eb = __double_as_longlong(et);
         if (eb > time_bits && (best_k < 0 || best_bits > eb)) {
@@ -250,14 +273,8 @@ __device__ __forceinline__ double poisson_next_event_time_ilp(uint64_t loc_term,
     const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
     uint64_t time_step = f64_to_u64(floor(q));
     for (;;) {
-        const uint64_t s0 = primed_state(loc_term, time_step);
-        const uint64_t s1 = primed_state(loc_term, time_step + 1);
         double best = 0.0;
-        int k = poisson_bucket(s0, time_step, time, p, best);
-        if (k < 0) {
-            time_step += 1;
-            k = poisson_bucket(s1, time_step, time, p, best);
-        }
+        const int k = poisson_bucket(primed_state(loc_term, time_step), time_step, time, p, best);
         if (k >= 0) {
             reprime = time_step + kInvPhi * (uint64_t)(k + 1);
             reprimed_state = primed_state(loc_term, reprime);

@@ -228,8 +228,10 @@ struct DeviceLineages {
 
 struct Control {  // small device scalars
     unsigned long long n_cur, out_count, work, mask, n_spec_total, n_disp_total, steps_total, visits;
-    unsigned int n_active;
+    unsigned int n_active;    // active simulations in the global rounds
     uint32_t status;
+    unsigned int n_resident;  // active simulations owned by the resident kernel
+    int graph_done;           // set when the global rounds beside a resident launch end
 };
 
 struct Engine {
@@ -237,6 +239,8 @@ struct Engine {
     int kind = 0;
     necsim_args args{};
     cudaStream_t stream = nullptr;
+    cudaStream_t stream_t = nullptr;  // resident kernel, concurrent with the global rounds
+    cudaEvent_t ev_fork = nullptr;
     int n_sms = 148;
 
     std::vector<SimHost> sims;
@@ -248,7 +252,9 @@ struct Engine {
     std::vector<AliasAtom *> d_atoms;
 
     DeviceLineages A, B;
+    DeviceLineages R;  // resident arena: small simulations' lineages, one segment each
     LineageSoA O{};  // resident origins (x, y, idx, sim, last, gref)
+    cudaEvent_t ev_res0 = nullptr, ev_res1 = nullptr;
     uint64_t h2d_bytes = 0, d2h_bytes = 0;  // host<->device traffic of the current call
     uint32_t *owner = nullptr, *slot = nullptr;
     unsigned long long *min_gref = nullptr;
@@ -284,6 +290,10 @@ struct Engine {
         ev_total0 = ev_total1 = nullptr;
         A.release();
         B.release();
+        R.release();
+        if (ev_res0) cudaEventDestroy(ev_res0);
+        if (ev_res1) cudaEventDestroy(ev_res1);
+        ev_res0 = ev_res1 = nullptr;
         void *optrs[] = {O.x, O.y, O.idx, O.sim, O.last, O.gref};
         for (void *p : optrs)
             if (p) cudaFree(p);
@@ -307,6 +317,10 @@ struct Engine {
         if (h_ctl) cudaFreeHost(h_ctl);
         h_ctl = nullptr;
         if (stream) cudaStreamDestroy(stream);
+        if (stream_t) cudaStreamDestroy(stream_t);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        stream_t = nullptr;
+        ev_fork = nullptr;
         stream = nullptr;
     }
 };
@@ -342,6 +356,8 @@ void setup_engine(Engine &E, const necsim_args &args) {
     CK(cudaGetDeviceProperties(&prop, E.device));
     E.n_sms = prop.multiProcessorCount;
     CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&E.stream_t, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreate(&E.ev_total0));
     CK(cudaEventCreate(&E.ev_total1));
     void *h = nullptr;
@@ -365,6 +381,9 @@ void choose_launch(Engine &E) {
 void alloc_run_buffers(Engine &E) {
     const uint64_t n = E.n_total;
     E.A.alloc(n);
+    E.R.alloc(n);
+    CK(cudaEventCreate(&E.ev_res0));
+    CK(cudaEventCreate(&E.ev_res1));
     E.B.alloc(n);
     unsigned long long want = (n * E.args.dedup_factor_pct + 99) / 100;
     if (want < 2) want = 2;
@@ -526,6 +545,27 @@ DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
     a.out_count = &E.d_ctl->out_count;
     a.counters = E.d_counters;
     a.status = &E.d_ctl->status;
+    if (E.args.resident_off == 0) a.arena = E.R.soa;  // route small simulations to the arena
+    a.params = E.d_params;
+    return a;
+}
+
+ResidentArgs make_resident_args(Engine &E, uint32_t budget, const int *stop_flag) {
+    ResidentArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.arena = E.R.soa;
+    a.params = E.d_params;
+    a.counters = E.d_counters;
+    a.n_sims = (uint32_t)E.sims.size();
+    a.budget = budget;
+    a.spec = E.d_spec;
+    a.n_spec_total = &E.d_ctl->n_spec_total;
+    a.spec_cap = E.spec_cap;
+    a.status = &E.d_ctl->status;
+    a.steps_total = &E.d_ctl->steps_total;
+    a.visits = &E.d_ctl->visits;
+    a.n_resident = &E.d_ctl->n_resident;
+    a.stop_flag = stop_flag;
     return a;
 }
 
@@ -543,6 +583,7 @@ ScheduleArgs make_schedule_args(Engine &E) {
     a.table_size = E.table_size;
     a.n_active = &E.d_ctl->n_active;
     a.visits = &E.d_ctl->visits;
+    a.n_resident = &E.d_ctl->n_resident;
     return a;
 }
 
@@ -596,6 +637,7 @@ void build_graph(Engine &E) {
 struct RunResult {
     double kernel_ms = 0.0;
     double total_ms = 0.0;
+    double resident_ms = 0.0;
     uint64_t launches = 0;
     uint64_t rounds_launched = 0;
 };
@@ -631,7 +673,12 @@ RunResult run_rounds(Engine &E) {
     uint64_t graph_launches = 0;
     uint64_t stalled = 0;
     unsigned long long last_steps = ~0ULL, last_live = ~0ULL;
-    while (E.h_ctl->n_active > 0) {
+    // one block per resident simulation, at most two per SM
+    // at most one block per SM beside the global rounds (room for their
+    // kernels), two per SM when only resident simulations are left
+    const unsigned grid_beside = (unsigned)std::min<size_t>(E.sims.size(), (size_t)E.n_sms);
+    const unsigned grid_alone = (unsigned)std::min<size_t>(E.sims.size(), (size_t)E.n_sms * 2);
+    while (E.h_ctl->n_active > 0 || E.h_ctl->n_resident > 0) {
         // every round advances each active simulation's horizon by at least
         // step_slice / lambda, so each live lineage expects >= step_slice
         // events per round: a valid run never reaches these bounds
@@ -643,19 +690,45 @@ RunResult run_rounds(Engine &E) {
         }
         last_steps = E.h_ctl->steps_total;
         last_live = E.h_ctl->n_cur;
-        if (E.graph_exec && E.timing_in_graph) {
-            CK(cudaGraphLaunch(E.graph_exec, E.stream));
-        } else {
-            enqueue_rounds(E, rounds, true, false);
+        const bool global = E.h_ctl->n_active > 0;
+        // both streams are idle here: hand routed simulations to the resident
+        // kernel, then run it on its own stream beside the global rounds
+        CK(launch_promote(E.d_params, (uint32_t)E.sims.size(), E.stream));
+        CK(cudaMemsetAsync(&E.d_ctl->graph_done, 0, sizeof(int), E.stream));
+        CK(cudaEventRecord(E.ev_fork, E.stream));
+        CK(cudaStreamWaitEvent(E.stream_t, E.ev_fork, 0));
+        // beside global rounds: until they end (at most 64 rounds, so the
+        // global kernels never wait long for SM space); alone: long stretches
+        const uint32_t budget = global ? 64 : 256;
+        CK(cudaEventRecord(E.ev_res0, E.stream_t));
+        CK(launch_resident(E.kind, make_resident_args(E, budget, global ? &E.d_ctl->graph_done : nullptr),
+                           global ? grid_beside : grid_alone, E.stream_t));
+        CK(cudaEventRecord(E.ev_res1, E.stream_t));
+        rr.launches += 2;
+        rr.rounds_launched += 1;
+        if (global) {
+            if (E.graph_exec && E.timing_in_graph) {
+                CK(cudaGraphLaunch(E.graph_exec, E.stream));
+            } else {
+                enqueue_rounds(E, rounds, true, false);
+            }
+            CK(cudaMemsetAsync(&E.d_ctl->graph_done, 1, sizeof(int), E.stream));
+            rr.launches += (uint64_t)rounds * 5;
+            rr.rounds_launched += rounds;
         }
-        rr.launches += (uint64_t)rounds * 5;
-        rr.rounds_launched += rounds;
+        CK(cudaStreamWaitEvent(E.stream, E.ev_res1, 0));
         CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
         E.d2h_bytes += sizeof(Control);
         CK(cudaStreamSynchronize(E.stream));
-        for (unsigned r = 0; r < rounds; ++r) {
+        if (global) {
+            for (unsigned r = 0; r < rounds; ++r) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, E.ev_start[r], E.ev_end[r]) == cudaSuccess) rr.kernel_ms += ms;
+            }
+        }
+        {
             float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, E.ev_start[r], E.ev_end[r]) == cudaSuccess) rr.kernel_ms += ms;
+            if (cudaEventElapsedTime(&ms, E.ev_res0, E.ev_res1) == cudaSuccess) rr.resident_ms += ms;
         }
         if (E.h_ctl->status & ~kErrDedupFull) break;
     }
@@ -715,7 +788,7 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
     CK(cudaMemcpy(cs.data(), E.d_counters, ns * sizeof(SimCounters), cudaMemcpyDeviceToHost));
     Control c;
     CK(cudaMemcpy(&c, E.d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
-    if (c.status & (kErrCellIndex | kErrAtomIndex | kErrEventOverflow | kErrDispersalOverflow))
+    if (c.status & (kErrCellIndex | kErrAtomIndex | kErrEventOverflow | kErrDispersalOverflow | kErrResident))
         fail(NECSIM_E_DEVICE_CHECK, "device bound check failed (status " + std::to_string(c.status) + ")");
     // surviving lineages live in A after an even number of rounds
     const uint64_t n = c.n_cur;
@@ -732,10 +805,35 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
         CK(cudaMemcpy(gref.data(), d.gref, n * 8, cudaMemcpyDeviceToHost));
         CK(cudaMemcpy(steps.data(), d.steps, n * 8, cudaMemcpyDeviceToHost));
     }
+    // simulations that ended in the resident kernel keep their survivors in
+    // their segment of the resident arena
+    std::vector<SimParams> ps(ns);
+    CK(cudaMemcpy(ps.data(), E.d_params, ns * sizeof(SimParams), cudaMemcpyDeviceToHost));
+    for (size_t s = 0; s < ns; ++s) {
+        if (!ps[s].resident || cs[s].n_live == 0) continue;
+        const uint64_t m = cs[s].n_live, o = ps[s].lineage_offset;
+        const size_t base = x.size();
+        x.resize(base + m);
+        y.resize(base + m);
+        idx.resize(base + m);
+        sim.resize(base + m);
+        last.resize(base + m);
+        gref.resize(base + m);
+        steps.resize(base + m);
+        const LineageSoA &r = E.R.soa;
+        CK(cudaMemcpy(x.data() + base, r.x + o, m * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(y.data() + base, r.y + o, m * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(idx.data() + base, r.idx + o, m * 4, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(last.data() + base, r.last + o, m * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(gref.data() + base, r.gref + o, m * 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(steps.data() + base, r.steps + o, m * 8, cudaMemcpyDeviceToHost));
+        for (uint64_t k = 0; k < m; ++k) sim[base + k] = (uint32_t)s;
+        E.d2h_bytes += m * 36;
+    }
     rem.per_sim.assign(ns, {});
     std::vector<uint64_t> extra_steps(ns, 0);
     std::vector<double> extra_time(ns, 0.0);
-    for (uint64_t j = 0; j < n; ++j) {
+    for (uint64_t j = 0; j < x.size(); ++j) {
         const uint32_t s = sim[j];
         extra_steps[s] += steps[j];
         extra_time[s] = std::max(extra_time[s], last[j]);
@@ -784,6 +882,7 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
         o.n_launches = rr.launches;
         o.kernel_ms = rr.kernel_ms;
         o.total_ms = rr.total_ms;
+        o.resident_ms = rr.resident_ms;
         o.h2d_bytes = E.h2d_bytes;
         o.d2h_bytes = E.d2h_bytes;
         o.n_step_launches = rr.rounds_launched;
@@ -896,6 +995,7 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
     uint64_t off = 0;
     for (auto &s : sims) {
         s.lineage_offset = off;
+        s.params.lineage_offset = off;
         off += s.n_origins;
     }
     if (off >= 0xffffffffULL) fail(NECSIM_E_TOO_LARGE, "more than 2^32 - 1 lineages");

@@ -78,7 +78,7 @@ __device__ __forceinline__ bool load_cell(const SimParams &p, uint32_t x, uint32
 // with the event's samples 2..4: the self-dispersal test (when taken) uses
 // the first, the alias draw the next; `d_coal` receives the sample after them.
 __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
-    uint64_t e2, uint64_t e3, uint64_t e4, const SimParams &p, uint32_t x, uint32_t y,
+    uint64_t e2, uint64_t e3, uint64_t rs, const SimParams &p, uint32_t x, uint32_t y,
     const CellRecord &rec, uint32_t &tx, uint32_t &ty, uint64_t &d_coal, uint32_t *status) {
     const uint64_t cell = (uint64_t)y * p.width + (uint64_t)x;
     uint64_t target;
@@ -96,7 +96,7 @@ __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
     } else {
         use_alias = unit_closed_open(e2) >= sd;
         d_alias = e3;
-        d_coal = use_alias ? e4 : e3;
+        d_coal = use_alias ? draw_at(rs, 4) : e3;
     }
     if (!use_alias) {
         target = cell;
@@ -123,6 +123,295 @@ __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
 
 }  // namespace
 
+// Where an event left the lineage.
+enum StepResult : int { kStepStop = 0, kStepMoved = 1, kStepSpeciated = 2, kStepDropped = 3 };
+
+// Outputs of lineage_step besides the lineage itself.
+struct EventSink {
+    DevSpeciationEvent *spec;
+    unsigned long long *n_spec_total;
+    uint64_t spec_cap;
+    DevDispersalEvent *disp;
+    unsigned long long *n_disp_total;
+    uint64_t disp_cap;
+    int report_dispersal;
+    uint32_t *status;
+    SimCounters *counters;
+};
+
+// One step of a lineage: peek its next event time (or use the peek kept from
+// the previous round) and stop if it is at or beyond the horizon; otherwise
+// execute the event (speciation, or dispersal + coalescence index).
+template <int KIND>
+__device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const EventSink &k) {
+    const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+    uint64_t rs;  // WyHash state re-primed for the event
+    if (!l.has_next) {
+        // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
+        // (active_lineage_sampler/independent/sampler.rs:69-116)
+        const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
+        const double t = poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
+        l.next = max_after(before, t);
+        l.has_next = true;
+    } else {
+        rs = primed_state(loc_term, l.reprime);
+    }
+    // the reference's early stop `next_event_time >= level_time`
+    // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
+    if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
+
+    // IndependentEventSampler::sample_event_for_lineage_at_event_time_or_emigrate
+    // (event_sampler/independent.rs:112-222)
+    l.steps += 1;
+    // the event's samples 1..4 after the re-prime, drawn up front; which of
+    // them the dispersal and coalescence use depends on the branch
+    const uint64_t e1 = draw_at(rs, 1);
+    // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
+    if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
+        const unsigned long long e = atomicAdd(k.n_spec_total, 1ULL);
+        if (e < k.spec_cap) {
+            DevSpeciationEvent ev;
+            ev.gref = l.gref;
+            ev.prior_time = l.last;
+            ev.event_time = l.next;
+            ev.x = l.x;
+            ev.y = l.y;
+            ev.idx = l.i;
+            ev.sim = l.s;
+            k.spec[e] = ev;
+        } else {
+            set_status(k.status, kErrEventOverflow);
+        }
+        SimCounters &c = k.counters[l.s];
+        atomicAdd(&c.steps, (unsigned long long)l.steps);
+        atomicMax(&c.max_time_bits, f64_bits(l.next));
+        atomicAdd(&c.n_speciation, 1ULL);
+        return kStepSpeciated;
+    }
+
+    const uint64_t e2 = draw_at(rs, 2);
+    const uint64_t e3 = draw_at(rs, 3);
+    uint32_t tx, ty, ti;
+    if (KIND == kNonSpatial) {
+        non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, tx, ty);
+        ti = coalescence_index(e3, p.deme);
+    } else if (KIND == kSpatiallyImplicit) {
+        // dispersal_sampler/spatially_implicit.rs:58-86
+        const bool local = in_local(p, l.x, l.y);
+        const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
+        const uint64_t d_index = local ? e3 : e2;
+        const uint64_t d_coal = local ? draw_at(rs, 4) : e3;
+        if (to_meta)
+            non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
+        else
+            non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, tx, ty);
+        // habitat/spatially_implicit.rs:95-103: local extent first
+        ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
+    } else if (KIND == kAlmostInfiniteNormal) {
+        // sample e4 is CoalescenceRngSample::new's draw; singleton demes -> index 0
+        normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
+        ti = 0;
+    } else {
+        uint64_t d_coal;
+        if (!spatially_explicit_dispersal_draw(e2, e3, rs, p, l.x, l.y, l.rec, tx, ty, d_coal, k.status) ||
+            !load_cell(p, tx, ty, l.rec, k.status))
+            return kStepDropped;
+        ti = coalescence_index(d_coal, l.rec.habitat);
+    }
+    if (k.report_dispersal) {
+        const unsigned long long e = atomicAdd(k.n_disp_total, 1ULL);
+        if (e < k.disp_cap) {
+            DevDispersalEvent ev;
+            ev.gref = l.gref;
+            ev.prior_time = l.last;
+            ev.event_time = l.next;
+            ev.x = l.x;
+            ev.y = l.y;
+            ev.idx = l.i;
+            ev.tx = tx;
+            ev.ty = ty;
+            ev.tidx = ti;
+            ev.sim = l.s;
+            ev.pad = 0;
+            k.disp[e] = ev;
+        } else {
+            set_status(k.status, kErrDispersalOverflow);
+        }
+    }
+    l.x = tx;
+    l.y = ty;
+    l.i = ti;
+    l.last = l.next;
+    l.has_next = false;
+    return kStepMoved;
+}
+
+// Copies lane 0's lineage registers to every lane of the warp.
+__device__ __forceinline__ void broadcast_from_lane0(Lane &l) {
+    l.slot = __shfl_sync(kFull, l.slot, 0);
+    l.x = __shfl_sync(kFull, l.x, 0);
+    l.y = __shfl_sync(kFull, l.y, 0);
+    l.i = __shfl_sync(kFull, l.i, 0);
+    l.s = __shfl_sync(kFull, l.s, 0);
+    l.last = __shfl_sync(kFull, l.last, 0);
+    l.next = __shfl_sync(kFull, l.next, 0);
+    l.horizon = __shfl_sync(kFull, l.horizon, 0);
+    l.reprime = __shfl_sync(kFull, l.reprime, 0);
+    l.gref = __shfl_sync(kFull, l.gref, 0);
+    l.steps = __shfl_sync(kFull, l.steps, 0);
+    l.has_next = __shfl_sync(kFull, l.has_next ? 1 : 0, 0) != 0;
+    l.rec.injection = __shfl_sync(kFull, l.rec.injection, 0);
+    l.rec.self_dispersal = __shfl_sync(kFull, l.rec.self_dispersal, 0);
+    l.rec.atom_start = __shfl_sync(kFull, l.rec.atom_start, 0);
+    l.rec.atom_count = __shfl_sync(kFull, l.rec.atom_count, 0);
+    l.rec.habitat = __shfl_sync(kFull, l.rec.habitat, 0);
+    l.rec.non_self_event = __shfl_sync(kFull, l.rec.non_self_event, 0);
+}
+
+// lineage_step for one lineage held (identically) by all 32 lanes of a warp:
+// the Poisson sampler evaluates 8 consecutive buckets at once (4 lanes per
+// bucket, one event-time sample each) and keeps the first bucket with an
+// event after `before` -- the same bucket and event the sequential loop of
+// poisson.rs:48-100 stops at -- and the event's four samples are drawn in
+// parallel lanes.  Side effects (events, counters) happen on lane 0 only;
+// every lane returns with the same updated lineage.
+template <int KIND>
+__device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, const EventSink &k) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+    uint64_t rs;
+    if (!l.has_next) {
+        const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
+        const long long before_bits = __double_as_longlong(before);
+        const double q = p.inv_delta_t != 0.0 ? __dmul_rn(before, p.inv_delta_t) : __ddiv_rn(before, p.delta_t);
+        const uint32_t b = lane >> 2, e = lane & 3u;
+        uint64_t base = f64_to_u64(floor(q));
+        long long best_bits = 0;
+        uint32_t best_k = 0;
+        uint64_t best_ts = 0;
+        for (;;) {
+            const uint64_t ts = base + b;
+            const uint64_t s0 = primed_state(loc_term, ts);
+            const uint32_t n_ev = poisson_count(draw_at(s0, 1), p);
+            const double step_start = __ull2double_rn(ts);
+            // this lane's candidates: event indices e, e + 4, ... < n_ev
+            long long mine = 0x7fffffffffffffffLL;
+            uint32_t mine_k = 0xffffffffu;
+            for (uint32_t kk = e; kk < n_ev; kk += 4) {
+                const double et =
+                    __dmul_rn(__dadd_rn(step_start, unit_closed_open(draw_at(s0, kk + 2))), p.delta_t);
+                const long long eb = __double_as_longlong(et);
+                if (eb > before_bits && eb < mine) {  // kk ascending: ties keep the lower index
+                    mine = eb;
+                    mine_k = kk;
+                }
+            }
+            // minimum over the bucket's 4 lanes (ties: lowest event index)
+#pragma unroll
+            for (int off = 1; off < 4; off <<= 1) {
+                const long long ob = __shfl_xor_sync(kFull, mine, off);
+                const uint32_t ok = __shfl_xor_sync(kFull, mine_k, off);
+                if (ob < mine || (ob == mine && ok < mine_k)) {
+                    mine = ob;
+                    mine_k = ok;
+                }
+            }
+            // the first of the 8 buckets with an event
+            const unsigned found = __ballot_sync(kFull, mine != 0x7fffffffffffffffLL && e == 0);
+            if (found) {
+                const int leader = __ffs(found) - 1;
+                best_bits = __shfl_sync(kFull, mine, leader);
+                best_k = __shfl_sync(kFull, mine_k, leader);
+                best_ts = base + (uint64_t)(leader >> 2);
+                break;
+            }
+            base += 8;
+        }
+        l.reprime = best_ts + kInvPhi * (uint64_t)(best_k + 1);
+        rs = primed_state(loc_term, l.reprime);
+        l.next = max_after(before, __longlong_as_double(best_bits));
+        l.has_next = true;
+    } else {
+        rs = primed_state(loc_term, l.reprime);
+    }
+    if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
+
+    l.steps += 1;
+    // samples 1..4 of the event, one per lane, shared
+    const uint64_t dk = draw_at(rs, (lane & 3u) + 1u);
+    const uint64_t e1 = __shfl_sync(kFull, dk, 0);
+    const uint64_t e2 = __shfl_sync(kFull, dk, 1);
+    const uint64_t e3 = __shfl_sync(kFull, dk, 2);
+    const uint64_t e4 = __shfl_sync(kFull, dk, 3);
+    if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
+        if (lane == 0) {
+            const unsigned long long ev_i = atomicAdd(k.n_spec_total, 1ULL);
+            if (ev_i < k.spec_cap) {
+                DevSpeciationEvent ev;
+                ev.gref = l.gref;
+                ev.prior_time = l.last;
+                ev.event_time = l.next;
+                ev.x = l.x;
+                ev.y = l.y;
+                ev.idx = l.i;
+                ev.sim = l.s;
+                k.spec[ev_i] = ev;
+            } else {
+                set_status(k.status, kErrEventOverflow);
+            }
+            SimCounters &c = k.counters[l.s];
+            atomicAdd(&c.steps, (unsigned long long)l.steps);
+            atomicMax(&c.max_time_bits, f64_bits(l.next));
+            atomicAdd(&c.n_speciation, 1ULL);
+        }
+        return kStepSpeciated;
+    }
+    uint32_t tx, ty, ti;
+    if (KIND == kNonSpatial) {
+        non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, tx, ty);
+        ti = coalescence_index(e3, p.deme);
+    } else if (KIND == kSpatiallyImplicit) {
+        const bool local = in_local(p, l.x, l.y);
+        const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
+        const uint64_t d_index = local ? e3 : e2;
+        const uint64_t d_coal = local ? e4 : e3;
+        if (to_meta)
+            non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
+        else
+            non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, tx, ty);
+        ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
+    } else if (KIND == kAlmostInfiniteNormal) {
+        normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
+        ti = 0;
+    } else {
+        uint64_t d_coal;
+        if (!spatially_explicit_dispersal_draw(e2, e3, rs, p, l.x, l.y, l.rec, tx, ty, d_coal, k.status) ||
+            !load_cell(p, tx, ty, l.rec, k.status))
+            return kStepDropped;
+        ti = coalescence_index(d_coal, l.rec.habitat);
+    }
+    l.x = tx;
+    l.y = ty;
+    l.i = ti;
+    l.last = l.next;
+    l.has_next = false;
+    return kStepMoved;
+}
+
+__device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
+    EventSink k;
+    k.spec = a.spec;
+    k.n_spec_total = a.n_spec_total;
+    k.spec_cap = a.spec_cap;
+    k.disp = a.disp;
+    k.n_disp_total = a.n_disp_total;
+    k.disp_cap = a.disp_cap;
+    k.report_dispersal = a.report_dispersal;
+    k.status = a.status;
+    k.counters = a.counters;
+    return k;
+}
+
 // One lane per lineage at a time; a lane whose lineage reaches the horizon
 // (or speciates) takes the next lineage of the queue, so warps stay full
 // while lineages of very different event counts drain.
@@ -137,6 +426,7 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         __syncthreads();
     }
     const SimParams *P = SINGLE ? reinterpret_cast<const SimParams *>(params_smem) : a.params;
+    const EventSink sink = sink_of(a);
     const uint64_t n = *a.n_cur;
     const unsigned lane_id = threadIdx.x & 31u;
     const unsigned lanemask_lt = (1u << lane_id) - 1u;
@@ -171,8 +461,6 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
                         l.steps = a.in.steps[slot];
                         l.has_next = a.in.has_next[slot] != 0;
                         l.horizon = p.horizon;
-                        l.g.seed = p.seed;
-                        l.g.state = p.seed;
                         have = true;
                         if (KIND == kSpatiallyExplicit) have = load_cell(p, l.x, l.y, l.rec, a.status);
                     }
@@ -184,22 +472,13 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         if (!__any_sync(kFull, have)) break;
         if (!have) continue;
 
-        const SimParams &p = P[SINGLE ? 0 : l.s];
-        const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
-        uint64_t rs;  // WyHash state re-primed for the event
-        if (!l.has_next) {
-            // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
-            // (active_lineage_sampler/independent/sampler.rs:69-116)
-            const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
-            const double t = poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
-            l.next = max_after(before, t);
-            l.has_next = true;
-        } else {
-            rs = primed_state(loc_term, l.reprime);
+        const int r = lineage_step<KIND>(l, P[SINGLE ? 0 : l.s], sink);
+        if (r == kStepMoved) {
+            local_steps += 1;
+            continue;
         }
-
-        if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) {  // non-negative
-            // early stop: keep the peeked time for the next round
+        if (r == kStepStop) {
+            // keep the peeked time for the next round
             a.in.x[l.slot] = l.x;
             a.in.y[l.slot] = l.y;
             a.in.idx[l.slot] = l.i;
@@ -208,107 +487,268 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
             a.in.reprime[l.slot] = l.reprime;
             a.in.steps[l.slot] = l.steps;
             a.in.has_next[l.slot] = 1;
-            have = false;
-            continue;
-        }
-
-        // IndependentEventSampler::sample_event_for_lineage_at_event_time_or_emigrate
-        // (event_sampler/independent.rs:112-222)
-        l.steps += 1;
-        local_steps += 1;
-        // the event's samples 1..4 after the re-prime, drawn up front; which
-        // of them the dispersal and coalescence use depends on the branch
-        const uint64_t e1 = draw_at(rs, 1);
-        const uint64_t e2 = draw_at(rs, 2);
-        const uint64_t e3 = draw_at(rs, 3);
-        const uint64_t e4 = (KIND == kNonSpatial) ? 0 : draw_at(rs, 4);
-        // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
-        if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
-            const unsigned long long e = atomicAdd(a.n_spec_total, 1ULL);
-            if (e < a.spec_cap) {
-                DevSpeciationEvent ev;
-                ev.gref = l.gref;
-                ev.prior_time = l.last;
-                ev.event_time = l.next;
-                ev.x = l.x;
-                ev.y = l.y;
-                ev.idx = l.i;
-                ev.sim = l.s;
-                a.spec[e] = ev;
-            } else {
-                set_status(a.status, kErrEventOverflow);
-            }
-            a.state[l.slot] = 1;
-            SimCounters &c = a.counters[l.s];
-            atomicAdd(&c.steps, (unsigned long long)l.steps);
-            atomicMax(&c.max_time_bits, f64_bits(l.next));
-            atomicAdd(&c.n_speciation, 1ULL);
-            have = false;
-            continue;
-        }
-
-        uint32_t tx, ty, ti;
-        if (KIND == kNonSpatial) {
-            non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, tx, ty);
-            ti = coalescence_index(e3, p.deme);
-        } else if (KIND == kSpatiallyImplicit) {
-            // dispersal_sampler/spatially_implicit.rs:58-86
-            const bool local = in_local(p, l.x, l.y);
-            const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
-            const uint64_t d_index = local ? e3 : e2;
-            const uint64_t d_coal = local ? e4 : e3;
-            if (to_meta)
-                non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
-            else
-                non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, tx, ty);
-            // habitat/spatially_implicit.rs:95-103: local extent first
-            ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
-        } else if (KIND == kAlmostInfiniteNormal) {
-            // sample e4 is CoalescenceRngSample::new's draw; singleton demes -> index 0
-            normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
-            ti = 0;
         } else {
-            uint64_t d_coal;
-            if (!spatially_explicit_dispersal_draw(e2, e3, e4, p, l.x, l.y, l.rec, tx, ty, d_coal,
-                                                   a.status) ||
-                !load_cell(p, tx, ty, l.rec, a.status)) {
-                a.state[l.slot] = 2;  // dropped by a failed bound check
-                have = false;
-                continue;
-            }
-            ti = coalescence_index(d_coal, l.rec.habitat);
+            if (r == kStepSpeciated) local_steps += 1;
+            a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
         }
-        if (a.report_dispersal) {
-            const unsigned long long e = atomicAdd(a.n_disp_total, 1ULL);
-            if (e < a.disp_cap) {
-                DevDispersalEvent ev;
-                ev.gref = l.gref;
-                ev.prior_time = l.last;
-                ev.event_time = l.next;
-                ev.x = l.x;
-                ev.y = l.y;
-                ev.idx = l.i;
-                ev.tx = tx;
-                ev.ty = ty;
-                ev.tidx = ti;
-                ev.sim = l.s;
-                ev.pad = 0;
-                a.disp[e] = ev;
-            } else {
-                set_status(a.status, kErrDispersalOverflow);
-            }
-        }
-        l.x = tx;
-        l.y = ty;
-        l.i = ti;
-        l.last = l.next;
-        l.has_next = false;
+        have = false;
     }
     if (a.steps_total) {
         // one atomic per warp for the launch's event count
         unsigned long long w = local_steps;
         for (int off = 16; off > 0; off >>= 1) w += __shfl_down_sync(kFull, w, off);
         if (lane_id == 0 && w) atomicAdd(a.steps_total, w);
+    }
+}
+
+// Per-simulation horizon rule (canonical schedule):
+// H' = min(H + clamp(ceil(min_round_events / n), step_slice, step_slice_max) / lambda, pause),
+// or no further round when n == 0 or H has reached pause_before.
+__device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long long live, double &h) {
+    const bool paused = p.pause_before >= 0.0 && !(p.horizon < p.pause_before);
+    if (live == 0 || paused) return false;
+    const unsigned long long step_slice = p.step_slice ? p.step_slice : 1ULL;
+    unsigned long long per = (p.min_round_events + live - 1) / live;
+    if (p.step_slice_max && per > p.step_slice_max) per = p.step_slice_max;
+    if (per < step_slice) per = step_slice;
+    h = __dadd_rn(p.horizon, __ddiv_rn(__ull2double_rn(per), p.lambda));
+    if (p.pause_before >= 0.0 && p.pause_before < h) h = p.pause_before;
+    return true;
+}
+
+// A simulation with at most kResidentMax live lineages is advanced by one
+// thread block on its own: the block runs the simulation's rounds (the same
+// horizons and the same smallest-global-reference dedup as the global
+// kernels) with its lineages in registers and the dedup in shared memory,
+// so small simulations progress at their own pace instead of waiting for
+// the whole batch at every round.  A launch runs at most `budget` rounds per
+// simulation; lineages are kept in the simulation's segment of the resident
+// arena between launches.
+//
+// Lineage slot j lives on warp j % 8, lane j / 8: a simulation with few
+// lineages gets one lineage per warp, so lineages never share (and diverge
+// within) a warp until there are more than eight of them.
+template <int KIND>
+__global__ void __launch_bounds__(kResidentMax) resident_kernel(ResidentArgs a) {
+    constexpr unsigned kWarps = kResidentMax / 32;
+    __shared__ uint32_t sx[kResidentMax], sy[kResidentMax], si[kResidentMax];
+    __shared__ unsigned long long slast[kResidentMax], sgref[kResidentMax];
+    __shared__ unsigned char salive[kResidentMax];
+    __shared__ unsigned int sscan[kResidentMax];
+    __shared__ unsigned int s_n;
+    __shared__ int s_go;
+    __shared__ double s_h;
+    // staging of surviving lineages during the block's compaction
+    __shared__ uint32_t tx_[kResidentMax], ty_[kResidentMax], ti_[kResidentMax];
+    __shared__ double tlast[kResidentMax], tnext[kResidentMax];
+    __shared__ unsigned long long trep[kResidentMax], tgref[kResidentMax], tsteps[kResidentMax];
+    __shared__ unsigned char thas[kResidentMax];
+
+    const unsigned t = threadIdx.x;
+    const unsigned j = (t & 31u) * kWarps + (t >> 5);  // this thread's lineage slot
+    EventSink sink;
+    sink.spec = a.spec;
+    sink.n_spec_total = a.n_spec_total;
+    sink.spec_cap = a.spec_cap;
+    sink.disp = nullptr;
+    sink.n_disp_total = nullptr;
+    sink.disp_cap = 0;
+    sink.report_dispersal = 0;
+    sink.status = a.status;
+    sink.counters = a.counters;
+
+    for (uint32_t s = blockIdx.x; s < a.n_sims; s += gridDim.x) {
+        SimParams &pm = a.params[s];
+        if (t == 0) {
+            // resident == 2: owned by this kernel (1: routed, handed over at
+            // the next launch boundary)
+            s_go = (pm.resident == 2 && pm.active) ? 1 : 0;
+            s_n = (unsigned)a.counters[s].n_live;
+            s_h = pm.horizon;
+        }
+        __syncthreads();
+        if (!s_go) {
+            __syncthreads();
+            continue;
+        }
+        const SimParams &p = pm;
+        const uint64_t seg = p.lineage_offset;
+        unsigned n = s_n;
+        if (n > (unsigned)kResidentMax) {  // never routed with more: guard the block's arrays
+            if (t == 0) set_status(a.status, kErrResident);
+            n = kResidentMax;
+        }
+        Lane l;
+        bool alive = j < n;
+        if (alive) {
+            const uint64_t g = seg + j;
+            l.slot = (uint32_t)g;
+            l.s = s;
+            l.x = a.arena.x[g];
+            l.y = a.arena.y[g];
+            l.i = a.arena.idx[g];
+            l.last = a.arena.last[g];
+            l.next = a.arena.next[g];
+            l.reprime = a.arena.reprime[g];
+            l.gref = a.arena.gref[g];
+            l.steps = a.arena.steps[g];
+            l.has_next = a.arena.has_next[g] != 0;
+            if (KIND == kSpatiallyExplicit) alive = load_cell(p, l.x, l.y, l.rec, a.status);
+        }
+        for (uint32_t round = 0; round < a.budget; ++round) {
+            // advance every lineage to the round's horizon
+            l.horizon = s_h;
+            unsigned long long my_events = 0;
+            if (n <= kWarps) {
+                // at most one lineage per warp (slot w on lane 0 of warp w):
+                // the whole warp steps it cooperatively
+                Lane c = l;
+                broadcast_from_lane0(c);
+                const bool c_alive = __shfl_sync(kFull, alive ? 1 : 0, 0) != 0;
+                if (c_alive) {
+                    bool c_live = true;
+                    for (;;) {
+                        const int r = lineage_step_coop<KIND>(c, p, sink);
+                        if (r == kStepMoved) {
+                            ++my_events;
+                            continue;
+                        }
+                        if (r == kStepSpeciated) {
+                            ++my_events;
+                            c_live = false;
+                        } else if (r == kStepDropped) {
+                            c_live = false;
+                        }
+                        break;
+                    }
+                    if ((t & 31u) == 0) {
+                        l = c;
+                        alive = c_live;
+                    } else {
+                        my_events = 0;
+                    }
+                }
+            } else if (alive) {
+                for (;;) {
+                    const int r = lineage_step<KIND>(l, p, sink);
+                    if (r == kStepMoved) {
+                        ++my_events;
+                        continue;
+                    }
+                    if (r == kStepSpeciated) {
+                        ++my_events;
+                        alive = false;
+                    } else if (r == kStepDropped) {
+                        alive = false;
+                    }
+                    break;
+                }
+            }
+            if (a.steps_total && my_events) atomicAdd(a.steps_total, my_events);
+            // dedup: a live lineage survives unless another live lineage in
+            // the same state (location, index, last event time) has a smaller
+            // global reference
+            if (j < n) {
+                sx[j] = l.x;
+                sy[j] = l.y;
+                si[j] = l.i;
+                slast[j] = (unsigned long long)__double_as_longlong(l.last);
+                sgref[j] = l.gref;
+                salive[j] = alive ? 1 : 0;
+            }
+            __syncthreads();
+            bool survivor = alive;
+            if (alive) {
+                const unsigned long long lb = (unsigned long long)__double_as_longlong(l.last);
+                for (unsigned k2 = 0; k2 < n; ++k2) {
+                    if (salive[k2] && sgref[k2] < l.gref && sx[k2] == l.x && sy[k2] == l.y &&
+                        si[k2] == l.i && slast[k2] == lb) {
+                        survivor = false;
+                        break;
+                    }
+                }
+                if (!survivor) {
+                    SimCounters &c = a.counters[s];
+                    atomicAdd(&c.steps, (unsigned long long)l.steps);
+                    atomicMax(&c.max_time_bits, f64_bits(l.last));
+                    atomicAdd(&c.n_dedup, 1ULL);
+                }
+            }
+            // inclusive scan of the survivor flags in slot order
+            sscan[j] = survivor ? 1u : 0u;
+            __syncthreads();
+            for (unsigned d = 1; d < (unsigned)kResidentMax; d <<= 1) {
+                const unsigned add = (j >= d) ? sscan[j - d] : 0u;
+                __syncthreads();
+                sscan[j] += add;
+                __syncthreads();
+            }
+            const unsigned total = sscan[kResidentMax - 1];
+            if (survivor) {
+                const unsigned d = sscan[j] - 1u;
+                tx_[d] = l.x;
+                ty_[d] = l.y;
+                ti_[d] = l.i;
+                tlast[d] = l.last;
+                tnext[d] = l.next;
+                trep[d] = l.reprime;
+                tgref[d] = l.gref;
+                tsteps[d] = l.steps;
+                thas[d] = l.has_next ? 1 : 0;
+            }
+            __syncthreads();
+            const unsigned n_prev = n;
+            n = total;
+            alive = j < n;
+            if (alive) {
+                l.x = tx_[j];
+                l.y = ty_[j];
+                l.i = ti_[j];
+                l.last = tlast[j];
+                l.next = tnext[j];
+                l.reprime = trep[j];
+                l.gref = tgref[j];
+                l.steps = tsteps[j];
+                l.has_next = thas[j] != 0;
+                if (KIND == kSpatiallyExplicit) alive = load_cell(p, l.x, l.y, l.rec, a.status);
+            }
+            // the simulation's schedule, as the global scheduler would do it
+            if (t == 0) {
+                SimCounters &c = a.counters[s];
+                atomicAdd(a.visits, (unsigned long long)n_prev);
+                c.n_live = n;
+                double h;
+                if (next_horizon(pm, n, h)) {
+                    pm.horizon = h;
+                    c.n_rounds += 1;
+                    s_h = h;
+                    s_go = 1;
+                    // the global rounds running beside this launch have
+                    // finished: hand control back (the state is consistent)
+                    if (a.stop_flag && *(volatile const int *)a.stop_flag) s_go = 2;
+                } else {
+                    pm.active = 0;
+                    atomicSub(a.n_resident, 1u);
+                    s_go = 0;
+                }
+            }
+            __syncthreads();
+            if (s_go != 1) break;
+        }
+        // keep the survivors (and their peeked next events) in the arena
+        if (j < n) {
+            const uint64_t g = seg + j;
+            a.arena.x[g] = l.x;
+            a.arena.y[g] = l.y;
+            a.arena.idx[g] = l.i;
+            a.arena.last[g] = l.last;
+            a.arena.next[g] = l.next;
+            a.arena.reprime[g] = l.reprime;
+            a.arena.gref[g] = l.gref;
+            a.arena.steps[g] = l.steps;
+            a.arena.has_next[g] = l.has_next ? 1 : 0;
+        }
+        __syncthreads();
     }
 }
 
@@ -370,14 +810,20 @@ __global__ void dedup_compact_kernel(DedupArgs a) {
             survivor = (slot == kEmpty) || a.min_gref[slot] == a.in.gref[j];
             dup = !survivor;
         }
-        const unsigned sv = __ballot_sync(kFull, survivor);
+        // survivors of a simulation that started the round with at most
+        // kResidentMax lineages move to its segment of the resident arena
+        // (the resident kernel owns the simulation from the next round on)
+        const bool to_arena = survivor && a.arena.x != nullptr &&
+                              a.counters[s].n_live <= (unsigned long long)kResidentMax;
+        const bool to_out = survivor && !to_arena;
+        const unsigned sv = __ballot_sync(kFull, to_out);
         unsigned long long dst_base = 0;
         if (sv) {
             const int leader = __ffs(sv) - 1;
             if ((int)lane_id == leader) dst_base = atomicAdd(a.out_count, (unsigned long long)__popc(sv));
             dst_base = __shfl_sync(kFull, dst_base, leader);
         }
-        if (survivor) {
+        if (to_out) {
             const uint64_t d = dst_base + __popc(sv & ((1u << lane_id) - 1u));
             a.out.x[d] = a.in.x[j];
             a.out.y[d] = a.in.y[j];
@@ -391,10 +837,26 @@ __global__ void dedup_compact_kernel(DedupArgs a) {
             a.out.has_next[d] = a.in.has_next[j];
             a.state_out[d] = 0;
         }
-        // per-simulation live counts, aggregated over lanes of the same simulation
-        const unsigned same = __match_any_sync(kFull, survivor ? s : 0xffffffffu);
-        if (survivor && (__ffs(same) - 1) == (int)lane_id)
+        // per-simulation live counts, aggregated over lanes of the same
+        // simulation (the count doubles as the arena slot of a moved lineage)
+        const unsigned same = __match_any_sync(kFull, to_out ? s : 0xffffffffu);
+        if (to_out && (__ffs(same) - 1) == (int)lane_id)
             atomicAdd(&a.counters[s].n_live_next, (unsigned long long)__popc(same));
+        if (to_arena) {
+            SimCounters &c = a.counters[s];
+            const uint64_t d = a.params[s].lineage_offset + atomicAdd(&c.n_live_next, 1ULL);
+            c.routed = 1;
+            a.arena.x[d] = a.in.x[j];
+            a.arena.y[d] = a.in.y[j];
+            a.arena.idx[d] = a.in.idx[j];
+            a.arena.sim[d] = s;
+            a.arena.last[d] = a.in.last[j];
+            a.arena.next[d] = a.in.next[j];
+            a.arena.reprime[d] = a.in.reprime[j];
+            a.arena.gref[d] = a.in.gref[j];
+            a.arena.steps[d] = a.in.steps[j];
+            a.arena.has_next[d] = a.in.has_next[j];
+        }
         if (dup) {
             SimCounters &c = a.counters[s];
             atomicAdd(&c.steps, (unsigned long long)a.in.steps[j]);
@@ -426,30 +888,30 @@ __global__ void schedule_kernel(ScheduleArgs a) {
     for (uint32_t s = threadIdx.x; s < a.n_sims; s += blockDim.x) {
         SimParams &p = a.params[s];
         SimCounters &c = a.counters[s];
+        if (p.resident) continue;  // the resident kernel schedules it
         const unsigned long long live = c.n_live_next;
         c.n_live = live;
         c.n_live_next = 0;
-        const bool paused = p.pause_before >= 0.0 && !(p.horizon < p.pause_before);
-        if (live > 0 && !paused) {
-            const unsigned long long step_slice = p.step_slice ? p.step_slice : 1ULL;
-            unsigned long long per = (p.min_round_events + live - 1) / live;
-            if (p.step_slice_max && per > p.step_slice_max) per = p.step_slice_max;
-            if (per < step_slice) per = step_slice;
-            double h = __dadd_rn(p.horizon, __ddiv_rn(__ull2double_rn(per), p.lambda));
-            if (p.pause_before >= 0.0 && p.pause_before < h) h = p.pause_before;
+        double h;
+        const bool more = next_horizon(p, live, h);
+        if (more) {
             p.horizon = h;
-            p.active = 1;
             c.n_rounds += 1;
+        }
+        p.active = more ? 1 : 0;
+        if (c.routed) {
+            // its survivors are in the resident arena
+            p.resident = 1;
+            if (more) atomicAdd(a.n_resident, 1u);
+        } else if (more) {
             my_active += 1;
-        } else {
-            p.active = 0;
         }
     }
     atomicAdd(&active_sum, my_active);
     __syncthreads();
     if (threadIdx.x == 0) {
         *a.n_active = active_sum;
-        if (active_sum > 0) *a.visits += *a.out_count;
+        if (active_sum > 0) atomicAdd(a.visits, *a.out_count);  // shared with the resident kernel
         const unsigned long long n = *a.out_count;
         *a.n_cur = n;
         *a.out_count = 0;
@@ -506,6 +968,29 @@ cudaError_t launch_dedup(const DedupArgs &a, unsigned grid, unsigned block, cuda
 
 cudaError_t launch_schedule(const ScheduleArgs &a, cudaStream_t st) {
     schedule_kernel<<<1, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+// Hands simulations routed to the resident arena (resident == 1) over to the
+// resident kernel (resident == 2); runs while no kernel of either kind does.
+__global__ void promote_kernel(SimParams *params, uint32_t n_sims) {
+    for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n_sims; s += gridDim.x * blockDim.x)
+        if (params[s].resident == 1) params[s].resident = 2;
+}
+
+cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st) {
+    promote_kernel<<<1, 256, 0, st>>>(params, n_sims);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st) {
+    switch (kind) {
+    case kNonSpatial: resident_kernel<kNonSpatial><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kSpatiallyImplicit: resident_kernel<kSpatiallyImplicit><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kAlmostInfiniteNormal: resident_kernel<kAlmostInfiniteNormal><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kSpatiallyExplicit: resident_kernel<kSpatiallyExplicit><<<grid, kResidentMax, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -10,6 +10,8 @@
 namespace necsim {
 
 constexpr int kStepBlockMax = 256;
+// simulations with at most this many live lineages run in the resident kernel
+constexpr int kResidentMax = 256;
 
 struct StepArgs {
     LineageSoA in;                       // lineages of this round (updated in place)
@@ -32,6 +34,8 @@ struct StepArgs {
 };
 
 struct DedupArgs {
+    LineageSoA arena;                    // resident arena (x == nullptr: no routing)
+    const SimParams *params;             // lineage_offset of each simulation
     LineageSoA in;
     LineageSoA out;
     const uint8_t *state;
@@ -58,11 +62,31 @@ struct ScheduleArgs {
     unsigned long long table_size;
     unsigned int *n_active;
     unsigned long long *visits;          // lineages the scheduled rounds process
+    unsigned int *n_resident;            // active simulations owned by the resident kernel
 };
 
 cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st);
 cudaError_t step_kernel_occupancy(int kind, int block, int *blocks_per_sm);
 cudaError_t launch_dedup(const DedupArgs &a, unsigned grid, unsigned block, cudaStream_t st);
 cudaError_t launch_schedule(const ScheduleArgs &a, cudaStream_t st);
+
+struct ResidentArgs {
+    LineageSoA arena;                    // lineages of resident simulations, by segment
+    SimParams *params;
+    SimCounters *counters;
+    uint32_t n_sims;
+    uint32_t budget;                     // rounds per simulation in this launch
+    DevSpeciationEvent *spec;
+    unsigned long long *n_spec_total;
+    uint64_t spec_cap;
+    uint32_t *status;
+    unsigned long long *steps_total;
+    unsigned long long *visits;
+    unsigned int *n_resident;
+    const int *stop_flag;                // set when the concurrent global rounds end (nullable)
+};
+
+cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st);
+cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st);
 
 }  // namespace necsim

@@ -85,6 +85,9 @@ struct alignas(16) SimParams {
     uint64_t step_slice;
     uint64_t min_round_events;
     uint64_t step_slice_max;
+    uint64_t lineage_offset;  // first slot of the simulation's resident-arena segment
+    int32_t resident;         // 1 once the resident kernel owns the simulation
+    int32_t pad1;
     int32_t active;           // 1 while the simulation still advances
     int32_t pad;
 };
@@ -102,6 +105,7 @@ struct SimCounters {
     unsigned long long n_live;         // live lineages at the round start
     unsigned long long n_live_next;    // survivors of the current round
     unsigned long long n_dispersal;
+    unsigned long long routed;         // survivors were moved to the resident arena
 };
 
 // Lineage state, structure of arrays.
@@ -141,6 +145,7 @@ enum : uint32_t {
     kErrEventOverflow = 1u << 2, // speciation event buffer full
     kErrDedupFull = 1u << 3,     // dedup probe sequence exhausted
     kErrDispersalOverflow = 1u << 4,
+    kErrResident = 1u << 5,      // a resident simulation exceeded the block's capacity
 };
 
 }  // namespace necsim

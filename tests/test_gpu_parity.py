@@ -165,3 +165,17 @@ def test_batch_equals_single_runs(nb, syn):
         assert same_stream(batch[j].speciation, single.speciation)
         assert (batch[j].steps, batch[j].biodiversity, batch[j].n_rounds) == (
             single.steps, single.biodiversity, single.n_rounds)
+
+
+def test_resident_kernel_matches_global_rounds(nb, syn):
+    """Small simulations run in the per-simulation resident kernel; with it
+    switched off they stay in the global rounds: identical output."""
+    sims = syn.config4(n_sims=5, max_local=2000)
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] * 50 for d, _ in sims]
+    seeds = [s for _, s in sims]
+    a = nb.simulate_batch(scen, nus, seeds, nb.CUDA(resident=True), collect=True)
+    b = nb.simulate_batch(scen, nus, seeds, nb.CUDA(resident=False), collect=True)
+    for x, y in zip(a, b):
+        assert same_stream(x.speciation, y.speciation)
+        assert (x.steps, x.n_rounds, x.n_dedup, x.time) == (y.steps, y.n_rounds, y.n_dedup, y.time)
