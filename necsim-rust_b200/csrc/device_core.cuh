@@ -125,12 +125,6 @@ __device__ __forceinline__ int64_t f64_to_i64(double v) {
     return __double2ll_rz(v);
 }
 
-// rng.rs:133-145 RngSampler::sample_index_u64
-__device__ __forceinline__ uint64_t sample_index_u64(Rng &g, uint64_t length) {
-    const uint64_t index = f64_to_u64(floor(__dmul_rn(g.closed_open(), __ull2double_rn(length))));
-    return index < length - 1 ? index : length - 1;
-}
-
 // necsim/core/bond/src/positive_f64.rs:103-113 PositiveF64::max_after
 __device__ __forceinline__ double max_after(double before, double value) {
     if (value > before || before != before) return value;
@@ -138,67 +132,18 @@ __device__ __forceinline__ double max_after(double before, double value) {
     return __longlong_as_double(__double_as_longlong(before) + 1);
 }
 
-// event_time_sampler/poisson.rs:30-109: the next event time strictly after
-// `time` at the location with injection `inj`.  Leaves `g` primed with
-// (inj, reprime) exactly as the reference leaves its RNG, and returns the
-// re-prime time index in `reprime`.  `p0 = exp(-lambda * delta_t)` is a
-// per-run constant computed on the host with the system libm (the
-// reference's IntrinsicsMathsCore); p0 == 0 is rejected at set-up.
-__device__ __forceinline__ double poisson_next_event_time(Rng &g, uint64_t inj, double time,
-                                                          const SimParams &p, uint64_t &reprime) {
-    const double delta_t = p.delta_t;
-    // floor(time / delta_t); with a power-of-two delta_t the product with the
-    // exact reciprocal is the same correctly rounded quotient
-    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, delta_t);
-    uint64_t time_step = f64_to_u64(floor(q));
-    double best;
-    uint32_t best_k;
-    for (;;) {
-        g.prime(inj, time_step);
-        // Devroye's sequential inversion of Poisson(lambda * delta_t)
-        uint32_t n_events = 0;
-        double prod = p.p0;
-        double acc = p.p0;
-        const double u = g.closed_open();
-        while (u > acc && prod > 0.0) {
-            n_events += 1;
-            // lambda_dt / n: host-divided table for small n, same IEEE quotient
-            const double ratio = n_events <= (uint32_t)kPoissonTable
-                                     ? p.lambda_dt_over_k[n_events - 1]
-                                     : __ddiv_rn(p.lambda_dt, __uint2double_rn(n_events));
-            prod = __dmul_rn(prod, ratio);
-            acc = __dadd_rn(acc, prod);
-        }
-        bool found = false;
-        best = 0.0;
-        best_k = 0;
-        const double step_start = __ull2double_rn(time_step);
-        for (uint32_t k = 0; k < n_events; ++k) {
-            const double et = __dmul_rn(__dadd_rn(step_start, g.closed_open()), delta_t);
-            if (et > time && (!found || best > et)) {
-                best = et;
-                best_k = k;
-                found = true;
-            }
-        }
-        if (found) break;
-        time_step += 1;
-    }
-    reprime = time_step + kInvPhi * (uint64_t)(best_k + 1);
-    g.prime(inj, reprime);
-    return best;
-}
-
 // Devroye's Poisson(lambda * delta_t) count (poisson.rs:51-65) from the
 // bucket's first sample d1: the loop passes rank n while
-// X > floor(acc_n * 2^53) and prod_n > 0, continued in f64 beyond the
-// tabulated ranks.
+// X > floor(acc_n * 2^53) and prod_n > 0.  The thresholds are
+// non-decreasing and a rank with prod_n == 0 carries the threshold ~0, so
+// the stopping rank is the number of thresholds X exceeds: eight independent
+// compares instead of a loop of dependent loads.  Beyond the tabulated ranks
+// the reference loop continues in f64.
 __device__ __forceinline__ uint32_t poisson_count(uint64_t d1, const SimParams &p) {
     const uint64_t X = d1 >> 11;
-    const uint32_t alive = (uint32_t)__popc(p.poisson_alive);
-    const uint32_t limit = alive < (uint32_t)kPoissonThresholds ? alive : (uint32_t)kPoissonThresholds;
     uint32_t n_events = 0;
-    while (n_events < limit && X > p.poisson_threshold[n_events]) ++n_events;
+#pragma unroll
+    for (int r = 0; r < kPoissonThresholds; ++r) n_events += X > p.poisson_threshold[r] ? 1u : 0u;
     if (n_events == (uint32_t)kPoissonThresholds) {
         const double u = unit_closed_open(d1);
         double prod = p.poisson_prod_k;
@@ -215,51 +160,61 @@ __device__ __forceinline__ uint32_t poisson_count(uint64_t d1, const SimParams &
     return n_events;
 }
 
+// event time (t_s + u) * delta_t of a bucket's sample, as its bit pattern
+// (non-negative doubles order like their bits)
+__device__ __forceinline__ long long event_time_bits(double step_start, uint64_t d, double delta_t) {
+    return __double_as_longlong(__dmul_rn(__dadd_rn(step_start, unit_closed_open(d)), delta_t));
+}
+
 // One bucket of the Poisson sampler (poisson.rs:50-95) primed to s0: the
-// earliest event strictly after `time` (ties: lowest index), or -1.  The
-// Devroye uniform and the first two event-time uniforms are drawn up front.
+// earliest event strictly after `time` (ties: lowest index), or -1.  Samples
+// are drawn only as the reference consumes them (throughput form).
 __device__ __forceinline__ int poisson_bucket(uint64_t s0, uint64_t time_step, double time,
                                               const SimParams &p, double &best) {
-    const uint64_t d1 = draw_at(s0, 1);
-    // Devroye's loop on the constant acc_n sequence: it passes rank n while
-    // X > floor(acc_n * 2^53) and prod_n > 0 (thresholds are non-decreasing,
-    // alive bits a prefix)
-    const uint64_t X = d1 >> 11;
-    const uint32_t alive = (uint32_t)__popc(p.poisson_alive);
-    const uint32_t limit = alive < (uint32_t)kPoissonThresholds ? alive : (uint32_t)kPoissonThresholds;
-    uint32_t n_events = 0;
-    while (n_events < limit && X > p.poisson_threshold[n_events]) ++n_events;
-    if (n_events == (uint32_t)kPoissonThresholds) {
-        // continue the reference loop beyond the tabulated ranks
-        const double u = unit_closed_open(d1);
-        double prod = p.poisson_prod_k;
-        double acc = p.poisson_acc_k;
-        while (u > acc && prod > 0.0) {
-            n_events += 1;
-            const double ratio = n_events <= (uint32_t)kPoissonTable
-                                     ? p.lambda_dt_over_k[n_events - 1]
-                                     : __ddiv_rn(p.lambda_dt, __uint2double_rn(n_events));
-            prod = __dmul_rn(prod, ratio);
-            acc = __dadd_rn(acc, prod);
-        }
-    }
+    const uint32_t n_events = poisson_count(draw_at(s0, 1), p);
     if (n_events == 0) return -1;
-    // event times (t_s + u_k) * delta_t; non-negative doubles compare like
-    // their bit patterns
     const double step_start = __ull2double_rn(time_step);
     const long long time_bits = __double_as_longlong(time);
     int best_k = -1;
     long long best_bits = 0;
     for (uint32_t k = 0; k < n_events; ++k) {
-        const uint64_t d = draw_at(s0, k + 2);
-        const double et = __dmul_rn(__dadd_rn(step_start, unit_closed_open(d)), p.delta_t);
-        const long long eb = __double_as_longlong(et);
+        const long long eb = event_time_bits(step_start, draw_at(s0, k + 2), p.delta_t);
         if (eb > time_bits && (best_k < 0 || best_bits > eb)) {
             best_bits = eb;
             best_k = (int)k;
         }
     }
     best = __longlong_as_double(best_bits);
+    return best_k;
+}
+
+// The same bucket from its first three samples drawn ahead (latency form):
+// events 0 and 1 use d2 and d3, further events draw their samples here.
+__device__ __forceinline__ int poisson_bucket_drawn(uint64_t s0, uint64_t d1, uint64_t d2, uint64_t d3,
+                                                    uint64_t time_step, long long time_bits,
+                                                    const SimParams &p, long long &best_bits) {
+    const double step_start = __ull2double_rn(time_step);
+    const long long e0 = event_time_bits(step_start, d2, p.delta_t);
+    const long long e1 = event_time_bits(step_start, d3, p.delta_t);
+    const uint32_t n_events = poisson_count(d1, p);
+    int best_k = -1;
+    long long bb = 0;
+    if (n_events >= 1 && e0 > time_bits) {
+        bb = e0;
+        best_k = 0;
+    }
+    if (n_events >= 2 && e1 > time_bits && (best_k < 0 || bb > e1)) {
+        bb = e1;
+        best_k = 1;
+    }
+    for (uint32_t k = 2; k < n_events; ++k) {
+        const long long eb = event_time_bits(step_start, draw_at(s0, k + 2), p.delta_t);
+        if (eb > time_bits && (best_k < 0 || bb > eb)) {
+            bb = eb;
+            best_k = (int)k;
+        }
+    }
+    best_bits = bb;
     return best_k;
 }
 
@@ -284,48 +239,39 @@ __device__ __forceinline__ double poisson_next_event_time_ilp(uint64_t loc_term,
     }
 }
 
-// habitat/almost_infinite.rs:100-114 clamp_round_dispersal of a Box-Muller
-// draw (rng.rs:180-197; almost_infinite_normal.rs:58-68).  The transcendental
-// calls are CUDA's double-precision log/sin/cos; their results only pass
-// through round(), whose outcome equals the reference's (glibc) except when
-// the displacement lies within a few ulp of a half-integer.
-__device__ __forceinline__ void normal_dispersal(Rng &g, double sigma, uint32_t x, uint32_t y,
-                                                 uint32_t &tx, uint32_t &ty) {
-    const double u0 = g.open_closed();
-    const double u1 = g.closed_open();
-    const double r = __dsqrt_rn(__dmul_rn(-2.0, log(u0)));
-    const double theta = __dmul_rn(-kTau, u1);
-    const double z0 = __dmul_rn(r, sin(theta));
-    const double z1 = __dmul_rn(r, cos(theta));
-    const double dx = __dadd_rn(__dmul_rn(z0, sigma), 0.0);
-    const double dy = __dadd_rn(__dmul_rn(z1, sigma), 0.0);
-    const int64_t wrap = (int64_t)1 << 32;
-    const int64_t nx = ((int64_t)x + f64_to_i64(round(dx))) % wrap;
-    const int64_t ny = ((int64_t)y + f64_to_i64(round(dy))) % wrap;
-    tx = (uint32_t)((nx + wrap) % wrap);
-    ty = (uint32_t)((ny + wrap) % wrap);
-}
-
-// dispersal_sampler/non_spatial.rs:42-66 over an extent (ox, oy, w, h)
-__device__ __forceinline__ void non_spatial_dispersal(Rng &g, uint32_t ox, uint32_t oy, uint64_t w,
-                                                      uint64_t h, uint32_t &tx, uint32_t &ty) {
-    const uint64_t n = w * h;
-    const uint64_t idx = sample_index_u64(g, n);
-    if (h == 1) {  // idx < w: quotient 0
-        tx = ox + (uint32_t)idx;
-        ty = oy;
-    } else if (n <= 0xffffffffULL) {  // 32-bit divide (same quotient)
-        const uint32_t i32 = (uint32_t)idx, w32 = (uint32_t)w;
-        const uint32_t q = i32 / w32;
-        tx = ox + (i32 - q * w32);
-        ty = oy + q;
-    } else {
-        tx = ox + (uint32_t)(idx % w);
-        ty = oy + (uint32_t)(idx / w);
+// poisson_next_event_time for a lineage whose warp has few others to run
+// (latency form): buckets are primed two at a time, the second
+// speculatively, with each bucket's first three samples drawn at once, so
+// the dependent chain per event is one prime, one draw and the compares.
+__device__ __forceinline__ double poisson_next_event_time_lat(uint64_t loc_term, double time,
+                                                              const SimParams &p,
+                                                              uint64_t &reprime,
+                                                              uint64_t &reprimed_state) {
+    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
+    uint64_t time_step = f64_to_u64(floor(q));
+    const long long time_bits = __double_as_longlong(time);
+    for (;;) {
+        const uint64_t s0 = primed_state(loc_term, time_step);
+        const uint64_t s1 = primed_state(loc_term, time_step + 1);
+        const uint64_t a1 = draw_at(s0, 1), a2 = draw_at(s0, 2), a3 = draw_at(s0, 3);
+        const uint64_t b1 = draw_at(s1, 1), b2 = draw_at(s1, 2), b3 = draw_at(s1, 3);
+        long long bits = 0;
+        uint64_t chosen = time_step;
+        int k = poisson_bucket_drawn(s0, a1, a2, a3, time_step, time_bits, p, bits);
+        if (k < 0) {
+            chosen = time_step + 1;
+            k = poisson_bucket_drawn(s1, b1, b2, b3, chosen, time_bits, p, bits);
+        }
+        if (k >= 0) {
+            reprime = chosen + kInvPhi * (uint64_t)(k + 1);
+            reprimed_state = primed_state(loc_term, reprime);
+            return __longlong_as_double(bits);
+        }
+        time_step += 2;
     }
 }
 
-// ---- the same samplers fed with pre-drawn samples ----
+// ---- the samplers fed with pre-drawn samples ----
 
 // rng.rs:133-145 sample_index_u64 of one sample
 __device__ __forceinline__ uint64_t index_from_draw(uint64_t d, uint64_t length) {
@@ -333,19 +279,24 @@ __device__ __forceinline__ uint64_t index_from_draw(uint64_t d, uint64_t length)
     return index < length - 1 ? index : length - 1;
 }
 
+// n / d for n, d < 2^32 from magic = ceil(2^64 / d) (0 when d == 1)
+__device__ __forceinline__ uint32_t div_by_magic(uint32_t n, uint64_t magic) {
+    return magic ? (uint32_t)__umul64hi(magic, (uint64_t)n) : n;
+}
+
 // dispersal_sampler/non_spatial.rs:42-66
 __device__ __forceinline__ void non_spatial_dispersal_draw(uint64_t d, uint32_t ox, uint32_t oy,
-                                                           uint64_t w, uint64_t h, uint32_t &tx,
-                                                           uint32_t &ty) {
+                                                           uint64_t w, uint64_t h, uint64_t w_magic,
+                                                           uint32_t &tx, uint32_t &ty) {
     const uint64_t n = w * h;
     const uint64_t idx = index_from_draw(d, n);
     if (h == 1) {  // idx < w: quotient 0
         tx = ox + (uint32_t)idx;
         ty = oy;
-    } else if (n <= 0xffffffffULL) {  // 32-bit divide (same quotient)
-        const uint32_t i32 = (uint32_t)idx, w32 = (uint32_t)w;
-        const uint32_t q = i32 / w32;
-        tx = ox + (i32 - q * w32);
+    } else if (n <= 0xffffffffULL) {  // 32-bit quotient by the width's magic
+        const uint32_t i32 = (uint32_t)idx;
+        const uint32_t q = div_by_magic(i32, w_magic);
+        tx = ox + (i32 - q * (uint32_t)w);
         ty = oy + q;
     } else {
         tx = ox + (uint32_t)(idx % w);

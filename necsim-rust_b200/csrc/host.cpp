@@ -130,6 +130,12 @@ uint64_t count_origins(const necsim_scenario &sc) {
     }
 }
 
+// ceil(2^64 / d) for 1 < d < 2^32, 0 for d <= 1 (quotient = dividend)
+uint64_t division_magic(uint32_t d) {
+    if (d <= 1) return 0;
+    return ~0ULL / d + 1ULL;
+}
+
 SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64_t wy_seed) {
     SimParams p;
     std::memset(&p, 0, sizeof(p));
@@ -168,7 +174,10 @@ SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64
         double prod = p.p0, acc = p.p0;
         p.poisson_alive = 0;
         for (int n = 0; n < kPoissonThresholds; ++n) {
-            p.poisson_threshold[n] = (uint64_t)std::floor(std::ldexp(acc, 53));
+            // a rank whose prod is 0 stops the loop whatever the sample: its
+            // threshold is the largest u64, which no 53-bit X exceeds, so the
+            // count of exceeded thresholds is the loop's stopping rank
+            p.poisson_threshold[n] = prod > 0.0 ? (uint64_t)std::floor(std::ldexp(acc, 53)) : ~0ULL;
             if (prod > 0.0) p.poisson_alive |= 1u << n;
             prod = prod * (p.lambda_dt / (double)(n + 1));
             acc = acc + prod;
@@ -179,6 +188,8 @@ SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64
     // u < c  <=>  X < ceil(c * 2^53) for the 53-bit integer X of the uniform
     p.nu_threshold = (uint64_t)std::ceil(std::ldexp(sc.speciation_probability, 53));
     p.migration_threshold = (uint64_t)std::ceil(std::ldexp(sc.migration_probability, 53));
+    p.width_magic = division_magic(p.width);
+    p.meta_width_magic = division_magic(p.meta_width);
     p.pause_before = -1.0;
     return p;
 }

@@ -77,8 +77,9 @@ __device__ __forceinline__ bool load_cell(const SimParams &p, uint32_t x, uint32
 // packed_separable_alias/dispersal.rs:16-77 and alias/packed.rs:135-163, fed
 // with the event's samples 2..4: the self-dispersal test (when taken) uses
 // the first, the alias draw the next; `d_coal` receives the sample after them.
+template <bool EAGER>
 __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
-    uint64_t e2, uint64_t e3, uint64_t rs, const SimParams &p, uint32_t x, uint32_t y,
+    uint64_t e2, uint64_t e3, uint64_t e4, uint64_t rs, const SimParams &p, uint32_t x, uint32_t y,
     const CellRecord &rec, uint32_t &tx, uint32_t &ty, uint64_t &d_coal, uint32_t *status) {
     const uint64_t cell = (uint64_t)y * p.width + (uint64_t)x;
     uint64_t target;
@@ -96,7 +97,7 @@ __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
     } else {
         use_alias = unit_closed_open(e2) >= sd;
         d_alias = e3;
-        d_coal = use_alias ? draw_at(rs, 4) : e3;
+        d_coal = use_alias ? (EAGER ? e4 : draw_at(rs, 4)) : e3;
     }
     if (!use_alias) {
         target = cell;
@@ -113,9 +114,9 @@ __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
         const AliasAtom atom = p.atoms[at];
         target = (frac < atom.u) ? atom.e : atom.k;
     }
-    // cell indices are < 2^32 (one CellRecord per cell): 32-bit divide
+    // cell indices are < 2^32 (one CellRecord per cell): 32-bit quotient
     const uint32_t t32 = (uint32_t)target, w32 = p.width;
-    const uint32_t q = t32 / w32;
+    const uint32_t q = div_by_magic(t32, p.width_magic);
     tx = t32 - q * w32;
     ty = q;
     return true;
@@ -139,72 +140,59 @@ struct EventSink {
     SimCounters *counters;
 };
 
-// One step of a lineage: peek its next event time (or use the peek kept from
-// the previous round) and stop if it is at or beyond the horizon; otherwise
-// execute the event (speciation, or dispersal + coalescence index).
-template <int KIND>
-__device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const EventSink &k) {
-    const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
-    uint64_t rs;  // WyHash state re-primed for the event
-    if (!l.has_next) {
-        // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
-        // (active_lineage_sampler/independent/sampler.rs:69-116)
-        const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
-        const double t = poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
-        l.next = max_after(before, t);
-        l.has_next = true;
-    } else {
-        rs = primed_state(loc_term, l.reprime);
-    }
-    // the reference's early stop `next_event_time >= level_time`
-    // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
-    if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
-
-    // IndependentEventSampler::sample_event_for_lineage_at_event_time_or_emigrate
-    // (event_sampler/independent.rs:112-222)
+// The event at l.next (event_sampler/independent.rs:112-222) from the
+// re-primed state rs: speciation, or dispersal + coalescence index.  With
+// EAGER the event's samples 1..4 arrive drawn (e1..e4); otherwise samples 2..4
+// are drawn here only when the branch consumes them.  Only a lane with
+// `emit` writes events and counters (all lanes of a cooperative warp hold
+// the same lineage).
+template <int KIND, bool EAGER>
+__device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const EventSink &k, uint64_t rs,
+                                             uint64_t e1, uint64_t e2, uint64_t e3, uint64_t e4, bool emit) {
     l.steps += 1;
-    // the event's samples 1..4 after the re-prime, drawn up front; which of
-    // them the dispersal and coalescence use depends on the branch
-    const uint64_t e1 = draw_at(rs, 1);
     // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
     if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
-        const unsigned long long e = atomicAdd(k.n_spec_total, 1ULL);
-        if (e < k.spec_cap) {
-            DevSpeciationEvent ev;
-            ev.gref = l.gref;
-            ev.prior_time = l.last;
-            ev.event_time = l.next;
-            ev.x = l.x;
-            ev.y = l.y;
-            ev.idx = l.i;
-            ev.sim = l.s;
-            k.spec[e] = ev;
-        } else {
-            set_status(k.status, kErrEventOverflow);
+        if (emit) {
+            const unsigned long long e = atomicAdd(k.n_spec_total, 1ULL);
+            if (e < k.spec_cap) {
+                DevSpeciationEvent ev;
+                ev.gref = l.gref;
+                ev.prior_time = l.last;
+                ev.event_time = l.next;
+                ev.x = l.x;
+                ev.y = l.y;
+                ev.idx = l.i;
+                ev.sim = l.s;
+                k.spec[e] = ev;
+            } else {
+                set_status(k.status, kErrEventOverflow);
+            }
+            SimCounters &c = k.counters[l.s];
+            atomicAdd(&c.steps, (unsigned long long)l.steps);
+            atomicMax(&c.max_time_bits, f64_bits(l.next));
+            atomicAdd(&c.n_speciation, 1ULL);
         }
-        SimCounters &c = k.counters[l.s];
-        atomicAdd(&c.steps, (unsigned long long)l.steps);
-        atomicMax(&c.max_time_bits, f64_bits(l.next));
-        atomicAdd(&c.n_speciation, 1ULL);
         return kStepSpeciated;
     }
-
-    const uint64_t e2 = draw_at(rs, 2);
-    const uint64_t e3 = draw_at(rs, 3);
+    if (!EAGER) {
+        e2 = draw_at(rs, 2);
+        e3 = draw_at(rs, 3);
+    }
     uint32_t tx, ty, ti;
     if (KIND == kNonSpatial) {
-        non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, tx, ty);
+        non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, p.width_magic, tx, ty);
         ti = coalescence_index(e3, p.deme);
     } else if (KIND == kSpatiallyImplicit) {
         // dispersal_sampler/spatially_implicit.rs:58-86
         const bool local = in_local(p, l.x, l.y);
         const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
         const uint64_t d_index = local ? e3 : e2;
-        const uint64_t d_coal = local ? draw_at(rs, 4) : e3;
+        const uint64_t d_coal = local ? (EAGER ? e4 : draw_at(rs, 4)) : e3;
         if (to_meta)
-            non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
+            non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height,
+                                       p.meta_width_magic, tx, ty);
         else
-            non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, tx, ty);
+            non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, p.width_magic, tx, ty);
         // habitat/spatially_implicit.rs:95-103: local extent first
         ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
     } else if (KIND == kAlmostInfiniteNormal) {
@@ -213,12 +201,13 @@ __device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const E
         ti = 0;
     } else {
         uint64_t d_coal;
-        if (!spatially_explicit_dispersal_draw(e2, e3, rs, p, l.x, l.y, l.rec, tx, ty, d_coal, k.status) ||
+        if (!spatially_explicit_dispersal_draw<EAGER>(e2, e3, e4, rs, p, l.x, l.y, l.rec, tx, ty, d_coal,
+                                                      k.status) ||
             !load_cell(p, tx, ty, l.rec, k.status))
             return kStepDropped;
         ti = coalescence_index(d_coal, l.rec.habitat);
     }
-    if (k.report_dispersal) {
+    if (emit && k.report_dispersal) {
         const unsigned long long e = atomicAdd(k.n_disp_total, 1ULL);
         if (e < k.disp_cap) {
             DevDispersalEvent ev;
@@ -246,6 +235,37 @@ __device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const E
     return kStepMoved;
 }
 
+// One step of a lineage: peek its next event time (or use the peek kept from
+// the previous round) and stop if it is at or beyond the horizon; otherwise
+// execute the event.  LAT selects the latency form (two buckets primed at a
+// time, all samples drawn ahead) for lanes whose warp has little else to run;
+// the throughput form draws only what the reference consumes.
+template <int KIND, bool LAT>
+__device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const EventSink &k) {
+    const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+    uint64_t rs;  // WyHash state re-primed for the event
+    if (!l.has_next) {
+        // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
+        // (active_lineage_sampler/independent/sampler.rs:69-116)
+        const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
+        const double t = LAT ? poisson_next_event_time_lat(loc_term, before, p, l.reprime, rs)
+                             : poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
+        l.next = max_after(before, t);
+        l.has_next = true;
+    } else {
+        rs = primed_state(loc_term, l.reprime);
+    }
+    // the reference's early stop `next_event_time >= level_time`
+    // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
+    if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
+    const uint64_t e1 = draw_at(rs, 1);
+    if (LAT) {
+        return lineage_event<KIND, true>(l, p, k, rs, e1, draw_at(rs, 2), draw_at(rs, 3), draw_at(rs, 4),
+                                         true);
+    }
+    return lineage_event<KIND, false>(l, p, k, rs, e1, 0, 0, 0, true);
+}
+
 // Copies lane 0's lineage registers to every lane of the warp.
 __device__ __forceinline__ void broadcast_from_lane0(Lane &l) {
     l.slot = __shfl_sync(kFull, l.slot, 0);
@@ -268,42 +288,66 @@ __device__ __forceinline__ void broadcast_from_lane0(Lane &l) {
     l.rec.non_self_event = __shfl_sync(kFull, l.rec.non_self_event, 0);
 }
 
-// lineage_step for one lineage held (identically) by all 32 lanes of a warp:
-// the Poisson sampler evaluates 8 consecutive buckets at once (4 lanes per
-// bucket, one event-time sample each) and keeps the first bucket with an
-// event after `before` -- the same bucket and event the sequential loop of
-// poisson.rs:48-100 stops at -- and the event's four samples are drawn in
-// parallel lanes.  Side effects (events, counters) happen on lane 0 only;
-// every lane returns with the same updated lineage.
+constexpr long long kNoEvent = 0x7fffffffffffffffLL;
+
+// lineage_step for one lineage held (identically) by all 32 lanes of a warp.
+// Every lane computes exactly one prime and one draw per pass, so the
+// event's hash work costs the instruction stream of a single prime + draw:
+//   lanes  0..15: bucket b = lane / 4 of four consecutive buckets; role
+//                 r = lane % 4 draws sample r + 1 of the bucket (r = 0: the
+//                 Devroye sample, r = 1..3: the times of events 0..2);
+//   lanes 16..31: candidate c = (lane - 16) / 4 = (bucket c / 2, event c % 2)
+//                 re-primed as if it came next, drawing the event's sample
+//                 lane % 4 + 1.
+// The first bucket with an event after `before` (the bucket and event the
+// sequential loop of poisson.rs:48-100 stops at) selects the candidate whose
+// four lanes hold the event's samples; other events re-prime after the
+// selection.  Side effects happen on lane 0 only; every lane returns with
+// the same updated lineage.
 template <int KIND>
 __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, const EventSink &k) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
-    uint64_t rs;
+    uint64_t rs, e1, e2, e3, e4;
+    bool drawn = false;
     if (!l.has_next) {
         const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
         const long long before_bits = __double_as_longlong(before);
         const double q = p.inv_delta_t != 0.0 ? __dmul_rn(before, p.inv_delta_t) : __ddiv_rn(before, p.delta_t);
-        const uint32_t b = lane >> 2, e = lane & 3u;
+        const bool bucket_lane = lane < 16u;
+        const uint32_t role = lane & 3u;
+        const uint32_t grp = (lane >> 2) & 3u;  // bucket (lanes 0..15) or candidate (16..31)
         uint64_t base = f64_to_u64(floor(q));
         long long best_bits = 0;
         uint32_t best_k = 0;
         uint64_t best_ts = 0;
         for (;;) {
-            const uint64_t ts = base + b;
-            const uint64_t s0 = primed_state(loc_term, ts);
-            const uint32_t n_ev = poisson_count(draw_at(s0, 1), p);
-            const double step_start = __ull2double_rn(ts);
-            // this lane's candidates: event indices e, e + 4, ... < n_ev
-            long long mine = 0x7fffffffffffffffLL;
+            const uint64_t ts = base + (bucket_lane ? grp : (grp >> 1));
+            const uint64_t tindex = bucket_lane ? ts : ts + kInvPhi * (uint64_t)((grp & 1u) + 1u);
+            const uint64_t s = primed_state(loc_term, tindex);
+            const uint64_t d = draw_at(s, role + 1u);
+            // bucket lanes: the Devroye count from role 0, shared in the bucket
+            const uint32_t n_own = poisson_count(d, p);
+            const uint32_t n_ev = __shfl_sync(kFull, n_own, (int)(lane & ~3u));
+            long long mine = kNoEvent;
             uint32_t mine_k = 0xffffffffu;
-            for (uint32_t kk = e; kk < n_ev; kk += 4) {
-                const double et =
-                    __dmul_rn(__dadd_rn(step_start, unit_closed_open(draw_at(s0, kk + 2))), p.delta_t);
-                const long long eb = __double_as_longlong(et);
-                if (eb > before_bits && eb < mine) {  // kk ascending: ties keep the lower index
-                    mine = eb;
-                    mine_k = kk;
+            if (bucket_lane) {
+                const double step_start = __ull2double_rn(ts);
+                if (role >= 1u && role - 1u < n_ev) {
+                    const long long eb = event_time_bits(step_start, d, p.delta_t);
+                    if (eb > before_bits) {
+                        mine = eb;
+                        mine_k = role - 1u;
+                    }
+                } else if (role == 0u) {
+                    // events 3.. of a bucket with more than three (rare)
+                    for (uint32_t kk = 3; kk < n_ev; ++kk) {
+                        const long long eb = event_time_bits(step_start, draw_at(s, kk + 2u), p.delta_t);
+                        if (eb > before_bits && eb < mine) {  // kk ascending: ties keep the lower index
+                            mine = eb;
+                            mine_k = kk;
+                        }
+                    }
                 }
             }
             // minimum over the bucket's 4 lanes (ties: lowest event index)
@@ -316,86 +360,45 @@ __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, co
                     mine_k = ok;
                 }
             }
-            // the first of the 8 buckets with an event
-            const unsigned found = __ballot_sync(kFull, mine != 0x7fffffffffffffffLL && e == 0);
+            // the first of the 4 buckets with an event
+            const unsigned found = __ballot_sync(kFull, bucket_lane && role == 0u && mine != kNoEvent);
             if (found) {
                 const int leader = __ffs(found) - 1;
+                const uint32_t bsel = (uint32_t)leader >> 2;
                 best_bits = __shfl_sync(kFull, mine, leader);
                 best_k = __shfl_sync(kFull, mine_k, leader);
-                best_ts = base + (uint64_t)(leader >> 2);
+                best_ts = base + bsel;
+                // the candidate lanes of (bsel, best_k), when speculated
+                // (bsel and best_k are the same on every lane)
+                if (bsel < 2u && best_k < 2u) {
+                    const int src = 16 + 4 * (int)(bsel * 2u + best_k);
+                    rs = __shfl_sync(kFull, s, src);
+                    e1 = __shfl_sync(kFull, d, src);
+                    e2 = __shfl_sync(kFull, d, src + 1);
+                    e3 = __shfl_sync(kFull, d, src + 2);
+                    e4 = __shfl_sync(kFull, d, src + 3);
+                    drawn = true;
+                }
                 break;
             }
-            base += 8;
+            base += 4;
         }
         l.reprime = best_ts + kInvPhi * (uint64_t)(best_k + 1);
-        rs = primed_state(loc_term, l.reprime);
         l.next = max_after(before, __longlong_as_double(best_bits));
         l.has_next = true;
-    } else {
+    }
+    if (!drawn) {
+        // a peek kept from the previous round, or an event outside the
+        // speculated candidates: re-prime, lanes 0..3 draw samples 1..4
         rs = primed_state(loc_term, l.reprime);
+        const uint64_t dk = draw_at(rs, (lane & 3u) + 1u);
+        e1 = __shfl_sync(kFull, dk, 0);
+        e2 = __shfl_sync(kFull, dk, 1);
+        e3 = __shfl_sync(kFull, dk, 2);
+        e4 = __shfl_sync(kFull, dk, 3);
     }
     if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
-
-    l.steps += 1;
-    // samples 1..4 of the event, one per lane, shared
-    const uint64_t dk = draw_at(rs, (lane & 3u) + 1u);
-    const uint64_t e1 = __shfl_sync(kFull, dk, 0);
-    const uint64_t e2 = __shfl_sync(kFull, dk, 1);
-    const uint64_t e3 = __shfl_sync(kFull, dk, 2);
-    const uint64_t e4 = __shfl_sync(kFull, dk, 3);
-    if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
-        if (lane == 0) {
-            const unsigned long long ev_i = atomicAdd(k.n_spec_total, 1ULL);
-            if (ev_i < k.spec_cap) {
-                DevSpeciationEvent ev;
-                ev.gref = l.gref;
-                ev.prior_time = l.last;
-                ev.event_time = l.next;
-                ev.x = l.x;
-                ev.y = l.y;
-                ev.idx = l.i;
-                ev.sim = l.s;
-                k.spec[ev_i] = ev;
-            } else {
-                set_status(k.status, kErrEventOverflow);
-            }
-            SimCounters &c = k.counters[l.s];
-            atomicAdd(&c.steps, (unsigned long long)l.steps);
-            atomicMax(&c.max_time_bits, f64_bits(l.next));
-            atomicAdd(&c.n_speciation, 1ULL);
-        }
-        return kStepSpeciated;
-    }
-    uint32_t tx, ty, ti;
-    if (KIND == kNonSpatial) {
-        non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, tx, ty);
-        ti = coalescence_index(e3, p.deme);
-    } else if (KIND == kSpatiallyImplicit) {
-        const bool local = in_local(p, l.x, l.y);
-        const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
-        const uint64_t d_index = local ? e3 : e2;
-        const uint64_t d_coal = local ? e4 : e3;
-        if (to_meta)
-            non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height, tx, ty);
-        else
-            non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, tx, ty);
-        ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
-    } else if (KIND == kAlmostInfiniteNormal) {
-        normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
-        ti = 0;
-    } else {
-        uint64_t d_coal;
-        if (!spatially_explicit_dispersal_draw(e2, e3, rs, p, l.x, l.y, l.rec, tx, ty, d_coal, k.status) ||
-            !load_cell(p, tx, ty, l.rec, k.status))
-            return kStepDropped;
-        ti = coalescence_index(d_coal, l.rec.habitat);
-    }
-    l.x = tx;
-    l.y = ty;
-    l.i = ti;
-    l.last = l.next;
-    l.has_next = false;
-    return kStepMoved;
+    return lineage_event<KIND, true>(l, p, k, rs, e1, e2, e3, e4, lane == 0);
 }
 
 __device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
@@ -428,6 +431,7 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
     const SimParams *P = SINGLE ? reinterpret_cast<const SimParams *>(params_smem) : a.params;
     const EventSink sink = sink_of(a);
     const uint64_t n = *a.n_cur;
+    const bool lat = n * 4 <= (uint64_t)gridDim.x * blockDim.x;
     const unsigned lane_id = threadIdx.x & 31u;
     const unsigned lanemask_lt = (1u << lane_id) - 1u;
     bool have = false;
@@ -472,7 +476,9 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         if (!__any_sync(kFull, have)) break;
         if (!have) continue;
 
-        const int r = lineage_step<KIND>(l, P[SINGLE ? 0 : l.s], sink);
+        // few lineages for the grid's lanes: latency form (uniform branch)
+        const int r = lat ? lineage_step<KIND, true>(l, P[SINGLE ? 0 : l.s], sink)
+                          : lineage_step<KIND, false>(l, P[SINGLE ? 0 : l.s], sink);
         if (r == kStepMoved) {
             local_steps += 1;
             continue;
@@ -629,8 +635,10 @@ __global__ void __launch_bounds__(kResidentMax) resident_kernel(ResidentArgs a) 
                     }
                 }
             } else if (alive) {
+                // up to 8 lineages per warp: latency form
+                const bool lat = n <= 8 * kWarps;
                 for (;;) {
-                    const int r = lineage_step<KIND>(l, p, sink);
+                    const int r = lat ? lineage_step<KIND, true>(l, p, sink) : lineage_step<KIND, false>(l, p, sink);
                     if (r == kStepMoved) {
                         ++my_events;
                         continue;

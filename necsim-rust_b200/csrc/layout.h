@@ -64,6 +64,11 @@ struct alignas(16) SimParams {
     double poisson_acc_k;
     uint64_t nu_threshold;    // ceil(nu * 2^53): speciation iff X < this
     uint64_t migration_threshold;  // ceil(migration * 2^53)
+    // ceil(2^64 / d) for d = width and d = meta_width (0 when d == 1): a
+    // 32-bit n divides as n / d = mulhi64(magic, n) (Lemire, Kaser & Kurz,
+    // "Faster remainder by direct computation", 2019, Theorem 1 with F = 64)
+    uint64_t width_magic;
+    uint64_t meta_width_magic;
     double inv_delta_t;       // 1 / delta_t if delta_t is a power of two, else 0
     uint64_t seed;            // WyHash seed word
     double nu;                // speciation probability
