@@ -86,6 +86,9 @@ typedef struct necsim_args {
     uint32_t rounds_per_graph; /* rounds captured per CUDA graph launch; 0 = default (16) */
     uint32_t resident_off;     /* 1: keep small simulations in the global rounds instead of
                                   the per-simulation resident kernel (same results) */
+    uint32_t reserved_args;
+    struct necsim_model *model; /* schedule == 1: the lifetime model ordering the step queue
+                                   (must stay alive during the call; same device) */
 } necsim_args;
 
 /* ---- events and lineages (reference layouts) ---- */
@@ -286,6 +289,53 @@ int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cel
  * count; at most `cap` are written (out may be NULL to size). */
 int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *out, uint64_t cap,
                              uint64_t *n_out);
+
+/* ---- learned lifetime scheduler ----
+ * A small MLP (8 -> 64 -> 64 -> 1, ReLU, bf16 weights, fp32 accumulation)
+ * predicting log(1 + remaining events) of a lineage from 8 features
+ * (position in the extent, habitat, dispersal entropy, time, speciation
+ * probability, live lineages of its simulation, events executed).  With
+ * necsim_args.schedule = 1 and .model set, every round's step queue is
+ * bucketed by expected work (min(events per round, predicted remaining)),
+ * largest first.  The model only reorders work: events, species counts and
+ * step counts are the same as with schedule = 0.  There is no reference
+ * interface for this part (it is new in this backend). */
+#define NECSIM_MODEL_FEATURES 8
+#define NECSIM_MODEL_PARAMS 4801 /* W1[64][8], b1[64], W2[64][64], b2[64], W3[64], b3 */
+
+typedef struct necsim_model necsim_model;
+
+/* He-initialised weights from `seed`, on CUDA device `device`. */
+int necsim_model_create(int32_t device, uint64_t seed, necsim_model **out);
+void necsim_model_destroy(necsim_model *model);
+const char *necsim_model_last_error(const necsim_model *model);
+/* The bf16 weights (as fp32) / set the weights (fp32 master copy, rounded
+ * to bf16 for use; resets the optimiser state). */
+int necsim_model_get_weights(necsim_model *model, float *out);
+int necsim_model_set_weights(necsim_model *model, const float *weights);
+/* y[i] = MLP(X[i * 8 .. i * 8 + 8]) for n rows (host buffers). */
+int necsim_model_predict(necsim_model *model, const float *X, uint64_t n, float *y);
+/* Gradient of L = sum_i 0.5 * (MLP(X_i) - T_i)^2 / n with respect to the
+ * NECSIM_MODEL_PARAMS parameters (evaluated at the bf16 weights), and L. */
+int necsim_model_gradients(necsim_model *model, const float *X, const float *T, uint64_t n, float *grads,
+                           double *loss);
+/* Adam on the device: `epochs` passes over the n rows in a fresh random
+ * order each (from `seed`), mini-batches of `batch` rows, learning rate
+ * `lr`; epoch_loss (nullable) receives the mean loss of each epoch. */
+int necsim_model_train(necsim_model *model, const float *X, const float *T, uint64_t n, uint32_t epochs,
+                       uint32_t batch, float lr, uint64_t seed, double *epoch_loss);
+
+/* Training traces: runs the batch (global rounds only) and every
+ * `snapshot_rounds` rounds (even, >= 2) records the features of the live
+ * lineages; a recorded lineage's label is log(1 + events it executed after
+ * the snapshot until it speciated or was removed as a duplicate).  Rows
+ * whose lineage outlives the run are dropped.  At most `max_rows` rows are
+ * returned, evenly subsampled; `features` holds max_rows * 8 floats,
+ * `labels` max_rows; *n_rows receives the count. */
+int necsim_gpu_trace_batch(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,
+                           const necsim_args *args, double pause_before, uint32_t snapshot_rounds,
+                           uint64_t max_rows, float *features, float *labels, uint64_t *n_rows,
+                           char *error, size_t error_cap);
 
 #ifdef __cplusplus
 }

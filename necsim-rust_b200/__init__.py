@@ -64,7 +64,8 @@ class CArgs(ctypes.Structure):
         ("grid_size", ctypes.c_uint32), ("dedup_factor_pct", ctypes.c_uint32),
         ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
-        ("resident_off", ctypes.c_uint32),
+        ("resident_off", ctypes.c_uint32), ("reserved_args", ctypes.c_uint32),
+        ("model", ctypes.c_void_p),
     ]
 
 
@@ -112,6 +113,9 @@ SYMBOLS = [
     "necsim_gpu_simulate_batch", "necsim_gpu_last_error", "necsim_gpu_destroy",
     "necsim_build_tables", "necsim_enumerate_origins", "necsim_gpu_batch_create",
     "necsim_gpu_batch_run", "necsim_gpu_batch_last_error", "necsim_gpu_batch_destroy",
+    "necsim_model_create", "necsim_model_destroy", "necsim_model_last_error",
+    "necsim_model_get_weights", "necsim_model_set_weights", "necsim_model_predict",
+    "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
 ]
 
 _lib = None
@@ -162,6 +166,28 @@ def lib():
     L.necsim_gpu_batch_last_error.restype = ctypes.c_char_p
     L.necsim_gpu_batch_destroy.argtypes = [vp]
     L.necsim_gpu_batch_destroy.restype = None
+    fp = P(ctypes.c_float)
+    L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
+    L.necsim_model_create.restype = ctypes.c_int
+    L.necsim_model_destroy.argtypes = [vp]
+    L.necsim_model_destroy.restype = None
+    L.necsim_model_last_error.argtypes = [vp]
+    L.necsim_model_last_error.restype = ctypes.c_char_p
+    L.necsim_model_get_weights.argtypes = [vp, fp]
+    L.necsim_model_get_weights.restype = ctypes.c_int
+    L.necsim_model_set_weights.argtypes = [vp, fp]
+    L.necsim_model_set_weights.restype = ctypes.c_int
+    L.necsim_model_predict.argtypes = [vp, fp, u64, fp]
+    L.necsim_model_predict.restype = ctypes.c_int
+    L.necsim_model_gradients.argtypes = [vp, fp, fp, u64, fp, P(ctypes.c_double)]
+    L.necsim_model_gradients.restype = ctypes.c_int
+    L.necsim_model_train.argtypes = [vp, fp, fp, u64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float,
+                                     u64, P(ctypes.c_double)]
+    L.necsim_model_train.restype = ctypes.c_int
+    L.necsim_gpu_trace_batch.argtypes = [P(CScenario), P(u64), ctypes.c_uint32, P(CArgs), ctypes.c_double,
+                                         ctypes.c_uint32, u64, fp, fp, P(u64), ctypes.c_char_p,
+                                         ctypes.c_size_t]
+    L.necsim_gpu_trace_batch.restype = ctypes.c_int
     if L.necsim_abi_version() != 1:
         raise ImportError("libnecsim_b200.so ABI version mismatch")
     _lib = L
@@ -231,10 +257,11 @@ class CUDA:
     min_round_events: int = 1 << 20
     step_slice_max: int = 1024
     dedup_factor_pct: int = 200
-    schedule: str = "plain"   # or "learned"
+    schedule: str = "plain"   # or "learned" (needs `model`)
     device: int = 0
     rounds_per_graph: int = 16
     resident: bool = True     # small simulations run in the per-simulation resident kernel
+    model: Optional["LifetimeModel"] = None
 
 
 Independent = CUDA
@@ -315,7 +342,13 @@ def _args_struct(algorithm: CUDA):
     a.block_size = algorithm.block_size
     a.grid_size = algorithm.grid_size
     a.dedup_factor_pct = algorithm.dedup_factor_pct
+    if algorithm.schedule not in ("plain", "learned"):
+        raise ValueError("schedule must be 'plain' or 'learned'")
     a.schedule = 1 if algorithm.schedule == "learned" else 0
+    if a.schedule == 1:
+        if algorithm.model is None:
+            raise ValueError("the learned schedule needs a LifetimeModel")
+        a.model = algorithm.model.handle
     a.report_dispersal = 0
     a.device = algorithm.device
     a.rounds_per_graph = algorithm.rounds_per_graph
@@ -570,3 +603,131 @@ def distinct_speciation_set(events: np.ndarray) -> np.ndarray:
     k = np.stack([events["event_time"].view(np.uint64), events["x"].astype(np.uint64),
                   events["y"].astype(np.uint64), events["index"].astype(np.uint64)], axis=1)
     return np.unique(k, axis=0)
+
+
+# ---------------------------------------------------------------------------
+# Learned lifetime scheduler
+# ---------------------------------------------------------------------------
+MODEL_FEATURES = 8
+MODEL_PARAMS = 4801
+# offsets of the flat parameter array: W1[64][8], b1[64], W2[64][64], b2[64], W3[64], b3
+MODEL_LAYOUT = {"W1": (0, (64, 8)), "b1": (512, (64,)), "W2": (576, (64, 64)),
+                "b2": (4672, (64,)), "W3": (4736, (64,)), "b3": (4800, (1,))}
+
+
+def _f32(a, shape_tail=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+class LifetimeModel:
+    """The MLP (8 -> 64 -> 64 -> 1, bf16 weights, fp32 accumulation) that
+    predicts log(1 + remaining events) of a lineage; trained and evaluated
+    by the backend's own CUDA kernels on `device`."""
+
+    def __init__(self, seed: int = 0, device: int = 0):
+        L = lib()
+        h = ctypes.c_void_p()
+        rc = L.necsim_model_create(device, seed, ctypes.byref(h))
+        self._h = h
+        if rc != 0:
+            msg = L.necsim_model_last_error(h).decode() if h.value else ""
+            self.close()
+            raise NecsimError(rc, msg)
+
+    @property
+    def handle(self):
+        return self._h.value
+
+    def _check(self, rc):
+        if rc != 0:
+            raise NecsimError(rc, lib().necsim_model_last_error(self._h).decode())
+
+    @property
+    def weights(self) -> np.ndarray:
+        out = np.zeros(MODEL_PARAMS, dtype=np.float32)
+        self._check(lib().necsim_model_get_weights(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return out
+
+    @weights.setter
+    def weights(self, w):
+        w, wp = _f32(w)
+        if w.size != MODEL_PARAMS:
+            raise ValueError("expected %d parameters" % MODEL_PARAMS)
+        self._check(lib().necsim_model_set_weights(self._h, wp))
+
+    def predict(self, X) -> np.ndarray:
+        X, xp = _f32(X)
+        n = X.shape[0] if X.ndim == 2 else X.size // MODEL_FEATURES
+        y = np.zeros(n, dtype=np.float32)
+        self._check(lib().necsim_model_predict(self._h, xp, n, y.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
+        return y
+
+    def gradients(self, X, T):
+        """(gradient of sum 0.5 (MLP(x) - t)^2 / n, loss)."""
+        X, xp = _f32(X)
+        T, tp = _f32(T)
+        g = np.zeros(MODEL_PARAMS, dtype=np.float32)
+        loss = ctypes.c_double()
+        self._check(lib().necsim_model_gradients(self._h, xp, tp, T.size,
+                                                 g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                                 ctypes.byref(loss)))
+        return g, loss.value
+
+    def train(self, X, T, epochs: int = 20, batch: int = 1024, lr: float = 2e-3, seed: int = 0) -> np.ndarray:
+        """Adam on the device; returns the mean loss of each epoch."""
+        X, xp = _f32(X)
+        T, tp = _f32(T)
+        losses = np.zeros(epochs, dtype=np.float64)
+        self._check(lib().necsim_model_train(self._h, xp, tp, T.size, epochs, batch, lr, seed,
+                                             losses.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return losses
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().necsim_model_destroy(self._h)
+        self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def collect_traces(scenarios: Sequence, speciations: Sequence[float], seeds: Sequence[int],
+                   algorithm: Optional[CUDA] = None, pause_before: Optional[float] = None,
+                   snapshot_rounds: int = 32, max_rows: int = 1 << 18):
+    """Training traces generated by the backend itself: (features [n, 8],
+    labels [n] = log(1 + remaining events)) of lineages snapshotted every
+    `snapshot_rounds` rounds of a batch run."""
+    L = lib()
+    n = len(scenarios)
+    structs = (CScenario * n)()
+    keep = []
+    for j, (sc, nu) in enumerate(zip(scenarios, speciations)):
+        c = _scenario_struct(sc, nu)
+        keep.append(c)
+        structs[j] = c
+    seeds_arr = (ctypes.c_uint64 * n)(*[seed_from_u64(s) for s in seeds])
+    alg = algorithm or CUDA()
+    if alg.schedule != "plain":
+        alg = CUDA(**{**alg.__dict__, "schedule": "plain", "model": None})
+    args = _args_struct(alg)
+    X = np.zeros((max_rows, MODEL_FEATURES), dtype=np.float32)
+    y = np.zeros(max_rows, dtype=np.float32)
+    got = ctypes.c_uint64()
+    err = ctypes.create_string_buffer(512)
+    pb = -1.0 if pause_before is None else float(pause_before)
+    rc = L.necsim_gpu_trace_batch(structs, seeds_arr, n, ctypes.byref(args), pb, snapshot_rounds, max_rows,
+                                  X.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                                  y.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), ctypes.byref(got), err, 512)
+    if rc != 0:
+        raise NecsimError(rc, err.value.decode())
+    return X[:got.value].copy(), y[:got.value].copy()

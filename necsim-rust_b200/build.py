@@ -14,7 +14,7 @@ LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libnecsim_b200.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["kernels.cu", "noalloc.cu"]
+CU_SOURCES = ["kernels.cu", "noalloc.cu", "learned.cu"]
 CPP_SOURCES = ["host.cpp", "tables.cpp"]
 
 

@@ -10,6 +10,8 @@
 #include <cstring>
 #include <memory>
 #include <new>
+#include <random>
+#include <unordered_map>
 #include <string>
 #include <thread>
 #include <vector>
@@ -20,6 +22,25 @@
 #include "tables.h"
 
 using namespace necsim;
+
+// The learned lifetime model: bf16 weights used by the kernels, the fp32
+// master copy and Adam moments, on one device.
+struct necsim_model {
+    int device = 0;
+    __nv_bfloat16 *w = nullptr;
+    float *master = nullptr, *m = nullptr, *v = nullptr, *grads = nullptr;
+    double *loss = nullptr;
+    int adam_step = 0;
+    cudaStream_t stream = nullptr;
+    std::string error;
+    ~necsim_model() {
+        if (device >= 0) cudaSetDevice(device);
+        void *ptrs[] = {w, master, m, v, grads, loss};
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+        if (stream) cudaStreamDestroy(stream);
+    }
+};
 
 namespace {
 
@@ -214,7 +235,8 @@ necsim_args with_defaults(const necsim_args *in) {
 struct DeviceLineages {
     LineageSoA soa{};
     uint8_t *state = nullptr;
-    void alloc(uint64_t n) {
+    void alloc(uint64_t n, bool with_pred = false) {
+        if (with_pred) soa.pred_end = dev_alloc<float>(n);
         soa.x = dev_alloc<uint32_t>(n);
         soa.y = dev_alloc<uint32_t>(n);
         soa.idx = dev_alloc<uint32_t>(n);
@@ -229,7 +251,7 @@ struct DeviceLineages {
     }
     void release() {
         void *ptrs[] = {soa.x, soa.y, soa.idx, soa.sim, soa.last, soa.next, soa.reprime,
-                        soa.gref, soa.steps, soa.has_next, state};
+                        soa.gref, soa.steps, soa.has_next, state, soa.pred_end};
         for (void *p : ptrs)
             if (p) cudaFree(p);
         soa = LineageSoA{};
@@ -282,6 +304,22 @@ struct Engine {
     unsigned step_grid = 0, step_block = 0;
     unsigned aux_grid = 0, aux_block = 256;
 
+    // learned schedule (schedule == 1): model weights (owned by the model)
+    // and the round's queue order
+    bool learned = false;
+    const __nv_bfloat16 *model_w = nullptr;
+    uint8_t *order_keys = nullptr;
+    unsigned *order_hist = nullptr;
+    uint32_t *order = nullptr;
+    std::vector<float *> d_entropy;  // SE: per-cell dispersal entropy, one per table set
+
+    // training traces (necsim_gpu_trace_batch)
+    bool tracing = false;
+    TraceRow *trace_rows = nullptr;
+    TraceDeath *trace_deaths = nullptr;
+    unsigned long long *trace_counts = nullptr;  // [0] rows, [1] deaths
+    uint64_t trace_rows_cap = 0, trace_deaths_cap = 0;
+
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<cudaEvent_t> ev_start, ev_end;
     cudaEvent_t ev_total0 = nullptr, ev_total1 = nullptr;
@@ -323,8 +361,20 @@ struct Engine {
             if (p) cudaFree(p);
         for (auto p : d_atoms)
             if (p) cudaFree(p);
+        for (auto p : d_entropy)
+            if (p) cudaFree(p);
         d_cells.clear();
         d_atoms.clear();
+        d_entropy.clear();
+        void *lptrs[] = {order_keys, order_hist, order, trace_rows, trace_deaths, trace_counts};
+        for (void *p : lptrs)
+            if (p) cudaFree(p);
+        order_keys = nullptr;
+        order_hist = nullptr;
+        order = nullptr;
+        trace_rows = nullptr;
+        trace_deaths = nullptr;
+        trace_counts = nullptr;
         if (h_ctl) cudaFreeHost(h_ctl);
         h_ctl = nullptr;
         if (stream) cudaStreamDestroy(stream);
@@ -348,6 +398,10 @@ void upload_tables(Engine &E, SimHost &s) {
     AliasAtom *da = dev_alloc<AliasAtom>(t.atoms.size());
     E.d_cells.push_back(dc);
     E.d_atoms.push_back(da);
+    float *de = dev_alloc<float>(t.entropy.size());
+    E.d_entropy.push_back(de);
+    CK(cudaMemcpyAsync(de, t.entropy.data(), t.entropy.size() * sizeof(float), cudaMemcpyHostToDevice, E.stream));
+    E.h2d_bytes += t.entropy.size() * sizeof(float);
     E.h2d_bytes += t.cells.size() * sizeof(CellRecord) + t.atoms.size() * sizeof(AliasAtom);
     CK(cudaMemcpyAsync(dc, t.cells.data(), t.cells.size() * sizeof(CellRecord), cudaMemcpyHostToDevice, E.stream));
     if (!t.atoms.empty())
@@ -355,6 +409,7 @@ void upload_tables(Engine &E, SimHost &s) {
     CK(cudaStreamSynchronize(E.stream));
     s.params.cells = dc;
     s.params.atoms = da;
+    s.params.cell_entropy = de;
     s.params.n_cells = t.cells.size();
     s.params.n_atoms = t.atoms.size();
 }
@@ -391,11 +446,24 @@ void choose_launch(Engine &E) {
 
 void alloc_run_buffers(Engine &E) {
     const uint64_t n = E.n_total;
-    E.A.alloc(n);
+    E.A.alloc(n, E.learned);
     E.R.alloc(n);
     CK(cudaEventCreate(&E.ev_res0));
     CK(cudaEventCreate(&E.ev_res1));
-    E.B.alloc(n);
+    E.B.alloc(n, E.learned);
+    if (E.learned) {
+        E.order_keys = dev_alloc<uint8_t>(n);
+        E.order = dev_alloc<uint32_t>(n);
+        E.order_hist = dev_alloc<unsigned>(2 * kOrderBuckets);
+        CK(cudaMemsetAsync(E.order_hist, 0, 2 * kOrderBuckets * sizeof(unsigned), E.stream));
+    }
+    if (E.tracing) {
+        E.trace_deaths_cap = n;
+        E.trace_deaths = dev_alloc<TraceDeath>(n);
+        E.trace_rows = dev_alloc<TraceRow>(E.trace_rows_cap);
+        E.trace_counts = dev_alloc<unsigned long long>(2);
+        CK(cudaMemsetAsync(E.trace_counts, 0, 2 * sizeof(unsigned long long), E.stream));
+    }
     unsigned long long want = (n * E.args.dedup_factor_pct + 99) / 100;
     if (want < 2) want = 2;
     unsigned long long size = 1;
@@ -516,6 +584,7 @@ void reset_lineages(Engine &E) {
     CK(cudaMemsetAsync(d.next, 0, n * 8, E.stream));
     CK(cudaMemsetAsync(d.reprime, 0, n * 8, E.stream));
     CK(cudaMemsetAsync(E.A.state, 0, n, E.stream));
+    if (d.pred_end) CK(cudaMemsetAsync(d.pred_end, 0, n * sizeof(float), E.stream));
 }
 
 StepArgs make_step_args(Engine &E, DeviceLineages &in) {
@@ -538,7 +607,23 @@ StepArgs make_step_args(Engine &E, DeviceLineages &in) {
     a.status = &E.d_ctl->status;
     a.steps_total = &E.d_ctl->steps_total;
     a.n_sims = (uint32_t)E.sims.size();
+    a.order = E.learned ? E.order : nullptr;
+    if (E.tracing) {
+        a.trace.deaths = E.trace_deaths;
+        a.trace.n_deaths = E.trace_counts + 1;
+        a.trace.cap = E.trace_deaths_cap;
+    }
     return a;
+}
+
+FeatureArgs make_feature_args(Engine &E, DeviceLineages &in) {
+    FeatureArgs f;
+    f.in = in.soa;
+    f.n_cur = &E.d_ctl->n_cur;
+    f.params = E.d_params;
+    f.counters = E.d_counters;
+    f.kind = E.kind;
+    return f;
 }
 
 DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
@@ -558,6 +643,11 @@ DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
     a.status = &E.d_ctl->status;
     if (E.args.resident_off == 0) a.arena = E.R.soa;  // route small simulations to the arena
     a.params = E.d_params;
+    if (E.tracing) {
+        a.trace.deaths = E.trace_deaths;
+        a.trace.n_deaths = E.trace_counts + 1;
+        a.trace.cap = E.trace_deaths_cap;
+    }
     return a;
 }
 
@@ -604,6 +694,13 @@ void enqueue_rounds(Engine &E, unsigned rounds, bool events, bool external) {
     for (unsigned r = 0; r < rounds; ++r) {
         DeviceLineages &in = (r % 2 == 0) ? E.A : E.B;
         DeviceLineages &out = (r % 2 == 0) ? E.B : E.A;
+        if (E.learned) {
+            // predictions for lineages without one, then this round's queue
+            // order by expected work (largest first)
+            const FeatureArgs f = make_feature_args(E, in);
+            CK(launch_lineage_predict(f, E.model_w, in.soa.pred_end, E.stream));
+            CK(launch_order(f, in.soa.pred_end, E.order_keys, E.order_hist, E.order, E.aux_grid, E.stream));
+        }
         if (events) {
             if (external)
                 CK(cudaEventRecordWithFlags(E.ev_start[r], E.stream, cudaEventRecordExternal));
@@ -679,6 +776,8 @@ RunResult run_rounds(Engine &E) {
     CK(cudaMemcpyAsync(E.d_counters, cs.data(), cs.size() * sizeof(SimCounters), cudaMemcpyHostToDevice, E.stream));
     CK(launch_schedule(make_schedule_args(E), E.stream));
     rr.launches += 1;
+    if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_rows, E.trace_counts,
+                                            E.trace_rows_cap, E.stream));
     CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
     uint64_t graph_launches = 0;
@@ -724,7 +823,10 @@ RunResult run_rounds(Engine &E) {
                 enqueue_rounds(E, rounds, true, false);
             }
             CK(cudaMemsetAsync(&E.d_ctl->graph_done, 1, sizeof(int), E.stream));
-            rr.launches += (uint64_t)rounds * 5;
+            rr.launches += (uint64_t)rounds * (E.learned ? 9 : 5);
+            // after an even number of rounds the live lineages are in A
+            if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_rows, E.trace_counts,
+                                                    E.trace_rows_cap, E.stream));
             rr.rounds_launched += rounds;
         }
         CK(cudaStreamWaitEvent(E.stream, E.ev_res1, 0));
@@ -1002,6 +1104,13 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
     E.kind = sims.front().sc.kind;
     for (auto &s : sims)
         if (s.sc.kind != E.kind) fail(NECSIM_E_UNSUPPORTED, "a batch must share one scenario kind");
+    if (args.schedule > 1) fail(NECSIM_E_INVALID_ARGUMENT, "schedule must be 0 (plain) or 1 (learned)");
+    E.learned = args.schedule == 1;
+    if (E.learned) {
+        if (!args.model) fail(NECSIM_E_INVALID_ARGUMENT, "the learned schedule needs a model");
+        if (args.model->device != E.device) fail(NECSIM_E_INVALID_ARGUMENT, "the model lives on another device");
+        E.model_w = args.model->w;
+    }
     if (args.report_dispersal) fail(NECSIM_E_UNSUPPORTED, "dispersal reporting is not enabled in this build");
     uint64_t off = 0;
     for (auto &s : sims) {
@@ -1020,6 +1129,7 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
                 sh.params.atoms = (*prebuilt_tables)[s].atoms;
                 sh.params.n_cells = (*prebuilt_tables)[s].n_cells;
                 sh.params.n_atoms = (*prebuilt_tables)[s].n_atoms;
+                sh.params.cell_entropy = (*prebuilt_tables)[s].cell_entropy;
             } else {
                 upload_tables(E, sh);
             }
@@ -1298,6 +1408,237 @@ int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *ou
 const char *necsim_gpu_last_error(const necsim_ctx *ctx) { return ctx ? ctx->error.c_str() : "null context"; }
 
 void necsim_gpu_destroy(necsim_ctx *ctx) { delete ctx; }
+
+}  // extern "C"
+
+// ---- learned lifetime model ----
+
+namespace {
+
+template <typename F>
+int model_guarded(necsim_model *m, F &&f) {
+    if (!m) return NECSIM_E_INVALID_ARGUMENT;
+    char msg[512] = {0};
+    const int rc = guarded(nullptr, msg, sizeof(msg), [&] {
+        CK(cudaSetDevice(m->device));
+        f();
+    });
+    m->error = msg;
+    return rc;
+}
+
+// device copy of a host array, freed by the caller
+template <typename T>
+T *upload(const T *src, size_t n, cudaStream_t st) {
+    T *d = dev_alloc<T>(n ? n : 1);
+    if (n) CK(cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, st));
+    return d;
+}
+
+struct DevFree {
+    std::vector<void *> ptrs;
+    ~DevFree() {
+        for (void *p : ptrs)
+            if (p) cudaFree(p);
+    }
+};
+
+void model_write_master(necsim_model *m, const std::vector<float> &w) {
+    std::vector<__nv_bfloat16> wb(kMlpParams);
+    for (int i = 0; i < kMlpParams; ++i) wb[i] = __float2bfloat16_rn(w[i]);
+    CK(cudaMemcpyAsync(m->master, w.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    CK(cudaMemcpyAsync(m->w, wb.data(), kMlpParams * sizeof(__nv_bfloat16), cudaMemcpyHostToDevice, m->stream));
+    CK(cudaMemsetAsync(m->m, 0, kMlpParams * sizeof(float), m->stream));
+    CK(cudaMemsetAsync(m->v, 0, kMlpParams * sizeof(float), m->stream));
+    CK(cudaMemsetAsync(m->grads, 0, kMlpParams * sizeof(float), m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    m->adam_step = 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int necsim_model_create(int32_t device, uint64_t seed, necsim_model **out) {
+    if (!out) return NECSIM_E_INVALID_ARGUMENT;
+    *out = nullptr;
+    necsim_model *m = new (std::nothrow) necsim_model();
+    if (!m) return NECSIM_E_OUT_OF_MEMORY;
+    m->device = device;
+    const int rc = model_guarded(m, [&] {
+        CK(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+        m->w = dev_alloc<__nv_bfloat16>(kMlpParams);
+        m->master = dev_alloc<float>(kMlpParams);
+        m->m = dev_alloc<float>(kMlpParams);
+        m->v = dev_alloc<float>(kMlpParams);
+        m->grads = dev_alloc<float>(kMlpParams);
+        m->loss = dev_alloc<double>(1);
+        // He initialisation for the ReLU layers, a linear output layer
+        // starting near log(1 + 100) events
+        std::mt19937_64 rng(seed);
+        std::normal_distribution<float> g1(0.f, std::sqrt(2.f / kFeat)), g2(0.f, std::sqrt(2.f / kHidden)),
+            g3(0.f, std::sqrt(1.f / kHidden));
+        std::vector<float> w(kMlpParams, 0.f);
+        for (int i = kW1; i < kB1; ++i) w[i] = g1(rng);
+        for (int i = kW2; i < kB2; ++i) w[i] = g2(rng);
+        for (int i = kW3; i < kB3; ++i) w[i] = g3(rng);
+        w[kB3] = 4.6f;
+        model_write_master(m, w);
+    });
+    *out = m;
+    return rc;
+}
+
+void necsim_model_destroy(necsim_model *model) { delete model; }
+
+const char *necsim_model_last_error(const necsim_model *model) {
+    return model ? model->error.c_str() : "null model";
+}
+
+int necsim_model_get_weights(necsim_model *model, float *out) {
+    if (!out) return NECSIM_E_INVALID_ARGUMENT;
+    return model_guarded(model, [&] {
+        std::vector<__nv_bfloat16> wb(kMlpParams);
+        CK(cudaMemcpyAsync(wb.data(), model->w, kMlpParams * sizeof(__nv_bfloat16), cudaMemcpyDeviceToHost,
+                           model->stream));
+        CK(cudaStreamSynchronize(model->stream));
+        for (int i = 0; i < kMlpParams; ++i) out[i] = __bfloat162float(wb[i]);
+    });
+}
+
+int necsim_model_set_weights(necsim_model *model, const float *weights) {
+    if (!weights) return NECSIM_E_INVALID_ARGUMENT;
+    return model_guarded(model, [&] {
+        model_write_master(model, std::vector<float>(weights, weights + kMlpParams));
+    });
+}
+
+int necsim_model_predict(necsim_model *model, const float *X, uint64_t n, float *y) {
+    if ((!X || !y) && n) return NECSIM_E_INVALID_ARGUMENT;
+    return model_guarded(model, [&] {
+        if (n == 0) return;
+        DevFree f;
+        float *dX = upload(X, n * kFeat, model->stream);
+        f.ptrs.push_back(dX);
+        float *dy = dev_alloc<float>(n);
+        f.ptrs.push_back(dy);
+        CK(launch_mlp_predict(model->w, dX, n, dy, model->stream));
+        CK(cudaMemcpyAsync(y, dy, n * sizeof(float), cudaMemcpyDeviceToHost, model->stream));
+        CK(cudaStreamSynchronize(model->stream));
+    });
+}
+
+int necsim_model_gradients(necsim_model *model, const float *X, const float *T, uint64_t n, float *grads,
+                           double *loss) {
+    if (!X || !T || !grads || n == 0) return NECSIM_E_INVALID_ARGUMENT;
+    return model_guarded(model, [&] {
+        DevFree f;
+        float *dX = upload(X, n * kFeat, model->stream);
+        f.ptrs.push_back(dX);
+        float *dT = upload(T, n, model->stream);
+        f.ptrs.push_back(dT);
+        CK(cudaMemsetAsync(model->grads, 0, kMlpParams * sizeof(float), model->stream));
+        CK(cudaMemsetAsync(model->loss, 0, sizeof(double), model->stream));
+        CK(launch_mlp_grad(model->w, dX, dT, nullptr, 0, n, 1.0f / (float)n, model->grads, model->loss,
+                           model->stream));
+        CK(cudaMemcpyAsync(grads, model->grads, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, model->stream));
+        double l = 0.0;
+        CK(cudaMemcpyAsync(&l, model->loss, sizeof(double), cudaMemcpyDeviceToHost, model->stream));
+        CK(cudaMemsetAsync(model->grads, 0, kMlpParams * sizeof(float), model->stream));
+        CK(cudaStreamSynchronize(model->stream));
+        if (loss) *loss = l;
+    });
+}
+
+int necsim_model_train(necsim_model *model, const float *X, const float *T, uint64_t n, uint32_t epochs,
+                       uint32_t batch, float lr, uint64_t seed, double *epoch_loss) {
+    if (!X || !T || n == 0 || batch == 0 || !(lr > 0.f)) return NECSIM_E_INVALID_ARGUMENT;
+    if (n >= 0xffffffffULL) return NECSIM_E_TOO_LARGE;
+    return model_guarded(model, [&] {
+        DevFree f;
+        float *dX = upload(X, n * kFeat, model->stream);
+        f.ptrs.push_back(dX);
+        float *dT = upload(T, n, model->stream);
+        f.ptrs.push_back(dT);
+        uint32_t *dperm = dev_alloc<uint32_t>(n);
+        f.ptrs.push_back(dperm);
+        std::vector<uint32_t> perm(n);
+        std::mt19937_64 rng(seed);
+        const uint64_t n_batches = (n + batch - 1) / batch;
+        for (uint32_t e = 0; e < epochs; ++e) {
+            for (uint64_t i = 0; i < n; ++i) perm[i] = (uint32_t)i;
+            std::shuffle(perm.begin(), perm.end(), rng);
+            CK(cudaMemcpyAsync(dperm, perm.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, model->stream));
+            CK(cudaMemsetAsync(model->loss, 0, sizeof(double), model->stream));
+            for (uint64_t b = 0; b < n_batches; ++b) {
+                const uint64_t off = b * batch;
+                const uint64_t bn = std::min<uint64_t>(batch, n - off);
+                CK(launch_mlp_grad(model->w, dX, dT, dperm, off, bn, 1.0f / (float)bn, model->grads, model->loss,
+                                   model->stream));
+                model->adam_step += 1;
+                CK(launch_adam(model->master, model->m, model->v, model->grads, model->w, lr, 0.9f, 0.999f, 1e-8f,
+                               model->adam_step, model->stream));
+            }
+            double l = 0.0;
+            CK(cudaMemcpyAsync(&l, model->loss, sizeof(double), cudaMemcpyDeviceToHost, model->stream));
+            CK(cudaStreamSynchronize(model->stream));
+            if (epoch_loss) epoch_loss[e] = l / (double)n_batches;
+        }
+    });
+}
+
+int necsim_gpu_trace_batch(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,
+                           const necsim_args *args_in, double pause_before, uint32_t snapshot_rounds,
+                           uint64_t max_rows, float *features, float *labels, uint64_t *n_rows, char *error,
+                           size_t error_cap) {
+    if (!scenarios || !wyhash_seeds || n_sims == 0 || !n_rows || (max_rows && (!features || !labels)))
+        return NECSIM_E_INVALID_ARGUMENT;
+    if (snapshot_rounds < 2 || snapshot_rounds % 2) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, error, error_cap, [&] {
+        necsim_args args = with_defaults(args_in);
+        args.resident_off = 1;  // every lineage stays in the global rounds, where it is snapshotted
+        args.schedule = 0;
+        args.model = nullptr;
+        args.rounds_per_graph = snapshot_rounds;
+        Engine E;
+        setup_engine(E, args);
+        E.tracing = true;
+        E.trace_rows_cap = std::max<uint64_t>(1024, std::min<uint64_t>(max_rows * 4, 1ULL << 25));
+        prepare_engine(E, batch_sims(scenarios, wyhash_seeds, n_sims, args, pause_before), args, nullptr, nullptr);
+        if (E.n_total > 0) run_rounds(E);
+        unsigned long long counts[2] = {0, 0};
+        CK(cudaMemcpy(counts, E.trace_counts, sizeof(counts), cudaMemcpyDeviceToHost));
+        const uint64_t nr = std::min<uint64_t>(counts[0], E.trace_rows_cap);
+        const uint64_t nd = std::min<uint64_t>(counts[1], E.trace_deaths_cap);
+        std::vector<TraceRow> rows(nr);
+        std::vector<TraceDeath> deaths(nd);
+        if (nr) CK(cudaMemcpy(rows.data(), E.trace_rows, nr * sizeof(TraceRow), cudaMemcpyDeviceToHost));
+        if (nd) CK(cudaMemcpy(deaths.data(), E.trace_deaths, nd * sizeof(TraceDeath), cudaMemcpyDeviceToHost));
+        // (simulation, global reference) -> step count at death
+        struct KeyHash {
+            size_t operator()(const std::pair<uint32_t, uint64_t> &k) const {
+                return std::hash<uint64_t>()(k.second * 0x9e3779b97f4a7c15ULL ^ (uint64_t)k.first);
+            }
+        };
+        std::unordered_map<std::pair<uint32_t, uint64_t>, uint64_t, KeyHash> death_steps;
+        death_steps.reserve(nd * 2 + 1);
+        for (const TraceDeath &d : deaths) death_steps[{d.sim, d.gref}] = d.steps;
+        std::vector<uint64_t> labelled;
+        labelled.reserve(nr);
+        for (uint64_t i = 0; i < nr; ++i) {
+            auto it = death_steps.find({rows[i].sim, rows[i].gref});
+            if (it != death_steps.end() && it->second >= rows[i].steps) labelled.push_back(i);
+        }
+        const uint64_t take = std::min<uint64_t>(max_rows, labelled.size());
+        for (uint64_t k = 0; k < take; ++k) {
+            // evenly spaced over the labelled rows (all snapshots, all sims)
+            const TraceRow &r = rows[labelled[(uint64_t)((double)k * (double)labelled.size() / (double)take)]];
+            for (int j = 0; j < kFeat; ++j) features[k * kFeat + j] = r.f[j];
+            labels[k] = (float)std::log1p((double)(death_steps[{r.sim, r.gref}] - r.steps));
+        }
+        *n_rows = take;
+    });
+}
 
 }  // extern "C"
 

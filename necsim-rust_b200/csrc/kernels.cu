@@ -138,7 +138,21 @@ struct EventSink {
     int report_dispersal;
     uint32_t *status;
     SimCounters *counters;
+    TraceSink trace;
 };
+
+__device__ __forceinline__ void record_death(const TraceSink &t, uint64_t gref, uint64_t steps, uint32_t sim) {
+    if (!t.deaths) return;
+    const unsigned long long i = atomicAdd(t.n_deaths, 1ULL);
+    if (i < t.cap) {
+        TraceDeath d;
+        d.gref = gref;
+        d.steps = steps;
+        d.sim = sim;
+        d.pad = 0;
+        t.deaths[i] = d;
+    }
+}
 
 // The event at l.next (event_sampler/independent.rs:112-222) from the
 // re-primed state rs: speciation, or dispersal + coalescence index.  With
@@ -171,6 +185,7 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
             atomicAdd(&c.steps, (unsigned long long)l.steps);
             atomicMax(&c.max_time_bits, f64_bits(l.next));
             atomicAdd(&c.n_speciation, 1ULL);
+            record_death(k.trace, l.gref, l.steps, l.s);
         }
         return kStepSpeciated;
     }
@@ -412,6 +427,7 @@ __device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
     k.report_dispersal = a.report_dispersal;
     k.status = a.status;
     k.counters = a.counters;
+    k.trace = a.trace;
     return k;
 }
 
@@ -562,6 +578,9 @@ __global__ void __launch_bounds__(kResidentMax) resident_kernel(ResidentArgs a) 
     sink.report_dispersal = 0;
     sink.status = a.status;
     sink.counters = a.counters;
+    sink.trace.deaths = nullptr;
+    sink.trace.n_deaths = nullptr;
+    sink.trace.cap = 0;
 
     for (uint32_t s = blockIdx.x; s < a.n_sims; s += gridDim.x) {
         SimParams &pm = a.params[s];
@@ -843,6 +862,7 @@ __global__ void dedup_compact_kernel(DedupArgs a) {
             a.out.gref[d] = a.in.gref[j];
             a.out.steps[d] = a.in.steps[j];
             a.out.has_next[d] = a.in.has_next[j];
+            if (a.out.pred_end) a.out.pred_end[d] = a.in.pred_end[j];
             a.state_out[d] = 0;
         }
         // per-simulation live counts, aggregated over lanes of the same
@@ -870,6 +890,7 @@ __global__ void dedup_compact_kernel(DedupArgs a) {
             atomicAdd(&c.steps, (unsigned long long)a.in.steps[j]);
             atomicMax(&c.max_time_bits, f64_bits(a.in.last[j]));
             atomicAdd(&c.n_dedup, 1ULL);
+            record_death(a.trace, a.in.gref[j], a.in.steps[j], s);
         }
     }
 }

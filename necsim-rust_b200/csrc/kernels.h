@@ -6,6 +6,7 @@
 #include <cstdint>
 
 #include "layout.h"
+#include "learned.h"
 
 namespace necsim {
 
@@ -31,6 +32,7 @@ struct StepArgs {
     uint32_t *status;
     unsigned long long *steps_total;     // optional per-launch event count
     uint32_t n_sims;                     // simulations in `params`
+    TraceSink trace;                     // death records of speciated lineages (tracing only)
 };
 
 struct DedupArgs {
@@ -48,6 +50,7 @@ struct DedupArgs {
     unsigned long long *out_count;
     SimCounters *counters;
     uint32_t *status;
+    TraceSink trace;                     // death records of removed duplicates (tracing only)
 };
 
 struct ScheduleArgs {

@@ -85,6 +85,8 @@ struct alignas(16) SimParams {
     uint32_t meta_ox, meta_oy, meta_width, meta_height, meta_deme;
     const CellRecord *cells;  // SE
     const AliasAtom *atoms;   // SE
+    const float *cell_entropy;  // SE: per-cell dispersal entropy (learned-model feature), nullable
+    uint64_t pad2;
     uint64_t n_cells;
     uint64_t n_atoms;
     uint64_t step_slice;
@@ -122,6 +124,9 @@ struct LineageSoA {
     uint64_t *gref;      // global lineage reference
     uint64_t *steps;     // events executed by this lineage
     uint8_t *has_next;
+    // learned schedule: predicted step count at which the lineage leaves the
+    // simulation (0: not predicted yet); nullptr when no model is used
+    float *pred_end = nullptr;
 };
 
 // Speciation event record written by the kernel (SpeciationEvent plus the

@@ -7,6 +7,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <thread>
 
 namespace necsim {
@@ -141,12 +142,19 @@ int build_spatially_explicit_tables(const necsim_scenario &sc, HostTables &out, 
     std::vector<uint64_t> count(n, 0);
     std::vector<double> sd_prob(n, 0.0);
     std::vector<uint8_t> sd_separate(n, 0);
+    out.entropy.assign(n, 0.0f);
     parallel_rows(n, threads, [&](uint64_t r, RowScratch &s) {
         double self_w;
         row_weights(sc, r, s, self_w);
         if (s.ev.empty()) return;
         double total = 0.0;
         for (double w : s.w) total = total + w;
+        double h = 0.0;
+        for (double w : s.w) {
+            const double q = w / total;
+            h -= q * std::log(q);
+        }
+        out.entropy[r] = (float)h;
         sd_prob[r] = self_w / total;
         const double sd_u = self_w * (double)s.ev.size() / total;
         if (sd_u < 1.0) {

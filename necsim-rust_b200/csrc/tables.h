@@ -12,6 +12,10 @@ namespace necsim {
 struct HostTables {
     std::vector<CellRecord> cells;  // one per habitat-map cell
     std::vector<AliasAtom> atoms;   // packed per cell, in the reference's atom order
+    // Shannon entropy (nats) of each cell's dispersal distribution
+    // p(c) = w(c) / sum(w), w(c) = dispersal(r, c) * habitat(c): a feature of
+    // the learned lifetime model (0 for non-habitat cells)
+    std::vector<float> entropy;
 };
 
 // Builds the packed separable alias tables of a SpatiallyExplicit scenario

@@ -1,0 +1,137 @@
+"""The learned lifetime scheduler: the MLP's gradients and predictions
+against the fp64 oracle (oracle/mlp_oracle.py), training on traces the
+backend generates itself, and outcomes that do not change when the trained
+model reorders the step queue."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_oracle_gradients_match_finite_differences():
+    rng = np.random.default_rng(0)
+    w = rng.normal(0.0, 0.3, mo.N_PARAMS)
+    X = rng.random((40, mo.N_FEATURES))
+    T = rng.random(40) * 5.0
+    _, g = mo.loss_and_gradients(w, X, T)
+    for i in [0, 7, 515, 600, 2000, 4671, 4700, 4740, 4800]:
+        e = np.zeros_like(w)
+        e[i] = 1e-6
+        fd = (mo.loss_and_gradients(w + e, X, T)[0] - mo.loss_and_gradients(w - e, X, T)[0]) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(g[i]))
+
+
+def test_bf16_rounding_is_nearest_even():
+    x = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -9, -2.5, 3.14159], dtype=np.float32)
+    assert mo.to_bf16(x).tolist() == [1.0, 1.0, 1.0078125, -2.5, 3.140625]
+
+
+def test_model_layout_matches_header(nb):
+    assert nb.MODEL_PARAMS == mo.N_PARAMS
+    assert nb.MODEL_LAYOUT == mo.LAYOUT
+    header = open(os.path.join(ROOT, "include", "necsim_b200.h")).read()
+    assert "#define NECSIM_MODEL_PARAMS 4801" in header
+    assert "#define NECSIM_MODEL_FEATURES 8" in header
+
+
+@pytest.mark.gpu
+def test_gradients_and_predictions_match_oracle(nb):
+    rng = np.random.default_rng(1)
+    with nb.LifetimeModel(seed=3) as m:
+        # bf16-representable weights: the device computes with exactly these
+        w = mo.to_bf16(rng.normal(0.0, 0.25, mo.N_PARAMS).astype(np.float32))
+        m.weights = w
+        assert np.array_equal(m.weights, w)
+        X = rng.random((300, mo.N_FEATURES)).astype(np.float32)
+        T = (rng.random(300) * 6.0).astype(np.float32)
+        g, L = m.gradients(X, T)
+        Lo, go = mo.loss_and_gradients(w.astype(np.float64), X.astype(np.float64), T.astype(np.float64))
+        # fp32 accumulation against fp64: relative to the gradient's scale
+        assert abs(L - Lo) <= 1e-5 * max(1.0, Lo)
+        assert np.max(np.abs(g - go)) <= 2e-5 * np.max(np.abs(go))
+        y = m.predict(X)
+        yo = mo.forward(w.astype(np.float64), X.astype(np.float64))
+        assert np.max(np.abs(y - yo)) <= 1e-4 * max(1.0, np.max(np.abs(yo)))
+
+
+@pytest.mark.gpu
+def test_training_fits_a_known_function(nb):
+    rng = np.random.default_rng(2)
+    X = rng.random((20000, mo.N_FEATURES)).astype(np.float32)
+    T = (3.0 + 2.0 * X[:, 0] - 1.5 * X[:, 3] * X[:, 5] + np.sin(3.0 * X[:, 6])).astype(np.float32)
+    with nb.LifetimeModel(seed=4) as m:
+        losses = m.train(X, T, epochs=15, batch=512, lr=2e-3, seed=5)
+        assert losses[-1] < 0.05 * losses[0]
+        pred = m.predict(X[:2000])
+        assert np.mean((pred - T[:2000]) ** 2) < 0.02
+
+
+def _trace_workloads(syn):
+    """Small versions of the trace sources: AlmostInfinite (radius 20) and a
+    SpatiallyExplicit map (16 x 16)."""
+    ai, _ = syn.config2(radius=20)
+    ai = dict(ai, speciation_probability=1e-3)
+    se, _ = syn.config3(width=16, height=16, map_seed=7)
+    se = dict(se, speciation_probability=1e-3)
+    return ai, se
+
+
+@pytest.mark.gpu
+def test_traces_train_a_model_that_beats_the_mean(nb, syn):
+    # a sweep over the speciation probability (as in the batched sweeps):
+    # within one simulation a lineage's remaining life is memoryless
+    # speciation plus coalescence decided by reference order, so most of the
+    # learnable signal is across simulations and over time
+    ai, se = _trace_workloads(syn)
+    nus = [1e-2, 1e-3, 1e-4] * 2
+    X, y = nb.collect_traces([syn.to_scenario(se)] * len(nus), nus, list(range(1, len(nus) + 1)),
+                             snapshot_rounds=8, max_rows=60000)
+    assert X.shape[0] > 5000 and X.shape[1] == mo.N_FEATURES
+    assert np.all(np.isfinite(X)) and np.all(np.isfinite(y)) and np.all(y >= 0.0)
+    rng = np.random.default_rng(0)
+    idx = rng.permutation(X.shape[0])
+    cut = int(0.8 * len(idx))
+    tr, te = idx[:cut], idx[cut:]
+    with nb.LifetimeModel(seed=7) as m:
+        m.train(X[tr], y[tr], epochs=10, batch=1024, lr=2e-3, seed=1)
+        mse = float(np.mean((m.predict(X[te]) - y[te]) ** 2))
+    # the gain over predicting every lineage's remaining events by the mean
+    var = float(np.var(y[te]))
+    print(f"held-out MSE {mse:.4f} vs constant predictor {var:.4f} ({var / mse:.2f}x)")
+    assert mse < 0.7 * var
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("resident", [False, True])
+def test_learned_schedule_is_bit_identical(nb, syn, resident):
+    ai, se = _trace_workloads(syn)
+    X, y = nb.collect_traces([syn.to_scenario(ai)], [ai["speciation_probability"]], [7],
+                             snapshot_rounds=8, max_rows=20000)
+    with nb.LifetimeModel(seed=9) as m:
+        m.train(X, y, epochs=5, batch=1024, lr=2e-3, seed=2)
+        sims = syn.config4(n_sims=6, max_local=3000)
+        cases = [
+            ([syn.to_scenario(d) for d, _ in sims], [d["speciation_probability"] for d, _ in sims],
+             [s for _, s in sims]),
+            ([syn.to_scenario(se)] * 2, [se["speciation_probability"]] * 2, [11, 12]),
+            ([syn.to_scenario(ai)], [ai["speciation_probability"]], [7]),
+        ]
+        for scen, nus, seeds in cases:
+            plain = nb.simulate_batch(scen, nus, seeds, nb.CUDA(resident=resident), collect=True)
+            learned = nb.simulate_batch(scen, nus, seeds, nb.CUDA(resident=resident, schedule="learned", model=m),
+                                        collect=True)
+            for a, b in zip(plain, learned):
+                assert (a.steps, a.biodiversity, a.n_speciation, a.n_dedup, a.time, a.n_rounds) == \
+                       (b.steps, b.biodiversity, b.n_speciation, b.n_dedup, b.time, b.n_rounds)
+                assert np.array_equal(a.speciation, b.speciation)
+
+
+def test_learned_schedule_requires_a_model(nb):
+    with pytest.raises(ValueError):
+        nb._args_struct(nb.CUDA(schedule="learned"))
+    with pytest.raises(ValueError):
+        nb._args_struct(nb.CUDA(schedule="sorted"))
