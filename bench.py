@@ -5,9 +5,14 @@ Workload (default): the batched sweep of 256 SpatiallyImplicit simulations
 cells, migration U(0.01, 0.2), speciation 10^U(-6,-3), seeds 0..255) run
 to completion in one batched launch per round.  One step = one full batch.
 
-  value      events/sec with the origins resident in HBM (device time of the
-             whole batch measured with CUDA events by the library, max over
-             ranks), events = executed lineage steps
+  value      events/sec of the learned-scheduled kernel (the step queue
+             ordered by the lifetime model, trained first on traces the
+             backend generates) with the origins resident in HBM (device time
+             of the whole batch measured with CUDA events by the library, max
+             over ranks), events = executed lineage steps
+  plain      the same for the plain (unordered) kernel on the same workload,
+             with `learned_over_plain` and `outcomes_identical` (the two arms'
+             steps, species, speciation and duplicate counts, times)
   e2e        the same metric through the public C ABI call
              necsim_gpu_simulate_batch with host buffers: scenario set-up,
              host->device origin upload, simulation, device->host events
@@ -30,6 +35,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -45,7 +52,11 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="c4", choices=["c4", "c4-small", "c5", "c2", "c3", "c1"])
-    p.add_argument("--schedule", default="plain", choices=["plain", "learned"])
+    p.add_argument("--schedule", default="both", choices=["plain", "learned", "both"],
+                   help="both: time the plain and the learned-scheduled kernel on the same workload "
+                        "(the line's value is the learned arm's)")
+    p.add_argument("--train-pause", type=float, default=3000.0,
+                   help="pause_before of the trace runs that train the lifetime model")
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pause", type=float, default=None,
@@ -239,6 +250,57 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+def train_lifetime_model(nb, syn, device, pause):
+    """The learned scheduler's model, trained before anything is timed on
+    traces the backend generates from the AlmostInfinite circle (r = 100,
+    sigma = 10) and the SpatiallyExplicit 64x64 landscape, each over a
+    sweep of speciation probabilities, every run paused at `pause`."""
+    ai, _ = syn.config2()
+    se, _ = syn.config3()
+    X, y = [], []
+    t0 = time.perf_counter()
+    for desc in (ai, se):
+        nus = [1e-2, 1e-3, 1e-4]
+        xs, ys = nb.collect_traces([syn.to_scenario(desc)] * len(nus), nus, [11, 12, 13],
+                                   nb.CUDA(device=device), pause_before=pause, snapshot_rounds=16,
+                                   max_rows=1 << 17)
+        X.append(xs)
+        y.append(ys)
+    X = np.concatenate(X)
+    y = np.concatenate(y)
+    model = nb.LifetimeModel(seed=1, device=device)
+    losses = model.train(X, y, epochs=8, batch=1024, lr=2e-3, seed=3)
+    info = {"trace_rows": int(X.shape[0]), "epochs": 8, "final_loss": float(losses[-1]),
+            "label_variance": float(np.var(y)), "seconds": time.perf_counter() - t0,
+            "traces": "AlmostInfinite r=100 sigma=10 and SpatiallyExplicit 64x64, speciation "
+                      "{1e-2,1e-3,1e-4}, paused at t=%g" % pause}
+    return model, info
+
+
+def time_arm(nb, scen, nus, seeds, algo, args, dist):
+    """Device-timed runs of a resident batch: warm-up, then `steps` runs."""
+    batch = nb.Batch(scen, nus, seeds, algo, pause_before=args.pause)
+    for _ in range(args.warmup):
+        batch.run()
+    dist.barrier()
+    r = {"steps": 0, "dev_ms": 0.0, "kernel_ms": 0.0, "step_launches": 0, "visits": 0, "launches": 0,
+         "n_spec": 0, "outs": None}
+    for _ in range(args.steps):
+        outs = batch.run()
+        o0 = outs[0]
+        r["steps"] += sum(o.steps for o in outs)
+        r["n_spec"] += sum(o.n_speciation for o in outs)
+        r["dev_ms"] += o0.total_ms          # device time of the whole batch (CUDA events)
+        r["kernel_ms"] += o0.kernel_ms      # step-kernel time (CUDA events around each launch)
+        r["step_launches"] += o0.n_step_launches
+        r["visits"] += o0.lineage_visits
+        r["launches"] += o0.n_launches
+        r["outs"] = outs
+    dist.barrier()
+    batch.close()
+    return r
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -251,54 +313,40 @@ def main():
     scen = [syn.to_scenario(d) for d, _ in sims]
     nus = [d["speciation_probability"] for d, _ in sims]
     seeds = [s for _, s in sims]
-    algo = nb.CUDA(schedule=args.schedule, device=dist.local_rank if dist.world > 1 else 0)
+    device = dist.local_rank if dist.world > 1 else 0
     se = sims[0][0]["kind"] == 3
     kind = sims[0][0]["kind"]
 
-    batch = nb.Batch(scen, nus, seeds, algo, pause_before=args.pause)
-    for _ in range(args.warmup):
-        batch.run()
+    model, model_info = None, None
+    if args.schedule in ("learned", "both"):
+        model, model_info = train_lifetime_model(nb, syn, device, args.train_pause)
+    plain_algo = nb.CUDA(device=device)
+    head_algo = nb.CUDA(schedule="learned", model=model, device=device) if model else plain_algo
 
+    plain = time_arm(nb, scen, nus, seeds, plain_algo, args, dist) if args.schedule == "both" else None
     clocks = Clocks(dist.local_rank)
-    dist.barrier()
     clocks.start()
-    steps = 0
-    dev_ms = 0.0
-    kernel_ms = 0.0
-    step_launches = 0
-    visits = 0
-    launches = 0
-    n_spec = 0
-    for _ in range(args.steps):
-        outs = batch.run()
-        o0 = outs[0]
-        steps += sum(o.steps for o in outs)
-        n_spec += sum(o.n_speciation for o in outs)
-        dev_ms += o0.total_ms          # device time of the whole batch (CUDA events)
-        kernel_ms += o0.kernel_ms      # step-kernel time (CUDA events around each launch)
-        step_launches += o0.n_step_launches
-        visits += o0.lineage_visits
-        launches += o0.n_launches
-    dist.barrier()
+    head = time_arm(nb, scen, nus, seeds, head_algo, args, dist)
     clk = clocks.stop()
-    batch.close()
 
     # end to end through the public C ABI with host buffers
     e2e_steps, e2e_sec, h2d, d2h = 0, 0.0, 0, 0
     for _ in range(args.steps):
         dist.barrier()
         t0 = time.perf_counter()
-        outs = nb.simulate_batch(scen, nus, seeds, algo, pause_before=args.pause)
+        outs = nb.simulate_batch(scen, nus, seeds, head_algo, pause_before=args.pause)
         dt = time.perf_counter() - t0
         e2e_sec += dist.max(dt)
         e2e_steps += sum(o.steps for o in outs)
         h2d += outs[0].h2d_bytes
         d2h += outs[0].d2h_bytes
 
-    max_ms = dist.max(dev_ms)
-    total_steps = dist.sum(steps)
+    max_ms = dist.max(head["dev_ms"])
+    total_steps = dist.sum(head["steps"])
     value = total_steps / (max_ms / 1e3)
     e2e_value = dist.sum(e2e_steps) / e2e_sec
+    steps, visits, n_spec = head["steps"], head["visits"], head["n_spec"]
+    outs = head["outs"]
 
     # roofline of the step kernel: algorithmic bytes = lineage state read and
     # written per visit (4 u32 + 5 u64/f64 + 1 flag, 57 B each way), speciation
@@ -306,8 +354,8 @@ def main():
     # and one 32-B atom sector per event
     state_bytes = 2 * 57
     alg_bytes = visits * state_bytes + n_spec * 40 + (steps * 64 if se else 0)
-    avg_launch_ms = kernel_ms / max(step_launches, 1)
-    per_launch_bytes = alg_bytes / max(step_launches, 1)
+    avg_launch_ms = head["kernel_ms"] / max(head["step_launches"], 1)
+    per_launch_bytes = alg_bytes / max(head["step_launches"], 1)
     achieved = per_launch_bytes / (avg_launch_ms / 1e3) / 1e9 if avg_launch_ms > 0 else 0.0
     peak, peak_kind = load_peaks()
     traffic = None
@@ -316,7 +364,7 @@ def main():
         try:
             with open(prof) as f:
                 t = json.load(f)
-            traffic = t["dram_bytes_per_lineage_visit"] * visits / max(step_launches, 1)
+            traffic = t["dram_bytes_per_lineage_visit"] * visits / max(head["step_launches"], 1)
         except Exception:
             traffic = None
 
@@ -325,7 +373,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
         "data": "synthetic",
-        "config": {"workload": desc, "schedule": args.schedule, "kind": kind,
+        "config": {"workload": desc, "schedule": "learned" if model else "plain", "kind": kind,
                    "pause_before": args.pause,
                    "simulations": len(sims), "lineages": int(sum(o.n_initial for o in outs)),
                    "l2": "inputs larger than L2 (lineage state %.2f GB)" % (
@@ -335,19 +383,33 @@ def main():
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps},
-        "gpu_launches": launches,
+        "gpu_launches": head["launches"],
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "kernel": "step_kernel", "avg_launch_ms": avg_launch_ms,
-                     "launches": step_launches},
+                     "launches": head["step_launches"]},
     }
+    if plain is not None:
+        p_ms = dist.max(plain["dev_ms"])
+        p_value = dist.sum(plain["steps"]) / (p_ms / 1e3)
+        same = all((a.steps, a.biodiversity, a.n_speciation, a.n_dedup, a.time) ==
+                   (b.steps, b.biodiversity, b.n_speciation, b.n_dedup, b.time)
+                   for a, b in zip(plain["outs"], head["outs"]))
+        line["plain"] = {"value": p_value, "unit": UNIT, "ms_per_step": p_ms / args.steps,
+                         "gpu_launches": plain["launches"]}
+        line["learned_over_plain"] = value / p_value
+        line["outcomes_identical"] = bool(same)
+    if model_info is not None:
+        line["model"] = model_info
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads)
         line["cpu_baseline"] = {"value": ev / sec, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
                                                           len(sims))}
+    if model is not None:
+        model.close()
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
     dist.close()
