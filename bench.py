@@ -96,21 +96,30 @@ def workload(name):
 # distributed plumbing (replicas only)
 # ---------------------------------------------------------------------------
 class Dist:
-    def __init__(self):
+    """One process per GPU (torchrun env); replicas only: the process group
+    carries the max-over-ranks time and the sum of events, never lineages.
+    `backend="gloo"` runs the same plumbing on CPU tensors (tests)."""
+
+    def __init__(self, backend="nccl", timeout_s=600):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
         self.torch = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as td
             self.torch = torch
-            torch.cuda.set_device(self.local_rank)
-            td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                  device_id=torch.device("cuda", self.local_rank))
             self.td = td
+            if backend == "nccl":
+                torch.cuda.set_device(self.local_rank)
+                self.device = "cuda"
+                td.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                      device_id=torch.device("cuda", self.local_rank))
+            else:
+                td.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
 
     def barrier(self):
         if self.torch is not None:
@@ -119,14 +128,14 @@ class Dist:
     def max(self, v):
         if self.torch is None:
             return v
-        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device=self.device)
         self.td.all_reduce(t, op=self.td.ReduceOp.MAX)
         return float(t.item())
 
     def sum(self, v):
         if self.torch is None:
             return v
-        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([float(v)], dtype=self.torch.float64, device=self.device)
         self.td.all_reduce(t, op=self.td.ReduceOp.SUM)
         return float(t.item())
 
@@ -283,8 +292,8 @@ def time_arm(nb, scen, nus, seeds, algo, args, dist):
     for _ in range(args.warmup):
         batch.run()
     dist.barrier()
-    r = {"steps": 0, "dev_ms": 0.0, "kernel_ms": 0.0, "step_launches": 0, "visits": 0, "launches": 0,
-         "n_spec": 0, "outs": None}
+    r = {"steps": 0, "dev_ms": 0.0, "kernel_ms": 0.0, "resident_ms": 0.0, "step_launches": 0, "visits": 0,
+         "launches": 0, "n_spec": 0, "outs": None}
     for _ in range(args.steps):
         outs = batch.run()
         o0 = outs[0]
@@ -292,6 +301,7 @@ def time_arm(nb, scen, nus, seeds, algo, args, dist):
         r["n_spec"] += sum(o.n_speciation for o in outs)
         r["dev_ms"] += o0.total_ms          # device time of the whole batch (CUDA events)
         r["kernel_ms"] += o0.kernel_ms      # step-kernel time (CUDA events around each launch)
+        r["resident_ms"] += o0.resident_ms  # resident-kernel time (its own stream, overlaps)
         r["step_launches"] += o0.n_step_launches
         r["visits"] += o0.lineage_visits
         r["launches"] += o0.n_launches
@@ -388,7 +398,13 @@ def main():
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                      "kernel": "step_kernel", "avg_launch_ms": avg_launch_ms,
-                     "launches": head["step_launches"]},
+                     "launches": head["step_launches"],
+                     "step_kernel_ms_per_step": head["kernel_ms"] / args.steps},
+        # the per-simulation resident kernel runs the small simulations' rounds
+        # on a second stream: a latency-bound chain of dependent 64-bit hash
+        # multiplies per lineage, not a bandwidth roofline
+        "resident": {"kernel": "resident_kernel", "ms_per_step": head["resident_ms"] / args.steps,
+                     "share_of_step": head["resident_ms"] / max(head["dev_ms"], 1e-9)},
     }
     if plain is not None:
         p_ms = dist.max(plain["dev_ms"])
