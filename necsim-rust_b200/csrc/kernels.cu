@@ -155,14 +155,15 @@ __device__ __forceinline__ void record_death(const TraceSink &t, uint64_t gref, 
 }
 
 // The event at l.next (event_sampler/independent.rs:112-222) from the
-// re-primed state rs: speciation, or dispersal + coalescence index.  With
-// EAGER the event's samples 1..4 arrive drawn (e1..e4); otherwise samples 2..4
-// are drawn here only when the branch consumes them.  Only a lane with
-// `emit` writes events and counters (all lanes of a cooperative warp hold
-// the same lineage).
-template <int KIND, bool EAGER>
+// re-primed state rs: speciation, or dispersal + coalescence index.  The
+// event's first DRAWN samples arrive drawn (e1..e4); later ones are drawn
+// here only when the branch consumes them.  Only a lane with `emit` writes
+// events and counters (all lanes of a cooperative warp hold the same
+// lineage).
+template <int KIND, int DRAWN>
 __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const EventSink &k, uint64_t rs,
                                              uint64_t e1, uint64_t e2, uint64_t e3, uint64_t e4, bool emit) {
+    constexpr bool EAGER = DRAWN >= 4;
     l.steps += 1;
     // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
     if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
@@ -189,10 +190,8 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
         }
         return kStepSpeciated;
     }
-    if (!EAGER) {
-        e2 = draw_at(rs, 2);
-        e3 = draw_at(rs, 3);
-    }
+    if (DRAWN < 2) e2 = draw_at(rs, 2);
+    if (DRAWN < 3) e3 = draw_at(rs, 3);
     uint32_t tx, ty, ti;
     if (KIND == kNonSpatial) {
         non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, p.width_magic, tx, ty);
@@ -275,10 +274,9 @@ __device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const E
     if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
     const uint64_t e1 = draw_at(rs, 1);
     if (LAT) {
-        return lineage_event<KIND, true>(l, p, k, rs, e1, draw_at(rs, 2), draw_at(rs, 3), draw_at(rs, 4),
-                                         true);
+        return lineage_event<KIND, 4>(l, p, k, rs, e1, draw_at(rs, 2), draw_at(rs, 3), draw_at(rs, 4), true);
     }
-    return lineage_event<KIND, false>(l, p, k, rs, e1, 0, 0, 0, true);
+    return lineage_event<KIND, 1>(l, p, k, rs, e1, 0, 0, 0, true);
 }
 
 // Copies lane 0's lineage registers to every lane of the warp.
@@ -413,7 +411,7 @@ __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, co
         e4 = __shfl_sync(kFull, dk, 3);
     }
     if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
-    return lineage_event<KIND, true>(l, p, k, rs, e1, e2, e3, e4, lane == 0);
+    return lineage_event<KIND, 4>(l, p, k, rs, e1, e2, e3, e4, lane == 0);
 }
 
 __device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
@@ -431,9 +429,61 @@ __device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
     return k;
 }
 
+// Loads queue position k's lineage into the lane (false: simulation idle or
+// a failed bound check).
+template <int KIND, bool SINGLE>
+__device__ __forceinline__ bool take_lineage(const StepArgs &a, const SimParams *P, unsigned long long k,
+                                             Lane &l) {
+    const uint32_t slot = a.order ? a.order[k] : (uint32_t)k;
+    const uint32_t s = a.in.sim[slot];
+    const SimParams &p = P[SINGLE ? 0 : s];
+    if (!p.active) return false;
+    l.slot = slot;
+    l.s = s;
+    l.x = a.in.x[slot];
+    l.y = a.in.y[slot];
+    l.i = a.in.idx[slot];
+    l.last = a.in.last[slot];
+    l.next = a.in.next[slot];
+    l.reprime = a.in.reprime[slot];
+    l.gref = a.in.gref[slot];
+    l.steps = a.in.steps[slot];
+    l.has_next = a.in.has_next[slot] != 0;
+    l.horizon = p.horizon;
+    if (KIND == kSpatiallyExplicit) return load_cell(p, l.x, l.y, l.rec, a.status);
+    return true;
+}
+
+// Keeps a lineage that reached the horizon (with its peeked next event).
+__device__ __forceinline__ void store_stopped(const StepArgs &a, const Lane &l) {
+    a.in.x[l.slot] = l.x;
+    a.in.y[l.slot] = l.y;
+    a.in.idx[l.slot] = l.i;
+    a.in.last[l.slot] = l.last;
+    a.in.next[l.slot] = l.next;
+    a.in.reprime[l.slot] = l.reprime;
+    a.in.steps[l.slot] = l.steps;
+    a.in.has_next[l.slot] = 1;
+}
+
+// floor(time / delta_t) as the Poisson sampler's first bucket (poisson.rs:44)
+__device__ __forceinline__ uint64_t first_bucket(const SimParams &p, double time) {
+    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
+    return f64_to_u64(floor(q));
+}
+
 // One lane per lineage at a time; a lane whose lineage reaches the horizon
 // (or speciates) takes the next lineage of the queue, so warps stay full
 // while lineages of very different event counts drain.
+//
+// With many lineages per lane (throughput) every lane runs the same pass
+// each iteration: prime the WyHash state for either its current Poisson
+// bucket or its current event, draw samples 1..3, then take the short
+// branch for what the pass was (bucket search or event).  Lanes at
+// different points of their lineages thus execute the same instructions
+// for the hash work instead of diverging through the bucket loop, the
+// event and the refill.  With few lineages per lane (latency) each lane
+// runs lineage_step's latency form.
 template <int KIND, bool SINGLE>
 __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
     // one simulation: its parameters live in shared memory for the launch
@@ -454,6 +504,10 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
     bool exhausted = (n == 0);
     Lane l;
     uint64_t local_steps = 0;
+    // converged form: pass kind, current bucket, search start, location term
+    bool searching = false;
+    uint64_t ts = 0, loc_term = 0;
+    double before = 0.0;
 
     for (;;) {
         const unsigned need = __ballot_sync(kFull, !have && !exhausted);
@@ -465,24 +519,23 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
             if (!have && !exhausted) {
                 const unsigned long long k = base + __popc(need & lanemask_lt);
                 if (k < n) {
-                    const uint32_t slot = a.order ? a.order[k] : (uint32_t)k;
-                    const uint32_t s = a.in.sim[slot];
-                    const SimParams &p = P[SINGLE ? 0 : s];
-                    if (p.active) {
-                        l.slot = slot;
-                        l.s = s;
-                        l.x = a.in.x[slot];
-                        l.y = a.in.y[slot];
-                        l.i = a.in.idx[slot];
-                        l.last = a.in.last[slot];
-                        l.next = a.in.next[slot];
-                        l.reprime = a.in.reprime[slot];
-                        l.gref = a.in.gref[slot];
-                        l.steps = a.in.steps[slot];
-                        l.has_next = a.in.has_next[slot] != 0;
-                        l.horizon = p.horizon;
-                        have = true;
-                        if (KIND == kSpatiallyExplicit) have = load_cell(p, l.x, l.y, l.rec, a.status);
+                    have = take_lineage<KIND, SINGLE>(a, P, k, l);
+                    if (have && !lat) {
+                        const SimParams &p = P[SINGLE ? 0 : l.s];
+                        loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+                        if (l.has_next) {
+                            searching = false;
+                            if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) {
+                                store_stopped(a, l);  // nothing to do before this horizon
+                                have = false;
+                            }
+                        } else {
+                            // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
+                            // (active_lineage_sampler/independent/sampler.rs:69-116)
+                            searching = true;
+                            before = l.last > p.min_event_time ? l.last : p.min_event_time;
+                            ts = first_bucket(p, before);
+                        }
                     }
                 } else {
                     exhausted = true;
@@ -491,28 +544,58 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         }
         if (!__any_sync(kFull, have)) break;
         if (!have) continue;
+        const SimParams &p = P[SINGLE ? 0 : l.s];
 
-        // few lineages for the grid's lanes: latency form (uniform branch)
-        const int r = lat ? lineage_step<KIND, true>(l, P[SINGLE ? 0 : l.s], sink)
-                          : lineage_step<KIND, false>(l, P[SINGLE ? 0 : l.s], sink);
-        if (r == kStepMoved) {
-            local_steps += 1;
+        if (lat) {
+            const int r = lineage_step<KIND, true>(l, p, sink);
+            if (r == kStepMoved) {
+                local_steps += 1;
+                continue;
+            }
+            if (r == kStepStop) {
+                store_stopped(a, l);  // keep the peeked time for the next round
+            } else {
+                if (r == kStepSpeciated) local_steps += 1;
+                a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
+            }
+            have = false;
             continue;
         }
-        if (r == kStepStop) {
-            // keep the peeked time for the next round
-            a.in.x[l.slot] = l.x;
-            a.in.y[l.slot] = l.y;
-            a.in.idx[l.slot] = l.i;
-            a.in.last[l.slot] = l.last;
-            a.in.next[l.slot] = l.next;
-            a.in.reprime[l.slot] = l.reprime;
-            a.in.steps[l.slot] = l.steps;
-            a.in.has_next[l.slot] = 1;
-        } else {
-            if (r == kStepSpeciated) local_steps += 1;
-            a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
+
+        // converged pass: one prime and samples 1..3, for a bucket or an event
+        const uint64_t st = primed_state(loc_term, searching ? ts : l.reprime);
+        const uint64_t d1 = draw_at(st, 1), d2 = draw_at(st, 2), d3 = draw_at(st, 3);
+        if (searching) {
+            // poisson.rs:48-100: the first bucket with an event after `before`
+            long long bits = 0;
+            const int k = poisson_bucket_drawn(st, d1, d2, d3, ts, __double_as_longlong(before), p, bits);
+            if (k < 0) {
+                ts += 1;
+                continue;
+            }
+            l.reprime = ts + kInvPhi * (uint64_t)(k + 1);
+            l.next = max_after(before, __longlong_as_double(bits));
+            l.has_next = true;
+            searching = false;
+            // the reference's early stop `next_event_time >= level_time`
+            // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
+            if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) {
+                store_stopped(a, l);
+                have = false;
+            }
+            continue;
         }
+        const int r = lineage_event<KIND, 3>(l, p, sink, st, d1, d2, d3, 0, true);
+        if (r == kStepMoved) {
+            local_steps += 1;
+            searching = true;
+            loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+            before = l.last;  // the event time, already after min_event_time
+            ts = first_bucket(p, before);
+            continue;
+        }
+        if (r == kStepSpeciated) local_steps += 1;
+        a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
         have = false;
     }
     if (a.steps_total) {
