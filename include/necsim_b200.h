@@ -81,7 +81,12 @@ typedef struct necsim_args {
     uint32_t grid_size;        /* blocks of the step kernel; 0 = autotuned */
     uint32_t dedup_factor_pct; /* dedup hash table load: slots = next_pow2(n*pct/100); default 200 */
     uint32_t schedule;         /* 0 = plain (unsorted) kernel, 1 = learned lifetime buckets */
-    int32_t report_dispersal;  /* reporters consume dispersal events (ReportDispersal) */
+    int32_t report_dispersal;  /* reporters consume dispersal events (ReportDispersal): events
+                                  leave the device after every round and reach the reporter
+                                  as one stream per simulation in PackedEvent order; every
+                                  lineage stays in the global rounds (no CUDA graphs, no
+                                  resident kernel); NECSIM_E_TOO_LARGE if one round's events
+                                  would exceed the buffer (2x the round's expected events) */
     int32_t device;            /* CUDA device ordinal; default 0 */
     uint32_t rounds_per_graph; /* rounds captured per CUDA graph launch; 0 = default (16) */
     uint32_t resident_off;     /* 1: keep small simulations in the global rounds instead of

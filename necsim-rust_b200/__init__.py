@@ -262,6 +262,9 @@ class CUDA:
     rounds_per_graph: int = 16
     resident: bool = True     # small simulations run in the per-simulation resident kernel
     model: Optional["LifetimeModel"] = None
+    # reporters consume dispersal events (ReportDispersal): the events leave
+    # the device after every round (global rounds only, no CUDA graphs)
+    report_dispersal: bool = False
 
 
 Independent = CUDA
@@ -288,6 +291,9 @@ class Outcome:
     resident_ms: float = 0.0
     speciation: Optional[np.ndarray] = None
     remaining: Optional[np.ndarray] = None
+    n_dispersal: int = 0
+    dispersal: Optional[np.ndarray] = None   # with CUDA(report_dispersal=True), collect=True
+    delivery: Optional[list] = None          # reporter calls in order: ("s" | "d", count)
 
 
 def seed_from_u64(seed: int) -> int:
@@ -349,7 +355,7 @@ def _args_struct(algorithm: CUDA):
         if algorithm.model is None:
             raise ValueError("the learned schedule needs a LifetimeModel")
         a.model = algorithm.model.handle
-    a.report_dispersal = 0
+    a.report_dispersal = 1 if algorithm.report_dispersal else 0
     a.device = algorithm.device
     a.rounds_per_graph = algorithm.rounds_per_graph
     a.resident_off = 0 if algorithm.resident else 1
@@ -357,17 +363,24 @@ def _args_struct(algorithm: CUDA):
 
 
 class _Collector:
-    """Reporter sink gathering speciation events (in delivery order)."""
+    """Reporter sink gathering speciation and dispersal events (in delivery
+    order; `kinds` records the sequence of calls as ("s" | "d", count))."""
 
     def __init__(self):
         self.chunks = []
+        self.disp_chunks = []
+        self.kinds = []
 
         def on_spec(user, ptr, n):
             buf = (ctypes.c_char * (n * SPECIATION_DTYPE.itemsize)).from_address(ptr)
             self.chunks.append(np.frombuffer(bytes(buf), dtype=SPECIATION_DTYPE))
+            self.kinds.append(("s", n))
             return 0
 
         def on_disp(user, ptr, n):
+            buf = (ctypes.c_char * (n * DISPERSAL_DTYPE.itemsize)).from_address(ptr)
+            self.disp_chunks.append(np.frombuffer(bytes(buf), dtype=DISPERSAL_DTYPE))
+            self.kinds.append(("d", n))
             return 0
 
         self._spec = _SPEC_CB(on_spec)
@@ -379,12 +392,22 @@ class _Collector:
             return np.zeros(0, dtype=SPECIATION_DTYPE)
         return np.concatenate(self.chunks)
 
+    def dispersal_events(self):
+        if not self.disp_chunks:
+            return np.zeros(0, dtype=DISPERSAL_DTYPE)
+        return np.concatenate(self.disp_chunks)
 
-def _outcome(o: COutcome, spec=None, remaining=None) -> Outcome:
-    return Outcome(bool(o.paused), o.time, o.steps, o.n_initial, o.n_remaining, o.n_speciation,
-                   o.biodiversity, o.n_rounds, o.n_dedup, o.n_launches, o.kernel_ms, o.total_ms,
-                   o.h2d_bytes, o.d2h_bytes, o.n_step_launches, o.lineage_visits, o.resident_ms,
-                   spec, remaining)
+
+def _outcome(o: COutcome, spec=None, remaining=None, col=None) -> Outcome:
+    out = Outcome(bool(o.paused), o.time, o.steps, o.n_initial, o.n_remaining, o.n_speciation,
+                  o.biodiversity, o.n_rounds, o.n_dedup, o.n_launches, o.kernel_ms, o.total_ms,
+                  o.h2d_bytes, o.d2h_bytes, o.n_step_launches, o.lineage_visits, o.resident_ms,
+                  spec, remaining)
+    out.n_dispersal = o.n_dispersal
+    if col is not None and col.disp_chunks:
+        out.dispersal = col.dispersal_events()
+        out.delivery = list(col.kinds)
+    return out
 
 
 class Simulation:
@@ -449,7 +472,7 @@ class Simulation:
                                    ctypes.byref(out))
         self._check(rc)
         return _outcome(out, col.events() if col else None,
-                        self._remaining() if out.paused else None)
+                        self._remaining() if out.paused else None, col)
 
     def resume(self, lineages: np.ndarray, resume_time: float, seed: int,
                pause_before: Optional[float] = None, collect: bool = True,
@@ -466,7 +489,7 @@ class Simulation:
                                             ctypes.byref(out))
         self._check(rc)
         return _outcome(out, col.events() if col else None,
-                        self._remaining() if out.paused else None)
+                        self._remaining() if out.paused else None, col)
 
 
 def simulate(speciation: float, scenario, seed: int, algorithm: Optional[CUDA] = None,
@@ -503,7 +526,8 @@ def simulate_batch(scenarios: Sequence, speciations: Sequence[float], seeds: Seq
                                      outs, err, 512)
     if rc != 0:
         raise NecsimError(rc, err.value.decode())
-    return [_outcome(outs[j], cols[j].events() if cols else None) for j in range(n)]
+    return [_outcome(outs[j], cols[j].events() if cols else None, None, cols[j] if cols else None)
+            for j in range(n)]
 
 
 class Batch:
@@ -543,7 +567,8 @@ class Batch:
                                     outs)
         if rc != 0:
             raise NecsimError(rc, L.necsim_gpu_batch_last_error(self._b).decode())
-        return [_outcome(outs[j], cols[j].events() if cols else None) for j in range(self.n)]
+        return [_outcome(outs[j], cols[j].events() if cols else None, None, cols[j] if cols else None)
+                for j in range(self.n)]
 
     def close(self):
         if getattr(self, "_b", None) is not None and self._b.value:

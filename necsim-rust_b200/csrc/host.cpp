@@ -267,6 +267,16 @@ struct Control {  // small device scalars
     int graph_done;           // set when the global rounds beside a resident launch end
 };
 
+// Events delivered round by round (dispersal reporting): per simulation the
+// species counted so far and the last speciation event delivered.
+struct Delivery {
+    const necsim_reporter *reporters = nullptr;
+    bool one_reporter = false;
+    std::vector<uint64_t> species, n_dispersal;
+    std::vector<DevSpeciationEvent> last;
+    std::vector<uint8_t> has_last;
+};
+
 struct Engine {
     int device = 0;
     int kind = 0;
@@ -312,6 +322,9 @@ struct Engine {
     unsigned *order_hist = nullptr;
     uint32_t *order = nullptr;
     std::vector<float *> d_entropy;  // SE: per-cell dispersal entropy, one per table set
+
+    // dispersal reporting: events drained and delivered after every round
+    Delivery *delivery = nullptr;
 
     // training traces (necsim_gpu_trace_batch)
     bool tracing = false;
@@ -479,6 +492,7 @@ void alloc_run_buffers(Engine &E) {
     E.d_ctl = dev_alloc<Control>(1);
     E.spec_cap = n;
     E.d_spec = dev_alloc<DevSpeciationEvent>(n);
+    if (E.disp_cap) E.d_disp = dev_alloc<DevDispersalEvent>(E.disp_cap);
 }
 
 // Calls push(x, y, index, global_reference) for every origin lineage of the
@@ -690,34 +704,39 @@ ScheduleArgs make_schedule_args(Engine &E) {
 
 // Enqueues `rounds` rounds (even) on the stream; with `events`, records a
 // timing event pair around every step kernel.
-void enqueue_rounds(Engine &E, unsigned rounds, bool events, bool external) {
-    for (unsigned r = 0; r < rounds; ++r) {
-        DeviceLineages &in = (r % 2 == 0) ? E.A : E.B;
-        DeviceLineages &out = (r % 2 == 0) ? E.B : E.A;
-        if (E.learned) {
-            // predictions for lineages without one, then this round's queue
-            // order by expected work (largest first)
-            const FeatureArgs f = make_feature_args(E, in);
-            CK(launch_lineage_predict(f, E.model_w, in.soa.pred_end, E.stream));
-            CK(launch_order(f, in.soa.pred_end, E.order_keys, E.order_hist, E.order, E.aux_grid, E.stream));
-        }
-        if (events) {
-            if (external)
-                CK(cudaEventRecordWithFlags(E.ev_start[r], E.stream, cudaEventRecordExternal));
-            else
-                CK(cudaEventRecord(E.ev_start[r], E.stream));
-        }
-        CK(launch_step(E.kind, make_step_args(E, in), E.step_grid, E.step_block, E.stream));
-        if (events) {
-            if (external)
-                CK(cudaEventRecordWithFlags(E.ev_end[r], E.stream, cudaEventRecordExternal));
-            else
-                CK(cudaEventRecord(E.ev_end[r], E.stream));
-        }
-        CK(launch_dedup(make_dedup_args(E, in, out), E.aux_grid, E.aux_block, E.stream));
-        CK(launch_schedule(make_schedule_args(E), E.stream));
+void enqueue_round(Engine &E, unsigned r, bool events, bool external) {
+    DeviceLineages &in = (r % 2 == 0) ? E.A : E.B;
+    DeviceLineages &out = (r % 2 == 0) ? E.B : E.A;
+    if (E.learned) {
+        // predictions for lineages without one, then this round's queue
+        // order by expected work (largest first)
+        const FeatureArgs f = make_feature_args(E, in);
+        CK(launch_lineage_predict(f, E.model_w, in.soa.pred_end, E.stream));
+        CK(launch_order(f, in.soa.pred_end, E.order_keys, E.order_hist, E.order, E.aux_grid, E.stream));
     }
+    if (events) {
+        if (external)
+            CK(cudaEventRecordWithFlags(E.ev_start[r], E.stream, cudaEventRecordExternal));
+        else
+            CK(cudaEventRecord(E.ev_start[r], E.stream));
+    }
+    CK(launch_step(E.kind, make_step_args(E, in), E.step_grid, E.step_block, E.stream));
+    if (events) {
+        if (external)
+            CK(cudaEventRecordWithFlags(E.ev_end[r], E.stream, cudaEventRecordExternal));
+        else
+            CK(cudaEventRecord(E.ev_end[r], E.stream));
+    }
+    CK(launch_dedup(make_dedup_args(E, in, out), E.aux_grid, E.aux_block, E.stream));
+    CK(launch_schedule(make_schedule_args(E), E.stream));
 }
+
+void enqueue_rounds(Engine &E, unsigned rounds, bool events, bool external) {
+    for (unsigned r = 0; r < rounds; ++r) enqueue_round(E, r, events, external);
+}
+
+// Delivers the events of the round that just ended (dispersal reporting).
+void drain_events(Engine &E);
 
 void build_graph(Engine &E) {
     const unsigned rounds = E.args.rounds_per_graph;
@@ -817,7 +836,14 @@ RunResult run_rounds(Engine &E) {
         rr.launches += 2;
         rr.rounds_launched += 1;
         if (global) {
-            if (E.graph_exec && E.timing_in_graph) {
+            if (E.delivery) {
+                // one round at a time: its events leave the device before the next
+                for (unsigned r = 0; r < rounds; ++r) {
+                    enqueue_round(E, r, true, false);
+                    CK(cudaStreamSynchronize(E.stream));
+                    drain_events(E);
+                }
+            } else if (E.graph_exec && E.timing_in_graph) {
                 CK(cudaGraphLaunch(E.graph_exec, E.stream));
             } else {
                 enqueue_rounds(E, rounds, true, false);
@@ -886,6 +912,106 @@ bool disp_less(const DevDispersalEvent &a, const DevDispersalEvent &b) {
     const uint64_t pa = bits_of(a.prior_time), pb = bits_of(b.prior_time);
     if (pa != pb) return pa < pb;
     return a.gref < b.gref;
+}
+
+// PackedEvent::cmp (event.rs:256-280) between a speciation event (whose
+// target is its origin, event.rs:105-115) and a dispersal event of the same
+// simulation: event time, origin, target, prior time, global reference.
+bool spec_before_disp(const DevSpeciationEvent &a, const DevDispersalEvent &b) {
+    const uint64_t ta = bits_of(a.event_time), tb = bits_of(b.event_time);
+    if (ta != tb) return ta < tb;
+    if (a.x != b.x) return a.x < b.x;
+    if (a.y != b.y) return a.y < b.y;
+    if (a.idx != b.idx) return a.idx < b.idx;
+    if (a.x != b.tx) return a.x < b.tx;
+    if (a.y != b.ty) return a.y < b.ty;
+    if (a.idx != b.tidx) return a.idx < b.tidx;
+    const uint64_t pa = bits_of(a.prior_time), pb = bits_of(b.prior_time);
+    if (pa != pb) return pa < pb;
+    return a.gref <= b.gref;
+}
+
+void drain_events(Engine &E) {
+    Delivery &dv = *E.delivery;
+    Control c;
+    CK(cudaMemcpy(&c, E.d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    if (c.n_disp_total > E.disp_cap || (c.status & kErrDispersalOverflow))
+        fail(NECSIM_E_TOO_LARGE, "one round produced more dispersal events than the event buffer holds "
+                                 "(lower min_round_events or batch fewer simulations)");
+    const uint64_t nd = c.n_disp_total, nsp = std::min<uint64_t>(c.n_spec_total, E.spec_cap);
+    std::vector<DevSpeciationEvent> sp(nsp);
+    std::vector<DevDispersalEvent> di(nd);
+    if (nsp) CK(cudaMemcpy(sp.data(), E.d_spec, nsp * sizeof(DevSpeciationEvent), cudaMemcpyDeviceToHost));
+    if (nd) CK(cudaMemcpy(di.data(), E.d_disp, nd * sizeof(DevDispersalEvent), cudaMemcpyDeviceToHost));
+    E.d2h_bytes += sizeof(c) + nsp * sizeof(DevSpeciationEvent) + nd * sizeof(DevDispersalEvent);
+    // the next round appends from the start of both buffers
+    CK(cudaMemset(&E.d_ctl->n_spec_total, 0, sizeof(unsigned long long)));
+    CK(cudaMemset(&E.d_ctl->n_disp_total, 0, sizeof(unsigned long long)));
+    std::sort(sp.begin(), sp.end(), spec_less);
+    std::sort(di.begin(), di.end(), disp_less);
+    // per simulation: one stream in PackedEvent order, consecutive events of
+    // one kind delivered in one call
+    size_t i = 0, j = 0;
+    std::vector<necsim_speciation_event> out_s;
+    std::vector<necsim_dispersal_event> out_d;
+    while (i < sp.size() || j < di.size()) {
+        const uint32_t s = (j >= di.size() || (i < sp.size() && sp[i].sim <= di[j].sim)) ? sp[i].sim : di[j].sim;
+        const necsim_reporter *rep = dv.reporters ? (dv.one_reporter ? dv.reporters : &dv.reporters[s]) : nullptr;
+        auto flush_s = [&] {
+            if (!out_s.empty() && rep && rep->report_speciation &&
+                rep->report_speciation(rep->user, out_s.data(), out_s.size()) != 0)
+                fail(NECSIM_E_CALLBACK, "reporter stopped the delivery");
+            out_s.clear();
+        };
+        auto flush_d = [&] {
+            if (!out_d.empty() && rep && rep->report_dispersal &&
+                rep->report_dispersal(rep->user, out_d.data(), out_d.size()) != 0)
+                fail(NECSIM_E_CALLBACK, "reporter stopped the delivery");
+            out_d.clear();
+        };
+        while ((i < sp.size() && sp[i].sim == s) || (j < di.size() && di[j].sim == s)) {
+            const bool take_s = i < sp.size() && sp[i].sim == s &&
+                                (j >= di.size() || di[j].sim != s || spec_before_disp(sp[i], di[j]));
+            if (take_s) {
+                flush_d();
+                const DevSpeciationEvent &e = sp[i++];
+                // BiodiversityReporter (plugins/common/src/biodiversity.rs:32-45)
+                if (!dv.has_last[s] || !(dv.last[s].x == e.x && dv.last[s].y == e.y && dv.last[s].idx == e.idx &&
+                                         dv.last[s].event_time == e.event_time))
+                    dv.species[s] += 1;
+                dv.last[s] = e;
+                dv.has_last[s] = 1;
+                necsim_speciation_event r;
+                r.global_lineage_reference = e.gref;
+                r.prior_time = e.prior_time;
+                r.event_time = e.event_time;
+                r.x = e.x;
+                r.y = e.y;
+                r.index = e.idx;
+                r.pad = 0;
+                out_s.push_back(r);
+            } else {
+                flush_s();
+                const DevDispersalEvent &e = di[j++];
+                dv.n_dispersal[s] += 1;
+                necsim_dispersal_event r;
+                r.global_lineage_reference = e.gref;
+                r.prior_time = e.prior_time;
+                r.event_time = e.event_time;
+                r.x = e.x;
+                r.y = e.y;
+                r.index = e.idx;
+                r.target_x = e.tx;
+                r.target_y = e.ty;
+                r.target_index = e.tidx;
+                r.pad = 0;
+                r.pad2 = 0;
+                out_d.push_back(r);
+            }
+        }
+        flush_s();
+        flush_d();
+    }
 }
 
 struct Remaining {
@@ -1002,6 +1128,12 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
         o.lineage_visits = c.visits;
         // deliver this simulation's events in PackedEvent order; count
         // species like BiodiversityReporter (plugins/common/src/biodiversity.rs:32-45)
+        if (E.delivery) {
+            // delivered round by round with the dispersal events
+            o.biodiversity = E.delivery->species[s];
+            o.n_dispersal = E.delivery->n_dispersal[s];
+            continue;
+        }
         size_t end = pos;
         while (end < ev.size() && ev[end].sim == s) ++end;
         std::vector<necsim_speciation_event> out;
@@ -1086,8 +1218,25 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
 void execute_engine(Engine &E, const necsim_reporter *reporters, bool one_reporter,
                     necsim_outcome *outcomes, Remaining &rem) {
     RunResult rr;
-    if (E.n_total > 0) rr = run_rounds(E);
-    finish(E, rr, reporters, one_reporter, outcomes, rem);
+    Delivery dv;
+    if (E.args.report_dispersal) {
+        const size_t ns = E.sims.size();
+        dv.reporters = reporters;
+        dv.one_reporter = one_reporter;
+        dv.species.assign(ns, 0);
+        dv.n_dispersal.assign(ns, 0);
+        dv.last.assign(ns, DevSpeciationEvent{});
+        dv.has_last.assign(ns, 0);
+        E.delivery = &dv;
+    }
+    try {
+        if (E.n_total > 0) rr = run_rounds(E);
+        finish(E, rr, reporters, one_reporter, outcomes, rem);
+    } catch (...) {
+        E.delivery = nullptr;
+        throw;
+    }
+    E.delivery = nullptr;
 }
 
 void run_simulations(Engine &E, std::vector<SimHost> sims, const necsim_args &args,
@@ -1111,7 +1260,19 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
         if (args.model->device != E.device) fail(NECSIM_E_INVALID_ARGUMENT, "the model lives on another device");
         E.model_w = args.model->w;
     }
-    if (args.report_dispersal) fail(NECSIM_E_UNSUPPORTED, "dispersal reporting is not enabled in this build");
+    if (args.report_dispersal) {
+        // every lineage stays in the global rounds, which drain the events
+        // after each round; the buffer holds twice a round's expected events
+        // (n * per <= max(min_round_events + n, step_slice * n) per simulation)
+        E.args.resident_off = 1;
+        uint64_t bound = 0;
+        for (auto &sh : sims)
+            bound += std::max<uint64_t>(args.min_round_events + sh.n_origins, args.step_slice * sh.n_origins);
+        E.disp_cap = 2 * bound + (1ULL << 20);
+        if (E.disp_cap * sizeof(DevDispersalEvent) > (16ULL << 30))
+            fail(NECSIM_E_TOO_LARGE, "dispersal event buffer above 16 GiB (lower min_round_events or batch "
+                                     "fewer simulations)");
+    }
     uint64_t off = 0;
     for (auto &s : sims) {
         s.lineage_offset = off;

@@ -179,3 +179,87 @@ def test_resident_kernel_matches_global_rounds(nb, syn):
     for x, y in zip(a, b):
         assert same_stream(x.speciation, y.speciation)
         assert (x.steps, x.n_rounds, x.n_dedup, x.time) == (y.steps, y.n_rounds, y.n_dedup, y.time)
+
+
+# ---- dispersal events (ReportDispersal) ----
+DISP_FIELDS = ("gref", "prior_time", "event_time", "x", "y", "index", "tx", "ty", "tindex")
+
+
+def same_disp_stream(a, b):
+    if len(a) != len(b):
+        return False
+    for f in DISP_FIELDS:
+        x, y = a[f], b[f]
+        if x.dtype.kind == "f":
+            x, y = x.view(np.uint64), y.view(np.uint64)
+        if not np.array_equal(x, y):
+            return False
+    return True
+
+
+def packed_key(e, speciation):
+    """PackedEvent::cmp key (event.rs:256-280); a speciation's target is its origin."""
+    t = (int(e["tx"]), int(e["ty"]), int(e["tindex"])) if not speciation else (int(e["x"]), int(e["y"]),
+                                                                               int(e["index"]))
+    return (int(np.float64(e["event_time"]).view(np.uint64)), int(e["x"]), int(e["y"]), int(e["index"])) + t + \
+        (int(np.float64(e["prior_time"]).view(np.uint64)), int(e["gref"]))
+
+
+def interleaved(g):
+    """The GPU's delivered stream, speciation and dispersal calls in order."""
+    out, i, j = [], 0, 0
+    for kind, n in g.delivery or []:
+        for _ in range(n):
+            if kind == "s":
+                out.append(packed_key(g.speciation[i], True))
+                i += 1
+            else:
+                out.append(packed_key(g.dispersal[j], False))
+                j += 1
+    return out
+
+
+DISP_CASES = {
+    "ns": (dict(kind=0, speciation_probability=0.01, width=12, height=10, deme=2), 3),
+    "si": (dict(kind=1, speciation_probability=5e-3, width=20, height=10, deme=3,
+                meta_width=300, meta_height=7, meta_deme=2, migration_probability=0.3), 6),
+    "ai": (dict(kind=2, speciation_probability=2e-3, sigma=3.0, radius=15, centre_x=2,
+                centre_y=0xFFFFFFFF - 1), 8),
+}
+
+
+@pytest.mark.parametrize("name", sorted(DISP_CASES) + ["se"])
+def test_dispersal_events_match_canonical_oracle(nb, syn, oracle, name):
+    desc, seed = DISP_CASES[name] if name != "se" else (se_desc(syn, 8, 8, 2e-3, 4), 4)
+    algo = nb.CUDA(report_dispersal=True)
+    g = run_gpu(nb, syn, desc, seed, algo)
+    c = oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, step_slice=algo.step_slice,
+                        min_round_events=algo.min_round_events, step_slice_max=algo.step_slice_max,
+                        report_dispersal=True, dispersal_cap=g.n_dispersal + 16)
+    assert g.n_dispersal == c.n_dispersal > 0
+    assert same_disp_stream(g.dispersal, c.dispersal)
+    assert same_stream(g.speciation, c.speciation)
+    assert (g.steps, g.n_rounds, g.n_dedup, g.biodiversity) == (c.steps, c.n_rounds, c.n_dedup, c.biodiversity)
+    # the two kinds reach the reporter as one stream in PackedEvent order
+    keys = interleaved(g)
+    assert len(keys) == len(g.speciation) + len(g.dispersal)
+    assert keys == sorted(keys)
+    # and the run without dispersal reporting has the same outcome
+    p = run_gpu(nb, syn, desc, seed)
+    assert (p.steps, p.biodiversity, p.n_dedup) == (g.steps, g.biodiversity, g.n_dedup)
+    assert same_stream(p.speciation, g.speciation)
+
+
+def test_dispersal_events_batch_and_pause(nb, syn, oracle):
+    sims = syn.config4(n_sims=3, max_local=400)
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] for d, _ in sims]
+    seeds = [s for _, s in sims]
+    outs = nb.simulate_batch(scen, nus, seeds, nb.CUDA(report_dispersal=True), pause_before=3000.0, collect=True)
+    for (d, s), g in zip(sims, outs):
+        c = oracle.simulate(d, s, mode=oracle.MODE_CANONICAL, min_round_events=1 << 20, step_slice_max=1024,
+                            report_dispersal=True, dispersal_cap=g.n_dispersal + 16, pause_before=3000.0)
+        assert g.n_dispersal == c.n_dispersal
+        assert same_disp_stream(g.dispersal, c.dispersal)
+        assert same_stream(g.speciation, c.speciation)
+        assert g.biodiversity == c.biodiversity and g.n_remaining == c.n_remaining
