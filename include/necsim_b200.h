@@ -295,6 +295,17 @@ int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cel
 int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *out, uint64_t cap,
                              uint64_t *n_out);
 
+/* Origin pre-sampling: positions, in the order of necsim_enumerate_origins,
+ * of the origins that OriginPreSampler::all().percentage(percentage)
+ * .partition(rank, size) selects among the first n
+ * (necsim/impls/no-std/src/cogs/origin_sampler/pre_sampler.rs:48-112: a
+ * golden-ratio quasi-random geometric skip sequence evaluated with the
+ * system libm's log, then every size-th starting at rank).  Simulate the
+ * selected origins with necsim_gpu_simulate_lineages (resume_time 0).
+ * *n_out receives the count; at most `cap` are written (out may be NULL). */
+int necsim_presample_origins(uint64_t n, double percentage, uint32_t rank, uint32_t size, uint64_t *out,
+                             uint64_t cap, uint64_t *n_out);
+
 /* ---- learned lifetime scheduler ----
  * A small MLP (8 -> 64 -> 64 -> 1, ReLU, bf16 weights, fp32 accumulation)
  * predicting log(1 + remaining events) of a lineage from 8 features

@@ -116,6 +116,7 @@ SYMBOLS = [
     "necsim_model_create", "necsim_model_destroy", "necsim_model_last_error",
     "necsim_model_get_weights", "necsim_model_set_weights", "necsim_model_predict",
     "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
+    "necsim_presample_origins",
 ]
 
 _lib = None
@@ -167,6 +168,8 @@ def lib():
     L.necsim_gpu_batch_destroy.argtypes = [vp]
     L.necsim_gpu_batch_destroy.restype = None
     fp = P(ctypes.c_float)
+    L.necsim_presample_origins.argtypes = [u64, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint32, vp, u64, P(u64)]
+    L.necsim_presample_origins.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
     L.necsim_model_create.restype = ctypes.c_int
     L.necsim_model_destroy.argtypes = [vp]
@@ -294,6 +297,25 @@ class Outcome:
     n_dispersal: int = 0
     dispersal: Optional[np.ndarray] = None   # with CUDA(report_dispersal=True), collect=True
     delivery: Optional[list] = None          # reporter calls in order: ("s" | "d", count)
+
+
+def presample_origins(n: int, percentage: float = 1.0, rank: int = 0, size: int = 1) -> np.ndarray:
+    """Positions (in enumerate_origins order) of the origins that
+    `Sample(percentage: p)` and an IsolatedIndividuals partition (rank, size)
+    select among the first n (origin_sampler/pre_sampler.rs:48-112)."""
+    L = lib()
+    k = ctypes.c_uint64()
+    rc = L.necsim_presample_origins(n, percentage, rank, size, None, 0, ctypes.byref(k))
+    if rc != 0:
+        raise NecsimError(rc, "invalid percentage or partition")
+    out = np.zeros(max(k.value, 1), dtype=np.uint64)
+    rc = L.necsim_presample_origins(n, percentage, rank, size, out.ctypes.data, k.value, ctypes.byref(k))
+    if rc != 0:
+        raise NecsimError(rc, "invalid percentage or partition")
+    return out[:k.value]
+
+
+DRIVER = os.path.join(os.path.dirname(LIB_PATH), "necsim-b200")
 
 
 def seed_from_u64(seed: int) -> int:

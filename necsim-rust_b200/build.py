@@ -12,10 +12,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libnecsim_b200.so")
+DRIVER = os.path.join(LIB_DIR, "necsim-b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels.cu", "noalloc.cu", "learned.cu"]
 CPP_SOURCES = ["host.cpp", "tables.cpp"]
+DRIVER_SOURCES = ["driver.cpp", "ron.cpp"]
 
 
 def _sources():
@@ -28,9 +30,9 @@ def _sources():
 
 
 def up_to_date():
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(DRIVER):
         return False
-    t = os.path.getmtime(LIB)
+    t = min(os.path.getmtime(LIB), os.path.getmtime(DRIVER))
     return all(os.path.getmtime(s) <= t for s in _sources())
 
 
@@ -58,6 +60,15 @@ def build(force=False, verbose=False):
     tmp = LIB + ".tmp"
     _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread"], verbose)
     os.replace(tmp, LIB)
+    # the rustcoalescence-style front end, linked against the library
+    drv_objs = []
+    for src in DRIVER_SOURCES:
+        obj = os.path.join(obj_dir, src + ".o")
+        _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-c", os.path.join(CSRC, src), "-o", obj], verbose)
+        drv_objs.append(obj)
+    tmp = DRIVER + ".tmp"
+    _run(["g++", "-o", tmp] + drv_objs + ["-L" + LIB_DIR, "-lnecsim_b200", "-Wl,-rpath,$ORIGIN"], verbose)
+    os.replace(tmp, DRIVER)
     return LIB
 
 

@@ -1,0 +1,497 @@
+// driver.cpp -- `necsim-b200`, a rustcoalescence-style command line front end
+// for the B200 backend: reads the reference's RON simulation configuration
+// (docs/simulate.ron; rustcoalescence/src/args/config/*), builds the
+// scenario, runs it through the C ABI and reports like the reference's
+// common plugins (necsim/plugins/common/src/{biodiversity,event_counter,
+// execution_time}.rs).
+//
+//   necsim-b200 simulate <config.ron>   run on the GPU
+//   necsim-b200 check <config.ron>      parse and validate, print the run (no GPU)
+//
+// Supported: speciation; sample (percentage, origin Habitat | List,
+// mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
+// which writes the configuration that resumes the run; rng Seed | Entropy;
+// the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle, Normal) and
+// SpatiallyExplicit (habitat and dispersal as .npy arrays, Uniform turnover,
+// Strict maps) scenarios; algorithm Independent(...) or CUDA(...) with
+// Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
+// Counter, Execution (others are ignored with a notice).
+#include <chrono>
+#include <cinttypes>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <random>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "../../include/necsim_b200.h"
+#include "ron.h"
+
+using necsim::ron::Value;
+
+namespace {
+
+struct Fail {
+    std::string msg;
+};
+
+[[noreturn]] void fail(const std::string &m) { throw Fail{m}; }
+
+const Value &need(const Value &v, const std::string &name) {
+    const Value *f = v.field(name);
+    if (!f) fail("missing field `" + name + "` in " + (v.text.empty() ? "(...)" : v.text));
+    return *f;
+}
+
+// `(a, b)` as two integers
+void pair_u64(const Value &v, uint64_t &a, uint64_t &b) {
+    if (v.kind != Value::Struct || v.items.size() != 2) fail("expected a pair (a, b)");
+    a = v.items[0].as_u64();
+    b = v.items[1].as_u64();
+}
+
+uint32_t as_u32(const Value &v, const char *what) {
+    const uint64_t x = v.as_u64();
+    if (x > 0xffffffffULL) fail(std::string(what) + " exceeds 2^32 - 1");
+    return (uint32_t)x;
+}
+
+// ---- .npy arrays (little-endian, C order) for SpatiallyExplicit maps ----
+template <typename T>
+std::vector<T> load_npy(const std::string &path, const char *descr, std::vector<uint64_t> &shape) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) fail("cannot open " + path);
+    char magic[6];
+    f.read(magic, 6);
+    if (!f || std::memcmp(magic, "\x93NUMPY", 6) != 0)
+        fail(path + ": not a .npy array (GeoTIFF maps are not read by this driver)");
+    unsigned char ver[2];
+    f.read((char *)ver, 2);
+    uint32_t hlen = 0;
+    if (ver[0] == 1) {
+        unsigned char b[2];
+        f.read((char *)b, 2);
+        hlen = b[0] | (b[1] << 8);
+    } else {
+        unsigned char b[4];
+        f.read((char *)b, 4);
+        hlen = b[0] | (b[1] << 8) | (b[2] << 16) | ((uint32_t)b[3] << 24);
+    }
+    std::string header(hlen, '\0');
+    f.read(&header[0], hlen);
+    if (header.find(std::string("'descr': '") + descr + "'") == std::string::npos)
+        fail(path + ": expected dtype " + descr);
+    if (header.find("'fortran_order': False") == std::string::npos) fail(path + ": expected C order");
+    const size_t a = header.find("'shape': (");
+    if (a == std::string::npos) fail(path + ": no shape");
+    shape.clear();
+    std::stringstream ss(header.substr(a + 10, header.find(')', a) - a - 10));
+    std::string tok;
+    uint64_t total = 1;
+    while (std::getline(ss, tok, ',')) {
+        if (tok.find_first_not_of(" ") == std::string::npos) continue;
+        shape.push_back(std::stoull(tok));
+        total *= shape.back();
+    }
+    std::vector<T> data(total);
+    f.read(reinterpret_cast<char *>(data.data()), total * sizeof(T));
+    if (!f) fail(path + ": truncated data");
+    return data;
+}
+
+struct Run {
+    necsim_scenario sc{};
+    necsim_args args{};
+    double speciation = 0.0;
+    uint64_t seed = 0;
+    bool entropy = false;
+    double percentage = 1.0;
+    uint32_t rank = 0, size = 1;
+    std::vector<necsim_lineage> list;  // sample origin List
+    bool resume = false;
+    double pause_before = -1.0;
+    std::string pause_config;
+    bool rep_biodiversity = false, rep_counter = false, rep_execution = false;
+    std::vector<uint32_t> habitat;
+    std::vector<double> dispersal;
+    std::string summary;
+};
+
+void parse_scenario(const Value &s, Run &r) {
+    const std::string &k = s.variant();
+    necsim_scenario &sc = r.sc;
+    sc.turnover_rate = 0.5;  // UniformTurnoverRate default
+    std::ostringstream o;
+    if (k == "NonSpatial") {
+        uint64_t w, h;
+        pair_u64(need(s, "area"), w, h);
+        sc.kind = NECSIM_NON_SPATIAL;
+        sc.width = (uint32_t)w;
+        sc.height = (uint32_t)h;
+        sc.deme = as_u32(need(s, "deme"), "deme");
+        o << "NonSpatial(area: (" << w << ", " << h << "), deme: " << sc.deme << ")";
+    } else if (k == "SpatiallyImplicit") {
+        uint64_t w, h, mw, mh;
+        pair_u64(need(s, "local_area"), w, h);
+        pair_u64(need(s, "meta_area"), mw, mh);
+        sc.kind = NECSIM_SPATIALLY_IMPLICIT;
+        sc.width = (uint32_t)w;
+        sc.height = (uint32_t)h;
+        sc.deme = as_u32(need(s, "local_deme"), "local_deme");
+        sc.meta_width = (uint32_t)mw;
+        sc.meta_height = (uint32_t)mh;
+        sc.meta_deme = as_u32(need(s, "meta_deme"), "meta_deme");
+        sc.migration_probability = need(s, "migration").as_f64();
+        o << "SpatiallyImplicit(local " << w << "x" << h << "x" << sc.deme << ", meta " << mw << "x" << mh << "x"
+          << sc.meta_deme << ", migration " << sc.migration_probability << ")";
+    } else if (k == "AlmostInfinite") {
+        const Value &sample = need(s, "sample");
+        const Value &disp = need(s, "dispersal");
+        if (sample.variant() != "Circle") fail("AlmostInfinite: only the Circle sample is supported");
+        if (disp.variant() != "Normal") fail("AlmostInfinite: only Normal dispersal is supported");
+        sc.kind = NECSIM_ALMOST_INFINITE_NORMAL;
+        // almost_infinite/mod.rs:103-107: the default centre
+        sc.centre_x = sc.centre_y = 0x7fffffffu;
+        if (const Value *c = sample.field("centre")) {
+            sc.centre_x = as_u32(need(*c, "x"), "centre.x");
+            sc.centre_y = as_u32(need(*c, "y"), "centre.y");
+        }
+        const uint64_t radius = need(sample, "radius").as_u64();
+        if (radius > 0xffff) fail("AlmostInfinite: the radius is a u16");
+        sc.radius = (uint32_t)radius;
+        sc.sigma = need(disp, "sigma").as_f64();
+        o << "AlmostInfinite(Circle(centre: (" << sc.centre_x << ", " << sc.centre_y << "), radius: " << radius
+          << "), Normal(sigma: " << sc.sigma << "))";
+    } else if (k == "SpatiallyExplicit") {
+        const Value &hab = need(s, "habitat"), &disp = need(s, "dispersal");
+        if (const Value *t = s.field("turnover")) {
+            if (t->variant() != "Uniform" || t->items.size() != 1)
+                fail("SpatiallyExplicit: only Uniform(rate) turnover is supported");
+            sc.turnover_rate = t->items[0].as_f64();
+        }
+        if (const Value *m = s.field("mode"))
+            if (m->variant() != "Strict") fail("SpatiallyExplicit: only Strict maps (no fix-up) are supported");
+        std::vector<uint64_t> hs, ds;
+        r.habitat = load_npy<uint32_t>(hab.text, "<u4", hs);
+        r.dispersal = load_npy<double>(disp.text, "<f8", ds);
+        if (hs.size() != 2) fail("habitat must be a 2D (height, width) array");
+        const uint64_t cells = hs[0] * hs[1];
+        if (ds.size() != 2 || ds[0] != cells || ds[1] != cells) fail("dispersal must be (cells, cells)");
+        sc.kind = NECSIM_SPATIALLY_EXPLICIT;
+        sc.height = (uint32_t)hs[0];
+        sc.width = (uint32_t)hs[1];
+        sc.habitat = r.habitat.data();
+        sc.dispersal = r.dispersal.data();
+        o << "SpatiallyExplicit(" << sc.width << "x" << sc.height << " map from " << hab.text << ")";
+    } else {
+        fail("scenario " + k + " is not supported by this backend");
+    }
+    r.summary = o.str();
+}
+
+void parse_algorithm(const Value &a, Run &r) {
+    const std::string &k = a.variant();
+    if (k != "Independent" && k != "CUDA")
+        fail("algorithm " + k + " is not the Independent algorithm this backend runs");
+    necsim_args &g = r.args;
+    if (const Value *v = a.field("delta_t")) g.delta_t = v->as_f64();
+    if (const Value *v = a.field("step_slice")) g.step_slice = v->as_u64();
+    if (const Value *v = a.field("block_size")) g.block_size = as_u32(*v, "block_size");
+    if (const Value *v = a.field("grid_size")) g.grid_size = as_u32(*v, "grid_size");
+    if (const Value *v = a.field("device")) g.device = (int32_t)as_u32(*v, "device");
+    // dedup_cache is accepted: duplicates are removed exactly here, so the
+    // reference's lossy cache capacity has no counterpart
+    if (const Value *p = a.field("parallelism_mode")) {
+        const std::string &m = p->variant();
+        if (m == "IsolatedIndividuals") {
+            const Value &part = need(*p, "partition");
+            r.rank = as_u32(need(part, "rank"), "rank");
+            r.size = as_u32(need(part, "size"), "size");
+        } else if (m != "Monolithic") {
+            fail("parallelism mode " + m + " is not supported (Monolithic, IsolatedIndividuals)");
+        }
+    }
+}
+
+Run parse_config(const std::string &text) {
+    Run r;
+    const Value root = necsim::ron::parse(text);
+    r.speciation = need(root, "speciation").as_f64();
+    if (const Value *s = root.field("sample")) {
+        if (const Value *p = s->field("percentage")) r.percentage = p->as_f64();
+        if (const Value *o = s->field("origin")) {
+            if (o->variant() == "List") {
+                if (o->items.size() != 1 || o->items[0].kind != Value::List) fail("List([...]) expected");
+                for (const Value &l : o->items[0].items) {
+                    necsim_lineage x{};
+                    x.global_reference = need(l, "ref").as_u64();
+                    x.last_event_time = need(l, "time").as_f64();
+                    const Value &loc = need(l, "loc");
+                    x.x = as_u32(need(loc, "x"), "x");
+                    x.y = as_u32(need(loc, "y"), "y");
+                    x.index = as_u32(need(loc, "i"), "i");
+                    r.list.push_back(x);
+                }
+            } else if (o->variant() != "Habitat") {
+                fail("sample origin " + o->variant() + " is not supported (Habitat, List)");
+            }
+        }
+        if (const Value *m = s->field("mode")) {
+            if (m->variant() == "Resume")
+                r.resume = true;
+            else if (m->variant() != "Genesis")
+                fail("sample mode " + m->variant() + " is not supported (Genesis, Resume)");
+        }
+    }
+    if (r.resume != !r.list.empty()) fail("Resume needs a List origin and a List origin needs Resume");
+    if (const Value *p = root.field("pause")) {
+        if (p->variant() == "Pause") {
+            r.pause_before = need(*p, "before").as_f64();
+            r.pause_config = need(*p, "config").text;
+            if (const Value *d = p->field("destiny"))
+                if (d->variant() != "List") fail("pause destiny " + d->variant() + " is not supported (List)");
+            if (const Value *m = p->field("mode"))
+                if (m->variant() != "Resume") fail("pause mode " + m->variant() + " is not supported (Resume)");
+        } else if (p->variant() != "None") {
+            fail("pause must be None or Pause(...)");
+        }
+    }
+    if (const Value *g = root.field("rng")) {
+        if (g->variant() == "Seed" && g->items.size() == 1)
+            r.seed = g->items[0].as_u64();
+        else if (g->variant() == "Entropy")
+            r.entropy = true;
+        else
+            fail("rng " + g->variant() + " is not supported (Seed(u64), Entropy)");
+    } else {
+        r.entropy = true;
+    }
+    parse_scenario(need(root, "scenario"), r);
+    r.sc.speciation_probability = r.speciation;
+    if (const Value *a = root.field("algorithm")) parse_algorithm(*a, r);
+    if (const Value *reps = root.field("reporters")) {
+        std::vector<const Value *> names;
+        for (const Value &p : reps->items) {
+            if (p.variant() == "Plugin") {
+                if (const Value *inner = p.field("reporters"))
+                    for (const Value &x : inner->items) names.push_back(&x);
+            } else {
+                names.push_back(&p);
+            }
+        }
+        for (const Value *n : names) {
+            const std::string &v = n->variant();
+            if (v == "Biodiversity")
+                r.rep_biodiversity = true;
+            else if (v == "Counter")
+                r.rep_counter = true;
+            else if (v == "Execution")
+                r.rep_execution = true;
+            else
+                std::fprintf(stderr, "necsim-b200: reporter %s is not provided here and is ignored\n", v.c_str());
+        }
+    }
+    r.args.report_dispersal = r.rep_counter ? 1 : 0;
+    return r;
+}
+
+// the configuration with the remaining lineages as a List sample in Resume
+// mode and no pause (rustcoalescence/src/cli/simulate/pause.rs:20-60)
+std::string resume_config(const std::string &text, uint64_t seed, const std::vector<necsim_lineage> &rem) {
+    Value root = necsim::ron::parse(text);
+    Value sample;
+    sample.kind = Value::Struct;
+    sample.text = "Sample";
+    Value pct;
+    pct.kind = Value::Number;
+    pct.text = "1.0";
+    sample.fields.emplace_back("percentage", pct);
+    Value origin;
+    origin.kind = Value::Struct;
+    origin.text = "List";
+    Value list;
+    list.kind = Value::List;
+    char buf[64];
+    for (const necsim_lineage &l : rem) {
+        Value lin;
+        lin.kind = Value::Struct;
+        lin.text = "Lineage";
+        Value ref, time, loc;
+        ref.kind = Value::Number;
+        ref.text = std::to_string(l.global_reference);
+        time.kind = Value::Number;
+        std::snprintf(buf, sizeof(buf), "%.17g", l.last_event_time);
+        time.text = buf;
+        if (time.text.find_first_of(".eEn") == std::string::npos) time.text += ".0";
+        loc.kind = Value::Struct;
+        for (auto kv : {std::make_pair("x", l.x), std::make_pair("y", l.y), std::make_pair("i", l.index)}) {
+            Value c;
+            c.kind = Value::Number;
+            c.text = std::to_string(kv.second);
+            loc.fields.emplace_back(kv.first, c);
+        }
+        lin.fields.emplace_back("ref", ref);
+        lin.fields.emplace_back("time", time);
+        lin.fields.emplace_back("loc", loc);
+        list.items.push_back(lin);
+    }
+    origin.items.push_back(list);
+    sample.fields.emplace_back("origin", origin);
+    Value mode;
+    mode.kind = Value::Ident;
+    mode.text = "Resume";
+    sample.fields.emplace_back("mode", mode);
+    Value none;
+    none.kind = Value::Ident;
+    none.text = "None";
+    Value rng;
+    rng.kind = Value::Struct;
+    rng.text = "Seed";
+    Value sv;
+    sv.kind = Value::Number;
+    sv.text = std::to_string(seed);
+    rng.items.push_back(sv);
+    bool has_sample = false, has_pause = false, has_rng = false;
+    for (auto &f : root.fields) {
+        if (f.first == "sample") f.second = sample, has_sample = true;
+        if (f.first == "pause") f.second = none, has_pause = true;
+        if (f.first == "rng") f.second = rng, has_rng = true;
+    }
+    if (!has_sample) root.fields.emplace_back("sample", sample);
+    if (!has_pause) root.fields.emplace_back("pause", none);
+    if (!has_rng) root.fields.emplace_back("rng", rng);
+    return necsim::ron::to_string(root) + "\n";
+}
+
+struct Counts {
+    uint64_t speciation = 0, self_dispersal = 0, out_dispersal = 0;
+};
+
+int on_speciation(void *, const necsim_speciation_event *, uint64_t) { return 0; }
+
+int on_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
+    Counts &c = *static_cast<Counts *>(user);
+    for (uint64_t i = 0; i < n; ++i) {
+        if (ev[i].x == ev[i].target_x && ev[i].y == ev[i].target_y)
+            c.self_dispersal += 1;
+        else
+            c.out_dispersal += 1;
+    }
+    return 0;
+}
+
+std::string slurp(const std::string &path) {
+    std::ifstream f(path);
+    if (!f) fail("cannot read " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return ss.str();
+}
+
+int simulate(const std::string &path, bool run) {
+    const std::string text = slurp(path);
+    Run r = parse_config(text);
+    if (r.entropy) {
+        std::random_device rd;
+        r.seed = ((uint64_t)rd() << 32) ^ rd();
+    }
+    // the origins to simulate
+    std::vector<necsim_lineage> lineages;
+    if (!r.resume) {
+        uint64_t n = 0;
+        int rc = necsim_enumerate_origins(&r.sc, nullptr, 0, &n);
+        if (rc) fail("invalid scenario (status " + std::to_string(rc) + ")");
+        std::vector<necsim_lineage> all(n);
+        rc = necsim_enumerate_origins(&r.sc, all.data(), n, &n);
+        if (rc) fail("origin enumeration failed (status " + std::to_string(rc) + ")");
+        uint64_t k = 0;
+        necsim_presample_origins(n, r.percentage, r.rank, r.size, nullptr, 0, &k);
+        std::vector<uint64_t> pos(k);
+        rc = necsim_presample_origins(n, r.percentage, r.rank, r.size, pos.data(), k, &k);
+        if (rc) fail("invalid sample percentage or partition");
+        lineages.reserve(k);
+        for (uint64_t p : pos) lineages.push_back(all[p]);
+    } else {
+        // a resumed sample is partitioned like fresh origins
+        for (size_t j = r.rank; j < r.list.size(); j += r.size) lineages.push_back(r.list[j]);
+    }
+    std::printf("necsim-b200: %s, speciation %g, seed %" PRIu64 ", %zu lineages%s\n", r.summary.c_str(),
+                r.speciation, r.seed, lineages.size(), r.resume ? " (resumed)" : "");
+    if (r.pause_before >= 0.0) std::printf("necsim-b200: pause before t = %g -> %s\n", r.pause_before,
+                                           r.pause_config.c_str());
+    if (!run) return 0;
+
+    const auto t0 = std::chrono::steady_clock::now();
+    necsim_ctx *ctx = nullptr;
+    int rc = necsim_gpu_create(&r.sc, &r.args, &ctx);
+    if (rc) {
+        const std::string m = ctx ? necsim_gpu_last_error(ctx) : "";
+        necsim_gpu_destroy(ctx);
+        fail("set-up failed (status " + std::to_string(rc) + "): " + m);
+    }
+    Counts counts;
+    necsim_reporter rep{&counts, on_speciation, on_dispersal};
+    necsim_outcome out{};
+    const auto t1 = std::chrono::steady_clock::now();
+    rc = necsim_gpu_simulate_lineages(ctx, lineages.data(), lineages.size(), 0.0, necsim_seed_from_u64(r.seed),
+                                      r.pause_before, &rep, &out);
+    const auto t2 = std::chrono::steady_clock::now();
+    if (rc) {
+        const std::string m = necsim_gpu_last_error(ctx);
+        necsim_gpu_destroy(ctx);
+        fail("simulation failed (status " + std::to_string(rc) + "): " + m);
+    }
+    std::vector<necsim_lineage> rem;
+    if (out.paused) {
+        uint64_t n = out.n_remaining;
+        rem.resize(n);
+        rc = necsim_gpu_remaining_lineages(ctx, rem.data(), n, &n);
+        if (rc) fail("could not read the remaining lineages");
+    }
+    necsim_gpu_destroy(ctx);
+    const auto t3 = std::chrono::steady_clock::now();
+
+    std::printf("necsim-b200: %s after %" PRIu64 " steps at time %.17g\n", out.paused ? "paused" : "done",
+                out.steps, out.time);
+    if (r.rep_biodiversity && out.biodiversity > 0)
+        std::printf("The simulation resulted in a biodiversity of %" PRIu64 " unique species.\n",
+                    out.biodiversity);
+    if (r.rep_counter)
+        std::printf("Event Summary:\n - Speciation:\n    %" PRIu64 "\n - Dispersal (raw):\n   - same location:\n"
+                    "     %" PRIu64 "\n   - new location:\n     %" PRIu64 "\n",
+                    out.n_speciation, counts.self_dispersal, counts.out_dispersal);
+    if (r.rep_execution) {
+        auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
+        std::printf("The simulation took:\n - initialisation: %.3f ms\n - execution: %.3f ms\n - cleanup: %.3f ms\n",
+                    ms(t0, t1), ms(t1, t2), ms(t2, t3));
+    }
+    if (out.paused && !r.pause_config.empty()) {
+        std::ofstream f(r.pause_config);
+        if (!f) fail("cannot write " + r.pause_config);
+        f << resume_config(text, r.seed, rem);
+        std::printf("necsim-b200: %zu remaining lineages written to %s\n", rem.size(), r.pause_config.c_str());
+    }
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    if (argc != 3 || (std::strcmp(argv[1], "simulate") != 0 && std::strcmp(argv[1], "check") != 0)) {
+        std::fprintf(stderr, "usage: necsim-b200 simulate|check <config.ron>\n");
+        return 2;
+    }
+    try {
+        return simulate(argv[2], std::strcmp(argv[1], "simulate") == 0);
+    } catch (const Fail &f) {
+        std::fprintf(stderr, "necsim-b200: %s\n", f.msg.c_str());
+    } catch (const necsim::ron::ParseError &e) {
+        std::fprintf(stderr, "necsim-b200: configuration error (line %zu): %s\n", e.line, e.msg.c_str());
+    } catch (const std::exception &e) {
+        std::fprintf(stderr, "necsim-b200: %s\n", e.what());
+    }
+    return 1;
+}

@@ -1570,6 +1570,43 @@ const char *necsim_gpu_last_error(const necsim_ctx *ctx) { return ctx ? ctx->err
 
 void necsim_gpu_destroy(necsim_ctx *ctx) { delete ctx; }
 
+int necsim_presample_origins(uint64_t n, double percentage, uint32_t rank, uint32_t size, uint64_t *out,
+                             uint64_t cap, uint64_t *n_out) {
+    if (!n_out || !(percentage >= 0.0 && percentage <= 1.0) || size == 0 || rank >= size)
+        return NECSIM_E_INVALID_ARGUMENT;
+    // pre_sampler.rs:12
+    const double kInvPhiF = 6.180339887498949e-1;
+    uint64_t count = 0, seen = 0;
+    auto take = [&](uint64_t pos) {
+        // partition: advance_by(rank), then step_by(size)
+        if (seen >= rank && (seen - rank) % size == 0) {
+            if (out && count < cap) out[count] = pos;
+            ++count;
+        }
+        ++seen;
+    };
+    if (percentage >= 1.0) {
+        for (uint64_t pos = 0; pos < n; ++pos) take(pos);
+    } else if (percentage > 0.0) {
+        // pre_sampler.rs:73-101: skip floor(ln(q) / ln(1 - p)) origins, q the
+        // fractional part of 0.5 + k * INV_PHI
+        const double inv_rate = 1.0 / std::log(1.0 - percentage);
+        double q = 0.5;
+        uint64_t pos = 0;
+        while (pos < n) {
+            q = q + kInvPhiF;
+            q = q - std::floor(q);
+            const double skip = std::floor(std::log(q) * inv_rate);
+            if (!(skip < (double)(n - pos))) break;  // Iterator::nth past the last origin
+            pos += (uint64_t)skip;
+            take(pos);
+            pos += 1;
+        }
+    }
+    *n_out = count;
+    return NECSIM_OK;
+}
+
 }  // extern "C"
 
 // ---- learned lifetime model ----
