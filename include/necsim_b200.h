@@ -89,8 +89,12 @@ typedef struct necsim_args {
                                   would exceed the buffer (2x the round's expected events) */
     int32_t device;            /* CUDA device ordinal; default 0 */
     uint32_t rounds_per_graph; /* rounds captured per CUDA graph launch; 0 = default (16) */
-    uint32_t resident_off;     /* 1: keep small simulations in the global rounds instead of
-                                  the per-simulation resident kernel (same results) */
+    uint32_t resident;         /* 1: in a batch, simulations with at most 256 live lineages leave
+                                  the global rounds for the per-simulation resident kernel (one
+                                  block each, its own rounds); default 0: every simulation stays
+                                  in the global rounds, whose sparse rounds step each lineage with
+                                  a whole warp (faster on every measured workload); same results
+                                  either way; a run of one simulation always stays global */
     uint32_t reserved_args;
     struct necsim_model *model; /* schedule == 1: the lifetime model ordering the step queue
                                    (must stay alive during the call; same device) */

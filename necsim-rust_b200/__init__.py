@@ -64,7 +64,7 @@ class CArgs(ctypes.Structure):
         ("grid_size", ctypes.c_uint32), ("dedup_factor_pct", ctypes.c_uint32),
         ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
-        ("resident_off", ctypes.c_uint32), ("reserved_args", ctypes.c_uint32),
+        ("resident", ctypes.c_uint32), ("reserved_args", ctypes.c_uint32),
         ("model", ctypes.c_void_p),
     ]
 
@@ -263,7 +263,7 @@ class CUDA:
     schedule: str = "plain"   # or "learned" (needs `model`)
     device: int = 0
     rounds_per_graph: int = 16
-    resident: bool = True     # small simulations run in the per-simulation resident kernel
+    resident: bool = False    # batches: small simulations move to the per-simulation resident kernel
     model: Optional["LifetimeModel"] = None
     # reporters consume dispersal events (ReportDispersal): the events leave
     # the device after every round (global rounds only, no CUDA graphs)
@@ -380,7 +380,7 @@ def _args_struct(algorithm: CUDA):
     a.report_dispersal = 1 if algorithm.report_dispersal else 0
     a.device = algorithm.device
     a.rounds_per_graph = algorithm.rounds_per_graph
-    a.resident_off = 0 if algorithm.resident else 1
+    a.resident = 1 if algorithm.resident else 0
     return a
 
 

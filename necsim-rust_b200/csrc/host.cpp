@@ -655,7 +655,7 @@ DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
     a.out_count = &E.d_ctl->out_count;
     a.counters = E.d_counters;
     a.status = &E.d_ctl->status;
-    if (E.args.resident_off == 0) a.arena = E.R.soa;  // route small simulations to the arena
+    if (E.args.resident) a.arena = E.R.soa;  // route small simulations to the arena
     a.params = E.d_params;
     if (E.tracing) {
         a.trace.deaths = E.trace_deaths;
@@ -820,21 +820,24 @@ RunResult run_rounds(Engine &E) {
         last_steps = E.h_ctl->steps_total;
         last_live = E.h_ctl->n_cur;
         const bool global = E.h_ctl->n_active > 0;
-        // both streams are idle here: hand routed simulations to the resident
-        // kernel, then run it on its own stream beside the global rounds
-        CK(launch_promote(E.d_params, (uint32_t)E.sims.size(), E.stream));
-        CK(cudaMemsetAsync(&E.d_ctl->graph_done, 0, sizeof(int), E.stream));
-        CK(cudaEventRecord(E.ev_fork, E.stream));
-        CK(cudaStreamWaitEvent(E.stream_t, E.ev_fork, 0));
-        // beside global rounds: until they end (at most 64 rounds, so the
-        // global kernels never wait long for SM space); alone: long stretches
-        const uint32_t budget = global ? 64 : 256;
-        CK(cudaEventRecord(E.ev_res0, E.stream_t));
-        CK(launch_resident(E.kind, make_resident_args(E, budget, global ? &E.d_ctl->graph_done : nullptr),
-                           global ? grid_beside : grid_alone, E.stream_t));
-        CK(cudaEventRecord(E.ev_res1, E.stream_t));
-        rr.launches += 2;
-        rr.rounds_launched += 1;
+        if (E.args.resident) {
+            // both streams are idle here: hand routed simulations to the
+            // resident kernel, then run it on its own stream beside the
+            // global rounds
+            CK(launch_promote(E.d_params, (uint32_t)E.sims.size(), E.stream));
+            CK(cudaMemsetAsync(&E.d_ctl->graph_done, 0, sizeof(int), E.stream));
+            CK(cudaEventRecord(E.ev_fork, E.stream));
+            CK(cudaStreamWaitEvent(E.stream_t, E.ev_fork, 0));
+            // beside global rounds: until they end (at most 64 rounds, so the
+            // global kernels never wait long for SM space); alone: long stretches
+            const uint32_t budget = global ? 64 : 256;
+            CK(cudaEventRecord(E.ev_res0, E.stream_t));
+            CK(launch_resident(E.kind, make_resident_args(E, budget, global ? &E.d_ctl->graph_done : nullptr),
+                               global ? grid_beside : grid_alone, E.stream_t));
+            CK(cudaEventRecord(E.ev_res1, E.stream_t));
+            rr.launches += 2;
+            rr.rounds_launched += 1;
+        }
         if (global) {
             if (E.delivery) {
                 // one round at a time: its events leave the device before the next
@@ -855,7 +858,7 @@ RunResult run_rounds(Engine &E) {
                                                     E.trace_rows_cap, E.stream));
             rr.rounds_launched += rounds;
         }
-        CK(cudaStreamWaitEvent(E.stream, E.ev_res1, 0));
+        if (E.args.resident) CK(cudaStreamWaitEvent(E.stream, E.ev_res1, 0));
         CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
         E.d2h_bytes += sizeof(Control);
         CK(cudaStreamSynchronize(E.stream));
@@ -865,7 +868,7 @@ RunResult run_rounds(Engine &E) {
                 if (cudaEventElapsedTime(&ms, E.ev_start[r], E.ev_end[r]) == cudaSuccess) rr.kernel_ms += ms;
             }
         }
-        {
+        if (E.args.resident) {
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, E.ev_res0, E.ev_res1) == cudaSuccess) rr.resident_ms += ms;
         }
@@ -1264,7 +1267,7 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
         // every lineage stays in the global rounds, which drain the events
         // after each round; the buffer holds twice a round's expected events
         // (n * per <= max(min_round_events + n, step_slice * n) per simulation)
-        E.args.resident_off = 1;
+        E.args.resident = 0;
         uint64_t bound = 0;
         for (auto &sh : sims)
             bound += std::max<uint64_t>(args.min_round_events + sh.n_origins, args.step_slice * sh.n_origins);
@@ -1297,6 +1300,10 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
         }
         if (!(sh.params.p0 > 0.0)) fail(NECSIM_E_UNSUPPORTED, "exp(-lambda * delta_t) underflows to 0");
     }
+    // a single simulation stays in the global rounds, whose sparse rounds
+    // step each lineage with a whole warp on any SM (the resident kernel
+    // gives a simulation one SM)
+    if (E.sims.size() == 1) E.args.resident = 0;
     choose_launch(E);
     alloc_run_buffers(E);
     upload_origins(E, given);
@@ -1794,7 +1801,7 @@ int necsim_gpu_trace_batch(const necsim_scenario *scenarios, const uint64_t *wyh
     if (snapshot_rounds < 2 || snapshot_rounds % 2) return NECSIM_E_INVALID_ARGUMENT;
     return guarded(nullptr, error, error_cap, [&] {
         necsim_args args = with_defaults(args_in);
-        args.resident_off = 1;  // every lineage stays in the global rounds, where it is snapshotted
+        args.resident = 0;  // every lineage stays in the global rounds, where it is snapshotted
         args.schedule = 0;
         args.model = nullptr;
         args.rounds_per_graph = snapshot_rounds;

@@ -472,6 +472,71 @@ __device__ __forceinline__ uint64_t first_bucket(const SimParams &p, double time
     return f64_to_u64(floor(q));
 }
 
+// A lane's lineage in converged passes: the pass kind, the current Poisson
+// bucket, the time the search starts after, and the location term.
+struct Pass {
+    bool searching;
+    uint64_t ts, loc_term;
+    double before;
+};
+
+// Result of one converged pass besides those of lineage_step.
+constexpr int kPassSearch = 4;
+
+// Prepares the passes of a lineage; false when its peeked next event is
+// already at or beyond the horizon (nothing to do this round).
+template <int KIND>
+__device__ __forceinline__ bool pass_begin(Lane &l, const SimParams &p, Pass &ps) {
+    ps.loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+    if (l.has_next) {
+        ps.searching = false;
+        return __double_as_longlong(l.next) < __double_as_longlong(l.horizon);
+    }
+    // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
+    // (active_lineage_sampler/independent/sampler.rs:69-116)
+    ps.searching = true;
+    ps.before = l.last > p.min_event_time ? l.last : p.min_event_time;
+    ps.ts = first_bucket(p, ps.before);
+    return true;
+}
+
+// One converged pass: prime the WyHash state for the current bucket or the
+// current event and draw samples 1..3 (the same instructions on every lane
+// whatever the pass is), then the short branch of that pass.  Returns
+// kPassSearch (the search goes on), kStepMoved (event executed, searching
+// again), kStepStop (next event at or beyond the horizon, peek kept),
+// kStepSpeciated or kStepDropped.
+template <int KIND>
+__device__ __forceinline__ int pass_run(Lane &l, const SimParams &p, const EventSink &k, Pass &ps) {
+    const uint64_t st = primed_state(ps.loc_term, ps.searching ? ps.ts : l.reprime);
+    const uint64_t d1 = draw_at(st, 1), d2 = draw_at(st, 2), d3 = draw_at(st, 3);
+    if (ps.searching) {
+        // poisson.rs:48-100: the first bucket with an event after `before`
+        long long bits = 0;
+        const int kk = poisson_bucket_drawn(st, d1, d2, d3, ps.ts, __double_as_longlong(ps.before), p, bits);
+        if (kk < 0) {
+            ps.ts += 1;
+            return kPassSearch;
+        }
+        l.reprime = ps.ts + kInvPhi * (uint64_t)(kk + 1);
+        l.next = max_after(ps.before, __longlong_as_double(bits));
+        l.has_next = true;
+        ps.searching = false;
+        // the reference's early stop `next_event_time >= level_time`
+        // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
+        if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) return kStepStop;
+        return kPassSearch;
+    }
+    const int r = lineage_event<KIND, 3>(l, p, k, st, d1, d2, d3, 0, true);
+    if (r == kStepMoved) {
+        ps.searching = true;
+        ps.loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+        ps.before = l.last;  // the event time, already after min_event_time
+        ps.ts = first_bucket(p, ps.before);
+    }
+    return r;
+}
+
 // One lane per lineage at a time; a lane whose lineage reaches the horizon
 // (or speciates) takes the next lineage of the queue, so warps stay full
 // while lineages of very different event counts drain.
@@ -497,17 +562,46 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
     const SimParams *P = SINGLE ? reinterpret_cast<const SimParams *>(params_smem) : a.params;
     const EventSink sink = sink_of(a);
     const uint64_t n = *a.n_cur;
-    const bool lat = n * 4 <= (uint64_t)gridDim.x * blockDim.x;
     const unsigned lane_id = threadIdx.x & 31u;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32u);
+    if (n <= warps) {
+        // at most one lineage per warp: each warp steps its lineages
+        // cooperatively (a lineage's events at warp latency, lineages on
+        // all SMs)
+        uint64_t warp_steps = 0;
+        for (;;) {
+            unsigned long long k = 0;
+            if (lane_id == 0) k = atomicAdd(a.work, 1ULL);
+            k = __shfl_sync(kFull, k, 0);
+            if (k >= n) break;
+            Lane c;
+            if (!take_lineage<KIND, SINGLE>(a, P, k, c)) continue;
+            const SimParams &p = P[SINGLE ? 0 : c.s];
+            int r;
+            for (;;) {
+                r = lineage_step_coop<KIND>(c, p, sink);
+                if (r != kStepMoved) break;
+                warp_steps += 1;
+            }
+            if (lane_id == 0) {
+                if (r == kStepStop) {
+                    store_stopped(a, c);
+                } else {
+                    if (r == kStepSpeciated) warp_steps += 1;
+                    a.state[c.slot] = (r == kStepSpeciated) ? 1 : 2;
+                }
+            }
+        }
+        if (a.steps_total && lane_id == 0 && warp_steps) atomicAdd(a.steps_total, (unsigned long long)warp_steps);
+        return;
+    }
+    const bool lat = n * 4 <= (uint64_t)gridDim.x * blockDim.x;
     const unsigned lanemask_lt = (1u << lane_id) - 1u;
     bool have = false;
     bool exhausted = (n == 0);
     Lane l;
     uint64_t local_steps = 0;
-    // converged form: pass kind, current bucket, search start, location term
-    bool searching = false;
-    uint64_t ts = 0, loc_term = 0;
-    double before = 0.0;
+    Pass ps;  // converged form
 
     for (;;) {
         const unsigned need = __ballot_sync(kFull, !have && !exhausted);
@@ -520,22 +614,9 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
                 const unsigned long long k = base + __popc(need & lanemask_lt);
                 if (k < n) {
                     have = take_lineage<KIND, SINGLE>(a, P, k, l);
-                    if (have && !lat) {
-                        const SimParams &p = P[SINGLE ? 0 : l.s];
-                        loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
-                        if (l.has_next) {
-                            searching = false;
-                            if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) {
-                                store_stopped(a, l);  // nothing to do before this horizon
-                                have = false;
-                            }
-                        } else {
-                            // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
-                            // (active_lineage_sampler/independent/sampler.rs:69-116)
-                            searching = true;
-                            before = l.last > p.min_event_time ? l.last : p.min_event_time;
-                            ts = first_bucket(p, before);
-                        }
+                    if (have && !lat && !pass_begin<KIND>(l, P[SINGLE ? 0 : l.s], ps)) {
+                        store_stopped(a, l);  // nothing to do before this horizon
+                        have = false;
                     }
                 } else {
                     exhausted = true;
@@ -546,56 +627,19 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         if (!have) continue;
         const SimParams &p = P[SINGLE ? 0 : l.s];
 
-        if (lat) {
-            const int r = lineage_step<KIND, true>(l, p, sink);
-            if (r == kStepMoved) {
-                local_steps += 1;
-                continue;
-            }
-            if (r == kStepStop) {
-                store_stopped(a, l);  // keep the peeked time for the next round
-            } else {
-                if (r == kStepSpeciated) local_steps += 1;
-                a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
-            }
-            have = false;
-            continue;
-        }
-
-        // converged pass: one prime and samples 1..3, for a bucket or an event
-        const uint64_t st = primed_state(loc_term, searching ? ts : l.reprime);
-        const uint64_t d1 = draw_at(st, 1), d2 = draw_at(st, 2), d3 = draw_at(st, 3);
-        if (searching) {
-            // poisson.rs:48-100: the first bucket with an event after `before`
-            long long bits = 0;
-            const int k = poisson_bucket_drawn(st, d1, d2, d3, ts, __double_as_longlong(before), p, bits);
-            if (k < 0) {
-                ts += 1;
-                continue;
-            }
-            l.reprime = ts + kInvPhi * (uint64_t)(k + 1);
-            l.next = max_after(before, __longlong_as_double(bits));
-            l.has_next = true;
-            searching = false;
-            // the reference's early stop `next_event_time >= level_time`
-            // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
-            if (__double_as_longlong(l.next) >= __double_as_longlong(l.horizon)) {
-                store_stopped(a, l);
-                have = false;
-            }
-            continue;
-        }
-        const int r = lineage_event<KIND, 3>(l, p, sink, st, d1, d2, d3, 0, true);
+        // few lineages for the grid's lanes: latency form (uniform branch)
+        const int r = lat ? lineage_step<KIND, true>(l, p, sink) : pass_run<KIND>(l, p, sink, ps);
+        if (r == kPassSearch) continue;
         if (r == kStepMoved) {
             local_steps += 1;
-            searching = true;
-            loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
-            before = l.last;  // the event time, already after min_event_time
-            ts = first_bucket(p, before);
             continue;
         }
-        if (r == kStepSpeciated) local_steps += 1;
-        a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
+        if (r == kStepStop) {
+            store_stopped(a, l);  // keep the peeked time for the next round
+        } else {
+            if (r == kStepSpeciated) local_steps += 1;
+            a.state[l.slot] = (r == kStepSpeciated) ? 1 : 2;  // 2: dropped by a failed bound check
+        }
         have = false;
     }
     if (a.steps_total) {
@@ -633,21 +677,22 @@ __device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long l
 // Lineage slot j lives on warp j % 8, lane j / 8: a simulation with few
 // lineages gets one lineage per warp, so lineages never share (and diverge
 // within) a warp until there are more than eight of them.
-template <int KIND>
-__global__ void __launch_bounds__(kResidentMax) resident_kernel(ResidentArgs a) {
-    constexpr unsigned kWarps = kResidentMax / 32;
-    __shared__ uint32_t sx[kResidentMax], sy[kResidentMax], si[kResidentMax];
-    __shared__ unsigned long long slast[kResidentMax], sgref[kResidentMax];
-    __shared__ unsigned char salive[kResidentMax];
-    __shared__ unsigned int sscan[kResidentMax];
+template <int KIND, int THREADS>
+__global__ void __launch_bounds__(THREADS) resident_kernel(ResidentArgs a) {
+    constexpr unsigned kWarps = THREADS / 32;
+    constexpr unsigned kSlots = THREADS;  // lineage slots (>= kResidentMax)
+    __shared__ uint32_t sx[kSlots], sy[kSlots], si[kSlots];
+    __shared__ unsigned long long slast[kSlots], sgref[kSlots];
+    __shared__ unsigned char salive[kSlots];
+    __shared__ unsigned int sscan[kSlots];
     __shared__ unsigned int s_n;
     __shared__ int s_go;
     __shared__ double s_h;
     // staging of surviving lineages during the block's compaction
-    __shared__ uint32_t tx_[kResidentMax], ty_[kResidentMax], ti_[kResidentMax];
-    __shared__ double tlast[kResidentMax], tnext[kResidentMax];
-    __shared__ unsigned long long trep[kResidentMax], tgref[kResidentMax], tsteps[kResidentMax];
-    __shared__ unsigned char thas[kResidentMax];
+    __shared__ uint32_t tx_[kSlots], ty_[kSlots], ti_[kSlots];
+    __shared__ double tlast[kSlots], tnext[kSlots];
+    __shared__ unsigned long long trep[kSlots], tgref[kSlots], tsteps[kSlots];
+    __shared__ unsigned char thas[kSlots];
 
     const unsigned t = threadIdx.x;
     const unsigned j = (t & 31u) * kWarps + (t >> 5);  // this thread's lineage slot
@@ -787,13 +832,13 @@ __global__ void __launch_bounds__(kResidentMax) resident_kernel(ResidentArgs a) 
             // inclusive scan of the survivor flags in slot order
             sscan[j] = survivor ? 1u : 0u;
             __syncthreads();
-            for (unsigned d = 1; d < (unsigned)kResidentMax; d <<= 1) {
+            for (unsigned d = 1; d < kSlots; d <<= 1) {
                 const unsigned add = (j >= d) ? sscan[j - d] : 0u;
                 __syncthreads();
                 sscan[j] += add;
                 __syncthreads();
             }
-            const unsigned total = sscan[kResidentMax - 1];
+            const unsigned total = sscan[kSlots - 1];
             if (survivor) {
                 const unsigned d = sscan[j] - 1u;
                 tx_[d] = l.x;
@@ -1097,10 +1142,12 @@ cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st) 
 
 cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st) {
     switch (kind) {
-    case kNonSpatial: resident_kernel<kNonSpatial><<<grid, kResidentMax, 0, st>>>(a); break;
-    case kSpatiallyImplicit: resident_kernel<kSpatiallyImplicit><<<grid, kResidentMax, 0, st>>>(a); break;
-    case kAlmostInfiniteNormal: resident_kernel<kAlmostInfiniteNormal><<<grid, kResidentMax, 0, st>>>(a); break;
-    case kSpatiallyExplicit: resident_kernel<kSpatiallyExplicit><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kNonSpatial: resident_kernel<kNonSpatial, kResidentMax><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kSpatiallyImplicit: resident_kernel<kSpatiallyImplicit, kResidentMax><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kAlmostInfiniteNormal:
+        resident_kernel<kAlmostInfiniteNormal, kResidentMax><<<grid, kResidentMax, 0, st>>>(a);
+        break;
+    case kSpatiallyExplicit: resident_kernel<kSpatiallyExplicit, kResidentMax><<<grid, kResidentMax, 0, st>>>(a); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
