@@ -55,6 +55,9 @@ def parse():
     p.add_argument("--schedule", default="both", choices=["plain", "learned", "both"],
                    help="both: time the plain and the learned-scheduled kernel on the same workload "
                         "(the line's value is the learned arm's)")
+    p.add_argument("--autotune", default="auto", choices=["auto", "on", "off"],
+                   help="pick block size, step_slice and dedup factor by timing a paused sample first "
+                        "(auto: on for the batched sweeps)")
     p.add_argument("--train-pause", type=float, default=3000.0,
                    help="pause_before of the trace runs that train the lifetime model")
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
@@ -331,7 +334,15 @@ def main():
     if args.schedule in ("learned", "both"):
         model, model_info = train_lifetime_model(nb, syn, device, args.train_pause)
     plain_algo = nb.CUDA(device=device)
-    head_algo = nb.CUDA(schedule="learned", model=model, device=device) if model else plain_algo
+    tune_info = None
+    if args.autotune == "on" or (args.autotune == "auto" and args.workload.startswith("c4")):
+        t0 = time.perf_counter()
+        plain_algo, res = nb.autotune(scen, nus, seeds, plain_algo, sample_pause=400.0)
+        tune_info = {"block_size": plain_algo.block_size, "step_slice": plain_algo.step_slice,
+                     "dedup_factor_pct": plain_algo.dedup_factor_pct, "candidates": int(len(res)),
+                     "sample": "every k-th simulation up to 4M origins, paused at t=400",
+                     "seconds": time.perf_counter() - t0}
+    head_algo = nb.CUDA(**{**plain_algo.__dict__, "schedule": "learned", "model": model}) if model else plain_algo
 
     plain = time_arm(nb, scen, nus, seeds, plain_algo, args, dist) if args.schedule == "both" else None
     clocks = Clocks(dist.local_rank)
@@ -418,6 +429,8 @@ def main():
         line["outcomes_identical"] = bool(same)
     if model_info is not None:
         line["model"] = model_info
+    if tune_info is not None:
+        line["autotune"] = tune_info
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads)

@@ -310,6 +310,30 @@ int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *ou
 int necsim_presample_origins(uint64_t n, double percentage, uint32_t rank, uint32_t size, uint64_t *out,
                              uint64_t cap, uint64_t *n_out);
 
+/* ---- launch autotuner ----
+ * Times a bounded sample of a batch -- every k-th simulation so that the
+ * sample holds at most `max_sample_lineages` origins, each paused at
+ * `sample_pause` -- under every combination of block size {64, 128, 256},
+ * step_slice {s, 2s, 4s} (s = args->step_slice) and dedup table factor
+ * {200, 400} %, on the device of `args`, and returns in *best the argument
+ * set with the shortest time to the pause (best of two runs after a
+ * warm-up run).  Every candidate yields the same species and speciation
+ * events; only steps (duplicate work) and time differ.  `results` (nullable)
+ * receives one record per candidate, at most `results_cap`; *n_results the
+ * count.  No counterpart in the reference (its arguments are set by hand). */
+typedef struct necsim_autotune_result {
+    uint32_t block_size;
+    uint32_t dedup_factor_pct;
+    uint64_t step_slice;
+    double ms;      /* best device time of the sample (CUDA events) */
+    uint64_t steps; /* events of the sample */
+} necsim_autotune_result;
+
+int necsim_gpu_autotune(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,
+                        const necsim_args *args, double sample_pause, uint64_t max_sample_lineages,
+                        necsim_args *best, necsim_autotune_result *results, uint32_t results_cap,
+                        uint32_t *n_results, char *error, size_t error_cap);
+
 /* ---- learned lifetime scheduler ----
  * A small MLP (8 -> 64 -> 64 -> 1, ReLU, bf16 weights, fp32 accumulation)
  * predicting log(1 + remaining events) of a lineage from 8 features

@@ -116,7 +116,7 @@ SYMBOLS = [
     "necsim_model_create", "necsim_model_destroy", "necsim_model_last_error",
     "necsim_model_get_weights", "necsim_model_set_weights", "necsim_model_predict",
     "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
-    "necsim_presample_origins",
+    "necsim_presample_origins", "necsim_gpu_autotune",
 ]
 
 _lib = None
@@ -168,6 +168,10 @@ def lib():
     L.necsim_gpu_batch_destroy.argtypes = [vp]
     L.necsim_gpu_batch_destroy.restype = None
     fp = P(ctypes.c_float)
+    L.necsim_gpu_autotune.argtypes = [P(CScenario), P(u64), ctypes.c_uint32, P(CArgs), ctypes.c_double, u64,
+                                      P(CArgs), vp, ctypes.c_uint32, P(ctypes.c_uint32), ctypes.c_char_p,
+                                      ctypes.c_size_t]
+    L.necsim_gpu_autotune.restype = ctypes.c_int
     L.necsim_presample_origins.argtypes = [u64, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint32, vp, u64, P(u64)]
     L.necsim_presample_origins.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
@@ -778,3 +782,40 @@ def collect_traces(scenarios: Sequence, speciations: Sequence[float], seeds: Seq
     if rc != 0:
         raise NecsimError(rc, err.value.decode())
     return X[:got.value].copy(), y[:got.value].copy()
+
+
+# ---------------------------------------------------------------------------
+# Launch autotuner
+# ---------------------------------------------------------------------------
+AUTOTUNE_DTYPE = np.dtype([("block_size", "<u4"), ("dedup_factor_pct", "<u4"), ("step_slice", "<u8"),
+                           ("ms", "<f8"), ("steps", "<u8")])
+
+
+def autotune(scenarios: Sequence, speciations: Sequence[float], seeds: Sequence[int],
+             algorithm: Optional[CUDA] = None, sample_pause: float = 400.0,
+             max_sample_lineages: int = 1 << 22):
+    """Picks block size, step_slice and the dedup table factor for a batch
+    by timing a bounded sample of it (necsim_gpu_autotune).  Returns
+    (CUDA arguments with the winner filled in, per-candidate results)."""
+    L = lib()
+    base = algorithm or CUDA()
+    n = len(scenarios)
+    structs = (CScenario * n)()
+    keep = []
+    for j, (sc, nu) in enumerate(zip(scenarios, speciations)):
+        c = _scenario_struct(sc, nu)
+        keep.append(c)
+        structs[j] = c
+    seeds_arr = (ctypes.c_uint64 * n)(*[seed_from_u64(s) for s in seeds])
+    args = _args_struct(CUDA(**{**base.__dict__, "schedule": "plain", "model": None}))
+    best = CArgs()
+    res = np.zeros(32, dtype=AUTOTUNE_DTYPE)
+    got = ctypes.c_uint32()
+    err = ctypes.create_string_buffer(512)
+    rc = L.necsim_gpu_autotune(structs, seeds_arr, n, ctypes.byref(args), sample_pause, max_sample_lineages,
+                               ctypes.byref(best), res.ctypes.data, len(res), ctypes.byref(got), err, 512)
+    if rc != 0:
+        raise NecsimError(rc, err.value.decode())
+    tuned = CUDA(**{**base.__dict__, "block_size": best.block_size, "step_slice": best.step_slice,
+                    "dedup_factor_pct": best.dedup_factor_pct})
+    return tuned, res[:got.value].copy()

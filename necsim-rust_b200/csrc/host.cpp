@@ -637,6 +637,8 @@ FeatureArgs make_feature_args(Engine &E, DeviceLineages &in) {
     f.params = E.d_params;
     f.counters = E.d_counters;
     f.kind = E.kind;
+    // the step kernel's cooperative regime (one warp per lineage)
+    f.skip_at_most = (uint64_t)E.step_grid * (E.step_block / 32);
     return f;
 }
 
@@ -1498,6 +1500,76 @@ static std::vector<SimHost> batch_sims(const necsim_scenario *scenarios, const u
         sh.n_origins = count_origins(scenarios[s]);
     }
     return sims;
+}
+
+int necsim_gpu_autotune(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,
+                        const necsim_args *args_in, double sample_pause, uint64_t max_sample_lineages,
+                        necsim_args *best, necsim_autotune_result *results, uint32_t results_cap,
+                        uint32_t *n_results, char *error, size_t error_cap) {
+    if (!scenarios || !wyhash_seeds || n_sims == 0 || !best || !(sample_pause > 0.0))
+        return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, error, error_cap, [&] {
+        const necsim_args base = with_defaults(args_in);
+        if (base.report_dispersal || base.schedule)
+            fail(NECSIM_E_INVALID_ARGUMENT, "tune the plain schedule without dispersal reporting");
+        // the sample: every k-th simulation, at most max_sample_lineages origins
+        uint64_t total = 0;
+        for (uint32_t s = 0; s < n_sims; ++s) {
+            validate(scenarios[s]);
+            total += count_origins(scenarios[s]);
+        }
+        const uint64_t cap = max_sample_lineages ? max_sample_lineages : (1ULL << 22);
+        uint32_t stride = 1;
+        while (stride < n_sims && total / stride > cap) ++stride;
+        std::vector<necsim_scenario> sc;
+        std::vector<uint64_t> seeds;
+        for (uint32_t s = 0; s < n_sims; s += stride) {
+            sc.push_back(scenarios[s]);
+            seeds.push_back(wyhash_seeds[s]);
+        }
+        const uint32_t blocks[] = {64, 128, 256};
+        const uint64_t slices[] = {base.step_slice, 2 * base.step_slice, 4 * base.step_slice};
+        const uint32_t dedups[] = {200, 400};
+        double best_ms = 0.0;
+        uint32_t count = 0;
+        for (uint32_t b : blocks)
+            for (uint64_t sl : slices)
+                for (uint32_t dd : dedups) {
+                    necsim_args a = base;
+                    a.block_size = b;
+                    a.step_slice = sl;
+                    a.dedup_factor_pct = dd;
+                    a = with_defaults(&a);
+                    Engine E;
+                    setup_engine(E, a);
+                    prepare_engine(E, batch_sims(sc.data(), seeds.data(), (uint32_t)sc.size(), a, sample_pause), a,
+                                   nullptr, nullptr);
+                    std::vector<necsim_outcome> outs(sc.size());
+                    Remaining rem;
+                    double ms = 0.0;
+                    uint64_t steps = 0;
+                    for (int rep = 0; rep < 3; ++rep) {
+                        execute_engine(E, nullptr, false, outs.data(), rem);
+                        if (rep == 0) continue;  // warm-up
+                        if (rep == 1 || outs[0].total_ms < ms) ms = outs[0].total_ms;
+                        steps = 0;
+                        for (const auto &o : outs) steps += o.steps;
+                    }
+                    if (results && count < results_cap) {
+                        results[count].block_size = b;
+                        results[count].dedup_factor_pct = dd;
+                        results[count].step_slice = sl;
+                        results[count].ms = ms;
+                        results[count].steps = steps;
+                    }
+                    ++count;
+                    if (count == 1 || ms < best_ms) {
+                        best_ms = ms;
+                        *best = a;
+                    }
+                }
+        if (n_results) *n_results = count;
+    });
 }
 
 int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,

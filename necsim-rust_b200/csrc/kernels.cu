@@ -433,8 +433,8 @@ __device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
 // a failed bound check).
 template <int KIND, bool SINGLE>
 __device__ __forceinline__ bool take_lineage(const StepArgs &a, const SimParams *P, unsigned long long k,
-                                             Lane &l) {
-    const uint32_t slot = a.order ? a.order[k] : (uint32_t)k;
+                                             Lane &l, bool ordered = true) {
+    const uint32_t slot = (ordered && a.order) ? a.order[k] : (uint32_t)k;
     const uint32_t s = a.in.sim[slot];
     const SimParams &p = P[SINGLE ? 0 : s];
     if (!p.active) return false;
@@ -575,7 +575,9 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
             k = __shfl_sync(kFull, k, 0);
             if (k >= n) break;
             Lane c;
-            if (!take_lineage<KIND, SINGLE>(a, P, k, c)) continue;
+            // every lineage gets a warp at once: the queue order is moot
+            // (and not computed for such rounds)
+            if (!take_lineage<KIND, SINGLE>(a, P, k, c, false)) continue;
             const SimParams &p = P[SINGLE ? 0 : c.s];
             int r;
             for (;;) {

@@ -134,10 +134,11 @@ __global__ void __launch_bounds__(256) mlp_predict_kernel(const __nv_bfloat16 *w
 }
 
 __global__ void __launch_bounds__(256) lineage_predict_kernel(FeatureArgs a, const __nv_bfloat16 *w, float *pred_end) {
+    const uint64_t n = *a.n_cur;
+    if (n <= a.skip_at_most) return;  // the step kernel gives every lineage a warp
     __shared__ __align__(16) float Ws[kMlpParams];
     stage_weights(w, Ws);
     __syncthreads();
-    const uint64_t n = *a.n_cur;
 #pragma unroll 1
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t steps = a.in.steps[j];
@@ -354,10 +355,11 @@ __device__ __forceinline__ float round_events(const SimParams &p, const SimCount
 }
 
 __global__ void order_key_kernel(FeatureArgs a, const float *pred_end, uint8_t *keys, unsigned *hist) {
+    const uint64_t n = *a.n_cur;
+    if (n <= a.skip_at_most) return;
     __shared__ unsigned h[kOrderBuckets];
     if (threadIdx.x < kOrderBuckets) h[threadIdx.x] = 0;
     __syncthreads();
-    const uint64_t n = *a.n_cur;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t s = a.in.sim[j];
         const float rem = pred_end[j] - (float)a.in.steps[j];
@@ -386,9 +388,10 @@ __global__ void order_scan_kernel(unsigned *hist) {
     hist[lane] = 0;
 }
 
-__global__ void order_scatter_kernel(const unsigned long long *n_cur, const uint8_t *keys, unsigned *hist,
-                                     uint32_t *order) {
+__global__ void order_scatter_kernel(const unsigned long long *n_cur, uint64_t skip_at_most, const uint8_t *keys,
+                                     unsigned *hist, uint32_t *order) {
     const uint64_t n = *n_cur;
+    if (n <= skip_at_most) return;
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -421,7 +424,7 @@ cudaError_t launch_order(const FeatureArgs &f, const float *pred_end, uint8_t *k
                          unsigned grid, cudaStream_t st) {
     order_key_kernel<<<grid, 256, 0, st>>>(f, pred_end, keys, hist);
     order_scan_kernel<<<1, 32, 0, st>>>(hist);
-    order_scatter_kernel<<<grid, 256, 0, st>>>(f.n_cur, keys, hist, order);
+    order_scatter_kernel<<<grid, 256, 0, st>>>(f.n_cur, f.skip_at_most, keys, hist, order);
     return cudaGetLastError();
 }
 

@@ -61,6 +61,7 @@ struct FeatureArgs {
     const SimParams *params;
     const SimCounters *counters;
     int kind;
+    uint64_t skip_at_most;  // rounds with at most this many live lineages need no order
 };
 
 // Appends a snapshot row for every live lineage of `f.in` (rows beyond `cap`
