@@ -47,6 +47,7 @@ enum necsim_scenario_kind {
     NECSIM_SPATIALLY_IMPLICIT = 1,     /* rustcoalescence/scenarios/src/spatially_implicit.rs        */
     NECSIM_ALMOST_INFINITE_NORMAL = 2, /* rustcoalescence/scenarios/src/almost_infinite/normal.rs    */
     NECSIM_SPATIALLY_EXPLICIT = 3,     /* rustcoalescence/scenarios/src/spatially_explicit/turnover/uniform.rs */
+    NECSIM_ALMOST_INFINITE_CLARK2DT = 4, /* rustcoalescence/scenarios/src/almost_infinite/clark2dt.rs */
 };
 
 /* Replaces the reference's `ScenarioCogs` as produced by `Scenario::new`
@@ -65,6 +66,8 @@ typedef struct necsim_scenario {
     uint32_t centre_x, centre_y, radius, reserved1; /* AlmostInfinite Circle sample */
     const uint32_t *habitat;         /* SpatiallyExplicit: width*height u32, row-major */
     const double *dispersal;         /* SpatiallyExplicit: (w*h) x (w*h) f64, row-major */
+    double shape_u, tail_p;          /* AlmostInfinite Clark2Dt dispersal (u > 0, p > 0); the
+                                        Circle sample fields as for Normal */
 } necsim_scenario;
 
 /* Replaces `CudaArguments` / `IndependentArguments`

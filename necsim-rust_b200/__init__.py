@@ -23,6 +23,7 @@ LIB_PATH = _build.LIB
 NON_SPATIAL = 0
 SPATIALLY_IMPLICIT = 1
 ALMOST_INFINITE_NORMAL = 2
+ALMOST_INFINITE_CLARK2DT = 4
 SPATIALLY_EXPLICIT = 3
 
 ERRORS = {
@@ -53,6 +54,7 @@ class CScenario(ctypes.Structure):
         ("radius", ctypes.c_uint32), ("reserved1", ctypes.c_uint32),
         ("habitat", ctypes.POINTER(ctypes.c_uint32)),
         ("dispersal", ctypes.POINTER(ctypes.c_double)),
+        ("shape_u", ctypes.c_double), ("tail_p", ctypes.c_double),
     ]
 
 
@@ -236,10 +238,18 @@ class Normal:
 
 
 @dataclass
+class Clark2Dt:
+    """`Clark2Dt(shape_u: u, tail_p: p)` dispersal (almost_infinite/clark2dt.rs;
+    dispersal_sampler/almost_infinite_clark2dt.rs)."""
+    shape_u: float
+    tail_p: float
+
+
+@dataclass
 class AlmostInfinite:
-    """`AlmostInfinite(sample: Circle(..), dispersal: Normal(..))`."""
+    """`AlmostInfinite(sample: Circle(..), dispersal: Normal(..) | Clark2Dt(..))`."""
     sample: Circle
-    dispersal: Normal
+    dispersal: object
 
 
 @dataclass
@@ -344,8 +354,13 @@ def _scenario_struct(scenario, speciation: float):
         c.meta_deme = scenario.meta_deme
         c.migration_probability = scenario.migration
     elif isinstance(scenario, AlmostInfinite):
-        c.kind = ALMOST_INFINITE_NORMAL
-        c.sigma = scenario.dispersal.sigma
+        if isinstance(scenario.dispersal, Clark2Dt):
+            c.kind = ALMOST_INFINITE_CLARK2DT
+            c.shape_u = scenario.dispersal.shape_u
+            c.tail_p = scenario.dispersal.tail_p
+        else:
+            c.kind = ALMOST_INFINITE_NORMAL
+            c.sigma = scenario.dispersal.sigma
         c.centre_x, c.centre_y = scenario.sample.centre
         c.radius = scenario.sample.radius
     elif isinstance(scenario, SpatiallyExplicit):

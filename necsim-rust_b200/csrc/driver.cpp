@@ -11,7 +11,7 @@
 // Supported: speciation; sample (percentage, origin Habitat | List,
 // mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
 // which writes the configuration that resumes the run; rng Seed | Entropy;
-// the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle, Normal) and
+// the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle; Normal or Clark2Dt) and
 // SpatiallyExplicit (habitat and dispersal as .npy arrays, Uniform turnover,
 // Strict maps) scenarios; algorithm Independent(...) or CUDA(...) with
 // Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
@@ -151,8 +151,9 @@ void parse_scenario(const Value &s, Run &r) {
         const Value &sample = need(s, "sample");
         const Value &disp = need(s, "dispersal");
         if (sample.variant() != "Circle") fail("AlmostInfinite: only the Circle sample is supported");
-        if (disp.variant() != "Normal") fail("AlmostInfinite: only Normal dispersal is supported");
-        sc.kind = NECSIM_ALMOST_INFINITE_NORMAL;
+        if (disp.variant() != "Normal" && disp.variant() != "Clark2Dt")
+            fail("AlmostInfinite: dispersal must be Normal or Clark2Dt");
+        sc.kind = disp.variant() == "Normal" ? NECSIM_ALMOST_INFINITE_NORMAL : NECSIM_ALMOST_INFINITE_CLARK2DT;
         // almost_infinite/mod.rs:103-107: the default centre
         sc.centre_x = sc.centre_y = 0x7fffffffu;
         if (const Value *c = sample.field("centre")) {
@@ -162,9 +163,16 @@ void parse_scenario(const Value &s, Run &r) {
         const uint64_t radius = need(sample, "radius").as_u64();
         if (radius > 0xffff) fail("AlmostInfinite: the radius is a u16");
         sc.radius = (uint32_t)radius;
-        sc.sigma = need(disp, "sigma").as_f64();
         o << "AlmostInfinite(Circle(centre: (" << sc.centre_x << ", " << sc.centre_y << "), radius: " << radius
-          << "), Normal(sigma: " << sc.sigma << "))";
+          << "), ";
+        if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL) {
+            sc.sigma = need(disp, "sigma").as_f64();
+            o << "Normal(sigma: " << sc.sigma << "))";
+        } else {
+            sc.shape_u = need(disp, "shape_u").as_f64();
+            sc.tail_p = need(disp, "tail_p").as_f64();
+            o << "Clark2Dt(shape_u: " << sc.shape_u << ", tail_p: " << sc.tail_p << "))";
+        }
     } else if (k == "SpatiallyExplicit") {
         const Value &hab = need(s, "habitat"), &disp = need(s, "dispersal");
         if (const Value *t = s.field("turnover")) {

@@ -119,6 +119,11 @@ void validate(const necsim_scenario &sc) {
         if (!(sc.sigma >= 0.0) || !std::isfinite(sc.sigma)) fail(NECSIM_E_INVALID_ARGUMENT, "sigma must be >= 0");
         if (sc.radius > 65535) fail(NECSIM_E_INVALID_ARGUMENT, "circle radius is a u16");
         break;
+    case NECSIM_ALMOST_INFINITE_CLARK2DT:
+        if (!(sc.shape_u > 0.0) || !std::isfinite(sc.shape_u) || !(sc.tail_p > 0.0) || !std::isfinite(sc.tail_p))
+            fail(NECSIM_E_INVALID_ARGUMENT, "Clark2Dt shape_u and tail_p must be positive");
+        if (sc.radius > 65535) fail(NECSIM_E_INVALID_ARGUMENT, "circle radius is a u16");
+        break;
     case NECSIM_SPATIALLY_EXPLICIT:
         if (!sc.width || !sc.height || !sc.habitat || !sc.dispersal)
             fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyExplicit needs habitat and dispersal maps");
@@ -134,7 +139,8 @@ uint64_t count_origins(const necsim_scenario &sc) {
     case NECSIM_NON_SPATIAL:
     case NECSIM_SPATIALLY_IMPLICIT:
         return (uint64_t)sc.width * sc.height * sc.deme;
-    case NECSIM_ALMOST_INFINITE_NORMAL: {
+    case NECSIM_ALMOST_INFINITE_NORMAL:
+    case NECSIM_ALMOST_INFINITE_CLARK2DT: {
         const int64_t r = sc.radius;
         uint64_t n = 0;
         for (int64_t dy = -r; dy <= r; ++dy)
@@ -211,6 +217,13 @@ SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64
     p.migration_threshold = (uint64_t)std::ceil(std::ldexp(sc.migration_probability, 53));
     p.width_magic = division_magic(p.width);
     p.meta_width_magic = division_magic(p.meta_width);
+    if (sc.kind == NECSIM_ALMOST_INFINITE_CLARK2DT) {
+        // clark2dt::cdf_inverse divides 1.0 / tail_p per draw: the same IEEE
+        // quotient, once
+        p.clark = 1;
+        p.clark_shape_u = sc.shape_u;
+        p.clark_exponent = 1.0 / sc.tail_p;
+    }
     p.pause_before = -1.0;
     return p;
 }
@@ -506,7 +519,7 @@ void for_each_origin(const necsim_scenario &sc, F &&push) {
         for (uint32_t yy = 0; yy < sc.height; ++yy)
             for (uint32_t xx = 0; xx < sc.width; ++xx)
                 for (uint32_t ii = 0; ii < sc.deme; ++ii) push(xx, yy, ii, g++);
-    } else if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL) {
+    } else if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL || sc.kind == NECSIM_ALMOST_INFINITE_CLARK2DT) {
         // origin_sampler/singleton_demes/circle.rs:36-70, 100-140
         const uint32_t r = sc.radius;
         const uint64_t d = (uint64_t)r * 2 + 1;
@@ -1255,9 +1268,11 @@ void run_simulations(Engine &E, std::vector<SimHost> sims, const necsim_args &ar
 void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &args,
                     const std::vector<std::vector<necsim_lineage>> *given,
                     const std::vector<SimParams> *prebuilt_tables) {
-    E.kind = sims.front().sc.kind;
+    // the device runs Clark2Dt as AlmostInfinite with its dispersal switch
+    auto device_kind = [](int32_t k) { return k == NECSIM_ALMOST_INFINITE_CLARK2DT ? NECSIM_ALMOST_INFINITE_NORMAL : k; };
+    E.kind = device_kind(sims.front().sc.kind);
     for (auto &s : sims)
-        if (s.sc.kind != E.kind) fail(NECSIM_E_UNSUPPORTED, "a batch must share one scenario kind");
+        if (device_kind(s.sc.kind) != E.kind) fail(NECSIM_E_UNSUPPORTED, "a batch must share one scenario kind");
     if (args.schedule > 1) fail(NECSIM_E_INVALID_ARGUMENT, "schedule must be 0 (plain) or 1 (learned)");
     E.learned = args.schedule == 1;
     if (E.learned) {
@@ -1412,6 +1427,7 @@ static int simulate_impl(necsim_ctx *ctx, const necsim_lineage *lineages, uint64
                     break;
                 }
                 case NECSIM_ALMOST_INFINITE_NORMAL:
+                case NECSIM_ALMOST_INFINITE_CLARK2DT:
                     h = 1;
                     break;
                 default:

@@ -211,7 +211,10 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
         ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
     } else if (KIND == kAlmostInfiniteNormal) {
         // sample e4 is CoalescenceRngSample::new's draw; singleton demes -> index 0
-        normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
+        if (p.clark)
+            clark2dt_dispersal_draw(e2, e3, p.clark_shape_u, p.clark_exponent, l.x, l.y, tx, ty);
+        else
+            normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
         ti = 0;
     } else {
         uint64_t d_coal;

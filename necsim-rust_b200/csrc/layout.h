@@ -87,6 +87,12 @@ struct alignas(16) SimParams {
     const AliasAtom *atoms;   // SE
     const float *cell_entropy;  // SE: per-cell dispersal entropy (learned-model feature), nullable
     uint64_t pad2;
+    // AlmostInfinite with Clark2Dt dispersal (clark != 0): shape u and the
+    // exponent 1 / p (almost_infinite_clark2dt.rs, clark2dt::cdf_inverse)
+    double clark_shape_u;
+    double clark_exponent;
+    uint32_t clark;
+    uint32_t pad3[3];
     uint64_t n_cells;
     uint64_t n_atoms;
     uint64_t step_slice;

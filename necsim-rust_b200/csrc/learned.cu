@@ -54,8 +54,10 @@ __device__ void lineage_features(int kind, const SimParams &p, const SimCounters
             ent = logf((float)p.meta_width * (float)p.meta_height);
         }
     } else if (kind == kAlmostInfiniteNormal) {
-        // differential entropy of the 2D normal dispersal kernel
-        ent = logf(2.0f * 3.14159265f * 2.71828183f * (float)p.sigma * (float)p.sigma);
+        // differential entropy of the 2D dispersal kernel: normal, or a
+        // Clark2Dt kernel of scale sqrt(u) (sigma 0: none)
+        const float scale2 = p.clark ? (float)p.clark_shape_u : (float)p.sigma * (float)p.sigma;
+        ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2, 1.0f));
     } else {
         fx = (float)x / (float)p.width;
         fy = (float)y / (float)p.height;

@@ -127,4 +127,7 @@ def to_scenario(desc):
     if k == 2:
         return nb.AlmostInfinite(nb.Circle(desc["radius"], (desc["centre_x"], desc["centre_y"])),
                                  nb.Normal(desc["sigma"]))
+    if k == 4:
+        return nb.AlmostInfinite(nb.Circle(desc["radius"], (desc["centre_x"], desc["centre_y"])),
+                                 nb.Clark2Dt(desc["shape_u"], desc["tail_p"]))
     return nb.SpatiallyExplicit(desc["habitat"], desc["dispersal"], desc.get("turnover_rate", 0.5))

@@ -188,6 +188,8 @@ typedef struct sim_t {
     double p0;          /* exp(-lambda * delta_t) (poisson.rs:42) */
     double migration;
     double sigma;
+    int clark;          /* AlmostInfinite with Clark2Dt dispersal */
+    double shape_u, tail_p;
     extent_t local;     /* NonSpatial / SI local / SE map extent */
     uint32_t deme;
     extent_t meta;      /* SI meta */
@@ -341,6 +343,28 @@ static inline void normal_disperse_from_draws(uint64_t d0, uint64_t d1, double s
     clamp_round_dispersal(x, y, dx, dy, tx, ty);
 }
 
+/* almost_infinite_clark2dt.rs:96-107 with clark2dt::cdf_inverse and
+ * pow_fast_one (:167-189): jump = sqrt(u * (pow(1 / (1 - u01), 1 / p) - 1)),
+ * theta = u2 * 2 * pi, (dx, dy) = (cos(theta) * jump, sin(theta) * jump) */
+static inline void clark2dt_disperse_from_draws(uint64_t d0, uint64_t d1, double shape_u, double tail_p,
+                                                uint32_t x, uint32_t y, uint32_t *tx, uint32_t *ty) {
+    double u01 = (double)(d0 >> 11) * 0x1.0p-53;
+    double u2 = (double)((d1 >> 11) + 1) * 0x1.0p-53;
+    double expo = 1.0 / tail_p;
+    double base = 1.0 / (1.0 - u01);
+    double powed = (expo == 1.0) ? base : pow(base, expo);
+    double jump = sqrt(shape_u * (powed - 1.0));
+    double theta = u2 * 2.0 * 3.141592653589793;
+    double dx = cos(theta) * jump;
+    double dy = sin(theta) * jump;
+    clamp_round_dispersal(x, y, dx, dy, tx, ty);
+}
+
+void oracle_clark2dt_dispersal(uint64_t draw0, uint64_t draw1, double shape_u, double tail_p, uint32_t x,
+                               uint32_t y, uint32_t *tx, uint32_t *ty) {
+    clark2dt_disperse_from_draws(draw0, draw1, shape_u, tail_p, x, y, tx, ty);
+}
+
 void oracle_normal_dispersal(uint64_t draw0, uint64_t draw1, double sigma, uint32_t x, uint32_t y,
                              uint32_t *tx, uint32_t *ty) {
     normal_disperse_from_draws(draw0, draw1, sigma, x, y, tx, ty);
@@ -395,7 +419,10 @@ static inline void disperse(sim_t *s, uint32_t x, uint32_t y, uint32_t *tx, uint
     case ORACLE_ALMOST_INFINITE_NORMAL: {
         uint64_t d0 = rng_sample_u64(g);
         uint64_t d1 = rng_sample_u64(g);
-        normal_disperse_from_draws(d0, d1, s->sigma, x, y, tx, ty);
+        if (s->clark)
+            clark2dt_disperse_from_draws(d0, d1, s->shape_u, s->tail_p, x, y, tx, ty);
+        else
+            normal_disperse_from_draws(d0, d1, s->sigma, x, y, tx, ty);
         break;
     }
     default:
@@ -633,6 +660,14 @@ static int sim_init(sim_t *s, const oracle_scenario *sc, const oracle_args *args
     s->p0 = exp(-s->lambda_dt);
     s->migration = sc->migration_probability;
     s->sigma = sc->sigma;
+    if (sc->kind == ORACLE_ALMOST_INFINITE_CLARK2DT) {
+        /* the same habitat, origins and coalescence as AlmostInfinite Normal */
+        s->kind = ORACLE_ALMOST_INFINITE_NORMAL;
+        s->clark = 1;
+        s->shape_u = sc->shape_u;
+        s->tail_p = sc->tail_p;
+        if (!(sc->shape_u > 0.0) || !(sc->tail_p > 0.0)) return -2;
+    }
     s->rng.seed = oracle_seed_from_u64(seed);
     s->rng.state = s->rng.seed;
     if (!(s->lambda > 0.0) || !(s->delta_t > 0.0)) return -2;
@@ -654,6 +689,7 @@ static int sim_init(sim_t *s, const oracle_scenario *sc, const oracle_args *args
         s->meta_deme = sc->meta_deme;
         break;
     case ORACLE_ALMOST_INFINITE_NORMAL:
+    case ORACLE_ALMOST_INFINITE_CLARK2DT:
         s->local = (extent_t){0, 0, 1ULL << 32, 1ULL << 32};
         break;
     case ORACLE_SPATIALLY_EXPLICIT: {
@@ -717,7 +753,8 @@ static int64_t enumerate_origins(const oracle_scenario *sc, const sim_t *s, line
                     n++;
                 }
         break;
-    case ORACLE_ALMOST_INFINITE_NORMAL: {
+    case ORACLE_ALMOST_INFINITE_NORMAL:
+    case ORACLE_ALMOST_INFINITE_CLARK2DT: {
         /* singleton_demes/circle.rs:36-70, 100-140 */
         uint32_t r = sc->radius;
         uint64_t d = (uint64_t)r * 2 + 1;

@@ -30,6 +30,7 @@ enum {
     ORACLE_SPATIALLY_IMPLICIT = 1,
     ORACLE_ALMOST_INFINITE_NORMAL = 2,
     ORACLE_SPATIALLY_EXPLICIT = 3,
+    ORACLE_ALMOST_INFINITE_CLARK2DT = 4,
 };
 
 /* Scenario description (same layout as the product's necsim_scenario). */
@@ -45,6 +46,7 @@ typedef struct oracle_scenario {
     uint32_t centre_x, centre_y, radius, reserved1;
     const uint32_t *habitat;                  /* SE: width*height row-major */
     const double *dispersal;                  /* SE: (w*h) x (w*h) row-major */
+    double shape_u, tail_p;                   /* AlmostInfinite Clark2Dt dispersal */
 } oracle_scenario;
 
 enum { ORACLE_MODE_REFERENCE = 0, ORACLE_MODE_CANONICAL = 1 };
@@ -150,6 +152,9 @@ void oracle_free_alias(oracle_alias_tables *t);
 int oracle_check_dispersal_contract(const oracle_scenario *sc);
 
 /* Box-Muller + clamp_round_dispersal for given raw u64 draws (AlmostInfinite). */
+/* Clark2Dt cdf_inverse + clamp_round_dispersal for given raw u64 draws. */
+void oracle_clark2dt_dispersal(uint64_t draw0, uint64_t draw1, double shape_u, double tail_p, uint32_t x,
+                               uint32_t y, uint32_t *tx, uint32_t *ty);
 void oracle_normal_dispersal(uint64_t draw0, uint64_t draw1, double sigma, uint32_t x, uint32_t y,
                              uint32_t *tx, uint32_t *ty);
 

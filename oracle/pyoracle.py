@@ -15,6 +15,7 @@ _LIB_PATH = os.path.join(_HERE, "libnecsim_oracle.so")
 NON_SPATIAL = 0
 SPATIALLY_IMPLICIT = 1
 ALMOST_INFINITE_NORMAL = 2
+ALMOST_INFINITE_CLARK2DT = 4
 SPATIALLY_EXPLICIT = 3
 
 MODE_REFERENCE = 0
@@ -41,6 +42,8 @@ class OracleScenario(ctypes.Structure):
         ("reserved1", ctypes.c_uint32),
         ("habitat", ctypes.POINTER(ctypes.c_uint32)),
         ("dispersal", ctypes.POINTER(ctypes.c_double)),
+        ("shape_u", ctypes.c_double),
+        ("tail_p", ctypes.c_double),
     ]
 
 
@@ -158,6 +161,10 @@ def lib():
                                               ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                               ctypes.POINTER(ctypes.c_uint32)]
         L.oracle_normal_dispersal.restype = None
+        L.oracle_clark2dt_dispersal.argtypes = [u64, u64, ctypes.c_double, ctypes.c_double, ctypes.c_uint32,
+                                                ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                                ctypes.POINTER(ctypes.c_uint32)]
+        L.oracle_clark2dt_dispersal.restype = None
         _lib = L
     return _lib
 
@@ -181,6 +188,8 @@ def make_scenario(desc):
     sc.centre_x = desc.get("centre_x", 0)
     sc.centre_y = desc.get("centre_y", 0)
     sc.radius = desc.get("radius", 0)
+    sc.shape_u = desc.get("shape_u", 0.0)
+    sc.tail_p = desc.get("tail_p", 0.0)
     keep = []
     if desc.get("habitat") is not None:
         h = np.ascontiguousarray(desc["habitat"], dtype=np.uint32)
@@ -331,3 +340,9 @@ def distinct_speciation_set(events):
     k = np.stack([events["event_time"].view(np.uint64), events["x"].astype(np.uint64),
                   events["y"].astype(np.uint64), events["index"].astype(np.uint64)], axis=1)
     return np.unique(k, axis=0)
+
+
+def clark2dt_dispersal(d0, d1, shape_u, tail_p, x, y):
+    tx, ty = ctypes.c_uint32(), ctypes.c_uint32()
+    lib().oracle_clark2dt_dispersal(d0, d1, shape_u, tail_p, x, y, ctypes.byref(tx), ctypes.byref(ty))
+    return tx.value, ty.value

@@ -81,6 +81,10 @@ CASES = {
                      centre_y=0xFFFFFFFF - 1), 8),
     "ai_sigma0": (dict(kind=2, speciation_probability=0.01, sigma=0.0, radius=5, centre_x=100,
                        centre_y=100), 9),
+    "ai_clark": (dict(kind=4, speciation_probability=1e-3, shape_u=4.0, tail_p=0.5, radius=25,
+                      centre_x=0xFFFFFFFF // 2, centre_y=0xFFFFFFFF // 2), 10),
+    "ai_clark_p1": (dict(kind=4, speciation_probability=2e-3, shape_u=1.0, tail_p=1.0, radius=12, centre_x=3,
+                         centre_y=0xFFFFFFFF - 2), 11),
 }
 
 

@@ -79,3 +79,31 @@ def test_nonspatial_origin_order(oracle):
     assert list(o["gref"]) == list(range(12))
     assert list(zip(o["x"], o["y"], o["index"]))[:5] == [(0, 0, 0), (0, 0, 1), (1, 0, 0),
                                                          (1, 0, 1), (2, 0, 0)]
+
+
+def _clark2dt_restated(d0, d1, shape_u, tail_p, x, y):
+    """almost_infinite_clark2dt.rs:96-107, clark2dt::cdf_inverse / pow_fast_one
+    (:167-189) and almost_infinite.rs:100-114, restated in Python."""
+    import math
+    u01 = (d0 >> 11) * 2.0 ** -53
+    u2 = ((d1 >> 11) + 1) * 2.0 ** -53
+    expo = 1.0 / tail_p
+    base = 1.0 / (1.0 - u01)
+    jump = math.sqrt(shape_u * ((base if expo == 1.0 else math.pow(base, expo)) - 1.0))
+    theta = u2 * 2.0 * math.pi
+    dx, dy = math.cos(theta) * jump, math.sin(theta) * jump
+
+    def rnd(v):  # f64::round: half away from zero
+        return int(math.floor(abs(v) + 0.5)) * (1 if v >= 0 else -1)
+    return (x + rnd(dx)) % (1 << 32), (y + rnd(dy)) % (1 << 32)
+
+
+def test_clark2dt_dispersal_matches_restatement(oracle):
+    import random
+    rng = random.Random(5)
+    for shape_u, tail_p in [(4.0, 0.5), (1.0, 1.0), (0.3, 2.5), (25.0, 0.2)]:
+        for _ in range(2000):
+            d0, d1 = rng.getrandbits(64), rng.getrandbits(64)
+            x, y = rng.getrandbits(32), rng.getrandbits(32)
+            assert oracle.clark2dt_dispersal(d0, d1, shape_u, tail_p, x, y) == \
+                _clark2dt_restated(d0, d1, shape_u, tail_p, x, y)
