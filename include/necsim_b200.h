@@ -313,6 +313,22 @@ int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *ou
 int necsim_presample_origins(uint64_t n, double percentage, uint32_t rank, uint32_t size, uint64_t *out,
                              uint64_t cap, uint64_t *n_out);
 
+/* ---- event log ----
+ * The reference's on-disk event log (EventLogRecorder,
+ * necsim/impls/std/src/event_log/recorder.rs): a reporter that buffers
+ * events as PackedEvents and writes segments of `segment_capacity` events,
+ * each sorted by PackedEvent::cmp, as files 0, 1, ... of `directory` in
+ * bincode 1.3 encoding (a 26-byte EventLogHeader, then 56-byte PackedEvents;
+ * dispersal events carry LineageInteraction::Maybe, as the Independent
+ * algorithm reports them), readable by the reference's replay.  `directory`
+ * must not exist (its parents are created).  Pass the reporter to any
+ * simulate call; close to write the last segment. */
+typedef struct necsim_event_log necsim_event_log;
+int necsim_event_log_create(const char *directory, uint64_t segment_capacity, int32_t record_speciation,
+                            int32_t record_dispersal, necsim_event_log **out);
+necsim_reporter necsim_event_log_reporter(necsim_event_log *log);
+int necsim_event_log_close(necsim_event_log *log);
+
 /* ---- launch autotuner ----
  * Times a bounded sample of a batch -- every k-th simulation so that the
  * sample holds at most `max_sample_lineages` origins, each paused at

@@ -118,7 +118,8 @@ SYMBOLS = [
     "necsim_model_create", "necsim_model_destroy", "necsim_model_last_error",
     "necsim_model_get_weights", "necsim_model_set_weights", "necsim_model_predict",
     "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
-    "necsim_presample_origins", "necsim_gpu_autotune",
+    "necsim_presample_origins", "necsim_gpu_autotune", "necsim_event_log_create",
+    "necsim_event_log_reporter", "necsim_event_log_close",
 ]
 
 _lib = None
@@ -174,6 +175,12 @@ def lib():
                                       P(CArgs), vp, ctypes.c_uint32, P(ctypes.c_uint32), ctypes.c_char_p,
                                       ctypes.c_size_t]
     L.necsim_gpu_autotune.restype = ctypes.c_int
+    L.necsim_event_log_create.argtypes = [ctypes.c_char_p, u64, ctypes.c_int32, ctypes.c_int32, P(vp)]
+    L.necsim_event_log_create.restype = ctypes.c_int
+    L.necsim_event_log_reporter.argtypes = [vp]
+    L.necsim_event_log_reporter.restype = CReporter
+    L.necsim_event_log_close.argtypes = [vp]
+    L.necsim_event_log_close.restype = ctypes.c_int
     L.necsim_presample_origins.argtypes = [u64, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint32, vp, u64, P(u64)]
     L.necsim_presample_origins.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
@@ -502,14 +509,15 @@ class Simulation:
         return out[:n.value]
 
     def simulate(self, seed: int, pause_before: Optional[float] = None, collect: bool = True,
-                 wyhash_seed: Optional[int] = None) -> Outcome:
+                 wyhash_seed: Optional[int] = None, event_log: Optional["EventLog"] = None) -> Outcome:
         """Simulates every origin lineage; `seed` is the RON `rng: Seed(seed)`."""
         L = lib()
         ws = seed_from_u64(seed) if wyhash_seed is None else wyhash_seed
-        col = _Collector() if collect else None
+        col = _Collector() if collect and event_log is None else None
         out = COutcome()
         pb = -1.0 if pause_before is None else float(pause_before)
-        rc = L.necsim_gpu_simulate(self._ctx, ws, pb, ctypes.byref(col.struct) if col else None,
+        rep = event_log.reporter if event_log is not None else (col.struct if col else None)
+        rc = L.necsim_gpu_simulate(self._ctx, ws, pb, ctypes.byref(rep) if rep is not None else None,
                                    ctypes.byref(out))
         self._check(rc)
         return _outcome(out, col.events() if col else None,
@@ -834,3 +842,78 @@ def autotune(scenarios: Sequence, speciations: Sequence[float], seeds: Sequence[
     tuned = CUDA(**{**base.__dict__, "block_size": best.block_size, "step_slice": best.step_slice,
                     "dedup_factor_pct": best.dedup_factor_pct})
     return tuned, res[:got.value].copy()
+
+
+# ---------------------------------------------------------------------------
+# Event log (event_log/recorder.rs format)
+# ---------------------------------------------------------------------------
+EVENT_LOG_HEADER_DTYPE = np.dtype([("min_time", "<f8"), ("max_time", "<f8"), ("length", "<u8"),
+                                   ("with_speciation", "u1"), ("with_dispersal", "u1")])
+PACKED_EVENT_DTYPE = np.dtype([("gref", "<u8"), ("prior_time", "<f8"), ("event_time", "<f8"),
+                               ("x", "<u4"), ("y", "<u4"), ("index", "<u4"),
+                               ("tx", "<u4"), ("ty", "<u4"), ("tindex", "<u4"), ("coalescence", "<u8")])
+
+
+class EventLog:
+    """An on-disk event log in the reference's format (EventLogRecorder,
+    necsim/impls/std/src/event_log/recorder.rs): pass it to
+    `Simulation.simulate(..., event_log=log)`; close() writes the last
+    segment.  `directory` must not exist yet."""
+
+    def __init__(self, directory: str, capacity: int = 1_000_000, speciation: bool = True,
+                 dispersal: bool = False):
+        L = lib()
+        h = ctypes.c_void_p()
+        rc = L.necsim_event_log_create(os.fsencode(directory), capacity, int(speciation), int(dispersal),
+                                       ctypes.byref(h))
+        if rc != 0:
+            raise NecsimError(rc, "cannot create the event log %s (it must not exist yet)" % directory)
+        self._h = h
+        self.directory = directory
+        self.reporter = L.necsim_event_log_reporter(h)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            rc = lib().necsim_event_log_close(self._h)
+            self._h = ctypes.c_void_p()
+            if rc != 0:
+                raise NecsimError(rc, "could not write the last event log segment")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def read_event_log(directory: str):
+    """Reads an event log directory like the reference's replay
+    (event_log/replay/segment.rs, sorted_segments.rs): (headers, events) with
+    the events of all segments merged in PackedEvent order and decoded:
+    `kind` 0 speciation (prior time negative, event time positive), 1
+    dispersal without coalescence, 2 dispersal maybe coalescing, 3 dispersal
+    with coalescence (event.rs:105-160); times are returned positive."""
+    headers, parts = [], []
+    names = sorted((n for n in os.listdir(directory) if n.isdigit()), key=int)
+    for n in names:
+        raw = open(os.path.join(directory, n), "rb").read()
+        h = np.frombuffer(raw[:26], dtype=EVENT_LOG_HEADER_DTYPE)[0]
+        ev = np.frombuffer(raw[26:], dtype=PACKED_EVENT_DTYPE)
+        if len(ev) != int(h["length"]):
+            raise ValueError("segment %s: header length %d, %d events" % (n, h["length"], len(ev)))
+        headers.append(h)
+        parts.append(ev)
+    ev = np.concatenate(parts) if parts else np.zeros(0, dtype=PACKED_EVENT_DTYPE)
+    prior_neg = (ev["prior_time"].view(np.uint64) >> np.uint64(63)).astype(bool)
+    event_neg = (ev["event_time"].view(np.uint64) >> np.uint64(63)).astype(bool)
+    kind = np.where(prior_neg & ~event_neg, 0, np.where(prior_neg & event_neg, 1,
+                    np.where(~prior_neg & event_neg, 2, 3))).astype(np.uint8)
+    out = np.zeros(len(ev), dtype=PACKED_EVENT_DTYPE.descr + [("kind", "u1")])
+    for f in PACKED_EVENT_DTYPE.names:
+        out[f] = ev[f]
+    out["prior_time"] = np.abs(ev["prior_time"])
+    out["event_time"] = np.abs(ev["event_time"])
+    out["kind"] = kind
+    order = np.lexsort((out["gref"], out["prior_time"].view(np.uint64), out["tindex"], out["ty"], out["tx"],
+                        out["index"], out["y"], out["x"], out["event_time"].view(np.uint64)))
+    return headers, out[order]

@@ -16,7 +16,7 @@ DRIVER = os.path.join(LIB_DIR, "necsim-b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels.cu", "noalloc.cu", "learned.cu"]
-CPP_SOURCES = ["host.cpp", "tables.cpp"]
+CPP_SOURCES = ["host.cpp", "tables.cpp", "event_log.cpp"]
 DRIVER_SOURCES = ["driver.cpp", "ron.cpp"]
 
 

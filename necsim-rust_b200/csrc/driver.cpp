@@ -15,7 +15,8 @@
 // SpatiallyExplicit (habitat and dispersal as .npy arrays, Uniform turnover,
 // Strict maps) scenarios; algorithm Independent(...) or CUDA(...) with
 // Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
-// Counter, Execution (others are ignored with a notice).
+// Counter, Execution (others are ignored with a notice); log EventLog(directory,
+// capacity) writes the reference's event log.
 #include <chrono>
 #include <cinttypes>
 #include <cmath>
@@ -115,6 +116,8 @@ struct Run {
     double pause_before = -1.0;
     std::string pause_config;
     bool rep_biodiversity = false, rep_counter = false, rep_execution = false;
+    std::string log_directory;  // log: EventLog(directory, capacity)
+    uint64_t log_capacity = 1000000;
     std::vector<uint32_t> habitat;
     std::vector<double> dispersal;
     std::string summary;
@@ -267,6 +270,15 @@ Run parse_config(const std::string &text) {
             fail("pause must be None or Pause(...)");
         }
     }
+    if (const Value *lg = root.field("log")) {
+        if (lg->variant() == "EventLog") {
+            r.log_directory = need(*lg, "directory").text;
+            if (const Value *c = lg->field("capacity")) r.log_capacity = c->as_u64();
+            if (r.log_capacity == 0) fail("log capacity must be positive");
+        } else if (lg->variant() != "None") {
+            fail("log must be None or EventLog(...)");
+        }
+    }
     if (const Value *g = root.field("rng")) {
         if (g->variant() == "Seed" && g->items.size() == 1)
             r.seed = g->items[0].as_u64();
@@ -376,12 +388,18 @@ std::string resume_config(const std::string &text, uint64_t seed, const std::vec
 
 struct Counts {
     uint64_t speciation = 0, self_dispersal = 0, out_dispersal = 0;
+    necsim_reporter log{};  // the event log's reporter, when one is written
 };
 
-int on_speciation(void *, const necsim_speciation_event *, uint64_t) { return 0; }
+int on_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
+    Counts &c = *static_cast<Counts *>(user);
+    if (c.log.report_speciation) return c.log.report_speciation(c.log.user, ev, n);
+    return 0;
+}
 
 int on_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     Counts &c = *static_cast<Counts *>(user);
+    if (c.log.report_dispersal && c.log.report_dispersal(c.log.user, ev, n) != 0) return 1;
     for (uint64_t i = 0; i < n; ++i) {
         if (ev[i].x == ev[i].target_x && ev[i].y == ev[i].target_y)
             c.self_dispersal += 1;
@@ -441,6 +459,15 @@ int simulate(const std::string &path, bool run) {
         fail("set-up failed (status " + std::to_string(rc) + "): " + m);
     }
     Counts counts;
+    necsim_event_log *log = nullptr;
+    if (!r.log_directory.empty()) {
+        rc = necsim_event_log_create(r.log_directory.c_str(), r.log_capacity, 1, r.args.report_dispersal, &log);
+        if (rc) {
+            necsim_gpu_destroy(ctx);
+            fail("cannot create the event log " + r.log_directory + " (start from a clean log directory)");
+        }
+        counts.log = necsim_event_log_reporter(log);
+    }
     necsim_reporter rep{&counts, on_speciation, on_dispersal};
     necsim_outcome out{};
     const auto t1 = std::chrono::steady_clock::now();
@@ -460,6 +487,8 @@ int simulate(const std::string &path, bool run) {
         if (rc) fail("could not read the remaining lineages");
     }
     necsim_gpu_destroy(ctx);
+    if (log && necsim_event_log_close(log) != 0) fail("could not write the event log");
+    if (log) std::printf("necsim-b200: events logged to %s\n", r.log_directory.c_str());
     const auto t3 = std::chrono::steady_clock::now();
 
     std::printf("necsim-b200: %s after %" PRIu64 " steps at time %.17g\n", out.paused ? "paused" : "done",

@@ -131,3 +131,16 @@ def test_driver_pause_writes_a_resumable_config(nb, tmp_path):
     assert "(resumed)" in r2.stdout and "done" in r2.stdout
     straight = nb.simulate(0.01, nb.NonSpatial((30, 20), 2), 42)
     assert first + species(r2.stdout) == straight.biodiversity
+
+
+@pytest.mark.gpu
+def test_driver_writes_an_event_log(nb, tmp_path):
+    logdir = tmp_path / "events"
+    cfg = CONFIG.replace("pause: None,", 'pause: None,\n    log: EventLog(directory: "%s", capacity: 5000),' % logdir)
+    r = run_driver(nb, "simulate", cfg, tmp_path, "l.ron")
+    assert r.returncode == 0, r.stderr
+    headers, ev = nb.read_event_log(str(logdir))
+    n_spec = int((ev["kind"] == 0).sum())
+    assert n_spec > 0 and int((ev["kind"] == 2).sum()) > 0  # Counter() turns on dispersal events
+    assert len({(int(e["x"]), int(e["y"]), int(e["index"]), float(e["event_time"]))
+                for e in ev[ev["kind"] == 0]}) == species(r.stdout)
