@@ -70,6 +70,12 @@ typedef struct necsim_scenario {
                                         Circle sample fields as for Normal */
 } necsim_scenario;
 
+/* necsim_args.event_time_sampler: which EventTimeSampler
+ * (necsim/impls/no-std/src/cogs/active_lineage_sampler/independent/event_time_sampler/)
+ * draws each lineage's next event time */
+#define NECSIM_SAMPLER_POISSON 0u /* poisson.rs, the Independent algorithm's (launch.rs:86) */
+#define NECSIM_SAMPLER_EXP 1u     /* exp.rs, the CUDA algorithm's (cuda/src/launch.rs:121) */
+
 /* Replaces `CudaArguments` / `IndependentArguments`
  * (rustcoalescence/algorithms/cuda/src/arguments.rs:61-138,
  *  rustcoalescence/algorithms/independent/src/arguments.rs:79-146).
@@ -98,7 +104,11 @@ typedef struct necsim_args {
                                   in the global rounds, whose sparse rounds step each lineage with
                                   a whole warp (faster on every measured workload); same results
                                   either way; a run of one simulation always stays global */
-    uint32_t reserved_args;
+    uint32_t event_time_sampler; /* NECSIM_SAMPLER_POISSON (0, default): PoissonEventTimeSampler,
+                                    the Independent algorithm's (event_time_sampler/poisson.rs);
+                                    NECSIM_SAMPLER_EXP (1): ExpEventTimeSampler, the CUDA
+                                    algorithm's (event_time_sampler/exp.rs), -ln(U(0,1]) / lambda
+                                    per event with a correctly rounded f64 ln */
     struct necsim_model *model; /* schedule == 1: the lifetime model ordering the step queue
                                    (must stay alive during the call; same device) */
 } necsim_args;

@@ -66,7 +66,7 @@ class CArgs(ctypes.Structure):
         ("grid_size", ctypes.c_uint32), ("dedup_factor_pct", ctypes.c_uint32),
         ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
-        ("resident", ctypes.c_uint32), ("reserved_args", ctypes.c_uint32),
+        ("resident", ctypes.c_uint32), ("event_time_sampler", ctypes.c_uint32),
         ("model", ctypes.c_void_p),
     ]
 
@@ -289,9 +289,15 @@ class CUDA:
     # reporters consume dispersal events (ReportDispersal): the events leave
     # the device after every round (global rounds only, no CUDA graphs)
     report_dispersal: bool = False
+    # "poisson": PoissonEventTimeSampler, the Independent algorithm's
+    # (event_time_sampler/poisson.rs); "exp": ExpEventTimeSampler, the CUDA
+    # algorithm's (event_time_sampler/exp.rs), -ln(U(0,1]) / lambda per event
+    event_time_sampler: str = "poisson"
 
 
 Independent = CUDA
+
+EVENT_TIME_SAMPLERS = {"poisson": 0, "exp": 1}
 
 
 @dataclass
@@ -407,6 +413,9 @@ def _args_struct(algorithm: CUDA):
     a.device = algorithm.device
     a.rounds_per_graph = algorithm.rounds_per_graph
     a.resident = 1 if algorithm.resident else 0
+    if algorithm.event_time_sampler not in EVENT_TIME_SAMPLERS:
+        raise ValueError("event_time_sampler must be 'poisson' or 'exp'")
+    a.event_time_sampler = EVENT_TIME_SAMPLERS[algorithm.event_time_sampler]
     return a
 
 

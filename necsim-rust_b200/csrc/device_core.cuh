@@ -1,6 +1,6 @@
 // device_core.cuh -- per-lineage arithmetic of the Independent algorithm on
-// sm_100a: WyHash priming/sampling, the Poisson event-time sampler, the
-// speciation test, the four dispersal samplers and the coalescence index.
+// sm_100a: WyHash priming/sampling, the Poisson and exponential event-time
+// samplers, the speciation test, the four dispersal samplers and the coalescence index.
 //
 // Every f64 expression is evaluated as one IEEE-754 round-to-nearest
 // operation per source operator in the reference's order (the file is
@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "layout.h"
+#include "ln_dd.h"
 
 namespace necsim {
 
@@ -269,6 +270,54 @@ __device__ __forceinline__ double poisson_next_event_time_lat(uint64_t loc_term,
         }
         time_step += 2;
     }
+}
+
+// ---- the exponential event-time sampler ----
+
+// rng.rs:163-167 sample_exponential of one sample: -ln(U(0,1]) / lambda,
+// with the logarithm shared bit for bit with the host (ln_dd.h)
+__device__ __forceinline__ double exp_sample(uint64_t d, double lambda) {
+    return __ddiv_rn(-necsim_ln(unit_open_closed(d)), lambda);
+}
+
+// floor(time / delta_t) as u64 (poisson.rs:44, exp.rs:52)
+__device__ __forceinline__ uint64_t time_bucket(const SimParams &p, double time) {
+    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
+    return f64_to_u64(floor(q));
+}
+
+// The loop of ExpEventTimeSampler (event_time_sampler/exp.rs:37-83) from
+// the state after sample j of bucket ts (running event time et, bucket
+// start ts * delta_t when j == 0): sample j + 1 of the bucket primed at ts
+// is draw_at(s0, j + 1) and its sub-index (j + 1) * INV_PHI, and a sum at
+// or past the bucket's end moves to the next bucket.  Returns the first
+// event time after `time` and its re-prime time index ts + j * INV_PHI.
+__device__ __forceinline__ double exp_continue(uint64_t loc_term, double time, const SimParams &p,
+                                               uint64_t ts, uint32_t j, double et, uint64_t &reprime) {
+    uint64_t s0 = primed_state(loc_term, ts);
+    double slice_end = __dmul_rn(__ull2double_rn(ts + 1), p.delta_t);
+    for (;;) {
+        j += 1;
+        et = __dadd_rn(et, exp_sample(draw_at(s0, j), p.lambda));
+        if (et >= slice_end) {
+            ts += 1;
+            j = 0;
+            et = slice_end;
+            slice_end = __dmul_rn(__ull2double_rn(ts + 1), p.delta_t);
+            s0 = primed_state(loc_term, ts);
+        } else if (et > time) {
+            break;
+        }
+    }
+    reprime = ts + kInvPhi * (uint64_t)j;
+    return et;
+}
+
+// exp.rs:37-83 ExpEventTimeSampler::next_event_time_at_indexed_location_weakly_after
+__device__ __forceinline__ double exp_next_event_time(uint64_t loc_term, double time, const SimParams &p,
+                                                      uint64_t &reprime) {
+    const uint64_t ts = time_bucket(p, time);
+    return exp_continue(loc_term, time, p, ts, 0, __dmul_rn(__ull2double_rn(ts), p.delta_t), reprime);
 }
 
 // ---- the samplers fed with pre-drawn samples ----

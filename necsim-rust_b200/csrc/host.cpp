@@ -462,7 +462,7 @@ void choose_launch(Engine &E) {
     if (block > (unsigned)kStepBlockMax) block = kStepBlockMax;
     block = std::max(32u, block / 32 * 32);
     int per_sm = 0;
-    CK(step_kernel_occupancy(E.kind, (int)block, &per_sm));
+    CK(step_kernel_occupancy(E.kind, E.args.event_time_sampler == NECSIM_SAMPLER_EXP, (int)block, &per_sm));
     if (per_sm < 1) per_sm = 1;
     E.step_block = block;
     E.step_grid = E.args.grid_size ? E.args.grid_size : (unsigned)(per_sm * E.n_sms);
@@ -635,6 +635,7 @@ StepArgs make_step_args(Engine &E, DeviceLineages &in) {
     a.steps_total = &E.d_ctl->steps_total;
     a.n_sims = (uint32_t)E.sims.size();
     a.order = E.learned ? E.order : nullptr;
+    a.exp_sampler = E.args.event_time_sampler == NECSIM_SAMPLER_EXP ? 1u : 0u;
     if (E.tracing) {
         a.trace.deaths = E.trace_deaths;
         a.trace.n_deaths = E.trace_counts + 1;
@@ -696,6 +697,7 @@ ResidentArgs make_resident_args(Engine &E, uint32_t budget, const int *stop_flag
     a.visits = &E.d_ctl->visits;
     a.n_resident = &E.d_ctl->n_resident;
     a.stop_flag = stop_flag;
+    a.exp_sampler = E.args.event_time_sampler == NECSIM_SAMPLER_EXP ? 1u : 0u;
     return a;
 }
 
@@ -1274,6 +1276,8 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
     for (auto &s : sims)
         if (device_kind(s.sc.kind) != E.kind) fail(NECSIM_E_UNSUPPORTED, "a batch must share one scenario kind");
     if (args.schedule > 1) fail(NECSIM_E_INVALID_ARGUMENT, "schedule must be 0 (plain) or 1 (learned)");
+    if (args.event_time_sampler > NECSIM_SAMPLER_EXP)
+        fail(NECSIM_E_INVALID_ARGUMENT, "event_time_sampler must be 0 (Poisson) or 1 (Exp)");
     E.learned = args.schedule == 1;
     if (E.learned) {
         if (!args.model) fail(NECSIM_E_INVALID_ARGUMENT, "the learned schedule needs a model");
@@ -1315,7 +1319,10 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
                 upload_tables(E, sh);
             }
         }
-        if (!(sh.params.p0 > 0.0)) fail(NECSIM_E_UNSUPPORTED, "exp(-lambda * delta_t) underflows to 0");
+        // the Poisson sampler's Devroye inversion needs p0 > 0 (the Exp
+        // sampler draws no counts)
+        if (args.event_time_sampler != NECSIM_SAMPLER_EXP && !(sh.params.p0 > 0.0))
+            fail(NECSIM_E_UNSUPPORTED, "exp(-lambda * delta_t) underflows to 0");
     }
     // a single simulation stays in the global rounds, whose sparse rounds
     // step each lineage with a whole warp on any SM (the resident kernel

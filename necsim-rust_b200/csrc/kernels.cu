@@ -256,8 +256,9 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
 // the previous round) and stop if it is at or beyond the horizon; otherwise
 // execute the event.  LAT selects the latency form (two buckets primed at a
 // time, all samples drawn ahead) for lanes whose warp has little else to run;
-// the throughput form draws only what the reference consumes.
-template <int KIND, bool LAT>
+// the throughput form draws only what the reference consumes.  EXP selects
+// the exponential event-time sampler (exp.rs) instead of the Poisson one.
+template <int KIND, bool LAT, bool EXP = false>
 __device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const EventSink &k) {
     const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
     uint64_t rs;  // WyHash state re-primed for the event
@@ -265,8 +266,14 @@ __device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const E
         // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
         // (active_lineage_sampler/independent/sampler.rs:69-116)
         const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
-        const double t = LAT ? poisson_next_event_time_lat(loc_term, before, p, l.reprime, rs)
-                             : poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
+        double t;
+        if (EXP) {
+            t = exp_next_event_time(loc_term, before, p, l.reprime);
+            rs = primed_state(loc_term, l.reprime);
+        } else {
+            t = LAT ? poisson_next_event_time_lat(loc_term, before, p, l.reprime, rs)
+                    : poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
+        }
         l.next = max_after(before, t);
         l.has_next = true;
     } else {
@@ -306,6 +313,56 @@ __device__ __forceinline__ void broadcast_from_lane0(Lane &l) {
 
 constexpr long long kNoEvent = 0x7fffffffffffffffLL;
 
+// The exponential sampler's search (exp.rs:37-83) for a lineage held by all
+// 32 lanes of a warp: lanes 8g..8g+7 evaluate samples 1..8 of bucket
+// base + g (one logarithm per lane, the costly part, all at once), then
+// every lane replays its bucket's running sum in sample order (the
+// reference's rounding order) from the shuffled samples.  The first bucket
+// that is not empty decides; one whose eight samples pass neither `time`
+// nor its end (rare for lambda * delta_t of order one) continues
+// sequentially from its ninth sample.  Every lane returns the same result.
+__device__ __forceinline__ double exp_search_coop(uint64_t loc_term, double time, const SimParams &p,
+                                                  uint64_t &reprime) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned first = lane & ~7u;  // the bucket's first lane
+    uint64_t base = time_bucket(p, time);
+    for (;;) {
+        const uint64_t ts = base + (lane >> 3);
+        const double e = exp_sample(draw_at(primed_state(loc_term, ts), (lane & 7u) + 1u), p.lambda);
+        const double slice_end = __dmul_rn(__ull2double_rn(ts + 1), p.delta_t);
+        double et = __dmul_rn(__ull2double_rn(ts), p.delta_t);
+        int state = 0;  // 0: undecided, 1: event after `time` at sample j, 2: empty
+        uint32_t j = 0;
+#pragma unroll
+        for (unsigned q = 0; q < 8u; ++q) {
+            const double eq = __shfl_sync(kFull, e, (int)(first + q));
+            if (state == 0) {
+                et = __dadd_rn(et, eq);
+                if (et >= slice_end) {
+                    state = 2;
+                } else if (et > time) {
+                    state = 1;
+                    j = q + 1u;
+                }
+            }
+        }
+        const unsigned open = __ballot_sync(kFull, (lane & 7u) == 0u && state != 2);
+        if (open) {
+            const int leader = __ffs(open) - 1;
+            const int st = __shfl_sync(kFull, state, leader);
+            const double et_l = __shfl_sync(kFull, et, leader);
+            const uint32_t j_l = __shfl_sync(kFull, j, leader);
+            const uint64_t ts_l = base + ((unsigned)leader >> 3);
+            if (st == 1) {
+                reprime = ts_l + kInvPhi * (uint64_t)j_l;
+                return et_l;
+            }
+            return exp_continue(loc_term, time, p, ts_l, 8u, et_l, reprime);
+        }
+        base += 4;
+    }
+}
+
 // lineage_step for one lineage held (identically) by all 32 lanes of a warp.
 // Every lane computes exactly one prime and one draw per pass, so the
 // event's hash work costs the instruction stream of a single prime + draw:
@@ -319,13 +376,19 @@ constexpr long long kNoEvent = 0x7fffffffffffffffLL;
 // sequential loop of poisson.rs:48-100 stops at) selects the candidate whose
 // four lanes hold the event's samples; other events re-prime after the
 // selection.  Side effects happen on lane 0 only; every lane returns with
-// the same updated lineage.
-template <int KIND>
+// the same updated lineage.  EXP selects the exponential event-time
+// sampler, searched by exp_search_coop.
+template <int KIND, bool EXP = false>
 __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, const EventSink &k) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
     uint64_t rs, e1, e2, e3, e4;
     bool drawn = false;
+    if (EXP && !l.has_next) {
+        const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
+        l.next = max_after(before, exp_search_coop(loc_term, before, p, l.reprime));
+        l.has_next = true;
+    }
     if (!l.has_next) {
         const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
         const long long before_bits = __double_as_longlong(before);
@@ -469,12 +532,6 @@ __device__ __forceinline__ void store_stopped(const StepArgs &a, const Lane &l) 
     a.in.has_next[l.slot] = 1;
 }
 
-// floor(time / delta_t) as the Poisson sampler's first bucket (poisson.rs:44)
-__device__ __forceinline__ uint64_t first_bucket(const SimParams &p, double time) {
-    const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
-    return f64_to_u64(floor(q));
-}
-
 // A lane's lineage in converged passes: the pass kind, the current Poisson
 // bucket, the time the search starts after, and the location term.
 struct Pass {
@@ -499,7 +556,7 @@ __device__ __forceinline__ bool pass_begin(Lane &l, const SimParams &p, Pass &ps
     // (active_lineage_sampler/independent/sampler.rs:69-116)
     ps.searching = true;
     ps.before = l.last > p.min_event_time ? l.last : p.min_event_time;
-    ps.ts = first_bucket(p, ps.before);
+    ps.ts = time_bucket(p, ps.before);
     return true;
 }
 
@@ -535,7 +592,7 @@ __device__ __forceinline__ int pass_run(Lane &l, const SimParams &p, const Event
         ps.searching = true;
         ps.loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
         ps.before = l.last;  // the event time, already after min_event_time
-        ps.ts = first_bucket(p, ps.before);
+        ps.ts = time_bucket(p, ps.before);
     }
     return r;
 }
@@ -552,7 +609,7 @@ __device__ __forceinline__ int pass_run(Lane &l, const SimParams &p, const Event
 // for the hash work instead of diverging through the bucket loop, the
 // event and the refill.  With few lineages per lane (latency) each lane
 // runs lineage_step's latency form.
-template <int KIND, bool SINGLE>
+template <int KIND, bool SINGLE, bool EXP>
 __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
     // one simulation: its parameters live in shared memory for the launch
     __shared__ __align__(16) unsigned char params_smem[SINGLE ? sizeof(SimParams) : 16];
@@ -584,7 +641,7 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
             const SimParams &p = P[SINGLE ? 0 : c.s];
             int r;
             for (;;) {
-                r = lineage_step_coop<KIND>(c, p, sink);
+                r = lineage_step_coop<KIND, EXP>(c, p, sink);
                 if (r != kStepMoved) break;
                 warp_steps += 1;
             }
@@ -619,7 +676,7 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
                 const unsigned long long k = base + __popc(need & lanemask_lt);
                 if (k < n) {
                     have = take_lineage<KIND, SINGLE>(a, P, k, l);
-                    if (have && !lat && !pass_begin<KIND>(l, P[SINGLE ? 0 : l.s], ps)) {
+                    if (have && !EXP && !lat && !pass_begin<KIND>(l, P[SINGLE ? 0 : l.s], ps)) {
                         store_stopped(a, l);  // nothing to do before this horizon
                         have = false;
                     }
@@ -632,8 +689,11 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         if (!have) continue;
         const SimParams &p = P[SINGLE ? 0 : l.s];
 
-        // few lineages for the grid's lanes: latency form (uniform branch)
-        const int r = lat ? lineage_step<KIND, true>(l, p, sink) : pass_run<KIND>(l, p, sink, ps);
+        // few lineages for the grid's lanes: latency form (uniform branch);
+        // the exponential sampler steps lineages one event at a time
+        const int r = EXP ? (lat ? lineage_step<KIND, true, true>(l, p, sink)
+                                 : lineage_step<KIND, false, true>(l, p, sink))
+                          : (lat ? lineage_step<KIND, true>(l, p, sink) : pass_run<KIND>(l, p, sink, ps));
         if (r == kPassSearch) continue;
         if (r == kStepMoved) {
             local_steps += 1;
@@ -682,7 +742,7 @@ __device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long l
 // Lineage slot j lives on warp j % 8, lane j / 8: a simulation with few
 // lineages gets one lineage per warp, so lineages never share (and diverge
 // within) a warp until there are more than eight of them.
-template <int KIND, int THREADS>
+template <int KIND, int THREADS, bool EXP>
 __global__ void __launch_bounds__(THREADS) resident_kernel(ResidentArgs a) {
     constexpr unsigned kWarps = THREADS / 32;
     constexpr unsigned kSlots = THREADS;  // lineage slots (>= kResidentMax)
@@ -766,7 +826,7 @@ __global__ void __launch_bounds__(THREADS) resident_kernel(ResidentArgs a) {
                 if (c_alive) {
                     bool c_live = true;
                     for (;;) {
-                        const int r = lineage_step_coop<KIND>(c, p, sink);
+                        const int r = lineage_step_coop<KIND, EXP>(c, p, sink);
                         if (r == kStepMoved) {
                             ++my_events;
                             continue;
@@ -790,7 +850,8 @@ __global__ void __launch_bounds__(THREADS) resident_kernel(ResidentArgs a) {
                 // up to 8 lineages per warp: latency form
                 const bool lat = n <= 8 * kWarps;
                 for (;;) {
-                    const int r = lat ? lineage_step<KIND, true>(l, p, sink) : lineage_step<KIND, false>(l, p, sink);
+                    const int r = lat ? lineage_step<KIND, true, EXP>(l, p, sink)
+                                      : lineage_step<KIND, false, EXP>(l, p, sink);
                     if (r == kStepMoved) {
                         ++my_events;
                         continue;
@@ -1090,10 +1151,16 @@ __global__ void schedule_kernel(ScheduleArgs a) {
 // ---- host-side launchers ----
 template <int KIND>
 static cudaError_t launch_step_t(const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st) {
-    if (a.n_sims == 1)
-        step_kernel<KIND, true><<<grid, block, 0, st>>>(a);
-    else
-        step_kernel<KIND, false><<<grid, block, 0, st>>>(a);
+    if (a.exp_sampler) {
+        if (a.n_sims == 1)
+            step_kernel<KIND, true, true><<<grid, block, 0, st>>>(a);
+        else
+            step_kernel<KIND, false, true><<<grid, block, 0, st>>>(a);
+    } else if (a.n_sims == 1) {
+        step_kernel<KIND, true, false><<<grid, block, 0, st>>>(a);
+    } else {
+        step_kernel<KIND, false, false><<<grid, block, 0, st>>>(a);
+    }
     return cudaGetLastError();
 }
 
@@ -1107,16 +1174,19 @@ cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned blo
     }
 }
 
-cudaError_t step_kernel_occupancy(int kind, int block, int *blocks_per_sm) {
+template <int KIND>
+static cudaError_t step_occupancy_t(bool exp_sampler, int block, int *blocks_per_sm) {
+    if (exp_sampler)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<KIND, false, true>, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<KIND, false, false>, block, 0);
+}
+
+cudaError_t step_kernel_occupancy(int kind, bool exp_sampler, int block, int *blocks_per_sm) {
     switch (kind) {
-    case kNonSpatial:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kNonSpatial, false>, block, 0);
-    case kSpatiallyImplicit:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kSpatiallyImplicit, false>, block, 0);
-    case kAlmostInfiniteNormal:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kAlmostInfiniteNormal, false>, block, 0);
-    case kSpatiallyExplicit:
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<kSpatiallyExplicit, false>, block, 0);
+    case kNonSpatial: return step_occupancy_t<kNonSpatial>(exp_sampler, block, blocks_per_sm);
+    case kSpatiallyImplicit: return step_occupancy_t<kSpatiallyImplicit>(exp_sampler, block, blocks_per_sm);
+    case kAlmostInfiniteNormal: return step_occupancy_t<kAlmostInfiniteNormal>(exp_sampler, block, blocks_per_sm);
+    case kSpatiallyExplicit: return step_occupancy_t<kSpatiallyExplicit>(exp_sampler, block, blocks_per_sm);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1145,14 +1215,20 @@ cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st) 
     return cudaGetLastError();
 }
 
+template <int KIND>
+static void launch_resident_t(const ResidentArgs &a, unsigned grid, cudaStream_t st) {
+    if (a.exp_sampler)
+        resident_kernel<KIND, kResidentMax, true><<<grid, kResidentMax, 0, st>>>(a);
+    else
+        resident_kernel<KIND, kResidentMax, false><<<grid, kResidentMax, 0, st>>>(a);
+}
+
 cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st) {
     switch (kind) {
-    case kNonSpatial: resident_kernel<kNonSpatial, kResidentMax><<<grid, kResidentMax, 0, st>>>(a); break;
-    case kSpatiallyImplicit: resident_kernel<kSpatiallyImplicit, kResidentMax><<<grid, kResidentMax, 0, st>>>(a); break;
-    case kAlmostInfiniteNormal:
-        resident_kernel<kAlmostInfiniteNormal, kResidentMax><<<grid, kResidentMax, 0, st>>>(a);
-        break;
-    case kSpatiallyExplicit: resident_kernel<kSpatiallyExplicit, kResidentMax><<<grid, kResidentMax, 0, st>>>(a); break;
+    case kNonSpatial: launch_resident_t<kNonSpatial>(a, grid, st); break;
+    case kSpatiallyImplicit: launch_resident_t<kSpatiallyImplicit>(a, grid, st); break;
+    case kAlmostInfiniteNormal: launch_resident_t<kAlmostInfiniteNormal>(a, grid, st); break;
+    case kSpatiallyExplicit: launch_resident_t<kSpatiallyExplicit>(a, grid, st); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

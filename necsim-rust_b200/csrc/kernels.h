@@ -33,6 +33,7 @@ struct StepArgs {
     unsigned long long *steps_total;     // optional per-launch event count
     uint32_t n_sims;                     // simulations in `params`
     TraceSink trace;                     // death records of speciated lineages (tracing only)
+    uint32_t exp_sampler;                // 1: exponential event-time sampler (exp.rs), else Poisson
 };
 
 struct DedupArgs {
@@ -69,7 +70,7 @@ struct ScheduleArgs {
 };
 
 cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st);
-cudaError_t step_kernel_occupancy(int kind, int block, int *blocks_per_sm);
+cudaError_t step_kernel_occupancy(int kind, bool exp_sampler, int block, int *blocks_per_sm);
 cudaError_t launch_dedup(const DedupArgs &a, unsigned grid, unsigned block, cudaStream_t st);
 cudaError_t launch_schedule(const ScheduleArgs &a, cudaStream_t st);
 
@@ -87,6 +88,7 @@ struct ResidentArgs {
     unsigned long long *visits;
     unsigned int *n_resident;
     const int *stop_flag;                // set when the concurrent global rounds end (nullable)
+    uint32_t exp_sampler;                // 1: exponential event-time sampler (exp.rs), else Poisson
 };
 
 cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st);

@@ -1,7 +1,10 @@
 /*
  * necsim_oracle.c -- CPU restatement of necsim-rust's Independent algorithm
  * (Monolithic parallelisation, Poisson event-time sampler, WyHash RNG,
- * IntrinsicsMathsCore = the system libm).
+ * IntrinsicsMathsCore = the system libm), with the CUDA algorithm's
+ * exponential event-time sampler as an option (its logarithm is the
+ * product's correctly rounded ln_dd.h, shared source, so event times agree
+ * bit for bit; glibc's log differs from it by one ulp on ~0.08% of inputs).
  *
  * TEST INFRASTRUCTURE ONLY: the parity checker for the GPU backend and the
  * timed CPU baseline.  The product never links or calls this file.
@@ -26,6 +29,7 @@
  * built here and its tests hold no golden vectors for this path.
  */
 #include "necsim_oracle.h"
+#include "../necsim-rust_b200/csrc/ln_dd.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -189,6 +193,7 @@ typedef struct sim_t {
     double migration;
     double sigma;
     int clark;          /* AlmostInfinite with Clark2Dt dispersal */
+    int exp_sampler;    /* ExpEventTimeSampler instead of the Poisson one */
     double shape_u, tail_p;
     extent_t local;     /* NonSpatial / SI local / SE map extent */
     uint32_t deme;
@@ -307,6 +312,40 @@ static double poisson_next_event_time(sim_t *s, uint64_t inj, double time, uint6
     rng_prime(g, inj, reprime);
     if (reprime_out) *reprime_out = reprime;
     return event_time;
+}
+
+/* event_time_sampler/exp.rs:37-83 ExpEventTimeSampler, with
+ * rng.rs:163-167 sample_exponential = -ln(U(0,1]) / lambda */
+static double exp_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out) {
+    rng_t *g = &s->rng;
+    uint64_t time_step = f64_as_u64(floor(time / s->delta_t));
+    double event_time = (double)time_step * s->delta_t;
+    double time_slice_end = (double)(time_step + 1) * s->delta_t;
+    uint64_t sub_index = 0;
+    rng_prime(g, inj, time_step);
+    for (;;) {
+        event_time += -necsim_ln(u01_open_closed(g)) / s->lambda;
+        sub_index += INV_PHI_U64;
+        /* the time slice is exclusive at time_slice_end */
+        if (event_time >= time_slice_end) {
+            time_step += 1;
+            sub_index = 0;
+            event_time = time_slice_end;
+            time_slice_end = (double)(time_step + 1) * s->delta_t;
+            rng_prime(g, inj, time_step);
+        } else if (event_time > time) {
+            break;
+        }
+    }
+    uint64_t reprime = time_step + sub_index;
+    rng_prime(g, inj, reprime);
+    if (reprime_out) *reprime_out = reprime;
+    return event_time;
+}
+
+static double next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out) {
+    return s->exp_sampler ? exp_next_event_time(s, inj, time, reprime_out)
+                          : poisson_next_event_time(s, inj, time, reprime_out);
 }
 
 /* dispersal_sampler/non_spatial.rs:42-66 */
@@ -658,6 +697,8 @@ static int sim_init(sim_t *s, const oracle_scenario *sc, const oracle_args *args
     s->delta_t = args->delta_t;
     s->lambda_dt = s->lambda * s->delta_t;
     s->p0 = exp(-s->lambda_dt);
+    s->exp_sampler = args->event_time_sampler == ORACLE_SAMPLER_EXP;
+    if (args->event_time_sampler != ORACLE_SAMPLER_POISSON && !s->exp_sampler) return -2;
     s->migration = sc->migration_probability;
     s->sigma = sc->sigma;
     if (sc->kind == ORACLE_ALMOST_INFINITE_CLARK2DT) {
@@ -801,7 +842,7 @@ static int64_t enumerate_origins(const oracle_scenario *sc, const sim_t *s, line
 }
 
 int64_t oracle_count_origins(const oracle_scenario *sc) {
-    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1, 0};
+    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1, 0, 0, 0};
     sim_t s;
     oracle_scenario tmp = *sc;
     int rc;
@@ -818,7 +859,7 @@ int64_t oracle_count_origins(const oracle_scenario *sc) {
 }
 
 int64_t oracle_enumerate_origins(const oracle_scenario *sc, oracle_lineage *out, uint64_t cap) {
-    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1, 0};
+    oracle_args a = {2.0, 10, 1.0, 2.0, 0, 0, 0, 0, 1, 0, 0, 0};
     sim_t s;
     int rc;
     if (sc->kind == ORACLE_SPATIALLY_EXPLICIT) {
@@ -994,7 +1035,7 @@ static int run_slice(sim_t *s, lineage_t *lin, double min_event_time, uint64_t s
         double before = lin->last > min_event_time ? lin->last : min_event_time;
         uint64_t inj = injection(s, lin->x, lin->y, lin->i);
         rng_t saved = s->rng;
-        double t = poisson_next_event_time(s, inj, before, NULL);
+        double t = next_event_time(s, inj, before, NULL);
         double next = max_after(before, t);
         o->peeked = 1;
         o->next = next;
@@ -1472,4 +1513,19 @@ double oracle_poisson_next_event_time(uint64_t seed, uint64_t inj, double t, dou
     s.lambda_dt = lambda * delta_t;
     s.p0 = exp(-s.lambda_dt);
     return poisson_next_event_time(&s, inj, t, reprime);
+}
+
+double oracle_exp_next_event_time(uint64_t seed, uint64_t inj, double t, double lambda,
+                                  double delta_t, uint64_t *reprime) {
+    sim_t s;
+    memset(&s, 0, sizeof(s));
+    s.rng.seed = seed;
+    s.rng.state = seed;
+    s.lambda = lambda;
+    s.delta_t = delta_t;
+    return exp_next_event_time(&s, inj, t, reprime);
+}
+
+void oracle_ln(const double *x, double *out, uint64_t n) {
+    for (uint64_t j = 0; j < n; ++j) out[j] = necsim_ln(x[j]);
 }

@@ -62,7 +62,12 @@ typedef struct oracle_args {
     uint32_t partition_rank;    /* IsolatedIndividuals partition (size 1 = monolithic) */
     uint32_t partition_size;
     uint64_t step_slice_max;    /* canonical schedule: cap on events per lineage per round (0: none) */
+    int32_t event_time_sampler; /* ORACLE_SAMPLER_POISSON (default) or ORACLE_SAMPLER_EXP */
+    int32_t pad;
 } oracle_args;
+
+#define ORACLE_SAMPLER_POISSON 0 /* event_time_sampler/poisson.rs */
+#define ORACLE_SAMPLER_EXP 1     /* event_time_sampler/exp.rs */
 
 typedef struct oracle_speciation_event {   /* SpeciationEvent, 40 bytes */
     uint64_t gref;
@@ -131,6 +136,11 @@ uint64_t oracle_wymum(uint64_t a, uint64_t b);
  * returns the re-prime time index in *reprime */
 double oracle_poisson_next_event_time(uint64_t seed, uint64_t injection, double t,
                                       double lambda, double delta_t, uint64_t *reprime);
+/* the same for the exponential sampler (exp.rs) */
+double oracle_exp_next_event_time(uint64_t seed, uint64_t injection, double t,
+                                  double lambda, double delta_t, uint64_t *reprime);
+/* the shared correctly rounded logarithm (ln_dd.h) of n values in (0, 1] */
+void oracle_ln(const double *x, double *out, uint64_t n);
 /* number of origins the scenario's origin sampler yields (100% sample) */
 int64_t oracle_count_origins(const oracle_scenario *sc);
 int64_t oracle_enumerate_origins(const oracle_scenario *sc, oracle_lineage *out, uint64_t cap);

@@ -21,6 +21,9 @@ SPATIALLY_EXPLICIT = 3
 MODE_REFERENCE = 0
 MODE_CANONICAL = 1
 
+SAMPLER_POISSON = 0  # event_time_sampler/poisson.rs
+SAMPLER_EXP = 1  # event_time_sampler/exp.rs
+
 
 class OracleScenario(ctypes.Structure):
     _fields_ = [
@@ -59,6 +62,8 @@ class OracleArgs(ctypes.Structure):
         ("partition_rank", ctypes.c_uint32),
         ("partition_size", ctypes.c_uint32),
         ("step_slice_max", ctypes.c_uint64),
+        ("event_time_sampler", ctypes.c_int32),
+        ("pad", ctypes.c_int32),
     ]
 
 
@@ -146,6 +151,11 @@ def lib():
         L.oracle_poisson_next_event_time.argtypes = [u64, u64, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_double, ctypes.POINTER(u64)]
         L.oracle_poisson_next_event_time.restype = ctypes.c_double
+        L.oracle_exp_next_event_time.argtypes = [u64, u64, ctypes.c_double, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.POINTER(u64)]
+        L.oracle_exp_next_event_time.restype = ctypes.c_double
+        L.oracle_ln.argtypes = [vp, vp, u64]
+        L.oracle_ln.restype = None
         L.oracle_count_origins.argtypes = [ctypes.POINTER(OracleScenario)]
         L.oracle_count_origins.restype = ctypes.c_int64
         L.oracle_enumerate_origins.argtypes = [ctypes.POINTER(OracleScenario), vp, u64]
@@ -205,7 +215,7 @@ def make_scenario(desc):
 
 def make_args(mode=MODE_REFERENCE, delta_t=2.0, step_slice=10, dedup_factor=1.0,
               event_slice_factor=2.0, min_round_events=0, report_dispersal=False,
-              partition=(0, 1), step_slice_max=0):
+              partition=(0, 1), step_slice_max=0, event_time_sampler=SAMPLER_POISSON):
     a = OracleArgs()
     a.delta_t = delta_t
     a.step_slice = step_slice
@@ -217,6 +227,7 @@ def make_args(mode=MODE_REFERENCE, delta_t=2.0, step_slice=10, dedup_factor=1.0,
     a.partition_rank = partition[0]
     a.partition_size = partition[1]
     a.step_slice_max = step_slice_max
+    a.event_time_sampler = event_time_sampler
     return a
 
 
@@ -289,6 +300,20 @@ def poisson_next_event_time(seed, injection, t, lam=0.5, delta_t=2.0):
     rp = ctypes.c_uint64(0)
     v = lib().oracle_poisson_next_event_time(seed, injection, t, lam, delta_t, ctypes.byref(rp))
     return v, rp.value
+
+
+def exp_next_event_time(seed, injection, t, lam=0.5, delta_t=2.0):
+    rp = ctypes.c_uint64(0)
+    v = lib().oracle_exp_next_event_time(seed, injection, t, lam, delta_t, ctypes.byref(rp))
+    return v, rp.value
+
+
+def ln(x):
+    """The shared correctly rounded logarithm (ln_dd.h) of values in (0, 1]."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    lib().oracle_ln(x.ctypes.data, out.ctypes.data, x.size)
+    return out
 
 
 def enumerate_origins(desc):
