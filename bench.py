@@ -64,6 +64,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--pause", type=float, default=None,
                    help="pause_before of every simulation (default: run to completion)")
+    p.add_argument("--event-time-sampler", default="poisson", choices=["poisson", "exp"],
+                   help="poisson: the Independent algorithm's PoissonEventTimeSampler (the headline); "
+                        "exp: the CUDA algorithm's ExpEventTimeSampler, -ln(U(0,1]) / lambda per event")
     return p.parse_args()
 
 
@@ -201,15 +204,17 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU restatement of the reference (bounded sample)
 # ---------------------------------------------------------------------------
-def cpu_sample(sims, pause, threads):
+def cpu_sample(sims, pause, threads, sampler="poisson"):
     """Runs the reference-faithful CPU restatement on every simulation of the
     workload up to time `pause` (a bounded sample), `threads` at a time.
     Returns (events, seconds)."""
     import oracle
+    code = oracle.SAMPLER_EXP if sampler == "exp" else oracle.SAMPLER_POISSON
 
     def one(item):
         d, seed = item
-        return oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause).steps
+        return oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause,
+                               event_time_sampler=code).steps
 
     oracle.lib()
     t0 = time.perf_counter()
@@ -230,10 +235,10 @@ def reference_arm(args, dist):
     desc, sims = workload(args.workload)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_sample(sims, args.cpu_sample_pause, threads)
+        cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler)
     ev, sec = 0, 0.0
     for _ in range(args.steps):
-        e, s = cpu_sample(sims, args.cpu_sample_pause, threads)
+        e, s = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler)
         ev += e
         sec += s
     value = ev / sec
@@ -241,7 +246,8 @@ def reference_arm(args, dist):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sec / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
-        "data": "synthetic", "config": {"workload": desc, "schedule": "reference Monolithic"},
+        "data": "synthetic", "config": {"workload": desc, "schedule": "reference Monolithic",
+                                        "event_time_sampler": args.event_time_sampler},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
                                                    len(sims))},
@@ -333,7 +339,7 @@ def main():
     model, model_info = None, None
     if args.schedule in ("learned", "both"):
         model, model_info = train_lifetime_model(nb, syn, device, args.train_pause)
-    plain_algo = nb.CUDA(device=device)
+    plain_algo = nb.CUDA(device=device, event_time_sampler=args.event_time_sampler)
     tune_info = None
     if args.autotune == "on" or (args.autotune == "auto" and args.workload.startswith("c4")):
         t0 = time.perf_counter()
@@ -395,7 +401,7 @@ def main():
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
         "data": "synthetic",
         "config": {"workload": desc, "schedule": "learned" if model else "plain", "kind": kind,
-                   "pause_before": args.pause,
+                   "pause_before": args.pause, "event_time_sampler": args.event_time_sampler,
                    "simulations": len(sims), "lineages": int(sum(o.n_initial for o in outs)),
                    "l2": "inputs larger than L2 (lineage state %.2f GB)" % (
                        sum(o.n_initial for o in outs) * 57 * 2 / 1e9),
@@ -433,7 +439,7 @@ def main():
         line["autotune"] = tune_info
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads)
+        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler)
         line["cpu_baseline"] = {"value": ev / sec, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
                                                           len(sims))}

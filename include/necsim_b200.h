@@ -323,6 +323,39 @@ int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *ou
 int necsim_presample_origins(uint64_t n, double percentage, uint32_t rank, uint32_t size, uint64_t *out,
                              uint64_t cap, uint64_t *n_out);
 
+/* ---- SpatiallyExplicit maps ----
+ * Replaces load_map_from_tiff (rustcoalescence/scenarios/src/spatially_explicit/
+ * maps/tiff/mod.rs:27-127): loads the first image of a one-band (Geo)TIFF --
+ * classic or BigTIFF, either byte order, strips or tiles, uncompressed, LZW,
+ * PackBits or Deflate, predictor 1, 2 or 3 -- as row-major samples:
+ * NECSIM_MAP_U32 (habitat: 32-bit, SampleFormat Uint or absent) or
+ * NECSIM_MAP_F64 (dispersal, turnover: 64-bit IEEEFP).  Unless `strict`,
+ * samples equal to the GDAL no-data value (tag 42113, parsed like Rust's
+ * `str::parse`) become 0.  *data is allocated here: release it with
+ * necsim_map_free.  Errors name the file in `error`. */
+#define NECSIM_MAP_U32 0
+#define NECSIM_MAP_F64 1
+int necsim_map_load(const char *path, int32_t sample, int32_t strict, void **data, uint32_t *width,
+                    uint32_t *height, char *error, size_t error_cap);
+void necsim_map_free(void *data);
+
+/* Map loading modes (maps/mod.rs:79-89, MapLoadingMode) and their fix-ups
+ * (maps/mod.rs:56-77, 90-215), applied in place:
+ *   OFF_BY_ONE (the reference's default): habitat values 0/1 become 1 where
+ *     any dispersal leaves the cell, else 0 (0 where turnover is 0);
+ *   FIX_ME: that, then habitat 0 where turnover is 0, then dispersal to and
+ *     from non-habitat removed and self-dispersal 1 added to habitat cells
+ *     with none left (the dispersal map must be (w*h) x (w*h));
+ *   STRICT: no change (maps load with `strict`).
+ * Every mode first rejects negative dispersal weights
+ * (NECSIM_E_DISPERSAL_MAP) and turnover rates.  `turnover` (w*h rates) may
+ * be NULL (uniform turnover). */
+#define NECSIM_MAPS_OFF_BY_ONE 0
+#define NECSIM_MAPS_FIX_ME 1
+#define NECSIM_MAPS_STRICT 2
+int necsim_maps_fix(uint32_t *habitat, uint32_t width, uint32_t height, double *dispersal, uint64_t dispersal_rows,
+                    uint64_t dispersal_cols, const double *turnover, int32_t mode, char *error, size_t error_cap);
+
 /* ---- event log ----
  * The reference's on-disk event log (EventLogRecorder,
  * necsim/impls/std/src/event_log/recorder.rs): a reporter that buffers

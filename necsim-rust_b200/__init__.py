@@ -183,6 +183,14 @@ def lib():
     L.necsim_event_log_close.restype = ctypes.c_int
     L.necsim_presample_origins.argtypes = [u64, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint32, vp, u64, P(u64)]
     L.necsim_presample_origins.restype = ctypes.c_int
+    L.necsim_map_load.argtypes = [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P(vp), P(ctypes.c_uint32),
+                                  P(ctypes.c_uint32), ctypes.c_char_p, ctypes.c_size_t]
+    L.necsim_map_load.restype = ctypes.c_int
+    L.necsim_map_free.argtypes = [vp]
+    L.necsim_map_free.restype = None
+    L.necsim_maps_fix.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, u64, u64, vp, ctypes.c_int32,
+                                  ctypes.c_char_p, ctypes.c_size_t]
+    L.necsim_maps_fix.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
     L.necsim_model_create.restype = ctypes.c_int
     L.necsim_model_destroy.argtypes = [vp]
@@ -267,6 +275,69 @@ class SpatiallyExplicit:
     habitat: np.ndarray
     dispersal: np.ndarray
     turnover: float = 0.5
+
+
+MAP_LOADING_MODES = {"OffByOne": 0, "FixMe": 1, "Strict": 2}
+
+
+def load_map(path: str, dtype: str = "u32", strict: bool = False) -> np.ndarray:
+    """A one-band (Geo)TIFF map as a [height, width] array: "u32" for habitat
+    maps, "f64" for dispersal and turnover maps (maps/tiff/mod.rs
+    load_map_from_tiff; GDAL no-data samples become 0 unless `strict`)."""
+    if dtype not in ("u32", "f64"):
+        raise ValueError("dtype must be 'u32' or 'f64'")
+    L = lib()
+    data = ctypes.c_void_p()
+    w, h = ctypes.c_uint32(), ctypes.c_uint32()
+    err = ctypes.create_string_buffer(512)
+    rc = L.necsim_map_load(os.fsencode(path), 0 if dtype == "u32" else 1, int(bool(strict)), ctypes.byref(data),
+                           ctypes.byref(w), ctypes.byref(h), err, 512)
+    if rc != 0:
+        raise NecsimError(rc, err.value.decode())
+    try:
+        n = w.value * h.value
+        ct = ctypes.c_uint32 if dtype == "u32" else ctypes.c_double
+        arr = np.ctypeslib.as_array(ctypes.cast(data, ctypes.POINTER(ct)), shape=(n,)).copy()
+    finally:
+        L.necsim_map_free(data)
+    return arr.reshape(h.value, w.value)
+
+
+def fix_maps(habitat: np.ndarray, dispersal: np.ndarray, turnover: Optional[np.ndarray] = None,
+             mode: str = "OffByOne"):
+    """The reference's map fix-ups for a loading mode (maps/mod.rs:56-215) on
+    copies of the maps: returns (habitat, dispersal)."""
+    if mode not in MAP_LOADING_MODES:
+        raise ValueError("mode must be one of %s" % sorted(MAP_LOADING_MODES))
+    hab = np.ascontiguousarray(habitat, dtype=np.uint32).copy()
+    disp = np.ascontiguousarray(dispersal, dtype=np.float64).copy()
+    if hab.ndim != 2 or disp.ndim != 2:
+        raise ValueError("habitat and dispersal must be 2-D")
+    tv = None
+    if turnover is not None:
+        tv = np.ascontiguousarray(turnover, dtype=np.float64)
+        if tv.shape != hab.shape:
+            raise ValueError("the turnover map must have the habitat map's shape")
+    err = ctypes.create_string_buffer(512)
+    rc = lib().necsim_maps_fix(hab.ctypes.data, hab.shape[1], hab.shape[0], disp.ctypes.data, disp.shape[0],
+                               disp.shape[1], tv.ctypes.data if tv is not None else None,
+                               MAP_LOADING_MODES[mode], err, 512)
+    if rc != 0:
+        raise NecsimError(rc, err.value.decode())
+    return hab, disp
+
+
+def spatially_explicit_from_maps(habitat_path: str, dispersal_path: str, turnover: float = 0.5,
+                                 mode: str = "OffByOne") -> "SpatiallyExplicit":
+    """`SpatiallyExplicit(habitat: "...", dispersal: "...", turnover:
+    Uniform(rate), mode: ...)` (spatially_explicit/turnover/uniform.rs
+    try_load): the dispersal map, then the habitat map, loaded and fixed up
+    as the loading mode says."""
+    strict = mode == "Strict"
+    disp = load_map(dispersal_path, "f64", strict)
+    hab = load_map(habitat_path, "u32", strict)
+    hab, disp = fix_maps(hab, disp, None, mode)
+    return SpatiallyExplicit(hab, disp, turnover)
 
 
 @dataclass

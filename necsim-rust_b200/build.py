@@ -16,7 +16,7 @@ DRIVER = os.path.join(LIB_DIR, "necsim-b200")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CU_SOURCES = ["kernels.cu", "noalloc.cu", "learned.cu"]
-CPP_SOURCES = ["host.cpp", "tables.cpp", "event_log.cpp"]
+CPP_SOURCES = ["host.cpp", "tables.cpp", "event_log.cpp", "maps.cpp"]
 DRIVER_SOURCES = ["driver.cpp", "ron.cpp"]
 
 
@@ -58,7 +58,7 @@ def build(force=False, verbose=False):
         _run(cmd, verbose)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread"], verbose)
+    _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread", "-lz"], verbose)
     os.replace(tmp, LIB)
     # the rustcoalescence-style front end, linked against the library
     drv_objs = []

@@ -12,11 +12,13 @@
 // mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
 // which writes the configuration that resumes the run; rng Seed | Entropy;
 // the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle; Normal or Clark2Dt) and
-// SpatiallyExplicit (habitat and dispersal as .npy arrays, Uniform turnover,
-// Strict maps) scenarios; algorithm Independent(...) or CUDA(...) with
-// Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
+// SpatiallyExplicit (habitat and dispersal maps as (Geo)TIFF files or .npy
+// arrays, Uniform turnover, loading mode FixMe | OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
+// or CUDA(...) (exponential event times, the reference CUDA algorithm's
+// defaults) with Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
 // Counter, Execution (others are ignored with a notice); log EventLog(directory,
 // capacity) writes the reference's event log.
+#include <cctype>
 #include <chrono>
 #include <cinttypes>
 #include <cmath>
@@ -67,8 +69,7 @@ std::vector<T> load_npy(const std::string &path, const char *descr, std::vector<
     if (!f) fail("cannot open " + path);
     char magic[6];
     f.read(magic, 6);
-    if (!f || std::memcmp(magic, "\x93NUMPY", 6) != 0)
-        fail(path + ": not a .npy array (GeoTIFF maps are not read by this driver)");
+    if (!f || std::memcmp(magic, "\x93NUMPY", 6) != 0) fail(path + ": not a .npy array");
     unsigned char ver[2];
     f.read((char *)ver, 2);
     uint32_t hlen = 0;
@@ -115,6 +116,7 @@ struct Run {
     bool resume = false;
     double pause_before = -1.0;
     std::string pause_config;
+    std::string algorithm = "Independent";
     bool rep_biodiversity = false, rep_counter = false, rep_execution = false;
     std::string log_directory;  // log: EventLog(directory, capacity)
     uint64_t log_capacity = 1000000;
@@ -122,6 +124,31 @@ struct Run {
     std::vector<double> dispersal;
     std::string summary;
 };
+
+bool ends_with(const std::string &s, const char *suffix) {
+    const size_t n = std::strlen(suffix);
+    if (s.size() < n) return false;
+    for (size_t j = 0; j < n; ++j)
+        if (std::tolower((unsigned char)s[s.size() - n + j]) != suffix[j]) return false;
+    return true;
+}
+
+// a map as a (height, width) array: .npy as stored, anything else as a
+// (Geo)TIFF through the library's loader (strict in Strict mode)
+template <typename T>
+std::vector<T> load_map(const std::string &path, int32_t mode, std::vector<uint64_t> &shape) {
+    if (ends_with(path, ".npy")) return load_npy<T>(path, sizeof(T) == 4 ? "<u4" : "<f8", shape);
+    void *data = nullptr;
+    uint32_t w = 0, h = 0;
+    char err[512];
+    const int rc = necsim_map_load(path.c_str(), sizeof(T) == 4 ? NECSIM_MAP_U32 : NECSIM_MAP_F64,
+                                   mode == NECSIM_MAPS_STRICT ? 1 : 0, &data, &w, &h, err, sizeof(err));
+    if (rc) fail(err);
+    std::vector<T> out(static_cast<T *>(data), static_cast<T *>(data) + (uint64_t)w * h);
+    necsim_map_free(data);
+    shape = {h, w};
+    return out;
+}
 
 void parse_scenario(const Value &s, Run &r) {
     const std::string &k = s.variant();
@@ -177,26 +204,48 @@ void parse_scenario(const Value &s, Run &r) {
             o << "Clark2Dt(shape_u: " << sc.shape_u << ", tail_p: " << sc.tail_p << "))";
         }
     } else if (k == "SpatiallyExplicit") {
-        const Value &hab = need(s, "habitat"), &disp = need(s, "dispersal");
-        if (const Value *t = s.field("turnover")) {
-            if (t->variant() != "Uniform" || t->items.size() != 1)
-                fail("SpatiallyExplicit: only Uniform(rate) turnover is supported");
+        // spatially_explicit/turnover/mod.rs:13-30 (field names and aliases),
+        // uniform.rs:131-175 (try_load: the dispersal map first, then the
+        // habitat map with the loading mode's fix-ups)
+        const Value *hab = s.field("habitat") ? s.field("habitat") : s.field("habitat_map");
+        const Value *disp = s.field("dispersal") ? s.field("dispersal") : s.field("dispersal_map");
+        if (!hab) fail("missing field `habitat`");
+        if (!disp) fail("missing field `dispersal`");
+        sc.turnover_rate = 0.5;
+        const Value *t = s.field("turnover") ? s.field("turnover") : s.field("turnover_rate");
+        if (t) {
+            const std::string &tv = t->variant();
+            if (tv == "Map") fail("SpatiallyExplicit: turnover maps are not supported (uniform turnover only)");
+            if ((tv != "Uniform" && tv != "Rate" && tv != "UniformRate") || t->items.size() != 1)
+                fail("SpatiallyExplicit: turnover must be Uniform(rate)");
             sc.turnover_rate = t->items[0].as_f64();
         }
-        if (const Value *m = s.field("mode"))
-            if (m->variant() != "Strict") fail("SpatiallyExplicit: only Strict maps (no fix-up) are supported");
+        int32_t mode = NECSIM_MAPS_OFF_BY_ONE;  // MapLoadingMode::default (maps/mod.rs:84-88)
+        const Value *m = s.field("mode") ? s.field("mode") : s.field("loading_mode");
+        if (m) {
+            const std::string &mv = m->variant();
+            if (mv == "FixMe") mode = NECSIM_MAPS_FIX_ME;
+            else if (mv == "OffByOne") mode = NECSIM_MAPS_OFF_BY_ONE;
+            else if (mv == "Strict") mode = NECSIM_MAPS_STRICT;
+            else fail("SpatiallyExplicit: mode must be FixMe, OffByOne or Strict");
+        }
         std::vector<uint64_t> hs, ds;
-        r.habitat = load_npy<uint32_t>(hab.text, "<u4", hs);
-        r.dispersal = load_npy<double>(disp.text, "<f8", ds);
+        r.dispersal = load_map<double>(disp->text, mode, ds);
+        r.habitat = load_map<uint32_t>(hab->text, mode, hs);
         if (hs.size() != 2) fail("habitat must be a 2D (height, width) array");
+        if (ds.size() != 2) fail("dispersal must be a 2D array");
+        char err[512];
+        const int rc = necsim_maps_fix(r.habitat.data(), (uint32_t)hs[1], (uint32_t)hs[0], r.dispersal.data(), ds[0],
+                                       ds[1], nullptr, mode, err, sizeof(err));
+        if (rc) fail(std::string("SpatiallyExplicit maps: ") + err);
         const uint64_t cells = hs[0] * hs[1];
-        if (ds.size() != 2 || ds[0] != cells || ds[1] != cells) fail("dispersal must be (cells, cells)");
+        if (ds[0] != cells || ds[1] != cells) fail("dispersal must be (cells, cells)");
         sc.kind = NECSIM_SPATIALLY_EXPLICIT;
         sc.height = (uint32_t)hs[0];
         sc.width = (uint32_t)hs[1];
         sc.habitat = r.habitat.data();
         sc.dispersal = r.dispersal.data();
-        o << "SpatiallyExplicit(" << sc.width << "x" << sc.height << " map from " << hab.text << ")";
+        o << "SpatiallyExplicit(" << sc.width << "x" << sc.height << " map from " << hab->text << ")";
     } else {
         fail("scenario " + k + " is not supported by this backend");
     }
@@ -208,6 +257,16 @@ void parse_algorithm(const Value &a, Run &r) {
     if (k != "Independent" && k != "CUDA")
         fail("algorithm " + k + " is not the Independent algorithm this backend runs");
     necsim_args &g = r.args;
+    if (k == "CUDA") {
+        // the CUDA algorithm samples event times with ExpEventTimeSampler
+        // (algorithms/cuda/src/launch.rs:121) and defaults delta_t to 3.0 and
+        // step_slice to 150 (algorithms/cuda/src/arguments.rs:125-139); its
+        // block_size / grid_size defaults are launch shapes of its own kernel
+        g.event_time_sampler = NECSIM_SAMPLER_EXP;
+        g.delta_t = 3.0;
+        g.step_slice = 150;
+    }
+    r.algorithm = k;
     if (const Value *v = a.field("delta_t")) g.delta_t = v->as_f64();
     if (const Value *v = a.field("step_slice")) g.step_slice = v->as_u64();
     if (const Value *v = a.field("block_size")) g.block_size = as_u32(*v, "block_size");
@@ -446,6 +505,9 @@ int simulate(const std::string &path, bool run) {
     }
     std::printf("necsim-b200: %s, speciation %g, seed %" PRIu64 ", %zu lineages%s\n", r.summary.c_str(),
                 r.speciation, r.seed, lineages.size(), r.resume ? " (resumed)" : "");
+    std::printf("necsim-b200: algorithm %s, %s event times, delta_t %g, step_slice %" PRIu64 "\n",
+                r.algorithm.c_str(), r.args.event_time_sampler == NECSIM_SAMPLER_EXP ? "exponential" : "Poisson",
+                r.args.delta_t > 0.0 ? r.args.delta_t : 2.0, r.args.step_slice ? r.args.step_slice : (uint64_t)10);
     if (r.pause_before >= 0.0) std::printf("necsim-b200: pause before t = %g -> %s\n", r.pause_before,
                                            r.pause_config.c_str());
     if (!run) return 0;

@@ -93,6 +93,22 @@ def test_check_partition_and_sample(nb, tmp_path):
     assert n == len(presample_restated(1200, 0.5, 1, 2))
 
 
+CUDA_CONFIG = CONFIG.replace("""    algorithm: Independent(
+        delta_t: 2.0, step_slice: 10, dedup_cache: Relative(factor: 1.0),
+        parallelism_mode: Monolithic(event_slice: Relative(factor: 2.0)),
+    ),""", """    algorithm: CUDA(ptx_jit: true, block_size: 64, grid_size: 64),""")
+
+
+def test_check_reports_the_event_time_sampler(nb, tmp_path):
+    r = run_driver(nb, "check", CONFIG, tmp_path)
+    assert "algorithm Independent, Poisson event times, delta_t 2, step_slice 10" in r.stdout
+    assert CUDA_CONFIG != CONFIG
+    r = run_driver(nb, "check", CUDA_CONFIG, tmp_path)
+    assert r.returncode == 0, r.stderr
+    # the reference CUDA algorithm: ExpEventTimeSampler, delta_t 3.0, step_slice 150
+    assert "algorithm CUDA, exponential event times, delta_t 3, step_slice 150" in r.stdout
+
+
 def species(out):
     m = re.search(r"biodiversity of (\d+) unique species", out)
     return int(m.group(1)) if m else 0
@@ -144,3 +160,84 @@ def test_driver_writes_an_event_log(nb, tmp_path):
     assert n_spec > 0 and int((ev["kind"] == 2).sum()) > 0  # Counter() turns on dispersal events
     assert len({(int(e["x"]), int(e["y"]), int(e["index"]), float(e["event_time"]))
                 for e in ev[ev["kind"] == 0]}) == species(r.stdout)
+
+
+@pytest.mark.gpu
+def test_driver_cuda_algorithm_runs_exponential_event_times(nb, oracle, tmp_path):
+    r = run_driver(nb, "simulate", CUDA_CONFIG, tmp_path, "cuda.ron")
+    assert r.returncode == 0, r.stderr
+    desc = dict(kind=0, speciation_probability=0.01, width=30, height=20, deme=2)
+    ref = oracle.simulate(desc, 42, mode=oracle.MODE_REFERENCE, delta_t=3.0, step_slice=150,
+                          event_time_sampler=oracle.SAMPLER_EXP)
+    assert species(r.stdout) == ref.biodiversity > 0
+    o = nb.simulate(0.01, nb.NonSpatial((30, 20), 2), 42,
+                    nb.CUDA(event_time_sampler="exp", delta_t=3.0, step_slice=150))
+    assert o.biodiversity == ref.biodiversity
+
+
+# ---- SpatiallyExplicit maps from (Geo)TIFF files ----
+def se_tiffs(tmp_path, syn, w=12, h=10, seed=5):
+    import tiff_util
+    hab = syn.habitat_map(w, h, 0.15, 20, seed)
+    hab[0, 0] = 1  # a 0/1 cell that OffByOne re-derives from the dispersal map
+    disp = syn.dispersal_map(hab, 2.0)
+    disp[0] = 0.0
+    hp, dp = tmp_path / "habitat.tif", tmp_path / "dispersal.tif"
+    tiff_util.write_tiff(str(hp), hab.astype(np.uint32), compression=5)
+    tiff_util.write_tiff(str(dp), disp.astype(np.float64), compression=8, predictor=2)
+    return hp, dp, hab, disp
+
+
+SE_CONFIG = """(
+    speciation: 0.001,
+    sample: Sample(percentage: 1.0, origin: Habitat, mode: Genesis),
+    rng: Seed(7),
+    algorithm: Independent(),
+    scenario: SpatiallyExplicit(habitat: "%s", dispersal: "%s", turnover: Uniform(0.5)%s),
+    reporters: [Plugin(library: "x.so", reporters: [Biodiversity()])],
+)
+"""
+
+
+def test_check_reads_tiff_maps(nb, syn, tmp_path):
+    hp, dp, hab, disp = se_tiffs(tmp_path, syn)
+    fixed, _ = nb.fix_maps(hab, disp, None, "OffByOne")
+    assert fixed[0, 0] == 0 and hab[0, 0] == 1
+    r = run_driver(nb, "check", SE_CONFIG % (hp, dp, ""), tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "SpatiallyExplicit(12x10 map" in r.stdout
+    assert "%d lineages" % int(fixed.sum()) in r.stdout
+    r = run_driver(nb, "check", SE_CONFIG % (hp, dp, ", mode: Strict"), tmp_path)
+    assert "%d lineages" % int(hab.sum()) in r.stdout
+    for extra, msg in ((", mode: Lenient", "FixMe, OffByOne or Strict"),):
+        r = run_driver(nb, "check", SE_CONFIG % (hp, dp, extra), tmp_path)
+        assert r.returncode == 1 and msg in r.stderr
+    r = run_driver(nb, "check", (SE_CONFIG % (hp, dp, "")).replace("Uniform(0.5)", 'Map("t.tif")'), tmp_path)
+    assert r.returncode == 1 and "turnover maps" in r.stderr
+    r = run_driver(nb, "check", SE_CONFIG % (dp, hp, ""), tmp_path)  # maps swapped: wrong bit widths
+    assert r.returncode == 1 and "bitwidth" in r.stderr
+
+
+@pytest.mark.skipif(not os.path.isdir("/root/reference/maps/test"), reason="reference map fixtures not present")
+def test_check_reads_the_reference_fixture(nb, tmp_path):
+    cfg = (SE_CONFIG % ("/root/reference/maps/test/habitat.tif", "/root/reference/maps/test/dispersal.tif", "")
+           ).replace("percentage: 1.0", "percentage: 0.01")
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "SpatiallyExplicit(35x41 map" in r.stdout
+    n = int(re.search(r"(\d+) lineages", r.stdout).group(1))
+    assert n == len(presample_restated(287933, 0.01))
+
+
+@pytest.mark.gpu
+def test_driver_tiff_maps_match_the_package(nb, syn, oracle, tmp_path):
+    hp, dp, hab, disp = se_tiffs(tmp_path, syn)
+    r = run_driver(nb, "simulate", SE_CONFIG % (hp, dp, ""), tmp_path, "se.ron")
+    assert r.returncode == 0, r.stderr
+    sc = nb.spatially_explicit_from_maps(str(hp), str(dp))
+    o = nb.simulate(0.001, sc, 7)
+    assert species(r.stdout) == o.biodiversity > 0
+    desc = dict(kind=3, speciation_probability=0.001, width=12, height=10, habitat=sc.habitat,
+                dispersal=sc.dispersal)
+    ref = oracle.simulate(desc, 7, mode=oracle.MODE_REFERENCE)
+    assert ref.biodiversity == o.biodiversity
