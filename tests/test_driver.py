@@ -179,13 +179,16 @@ def test_driver_cuda_algorithm_runs_exponential_event_times(nb, oracle, tmp_path
 def se_tiffs(tmp_path, syn, w=12, h=10, seed=5):
     import tiff_util
     hab = syn.habitat_map(w, h, 0.15, 20, seed)
-    hab[0, 0] = 1  # a 0/1 cell that OffByOne re-derives from the dispersal map
     disp = syn.dispersal_map(hab, 2.0)
-    disp[0] = 0.0
+    # a habitable cell stored as 0 (an off-by-one rounding in the map):
+    # OffByOne restores it to 1 because dispersal leaves it
+    stored = hab.astype(np.uint32).copy()
+    c = np.flatnonzero(hab.reshape(-1) > 1)[0]
+    stored.reshape(-1)[c] = 0
     hp, dp = tmp_path / "habitat.tif", tmp_path / "dispersal.tif"
-    tiff_util.write_tiff(str(hp), hab.astype(np.uint32), compression=5)
+    tiff_util.write_tiff(str(hp), stored, compression=5)
     tiff_util.write_tiff(str(dp), disp.astype(np.float64), compression=8, predictor=2)
-    return hp, dp, hab, disp
+    return hp, dp, stored, disp
 
 
 SE_CONFIG = """(
@@ -202,7 +205,8 @@ SE_CONFIG = """(
 def test_check_reads_tiff_maps(nb, syn, tmp_path):
     hp, dp, hab, disp = se_tiffs(tmp_path, syn)
     fixed, _ = nb.fix_maps(hab, disp, None, "OffByOne")
-    assert fixed[0, 0] == 0 and hab[0, 0] == 1
+    changed = np.flatnonzero(fixed != hab)
+    assert len(changed) == 1 and fixed.reshape(-1)[changed[0]] == 1 and hab.reshape(-1)[changed[0]] == 0
     r = run_driver(nb, "check", SE_CONFIG % (hp, dp, ""), tmp_path)
     assert r.returncode == 0, r.stderr
     assert "SpatiallyExplicit(12x10 map" in r.stdout
