@@ -321,14 +321,22 @@ constexpr long long kNoEvent = 0x7fffffffffffffffLL;
 // that is not empty decides; one whose eight samples pass neither `time`
 // nor its end (rare for lambda * delta_t of order one) continues
 // sequentially from its ninth sample.  Every lane returns the same result.
+// Alongside its logarithm each lane primes the event state its sample would
+// select (re-prime index ts + (j + 1) * INV_PHI) and draws the event's four
+// samples, so a decided bucket hands the event its samples at once
+// (drawn = true); the sequential continuation leaves them undrawn.
 __device__ __forceinline__ double exp_search_coop(uint64_t loc_term, double time, const SimParams &p,
-                                                  uint64_t &reprime) {
+                                                  uint64_t &reprime, uint64_t &rs, uint64_t &e1, uint64_t &e2,
+                                                  uint64_t &e3, uint64_t &e4, bool &drawn) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned first = lane & ~7u;  // the bucket's first lane
     uint64_t base = time_bucket(p, time);
     for (;;) {
         const uint64_t ts = base + (lane >> 3);
-        const double e = exp_sample(draw_at(primed_state(loc_term, ts), (lane & 7u) + 1u), p.lambda);
+        const uint64_t mine = (uint64_t)(lane & 7u) + 1u;  // this lane's sample of the bucket
+        const double e = exp_sample(draw_at(primed_state(loc_term, ts), (uint32_t)mine), p.lambda);
+        const uint64_t sc = primed_state(loc_term, ts + kInvPhi * mine);
+        const uint64_t c1 = draw_at(sc, 1), c2 = draw_at(sc, 2), c3 = draw_at(sc, 3), c4 = draw_at(sc, 4);
         const double slice_end = __dmul_rn(__ull2double_rn(ts + 1), p.delta_t);
         double et = __dmul_rn(__ull2double_rn(ts), p.delta_t);
         int state = 0;  // 0: undecided, 1: event after `time` at sample j, 2: empty
@@ -354,9 +362,17 @@ __device__ __forceinline__ double exp_search_coop(uint64_t loc_term, double time
             const uint32_t j_l = __shfl_sync(kFull, j, leader);
             const uint64_t ts_l = base + ((unsigned)leader >> 3);
             if (st == 1) {
+                const int src = leader + (int)j_l - 1;  // the lane of sample j_l
+                rs = __shfl_sync(kFull, sc, src);
+                e1 = __shfl_sync(kFull, c1, src);
+                e2 = __shfl_sync(kFull, c2, src);
+                e3 = __shfl_sync(kFull, c3, src);
+                e4 = __shfl_sync(kFull, c4, src);
+                drawn = true;
                 reprime = ts_l + kInvPhi * (uint64_t)j_l;
                 return et_l;
             }
+            drawn = false;
             return exp_continue(loc_term, time, p, ts_l, 8u, et_l, reprime);
         }
         base += 4;
@@ -386,7 +402,7 @@ __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, co
     bool drawn = false;
     if (EXP && !l.has_next) {
         const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
-        l.next = max_after(before, exp_search_coop(loc_term, before, p, l.reprime));
+        l.next = max_after(before, exp_search_coop(loc_term, before, p, l.reprime, rs, e1, e2, e3, e4, drawn));
         l.has_next = true;
     }
     if (!l.has_next) {
@@ -608,9 +624,10 @@ __device__ __forceinline__ int pass_run(Lane &l, const SimParams &p, const Event
 // different points of their lineages thus execute the same instructions
 // for the hash work instead of diverging through the bucket loop, the
 // event and the refill.  With few lineages per lane (latency) each lane
-// runs lineage_step's latency form.
+// runs lineage_step's latency form.  EXP: the exponential event-time
+// sampler, one event at a time per lane (no converged-pass form).
 template <int KIND, bool SINGLE, bool EXP>
-__global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
+__device__ __forceinline__ void step_body(const StepArgs &a) {
     // one simulation: its parameters live in shared memory for the launch
     __shared__ __align__(16) unsigned char params_smem[SINGLE ? sizeof(SimParams) : 16];
     if (SINGLE) {
@@ -713,6 +730,19 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
         for (int off = 16; off > 0; off >>= 1) w += __shfl_down_sync(kFull, w, off);
         if (lane_id == 0 && w) atomicAdd(a.steps_total, w);
     }
+}
+
+// The step kernel with the Poisson sampler, and with the exponential one:
+// the latter's logarithm needs more registers than the allocation ptxas
+// picks by default (which spills), so it asks for one block per SM at least
+// instead; the Poisson kernel keeps its allocation.
+template <int KIND, bool SINGLE>
+__global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
+    step_body<KIND, SINGLE, false>(a);
+}
+template <int KIND, bool SINGLE>
+__global__ void __launch_bounds__(kStepBlockMax, 1) step_kernel_exp(StepArgs a) {
+    step_body<KIND, SINGLE, true>(a);
 }
 
 // Per-simulation horizon rule (canonical schedule):
@@ -1153,13 +1183,13 @@ template <int KIND>
 static cudaError_t launch_step_t(const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st) {
     if (a.exp_sampler) {
         if (a.n_sims == 1)
-            step_kernel<KIND, true, true><<<grid, block, 0, st>>>(a);
+            step_kernel_exp<KIND, true><<<grid, block, 0, st>>>(a);
         else
-            step_kernel<KIND, false, true><<<grid, block, 0, st>>>(a);
+            step_kernel_exp<KIND, false><<<grid, block, 0, st>>>(a);
     } else if (a.n_sims == 1) {
-        step_kernel<KIND, true, false><<<grid, block, 0, st>>>(a);
+        step_kernel<KIND, true><<<grid, block, 0, st>>>(a);
     } else {
-        step_kernel<KIND, false, false><<<grid, block, 0, st>>>(a);
+        step_kernel<KIND, false><<<grid, block, 0, st>>>(a);
     }
     return cudaGetLastError();
 }
@@ -1177,8 +1207,8 @@ cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned blo
 template <int KIND>
 static cudaError_t step_occupancy_t(bool exp_sampler, int block, int *blocks_per_sm) {
     if (exp_sampler)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<KIND, false, true>, block, 0);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<KIND, false, false>, block, 0);
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel_exp<KIND, false>, block, 0);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, step_kernel<KIND, false>, block, 0);
 }
 
 cudaError_t step_kernel_occupancy(int kind, bool exp_sampler, int block, int *blocks_per_sm) {
