@@ -4,8 +4,9 @@
  *
  * The backend is a drop-in for the reference's `algorithm: CUDA(...)` /
  * `Independent(...)` path: it takes a scenario (NonSpatial,
- * SpatiallyImplicit, AlmostInfinite with Normal dispersal,
- * SpatiallyExplicit with uniform turnover), a seeded WyHash RNG and the
+ * SpatiallyImplicit, AlmostInfinite with Normal or Clark2Dt dispersal,
+ * SpatiallyExplicit with uniform turnover or a turnover map), a seeded
+ * WyHash RNG and the
  * algorithm arguments, simulates every lineage on the GPU and hands the
  * events to reporters in the reference's reporting order.
  *
@@ -46,7 +47,7 @@ enum necsim_scenario_kind {
     NECSIM_NON_SPATIAL = 0,            /* rustcoalescence/scenarios/src/non_spatial.rs               */
     NECSIM_SPATIALLY_IMPLICIT = 1,     /* rustcoalescence/scenarios/src/spatially_implicit.rs        */
     NECSIM_ALMOST_INFINITE_NORMAL = 2, /* rustcoalescence/scenarios/src/almost_infinite/normal.rs    */
-    NECSIM_SPATIALLY_EXPLICIT = 3,     /* rustcoalescence/scenarios/src/spatially_explicit/turnover/uniform.rs */
+    NECSIM_SPATIALLY_EXPLICIT = 3,     /* rustcoalescence/scenarios/src/spatially_explicit/turnover/{uniform,map}.rs */
     NECSIM_ALMOST_INFINITE_CLARK2DT = 4, /* rustcoalescence/scenarios/src/almost_infinite/clark2dt.rs */
 };
 
@@ -68,6 +69,9 @@ typedef struct necsim_scenario {
     const double *dispersal;         /* SpatiallyExplicit: (w*h) x (w*h) f64, row-major */
     double shape_u, tail_p;          /* AlmostInfinite Clark2Dt dispersal (u > 0, p > 0); the
                                         Circle sample fields as for Normal */
+    const double *turnover_map;      /* SpatiallyExplicit: width*height f64 turnover rates, row-major
+                                        (spatially_explicit/turnover/map.rs, InMemoryTurnoverRate); NULL:
+                                        uniform `turnover_rate`.  Rates >= 0, > 0 on habitable cells */
 } necsim_scenario;
 
 /* necsim_args.event_time_sampler: which EventTimeSampler

@@ -11,7 +11,7 @@ the CUDA error the library reports.
 import ctypes
 import os
 from dataclasses import dataclass, field
-from typing import List, Optional, Sequence, Tuple
+from typing import List, Optional, Sequence, Tuple, Union
 
 import numpy as np
 
@@ -55,6 +55,7 @@ class CScenario(ctypes.Structure):
         ("habitat", ctypes.POINTER(ctypes.c_uint32)),
         ("dispersal", ctypes.POINTER(ctypes.c_double)),
         ("shape_u", ctypes.c_double), ("tail_p", ctypes.c_double),
+        ("turnover_map", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -269,12 +270,13 @@ class AlmostInfinite:
 
 @dataclass
 class SpatiallyExplicit:
-    """`SpatiallyExplicit(habitat, dispersal, turnover)` with in-memory maps
-    (spatially_explicit/turnover/uniform.rs): habitat u32 [h, w], dispersal
-    f64 [h*w, h*w]."""
+    """`SpatiallyExplicit(habitat, dispersal, turnover)` with in-memory maps:
+    habitat u32 [h, w], dispersal f64 [h*w, h*w]; turnover a uniform rate
+    (spatially_explicit/turnover/uniform.rs) or an f64 [h, w] turnover map
+    (turnover/map.rs: every habitable cell's rate > 0)."""
     habitat: np.ndarray
     dispersal: np.ndarray
-    turnover: float = 0.5
+    turnover: Union[float, np.ndarray] = 0.5
 
 
 MAP_LOADING_MODES = {"OffByOne": 0, "FixMe": 1, "Strict": 2}
@@ -327,17 +329,19 @@ def fix_maps(habitat: np.ndarray, dispersal: np.ndarray, turnover: Optional[np.n
     return hab, disp
 
 
-def spatially_explicit_from_maps(habitat_path: str, dispersal_path: str, turnover: float = 0.5,
+def spatially_explicit_from_maps(habitat_path: str, dispersal_path: str, turnover: Union[float, str] = 0.5,
                                  mode: str = "OffByOne") -> "SpatiallyExplicit":
     """`SpatiallyExplicit(habitat: "...", dispersal: "...", turnover:
-    Uniform(rate), mode: ...)` (spatially_explicit/turnover/uniform.rs
-    try_load): the dispersal map, then the habitat map, loaded and fixed up
-    as the loading mode says."""
+    Uniform(rate) | Map("..."), mode: ...)` (spatially_explicit/turnover/
+    uniform.rs and map.rs try_load): the dispersal map, then the turnover map
+    when given as a path, then the habitat map, loaded and fixed up as the
+    loading mode says."""
     strict = mode == "Strict"
     disp = load_map(dispersal_path, "f64", strict)
+    tmap = load_map(turnover, "f64", strict) if isinstance(turnover, (str, bytes, os.PathLike)) else None
     hab = load_map(habitat_path, "u32", strict)
-    hab, disp = fix_maps(hab, disp, None, mode)
-    return SpatiallyExplicit(hab, disp, turnover)
+    hab, disp = fix_maps(hab, disp, tmap, mode)
+    return SpatiallyExplicit(hab, disp, tmap if tmap is not None else turnover)
 
 
 @dataclass
@@ -454,10 +458,17 @@ def _scenario_struct(scenario, speciation: float):
         if h.ndim != 2 or d.shape != (h.size, h.size):
             raise ValueError("habitat must be [h, w] and dispersal [h*w, h*w]")
         c.height, c.width = h.shape
-        c.turnover_rate = scenario.turnover
         c.habitat = h.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
         c.dispersal = d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         keep += [h, d]
+        if np.ndim(scenario.turnover) == 0:
+            c.turnover_rate = float(scenario.turnover)
+        else:  # a turnover map (spatially_explicit/turnover/map.rs)
+            t = np.ascontiguousarray(scenario.turnover, dtype=np.float64)
+            if t.shape != h.shape:
+                raise ValueError("the turnover map must have the habitat map's shape")
+            c.turnover_map = t.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            keep.append(t)
     else:
         raise TypeError("unknown scenario %r" % (scenario,))
     c._keep = keep

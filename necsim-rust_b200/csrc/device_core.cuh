@@ -140,20 +140,20 @@ __device__ __forceinline__ double max_after(double before, double value) {
 // the stopping rank is the number of thresholds X exceeds: eight independent
 // compares instead of a loop of dependent loads.  Beyond the tabulated ranks
 // the reference loop continues in f64.
-__device__ __forceinline__ uint32_t poisson_count(uint64_t d1, const SimParams &p) {
+__device__ __forceinline__ uint32_t poisson_count(uint64_t d1, const PoissonConsts &pc) {
     const uint64_t X = d1 >> 11;
     uint32_t n_events = 0;
 #pragma unroll
-    for (int r = 0; r < kPoissonThresholds; ++r) n_events += X > p.poisson_threshold[r] ? 1u : 0u;
+    for (int r = 0; r < kPoissonThresholds; ++r) n_events += X > pc.threshold[r] ? 1u : 0u;
     if (n_events == (uint32_t)kPoissonThresholds) {
         const double u = unit_closed_open(d1);
-        double prod = p.poisson_prod_k;
-        double acc = p.poisson_acc_k;
+        double prod = pc.prod_k;
+        double acc = pc.acc_k;
         while (u > acc && prod > 0.0) {
             n_events += 1;
             const double ratio = n_events <= (uint32_t)kPoissonTable
-                                     ? p.lambda_dt_over_k[n_events - 1]
-                                     : __ddiv_rn(p.lambda_dt, __uint2double_rn(n_events));
+                                     ? pc.lambda_dt_over_k[n_events - 1]
+                                     : __ddiv_rn(pc.lambda_dt, __uint2double_rn(n_events));
             prod = __dmul_rn(prod, ratio);
             acc = __dadd_rn(acc, prod);
         }
@@ -171,8 +171,8 @@ __device__ __forceinline__ long long event_time_bits(double step_start, uint64_t
 // earliest event strictly after `time` (ties: lowest index), or -1.  Samples
 // are drawn only as the reference consumes them (throughput form).
 __device__ __forceinline__ int poisson_bucket(uint64_t s0, uint64_t time_step, double time,
-                                              const SimParams &p, double &best) {
-    const uint32_t n_events = poisson_count(draw_at(s0, 1), p);
+                                              const SimParams &p, const PoissonConsts &pc, double &best) {
+    const uint32_t n_events = poisson_count(draw_at(s0, 1), pc);
     if (n_events == 0) return -1;
     const double step_start = __ull2double_rn(time_step);
     const long long time_bits = __double_as_longlong(time);
@@ -193,11 +193,12 @@ __device__ __forceinline__ int poisson_bucket(uint64_t s0, uint64_t time_step, d
 // events 0 and 1 use d2 and d3, further events draw their samples here.
 __device__ __forceinline__ int poisson_bucket_drawn(uint64_t s0, uint64_t d1, uint64_t d2, uint64_t d3,
                                                     uint64_t time_step, long long time_bits,
-                                                    const SimParams &p, long long &best_bits) {
+                                                    const SimParams &p, const PoissonConsts &pc,
+                                                    long long &best_bits) {
     const double step_start = __ull2double_rn(time_step);
     const long long e0 = event_time_bits(step_start, d2, p.delta_t);
     const long long e1 = event_time_bits(step_start, d3, p.delta_t);
-    const uint32_t n_events = poisson_count(d1, p);
+    const uint32_t n_events = poisson_count(d1, pc);
     int best_k = -1;
     long long bb = 0;
     if (n_events >= 1 && e0 > time_bits) {
@@ -223,14 +224,14 @@ __device__ __forceinline__ int poisson_bucket_drawn(uint64_t s0, uint64_t d1, ui
 // (the second speculatively) from the shared location term.  Returns the
 // event time, the re-prime time index and the re-primed state.
 __device__ __forceinline__ double poisson_next_event_time_ilp(uint64_t loc_term, double time,
-                                                              const SimParams &p,
+                                                              const SimParams &p, const PoissonConsts &pc,
                                                               uint64_t &reprime,
                                                               uint64_t &reprimed_state) {
     const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
     uint64_t time_step = f64_to_u64(floor(q));
     for (;;) {
         double best = 0.0;
-        const int k = poisson_bucket(primed_state(loc_term, time_step), time_step, time, p, best);
+        const int k = poisson_bucket(primed_state(loc_term, time_step), time_step, time, p, pc, best);
         if (k >= 0) {
             reprime = time_step + kInvPhi * (uint64_t)(k + 1);
             reprimed_state = primed_state(loc_term, reprime);
@@ -245,7 +246,7 @@ __device__ __forceinline__ double poisson_next_event_time_ilp(uint64_t loc_term,
 // speculatively, with each bucket's first three samples drawn at once, so
 // the dependent chain per event is one prime, one draw and the compares.
 __device__ __forceinline__ double poisson_next_event_time_lat(uint64_t loc_term, double time,
-                                                              const SimParams &p,
+                                                              const SimParams &p, const PoissonConsts &pc,
                                                               uint64_t &reprime,
                                                               uint64_t &reprimed_state) {
     const double q = p.inv_delta_t != 0.0 ? __dmul_rn(time, p.inv_delta_t) : __ddiv_rn(time, p.delta_t);
@@ -258,10 +259,10 @@ __device__ __forceinline__ double poisson_next_event_time_lat(uint64_t loc_term,
         const uint64_t b1 = draw_at(s1, 1), b2 = draw_at(s1, 2), b3 = draw_at(s1, 3);
         long long bits = 0;
         uint64_t chosen = time_step;
-        int k = poisson_bucket_drawn(s0, a1, a2, a3, time_step, time_bits, p, bits);
+        int k = poisson_bucket_drawn(s0, a1, a2, a3, time_step, time_bits, p, pc, bits);
         if (k < 0) {
             chosen = time_step + 1;
-            k = poisson_bucket_drawn(s1, b1, b2, b3, chosen, time_bits, p, bits);
+            k = poisson_bucket_drawn(s1, b1, b2, b3, chosen, time_bits, p, pc, bits);
         }
         if (k >= 0) {
             reprime = chosen + kInvPhi * (uint64_t)(k + 1);
@@ -293,12 +294,13 @@ __device__ __forceinline__ uint64_t time_bucket(const SimParams &p, double time)
 // or past the bucket's end moves to the next bucket.  Returns the first
 // event time after `time` and its re-prime time index ts + j * INV_PHI.
 __device__ __forceinline__ double exp_continue(uint64_t loc_term, double time, const SimParams &p,
-                                               uint64_t ts, uint32_t j, double et, uint64_t &reprime) {
+                                               const PoissonConsts &pc, uint64_t ts, uint32_t j, double et,
+                                               uint64_t &reprime) {
     uint64_t s0 = primed_state(loc_term, ts);
     double slice_end = __dmul_rn(__ull2double_rn(ts + 1), p.delta_t);
     for (;;) {
         j += 1;
-        et = __dadd_rn(et, exp_sample(draw_at(s0, j), p.lambda));
+        et = __dadd_rn(et, exp_sample(draw_at(s0, j), pc.lambda));
         if (et >= slice_end) {
             ts += 1;
             j = 0;
@@ -315,9 +317,9 @@ __device__ __forceinline__ double exp_continue(uint64_t loc_term, double time, c
 
 // exp.rs:37-83 ExpEventTimeSampler::next_event_time_at_indexed_location_weakly_after
 __device__ __forceinline__ double exp_next_event_time(uint64_t loc_term, double time, const SimParams &p,
-                                                      uint64_t &reprime) {
+                                                      const PoissonConsts &pc, uint64_t &reprime) {
     const uint64_t ts = time_bucket(p, time);
-    return exp_continue(loc_term, time, p, ts, 0, __dmul_rn(__ull2double_rn(ts), p.delta_t), reprime);
+    return exp_continue(loc_term, time, p, pc, ts, 0, __dmul_rn(__ull2double_rn(ts), p.delta_t), reprime);
 }
 
 // ---- the samplers fed with pre-drawn samples ----

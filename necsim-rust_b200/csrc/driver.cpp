@@ -12,8 +12,9 @@
 // mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
 // which writes the configuration that resumes the run; rng Seed | Entropy;
 // the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle; Normal or Clark2Dt) and
-// SpatiallyExplicit (habitat and dispersal maps as (Geo)TIFF files or .npy
-// arrays, Uniform turnover, loading mode FixMe | OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
+// SpatiallyExplicit (habitat, dispersal and turnover maps as (Geo)TIFF files
+// or .npy arrays, Uniform(rate) or Map(path) turnover, loading mode FixMe |
+// OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
 // or CUDA(...) (exponential event times, the reference CUDA algorithm's
 // defaults) with Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
 // Counter, Execution (others are ignored with a notice); log EventLog(directory,
@@ -122,6 +123,7 @@ struct Run {
     uint64_t log_capacity = 1000000;
     std::vector<uint32_t> habitat;
     std::vector<double> dispersal;
+    std::vector<double> turnover;  // SpatiallyExplicit turnover map (when given)
     std::string summary;
 };
 
@@ -213,12 +215,16 @@ void parse_scenario(const Value &s, Run &r) {
         if (!disp) fail("missing field `dispersal`");
         sc.turnover_rate = 0.5;
         const Value *t = s.field("turnover") ? s.field("turnover") : s.field("turnover_rate");
+        const Value *tmap = nullptr;  // Map("path") (turnover/map.rs)
         if (t) {
             const std::string &tv = t->variant();
-            if (tv == "Map") fail("SpatiallyExplicit: turnover maps are not supported (uniform turnover only)");
-            if ((tv != "Uniform" && tv != "Rate" && tv != "UniformRate") || t->items.size() != 1)
-                fail("SpatiallyExplicit: turnover must be Uniform(rate)");
-            sc.turnover_rate = t->items[0].as_f64();
+            if (tv == "Map" && t->items.size() == 1) {
+                tmap = &t->items[0];
+            } else if ((tv == "Uniform" || tv == "Rate" || tv == "UniformRate") && t->items.size() == 1) {
+                sc.turnover_rate = t->items[0].as_f64();
+            } else {
+                fail("SpatiallyExplicit: turnover must be Uniform(rate) or Map(path)");
+            }
         }
         int32_t mode = NECSIM_MAPS_OFF_BY_ONE;  // MapLoadingMode::default (maps/mod.rs:84-88)
         const Value *m = s.field("mode") ? s.field("mode") : s.field("loading_mode");
@@ -229,14 +235,16 @@ void parse_scenario(const Value &s, Run &r) {
             else if (mv == "Strict") mode = NECSIM_MAPS_STRICT;
             else fail("SpatiallyExplicit: mode must be FixMe, OffByOne or Strict");
         }
-        std::vector<uint64_t> hs, ds;
+        std::vector<uint64_t> hs, ds, ts;
         r.dispersal = load_map<double>(disp->text, mode, ds);
+        if (tmap) r.turnover = load_map<double>(tmap->text, mode, ts);
         r.habitat = load_map<uint32_t>(hab->text, mode, hs);
         if (hs.size() != 2) fail("habitat must be a 2D (height, width) array");
         if (ds.size() != 2) fail("dispersal must be a 2D array");
+        if (tmap && ts != hs) fail("the turnover map must have the habitat map's dimensions");
         char err[512];
         const int rc = necsim_maps_fix(r.habitat.data(), (uint32_t)hs[1], (uint32_t)hs[0], r.dispersal.data(), ds[0],
-                                       ds[1], nullptr, mode, err, sizeof(err));
+                                       ds[1], tmap ? r.turnover.data() : nullptr, mode, err, sizeof(err));
         if (rc) fail(std::string("SpatiallyExplicit maps: ") + err);
         const uint64_t cells = hs[0] * hs[1];
         if (ds[0] != cells || ds[1] != cells) fail("dispersal must be (cells, cells)");
@@ -245,7 +253,9 @@ void parse_scenario(const Value &s, Run &r) {
         sc.width = (uint32_t)hs[1];
         sc.habitat = r.habitat.data();
         sc.dispersal = r.dispersal.data();
-        o << "SpatiallyExplicit(" << sc.width << "x" << sc.height << " map from " << hab->text << ")";
+        if (tmap) sc.turnover_map = r.turnover.data();
+        o << "SpatiallyExplicit(" << sc.width << "x" << sc.height << " map from " << hab->text
+          << (tmap ? ", turnover map " + tmap->text : std::string()) << ")";
     } else {
         fail("scenario " + k + " is not supported by this backend");
     }

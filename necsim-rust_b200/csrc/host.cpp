@@ -103,8 +103,12 @@ struct SimHost {
 void validate(const necsim_scenario &sc) {
     if (!(sc.speciation_probability > 0.0) || !(sc.speciation_probability <= 1.0))
         fail(NECSIM_E_INVALID_ARGUMENT, "speciation_probability must be in (0, 1]");
-    if (!(sc.turnover_rate > 0.0) || !std::isfinite(sc.turnover_rate))
+    if (sc.turnover_map) {
+        if (sc.kind != NECSIM_SPATIALLY_EXPLICIT)
+            fail(NECSIM_E_INVALID_ARGUMENT, "turnover maps apply to SpatiallyExplicit scenarios only");
+    } else if (!(sc.turnover_rate > 0.0) || !std::isfinite(sc.turnover_rate)) {
         fail(NECSIM_E_INVALID_ARGUMENT, "turnover_rate must be positive");
+    }
     switch (sc.kind) {
     case NECSIM_NON_SPATIAL:
         if (!sc.width || !sc.height || !sc.deme) fail(NECSIM_E_INVALID_ARGUMENT, "NonSpatial area and deme must be >= 1");
@@ -127,6 +131,18 @@ void validate(const necsim_scenario &sc) {
     case NECSIM_SPATIALLY_EXPLICIT:
         if (!sc.width || !sc.height || !sc.habitat || !sc.dispersal)
             fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyExplicit needs habitat and dispersal maps");
+        if (sc.turnover_map) {
+            // maps/mod.rs:34-53 (non-negative rates) and turnover_rate/in_memory.rs:50-72
+            // (InMemoryTurnoverRateError::ZeroTurnoverHabitat)
+            const uint64_t cells = (uint64_t)sc.width * sc.height;
+            for (uint64_t c = 0; c < cells; ++c) {
+                const double t = sc.turnover_map[c];
+                if (!(t >= 0.0) || !std::isfinite(t))
+                    fail(NECSIM_E_INVALID_ARGUMENT, "turnover rates must be finite and non-negative");
+                if (t == 0.0 && sc.habitat[c] != 0)
+                    fail(NECSIM_E_INVALID_ARGUMENT, "zero turnover at a habitable location (ZeroTurnoverHabitat)");
+            }
+        }
         break;
     default:
         fail(NECSIM_E_INVALID_ARGUMENT, "unknown scenario kind");
@@ -163,12 +179,47 @@ uint64_t division_magic(uint32_t d) {
     return ~0ULL / d + 1ULL;
 }
 
+// The samplers' constants for turnover rate lambda (poisson.rs:38-65,
+// exp.rs:43-49): exp(-lambda * delta_t) with the system libm like
+// IntrinsicsMathsCore, lambda * delta_t / k with the reference's IEEE
+// division, and the constant Devroye sequence as integer thresholds.
+PoissonConsts make_poisson_consts(double lambda, double delta_t) {
+    PoissonConsts c;
+    std::memset(&c, 0, sizeof(c));
+    c.lambda = lambda;
+    c.lambda_dt = lambda * delta_t;  // poisson.rs:40
+    const double p0 = std::exp(-c.lambda_dt);  // poisson.rs:42
+    for (int k = 1; k <= kPoissonTable; ++k) c.lambda_dt_over_k[k - 1] = c.lambda_dt / (double)k;
+    double prod = p0, acc = p0;
+    for (int n = 0; n < kPoissonThresholds; ++n) {
+        // a rank whose prod is 0 stops the loop whatever the sample: its
+        // threshold is the largest u64, which no 53-bit X exceeds, so the
+        // count of exceeded thresholds is the loop's stopping rank
+        c.threshold[n] = prod > 0.0 ? (uint64_t)std::floor(std::ldexp(acc, 53)) : ~0ULL;
+        if (prod > 0.0) c.alive |= 1u << n;
+        prod = prod * (c.lambda_dt / (double)(n + 1));
+        acc = acc + prod;
+    }
+    c.prod_k = prod;
+    c.acc_k = acc;
+    return c;
+}
+
 SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64_t wy_seed) {
     SimParams p;
     std::memset(&p, 0, sizeof(p));
     p.seed = wy_seed;
     p.nu = sc.speciation_probability;
     p.lambda = sc.turnover_rate;
+    if (sc.kind == NECSIM_SPATIALLY_EXPLICIT && sc.turnover_map) {
+        // a turnover map: the rounds advance at the largest habitable rate
+        // (the samplers read each cell's own constants)
+        const uint64_t cells = (uint64_t)sc.width * sc.height;
+        double top = 0.0;
+        for (uint64_t c = 0; c < cells; ++c)
+            if (sc.habitat[c] != 0 && sc.turnover_map[c] > top) top = sc.turnover_map[c];
+        p.lambda = top;
+    }
     p.delta_t = args.delta_t;
     p.lambda_dt = p.lambda * p.delta_t;  // poisson.rs:40
     p.p0 = std::exp(-p.lambda_dt);       // poisson.rs:42, system libm like IntrinsicsMathsCore
@@ -193,25 +244,7 @@ SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64
     int exp2 = 0;
     const double mant = std::frexp(p.delta_t, &exp2);
     p.inv_delta_t = (mant == 0.5) ? 1.0 / p.delta_t : 0.0;
-    // lambda * delta_t / k for the first Poisson ranks (poisson.rs:58),
-    // divided here with the same IEEE division the reference performs
-    for (int k = 1; k <= kPoissonTable; ++k) p.lambda_dt_over_k[k - 1] = p.lambda_dt / (double)k;
-    // the constant Devroye sequence (poisson.rs:51-65) as integer thresholds
-    {
-        double prod = p.p0, acc = p.p0;
-        p.poisson_alive = 0;
-        for (int n = 0; n < kPoissonThresholds; ++n) {
-            // a rank whose prod is 0 stops the loop whatever the sample: its
-            // threshold is the largest u64, which no 53-bit X exceeds, so the
-            // count of exceeded thresholds is the loop's stopping rank
-            p.poisson_threshold[n] = prod > 0.0 ? (uint64_t)std::floor(std::ldexp(acc, 53)) : ~0ULL;
-            if (prod > 0.0) p.poisson_alive |= 1u << n;
-            prod = prod * (p.lambda_dt / (double)(n + 1));
-            acc = acc + prod;
-        }
-        p.poisson_prod_k = prod;
-        p.poisson_acc_k = acc;
-    }
+    p.pois = make_poisson_consts(p.lambda, p.delta_t);
     // u < c  <=>  X < ceil(c * 2^53) for the 53-bit integer X of the uniform
     p.nu_threshold = (uint64_t)std::ceil(std::ldexp(sc.speciation_probability, 53));
     p.migration_threshold = (uint64_t)std::ceil(std::ldexp(sc.migration_probability, 53));
@@ -335,6 +368,7 @@ struct Engine {
     unsigned *order_hist = nullptr;
     uint32_t *order = nullptr;
     std::vector<float *> d_entropy;  // SE: per-cell dispersal entropy, one per table set
+    std::vector<PoissonConsts *> d_turnover;  // SE turnover maps: per-cell sampler constants
 
     // dispersal reporting: events drained and delivered after every round
     Delivery *delivery = nullptr;
@@ -389,9 +423,12 @@ struct Engine {
             if (p) cudaFree(p);
         for (auto p : d_entropy)
             if (p) cudaFree(p);
+        for (auto p : d_turnover)
+            if (p) cudaFree(p);
         d_cells.clear();
         d_atoms.clear();
         d_entropy.clear();
+        d_turnover.clear();
         void *lptrs[] = {order_keys, order_hist, order, trace_rows, trace_deaths, trace_counts};
         for (void *p : lptrs)
             if (p) cudaFree(p);
@@ -438,6 +475,17 @@ void upload_tables(Engine &E, SimHost &s) {
     s.params.cell_entropy = de;
     s.params.n_cells = t.cells.size();
     s.params.n_atoms = t.atoms.size();
+    if (s.sc.turnover_map) {
+        // the samplers' constants of every cell (InMemoryTurnoverRate)
+        const uint64_t cells = (uint64_t)s.sc.width * s.sc.height;
+        std::vector<PoissonConsts> tc(cells);
+        for (uint64_t c = 0; c < cells; ++c) tc[c] = make_poisson_consts(s.sc.turnover_map[c], s.params.delta_t);
+        PoissonConsts *dt = dev_alloc<PoissonConsts>(cells);
+        E.d_turnover.push_back(dt);
+        CK(cudaMemcpy(dt, tc.data(), cells * sizeof(PoissonConsts), cudaMemcpyHostToDevice));
+        E.h2d_bytes += cells * sizeof(PoissonConsts);
+        s.params.turnover_cells = dt;
+    }
 }
 
 void setup_engine(Engine &E, const necsim_args &args) {
@@ -1194,6 +1242,7 @@ struct necsim_ctx {
     necsim_scenario scenario{};
     necsim_args args{};
     std::vector<uint32_t> habitat;  // owned copies of the SE maps' habitat
+    std::vector<double> turnover;   // and turnover map (when given)
     std::string error;
     Remaining remaining;
     bool tables_ready = false;
@@ -1315,6 +1364,7 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
                 sh.params.n_cells = (*prebuilt_tables)[s].n_cells;
                 sh.params.n_atoms = (*prebuilt_tables)[s].n_atoms;
                 sh.params.cell_entropy = (*prebuilt_tables)[s].cell_entropy;
+                sh.params.turnover_cells = (*prebuilt_tables)[s].turnover_cells;
             } else {
                 upload_tables(E, sh);
             }
@@ -1354,6 +1404,10 @@ int necsim_gpu_create(const necsim_scenario *scenario, const necsim_args *args, 
         if (scenario->kind == NECSIM_SPATIALLY_EXPLICIT) {
             const uint64_t cells = (uint64_t)scenario->width * scenario->height;
             ctx->habitat.assign(scenario->habitat, scenario->habitat + cells);
+            if (scenario->turnover_map) {
+                ctx->turnover.assign(scenario->turnover_map, scenario->turnover_map + cells);
+                ctx->scenario.turnover_map = ctx->turnover.data();
+            }
             // tables are built and uploaded once per context
             ctx->engine.reset(new Engine());
             setup_engine(*ctx->engine, ctx->args);

@@ -63,6 +63,15 @@ __device__ __forceinline__ uint64_t lane_injection(const Lane &l, const SimParam
     return l.rec.injection + (uint64_t)l.i;                                          // in_memory.rs:70-80
 }
 
+// The event-time samplers' constants at the lineage's location: per cell
+// under a SpatiallyExplicit turnover map (turnover_rate/in_memory.rs:22-40,
+// the cell of a loaded lineage is in range), else the simulation's.
+template <int KIND>
+__device__ __forceinline__ const PoissonConsts &poisson_consts(const Lane &l, const SimParams &p) {
+    if (KIND == kSpatiallyExplicit && p.turnover_cells) return p.turnover_cells[(uint64_t)l.y * p.width + l.x];
+    return p.pois;
+}
+
 __device__ __forceinline__ bool load_cell(const SimParams &p, uint32_t x, uint32_t y, CellRecord &rec,
                                           uint32_t *status) {
     const uint64_t cell = (uint64_t)y * p.width + (uint64_t)x;
@@ -263,16 +272,17 @@ __device__ __forceinline__ int lineage_step(Lane &l, const SimParams &p, const E
     const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
     uint64_t rs;  // WyHash state re-primed for the event
     if (!l.has_next) {
+        const PoissonConsts &pc = poisson_consts<KIND>(l, p);
         // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
         // (active_lineage_sampler/independent/sampler.rs:69-116)
         const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
         double t;
         if (EXP) {
-            t = exp_next_event_time(loc_term, before, p, l.reprime);
+            t = exp_next_event_time(loc_term, before, p, pc, l.reprime);
             rs = primed_state(loc_term, l.reprime);
         } else {
-            t = LAT ? poisson_next_event_time_lat(loc_term, before, p, l.reprime, rs)
-                    : poisson_next_event_time_ilp(loc_term, before, p, l.reprime, rs);
+            t = LAT ? poisson_next_event_time_lat(loc_term, before, p, pc, l.reprime, rs)
+                    : poisson_next_event_time_ilp(loc_term, before, p, pc, l.reprime, rs);
         }
         l.next = max_after(before, t);
         l.has_next = true;
@@ -326,7 +336,7 @@ constexpr long long kNoEvent = 0x7fffffffffffffffLL;
 // samples, so a decided bucket hands the event its samples at once
 // (drawn = true); the sequential continuation leaves them undrawn.
 __device__ __forceinline__ double exp_search_coop(uint64_t loc_term, double time, const SimParams &p,
-                                                  uint64_t &reprime, uint64_t &rs, uint64_t &e1, uint64_t &e2,
+                                                  const PoissonConsts &pc, uint64_t &reprime, uint64_t &rs, uint64_t &e1, uint64_t &e2,
                                                   uint64_t &e3, uint64_t &e4, bool &drawn) {
     const unsigned lane = threadIdx.x & 31u;
     const unsigned first = lane & ~7u;  // the bucket's first lane
@@ -334,7 +344,7 @@ __device__ __forceinline__ double exp_search_coop(uint64_t loc_term, double time
     for (;;) {
         const uint64_t ts = base + (lane >> 3);
         const uint64_t mine = (uint64_t)(lane & 7u) + 1u;  // this lane's sample of the bucket
-        const double e = exp_sample(draw_at(primed_state(loc_term, ts), (uint32_t)mine), p.lambda);
+        const double e = exp_sample(draw_at(primed_state(loc_term, ts), (uint32_t)mine), pc.lambda);
         const uint64_t sc = primed_state(loc_term, ts + kInvPhi * mine);
         const uint64_t c1 = draw_at(sc, 1), c2 = draw_at(sc, 2), c3 = draw_at(sc, 3), c4 = draw_at(sc, 4);
         const double slice_end = __dmul_rn(__ull2double_rn(ts + 1), p.delta_t);
@@ -373,7 +383,7 @@ __device__ __forceinline__ double exp_search_coop(uint64_t loc_term, double time
                 return et_l;
             }
             drawn = false;
-            return exp_continue(loc_term, time, p, ts_l, 8u, et_l, reprime);
+            return exp_continue(loc_term, time, p, pc, ts_l, 8u, et_l, reprime);
         }
         base += 4;
     }
@@ -398,11 +408,13 @@ template <int KIND, bool EXP = false>
 __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, const EventSink &k) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t loc_term = location_term(p.seed, lane_injection<KIND>(l, p));
+    const PoissonConsts &pc = poisson_consts<KIND>(l, p);
     uint64_t rs, e1, e2, e3, e4;
     bool drawn = false;
     if (EXP && !l.has_next) {
         const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
-        l.next = max_after(before, exp_search_coop(loc_term, before, p, l.reprime, rs, e1, e2, e3, e4, drawn));
+        l.next = max_after(before,
+                           exp_search_coop(loc_term, before, p, pc, l.reprime, rs, e1, e2, e3, e4, drawn));
         l.has_next = true;
     }
     if (!l.has_next) {
@@ -422,7 +434,7 @@ __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, co
             const uint64_t s = primed_state(loc_term, tindex);
             const uint64_t d = draw_at(s, role + 1u);
             // bucket lanes: the Devroye count from role 0, shared in the bucket
-            const uint32_t n_own = poisson_count(d, p);
+            const uint32_t n_own = poisson_count(d, pc);
             const uint32_t n_ev = __shfl_sync(kFull, n_own, (int)(lane & ~3u));
             long long mine = kNoEvent;
             uint32_t mine_k = 0xffffffffu;
@@ -589,7 +601,8 @@ __device__ __forceinline__ int pass_run(Lane &l, const SimParams &p, const Event
     if (ps.searching) {
         // poisson.rs:48-100: the first bucket with an event after `before`
         long long bits = 0;
-        const int kk = poisson_bucket_drawn(st, d1, d2, d3, ps.ts, __double_as_longlong(ps.before), p, bits);
+        const int kk = poisson_bucket_drawn(st, d1, d2, d3, ps.ts, __double_as_longlong(ps.before), p,
+                                            poisson_consts<KIND>(l, p), bits);
         if (kk < 0) {
             ps.ts += 1;
             return kPassSearch;

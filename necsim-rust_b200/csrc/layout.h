@@ -47,21 +47,34 @@ static_assert(sizeof(AliasAtom) == 16, "AliasAtom must be 16 bytes");
 constexpr int kPoissonTable = 16;
 constexpr int kPoissonThresholds = 8;
 
-// Per-simulation scalars, read by every lineage of the simulation.
+// The event-time samplers' constants for one turnover rate lambda: the
+// exponential sampler's lambda and the Poisson sampler's Devroye sequence.
 //
 // Comparisons of a uniform u = X * 2^-53 (X the 53-bit integer of a draw)
 // with a constant c are done on integers: u > c  <=>  X > floor(c * 2^53) and
 // u < c  <=>  X < ceil(c * 2^53), both exact (scaling by 2^53 is exact).
-struct alignas(16) SimParams {
-    double lambda_dt_over_k[kPoissonTable];  // lambda_dt / k, k = 1..16
+struct alignas(16) PoissonConsts {
     // Devroye's loop (poisson.rs:51-65) visits the constant sequence
     // acc_n = acc_{n-1} + prod_n, prod_n = prod_{n-1} * (lambda_dt / n); the
-    // draw continues past rank n iff X > poisson_threshold[n] (and prod_n > 0)
-    uint64_t poisson_threshold[kPoissonThresholds];  // floor(acc_n * 2^53)
-    uint32_t poisson_alive;   // bit n: prod_n > 0
-    uint32_t pad0;
-    double poisson_prod_k;    // prod_n and acc_n at n = kPoissonThresholds
-    double poisson_acc_k;
+    // draw continues past rank n iff X > threshold[n] (and prod_n > 0)
+    uint64_t threshold[kPoissonThresholds];  // floor(acc_n * 2^53)
+    uint32_t alive;           // bit n: prod_n > 0
+    uint32_t pad;
+    double prod_k;            // prod_n and acc_n at n = kPoissonThresholds
+    double acc_k;
+    double lambda;            // turnover rate
+    double lambda_dt;         // lambda * delta_t   (poisson.rs:40)
+    double lambda_dt_over_k[kPoissonTable];  // lambda_dt / k, k = 1..16
+};
+static_assert(sizeof(PoissonConsts) % 16 == 0, "PoissonConsts must be whole 16-byte words");
+
+// Per-simulation scalars, read by every lineage of the simulation.
+struct alignas(16) SimParams {
+    PoissonConsts pois;       // the samplers' constants under uniform turnover
+    // SpatiallyExplicit with a turnover map (turnover_rate/in_memory.rs): the
+    // constants of every cell, row-major (nullptr: uniform turnover, `pois`)
+    const PoissonConsts *turnover_cells;
+    uint64_t pad4;
     uint64_t nu_threshold;    // ceil(nu * 2^53): speciation iff X < this
     uint64_t migration_threshold;  // ceil(migration * 2^53)
     // ceil(2^64 / d) for d = width and d = meta_width (0 when d == 1): a
@@ -72,10 +85,10 @@ struct alignas(16) SimParams {
     double inv_delta_t;       // 1 / delta_t if delta_t is a power of two, else 0
     uint64_t seed;            // WyHash seed word
     double nu;                // speciation probability
-    double lambda;            // uniform turnover rate
+    double lambda;            // the rounds' rate: the turnover rate, or the largest habitable one of a map
     double delta_t;
-    double lambda_dt;         // lambda * delta_t
-    double p0;                // exp(-lambda * delta_t), host libm
+    double lambda_dt;         // lambda * delta_t (uniform turnover)
+    double p0;                // exp(-lambda * delta_t), host libm (uniform turnover)
     double migration;         // SI
     double sigma;             // AlmostInfinite
     double min_event_time;    // resume time (0 for a fresh start)

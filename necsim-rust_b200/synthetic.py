@@ -130,4 +130,6 @@ def to_scenario(desc):
     if k == 4:
         return nb.AlmostInfinite(nb.Circle(desc["radius"], (desc["centre_x"], desc["centre_y"])),
                                  nb.Clark2Dt(desc["shape_u"], desc["tail_p"]))
-    return nb.SpatiallyExplicit(desc["habitat"], desc["dispersal"], desc.get("turnover_rate", 0.5))
+    turnover = desc.get("turnover_map")
+    return nb.SpatiallyExplicit(desc["habitat"], desc["dispersal"],
+                                turnover if turnover is not None else desc.get("turnover_rate", 0.5))

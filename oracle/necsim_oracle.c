@@ -194,6 +194,7 @@ typedef struct sim_t {
     double sigma;
     int clark;          /* AlmostInfinite with Clark2Dt dispersal */
     int exp_sampler;    /* ExpEventTimeSampler instead of the Poisson one */
+    const double *turnover;  /* SE turnover map (InMemoryTurnoverRate), NULL: uniform lambda */
     double shape_u, tail_p;
     extent_t local;     /* NonSpatial / SI local / SE map extent */
     uint32_t deme;
@@ -257,24 +258,34 @@ static inline double speciation_probability(const sim_t *s, uint32_t x, uint32_t
     return s->nu;
 }
 
-/* event_time_sampler/poisson.rs:30-109 */
-static double poisson_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out) {
+/* turnover_rate/uniform.rs, turnover_rate/in_memory.rs:22-40 (a cell
+ * outside the map has rate 0) */
+static inline double turnover_at(const sim_t *s, uint32_t x, uint32_t y) {
+    if (!s->turnover) return s->lambda;
+    uint64_t cell = (uint64_t)y * s->local.w + (uint64_t)x;
+    return cell < s->local.w * s->local.h ? s->turnover[cell] : 0.0;
+}
+
+/* event_time_sampler/poisson.rs:30-109, at a location with turnover rate lam */
+static double poisson_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out, double lam) {
     rng_t *g = &s->rng;
+    const double lambda_dt = s->turnover ? lam * s->delta_t : s->lambda_dt;  /* poisson.rs:40 */
+    const double p0 = s->turnover ? exp(-lambda_dt) : s->p0;                  /* poisson.rs:42 */
     uint64_t time_step = f64_as_u64(floor(time / s->delta_t));
     double event_time;
     uint32_t event_index;
     for (;;) {
         rng_prime(g, inj, time_step);
         uint32_t n_events;
-        if (s->p0 > 0.0) {
+        if (p0 > 0.0) {
             /* Devroye inversion of Poisson(lambda * delta_t) */
             uint32_t poisson = 0;
-            double prod = s->p0;
-            double acc = s->p0;
+            double prod = p0;
+            double acc = p0;
             double u = u01_closed_open(g);
             while (u > acc && prod > 0.0) {
                 poisson += 1;
-                prod *= s->lambda_dt / (double)poisson;
+                prod *= lambda_dt / (double)poisson;
                 acc += prod;
             }
             n_events = poisson;
@@ -285,7 +296,7 @@ static double poisson_next_event_time(sim_t *s, uint64_t inj, double time, uint6
             double r = sqrt(-2.0 * log(u0));
             double theta = -6.283185307179586 * u1;
             double z0 = r * sin(theta);
-            double v = z0 * sqrt(s->lambda_dt) + s->lambda_dt;
+            double v = z0 * sqrt(lambda_dt) + lambda_dt;
             n_events = f64_as_u32(v > 0.0 ? v : 0.0);
         }
         int found = 0;
@@ -316,7 +327,7 @@ static double poisson_next_event_time(sim_t *s, uint64_t inj, double time, uint6
 
 /* event_time_sampler/exp.rs:37-83 ExpEventTimeSampler, with
  * rng.rs:163-167 sample_exponential = -ln(U(0,1]) / lambda */
-static double exp_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out) {
+static double exp_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out, double lam) {
     rng_t *g = &s->rng;
     uint64_t time_step = f64_as_u64(floor(time / s->delta_t));
     double event_time = (double)time_step * s->delta_t;
@@ -324,7 +335,7 @@ static double exp_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t 
     uint64_t sub_index = 0;
     rng_prime(g, inj, time_step);
     for (;;) {
-        event_time += -necsim_ln(u01_open_closed(g)) / s->lambda;
+        event_time += -necsim_ln(u01_open_closed(g)) / lam;
         sub_index += INV_PHI_U64;
         /* the time slice is exclusive at time_slice_end */
         if (event_time >= time_slice_end) {
@@ -343,9 +354,9 @@ static double exp_next_event_time(sim_t *s, uint64_t inj, double time, uint64_t 
     return event_time;
 }
 
-static double next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out) {
-    return s->exp_sampler ? exp_next_event_time(s, inj, time, reprime_out)
-                          : poisson_next_event_time(s, inj, time, reprime_out);
+static double next_event_time(sim_t *s, uint64_t inj, double time, uint64_t *reprime_out, double lam) {
+    return s->exp_sampler ? exp_next_event_time(s, inj, time, reprime_out, lam)
+                          : poisson_next_event_time(s, inj, time, reprime_out, lam);
 }
 
 /* dispersal_sampler/non_spatial.rs:42-66 */
@@ -711,6 +722,24 @@ static int sim_init(sim_t *s, const oracle_scenario *sc, const oracle_args *args
     }
     s->rng.seed = oracle_seed_from_u64(seed);
     s->rng.state = s->rng.seed;
+    if (sc->turnover) {
+        /* turnover/map.rs: SpatiallyExplicit only; rates >= 0 (maps/mod.rs:34-53),
+         * > 0 on habitable cells (turnover_rate/in_memory.rs:50-72); the canonical
+         * rounds advance at the largest habitable rate */
+        if (sc->kind != ORACLE_SPATIALLY_EXPLICIT || !sc->habitat) return -2;
+        uint64_t cells = (uint64_t)sc->width * sc->height;
+        double top = 0.0;
+        for (uint64_t c = 0; c < cells; ++c) {
+            double t = sc->turnover[c];
+            if (!(t >= 0.0) || !isfinite(t)) return -2;
+            if (t == 0.0 && sc->habitat[c] != 0) return -2;
+            if (sc->habitat[c] != 0 && t > top) top = t;
+        }
+        s->turnover = sc->turnover;
+        s->lambda = top;
+        s->lambda_dt = s->lambda * s->delta_t;
+        s->p0 = exp(-s->lambda_dt);
+    }
     if (!(s->lambda > 0.0) || !(s->delta_t > 0.0)) return -2;
     switch (sc->kind) {
     case ORACLE_NON_SPATIAL:
@@ -1035,7 +1064,7 @@ static int run_slice(sim_t *s, lineage_t *lin, double min_event_time, uint64_t s
         double before = lin->last > min_event_time ? lin->last : min_event_time;
         uint64_t inj = injection(s, lin->x, lin->y, lin->i);
         rng_t saved = s->rng;
-        double t = next_event_time(s, inj, before, NULL);
+        double t = next_event_time(s, inj, before, NULL, turnover_at(s, lin->x, lin->y));
         double next = max_after(before, t);
         o->peeked = 1;
         o->next = next;
@@ -1201,9 +1230,9 @@ static int simulate_reference(sim_t *s, const oracle_args *args, lineage_t *init
         for (uint64_t j = 0; j < slow.n; ++j) {
             const lineage_t *l = &slow.v[(slow.head + j) % slow.cap].lin;
             if (args->report_dispersal)
-                rate = rate + s->lambda;
+                rate = rate + turnover_at(s, l->x, l->y);
             else
-                rate = rate + s->lambda * speciation_probability(s, l->x, l->y);
+                rate = rate + turnover_at(s, l->x, l->y) * speciation_probability(s, l->x, l->y);
         }
         level = level + (double)event_slice / rate;
         if (has_pause && pause_before < level) level = pause_before;
@@ -1512,7 +1541,7 @@ double oracle_poisson_next_event_time(uint64_t seed, uint64_t inj, double t, dou
     s.delta_t = delta_t;
     s.lambda_dt = lambda * delta_t;
     s.p0 = exp(-s.lambda_dt);
-    return poisson_next_event_time(&s, inj, t, reprime);
+    return poisson_next_event_time(&s, inj, t, reprime, lambda);
 }
 
 double oracle_exp_next_event_time(uint64_t seed, uint64_t inj, double t, double lambda,
@@ -1523,7 +1552,7 @@ double oracle_exp_next_event_time(uint64_t seed, uint64_t inj, double t, double 
     s.rng.state = seed;
     s.lambda = lambda;
     s.delta_t = delta_t;
-    return exp_next_event_time(&s, inj, t, reprime);
+    return exp_next_event_time(&s, inj, t, reprime, lambda);
 }
 
 void oracle_ln(const double *x, double *out, uint64_t n) {

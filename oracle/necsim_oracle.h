@@ -47,6 +47,7 @@ typedef struct oracle_scenario {
     const uint32_t *habitat;                  /* SE: width*height row-major */
     const double *dispersal;                  /* SE: (w*h) x (w*h) row-major */
     double shape_u, tail_p;                   /* AlmostInfinite Clark2Dt dispersal */
+    const double *turnover;                   /* SE turnover map, width*height row-major (NULL: uniform) */
 } oracle_scenario;
 
 enum { ORACLE_MODE_REFERENCE = 0, ORACLE_MODE_CANONICAL = 1 };

@@ -47,6 +47,7 @@ class OracleScenario(ctypes.Structure):
         ("dispersal", ctypes.POINTER(ctypes.c_double)),
         ("shape_u", ctypes.c_double),
         ("tail_p", ctypes.c_double),
+        ("turnover", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -205,6 +206,10 @@ def make_scenario(desc):
         h = np.ascontiguousarray(desc["habitat"], dtype=np.uint32)
         keep.append(h)
         sc.habitat = h.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+    if desc.get("turnover_map") is not None:
+        t = np.ascontiguousarray(desc["turnover_map"], dtype=np.float64)
+        keep.append(t)
+        sc.turnover = t.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     if desc.get("dispersal") is not None:
         d = np.ascontiguousarray(desc["dispersal"], dtype=np.float64)
         keep.append(d)
