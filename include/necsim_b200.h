@@ -376,6 +376,20 @@ int necsim_event_log_create(const char *directory, uint64_t segment_capacity, in
 necsim_reporter necsim_event_log_reporter(necsim_event_log *log);
 int necsim_event_log_close(necsim_event_log *log);
 
+/* Replays event-log segments (EventLogReplay, necsim/impls/std/src/
+ * event_log/replay/mod.rs; rustcoalescence replay): reads the segment files
+ * `segments[0..n)` -- `capacity` events at a time per segment -- and hands
+ * every event to `reporter` as one stream in PackedEvent order, speciation
+ * and dispersal batches interleaved as the stream requires.  Segments must
+ * agree on the kinds they record.  The reporters' needs (need_speciation,
+ * need_dispersal) are checked against the log as the replay's `mode` does:
+ * an unmet need fails when `strict` (ReplayMode::Strict) and is returned as
+ * a warning in `error` with NECSIM_OK otherwise (WarnOnly).  *n_events
+ * receives the number of events replayed. */
+int necsim_event_log_replay(const char *const *segments, uint64_t n_segments, uint64_t capacity,
+                            int32_t need_speciation, int32_t need_dispersal, int32_t strict,
+                            const necsim_reporter *reporter, uint64_t *n_events, char *error, size_t error_cap);
+
 /* ---- launch autotuner ----
  * Times a bounded sample of a batch -- every k-th simulation so that the
  * sample holds at most `max_sample_lineages` origins, each paused at

@@ -120,7 +120,8 @@ SYMBOLS = [
     "necsim_model_get_weights", "necsim_model_set_weights", "necsim_model_predict",
     "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
     "necsim_presample_origins", "necsim_gpu_autotune", "necsim_event_log_create",
-    "necsim_event_log_reporter", "necsim_event_log_close",
+    "necsim_event_log_reporter", "necsim_event_log_close", "necsim_event_log_replay", "necsim_map_load",
+    "necsim_map_free", "necsim_maps_fix",
 ]
 
 _lib = None
@@ -192,6 +193,9 @@ def lib():
     L.necsim_maps_fix.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, vp, u64, u64, vp, ctypes.c_int32,
                                   ctypes.c_char_p, ctypes.c_size_t]
     L.necsim_maps_fix.restype = ctypes.c_int
+    L.necsim_event_log_replay.argtypes = [vp, u64, u64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                          P(CReporter), P(u64), ctypes.c_char_p, ctypes.c_size_t]
+    L.necsim_event_log_replay.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
     L.necsim_model_create.restype = ctypes.c_int
     L.necsim_model_destroy.argtypes = [vp]
@@ -943,6 +947,47 @@ EVENT_LOG_HEADER_DTYPE = np.dtype([("min_time", "<f8"), ("max_time", "<f8"), ("l
 PACKED_EVENT_DTYPE = np.dtype([("gref", "<u8"), ("prior_time", "<f8"), ("event_time", "<f8"),
                                ("x", "<u4"), ("y", "<u4"), ("index", "<u4"),
                                ("tx", "<u4"), ("ty", "<u4"), ("tindex", "<u4"), ("coalescence", "<u8")])
+
+
+@dataclass
+class Replay:
+    """Events of a replayed event log, in PackedEvent order: speciation and
+    dispersal arrays, `delivery` the sequence of reporter calls
+    (("s" | "d", count)), `warning` the unmet-reporter-needs message of a
+    non-strict replay (empty otherwise)."""
+    speciation: np.ndarray
+    dispersal: np.ndarray
+    delivery: list
+    n_events: int
+    warning: str
+
+
+def replay_event_log(segments, capacity: int = 100_000, need_speciation: bool = False,
+                     need_dispersal: bool = False, strict: bool = True) -> Replay:
+    """Reads event-log segments back as one stream (EventLogReplay,
+    necsim/impls/std/src/event_log/replay/mod.rs).  `segments` are paths or
+    glob patterns (a pattern's matches in order, files only when several
+    match, the pattern itself when nothing matches, as replay/globbed.rs)."""
+    import glob as _glob
+    if isinstance(segments, (str, bytes, os.PathLike)):
+        segments = [segments]
+    paths = []
+    for pat in segments:
+        pat = os.fspath(pat)
+        found = sorted(_glob.glob(pat))
+        if len(found) > 1:
+            found = [f for f in found if os.path.isfile(f) or not os.path.exists(f)]
+        paths += found if found else [pat]
+    arr = (ctypes.c_char_p * len(paths))(*[os.fsencode(p) for p in paths])
+    col = _Collector()
+    n = ctypes.c_uint64(0)
+    err = ctypes.create_string_buffer(512)
+    rc = lib().necsim_event_log_replay(ctypes.cast(arr, ctypes.c_void_p), len(paths), capacity,
+                                       int(need_speciation), int(need_dispersal), int(strict),
+                                       ctypes.byref(col.struct), ctypes.byref(n), err, 512)
+    if rc != 0:
+        raise NecsimError(rc, err.value.decode())
+    return Replay(col.events(), col.dispersal_events(), list(col.kinds), n.value, err.value.decode())
 
 
 class EventLog:

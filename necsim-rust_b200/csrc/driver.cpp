@@ -7,6 +7,8 @@
 //
 //   necsim-b200 simulate <config.ron>   run on the GPU
 //   necsim-b200 check <config.ron>      parse and validate, print the run (no GPU)
+//   necsim-b200 replay <config.ron>     replay event-log segments through the
+//                                       reporters (no GPU)
 //
 // Supported: speciation; sample (percentage, origin Habitat | List,
 // mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
@@ -19,6 +21,9 @@
 // defaults) with Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
 // Counter, Execution (others are ignored with a notice); log EventLog(directory,
 // capacity) writes the reference's event log.
+#include <glob.h>
+#include <sys/stat.h>
+
 #include <cctype>
 #include <chrono>
 #include <cinttypes>
@@ -296,6 +301,8 @@ void parse_algorithm(const Value &a, Run &r) {
     }
 }
 
+void parse_reporters(const Value &root, Run &r);
+
 Run parse_config(const std::string &text) {
     Run r;
     const Value root = necsim::ron::parse(text);
@@ -361,6 +368,13 @@ Run parse_config(const std::string &text) {
     parse_scenario(need(root, "scenario"), r);
     r.sc.speciation_probability = r.speciation;
     if (const Value *a = root.field("algorithm")) parse_algorithm(*a, r);
+    parse_reporters(root, r);
+    r.args.report_dispersal = r.rep_counter ? 1 : 0;
+    return r;
+}
+
+// reporters: [Plugin(library: .., reporters: [Biodiversity(), ..]), ..]
+void parse_reporters(const Value &root, Run &r) {
     if (const Value *reps = root.field("reporters")) {
         std::vector<const Value *> names;
         for (const Value &p : reps->items) {
@@ -383,8 +397,6 @@ Run parse_config(const std::string &text) {
                 std::fprintf(stderr, "necsim-b200: reporter %s is not provided here and is ignored\n", v.c_str());
         }
     }
-    r.args.report_dispersal = r.rep_counter ? 1 : 0;
-    return r;
 }
 
 // the configuration with the remaining lineages as a List sample in Resume
@@ -586,14 +598,117 @@ int simulate(const std::string &path, bool run) {
     return 0;
 }
 
+// ---- replay (rustcoalescence/src/cli/replay.rs, args/cli/replay.rs) ----
+
+// The reporters of a replay: Biodiversity counts speciation events that
+// differ from the previous one by origin or event time (biodiversity.rs:33-41),
+// Counter the events by kind.
+struct ReplayCounts {
+    uint64_t biodiversity = 0, speciation = 0, self_dispersal = 0, out_dispersal = 0;
+    bool have_last = false;
+    necsim_speciation_event last{};
+};
+
+int replay_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
+    ReplayCounts &c = *static_cast<ReplayCounts *>(user);
+    for (uint64_t i = 0; i < n; ++i) {
+        c.speciation += 1;
+        const necsim_speciation_event &e = ev[i];
+        if (c.have_last && e.x == c.last.x && e.y == c.last.y && e.index == c.last.index &&
+            e.event_time == c.last.event_time)
+            continue;
+        c.last = e;
+        c.have_last = true;
+        c.biodiversity += 1;
+    }
+    return 0;
+}
+
+int replay_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
+    ReplayCounts &c = *static_cast<ReplayCounts *>(user);
+    for (uint64_t i = 0; i < n; ++i) {
+        if (ev[i].x == ev[i].target_x && ev[i].y == ev[i].target_y)
+            c.self_dispersal += 1;
+        else
+            c.out_dispersal += 1;
+    }
+    return 0;
+}
+
+// the segment files a pattern names (replay/globbed.rs): its matches in
+// order, files only when several match, or the pattern itself when nothing
+// matches
+std::vector<std::string> expand_segments(const std::string &pattern) {
+    std::vector<std::string> out;
+    glob_t g;
+    std::memset(&g, 0, sizeof(g));
+    const int rc = glob(pattern.c_str(), 0, nullptr, &g);
+    if (rc == 0 && g.gl_pathc == 1) {
+        out.push_back(g.gl_pathv[0]);
+    } else if (rc == 0) {
+        for (size_t i = 0; i < g.gl_pathc; ++i) {
+            struct stat st;
+            if (stat(g.gl_pathv[i], &st) != 0 || S_ISREG(st.st_mode)) out.push_back(g.gl_pathv[i]);
+        }
+    } else {
+        out.push_back(pattern);
+    }
+    globfree(&g);
+    return out;
+}
+
+int replay(const std::string &path) {
+    const Value root = necsim::ron::parse(slurp(path));
+    const Value *log = root.field("log") ? root.field("log") : root.field("event_log");
+    if (!log) fail("missing field `log`");
+    std::vector<std::string> segs;
+    for (const Value &p : need(*log, "segments").items)
+        for (const std::string &s : expand_segments(p.text)) segs.push_back(s);
+    uint64_t capacity = 100000;  // default_event_log_replay_segment_capacity
+    if (const Value *c = log->field("capacity")) capacity = c->as_u64();
+    bool strict = true;
+    if (const Value *m = root.field("mode")) {
+        if (m->variant() == "WarnOnly") strict = false;
+        else if (m->variant() != "Strict") fail("replay mode must be Strict or WarnOnly");
+    }
+    Run r;
+    parse_reporters(root, r);
+    std::printf("necsim-b200: replaying %zu event log segment(s)\n", segs.size());
+    std::vector<const char *> ptrs;
+    for (const std::string &s : segs) ptrs.push_back(s.c_str());
+    ReplayCounts counts;
+    necsim_reporter rep{&counts, replay_speciation, replay_dispersal};
+    char err[512];
+    uint64_t n = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    const int rc = necsim_event_log_replay(ptrs.data(), ptrs.size(), capacity, r.rep_biodiversity ? 1 : 0,
+                                           r.rep_counter ? 1 : 0, strict ? 1 : 0, &rep, &n, err, sizeof(err));
+    const auto t1 = std::chrono::steady_clock::now();
+    if (rc) fail(std::string("replay failed: ") + err);
+    if (err[0]) std::fprintf(stderr, "necsim-b200: warning: %s\n", err);
+    std::printf("necsim-b200: replayed %" PRIu64 " events\n", n);
+    if (r.rep_biodiversity && counts.biodiversity > 0)
+        std::printf("The simulation resulted in a biodiversity of %" PRIu64 " unique species.\n", counts.biodiversity);
+    if (r.rep_counter)
+        std::printf("Event Summary:\n - Speciation:\n    %" PRIu64 "\n - Dispersal (raw):\n   - same location:\n"
+                    "     %" PRIu64 "\n   - new location:\n     %" PRIu64 "\n",
+                    counts.speciation, counts.self_dispersal, counts.out_dispersal);
+    if (r.rep_execution)
+        std::printf("The replay took %.3f ms\n", std::chrono::duration<double, std::milli>(t1 - t0).count());
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
-    if (argc != 3 || (std::strcmp(argv[1], "simulate") != 0 && std::strcmp(argv[1], "check") != 0)) {
-        std::fprintf(stderr, "usage: necsim-b200 simulate|check <config.ron>\n");
+    const bool known = argc == 3 && (std::strcmp(argv[1], "simulate") == 0 || std::strcmp(argv[1], "check") == 0 ||
+                                      std::strcmp(argv[1], "replay") == 0);
+    if (!known) {
+        std::fprintf(stderr, "usage: necsim-b200 simulate|check|replay <config.ron>\n");
         return 2;
     }
     try {
+        if (std::strcmp(argv[1], "replay") == 0) return replay(argv[2]);
         return simulate(argv[2], std::strcmp(argv[1], "simulate") == 0);
     } catch (const Fail &f) {
         std::fprintf(stderr, "necsim-b200: %s\n", f.msg.c_str());

@@ -17,13 +17,19 @@
 // -- p(+) e(-) with coalescence = the lineage.  Each segment is sorted by
 // PackedEvent::cmp (event.rs:256-280) before it is written, segments are
 // numbered 0, 1, ... in a directory that must not exist yet.
+//
+// The replay (event_log/replay/*.rs) reads any set of segments back as one
+// stream in PackedEvent order: segments are chained into groups of
+// time-disjoint segments, the groups merged on their next events.
 #include <sys/stat.h>
 #include <unistd.h>
 
 #include <algorithm>
 #include <cerrno>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -204,3 +210,229 @@ int necsim_event_log_close(necsim_event_log *log) {
 }
 
 }  // extern "C"
+
+// ---- replay: necsim/impls/std/src/event_log/replay/{mod,segment,sorted_segments}.rs ----
+namespace {
+
+// A segment read lazily, `capacity` events at a time (segment.rs:35-133).
+struct ReplaySegment {
+    std::string path;
+    FILE *f = nullptr;
+    double min_time = 0.0, max_time = 0.0;
+    uint64_t length = 0, consumed = 0;
+    bool with_speciation = false, with_dispersal = false;
+    std::vector<Packed> buf;
+    size_t pos = 0;
+    uint64_t capacity = 1;
+
+    ~ReplaySegment() {
+        if (f) std::fclose(f);
+    }
+
+    // the next event, or false at the end (a truncated file ends early, as
+    // the reference's failing deserialisation does)
+    bool next(Packed &e) {
+        if (pos == buf.size()) {
+            if (!f || consumed >= length) return false;
+            const uint64_t want = std::min<uint64_t>(capacity, length - consumed);
+            buf.resize(want);
+            const size_t got = std::fread(buf.data(), sizeof(Packed), want, f);
+            buf.resize(got);
+            consumed += got;
+            pos = 0;
+            if (got < want) length = consumed;
+            if (got == 0) return false;
+        }
+        e = buf[pos++];
+        return true;
+    }
+};
+
+// A chain of time-disjoint segments read one after the other
+// (sorted_segments.rs:41-90), with its next event.
+struct ReplayGroup {
+    std::vector<ReplaySegment *> segs;
+    size_t k = 0;
+    Packed next{};
+    bool has = false;
+
+    void advance() {
+        has = false;
+        while (k < segs.size()) {
+            if (segs[k]->next(next)) {
+                has = true;
+                return;
+            }
+            ++k;
+        }
+    }
+};
+
+struct ReplaySink {
+    const necsim_reporter *rep;
+    std::vector<necsim_speciation_event> spec;
+    std::vector<necsim_dispersal_event> disp;
+
+    int flush() {
+        int rc = 0;
+        if (!spec.empty() && rep->report_speciation) rc = rep->report_speciation(rep->user, spec.data(), spec.size());
+        spec.clear();
+        if (rc) return rc;
+        if (!disp.empty() && rep->report_dispersal) rc = rep->report_dispersal(rep->user, disp.data(), disp.size());
+        disp.clear();
+        return rc;
+    }
+
+    // PackedEvent -> TypedEvent (event.rs:186-240): prior negative and event
+    // positive is a speciation, every other sign pair a dispersal (the
+    // interaction the signs encode is not carried by necsim_dispersal_event)
+    int push(const Packed &e) {
+        const bool prior_neg = std::signbit(e.prior), event_neg = std::signbit(e.event);
+        const double prior = with_sign(e.prior, false), event = with_sign(e.event, false);
+        if (prior_neg && !event_neg) {
+            if (!disp.empty() && flush()) return 1;
+            necsim_speciation_event s{};
+            s.global_lineage_reference = e.gref;
+            s.prior_time = prior;
+            s.event_time = event;
+            s.x = e.ox;
+            s.y = e.oy;
+            s.index = e.oi;
+            spec.push_back(s);
+        } else {
+            if (!spec.empty() && flush()) return 1;
+            necsim_dispersal_event d{};
+            d.global_lineage_reference = e.gref;
+            d.prior_time = prior;
+            d.event_time = event;
+            d.x = e.ox;
+            d.y = e.oy;
+            d.index = e.oi;
+            d.target_x = e.tx;
+            d.target_y = e.ty;
+            d.target_index = e.ti;
+            disp.push_back(d);
+        }
+        if (spec.size() + disp.size() >= 4096) return flush();
+        return 0;
+    }
+};
+
+int replay_fail(char *err, size_t cap, int code, const std::string &msg) {
+    if (err && cap) std::snprintf(err, cap, "%s", msg.c_str());
+    return code;
+}
+
+}  // namespace
+
+extern "C" int necsim_event_log_replay(const char *const *segments, uint64_t n_segments, uint64_t capacity,
+                                       int32_t need_speciation, int32_t need_dispersal, int32_t strict,
+                                       const necsim_reporter *reporter, uint64_t *n_events, char *err,
+                                       size_t err_cap) {
+    if (err && err_cap) err[0] = '\0';
+    if (!segments || !reporter || capacity == 0)
+        return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT, "invalid argument");
+    if (n_segments == 0)
+        return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT,
+                           "The EventLogReplay requires at least one event log segment.");
+    try {
+        std::vector<std::unique_ptr<ReplaySegment>> owned;
+        for (uint64_t j = 0; j < n_segments; ++j) {
+            auto s = std::make_unique<ReplaySegment>();
+            s->path = segments[j];
+            s->capacity = capacity;
+            s->f = std::fopen(segments[j], "rb");
+            if (!s->f) return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT, "cannot read " + s->path);
+            unsigned char h[26];
+            if (std::fread(h, 1, 26, s->f) != 26)
+                return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT, s->path + ": not an event log segment");
+            std::memcpy(&s->min_time, h, 8);
+            std::memcpy(&s->max_time, h + 8, 8);
+            std::memcpy(&s->length, h + 16, 8);
+            if (h[24] > 1 || h[25] > 1)
+                return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT, s->path + ": not an event log segment");
+            s->with_speciation = h[24] != 0;
+            s->with_dispersal = h[25] != 0;
+            owned.push_back(std::move(s));
+        }
+        // every segment reports the same kinds (replay/mod.rs:93-118)
+        for (auto &s : owned) {
+            if (s->with_speciation != owned[0]->with_speciation)
+                return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT,
+                                   "There is a mismatch in reporting speciation events between some segments.");
+            if (s->with_dispersal != owned[0]->with_dispersal)
+                return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT,
+                                   "There is a mismatch in reporting dispersal events between some segments.");
+        }
+        // the reporters' needs (rustcoalescence/src/args/cli/replay.rs:61-94)
+        const bool ws = owned[0]->with_speciation, wd = owned[0]->with_dispersal;
+        std::string need;
+        if (need_speciation && !ws && need_dispersal && !wd)
+            need = "The reporters require speciation and dispersal events, but the event log cannot provide either.";
+        else if (need_speciation && !ws)
+            need = "The reporters require speciation events, but the event log cannot provide them.";
+        else if (need_dispersal && !wd)
+            need = "The reporters require dispersal events, but the event log cannot provide them.";
+        if (!need.empty()) {
+            if (strict) return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT, need);
+            replay_fail(err, err_cap, NECSIM_OK, need);  // WarnOnly: the message stays as a warning
+        }
+        // chains of time-disjoint segments (replay/mod.rs:120-164)
+        std::vector<ReplaySegment *> rest;
+        for (auto &s : owned) rest.push_back(s.get());
+        std::vector<std::unique_ptr<ReplayGroup>> groups;
+        auto current = std::make_unique<ReplayGroup>();
+        double max_time = -INFINITY;
+        while (!rest.empty()) {
+            double min_time = INFINITY;
+            long min_index = -1;
+            for (size_t i = 0; i < rest.size(); ++i)
+                if (rest[i]->min_time > max_time && rest[i]->min_time < min_time) {
+                    min_time = rest[i]->min_time;
+                    min_index = (long)i;
+                }
+            if (min_index < 0) {
+                if (current->segs.empty())  // no segment orders after -inf: a NaN or infinite time
+                    return replay_fail(err, err_cap, NECSIM_E_INVALID_ARGUMENT,
+                                       "event log segment with an invalid minimum time");
+                groups.push_back(std::move(current));
+                current = std::make_unique<ReplayGroup>();
+                max_time = -INFINITY;
+                continue;
+            }
+            ReplaySegment *s = rest[(size_t)min_index];
+            rest[(size_t)min_index] = rest.back();  // swap_remove
+            rest.pop_back();
+            max_time = s->max_time;
+            current->segs.push_back(s);
+        }
+        if (!current->segs.empty()) groups.push_back(std::move(current));
+        // k-way merge by PackedEvent::cmp (replay/mod.rs:167-178)
+        auto later = [](const ReplayGroup *a, const ReplayGroup *b) { return packed_less(b->next, a->next); };
+        std::vector<ReplayGroup *> heap;
+        for (auto &g : groups) {
+            g->advance();
+            if (g->has) heap.push_back(g.get());
+        }
+        std::make_heap(heap.begin(), heap.end(), later);
+        ReplaySink sink{reporter, {}, {}};
+        uint64_t count = 0;
+        while (!heap.empty()) {
+            std::pop_heap(heap.begin(), heap.end(), later);
+            ReplayGroup *g = heap.back();
+            heap.pop_back();
+            if (sink.push(g->next)) return replay_fail(err, err_cap, NECSIM_E_CALLBACK, "a reporter stopped the replay");
+            ++count;
+            g->advance();
+            if (g->has) {
+                heap.push_back(g);
+                std::push_heap(heap.begin(), heap.end(), later);
+            }
+        }
+        if (sink.flush()) return replay_fail(err, err_cap, NECSIM_E_CALLBACK, "a reporter stopped the replay");
+        if (n_events) *n_events = count;
+        return NECSIM_OK;
+    } catch (const std::bad_alloc &) {
+        return replay_fail(err, err_cap, NECSIM_E_OUT_OF_MEMORY, "out of host memory");
+    }
+}

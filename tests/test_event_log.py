@@ -104,3 +104,126 @@ def test_simulation_logged_to_disk(nb, syn, tmp_path):
     assert np.array_equal(np.sort(s["event_time"]), np.sort(ref.speciation["event_time"]))
     assert len(ev[ev["kind"] == 2]) == ref.n_dispersal
     assert o.biodiversity == ref.biodiversity
+
+
+# ---- replay (event_log/replay/*.rs) ----
+def random_events(nb, n, seed):
+    rng = np.random.default_rng(seed)
+    spec = np.zeros(n, dtype=nb.SPECIATION_DTYPE)
+    spec["gref"] = rng.integers(0, 1 << 40, n)
+    spec["prior_time"] = rng.random(n) * 10
+    spec["event_time"] = spec["prior_time"] + rng.random(n) + 1e-9
+    spec["x"], spec["y"], spec["index"] = rng.integers(0, 30, (3, n))
+    disp = np.zeros(n, dtype=nb.DISPERSAL_DTYPE)
+    disp["gref"] = rng.integers(0, 1 << 40, n)
+    disp["prior_time"] = rng.random(n) * 10
+    disp["event_time"] = disp["prior_time"] + rng.random(n) + 1e-9
+    for f in ("x", "y", "index", "tx", "ty", "tindex"):
+        disp[f] = rng.integers(0, 30, n)
+    return spec, disp
+
+
+def packed_key(e, speciation):
+    t = (int(e["x"]), int(e["y"]), int(e["index"])) if speciation else (int(e["tx"]), int(e["ty"]), int(e["tindex"]))
+    return (float(e["event_time"]), int(e["x"]), int(e["y"]), int(e["index"])) + t + \
+        (float(e["prior_time"]), int(e["gref"]))
+
+
+def test_replay_merges_overlapping_segments_in_packed_order(nb, tmp_path):
+    # several logs whose segments overlap in time, written in delivery batches
+    logs, keys = [], []
+    for j in range(3):
+        spec, disp = random_events(nb, 700, 10 + j)
+        d = str(tmp_path / ("log%d" % j))
+        log = nb.EventLog(d, capacity=97, speciation=True, dispersal=True)
+        r = log.reporter
+        for k in range(0, 700, 150):  # several batches per log: segments overlap
+            a = np.ascontiguousarray(spec[k:k + 150])
+            assert r.report_speciation(r.user, a.ctypes.data, len(a)) == 0
+            b = np.ascontiguousarray(disp[k:k + 150])
+            assert r.report_dispersal(r.user, b.ctypes.data, len(b)) == 0
+        log.close()
+        logs.append(os.path.join(d, "*"))
+        keys += [(packed_key(e, True), "s") for e in spec] + [(packed_key(e, False), "d") for e in disp]
+    out = nb.replay_event_log(logs, capacity=13)
+    assert out.n_events == len(keys) == len(out.speciation) + len(out.dispersal)
+    got = []
+    i = j = 0
+    for kind, n in out.delivery:
+        for _ in range(n):
+            if kind == "s":
+                got.append((packed_key(out.speciation[i], True), "s"))
+                i += 1
+            else:
+                got.append((packed_key(out.dispersal[j], False), "d"))
+                j += 1
+    assert got == sorted(keys)
+    # delivery batches alternate kinds only where the stream does
+    assert all(a[0] != b[0] for a, b in zip(out.delivery, out.delivery[1:]) if a[1] < 4096)
+
+
+def raw_segment(path, events, with_speciation=True, with_dispersal=True):
+    times = [abs(e[2]) for e in events]
+    data = struct.pack("<ddQ??", min(times), max(times), len(events), with_speciation, with_dispersal)
+    for e in events:
+        data += struct.pack("<QddIIIIIIQ", *e)
+    open(path, "wb").write(data)
+
+
+def test_replay_decodes_every_sign_pair(nb, tmp_path):
+    # (prior, event) signs: (-, +) speciation; (+, -) Maybe, (+, +) None and
+    # (-, -) Coalescence dispersal (event.rs:186-240)
+    ev = [(1, -0.5, 1.0, 1, 1, 0, 1, 1, 0, 1), (2, 0.5, -2.0, 1, 1, 0, 2, 2, 0, 2),
+          (3, 0.5, 3.0, 1, 1, 0, 3, 3, 0, 3), (4, -0.5, -4.0, 1, 1, 0, 4, 4, 0, 9)]
+    raw_segment(str(tmp_path / "0"), ev)
+    out = nb.replay_event_log(str(tmp_path / "0"))
+    assert out.delivery == [("s", 1), ("d", 3)]
+    assert out.speciation[0]["prior_time"] == 0.5 and out.speciation[0]["event_time"] == 1.0
+    assert out.dispersal["event_time"].tolist() == [2.0, 3.0, 4.0]
+    assert out.dispersal["prior_time"].tolist() == [0.5, 0.5, 0.5]
+    assert out.dispersal["tx"].tolist() == [2, 3, 4]
+
+
+def test_replay_checks_segments_and_needs(nb, tmp_path):
+    a = [(1, -0.5, 1.0, 1, 1, 0, 1, 1, 0, 1)]
+    raw_segment(str(tmp_path / "a"), a, True, False)
+    raw_segment(str(tmp_path / "b"), [(2, -0.5, 2.0, 1, 1, 0, 1, 1, 0, 2)], True, True)
+    with pytest.raises(nb.NecsimError, match="mismatch in reporting dispersal"):
+        nb.replay_event_log([str(tmp_path / "a"), str(tmp_path / "b")])
+    with pytest.raises(nb.NecsimError, match="require dispersal events"):
+        nb.replay_event_log(str(tmp_path / "a"), need_dispersal=True)
+    out = nb.replay_event_log(str(tmp_path / "a"), need_dispersal=True, strict=False)
+    assert "require dispersal events" in out.warning and out.n_events == 1
+    with pytest.raises(nb.NecsimError, match="at least one"):
+        nb.replay_event_log([])
+    with pytest.raises(nb.NecsimError, match="cannot read"):
+        nb.replay_event_log(str(tmp_path / "missing"))
+    (tmp_path / "short").write_bytes(b"\0" * 10)
+    with pytest.raises(nb.NecsimError, match="not an event log segment"):
+        nb.replay_event_log(str(tmp_path / "short"))
+
+
+def test_driver_replays_a_log(nb, tmp_path):
+    import subprocess
+    spec, disp = random_events(nb, 400, 21)
+    spec[1::3]["x"] = spec[0::3][: len(spec[1::3])]["x"]  # some equal neighbours for the species count
+    write(nb, str(tmp_path / "log"), spec, disp, capacity=64)
+    cfg = """(
+        log: EventLog(segments: ["%s/*"], capacity: 7),
+        mode: Strict,
+        reporters: [Plugin(library: "x.so", reporters: [Biodiversity(), Counter()])],
+    )""" % (tmp_path / "log")
+    (tmp_path / "r.ron").write_text(cfg)
+    r = subprocess.run([nb.DRIVER, "replay", str(tmp_path / "r.ron")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = nb.replay_event_log(str(tmp_path / "log/*"))
+    species, last = 0, None
+    for e in out.speciation:  # biodiversity.rs:33-41 on the replayed stream
+        key = (int(e["x"]), int(e["y"]), int(e["index"]), float(e["event_time"]))
+        if key != last:
+            species += 1
+        last = key
+    assert "biodiversity of %d unique species" % species in r.stdout
+    assert "replayed %d events" % (2 * 400) in r.stdout
+    same = int(((disp["x"] == disp["tx"]) & (disp["y"] == disp["ty"])).sum())
+    assert "same location:\n     %d\n" % same in r.stdout
