@@ -204,23 +204,28 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU restatement of the reference (bounded sample)
 # ---------------------------------------------------------------------------
-def cpu_sample(sims, pause, threads, sampler="poisson"):
+def cpu_sample(sims, pause, threads, sampler="poisson", counts=None):
     """Runs the reference-faithful CPU restatement on every simulation of the
     workload up to time `pause` (a bounded sample), `threads` at a time.
-    Returns (events, seconds)."""
+    Returns (events, seconds); `counts`, when given, receives the sample's
+    WyHash primes and draws (the reference's hash work for those events)."""
     import oracle
     code = oracle.SAMPLER_EXP if sampler == "exp" else oracle.SAMPLER_POISSON
 
     def one(item):
         d, seed = item
-        return oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause,
-                               event_time_sampler=code).steps
+        o = oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause, event_time_sampler=code)
+        return o.steps, o.n_primes, o.n_draws
 
     oracle.lib()
     t0 = time.perf_counter()
     with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as ex:
-        steps = sum(ex.map(one, sims))
-    return steps, time.perf_counter() - t0
+        res = list(ex.map(one, sims))
+    if counts is not None:
+        counts["steps"] = sum(r[0] for r in res)
+        counts["primes"] = sum(r[1] for r in res)
+        counts["draws"] = sum(r[2] for r in res)
+    return sum(r[0] for r in res), time.perf_counter() - t0
 
 
 def cpu_sample_desc(name, pause, n):
@@ -293,6 +298,33 @@ def train_lifetime_model(nb, syn, device, pause):
             "traces": "AlmostInfinite r=100 sigma=10 and SpatiallyExplicit 64x64, speciation "
                       "{1e-2,1e-3,1e-4}, paused at t=%g" % pause}
     return model, info
+
+
+def issue_roofline(nb, sims, args, device, counts, events, kernel_ms):
+    """The step kernel against its integer-issue bound: algorithmic WyHash
+    mixing work (wymum, the 64x64 -> 128-bit multiply-fold) per event, from
+    the reference restatement's prime and draw counts on a sample of the
+    workload (a prime costs 2 wymum, a draw 1), times the events, over the
+    step kernel's CUDA-event time, against the measured rate of independent
+    wymum chains on this GPU."""
+    try:
+        if not counts:
+            # no CPU leg: the ratios from a small sample of the same workload
+            cpu_sample(sims[:: max(1, len(sims) // 4)][:4], 50.0, 4, args.event_time_sampler, counts)
+        per_event = (2.0 * counts["primes"] + counts["draws"]) / max(counts["steps"], 1)
+        achieved = per_event * events / (kernel_ms / 1e3) if kernel_ms > 0 else 0.0
+        peak = nb.hash_peak(device)
+        return {"bound": "integer-issue", "achieved": achieved, "peak": peak, "unit": "wymum/s",
+                "frac": achieved / peak, "kernel": "step_kernel",
+                "wymum_per_event": per_event,
+                "primes_per_event": counts["primes"] / max(counts["steps"], 1),
+                "draws_per_event": counts["draws"] / max(counts["steps"], 1),
+                "peak_source": "measured: 8 independent wymum chains per thread on every SM "
+                               "(necsim_gpu_hash_peak)",
+                "work_source": "reference-schedule restatement on the CPU sample (%d events)"
+                               % counts["steps"]}
+    except Exception as e:  # reported, never fatal to the benchmark line
+        return {"error": "%s: %s" % (type(e).__name__, e)}
 
 
 def time_arm(nb, scen, nus, seeds, algo, args, dist):
@@ -437,12 +469,14 @@ def main():
         line["model"] = model_info
     if tune_info is not None:
         line["autotune"] = tune_info
+    counts = {}
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler)
+        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler, counts)
         line["cpu_baseline"] = {"value": ev / sec, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
                                                           len(sims))}
+    line["issue_roofline"] = issue_roofline(nb, sims, args, device, counts, steps, head["kernel_ms"])
     if model is not None:
         model.close()
     if dist.rank == 0:

@@ -390,6 +390,12 @@ int necsim_event_log_replay(const char *const *segments, uint64_t n_segments, ui
                             int32_t need_speciation, int32_t need_dispersal, int32_t strict,
                             const necsim_reporter *reporter, uint64_t *n_events, char *error, size_t error_cap);
 
+/* The integer-issue ceiling of the path's hash work, measured on `device`:
+ * the rate of wymum (64x64 -> 128-bit multiply, WyHash's mixing step,
+ * wyhash.rs:85-96) over independent chains filling every SM.  No reference
+ * counterpart: the denominator of the benchmark's integer-issue roofline. */
+int necsim_gpu_hash_peak(int32_t device, double *wymum_per_second);
+
 /* ---- launch autotuner ----
  * Times a bounded sample of a batch -- every k-th simulation so that the
  * sample holds at most `max_sample_lineages` origins, each paused at

@@ -121,7 +121,7 @@ SYMBOLS = [
     "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
     "necsim_presample_origins", "necsim_gpu_autotune", "necsim_event_log_create",
     "necsim_event_log_reporter", "necsim_event_log_close", "necsim_event_log_replay", "necsim_map_load",
-    "necsim_map_free", "necsim_maps_fix",
+    "necsim_map_free", "necsim_maps_fix", "necsim_gpu_hash_peak",
 ]
 
 _lib = None
@@ -196,6 +196,8 @@ def lib():
     L.necsim_event_log_replay.argtypes = [vp, u64, u64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                           P(CReporter), P(u64), ctypes.c_char_p, ctypes.c_size_t]
     L.necsim_event_log_replay.restype = ctypes.c_int
+    L.necsim_gpu_hash_peak.argtypes = [ctypes.c_int32, P(ctypes.c_double)]
+    L.necsim_gpu_hash_peak.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
     L.necsim_model_create.restype = ctypes.c_int
     L.necsim_model_destroy.argtypes = [vp]
@@ -947,6 +949,16 @@ EVENT_LOG_HEADER_DTYPE = np.dtype([("min_time", "<f8"), ("max_time", "<f8"), ("l
 PACKED_EVENT_DTYPE = np.dtype([("gref", "<u8"), ("prior_time", "<f8"), ("event_time", "<f8"),
                                ("x", "<u4"), ("y", "<u4"), ("index", "<u4"),
                                ("tx", "<u4"), ("ty", "<u4"), ("tindex", "<u4"), ("coalescence", "<u8")])
+
+
+def hash_peak(device: int = 0) -> float:
+    """wymum (64x64 -> 128-bit multiply-fold) per second over independent
+    chains on every SM of `device`: the hash work's integer-issue ceiling."""
+    v = ctypes.c_double(0.0)
+    rc = lib().necsim_gpu_hash_peak(device, ctypes.byref(v))
+    if rc != 0:
+        raise NecsimError(rc, "hash peak measurement failed")
+    return v.value
 
 
 @dataclass

@@ -1579,6 +1579,41 @@ static std::vector<SimHost> batch_sims(const necsim_scenario *scenarios, const u
     return sims;
 }
 
+int necsim_gpu_hash_peak(int32_t device, double *wymum_per_second) {
+    if (!wymum_per_second) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, nullptr, 0, [&] {
+        CK(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        struct Res {
+            unsigned long long *sink = nullptr;
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            ~Res() {
+                if (sink) cudaFree(sink);
+                if (e0) cudaEventDestroy(e0);
+                if (e1) cudaEventDestroy(e1);
+            }
+        } r;
+        r.sink = dev_alloc<unsigned long long>(1);
+        CK(cudaEventCreate(&r.e0));
+        CK(cudaEventCreate(&r.e1));
+        const unsigned grid = (unsigned)prop.multiProcessorCount * 8;
+        const uint32_t iters = 4096;
+        CK(launch_hash_peak(grid, 1, iters, r.sink, 0));  // warm-up
+        float best = 0.0f;
+        for (int rep = 0; rep < 3; ++rep) {
+            CK(cudaEventRecord(r.e0, 0));
+            CK(launch_hash_peak(grid, (uint64_t)rep + 2, iters, r.sink, 0));
+            CK(cudaEventRecord(r.e1, 0));
+            CK(cudaEventSynchronize(r.e1));
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, r.e0, r.e1));
+            if (rep == 0 || ms < best) best = ms;
+        }
+        *wymum_per_second = (double)grid * 256.0 * 8.0 * (double)iters / ((double)best * 1e-3);
+    });
+}
+
 int necsim_gpu_autotune(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds, uint32_t n_sims,
                         const necsim_args *args_in, double sample_pause, uint64_t max_sample_lineages,
                         necsim_args *best, necsim_autotune_result *results, uint32_t results_cap,

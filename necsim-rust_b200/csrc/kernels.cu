@@ -1253,6 +1253,31 @@ __global__ void promote_kernel(SimParams *params, uint32_t n_sims) {
         if (params[s].resident == 1) params[s].resident = 2;
 }
 
+// The integer-issue ceiling of the hash work: eight independent chains of
+// wymum (64x64 -> 128-bit multiply, halves xor-folded) per thread on every
+// SM; the step kernel's algorithmic wymum rate is measured against it.
+__global__ void __launch_bounds__(256) hash_peak_kernel(uint64_t seed, uint32_t iters, unsigned long long *sink) {
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    uint64_t a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = seahash_diffuse(seed + t * 8 + (uint64_t)j);
+    const uint64_t b = kWyP1 ^ seed;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = wymum(a[j], b);
+    }
+    uint64_t x = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x ^= a[j];
+    if (x == 0) atomicAdd(sink, 1ULL);  // keeps every chain live
+}
+
+cudaError_t launch_hash_peak(unsigned grid, uint64_t seed, uint32_t iters, unsigned long long *sink,
+                             cudaStream_t st) {
+    hash_peak_kernel<<<grid, 256, 0, st>>>(seed, iters, sink);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st) {
     promote_kernel<<<1, 256, 0, st>>>(params, n_sims);
     return cudaGetLastError();

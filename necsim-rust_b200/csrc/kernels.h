@@ -93,5 +93,8 @@ struct ResidentArgs {
 
 cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st);
 cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st);
+// 8 * 256 * grid * iters wymum in independent chains (the hash-issue ceiling)
+cudaError_t launch_hash_peak(unsigned grid, uint64_t seed, uint32_t iters, unsigned long long *sink,
+                             cudaStream_t st);
 
 }  // namespace necsim

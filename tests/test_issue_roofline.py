@@ -1,0 +1,39 @@
+"""The benchmark's integer-issue roofline: the step kernel's algorithmic
+WyHash mixing work (wymum per event, from the reference restatement's prime
+and draw counts) against the measured rate of independent wymum chains."""
+import types
+
+import pytest
+
+
+def test_counts_per_event_from_the_reference_sample():
+    import bench
+    _, sims = bench.workload("c1")
+    counts = {}
+    ev, _ = bench.cpu_sample(sims, 30.0, 2, "poisson", counts)
+    assert counts["steps"] == ev > 0
+    primes, draws = counts["primes"] / ev, counts["draws"] / ev
+    # a Poisson event re-primes once and searches 1-3 buckets; it draws the
+    # Devroye sample, the event times and the event's own samples
+    assert 2.0 < primes < 5.0 and 4.0 < draws < 10.0
+
+
+def test_roofline_entry_is_never_fatal(nb):
+    import bench
+    _, sims = bench.workload("c1")
+    args = types.SimpleNamespace(event_time_sampler="poisson")
+    broken = types.SimpleNamespace(hash_peak=lambda device: (_ for _ in ()).throw(RuntimeError("no GPU")))
+    out = bench.issue_roofline(broken, sims, args, 0, {}, 1000, 1.0)
+    assert set(out) == {"error"} and "no GPU" in out["error"]
+
+
+@pytest.mark.gpu
+def test_hash_peak_and_roofline(nb):
+    import bench
+    peak = nb.hash_peak(0)
+    assert 1e10 < peak < 1e14
+    _, sims = bench.workload("c1")
+    args = types.SimpleNamespace(event_time_sampler="poisson")
+    out = bench.issue_roofline(nb, sims, args, 0, {}, 2_500_000, 10.0)
+    assert out["bound"] == "integer-issue" and 0.0 < out["frac"] < 1.5
+    assert 10.0 < out["wymum_per_event"] < 20.0
