@@ -91,6 +91,8 @@ struct Ifd {
         const int s = type_size(e->type);
         if (!(e->type == 1 || e->type == 3 || e->type == 4 || e->type == 16 || e->type == 13))
             bad(std::string("TIFF tag ") + name + " does not hold unsigned integers");
+        if (e->count > f->b.size()) bad("truncated TIFF file (read past its end)");
+        f->need(e->at, e->count * (uint64_t)s);  // before allocating for a corrupt count
         std::vector<uint64_t> v(e->count);
         for (uint64_t j = 0; j < e->count; ++j) v[j] = f->get(e->at + j * (uint64_t)s, s);
         return v;
@@ -320,6 +322,7 @@ Image read_tiff(const char *path, int bits, uint64_t want_format, std::string *n
     const uint64_t w = ifd.uint1(256, "ImageWidth", 0, true);
     const uint64_t h = ifd.uint1(257, "ImageLength", 0, true);
     if (w == 0 || h == 0 || w > 0xffffffffULL || h > 0xffffffffULL) bad("TIFF image dimensions out of range");
+    if (w > (1ULL << 40) / h) bad("TIFF image too large");  // keeps w * h * 8 far from overflow
     const uint64_t spp = ifd.uint1(277, "SamplesPerPixel", 1);
     const uint64_t photometric = ifd.uint1(262, "PhotometricInterpretation", 0, true);
     std::vector<uint64_t> bps = ifd.uints(258, "BitsPerSample");

@@ -249,3 +249,24 @@ def test_fixups_reject_negative_maps_and_bad_shapes(nb):
     nb.fix_maps(hab, np.eye(3), None, "OffByOne")  # only FixMe indexes the map as (w*h)^2
     with pytest.raises(ValueError):
         nb.fix_maps(hab, np.eye(4), None, "Lenient")
+
+
+def test_corrupt_counts_and_sizes_are_rejected(nb, tmp_path):
+    import struct
+    p = tmp_path / "c.tif"
+    tiff_util.write_tiff(str(p), np.arange(12, dtype=np.uint32).reshape(3, 4))
+    raw = bytearray(p.read_bytes())
+    (ifd,) = struct.unpack("<I", raw[4:8])
+    (n,) = struct.unpack("<H", raw[ifd:ifd + 2])
+    entries = {struct.unpack("<H", raw[ifd + 2 + 12 * j: ifd + 4 + 12 * j])[0]: ifd + 2 + 12 * j for j in range(n)}
+    bad = bytearray(raw)
+    bad[entries[273] + 4: entries[273] + 8] = struct.pack("<I", 0x7FFFFFFF)  # StripOffsets count
+    p.write_bytes(bytes(bad))
+    with pytest.raises(nb.NecsimError, match="truncated"):
+        nb.load_map(str(p), "u32")
+    bad = bytearray(raw)
+    bad[entries[256] + 8: entries[256] + 12] = struct.pack("<I", 0xFFFFFFFF)  # ImageWidth
+    bad[entries[257] + 8: entries[257] + 12] = struct.pack("<I", 0xFFFFFFFF)  # ImageLength
+    p.write_bytes(bytes(bad))
+    with pytest.raises(nb.NecsimError, match="too large"):
+        nb.load_map(str(p), "u32")
