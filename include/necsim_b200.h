@@ -202,7 +202,10 @@ int necsim_gpu_simulate(necsim_ctx *ctx, uint64_t wyhash_seed, double pause_befo
 
 /* Simulate caller-provided lineages (resume), with min_event_time =
  * resume_time.  Replaces `Algorithm::resume_and_simulate`
- * (algorithms/src/lib.rs:95-107). */
+ * (algorithms/src/lib.rs:95-107).  A lineage outside the habitat (its
+ * location off the landscape or of habitat 0) or outside its deme (index >=
+ * habitat) fails the call with NECSIM_E_INVALID_ARGUMENT, as the reference's
+ * ResumeError::Sample does (algorithms/src/result.rs:29-31). */
 int necsim_gpu_simulate_lineages(necsim_ctx *ctx, const necsim_lineage *lineages, uint64_t n,
                                  double resume_time, uint64_t wyhash_seed, double pause_before,
                                  const necsim_reporter *reporter, necsim_outcome *outcome);

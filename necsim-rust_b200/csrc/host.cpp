@@ -1468,9 +1468,12 @@ static int simulate_impl(necsim_ctx *ctx, const necsim_lineage *lineages, uint64
         std::vector<std::vector<necsim_lineage>> given;
         if (resume) {
             sh.params.min_event_time = resume_time;
-            // independent/mod.rs:98-117: lineages outside the habitat are not simulated
+            // independent/mod.rs:98-117 sets lineages outside the habitat or the
+            // deme aside as exceptional, and the resume initialiser then fails
+            // (initialiser/resume.rs:79-85, ResumeError::Sample)
             std::vector<necsim_lineage> keep;
             keep.reserve(n_lineages);
+            uint64_t out_of_habitat = 0, out_of_deme = 0;
             for (uint64_t j = 0; j < n_lineages; ++j) {
                 const necsim_lineage &l = lineages[j];
                 uint32_t h = 0;
@@ -1495,8 +1498,17 @@ static int simulate_impl(necsim_ctx *ctx, const necsim_lineage *lineages, uint64
                     h = (l.x < sc.width && l.y < sc.height) ? ctx->habitat[(uint64_t)l.y * sc.width + l.x] : 0;
                     break;
                 }
-                if (h > 0 && l.index < h) keep.push_back(l);
+                if (h == 0)
+                    out_of_habitat += 1;
+                else if (l.index >= h)
+                    out_of_deme += 1;
+                else
+                    keep.push_back(l);
             }
+            if (out_of_habitat || out_of_deme)
+                fail(NECSIM_E_INVALID_ARGUMENT, std::to_string(out_of_habitat) + " resumed lineage(s) out of habitat and " +
+                                                    std::to_string(out_of_deme) +
+                                                    " out of deme (ResumeError::Sample)");
             sh.n_origins = keep.size();
             given.push_back(std::move(keep));
         } else {

@@ -1503,9 +1503,19 @@ int oracle_simulate_lineages(const oracle_scenario *sc, const oracle_args *args,
     uint64_t n = 0;
     for (uint64_t j = 0; j < n_lineages; ++j) {
         const oracle_lineage *l = &lineages[j];
-        /* independent/mod.rs:98-117: drop lineages outside the habitat */
-        uint32_t h = habitat_at(&s, l->x, l->y);
-        if (h == 0 || l->index >= h) continue;
+        /* independent/mod.rs:98-117: a lineage off the habitat (Habitat::
+         * is_location_habitable = extent contains it and habitat > 0) or off
+         * its deme is exceptional, and initialiser/resume.rs:79-85 then fails */
+        int on_map = 1;
+        if (s.kind == ORACLE_NON_SPATIAL || s.kind == ORACLE_SPATIALLY_EXPLICIT)
+            on_map = extent_contains(&s.local, l->x, l->y);
+        uint32_t h = on_map ? habitat_at(&s, l->x, l->y) : 0;
+        if (h == 0 || l->index >= h) {
+            free(lins);
+            sim_free(&s);
+            out->status = -5;
+            return -5;
+        }
         lins[n].gref = l->gref;
         lins[n].last = l->last_event_time;
         lins[n].x = l->x;

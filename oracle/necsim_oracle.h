@@ -120,6 +120,8 @@ int oracle_simulate(const oracle_scenario *sc, const oracle_args *args, uint64_t
 
 /* Same as oracle_simulate but starting from caller-provided lineages
  * (resume), with min_event_time = resume_time. */
+/* resume the given lineages; -5 when one is off the habitat or its deme
+ * (the reference's ResumeError::Sample) */
 int oracle_simulate_lineages(const oracle_scenario *sc, const oracle_args *args, uint64_t seed,
                              const oracle_lineage *lineages, uint64_t n_lineages,
                              double resume_time, double pause_before, oracle_result *out,
