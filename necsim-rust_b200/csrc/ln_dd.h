@@ -259,6 +259,33 @@ NECSIM_DD_FN necsim_dd necsim_dd_mul(necsim_dd a, necsim_dd b) {
     return necsim_dd_quick_two_sum(p.hi, NECSIM_DD_ADD(p.lo, cross));
 }
 
+/* a + b with one two-sum (Dekker's addition): relative error ~2^-104 as long
+ * as a and b do not nearly cancel, which holds for every sum below (the
+ * worst cancellation, -ln c + ln(1 + r) next to the interval centred on 1,
+ * loses one bit) */
+NECSIM_DD_FN necsim_dd necsim_dd_add_fast(necsim_dd a, necsim_dd b) {
+    const necsim_dd s = necsim_dd_two_sum(a.hi, b.hi);
+    return necsim_dd_quick_two_sum(s.hi, NECSIM_DD_ADD(s.lo, NECSIM_DD_ADD(a.lo, b.lo)));
+}
+
+/* a + b for a double b */
+NECSIM_DD_FN necsim_dd necsim_dd_add_d(necsim_dd a, double b) {
+    const necsim_dd s = necsim_dd_two_sum(a.hi, b);
+    return necsim_dd_quick_two_sum(s.hi, NECSIM_DD_ADD(s.lo, a.lo));
+}
+
+/* a * b for a double b */
+NECSIM_DD_FN necsim_dd necsim_dd_mul_d(necsim_dd a, double b) {
+    const necsim_dd p = necsim_dd_two_prod(a.hi, b);
+    return necsim_dd_quick_two_sum(p.hi, NECSIM_DD_ADD(p.lo, NECSIM_DD_MUL(a.lo, b)));
+}
+
+/* a * a */
+NECSIM_DD_FN necsim_dd necsim_dd_sqr(necsim_dd a) {
+    const necsim_dd p = necsim_dd_two_prod(a.hi, a.hi);
+    return necsim_dd_quick_two_sum(p.hi, NECSIM_DD_ADD(p.lo, NECSIM_DD_MUL(NECSIM_DD_ADD(a.hi, a.hi), a.lo)));
+}
+
 /* ln(x) for normal doubles 0 < x <= 1, one rounding of a double-double */
 NECSIM_DD_FN double necsim_ln(double x) {
     uint64_t bits;
@@ -280,10 +307,11 @@ NECSIM_DD_FN double necsim_ln(double x) {
     /* r = m * c_i - 1 exactly: p + e = m * c_i, p - 1 exact (p within 2^-8 of 1) */
     r = necsim_dd_two_prod(m, NECSIM_LN_C[i]);
     r = necsim_dd_two_sum(NECSIM_DD_SUB(r.hi, 1.0), r.lo);
-    /* k ln 2 - ln c_i, independent of the series */
-    base = necsim_dd_add(necsim_dd_mul(necsim_dd_make(0x1.62e42fefa39efp-1, 0x1.abc9e3b39803fp-56),
-                                       necsim_dd_make((double)k, 0.0)),
-                         necsim_dd_make(NECSIM_LN_LHI[i], NECSIM_LN_LLO[i]));
+    /* k ln 2 - ln c_i, independent of the series (|k ln 2| >= 0.69 > 2 |ln c_i|
+     * when k != 0) */
+    base = necsim_dd_add_fast(necsim_dd_mul_d(necsim_dd_make(0x1.62e42fefa39efp-1, 0x1.abc9e3b39803fp-56),
+                                              (double)k),
+                              necsim_dd_make(NECSIM_LN_LHI[i], NECSIM_LN_LLO[i]));
     /* terms 7..12 in double: r^6 (1/7 - r/8 + r^2/9 - r^3/10 + r^4/11 - r^5/12) */
     rh = r.hi;
     tail = -0x1.5555555555555p-4;
@@ -295,16 +323,17 @@ NECSIM_DD_FN double necsim_ln(double x) {
     r6 = NECSIM_DD_MUL(rh, rh);
     r6 = NECSIM_DD_MUL(NECSIM_DD_MUL(r6, r6), r6);
     tail = NECSIM_DD_MUL(r6, tail);
-    /* terms 1..6 in double-double: (1 - r/2) + r^2 ((1/3 - r/4) + r^2 (1/5 - r/6)) */
-    a = necsim_dd_add(necsim_dd_make(1.0, 0.0), necsim_dd_make(NECSIM_DD_MUL(r.hi, -0.5), NECSIM_DD_MUL(r.lo, -0.5)));
-    b = necsim_dd_add(necsim_dd_make(0x1.5555555555555p-2, 0x1.5555555555555p-56),
-                      necsim_dd_make(NECSIM_DD_MUL(r.hi, -0.25), NECSIM_DD_MUL(r.lo, -0.25)));
-    c = necsim_dd_add(necsim_dd_make(0x1.999999999999ap-3, -0x1.999999999999ap-57),
-                      necsim_dd_mul(necsim_dd_make(-0x1.5555555555555p-3, -0x1.5555555555555p-57), r));
-    r2 = necsim_dd_mul(r, r);
-    p = necsim_dd_add(a, necsim_dd_mul(r2, necsim_dd_add(b, necsim_dd_mul(r2, c))));
-    p = necsim_dd_add(p, necsim_dd_make(tail, 0.0));
-    res = necsim_dd_add(base, necsim_dd_mul(r, p));
+    /* terms 1..6 in double-double: (1 - r/2) + r^2 ((1/3 - r/4) + r^2 (1/5 - r/6));
+     * each sum adds a term at most 2^-6 the size of the other */
+    a = necsim_dd_add_d(necsim_dd_make(NECSIM_DD_MUL(r.hi, -0.5), NECSIM_DD_MUL(r.lo, -0.5)), 1.0);
+    b = necsim_dd_add_fast(necsim_dd_make(0x1.5555555555555p-2, 0x1.5555555555555p-56),
+                           necsim_dd_make(NECSIM_DD_MUL(r.hi, -0.25), NECSIM_DD_MUL(r.lo, -0.25)));
+    c = necsim_dd_add_fast(necsim_dd_make(0x1.999999999999ap-3, -0x1.999999999999ap-57),
+                           necsim_dd_mul(necsim_dd_make(-0x1.5555555555555p-3, -0x1.5555555555555p-57), r));
+    r2 = necsim_dd_sqr(r);
+    p = necsim_dd_add_fast(a, necsim_dd_mul(r2, necsim_dd_add_fast(b, necsim_dd_mul(r2, c))));
+    p = necsim_dd_add_d(p, tail);
+    res = necsim_dd_add_fast(base, necsim_dd_mul(r, p));
     return NECSIM_DD_ADD(res.hi, res.lo);
 }
 
