@@ -551,6 +551,10 @@ void alloc_run_buffers(Engine &E) {
     E.d_params = dev_alloc<SimParams>(E.sims.size());
     E.d_counters = dev_alloc<SimCounters>(E.sims.size());
     E.d_ctl = dev_alloc<Control>(1);
+    // each run resets both; a run without lineages runs no round and reads
+    // them as they are here (upload_origins synchronises the stream next)
+    CK(cudaMemsetAsync(E.d_counters, 0, E.sims.size() * sizeof(SimCounters), E.stream));
+    CK(cudaMemsetAsync(E.d_ctl, 0, sizeof(Control), E.stream));
     E.spec_cap = n;
     E.d_spec = dev_alloc<DevSpeciationEvent>(n);
     if (E.disp_cap) E.d_disp = dev_alloc<DevDispersalEvent>(E.disp_cap);

@@ -2,9 +2,8 @@
 ragged inputs, a pause before any event, resumed lineages outside the
 habitat or with an index beyond the deme (the resume fails, as the
 reference's ResumeError::Sample), identical resumed lineages (merged by the
-first dedup), a
-single-lineage simulation inside a batch of large ones, and the documented
-size limit of the dispersal buffer."""
+first dedup), a single-lineage simulation inside a batch of large ones, and
+the documented size limit of the dispersal buffer."""
 import numpy as np
 import pytest
 
@@ -72,7 +71,9 @@ def test_resume_rejects_exceptional_lineages_and_merges_duplicates(nb, syn, orac
 
 def test_single_lineage_simulation_in_a_ragged_batch(nb, syn):
     sims = syn.config4(n_sims=3, max_local=3000)
-    one = dict(kind=0, speciation_probability=0.05, width=1, height=1, deme=1)
+    # a batch shares one scenario kind: a SpatiallyImplicit local community of one individual
+    one = dict(kind=1, speciation_probability=0.05, width=1, height=1, deme=1, meta_width=1000, meta_height=1,
+               meta_deme=1, migration_probability=0.1)
     descs = [d for d, _ in sims] + [one]
     seeds = [s for _, s in sims] + [77]
     nus = [d["speciation_probability"] * 100 for d, _ in sims] + [0.05]
