@@ -7,7 +7,10 @@ through it the GPU backend) is pinned by a second implementation:
   * SeedableRng::seed_from_u64        necsim/core/src/cogs/rng.rs:33-63
   * WyHash prime_with / sample_u64    necsim/impls/no-std/src/cogs/rng/wyhash.rs:53-119
   * sample_uniform_closed_open        rng.rs:75-82
-  * PoissonEventTimeSampler           .../event_time_sampler/poisson.rs:30-109
+  * PoissonEventTimeSampler           .../event_time_sampler/poisson.rs:30-109, at several
+    turnover rates (lambda * delta_t up to 20: Devroye counts beyond eight ranks)
+  * ExpEventTimeSampler               .../event_time_sampler/exp.rs:37-83 with rng.rs:163-167
+    sample_exponential, its logarithm the correctly rounded one (60-digit decimal)
   * Box-Muller + clamp_round_dispersal  rng.rs:180-197, habitat/almost_infinite.rs:100-114
   * LandscapeExtent iteration order   necsim/core/src/landscape/extent.rs:80-100, with the
     reference's own test cases (extent.rs:110-160)
@@ -19,6 +22,7 @@ import json
 import math
 import os
 import struct
+from decimal import Decimal, getcontext
 
 M64 = (1 << 64) - 1
 P0, P1, P2, P5 = 0xA0761D6478BD642F, 0xE7037ED1A0B428DB, 0x8EBC6AF09C88C6E3, 0xEB44ACCAB455D165
@@ -98,6 +102,34 @@ def poisson_next(g, inj, t, lam, dt):
     return best[0], reprime
 
 
+def ln_correctly_rounded(u):
+    getcontext().prec = 60
+    return float(Decimal(u).ln())  # Decimal(float) is exact; float() rounds to nearest
+
+
+def exp_next(g, inj, t, lam, dt):
+    """exp.rs:37-83: exponential inter-event times inside delta_t buckets."""
+    ts = int(math.floor(t / dt))
+    event_time = float(ts) * dt
+    slice_end = float(ts + 1) * dt
+    g.prime(inj, ts)
+    sub = 0
+    while True:
+        event_time += -ln_correctly_rounded(g.oc()) / lam
+        sub = (sub + INV_PHI) & M64
+        if event_time >= slice_end:
+            ts += 1
+            sub = 0
+            event_time = slice_end
+            slice_end = float(ts + 1) * dt
+            g.prime(inj, ts)
+        elif event_time > t:
+            break
+    reprime = (ts + sub) & M64
+    g.prime(inj, reprime)
+    return event_time, reprime
+
+
 def normal_dispersal(d0, d1, sigma, x, y):
     u0 = float((d0 >> 11) + 1) * 2.0 ** -53
     u1 = float(d1 >> 11) * 2.0 ** -53
@@ -148,7 +180,8 @@ def fnv_sample(x, y, i, t, u):
 
 
 def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0,
-                             lam=0.5, dt=2.0):
+                             lam=0.5, dt=2.0, sampler=None):
+    sampler = sampler or poisson_next
     g = Wy(seed_from_u64(seed))
     lineages = []
     for yy in range(h):
@@ -207,7 +240,7 @@ def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, eve
             new_time = lin[1]
             while True:
                 before = lin[1]
-                t, _ = poisson_next(g, inj(lin), before, lam, dt)
+                t, _ = sampler(g, inj(lin), before, lam, dt)
                 nt = t if t > before else struct.unpack("<d", struct.pack("<Q", struct.unpack("<Q", struct.pack("<d", before))[0] + 1))[0]
                 prev_next = nt
                 if k >= step_slice or nt >= level:
@@ -264,6 +297,29 @@ def main():
                      "event_time_bits": struct.unpack("<Q", struct.pack("<d", et))[0],
                      "reprime": rp})
     kat["poisson_next_event_time"] = pois
+    # other turnover rates and intervals; lambda * delta_t = 20 draws Devroye
+    # counts past the eight tabulated ranks
+    pois_l = []
+    for seed, inj, t, lam, dt in [(seed_from_u64(5), 3, 0.0, 0.05, 2.0), (seed_from_u64(5), 3, 10.25, 3.0, 1.0),
+                                  (seed_from_u64(11), 2 ** 33 + 1, 7.0, 10.0, 2.0),
+                                  (seed_from_u64(12), 77, 123.5, 1.0, 3.0),
+                                  (seed_from_u64(13), 0, 0.0, 0.5, 0.25)]:
+        for j in range(4):
+            g = Wy(seed)
+            et, rp = poisson_next(g, inj + j, t, lam, dt)
+            pois_l.append({"seed": seed, "injection": inj + j, "time": t, "lambda": lam, "delta_t": dt,
+                           "event_time_bits": struct.unpack("<Q", struct.pack("<d", et))[0], "reprime": rp})
+    kat["poisson_next_event_time_rates"] = pois_l
+    expv = []
+    for seed, inj, t, lam, dt in [(seed_from_u64(42), 0, 0.0, 0.5, 2.0), (seed_from_u64(42), 99, 3.5, 0.5, 2.0),
+                                  (seed_from_u64(7), 2 ** 40, 1234.25, 0.5, 3.0),
+                                  (seed_from_u64(9), 5, 0.0, 5.0, 2.0), (seed_from_u64(9), 6, 40.0, 0.1, 0.5)]:
+        for j in range(4):
+            g = Wy(seed)
+            et, rp = exp_next(g, inj + j, t, lam, dt)
+            expv.append({"seed": seed, "injection": inj + j, "time": t, "lambda": lam, "delta_t": dt,
+                         "event_time_bits": struct.unpack("<Q", struct.pack("<d", et))[0], "reprime": rp})
+    kat["exp_next_event_time"] = expv
     nd = []
     g = Wy(seed_from_u64(3))
     g.prime(1, 1)
@@ -290,6 +346,11 @@ def main():
         r = nonspatial_reference_run(w, h, deme, nu, seed)
         r.update({"width": w, "height": h, "deme": deme, "speciation": nu, "seed": seed})
         kat["nonspatial_runs"].append(r)
+    kat["nonspatial_runs_exp"] = []
+    for (w, h, deme, nu, seed) in [(2, 2, 2, 0.05, 3), (4, 3, 2, 0.02, 42)]:
+        r = nonspatial_reference_run(w, h, deme, nu, seed, sampler=exp_next)
+        r.update({"width": w, "height": h, "deme": deme, "speciation": nu, "seed": seed})
+        kat["nonspatial_runs_exp"].append(r)
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "kat.json")
     with open(path, "w") as f:
         json.dump(kat, f, indent=1)

@@ -32,6 +32,27 @@ def test_poisson_next_event_time(oracle, kat):
         assert t > case["time"]
 
 
+def test_poisson_next_event_time_at_other_rates(oracle, kat):
+    """Turnover rates 0.05..10 and other intervals (per-cell rates of a
+    turnover map use the same function); lambda * delta_t = 20 counts past
+    the eight tabulated Devroye ranks."""
+    for case in kat["poisson_next_event_time_rates"]:
+        t, rp = oracle.poisson_next_event_time(case["seed"], case["injection"], case["time"], case["lambda"],
+                                               case["delta_t"])
+        assert np.float64(t).view(np.uint64) == case["event_time_bits"]
+        assert rp == case["reprime"]
+
+
+def test_exp_next_event_time(oracle, kat):
+    """exp.rs against a restatement whose logarithm is the correctly rounded
+    one from 60-digit decimal arithmetic (independent of ln_dd.h)."""
+    for case in kat["exp_next_event_time"]:
+        t, rp = oracle.exp_next_event_time(case["seed"], case["injection"], case["time"], case["lambda"],
+                                           case["delta_t"])
+        assert np.float64(t).view(np.uint64) == case["event_time_bits"]
+        assert rp == case["reprime"]
+
+
 def test_normal_dispersal(oracle, kat):
     for d0, d1, sigma, x, y, tx, ty in kat["normal_dispersal"]:
         assert oracle.normal_dispersal(d0, d1, sigma, x, y) == (tx, ty)
@@ -68,6 +89,17 @@ def test_nonspatial_reference_runs(oracle, kat):
         assert r.steps == case["steps"]
         assert r.time == case["time"]
         assert r.biodiversity == case["biodiversity"]
+        got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
+                int(e["y"]), int(e["index"])] for e in r.speciation]
+        assert got == case["events"]
+
+
+def test_nonspatial_reference_runs_with_exponential_event_times(oracle, kat):
+    for case in kat["nonspatial_runs_exp"]:
+        desc = dict(kind=oracle.NON_SPATIAL, speciation_probability=case["speciation"],
+                    width=case["width"], height=case["height"], deme=case["deme"])
+        r = oracle.simulate(desc, case["seed"], mode=oracle.MODE_REFERENCE, event_time_sampler=oracle.SAMPLER_EXP)
+        assert (r.steps, r.time, r.biodiversity) == (case["steps"], case["time"], case["biodiversity"])
         got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
                 int(e["y"]), int(e["index"])] for e in r.speciation]
         assert got == case["events"]
