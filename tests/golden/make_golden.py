@@ -14,7 +14,10 @@ through it the GPU backend) is pinned by a second implementation:
   * Box-Muller + clamp_round_dispersal  rng.rs:180-197, habitat/almost_infinite.rs:100-114
   * LandscapeExtent iteration order   necsim/core/src/landscape/extent.rs:80-100, with the
     reference's own test cases (extent.rs:110-160)
-  * full reference-schedule runs of tiny scenarios (monolithic/mod.rs:43-270)
+  * InMemoryPackedSeparableAliasDispersalSampler tables and draws
+    (alias/packed.rs:59-163, packed_separable_alias/{mod,dispersal}.rs)
+  * full reference-schedule runs of tiny NonSpatial and SpatiallyExplicit
+    scenarios (monolithic/mod.rs:43-270)
 
 Run:  python tests/golden/make_golden.py
 """
@@ -179,15 +182,134 @@ def fnv_sample(x, y, i, t, u):
     return h
 
 
+class NonSpatialLandscape:
+    """habitat/non_spatial.rs, dispersal_sampler/non_spatial.rs:42-66."""
+
+    def __init__(self, w, h, deme):
+        self.w, self.h, self.deme = w, h, deme
+
+    def origins(self):
+        return [[((yy * self.w + xx) * self.deme + ii), 0.0, xx, yy, ii]
+                for yy in range(self.h) for xx in range(self.w) for ii in range(self.deme)]
+
+    def injection(self, x, y, i):
+        return (y * self.w + x) * self.deme + i
+
+    def habitat(self, x, y):
+        return self.deme
+
+    def disperse(self, g, x, y):
+        idx = min(int(math.floor(g.co() * float(self.w * self.h))), self.w * self.h - 1)
+        return idx % self.w, idx // self.w
+
+
+def alias_atoms(events):
+    """AliasMethodSamplerAtom::create (alias/packed.rs:59-121): Vose's
+    construction with stack-ordered pairing; events = [(event, weight)]."""
+    total = 0.0
+    for _, wt in events:
+        total = total + wt
+    n = float(len(events))
+    atoms = [[wt * n / total, e, e] for e, wt in events]
+    over = [i for i, a in enumerate(atoms) if a[0] > 1.0]
+    under = [i for i, a in enumerate(atoms) if a[0] < 1.0]
+    while over and under:
+        o, u = over.pop(), under.pop()
+        atoms[o][0] = atoms[o][0] + atoms[u][0] - 1.0
+        atoms[u][2] = atoms[o][1]
+        if atoms[o][0] < 1.0:
+            under.append(o)
+        elif atoms[o][0] > 1.0:
+            over.append(o)
+    for i in over + under:  # rounding leftovers are full buckets (Vose 1991)
+        atoms[i][0] = 1.0
+    return atoms
+
+
+class SpatiallyExplicitLandscape:
+    """habitat/in_memory.rs, packed_separable_alias/mod.rs:64-203 (tables) and
+    dispersal.rs:16-77 (a draw), coalescence index floor(u * habitat)."""
+
+    def __init__(self, habitat, dispersal):
+        self.hab = habitat  # [h][w]
+        self.h, self.w = len(habitat), len(habitat[0])
+        cells = self.w * self.h
+        self.prefix, acc = [], 0
+        for c in range(cells):
+            self.prefix.append(acc)
+            acc += habitat[c // self.w][c % self.w]
+        self.rows = []
+        for row in range(cells):
+            events, self_w = [], 0.0
+            for col in range(cells):
+                wt = dispersal[row][col] * float(habitat[col // self.w][col % self.w])
+                if wt > 0.0:
+                    events.append((col, wt))
+                    if col == row:
+                        self_w = wt
+            if not events:
+                self.rows.append((0.0, row, []))
+                continue
+            total = 0.0
+            for _, wt in events:
+                total = total + wt
+            self_p = self_w / total
+            self_u = self_w * float(len(events)) / total
+            non_self = row
+            if self_u < 1.0:
+                atoms = alias_atoms(events)
+                for j, a in enumerate(atoms):
+                    if a[1] == row or a[2] == row:
+                        if a[1] == row:  # flip: swap the events, u -> 1 - u
+                            a[0], a[1], a[2] = 1.0 - a[0], a[2], a[1]
+                        non_self = a[1]
+                        atoms[j], atoms[-1] = atoms[-1], atoms[j]
+                        break
+            else:
+                atoms = alias_atoms([(e, wt) for e, wt in events if e != row])
+            self.rows.append((self_p, non_self, atoms))
+
+    def origins(self):
+        out = []
+        for y in range(self.h):
+            for x in range(self.w):
+                for i in range(self.hab[y][x]):
+                    out.append([self.injection(x, y, i), 0.0, x, y, i])
+        return out
+
+    def injection(self, x, y, i):
+        return self.prefix[y * self.w + x] + i
+
+    def habitat(self, x, y):
+        return self.hab[y][x]
+
+    def disperse(self, g, x, y):
+        cell = y * self.w + x
+        self_p, non_self, atoms = self.rows[cell]
+        if self_p == 1.0:
+            target = cell
+        elif self_p == 0.0 or non_self != cell or g.co() >= self_p:
+            f = g.co() * 1.0 * float(len(atoms))
+            i = int(math.floor(f))
+            a = atoms[i]
+            target = a[1] if (f - float(i)) < a[0] else a[2]
+        else:
+            target = cell
+        return target % self.w, target // self.w
+
+
 def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0,
                              lam=0.5, dt=2.0, sampler=None):
+    return reference_run(NonSpatialLandscape(w, h, deme), nu, seed, step_slice, dedup, event_slice, lam,
+                         dt, sampler)
+
+
+def reference_run(land, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0, lam=0.5, dt=2.0, sampler=None):
+    """A full reference-schedule run (parallelisation/independent/monolithic/
+    mod.rs:43-270 with the water-level reporter) on a landscape."""
     sampler = sampler or poisson_next
     g = Wy(seed_from_u64(seed))
-    lineages = []
-    for yy in range(h):
-        for xx in range(w):
-            for ii in range(deme):
-                lineages.append([((yy * w + xx) * deme + ii), 0.0, xx, yy, ii])
+    lineages = land.origins()
     n = len(lineages)
     slow = [(lin, lin[1]) for lin in lineages]
     fast = []
@@ -201,7 +323,7 @@ def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, eve
     slow_ev = []
 
     def inj(lin):
-        return ((lin[3] * w + lin[2]) * deme + lin[4])
+        return land.injection(lin[2], lin[3], lin[4])
 
     while slow:
         rate = 0.0
@@ -254,9 +376,8 @@ def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, eve
                     slow_ev.append((nt, lin[2], lin[3], lin[4], lin[1], lin[0]))
                     active = None
                     break
-                idx = min(int(math.floor(g.co() * float(w * h))), w * h - 1)
-                tx, ty = idx % w, idx // w
-                ti = int(math.floor(g.co() * float(deme)))
+                tx, ty = land.disperse(g, lin[2], lin[3])
+                ti = int(math.floor(g.co() * float(land.habitat(tx, ty))))
                 lin = [lin[0], nt, tx, ty, ti]
                 active = lin
             steps += k
@@ -273,6 +394,34 @@ def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, eve
         last = key
     return {"steps": steps, "time": max_time, "biodiversity": species,
             "events": [[e[5], e[4], e[0], e[1], e[2], e[3]] for e in delivered]}
+
+
+def se_case(w, h, case):
+    """Small habitat and dispersal maps with zero cells, self-dispersal only
+    rows, rows without self-dispersal and a full self-dispersal bucket."""
+    import random
+    rnd = random.Random(100 + case)
+    hab = [[rnd.choice([0, 1, 2, 3]) for _ in range(w)] for _ in range(h)]
+    hab[0][0] = 2
+    cells = w * h
+    disp = []
+    for row in range(cells):
+        if hab[row // w][row % w] == 0:
+            disp.append([0.0] * cells)
+            continue
+        r = [0.0] * cells
+        for col in range(cells):
+            if hab[col // w][col % w] > 0 and rnd.random() < 0.6:
+                r[col] = float(rnd.randint(1, 9))
+        if case == 1 and row % 3 == 0:
+            r = [0.0] * cells
+            r[row] = 1.0  # self-dispersal only
+        if case == 2 and row % 2 == 0:
+            r[row] = 50.0  # self-dispersal fills its bucket: removed from the atoms
+        if not any(r):
+            r[row] = 1.0
+        disp.append(r)
+    return hab, disp
 
 
 def main():
@@ -346,6 +495,15 @@ def main():
         r = nonspatial_reference_run(w, h, deme, nu, seed)
         r.update({"width": w, "height": h, "deme": deme, "speciation": nu, "seed": seed})
         kat["nonspatial_runs"].append(r)
+    kat["spatially_explicit_runs"] = []
+    for (w, h, nu, seed, case) in [(3, 3, 0.05, 4, 0), (4, 3, 0.02, 8, 1), (3, 2, 0.1, 2, 2)]:
+        hab, disp = se_case(w, h, case)
+        r = reference_run(SpatiallyExplicitLandscape(hab, disp), nu, seed)
+        land = SpatiallyExplicitLandscape(hab, disp)
+        r.update({"width": w, "height": h, "habitat": hab, "dispersal": disp, "speciation": nu, "seed": seed,
+                  "tables": [{"self_dispersal": p, "non_self_event": ns, "atoms": atoms}
+                             for p, ns, atoms in land.rows]})
+        kat["spatially_explicit_runs"].append(r)
     kat["nonspatial_runs_exp"] = []
     for (w, h, deme, nu, seed) in [(2, 2, 2, 0.05, 3), (4, 3, 2, 0.02, 42)]:
         r = nonspatial_reference_run(w, h, deme, nu, seed, sampler=exp_next)
