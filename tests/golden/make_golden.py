@@ -16,8 +16,8 @@ through it the GPU backend) is pinned by a second implementation:
     reference's own test cases (extent.rs:110-160)
   * InMemoryPackedSeparableAliasDispersalSampler tables and draws
     (alias/packed.rs:59-163, packed_separable_alias/{mod,dispersal}.rs)
-  * full reference-schedule runs of tiny NonSpatial and SpatiallyExplicit
-    scenarios (monolithic/mod.rs:43-270)
+  * full reference-schedule runs of tiny NonSpatial, SpatiallyImplicit,
+    AlmostInfinite and SpatiallyExplicit scenarios (monolithic/mod.rs:43-270)
 
 Run:  python tests/golden/make_golden.py
 """
@@ -198,9 +198,73 @@ class NonSpatialLandscape:
     def habitat(self, x, y):
         return self.deme
 
+    def nu(self, x, y, nu):
+        return nu
+
     def disperse(self, g, x, y):
         idx = min(int(math.floor(g.co() * float(self.w * self.h))), self.w * self.h - 1)
         return idx % self.w, idx // self.w
+
+
+class SpatiallyImplicitLandscape:
+    """habitat/spatially_implicit.rs (the metacommunity at origin
+    (2^32 - mw, 2^32 - mh)), dispersal_sampler/spatially_implicit.rs:58-86,
+    speciation_probability/spatially_implicit.rs:31-44 (0 in the local
+    community); origins are the local community's."""
+
+    def __init__(self, w, h, deme, mw, mh, mdeme, m):
+        self.w, self.h, self.deme, self.mw, self.mh, self.mdeme, self.m = w, h, deme, mw, mh, mdeme, m
+        self.mox, self.moy = (1 << 32) - mw, (1 << 32) - mh
+
+    def local(self, x, y):
+        return x < self.w and y < self.h
+
+    def origins(self):
+        return NonSpatialLandscape(self.w, self.h, self.deme).origins()
+
+    def injection(self, x, y, i):
+        if self.local(x, y):
+            return (y * self.w + x) * self.deme + i
+        return ((((y - self.moy) & 0xFFFFFFFF) * self.mw + ((x - self.mox) & 0xFFFFFFFF)) * self.mdeme + i) & M64
+
+    def habitat(self, x, y):
+        return self.deme if self.local(x, y) else self.mdeme
+
+    def nu(self, x, y, nu):
+        return 0.0 if self.local(x, y) else nu
+
+    def disperse(self, g, x, y):
+        if self.local(x, y) and not (g.co() < self.m):
+            idx = min(int(math.floor(g.co() * float(self.w * self.h))), self.w * self.h - 1)
+            return idx % self.w, idx // self.w
+        n = self.mw * self.mh
+        idx = min(int(math.floor(g.co() * float(n))), n - 1)
+        return (self.mox + idx % self.mw) & 0xFFFFFFFF, (self.moy + idx // self.mw) & 0xFFFFFFFF
+
+
+class AlmostInfiniteLandscape:
+    """habitat/almost_infinite.rs (one individual per location, injection
+    y << 32 | x), the circle origin sampler, Normal dispersal (rng.rs:180-197
+    + clamp_round_dispersal); the singleton demes still draw the coalescence
+    sample (index 0)."""
+
+    def __init__(self, cx, cy, r, sigma):
+        self.cx, self.cy, self.r, self.sigma = cx, cy, r, sigma
+
+    def origins(self):
+        return [[(y << 32) | x, 0.0, x, y, 0] for (x, y) in circle_origins(self.cx, self.cy, self.r)]
+
+    def injection(self, x, y, i):
+        return (y << 32) | x
+
+    def habitat(self, x, y):
+        return 1
+
+    def nu(self, x, y, nu):
+        return nu
+
+    def disperse(self, g, x, y):
+        return normal_dispersal(g.u64(), g.u64(), self.sigma, x, y)
 
 
 def alias_atoms(events):
@@ -283,6 +347,9 @@ class SpatiallyExplicitLandscape:
     def habitat(self, x, y):
         return self.hab[y][x]
 
+    def nu(self, x, y, nu):
+        return nu
+
     def disperse(self, g, x, y):
         cell = y * self.w + x
         self_p, non_self, atoms = self.rows[cell]
@@ -327,9 +394,9 @@ def reference_run(land, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0, lam
 
     while slow:
         rate = 0.0
-        for _ in slow:
-            rate = rate + lam * nu
-        level = level + float(es) / rate
+        for (lin, _) in slow:
+            rate = rate + lam * land.nu(lin[2], lin[3], nu)
+        level = level + (float(es) / rate if rate > 0.0 else math.inf)  # f64 division
         slow_ev.sort()
         delivered += slow_ev
         slow_ev = []
@@ -372,7 +439,7 @@ def reference_run(land, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0, lam
                 if prev_sample is None or not (prev_sample[4] <= us):
                     prev_sample = (lin[2], lin[3], lin[4], nt, us)
                 k += 1
-                if us < nu:
+                if us < land.nu(lin[2], lin[3], nu):
                     slow_ev.append((nt, lin[2], lin[3], lin[4], lin[1], lin[0]))
                     active = None
                     break
@@ -504,6 +571,18 @@ def main():
                   "tables": [{"self_dispersal": p, "non_self_event": ns, "atoms": atoms}
                              for p, ns, atoms in land.rows]})
         kat["spatially_explicit_runs"].append(r)
+    kat["spatially_implicit_runs"] = []
+    for (w, h, deme, mw, mh, mdeme, m, nu, seed) in [(3, 2, 2, 40, 1, 1, 0.2, 0.05, 5),
+                                                     (2, 2, 1, 7, 3, 2, 0.5, 0.1, 6)]:
+        r = reference_run(SpatiallyImplicitLandscape(w, h, deme, mw, mh, mdeme, m), nu, seed)
+        r.update({"width": w, "height": h, "deme": deme, "meta_width": mw, "meta_height": mh, "meta_deme": mdeme,
+                  "migration": m, "speciation": nu, "seed": seed})
+        kat["spatially_implicit_runs"].append(r)
+    kat["almost_infinite_runs"] = []
+    for (cx, cy, rad, sigma, nu, seed) in [(2 ** 31 - 1, 2 ** 31 - 1, 2, 3.0, 0.05, 7), (1, 0xFFFFFFFF, 3, 1.5, 0.02, 8)]:
+        r = reference_run(AlmostInfiniteLandscape(cx, cy, rad, sigma), nu, seed)
+        r.update({"centre": [cx, cy], "radius": rad, "sigma": sigma, "speciation": nu, "seed": seed})
+        kat["almost_infinite_runs"].append(r)
     kat["nonspatial_runs_exp"] = []
     for (w, h, deme, nu, seed) in [(2, 2, 2, 0.05, 3), (4, 3, 2, 0.02, 42)]:
         r = nonspatial_reference_run(w, h, deme, nu, seed, sampler=exp_next)

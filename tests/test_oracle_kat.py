@@ -192,3 +192,32 @@ def test_spatially_explicit_reference_runs(oracle, kat):
         got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
                 int(e["y"]), int(e["index"])] for e in r.speciation]
         assert got == case["events"]
+
+
+def check_run(oracle, desc, case):
+    r = oracle.simulate(desc, case["seed"], mode=oracle.MODE_REFERENCE)
+    assert (r.steps, r.time, r.biodiversity) == (case["steps"], case["time"], case["biodiversity"])
+    got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
+            int(e["y"]), int(e["index"])] for e in r.speciation]
+    assert got == case["events"]
+
+
+def test_spatially_implicit_reference_runs(oracle, kat):
+    """Local community with migration into a metacommunity at the far corner
+    of the plane; no speciation locally, so the water level can be infinite."""
+    for case in kat["spatially_implicit_runs"]:
+        desc = dict(kind=oracle.SPATIALLY_IMPLICIT, speciation_probability=case["speciation"],
+                    width=case["width"], height=case["height"], deme=case["deme"],
+                    meta_width=case["meta_width"], meta_height=case["meta_height"],
+                    meta_deme=case["meta_deme"], migration_probability=case["migration"])
+        check_run(oracle, desc, case)
+
+
+def test_almost_infinite_reference_runs(oracle, kat):
+    """Circle origins (one wrapping across the plane's edge), Normal dispersal
+    with clamp-and-round, singleton demes."""
+    for case in kat["almost_infinite_runs"]:
+        desc = dict(kind=oracle.ALMOST_INFINITE_NORMAL, speciation_probability=case["speciation"],
+                    sigma=case["sigma"], radius=case["radius"], centre_x=case["centre"][0],
+                    centre_y=case["centre"][1])
+        check_run(oracle, desc, case)
