@@ -294,8 +294,9 @@ class SpatiallyExplicitLandscape:
     """habitat/in_memory.rs, packed_separable_alias/mod.rs:64-203 (tables) and
     dispersal.rs:16-77 (a draw), coalescence index floor(u * habitat)."""
 
-    def __init__(self, habitat, dispersal):
+    def __init__(self, habitat, dispersal, turnover=None):
         self.hab = habitat  # [h][w]
+        self.turnover = turnover  # [h][w] rates of a turnover map, or None
         self.h, self.w = len(habitat), len(habitat[0])
         cells = self.w * self.h
         self.prefix, acc = [], 0
@@ -392,10 +393,13 @@ def reference_run(land, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0, lam
     def inj(lin):
         return land.injection(lin[2], lin[3], lin[4])
 
+    def rate_at(lin):  # turnover_rate/{uniform,in_memory}.rs
+        return land.turnover[lin[3]][lin[2]] if getattr(land, "turnover", None) else lam
+
     while slow:
         rate = 0.0
         for (lin, _) in slow:
-            rate = rate + lam * land.nu(lin[2], lin[3], nu)
+            rate = rate + rate_at(lin) * land.nu(lin[2], lin[3], nu)
         level = level + (float(es) / rate if rate > 0.0 else math.inf)  # f64 division
         slow_ev.sort()
         delivered += slow_ev
@@ -429,7 +433,7 @@ def reference_run(land, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0, lam
             new_time = lin[1]
             while True:
                 before = lin[1]
-                t, _ = sampler(g, inj(lin), before, lam, dt)
+                t, _ = sampler(g, inj(lin), before, rate_at(lin), dt)
                 nt = t if t > before else struct.unpack("<d", struct.pack("<Q", struct.unpack("<Q", struct.pack("<d", before))[0] + 1))[0]
                 prev_next = nt
                 if k >= step_slice or nt >= level:
@@ -571,6 +575,16 @@ def main():
                   "tables": [{"self_dispersal": p, "non_self_event": ns, "atoms": atoms}
                              for p, ns, atoms in land.rows]})
         kat["spatially_explicit_runs"].append(r)
+    kat["turnover_map_runs"] = []
+    for (w, h, nu, seed, case) in [(3, 3, 0.05, 14, 0), (4, 3, 0.02, 18, 1)]:
+        hab, disp = se_case(w, h, case)
+        import random
+        rnd = random.Random(200 + case)
+        turnover = [[(rnd.choice([0.1, 0.5, 2.0, 7.5]) if hab[y][x] else 0.0) for x in range(w)] for y in range(h)]
+        r = reference_run(SpatiallyExplicitLandscape(hab, disp, turnover), nu, seed)
+        r.update({"width": w, "height": h, "habitat": hab, "dispersal": disp, "turnover": turnover,
+                  "speciation": nu, "seed": seed})
+        kat["turnover_map_runs"].append(r)
     kat["spatially_implicit_runs"] = []
     for (w, h, deme, mw, mh, mdeme, m, nu, seed) in [(3, 2, 2, 40, 1, 1, 0.2, 0.05, 5),
                                                      (2, 2, 1, 7, 3, 2, 0.5, 0.1, 6)]:

@@ -221,3 +221,12 @@ def test_almost_infinite_reference_runs(oracle, kat):
                     sigma=case["sigma"], radius=case["radius"], centre_x=case["centre"][0],
                     centre_y=case["centre"][1])
         check_run(oracle, desc, case)
+
+
+def test_turnover_map_reference_runs(oracle, kat):
+    """SpatiallyExplicit with a turnover map: each lineage's event times and
+    its share of the water level follow its cell's rate (0.1 to 7.5)."""
+    for case in kat["turnover_map_runs"]:
+        desc = se_desc(oracle, case)
+        desc["turnover_map"] = np.array(case["turnover"], dtype=np.float64)
+        check_run(oracle, desc, case)
