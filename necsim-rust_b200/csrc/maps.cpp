@@ -107,11 +107,11 @@ struct Ifd {
     }
 };
 
-Ifd first_ifd(const Bytes &f) {
+// reads the byte order mark into f.big, then the first IFD's entries
+Ifd first_ifd(Bytes &f) {
     if (f.b.size() < 8) bad("not a TIFF file (too short)");
-    Bytes &w = const_cast<Bytes &>(f);
-    if (f.b[0] == 'I' && f.b[1] == 'I') w.big = false;
-    else if (f.b[0] == 'M' && f.b[1] == 'M') w.big = true;
+    if (f.b[0] == 'I' && f.b[1] == 'I') f.big = false;
+    else if (f.b[0] == 'M' && f.b[1] == 'M') f.big = true;
     else bad("not a TIFF file (byte order mark)");
     const uint64_t magic = f.get(2, 2);
     Ifd ifd;
