@@ -204,23 +204,34 @@ class Clocks:
 # ---------------------------------------------------------------------------
 # CPU restatement of the reference (bounded sample)
 # ---------------------------------------------------------------------------
+def cpu_partitions(n_sims, threads):
+    """IsolatedIndividuals partitions per simulation: one when the workload
+    has a simulation per thread, else enough to occupy every thread, as the
+    reference spreads one simulation over cores (pre_sampler.rs:103-112)."""
+    return max(1, threads // max(n_sims, 1))
+
+
 def cpu_sample(sims, pause, threads, sampler="poisson", counts=None):
     """Runs the reference-faithful CPU restatement on every simulation of the
-    workload up to time `pause` (a bounded sample), `threads` at a time.
+    workload up to time `pause` (a bounded sample), `threads` at a time, each
+    simulation split into cpu_partitions() IsolatedIndividuals partitions.
     Returns (events, seconds); `counts`, when given, receives the sample's
     WyHash primes and draws (the reference's hash work for those events)."""
     import oracle
     code = oracle.SAMPLER_EXP if sampler == "exp" else oracle.SAMPLER_POISSON
+    parts = cpu_partitions(len(sims), threads)
+    tasks = [(d, seed, r) for d, seed in sims for r in range(parts)]
 
     def one(item):
-        d, seed = item
-        o = oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause, event_time_sampler=code)
+        d, seed, rank = item
+        o = oracle.simulate(d, seed, mode=oracle.MODE_REFERENCE, pause_before=pause, event_time_sampler=code,
+                            partition=(rank, parts))
         return o.steps, o.n_primes, o.n_draws
 
     oracle.lib()
     t0 = time.perf_counter()
     with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as ex:
-        res = list(ex.map(one, sims))
+        res = list(ex.map(one, tasks))
     if counts is not None:
         counts["steps"] = sum(r[0] for r in res)
         counts["primes"] = sum(r[1] for r in res)
@@ -228,9 +239,11 @@ def cpu_sample(sims, pause, threads, sampler="poisson", counts=None):
     return sum(r[0] for r in res), time.perf_counter() - t0
 
 
-def cpu_sample_desc(name, pause, n):
-    return "%s: all %d simulation(s) advanced to t=%g (pause_before) with the reference schedule" % (
-        name, n, pause)
+def cpu_sample_desc(name, pause, n, threads=1):
+    parts = cpu_partitions(n, threads)
+    split = (", each in %d IsolatedIndividuals partitions" % parts) if parts > 1 else ""
+    return "%s: all %d simulation(s) advanced to t=%g (pause_before) with the reference schedule%s" % (
+        name, n, pause, split)
 
 
 def reference_arm(args, dist):
@@ -255,7 +268,7 @@ def reference_arm(args, dist):
                                         "event_time_sampler": args.event_time_sampler},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
-                                                   len(sims))},
+                                                   len(sims), threads)},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -475,7 +488,7 @@ def main():
         ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler, counts)
         line["cpu_baseline"] = {"value": ev / sec, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
-                                                          len(sims))}
+                                                          len(sims), threads)}
     line["issue_roofline"] = issue_roofline(nb, sims, args, device, counts, steps, head["kernel_ms"])
     if model is not None:
         model.close()

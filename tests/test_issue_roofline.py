@@ -37,3 +37,17 @@ def test_hash_peak_and_roofline(nb):
     out = bench.issue_roofline(nb, sims, args, 0, {}, 2_500_000, 10.0)
     assert out["bound"] == "integer-issue" and 0.0 < out["frac"] < 1.5
     assert 10.0 < out["wymum_per_event"] < 20.0
+
+
+def test_cpu_baseline_partitions_single_simulations():
+    """The CPU leg spreads a simulation over threads with IsolatedIndividuals
+    partitions when the workload has fewer simulations than threads."""
+    import bench
+    assert bench.cpu_partitions(256, 16) == 1 and bench.cpu_partitions(1, 8) == 8
+    assert bench.cpu_partitions(3, 8) == 2 and bench.cpu_partitions(1, 1) == 1
+    assert "8 IsolatedIndividuals partitions" in bench.cpu_sample_desc("c1", 400.0, 1, 8)
+    assert "partitions" not in bench.cpu_sample_desc("c4", 400.0, 256, 16)
+    _, sims = bench.workload("c1")
+    one, _ = bench.cpu_sample(sims, 20.0, 1)
+    split, _ = bench.cpu_sample(sims, 20.0, 4)
+    assert split >= one > 0  # partitions re-simulate duplicates a monolithic run merges
