@@ -185,7 +185,7 @@ typedef struct necsim_ctx necsim_ctx;
 /* Create a context: validates the scenario, builds the dispersal tables
  * (SpatiallyExplicit: packed separable alias, packed_separable_alias/mod.rs:64-203),
  * uploads them to the device and enumerates the origin lineages
- * (OriginPreSampler::all(), origin_sampler/*.rs).  Replaces the set-up half of
+ * (OriginPreSampler::all() and the origin samplers).  Replaces the set-up half of
  * `Algorithm::initialise_and_simulate` (rustcoalescence/algorithms/src/lib.rs:81-93). */
 int necsim_gpu_create(const necsim_scenario *scenario, const necsim_args *args,
                       necsim_ctx **out_ctx);

@@ -49,9 +49,10 @@ struct Fail {
 
 [[noreturn]] void fail(const std::string &m) { throw Fail{m}; }
 
-const Value &need(const Value &v, const std::string &name) {
+// the field `name` of v (a reference into v; field names are literals)
+const Value &need(const Value &v, const char *name) {
     const Value *f = v.field(name);
-    if (!f) fail("missing field `" + name + "` in " + (v.text.empty() ? "(...)" : v.text));
+    if (!f) fail("missing field `" + std::string(name) + "` in " + (v.text.empty() ? "(...)" : v.text));
     return *f;
 }
 

@@ -667,8 +667,7 @@ void reset_lineages(Engine &E) {
 }
 
 StepArgs make_step_args(Engine &E, DeviceLineages &in) {
-    StepArgs a;
-    std::memset(&a, 0, sizeof(a));
+    StepArgs a{};  // every field zero, pointers null
     a.in = in.soa;
     a.state = in.state;
     a.order = nullptr;
@@ -709,8 +708,7 @@ FeatureArgs make_feature_args(Engine &E, DeviceLineages &in) {
 }
 
 DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
-    DedupArgs a;
-    std::memset(&a, 0, sizeof(a));
+    DedupArgs a{};  // every field zero, pointers null
     a.in = in.soa;
     a.out = out.soa;
     a.state = in.state;
@@ -734,8 +732,7 @@ DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
 }
 
 ResidentArgs make_resident_args(Engine &E, uint32_t budget, const int *stop_flag) {
-    ResidentArgs a;
-    std::memset(&a, 0, sizeof(a));
+    ResidentArgs a{};  // every field zero, pointers null
     a.arena = E.R.soa;
     a.params = E.d_params;
     a.counters = E.d_counters;
