@@ -468,13 +468,79 @@ std::string resume_config(const std::string &text, uint64_t seed, const std::vec
     return necsim::ron::to_string(root) + "\n";
 }
 
+// The Counter reporter (necsim/plugins/common/src/event_counter.rs): it
+// collapses an event equal to the one before it (speciation: origin and time;
+// dispersal: origin, time and target) and counts such a repeat as a late
+// coalescence when its prior time differs from the last one seen.  Every
+// dispersal here carries LineageInteraction::Maybe, the Independent
+// coalescence sampler's (coalescence_sampler/independent.rs:52), so every
+// deduplicated dispersal is "detected late".
+struct EventCounter {
+    uint64_t raw_total = 0, speciation = 0, self_dispersal = 0, out_dispersal = 0, self_coalescence = 0,
+             out_coalescence = 0, late_dispersal_coalescence = 0, late_coalescence = 0;
+    bool has_spec = false, has_disp = false, has_prior = false;
+    necsim_speciation_event last_spec{};
+    necsim_dispersal_event last_disp{};
+    double last_prior = 0.0;
+
+    void repeat(double prior) {
+        if (!has_prior || prior != last_prior) late_coalescence += 1;
+        last_prior = prior;
+        has_prior = true;
+    }
+    void on(const necsim_speciation_event &e) {
+        raw_total += 1;
+        if (has_spec && e.x == last_spec.x && e.y == last_spec.y && e.index == last_spec.index &&
+            e.event_time == last_spec.event_time)
+            return repeat(e.prior_time);
+        last_spec = e;
+        has_spec = true;
+        last_prior = e.prior_time;
+        has_prior = true;
+        speciation += 1;
+    }
+    void on(const necsim_dispersal_event &e) {
+        raw_total += 1;
+        if (has_disp && e.x == last_disp.x && e.y == last_disp.y && e.index == last_disp.index &&
+            e.event_time == last_disp.event_time && e.target_x == last_disp.target_x &&
+            e.target_y == last_disp.target_y && e.target_index == last_disp.target_index)
+            return repeat(e.prior_time);
+        last_disp = e;
+        has_disp = true;
+        last_prior = e.prior_time;
+        has_prior = true;
+        late_dispersal_coalescence += 1;  // LineageInteraction::Maybe
+    }
+    // event_counter.rs finalise: the summary, when any event was seen
+    void print() const {
+        if (!has_spec && !has_disp) return;
+        std::printf("Event Summary:\n - Total #individuals:\n   %" PRIu64 "\n",
+                    speciation + self_coalescence + out_coalescence + late_coalescence);
+        std::printf(" - Total #events:\n   - raw:\n     %" PRIu64 "\n   - deduplicated:\n     %" PRIu64 "\n",
+                    raw_total,
+                    speciation + self_coalescence + out_coalescence + self_dispersal + out_dispersal +
+                        late_dispersal_coalescence);
+        std::printf(" - Speciation:\n    %" PRIu64 "\n", speciation);
+        std::printf(" - Dispersal:\n   - same location, no coalescence:\n     %" PRIu64
+                    "\n   - same location, with coalescence:\n     %" PRIu64
+                    "\n   - new location, no coalescence:\n     %" PRIu64
+                    "\n   - new location, with coalescence:\n     %" PRIu64
+                    "\n   - detected late, no coalescence:\n     %" PRIu64
+                    "\n   - detected late, with coalescence:\n     %" PRIu64 "\n",
+                    self_dispersal, self_coalescence, out_dispersal, out_coalescence,
+                    late_dispersal_coalescence - late_coalescence,  // usize arithmetic, wrapping in release
+                    late_coalescence);
+    }
+};
+
 struct Counts {
-    uint64_t speciation = 0, self_dispersal = 0, out_dispersal = 0;
+    EventCounter counter;
     necsim_reporter log{};  // the event log's reporter, when one is written
 };
 
 int on_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
     Counts &c = *static_cast<Counts *>(user);
+    for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
     if (c.log.report_speciation) return c.log.report_speciation(c.log.user, ev, n);
     return 0;
 }
@@ -482,12 +548,7 @@ int on_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
 int on_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     Counts &c = *static_cast<Counts *>(user);
     if (c.log.report_dispersal && c.log.report_dispersal(c.log.user, ev, n) != 0) return 1;
-    for (uint64_t i = 0; i < n; ++i) {
-        if (ev[i].x == ev[i].target_x && ev[i].y == ev[i].target_y)
-            c.self_dispersal += 1;
-        else
-            c.out_dispersal += 1;
-    }
+    for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
     return 0;
 }
 
@@ -581,10 +642,7 @@ int simulate(const std::string &path, bool run) {
     if (r.rep_biodiversity && out.biodiversity > 0)
         std::printf("The simulation resulted in a biodiversity of %" PRIu64 " unique species.\n",
                     out.biodiversity);
-    if (r.rep_counter)
-        std::printf("Event Summary:\n - Speciation:\n    %" PRIu64 "\n - Dispersal (raw):\n   - same location:\n"
-                    "     %" PRIu64 "\n   - new location:\n     %" PRIu64 "\n",
-                    out.n_speciation, counts.self_dispersal, counts.out_dispersal);
+    if (r.rep_counter) counts.counter.print();
     if (r.rep_execution) {
         auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
         std::printf("The simulation took:\n - initialisation: %.3f ms\n - execution: %.3f ms\n - cleanup: %.3f ms\n",
@@ -603,17 +661,18 @@ int simulate(const std::string &path, bool run) {
 
 // The reporters of a replay: Biodiversity counts speciation events that
 // differ from the previous one by origin or event time (biodiversity.rs:33-41),
-// Counter the events by kind.
+// Counter as in a simulation.
 struct ReplayCounts {
-    uint64_t biodiversity = 0, speciation = 0, self_dispersal = 0, out_dispersal = 0;
+    uint64_t biodiversity = 0;
     bool have_last = false;
     necsim_speciation_event last{};
+    EventCounter counter;
 };
 
 int replay_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
     ReplayCounts &c = *static_cast<ReplayCounts *>(user);
     for (uint64_t i = 0; i < n; ++i) {
-        c.speciation += 1;
+        c.counter.on(ev[i]);
         const necsim_speciation_event &e = ev[i];
         if (c.have_last && e.x == c.last.x && e.y == c.last.y && e.index == c.last.index &&
             e.event_time == c.last.event_time)
@@ -627,12 +686,7 @@ int replay_speciation(void *user, const necsim_speciation_event *ev, uint64_t n)
 
 int replay_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     ReplayCounts &c = *static_cast<ReplayCounts *>(user);
-    for (uint64_t i = 0; i < n; ++i) {
-        if (ev[i].x == ev[i].target_x && ev[i].y == ev[i].target_y)
-            c.self_dispersal += 1;
-        else
-            c.out_dispersal += 1;
-    }
+    for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
     return 0;
 }
 
@@ -690,10 +744,7 @@ int replay(const std::string &path) {
     std::printf("necsim-b200: replayed %" PRIu64 " events\n", n);
     if (r.rep_biodiversity && counts.biodiversity > 0)
         std::printf("The simulation resulted in a biodiversity of %" PRIu64 " unique species.\n", counts.biodiversity);
-    if (r.rep_counter)
-        std::printf("Event Summary:\n - Speciation:\n    %" PRIu64 "\n - Dispersal (raw):\n   - same location:\n"
-                    "     %" PRIu64 "\n   - new location:\n     %" PRIu64 "\n",
-                    counts.speciation, counts.self_dispersal, counts.out_dispersal);
+    if (r.rep_counter) counts.counter.print();
     if (r.rep_execution)
         std::printf("The replay took %.3f ms\n", std::chrono::duration<double, std::milli>(t1 - t0).count());
     return 0;

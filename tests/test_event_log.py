@@ -207,6 +207,11 @@ def test_driver_replays_a_log(nb, tmp_path):
     import subprocess
     spec, disp = random_events(nb, 400, 21)
     spec[1::3]["x"] = spec[0::3][: len(spec[1::3])]["x"]  # some equal neighbours for the species count
+    # repeats of events (a duplicate lineage's copy), some with another prior time: late coalescences
+    spec[5::40] = spec[4::40][: len(spec[5::40])]
+    spec["prior_time"][5::80] -= 1e-3
+    disp[7::30] = disp[6::30][: len(disp[7::30])]
+    disp["prior_time"][7::60] -= 1e-3
     write(nb, str(tmp_path / "log"), spec, disp, capacity=64)
     cfg = """(
         log: EventLog(segments: ["%s/*"], capacity: 7),
@@ -225,5 +230,42 @@ def test_driver_replays_a_log(nb, tmp_path):
         last = key
     assert "biodiversity of %d unique species" % species in r.stdout
     assert "replayed %d events" % (2 * 400) in r.stdout
-    same = int(((disp["x"] == disp["tx"]) & (disp["y"] == disp["ty"])).sum())
-    assert "same location:\n     %d\n" % same in r.stdout
+    assert counter_summary(out) in r.stdout
+
+
+def counter_summary(out):
+    """EventCounterReporter (necsim/plugins/common/src/event_counter.rs) on a
+    replayed stream whose dispersal events carry LineageInteraction::Maybe."""
+    raw = spec = late_disp = late = 0
+    last_s = last_d = last_prior = None
+    i = j = 0
+    for kind, n in out.delivery:
+        for _ in range(n):
+            if kind == "s":
+                e = out.speciation[i]
+                i += 1
+                key = (int(e["x"]), int(e["y"]), int(e["index"]), float(e["event_time"]))
+                raw += 1
+                if key == last_s:
+                    late += float(e["prior_time"]) != last_prior
+                else:
+                    last_s = key
+                    spec += 1
+            else:
+                e = out.dispersal[j]
+                j += 1
+                key = (int(e["x"]), int(e["y"]), int(e["index"]), float(e["event_time"]), int(e["tx"]),
+                       int(e["ty"]), int(e["tindex"]))
+                raw += 1
+                if key == last_d:
+                    late += float(e["prior_time"]) != last_prior
+                else:
+                    last_d = key
+                    late_disp += 1
+            last_prior = float(e["prior_time"])
+    return ("Event Summary:\n - Total #individuals:\n   %d\n - Total #events:\n   - raw:\n     %d\n"
+            "   - deduplicated:\n     %d\n - Speciation:\n    %d\n - Dispersal:\n"
+            "   - same location, no coalescence:\n     0\n   - same location, with coalescence:\n     0\n"
+            "   - new location, no coalescence:\n     0\n   - new location, with coalescence:\n     0\n"
+            "   - detected late, no coalescence:\n     %d\n   - detected late, with coalescence:\n     %d\n"
+            % (spec + late, raw, spec + late_disp, spec, (late_disp - late) % (1 << 64), late))
