@@ -552,6 +552,34 @@ int on_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     return 0;
 }
 
+// A duration as Rust's `Debug for Duration` prints it (the Execution
+// reporter's `{:?}`, plugins/common/src/execution_time.rs:65-76): the
+// largest unit among s, ms, µs and ns with at least one whole unit, then the
+// fraction's significant digits
+template <typename D>
+std::string rust_duration(D d) {
+    const uint64_t ns = (uint64_t)std::max<int64_t>(0, std::chrono::duration_cast<std::chrono::nanoseconds>(d).count());
+    uint64_t unit = 1;
+    const char *name = "ns";
+    int digits = 0;
+    if (ns >= 1000000000ULL) {
+        unit = 1000000000ULL, name = "s", digits = 9;
+    } else if (ns >= 1000000ULL) {
+        unit = 1000000ULL, name = "ms", digits = 6;
+    } else if (ns >= 1000ULL) {
+        unit = 1000ULL, name = "\u00b5s", digits = 3;
+    }
+    std::string out = std::to_string(ns / unit);
+    uint64_t frac = ns % unit;
+    if (frac) {
+        std::string f = std::to_string(frac);
+        f.insert(0, (size_t)digits - f.size(), '0');
+        while (!f.empty() && f.back() == '0') f.pop_back();
+        out += "." + f;
+    }
+    return out + name;
+}
+
 std::string slurp(const std::string &path) {
     std::ifstream f(path);
     if (!f) fail("cannot read " + path);
@@ -644,9 +672,8 @@ int simulate(const std::string &path, bool run) {
                     out.biodiversity);
     if (r.rep_counter) counts.counter.print();
     if (r.rep_execution) {
-        auto ms = [](auto a, auto b) { return std::chrono::duration<double, std::milli>(b - a).count(); };
-        std::printf("The simulation took:\n - initialisation: %.3f ms\n - execution: %.3f ms\n - cleanup: %.3f ms\n",
-                    ms(t0, t1), ms(t1, t2), ms(t2, t3));
+        std::printf("The simulation took:\n - initialisation: %s\n - execution: %s\n - cleanup: %s\n",
+                    rust_duration(t1 - t0).c_str(), rust_duration(t2 - t1).c_str(), rust_duration(t3 - t2).c_str());
     }
     if (out.paused && !r.pause_config.empty()) {
         std::ofstream f(r.pause_config);
@@ -746,7 +773,7 @@ int replay(const std::string &path) {
         std::printf("The simulation resulted in a biodiversity of %" PRIu64 " unique species.\n", counts.biodiversity);
     if (r.rep_counter) counts.counter.print();
     if (r.rep_execution)
-        std::printf("The replay took %.3f ms\n", std::chrono::duration<double, std::milli>(t1 - t0).count());
+        std::printf("The replay took %s\n", rust_duration(t1 - t0).c_str());
     return 0;
 }
 

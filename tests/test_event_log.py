@@ -216,7 +216,7 @@ def test_driver_replays_a_log(nb, tmp_path):
     cfg = """(
         log: EventLog(segments: ["%s/*"], capacity: 7),
         mode: Strict,
-        reporters: [Plugin(library: "x.so", reporters: [Biodiversity(), Counter()])],
+        reporters: [Plugin(library: "x.so", reporters: [Biodiversity(), Counter(), Execution()])],
     )""" % (tmp_path / "log")
     (tmp_path / "r.ron").write_text(cfg)
     r = subprocess.run([nb.DRIVER, "replay", str(tmp_path / "r.ron")], capture_output=True, text=True, timeout=120)
@@ -231,6 +231,9 @@ def test_driver_replays_a_log(nb, tmp_path):
     assert "biodiversity of %d unique species" % species in r.stdout
     assert "replayed %d events" % (2 * 400) in r.stdout
     assert counter_summary(out) in r.stdout
+    import re
+    # Rust's Debug for Duration, as the Execution reporter prints it
+    assert re.search(r"The replay took \d+(\.\d*[1-9])?(s|ms|\u00b5s|ns)\n", r.stdout), r.stdout
 
 
 def counter_summary(out):
