@@ -242,6 +242,50 @@ class SpatiallyImplicitLandscape:
         return (self.mox + idx % self.mw) & 0xFFFFFFFF, (self.moy + idx // self.mw) & 0xFFFFFFFF
 
 
+def clark2dt_dispersal(u01, u2, shape_u, tail_p, x, y):
+    """almost_infinite_clark2dt.rs:96-107 with clark2dt::cdf_inverse and
+    pow_fast_one (x^1 is x itself); the angle is (u2 * 2) * pi."""
+    e = 1.0 / tail_p
+    base = 1.0 / (1.0 - u01)
+    jump = math.sqrt(shape_u * ((base if e == 1.0 else math.pow(base, e)) - 1.0))
+    theta = u2 * 2.0 * math.pi
+    dx, dy = math.cos(theta) * jump, math.sin(theta) * jump
+
+    def rnd(v):  # f64::round, half away from zero
+        a = abs(v)
+        f = math.floor(a)
+        r = int(f) + (1 if a - f >= 0.5 else 0)
+        return r if v >= 0 else -r
+
+    W = 1 << 32
+    return (x + rnd(dx)) % W, (y + rnd(dy)) % W
+
+
+class AlmostInfiniteClarkLandscape:
+    """AlmostInfinite habitat with Clark2Dt dispersal (a closed-open then an
+    open-closed sample per dispersal)."""
+
+    def __init__(self, cx, cy, r, shape_u, tail_p):
+        self.cx, self.cy, self.r, self.shape_u, self.tail_p = cx, cy, r, shape_u, tail_p
+
+    def origins(self):
+        return AlmostInfiniteLandscape(self.cx, self.cy, self.r, 0.0).origins()
+
+    def injection(self, x, y, i):
+        return (y << 32) | x
+
+    def habitat(self, x, y):
+        return 1
+
+    def nu(self, x, y, nu):
+        return nu
+
+    def disperse(self, g, x, y):
+        u01 = g.co()
+        u2 = g.oc()
+        return clark2dt_dispersal(u01, u2, self.shape_u, self.tail_p, x, y)
+
+
 class AlmostInfiniteLandscape:
     """habitat/almost_infinite.rs (one individual per location, injection
     y << 32 | x), the circle origin sampler, Normal dispersal (rng.rs:180-197
@@ -597,6 +641,13 @@ def main():
         r = reference_run(AlmostInfiniteLandscape(cx, cy, rad, sigma), nu, seed)
         r.update({"centre": [cx, cy], "radius": rad, "sigma": sigma, "speciation": nu, "seed": seed})
         kat["almost_infinite_runs"].append(r)
+    kat["clark2dt_runs"] = []
+    for (cx, cy, rad, shape_u, tail_p, nu, seed) in [(2 ** 31, 2 ** 31, 2, 4.0, 0.5, 0.05, 21),
+                                                     (0, 3, 2, 1.0, 1.0, 0.05, 22)]:
+        r = reference_run(AlmostInfiniteClarkLandscape(cx, cy, rad, shape_u, tail_p), nu, seed)
+        r.update({"centre": [cx, cy], "radius": rad, "shape_u": shape_u, "tail_p": tail_p, "speciation": nu,
+                  "seed": seed})
+        kat["clark2dt_runs"].append(r)
     kat["nonspatial_runs_exp"] = []
     for (w, h, deme, nu, seed) in [(2, 2, 2, 0.05, 3), (4, 3, 2, 0.02, 42)]:
         r = nonspatial_reference_run(w, h, deme, nu, seed, sampler=exp_next)

@@ -230,3 +230,13 @@ def test_turnover_map_reference_runs(oracle, kat):
         desc = se_desc(oracle, case)
         desc["turnover_map"] = np.array(case["turnover"], dtype=np.float64)
         check_run(oracle, desc, case)
+
+
+def test_clark2dt_reference_runs(oracle, kat):
+    """AlmostInfinite with Clark2Dt dispersal, a fat tail (p = 0.5) and the
+    pow-free case (p = 1), one circle wrapping across the plane's edge."""
+    for case in kat["clark2dt_runs"]:
+        desc = dict(kind=oracle.ALMOST_INFINITE_CLARK2DT, speciation_probability=case["speciation"],
+                    shape_u=case["shape_u"], tail_p=case["tail_p"], radius=case["radius"],
+                    centre_x=case["centre"][0], centre_y=case["centre"][1])
+        check_run(oracle, desc, case)
