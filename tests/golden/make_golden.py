@@ -410,6 +410,83 @@ class SpatiallyExplicitLandscape:
         return target % self.w, target // self.w
 
 
+def f64_bits(v):
+    return struct.unpack("<Q", struct.pack("<d", v))[0]
+
+
+def max_after(before, t):
+    """PositiveF64::max_after (positive_f64.rs:103-113) for finite times."""
+    if t > before:
+        return t
+    return struct.unpack("<d", struct.pack("<Q", f64_bits(before) + 1))[0]
+
+
+def canonical_run(land, nu, seed, step_slice=10, min_round_events=1 << 20, step_slice_max=1024, lam=0.5,
+                  dt=2.0, sampler=None):
+    """The GPU backend's own schedule: every round advances each live
+    lineage to a common horizon H' = H + clamp(ceil(min_round_events / n),
+    step_slice, step_slice_max) / lambda (lambda the largest habitable rate
+    of a turnover map), then merges lineages in identical state (location,
+    index, last event time) keeping the smallest global reference."""
+    sampler = sampler or poisson_next
+    g = Wy(seed_from_u64(seed))
+    turnover = getattr(land, "turnover", None)
+    lam_rounds = lam
+    if turnover:
+        lam_rounds = max(turnover[y][x] for y in range(land.h) for x in range(land.w) if land.habitat(x, y) > 0)
+    lins = land.origins()
+    horizon = min(l[1] for l in lins)
+    max_time = max(l[1] for l in lins)
+    steps = rounds = dedups = 0
+    events = []
+    while lins:
+        n = len(lins)
+        per = -(-min_round_events // n)
+        if step_slice_max and per > step_slice_max:
+            per = step_slice_max
+        per = max(per, step_slice)
+        nh = horizon + float(per) / lam_rounds
+        rounds += 1
+        alive = []
+        for lin in lins:
+            dead = False
+            while True:
+                before = lin[1]
+                rate = turnover[lin[3]][lin[2]] if turnover else lam
+                t, _ = sampler(g, land.injection(lin[2], lin[3], lin[4]), before, rate, dt)
+                nxt = max_after(before, t)
+                if nxt >= nh:
+                    break
+                us = g.co()
+                steps += 1
+                max_time = max(max_time, nxt)
+                if us < land.nu(lin[2], lin[3], nu):
+                    events.append((nxt, lin[2], lin[3], lin[4], lin[1], lin[0]))
+                    dead = True
+                    break
+                tx, ty = land.disperse(g, lin[2], lin[3])
+                ti = int(math.floor(g.co() * float(land.habitat(tx, ty))))
+                lin = [lin[0], nxt, tx, ty, ti]
+            if not dead:
+                alive.append(lin)
+        alive.sort(key=lambda l: (l[2], l[3], l[4], f64_bits(l[1]), l[0]))
+        lins = []
+        for l in alive:
+            if lins and lins[-1][2:5] == l[2:5] and f64_bits(lins[-1][1]) == f64_bits(l[1]):
+                dedups += 1
+                continue
+            lins.append(l)
+        horizon = nh
+    events.sort(key=lambda e: (f64_bits(e[0]), e[1], e[2], e[3], e[1], e[2], e[3], f64_bits(e[4]), e[5]))
+    species, last = 0, None
+    for e in events:
+        key = (e[0], e[1], e[2], e[3])
+        species += key != last
+        last = key
+    return {"steps": steps, "rounds": rounds, "dedups": dedups, "time": max_time, "biodiversity": species,
+            "events": [[e[5], e[4], e[0], e[1], e[2], e[3]] for e in events]}
+
+
 def nonspatial_reference_run(w, h, deme, nu, seed, step_slice=10, dedup=1.0, event_slice=2.0,
                              lam=0.5, dt=2.0, sampler=None):
     return reference_run(NonSpatialLandscape(w, h, deme), nu, seed, step_slice, dedup, event_slice, lam,
@@ -648,6 +725,28 @@ def main():
         r.update({"centre": [cx, cy], "radius": rad, "shape_u": shape_u, "tail_p": tail_p, "speciation": nu,
                   "seed": seed})
         kat["clark2dt_runs"].append(r)
+    canon = []
+    hab, disp = se_case(3, 3, 0)
+    turnover = kat["turnover_map_runs"][0]["turnover"]
+    for name, params, land, nu, seed, sampler in [
+            ("ns", {"width": 4, "height": 3, "deme": 2}, NonSpatialLandscape(4, 3, 2), 0.02, 42, None),
+            ("ns", {"width": 3, "height": 3, "deme": 2}, NonSpatialLandscape(3, 3, 2), 0.03, 5, exp_next),
+            ("si", {"width": 3, "height": 2, "deme": 2, "meta_width": 40, "meta_height": 1, "meta_deme": 1,
+                    "migration": 0.2}, SpatiallyImplicitLandscape(3, 2, 2, 40, 1, 1, 0.2), 0.05, 5, None),
+            ("ai", {"centre": [2 ** 31 - 1, 2 ** 31 - 1], "radius": 2, "sigma": 3.0},
+             AlmostInfiniteLandscape(2 ** 31 - 1, 2 ** 31 - 1, 2, 3.0), 0.05, 7, None),
+            ("se", {"width": 3, "height": 3, "habitat": hab, "dispersal": disp},
+             SpatiallyExplicitLandscape(hab, disp), 0.05, 4, None),
+            ("se", {"width": 3, "height": 3, "habitat": hab, "dispersal": disp, "turnover": turnover},
+             SpatiallyExplicitLandscape(hab, disp, turnover), 0.05, 14, None)]:
+        for step_slice_max in (1024, 10):
+            r = canonical_run(land, nu, seed, step_slice_max=step_slice_max, sampler=sampler)
+            r.update(params)
+            r.update({"case": name, "speciation": nu, "seed": seed, "step_slice": 10,
+                      "min_round_events": 1 << 20, "step_slice_max": step_slice_max,
+                      "sampler": "exp" if sampler else "poisson"})
+            canon.append(r)
+    kat["canonical_runs"] = canon
     kat["nonspatial_runs_exp"] = []
     for (w, h, deme, nu, seed) in [(2, 2, 2, 0.05, 3), (4, 3, 2, 0.02, 42)]:
         r = nonspatial_reference_run(w, h, deme, nu, seed, sampler=exp_next)

@@ -240,3 +240,41 @@ def test_clark2dt_reference_runs(oracle, kat):
                     shape_u=case["shape_u"], tail_p=case["tail_p"], radius=case["radius"],
                     centre_x=case["centre"][0], centre_y=case["centre"][1])
         check_run(oracle, desc, case)
+
+
+def canonical_desc(oracle, case):
+    """The scenario a canonical-schedule vector was generated on."""
+    nu = case["speciation"]
+    if case["case"] == "ns":
+        return dict(kind=oracle.NON_SPATIAL, speciation_probability=nu, width=case["width"],
+                    height=case["height"], deme=case["deme"])
+    if case["case"] == "si":
+        return dict(kind=oracle.SPATIALLY_IMPLICIT, speciation_probability=nu, width=case["width"],
+                    height=case["height"], deme=case["deme"], meta_width=case["meta_width"],
+                    meta_height=case["meta_height"], meta_deme=case["meta_deme"],
+                    migration_probability=case["migration"])
+    if case["case"] == "ai":
+        return dict(kind=oracle.ALMOST_INFINITE_NORMAL, speciation_probability=nu, sigma=case["sigma"],
+                    radius=case["radius"], centre_x=case["centre"][0], centre_y=case["centre"][1])
+    desc = se_desc(oracle, case)
+    if "turnover" in case:
+        desc["turnover_map"] = np.array(case["turnover"], dtype=np.float64)
+    return desc
+
+
+def test_canonical_schedule_runs(oracle, kat):
+    """The horizon-synchronised schedule the CUDA backend runs: per-round
+    horizons from the live lineage count, each lineage advanced to the
+    horizon, identical states merged keeping the smallest reference. Pins the
+    step, round and merge counts as well as the speciation stream, with long
+    rounds (step_slice_max 1024: one round) and short ones (10)."""
+    for case in kat["canonical_runs"]:
+        sampler = oracle.SAMPLER_EXP if case["sampler"] == "exp" else oracle.SAMPLER_POISSON
+        r = oracle.simulate(canonical_desc(oracle, case), case["seed"], mode=oracle.MODE_CANONICAL,
+                            step_slice=case["step_slice"], min_round_events=case["min_round_events"],
+                            step_slice_max=case["step_slice_max"], event_time_sampler=sampler)
+        assert (r.steps, r.n_rounds, r.n_dedup, r.time, r.biodiversity) == (
+            case["steps"], case["rounds"], case["dedups"], case["time"], case["biodiversity"]), case["case"]
+        got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
+                int(e["y"]), int(e["index"])] for e in r.speciation]
+        assert got == case["events"], case["case"]
