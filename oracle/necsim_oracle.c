@@ -204,6 +204,11 @@ typedef struct sim_t {
     const uint32_t *habitat;
     uint64_t *injection;  /* prefix sums, n_cells + 1 */
     alias_t alias;
+    /* WrappingNoise */
+    int64_t perm[2048];   /* OpenSimplexNoise permutation */
+    double coverage, scale, persistence, threshold, p_self;
+    uint64_t octaves;
+    int fault;            /* -6 once a dispersal ran out of rejections */
     rng_t rng;
 } sim_t;
 
@@ -223,7 +228,9 @@ static inline uint64_t injection(const sim_t *s, uint32_t x, uint32_t y, uint32_
             return non_spatial_injection(&s->local, s->deme, x, y, i);
         return non_spatial_injection(&s->meta, s->meta_deme, x, y, i);
     case ORACLE_ALMOST_INFINITE_NORMAL:
-        /* habitat/almost_infinite.rs:66-70 */
+    case ORACLE_WRAPPING_NOISE:
+        /* habitat/almost_infinite.rs:66-70 (WrappingNoise defers to it,
+         * habitat/wrapping_noise/mod.rs:170-175) */
         return ((uint64_t)y << 32) | (uint64_t)x;
     default: {
         /* habitat/in_memory.rs:70-80 */
@@ -233,6 +240,8 @@ static inline uint64_t injection(const sim_t *s, uint32_t x, uint32_t y, uint32_
     }
     }
 }
+
+static double noise_octaves(const sim_t *s, uint32_t x, uint32_t y);
 
 static inline uint32_t habitat_at(const sim_t *s, uint32_t x, uint32_t y) {
     switch (s->kind) {
@@ -245,6 +254,11 @@ static inline uint32_t habitat_at(const sim_t *s, uint32_t x, uint32_t y) {
         return 0;
     case ORACLE_ALMOST_INFINITE_NORMAL:
         return 1;
+    case ORACLE_WRAPPING_NOISE:
+        /* habitat/wrapping_noise/mod.rs:148-168 */
+        if (s->coverage <= 0.0) return 0;
+        if (s->coverage >= 1.0) return 1;
+        return noise_octaves(s, x, y) <= s->threshold ? 1u : 0u;
     default: {
         uint64_t cell = (uint64_t)y * s->local.w + (uint64_t)x;
         return cell < s->local.w * s->local.h ? s->habitat[cell] : 0;
@@ -420,6 +434,183 @@ void oracle_normal_dispersal(uint64_t draw0, uint64_t draw1, double sigma, uint3
     normal_disperse_from_draws(draw0, draw1, sigma, x, y, tx, ty);
 }
 
+/* ------------------------------------------------------------------------ */
+/* WrappingNoise: OpenSimplex 2D noise with wrapping                        */
+/* habitat/wrapping_noise/{mod.rs, opensimplex_noise/{mod.rs,               */
+/*                         open_simplex_noise_2d.rs,utils.rs}}              */
+/* ------------------------------------------------------------------------ */
+#define OS_STRETCH (-0.211324865405187) /* open_simplex_noise_2d.rs:9, as written there */
+#define OS_SQUISH 0.366025403784439     /* open_simplex_noise_2d.rs:10 */
+#define NOISE_2_32 4294967296.0         /* (u32::MAX as f64) + 1.0 */
+#define NOISE_FRAC_1_PI 0.318309886183790671537767526745028724
+#define NOISE_SQRT_2 1.41421356237309504880168872420969808
+
+/* Rust's `v as i64`: truncating, saturating, NaN -> 0 */
+static inline int64_t sat_i64(double v) {
+    if (v != v) return 0;
+    if (v >= 9223372036854775808.0) return INT64_MAX;
+    if (v <= -9223372036854775808.0) return INT64_MIN;
+    return (int64_t)v;
+}
+
+/* opensimplex_noise/mod.rs:76-96 generate_perm_array: the i128 seed is
+ * never advanced, so every swap index comes from the same value */
+static void opensimplex_perm(int64_t seed, int64_t *perm) {
+    int64_t source[2048];
+    __int128 a = (__int128)seed * (__int128)6364136223846793005LL + (__int128)1442695040888963407LL;
+    for (int64_t i = 0; i < 2048; ++i) source[i] = i;
+    for (int64_t i = 2047; i >= 0; --i) {
+        int64_t r = (int64_t)((a + 31) % (__int128)(i + 1)); /* C's % truncates, like Rust's */
+        if (r < 0) r += i + 1;
+        perm[i] = source[r];
+        source[r] = source[i];
+    }
+}
+
+/* open_simplex_noise_2d.rs:21-59 extrapolate: wrap the lattice point into
+ * [0, wrap), then the gradient (+-5, +-2) or (+-2, +-5) from two perm reads */
+static double os_extrapolate(const int64_t *perm, double gx, double gy, double dx, double dy,
+                             double wrap) {
+    gx = floor(gx - floor(gx / wrap) * wrap);
+    gy = floor(gy - floor(gy / wrap) * wrap);
+    /* i64 arithmetic (wrapping), masked to the low byte */
+    uint64_t i0 = ((uint64_t)perm[(uint64_t)sat_i64(gx) & 0xFF] + (uint64_t)sat_i64(gy)) & 0xFF;
+    uint64_t idx = ((uint64_t)perm[i0] & 0x0E) >> 1;
+    double px = (idx & 1) == 0 ? 5.0 : 2.0;
+    double py = (idx & 1) == 0 ? 2.0 : 5.0;
+    if (idx & 2) px *= -1.0;
+    if (idx & 4) py *= -1.0;
+    return px * dx + py * dy;
+}
+
+/* opensimplex_noise/utils.rs:5-23 contribute */
+static double os_contribute(const int64_t *perm, double dx, double dy, double ox, double oy, double gx,
+                            double gy, double wrap) {
+    double ds = dx + dy;
+    double sx = (ox - dx) - OS_SQUISH * ds;
+    double sy = (oy - dy) - OS_SQUISH * ds;
+    double attn = 2.0 - (sx * sx + sy * sy);
+    if (attn <= 0.0) return 0.0;
+    double a2 = attn * attn;
+    double a4 = a2 * a2;
+    return a4 * os_extrapolate(perm, gx + dx, gy + dy, sx, sy, wrap);
+}
+
+/* open_simplex_noise_2d.rs:61-128 eval, get_value, evaluate_inside_triangle */
+static double os_eval(const int64_t *perm, double x, double y, double wrap) {
+    double s = x + y;
+    double ix = x + OS_SQUISH * s, iy = y + OS_SQUISH * s; /* pre-squished input */
+    double s2 = ix + iy;
+    double stx = ix + OS_STRETCH * s2, sty = iy + OS_STRETCH * s2;
+    double gx = floor(stx), gy = floor(sty);
+    double gs = gx + gy;
+    double sqx = gx + OS_SQUISH * gs, sqy = gy + OS_SQUISH * gs;
+    double insx = stx - gx, insy = sty - gy;
+    double ox = ix - sqx, oy = iy - sqy;
+    double value = os_contribute(perm, 1.0, 0.0, ox, oy, gx, gy, wrap) +
+                   os_contribute(perm, 0.0, 1.0, ox, oy, gx, gy, wrap);
+    double in_sum = insx + insy;
+    double f = in_sum <= 1.0 ? 0.0 : 1.0;
+    double z = 1.0 + f - in_sum;
+    double px, py;
+    if (z > insx || z > insy) {
+        if (insx > insy) {
+            px = 1.0 + f;
+            py = -1.0 + f;
+        } else {
+            px = -1.0 + f;
+            py = 1.0 + f;
+        }
+    } else {
+        px = 1.0 - f;
+        py = 1.0 - f;
+    }
+    double tri = os_contribute(perm, 0.0 + f, 0.0 + f, ox, oy, gx, gy, wrap) +
+                 os_contribute(perm, px, py, ox, oy, gx, gy, wrap);
+    return (value + tri) / 47.0;
+}
+
+/* habitat/wrapping_noise/mod.rs:216-249 sum_noise_octaves */
+static double noise_sum(const int64_t *perm, double persistence, double scale, uint64_t octaves, uint32_t x,
+                        uint32_t y) {
+    double max_amplitude = 0.0, amplitude = 1.0;
+    double frequency = scale * NOISE_FRAC_1_PI * 3.0;
+    double result = 0.0;
+    for (uint64_t o = 0; o < octaves; ++o) {
+        double wrap = round(NOISE_2_32 * frequency);
+        double fixed = wrap / NOISE_2_32;
+        result += os_eval(perm, (double)x * fixed, (double)y * fixed, wrap) * amplitude;
+        max_amplitude += amplitude;
+        amplitude *= persistence;
+        frequency *= 2.0;
+    }
+    return result / max_amplitude;
+}
+
+static double noise_octaves(const sim_t *s, uint32_t x, uint32_t y) {
+    return noise_sum(s->perm, s->persistence, s->scale, s->octaves, x, y);
+}
+
+/* f64::total_cmp */
+static int total_cmp(const void *pa, const void *pb) {
+    int64_t a, b;
+    memcpy(&a, pa, 8);
+    memcpy(&b, pb, 8);
+    a ^= (int64_t)((uint64_t)(a >> 63) >> 1);
+    b ^= (int64_t)((uint64_t)(b >> 63) >> 1);
+    return a < b ? -1 : (a > b ? 1 : 0);
+}
+
+/* habitat/wrapping_noise/mod.rs:47-99: the noise at 2^16 locations drawn by
+ * WyHash::from_seed(seed.to_le_bytes()), sorted, read at the coverage */
+static int noise_threshold(const int64_t *perm, int64_t seed, double coverage, double scale, double persistence,
+                           uint64_t octaves, double *out) {
+    enum { N = 1 << 16 };
+    double *samples = (double *)malloc(N * sizeof(double));
+    if (!samples) return -1;
+    rng_t g = {(uint64_t)seed, (uint64_t)seed, 0, 0};
+    for (int j = 0; j < N; ++j) {
+        uint64_t loc = rng_sample_u64(&g);
+        samples[j] = noise_sum(perm, persistence, scale, octaves, (uint32_t)loc, (uint32_t)(loc >> 32));
+    }
+    qsort(samples, N, sizeof(double), total_cmp);
+    double k = floor((double)N * coverage);
+    uint64_t at = k >= (double)(N - 1) ? (uint64_t)(N - 1) : (uint64_t)k;
+    *out = samples[at];
+    free(samples);
+    return 0;
+}
+
+/* dispersal_sampler/wrapping_noise.rs:89-110 with almost_infinite_normal.rs:22-37:
+ * ps = erf(0.5 / (sigma * sqrt 2))^2 (libm's erf; the C library's here),
+ * self-dispersal ps / (ps + (1 - ps) * coverage) */
+static double noise_self_dispersal(double sigma, double coverage) {
+    double p1 = sigma > 0.0 ? erf(0.5 / (sigma * NOISE_SQRT_2)) : 1.0;
+    double ps = p1 * p1;
+    double pout = (1.0 - ps) * coverage;
+    return ps / (ps + pout);
+}
+
+double oracle_wrapping_noise(int64_t seed, double scale, double persistence, uint64_t octaves, uint32_t x,
+                             uint32_t y) {
+    int64_t perm[2048];
+    opensimplex_perm(seed, perm);
+    return noise_sum(perm, persistence, scale, octaves, x, y);
+}
+
+double oracle_wrapping_noise_threshold(int64_t seed, double coverage, double scale, double persistence,
+                                       uint64_t octaves) {
+    int64_t perm[2048];
+    double t = NAN;
+    opensimplex_perm(seed, perm);
+    if (noise_threshold(perm, seed, coverage, scale, persistence, octaves, &t)) return NAN;
+    return t;
+}
+
+double oracle_wrapping_noise_self_dispersal(double sigma, double coverage) {
+    return noise_self_dispersal(sigma, coverage);
+}
+
 /* alias/packed.rs:135-163 sample_event_with_cdf_limit (limit = 1) */
 static inline uint32_t alias_sample(const alias_t *a, uint64_t start, uint64_t end, rng_t *g) {
     uint64_t len = end - start;
@@ -475,6 +666,28 @@ static inline void disperse(sim_t *s, uint32_t x, uint32_t y, uint32_t *tx, uint
             normal_disperse_from_draws(d0, d1, s->sigma, x, y, tx, ty);
         break;
     }
+    case ORACLE_WRAPPING_NOISE:
+        /* dispersal_sampler/wrapping_noise.rs:42-87: sample_event(p_self)
+         * (rng.rs:97-102), else Normal draws until the target is habitable
+         * and not the origin (bounded here, unbounded in the reference) */
+        if (u01_closed_open(g) < s->p_self) {
+            *tx = x;
+            *ty = y;
+            break;
+        }
+        for (uint32_t k = 0;; ++k) {
+            if (k == ORACLE_MAX_DISPERSAL_REJECTIONS) {
+                s->fault = -6;
+                *tx = x;
+                *ty = y;
+                break;
+            }
+            uint64_t d0 = rng_sample_u64(g);
+            uint64_t d1 = rng_sample_u64(g);
+            normal_disperse_from_draws(d0, d1, s->sigma, x, y, tx, ty);
+            if (habitat_at(s, *tx, *ty) != 0 && !(*tx == x && *ty == y)) break;
+        }
+        break;
     default:
         spatially_explicit_disperse(s, g, x, y, tx, ty);
         break;
@@ -762,6 +975,25 @@ static int sim_init(sim_t *s, const oracle_scenario *sc, const oracle_args *args
     case ORACLE_ALMOST_INFINITE_CLARK2DT:
         s->local = (extent_t){0, 0, 1ULL << 32, 1ULL << 32};
         break;
+    case ORACLE_WRAPPING_NOISE:
+        /* WrappingNoiseArguments (wrapping_noise.rs:39-48): coverage in [0, 1],
+         * scale and persistence in (0, 1], octaves >= 1, sigma >= 0 */
+        if (!(sc->coverage >= 0.0 && sc->coverage <= 1.0) || !(sc->scale > 0.0 && sc->scale <= 1.0) ||
+            !(sc->persistence > 0.0 && sc->persistence <= 1.0) || sc->octaves == 0 ||
+            !(sc->sigma >= 0.0) || !isfinite(sc->sigma) || sc->sample_width == 0 || sc->sample_height == 0 ||
+            sc->sample_width > (1ULL << 32) || sc->sample_height > (1ULL << 32))
+            return -2;
+        s->local = (extent_t){0, 0, 1ULL << 32, 1ULL << 32};
+        s->coverage = sc->coverage;
+        s->scale = sc->scale;
+        s->persistence = sc->persistence;
+        s->octaves = sc->octaves;
+        opensimplex_perm(sc->noise_seed, s->perm);
+        if (noise_threshold(s->perm, sc->noise_seed, sc->coverage, sc->scale, sc->persistence, sc->octaves,
+                            &s->threshold))
+            return -1;
+        s->p_self = noise_self_dispersal(sc->sigma, sc->coverage);
+        break;
     case ORACLE_SPATIALLY_EXPLICIT: {
         if (!sc->width || !sc->height || !sc->habitat || !sc->dispersal) return -2;
         s->local = (extent_t){0, 0, sc->width, sc->height};
@@ -850,6 +1082,23 @@ static int64_t enumerate_origins(const oracle_scenario *sc, const sim_t *s, line
             }
         break;
     }
+    case ORACLE_WRAPPING_NOISE:
+        /* singleton_demes/rectangle.rs:93-120: the habitable locations of the
+         * sample extent in its row-major order (extent.rs:80-100, wrapping) */
+        for (uint64_t yy = 0; yy < sc->sample_height; ++yy)
+            for (uint64_t xx = 0; xx < sc->sample_width; ++xx) {
+                uint32_t x = sc->sample_x + (uint32_t)xx, y = sc->sample_y + (uint32_t)yy;
+                if (habitat_at(s, x, y) == 0) continue;
+                if (out && n < cap) {
+                    out[n].x = x;
+                    out[n].y = y;
+                    out[n].i = 0;
+                    out[n].last = 0.0;
+                    out[n].gref = ((uint64_t)y << 32) | x;
+                }
+                n++;
+            }
+        break;
     default:
         for (uint64_t y = 0; y < sc->height; ++y)
             for (uint64_t x = 0; x < sc->width; ++x) {
@@ -1097,6 +1346,7 @@ static int run_slice(sim_t *s, lineage_t *lin, double min_event_time, uint64_t s
         }
         uint32_t tx, ty;
         disperse(s, lin->x, lin->y, &tx, &ty);
+        if (s->fault) return s->fault;
         uint32_t ti = coalescence_index(s, tx, ty);
         if (report_dispersal) {
             event_t e = {lin->gref, lin->last, next, lin->x, lin->y, lin->i, tx, ty, ti, 0};
@@ -1298,7 +1548,7 @@ static int simulate_reference(sim_t *s, const oracle_args *args, lineage_t *init
             if (has_active) {
                 if (run_slice(s, &active, min_event_time, args->step_slice, level,
                               args->report_dispersal, &slow_ev, &fast_ev, water, &so))
-                    return -1;
+                    return s->fault ? s->fault : -1;
                 new_steps = so.steps;
                 new_time = so.new_time;
                 if (so.peeked) {
@@ -1384,7 +1634,7 @@ static int simulate_canonical(sim_t *s, const oracle_args *args, lineage_t *lins
             slice_out_t so;
             if (run_slice(s, &lins[j], min_event_time, UINT64_MAX, next_horizon,
                           args->report_dispersal, &ev, &none, INFINITY, &so))
-                return -1;
+                return s->fault ? s->fault : -1;
             total_steps += so.steps;
             if (so.new_time > max_time) max_time = so.new_time;
             if (so.alive) lins[m++] = lins[j];

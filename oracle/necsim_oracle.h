@@ -31,6 +31,7 @@ enum {
     ORACLE_ALMOST_INFINITE_NORMAL = 2,
     ORACLE_SPATIALLY_EXPLICIT = 3,
     ORACLE_ALMOST_INFINITE_CLARK2DT = 4,
+    ORACLE_WRAPPING_NOISE = 5,
 };
 
 /* Scenario description (same layout as the product's necsim_scenario). */
@@ -48,6 +49,14 @@ typedef struct oracle_scenario {
     const double *dispersal;                  /* SE: (w*h) x (w*h) row-major */
     double shape_u, tail_p;                   /* AlmostInfinite Clark2Dt dispersal */
     const double *turnover;                   /* SE turnover map, width*height row-major (NULL: uniform) */
+    /* WrappingNoise (rustcoalescence/scenarios/src/wrapping_noise.rs); `sigma` is its
+     * Normal dispersal */
+    int64_t noise_seed;
+    double coverage;                          /* [0, 1] */
+    double scale, persistence;                /* (0, 1] */
+    uint64_t octaves;                         /* >= 1 */
+    uint32_t sample_x, sample_y;              /* Rectangle sample: LandscapeExtent origin */
+    uint64_t sample_width, sample_height;     /* 1 ..= 2^32 */
 } oracle_scenario;
 
 enum { ORACLE_MODE_REFERENCE = 0, ORACLE_MODE_CANONICAL = 1 };
@@ -121,7 +130,10 @@ int oracle_simulate(const oracle_scenario *sc, const oracle_args *args, uint64_t
 /* Same as oracle_simulate but starting from caller-provided lineages
  * (resume), with min_event_time = resume_time. */
 /* resume the given lineages; -5 when one is off the habitat or its deme
- * (the reference's ResumeError::Sample) */
+ * (the reference's ResumeError::Sample).  Both entry points return -6 when a
+ * WrappingNoise dispersal rejects ORACLE_MAX_DISPERSAL_REJECTIONS targets in
+ * a row, where the reference keeps drawing. */
+#define ORACLE_MAX_DISPERSAL_REJECTIONS (1u << 20)
 int oracle_simulate_lineages(const oracle_scenario *sc, const oracle_args *args, uint64_t seed,
                              const oracle_lineage *lineages, uint64_t n_lineages,
                              double resume_time, double pause_before, oracle_result *out,
@@ -170,6 +182,15 @@ void oracle_clark2dt_dispersal(uint64_t draw0, uint64_t draw1, double shape_u, d
                                uint32_t y, uint32_t *tx, uint32_t *ty);
 void oracle_normal_dispersal(uint64_t draw0, uint64_t draw1, double sigma, uint32_t x, uint32_t y,
                              uint32_t *tx, uint32_t *ty);
+
+/* WrappingNoise: the octave noise at (x, y) (sum_noise_octaves), the
+ * habitat threshold of WrappingNoiseHabitat::new, and the self-dispersal
+ * probability of the approximate Normal dispersal */
+double oracle_wrapping_noise(int64_t seed, double scale, double persistence, uint64_t octaves, uint32_t x,
+                             uint32_t y);
+double oracle_wrapping_noise_threshold(int64_t seed, double coverage, double scale, double persistence,
+                                       uint64_t octaves);
+double oracle_wrapping_noise_self_dispersal(double sigma, double coverage);
 
 #ifdef __cplusplus
 }

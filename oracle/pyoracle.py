@@ -17,6 +17,7 @@ SPATIALLY_IMPLICIT = 1
 ALMOST_INFINITE_NORMAL = 2
 ALMOST_INFINITE_CLARK2DT = 4
 SPATIALLY_EXPLICIT = 3
+WRAPPING_NOISE = 5
 
 MODE_REFERENCE = 0
 MODE_CANONICAL = 1
@@ -48,6 +49,15 @@ class OracleScenario(ctypes.Structure):
         ("shape_u", ctypes.c_double),
         ("tail_p", ctypes.c_double),
         ("turnover", ctypes.POINTER(ctypes.c_double)),
+        ("noise_seed", ctypes.c_int64),
+        ("coverage", ctypes.c_double),
+        ("scale", ctypes.c_double),
+        ("persistence", ctypes.c_double),
+        ("octaves", ctypes.c_uint64),
+        ("sample_x", ctypes.c_uint32),
+        ("sample_y", ctypes.c_uint32),
+        ("sample_width", ctypes.c_uint64),
+        ("sample_height", ctypes.c_uint64),
     ]
 
 
@@ -176,6 +186,13 @@ def lib():
                                                 ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                                 ctypes.POINTER(ctypes.c_uint32)]
         L.oracle_clark2dt_dispersal.restype = None
+        f64 = ctypes.c_double
+        L.oracle_wrapping_noise.argtypes = [ctypes.c_int64, f64, f64, u64, ctypes.c_uint32, ctypes.c_uint32]
+        L.oracle_wrapping_noise.restype = f64
+        L.oracle_wrapping_noise_threshold.argtypes = [ctypes.c_int64, f64, f64, f64, u64]
+        L.oracle_wrapping_noise_threshold.restype = f64
+        L.oracle_wrapping_noise_self_dispersal.argtypes = [f64, f64]
+        L.oracle_wrapping_noise_self_dispersal.restype = f64
         _lib = L
     return _lib
 
@@ -201,6 +218,13 @@ def make_scenario(desc):
     sc.radius = desc.get("radius", 0)
     sc.shape_u = desc.get("shape_u", 0.0)
     sc.tail_p = desc.get("tail_p", 0.0)
+    sc.noise_seed = desc.get("noise_seed", 0)
+    sc.coverage = desc.get("coverage", 0.0)
+    sc.scale = desc.get("scale", 0.0)
+    sc.persistence = desc.get("persistence", 0.0)
+    sc.octaves = desc.get("octaves", 0)
+    sample = desc.get("sample", (0, 0, 0, 0))  # Rectangle: (x, y, width, height)
+    sc.sample_x, sc.sample_y, sc.sample_width, sc.sample_height = sample
     keep = []
     if desc.get("habitat") is not None:
         h = np.ascontiguousarray(desc["habitat"], dtype=np.uint32)
@@ -376,3 +400,18 @@ def clark2dt_dispersal(d0, d1, shape_u, tail_p, x, y):
     tx, ty = ctypes.c_uint32(), ctypes.c_uint32()
     lib().oracle_clark2dt_dispersal(d0, d1, shape_u, tail_p, x, y, ctypes.byref(tx), ctypes.byref(ty))
     return tx.value, ty.value
+
+
+def wrapping_noise(seed, scale, persistence, octaves, x, y):
+    """sum_noise_octaves at (x, y) for the noise seeded with `seed`."""
+    return lib().oracle_wrapping_noise(seed, scale, persistence, octaves, x, y)
+
+
+def wrapping_noise_threshold(seed, coverage, scale, persistence, octaves):
+    """WrappingNoiseHabitat's habitable-noise threshold."""
+    return lib().oracle_wrapping_noise_threshold(seed, coverage, scale, persistence, octaves)
+
+
+def wrapping_noise_self_dispersal(sigma, coverage):
+    """The approximate Normal dispersal's self-dispersal probability."""
+    return lib().oracle_wrapping_noise_self_dispersal(sigma, coverage)

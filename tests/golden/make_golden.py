@@ -18,6 +18,10 @@ through it the GPU backend) is pinned by a second implementation:
     (alias/packed.rs:59-163, packed_separable_alias/{mod,dispersal}.rs)
   * full reference-schedule runs of tiny NonSpatial, SpatiallyImplicit,
     AlmostInfinite and SpatiallyExplicit scenarios (monolithic/mod.rs:43-270)
+  * WrappingNoise: OpenSimplex 2D noise with wrapping and its octave sum
+    (habitat/wrapping_noise/**), the coverage threshold, the rectangle origin
+    sampler and the rejection-sampled Normal dispersal
+    (dispersal_sampler/wrapping_noise.rs), with full tiny runs
 
 Run:  python tests/golden/make_golden.py
 """
@@ -309,6 +313,210 @@ class AlmostInfiniteLandscape:
 
     def disperse(self, g, x, y):
         return normal_dispersal(g.u64(), g.u64(), self.sigma, x, y)
+
+
+FRAC_1_PI = float("0.318309886183790671537767526745028724")  # core::f64::consts::FRAC_1_PI
+SQRT_2 = float("1.41421356237309504880168872420969808")     # core::f64::consts::SQRT_2
+OS_STRETCH = float("-0.211324865405187")  # open_simplex_noise_2d.rs:9, as written there
+OS_SQUISH = float("0.366025403784439")    # open_simplex_noise_2d.rs:10
+F64_2_32 = 4294967296.0
+
+
+def f64_floor(v):
+    return v if not math.isfinite(v) else float(math.floor(v))
+
+
+def f64_round(v):
+    """f64::round: half away from zero (v - trunc(v) is exact)."""
+    if not math.isfinite(v):
+        return v
+    t = float(math.trunc(v))
+    if abs(v - t) >= 0.5:
+        t += math.copysign(1.0, v)
+    return t
+
+
+def f64_div(a, b):
+    """IEEE division, also by zero."""
+    if b != 0.0:
+        return a / b
+    if a != a or a == 0.0:
+        return math.nan
+    return math.copysign(math.inf, a) * math.copysign(1.0, b)
+
+
+def as_i64(v):
+    """Rust's `v as i64`: truncation, saturating, NaN -> 0."""
+    if v != v:
+        return 0
+    if v >= 9223372036854775808.0:
+        return (1 << 63) - 1
+    if v <= -9223372036854775808.0:
+        return -(1 << 63)
+    return int(v)
+
+
+def opensimplex_perm(seed):
+    """generate_perm_array (opensimplex_noise/mod.rs:76-96): a Fisher-Yates
+    style shuffle of 0..2048 whose i128 seed is never advanced, so the swap
+    index at i is (seed * 6364136223846793005 + 1442695040888963407 + 31)
+    mod (i + 1) (a truncated remainder made non-negative)."""
+    a = seed * 6364136223846793005 + 1442695040888963407 + 31
+    source = list(range(2048))
+    perm = [0] * 2048
+    for i in range(2047, -1, -1):
+        r = abs(a) % (i + 1)
+        if a < 0:
+            r = -r
+        if r < 0:
+            r += i + 1
+        perm[i] = source[r]
+        source[r] = source[i]
+    return perm
+
+
+def os_extrapolate(perm, gx, gy, dx, dy, wrap):
+    """OpenSimplexNoise2D::extrapolate (open_simplex_noise_2d.rs:21-59): the
+    grid point wrapped into [0, wrap), its gradient from two perm lookups."""
+    gx = f64_floor(gx - f64_floor(f64_div(gx, wrap)) * wrap)
+    gy = f64_floor(gy - f64_floor(f64_div(gy, wrap)) * wrap)
+    i0 = (perm[as_i64(gx) & 0xFF] + as_i64(gy)) & 0xFF
+    idx = (perm[i0] & 0x0E) >> 1
+    px, py = (5.0, 2.0) if idx & 1 == 0 else (2.0, 5.0)
+    if idx & 2:
+        px *= -1.0
+    if idx & 4:
+        py *= -1.0
+    return px * dx + py * dy
+
+
+def os_contribute(perm, dx, dy, ox, oy, gx, gy, wrap):
+    """utils.rs:5-23 contribute for the 2D evaluator."""
+    ds = dx + dy
+    sx = (ox - dx) - OS_SQUISH * ds
+    sy = (oy - dy) - OS_SQUISH * ds
+    attn = 2.0 - (sx * sx + sy * sy)
+    if attn <= 0.0:
+        return 0.0
+    a2 = attn * attn
+    a4 = a2 * a2
+    return a4 * os_extrapolate(perm, gx + dx, gy + dy, sx, sy, wrap)
+
+
+def os_eval(perm, x, y, wrap):
+    """OpenSimplexNoise2D::eval + get_value + evaluate_inside_triangle
+    (open_simplex_noise_2d.rs:61-128): the input pre-squished so that the
+    wrap applies in lattice space."""
+    s = x + y
+    ix, iy = x + OS_SQUISH * s, y + OS_SQUISH * s
+    s = ix + iy
+    stx, sty = ix + OS_STRETCH * s, iy + OS_STRETCH * s
+    gx, gy = f64_floor(stx), f64_floor(sty)
+    gs = gx + gy
+    sqx, sqy = gx + OS_SQUISH * gs, gy + OS_SQUISH * gs
+    insx, insy = stx - gx, sty - gy
+    ox, oy = ix - sqx, iy - sqy
+
+    def c(dx, dy):
+        return os_contribute(perm, dx, dy, ox, oy, gx, gy, wrap)
+
+    value = c(1.0, 0.0) + c(0.0, 1.0)
+    in_sum = insx + insy
+    f = 0.0 if in_sum <= 1.0 else 1.0
+    z = 1.0 + f - in_sum
+    if z > insx or z > insy:
+        px, py = (1.0 + f, -1.0 + f) if insx > insy else (-1.0 + f, 1.0 + f)
+    else:
+        px, py = 1.0 - f, 1.0 - f
+    value = value + (c(0.0 + f, 0.0 + f) + c(px, py))
+    return value / 47.0
+
+
+def noise_octaves(perm, x, y, persistence, scale, octaves):
+    """sum_noise_octaves (habitat/wrapping_noise/mod.rs:216-249): each octave
+    wraps at round(2^32 * frequency), an integer lattice period."""
+    max_amp, amp = 0.0, 1.0
+    freq = scale * FRAC_1_PI * 3.0
+    result = 0.0
+    for _ in range(octaves):
+        wrap = f64_round(F64_2_32 * freq)
+        fixed = wrap / F64_2_32
+        result += os_eval(perm, float(x) * fixed, float(y) * fixed, wrap) * amp
+        max_amp += amp
+        amp *= persistence
+        freq *= 2.0
+    return result / max_amp
+
+
+def total_order_key(v):
+    """f64::total_cmp as a signed integer key."""
+    b = struct.unpack("<q", struct.pack("<d", v))[0]
+    return b ^ 0x7FFFFFFFFFFFFFFF if b < 0 else b
+
+
+def noise_threshold(perm, seed, coverage, scale, persistence, octaves):
+    """WrappingNoiseHabitat::new (habitat/wrapping_noise/mod.rs:47-99): the
+    noise at 2^16 locations drawn by WyHash::from_seed(seed.to_le_bytes())
+    (seed and state the i64's bits), sorted by total order, taken at
+    min(floor(2^16 * coverage), 2^16 - 1)."""
+    g = Wy(seed & M64)
+    samples = []
+    for _ in range(1 << 16):
+        loc = g.u64()
+        samples.append(noise_octaves(perm, loc & 0xFFFFFFFF, loc >> 32, persistence, scale, octaves))
+    samples.sort(key=total_order_key)
+    return samples[min(int(f64_floor(65536.0 * coverage)), 65535)]
+
+
+class WrappingNoiseLandscape:
+    """WrappingNoise (rustcoalescence/scenarios/src/wrapping_noise.rs): the
+    almost-infinite plane, habitable where the octave noise is at most the
+    coverage threshold (habitat/wrapping_noise/mod.rs:148-168), the rectangle
+    origin sampler over habitable cells (singleton_demes/rectangle.rs:93-120),
+    and approximate Normal dispersal (dispersal_sampler/wrapping_noise.rs):
+    self-dispersal with probability ps / (ps + (1 - ps) * coverage), ps the
+    Normal kernel's own (almost_infinite_normal.rs:22-37, erf from the C
+    library), else Normal draws rejected until the target is habitable and
+    not the origin."""
+
+    def __init__(self, seed, coverage, scale, persistence, octaves, sample, sigma):
+        self.seed, self.coverage, self.scale = seed, coverage, scale
+        self.persistence, self.octaves, self.sample, self.sigma = persistence, octaves, sample, sigma
+        self.perm = opensimplex_perm(seed)
+        self.threshold = noise_threshold(self.perm, seed, coverage, scale, persistence, octaves)
+        p1 = math.erf(0.5 / (sigma * SQRT_2)) if sigma > 0.0 else 1.0
+        ps = p1 * p1
+        self.p_self = ps / (ps + (1.0 - ps) * coverage)
+        self.rejections = 0
+
+    def noise(self, x, y):
+        return noise_octaves(self.perm, x, y, self.persistence, self.scale, self.octaves)
+
+    def habitat(self, x, y):
+        if self.coverage <= 0.0:
+            return 0
+        if self.coverage >= 1.0:
+            return 1
+        return 1 if self.noise(x, y) <= self.threshold else 0
+
+    def origins(self):
+        ox, oy, w, h = self.sample
+        return [[(y << 32) | x, 0.0, x, y, 0] for (x, y) in extent_iter(ox, oy, w, h) if self.habitat(x, y)]
+
+    def injection(self, x, y, i):
+        return (y << 32) | x
+
+    def nu(self, x, y, nu):
+        return nu
+
+    def disperse(self, g, x, y):
+        if g.co() < self.p_self:
+            return x, y
+        while True:
+            tx, ty = normal_dispersal(g.u64(), g.u64(), self.sigma, x, y)
+            if self.habitat(tx, ty) != 0 and (tx, ty) != (x, y):
+                return tx, ty
+            self.rejections += 1
 
 
 def alias_atoms(events):
@@ -725,6 +933,52 @@ def main():
         r.update({"centre": [cx, cy], "radius": rad, "shape_u": shape_u, "tail_p": tail_p, "speciation": nu,
                   "seed": seed})
         kat["clark2dt_runs"].append(r)
+    M32 = 0xFFFFFFFF
+    noise = []
+    for (seed, scale, persistence, octaves) in [(0, 0.07, 0.5, 16), (-7, 1.0, 1.0, 3), (123456789, 0.003, 0.8, 5),
+                                                (-(1 << 63), 0.5, 0.25, 2)]:
+        perm = opensimplex_perm(seed)
+        pts = [(0, 0), (1, 0), (0, 1), (M32, M32), (M32, 0), (12345, 67890), (1 << 31, (1 << 31) - 1)]
+        import random
+        rnd = random.Random(seed & 0xFFFF)
+        pts += [(rnd.randrange(1 << 32), rnd.randrange(1 << 32)) for _ in range(20)]
+        pts += [(rnd.randrange(64), rnd.randrange(64)) for _ in range(20)]
+        noise.append({"seed": seed, "scale": scale, "persistence": persistence, "octaves": octaves,
+                      "points": [[x, y, noise_octaves(perm, x, y, persistence, scale, octaves)] for x, y in pts]})
+    kat["wrapping_noise"] = noise
+    thresholds = []
+    for (seed, coverage, scale, persistence, octaves) in [(0, 0.5, 0.07, 0.5, 16), (-7, 0.25, 1.0, 1.0, 3),
+                                                          (123456789, 0.9, 0.003, 0.8, 5), (5, 0.0, 0.1, 0.5, 2),
+                                                          (5, 1.0, 0.1, 0.5, 2), (5, 0.99999, 0.1, 0.5, 2)]:
+        perm = opensimplex_perm(seed)
+        thresholds.append({"seed": seed, "coverage": coverage, "scale": scale, "persistence": persistence,
+                           "octaves": octaves,
+                           "threshold": noise_threshold(perm, seed, coverage, scale, persistence, octaves)})
+    kat["wrapping_noise_thresholds"] = thresholds
+    kat["wrapping_noise_self_dispersal"] = []
+    for sigma, coverage in [(0.0, 0.5), (0.05, 0.5), (1.0, 0.5), (3.0, 0.4), (3.0, 0.0), (100.0, 1.0)]:
+        p1 = math.erf(0.5 / (sigma * SQRT_2)) if sigma > 0.0 else 1.0
+        ps = p1 * p1
+        kat["wrapping_noise_self_dispersal"].append([sigma, coverage, ps / (ps + (1.0 - ps) * coverage)])
+    origins = []
+    for (seed, coverage, scale, persistence, octaves, sample) in [
+            (-7, 0.25, 1.0, 1.0, 3, (M32 - 19, 5, 40, 30)), (3, 0.4, 0.07, 0.5, 4, (0, 0, 24, 16))]:
+        land = WrappingNoiseLandscape(seed, coverage, scale, persistence, octaves, sample, 1.0)
+        origins.append({"seed": seed, "coverage": coverage, "scale": scale, "persistence": persistence,
+                        "octaves": octaves, "sample": list(sample),
+                        "origins": [[o[2], o[3]] for o in land.origins()]})
+    kat["wrapping_noise_origins"] = origins
+    kat["wrapping_noise_runs"] = []
+    wn_cases = [(3, 0.4, 0.07, 0.5, 4, (0, 0, 6, 5), 3.0, 0.05, 11),
+                (-2, 0.7, 0.2, 0.7, 3, (M32 - 2, M32 - 1, 5, 4), 1.5, 0.08, 12)]
+    for (seed, coverage, scale, persistence, octaves, sample, sigma, nu, rng_seed) in wn_cases:
+        land = WrappingNoiseLandscape(seed, coverage, scale, persistence, octaves, sample, sigma)
+        r = reference_run(land, nu, rng_seed)
+        assert land.rejections > 0
+        r.update({"noise_seed": seed, "coverage": coverage, "scale": scale, "persistence": persistence,
+                  "octaves": octaves, "sample": list(sample), "sigma": sigma, "speciation": nu, "seed": rng_seed,
+                  "rejections": land.rejections})
+        kat["wrapping_noise_runs"].append(r)
     canon = []
     hab, disp = se_case(3, 3, 0)
     turnover = kat["turnover_map_runs"][0]["turnover"]
@@ -738,7 +992,10 @@ def main():
             ("se", {"width": 3, "height": 3, "habitat": hab, "dispersal": disp},
              SpatiallyExplicitLandscape(hab, disp), 0.05, 4, None),
             ("se", {"width": 3, "height": 3, "habitat": hab, "dispersal": disp, "turnover": turnover},
-             SpatiallyExplicitLandscape(hab, disp, turnover), 0.05, 14, None)]:
+             SpatiallyExplicitLandscape(hab, disp, turnover), 0.05, 14, None),
+            ("wn", {"noise_seed": 3, "coverage": 0.4, "scale": 0.07, "persistence": 0.5, "octaves": 4,
+                    "sample": [0, 0, 6, 5], "sigma": 3.0},
+             WrappingNoiseLandscape(3, 0.4, 0.07, 0.5, 4, (0, 0, 6, 5), 3.0), 0.05, 11, None)]:
         for step_slice_max in (1024, 10):
             r = canonical_run(land, nu, seed, step_slice_max=step_slice_max, sampler=sampler)
             r.update(params)

@@ -256,6 +256,8 @@ def canonical_desc(oracle, case):
     if case["case"] == "ai":
         return dict(kind=oracle.ALMOST_INFINITE_NORMAL, speciation_probability=nu, sigma=case["sigma"],
                     radius=case["radius"], centre_x=case["centre"][0], centre_y=case["centre"][1])
+    if case["case"] == "wn":
+        return wn_desc(oracle, case)
     desc = se_desc(oracle, case)
     if "turnover" in case:
         desc["turnover_map"] = np.array(case["turnover"], dtype=np.float64)
@@ -278,3 +280,52 @@ def test_canonical_schedule_runs(oracle, kat):
         got = [[int(e["gref"]), float(e["prior_time"]), float(e["event_time"]), int(e["x"]),
                 int(e["y"]), int(e["index"])] for e in r.speciation]
         assert got == case["events"], case["case"]
+
+
+def wn_desc(oracle, case, speciation=None):
+    """A WrappingNoise scenario from a golden case."""
+    return dict(kind=oracle.WRAPPING_NOISE, speciation_probability=case.get("speciation", speciation or 0.5),
+                noise_seed=case["noise_seed"] if "noise_seed" in case else case["seed"], coverage=case["coverage"],
+                scale=case["scale"], persistence=case["persistence"], octaves=case["octaves"],
+                sample=tuple(case["sample"]), sigma=case.get("sigma", 1.0))
+
+
+def test_wrapping_noise_values(oracle, kat):
+    """OpenSimplex 2D with wrapping summed over octaves, at lattice corners,
+    the plane's far edge and random points, for seeds including i64::MIN."""
+    for case in kat["wrapping_noise"]:
+        for x, y, v in case["points"]:
+            got = oracle.wrapping_noise(case["seed"], case["scale"], case["persistence"], case["octaves"], x, y)
+            assert got == v, (case["seed"], x, y)
+
+
+def test_wrapping_noise_thresholds(oracle, kat):
+    """The coverage quantile of 2^16 WyHash-drawn locations' noise, including
+    coverage 0 and 1 (the ends of the sorted sample)."""
+    for case in kat["wrapping_noise_thresholds"]:
+        got = oracle.wrapping_noise_threshold(case["seed"], case["coverage"], case["scale"], case["persistence"],
+                                              case["octaves"])
+        assert got == case["threshold"], case
+
+
+def test_wrapping_noise_self_dispersal(oracle, kat):
+    for sigma, coverage, p in kat["wrapping_noise_self_dispersal"]:
+        assert oracle.wrapping_noise_self_dispersal(sigma, coverage) == p
+
+
+def test_wrapping_noise_origins(oracle, kat):
+    """The rectangle origin sampler keeps the habitable cells in row-major
+    order, here over a sample that wraps across the plane's edge."""
+    for case in kat["wrapping_noise_origins"]:
+        o = oracle.enumerate_origins(wn_desc(oracle, case))
+        assert [[int(a), int(b)] for a, b in zip(o["x"], o["y"])] == case["origins"]
+        assert list(o["gref"]) == [(y << 32) | x for x, y in case["origins"]]
+        assert not o["index"].any()
+
+
+def test_wrapping_noise_reference_runs(oracle, kat):
+    """Full tiny WrappingNoise runs: approximate Normal dispersal with its
+    rejection loop (the generator asserts that targets were rejected)."""
+    for case in kat["wrapping_noise_runs"]:
+        assert case["rejections"] > 0
+        check_run(oracle, wn_desc(oracle, case), case)
