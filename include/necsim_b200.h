@@ -5,7 +5,7 @@
  * The backend is a drop-in for the reference's `algorithm: CUDA(...)` /
  * `Independent(...)` path: it takes a scenario (NonSpatial,
  * SpatiallyImplicit, AlmostInfinite with Normal or Clark2Dt dispersal,
- * SpatiallyExplicit with uniform turnover or a turnover map), a seeded
+ * SpatiallyExplicit with uniform turnover or a turnover map, WrappingNoise), a seeded
  * WyHash RNG and the
  * algorithm arguments, simulates every lineage on the GPU and hands the
  * events to reporters in the reference's reporting order.
@@ -41,6 +41,9 @@ extern "C" {
 #define NECSIM_E_UNSUPPORTED (-8)        /* valid in the reference, not here    */
 #define NECSIM_E_CALLBACK (-9)           /* a reporter callback asked to stop   */
 #define NECSIM_E_TOO_LARGE (-10)         /* exceeds a documented size limit     */
+#define NECSIM_E_DISPERSAL_REJECTED (-11) /* a WrappingNoise dispersal rejected
+                                            2^20 targets in a row (the reference
+                                            keeps drawing)                      */
 
 /* ---- scenarios ---- */
 enum necsim_scenario_kind {
@@ -49,6 +52,7 @@ enum necsim_scenario_kind {
     NECSIM_ALMOST_INFINITE_NORMAL = 2, /* rustcoalescence/scenarios/src/almost_infinite/normal.rs    */
     NECSIM_SPATIALLY_EXPLICIT = 3,     /* rustcoalescence/scenarios/src/spatially_explicit/turnover/{uniform,map}.rs */
     NECSIM_ALMOST_INFINITE_CLARK2DT = 4, /* rustcoalescence/scenarios/src/almost_infinite/clark2dt.rs */
+    NECSIM_WRAPPING_NOISE = 5,         /* rustcoalescence/scenarios/src/wrapping_noise.rs            */
 };
 
 /* Replaces the reference's `ScenarioCogs` as produced by `Scenario::new`
@@ -72,6 +76,17 @@ typedef struct necsim_scenario {
     const double *turnover_map;      /* SpatiallyExplicit: width*height f64 turnover rates, row-major
                                         (spatially_explicit/turnover/map.rs, InMemoryTurnoverRate); NULL:
                                         uniform `turnover_rate`.  Rates >= 0, > 0 on habitable cells */
+    /* WrappingNoise (WrappingNoiseArguments, wrapping_noise.rs:36-48): habitable where the
+       OpenSimplex octave noise is at most its coverage quantile; `sigma` is the approximate
+       Normal dispersal; origins are the habitable cells of the Rectangle sample.
+       AlmostInfinite: sample_width > 0 selects the Rectangle sample (sample_x, sample_y,
+       sample_width, sample_height) instead of the Circle (almost_infinite/mod.rs:92-122) */
+    int64_t noise_seed;
+    double coverage;                 /* [0, 1] */
+    double scale, persistence;       /* (0, 1] */
+    uint64_t octaves;                /* >= 1 */
+    uint32_t sample_x, sample_y;     /* Rectangle sample: LandscapeExtent origin */
+    uint64_t sample_width, sample_height; /* 1 ..= 2^32 (OffByOneU32) */
 } necsim_scenario;
 
 /* necsim_args.event_time_sampler: which EventTimeSampler
@@ -313,7 +328,7 @@ int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cel
 
 /* The scenario's origin lineages in the reference's origin-sampler order
  * (OriginPreSampler::all() through origin_sampler/{non_spatial,in_memory,
- * spatially_implicit,singleton_demes/circle}.rs, Lineage::new gives the
+ * spatially_implicit,singleton_demes/{circle,rectangle}}.rs, Lineage::new gives the
  * global reference = the location's u64 injection).  *n_out receives the
  * count; at most `cap` are written (out may be NULL to size). */
 int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *out, uint64_t cap,

@@ -25,11 +25,13 @@ SPATIALLY_IMPLICIT = 1
 ALMOST_INFINITE_NORMAL = 2
 ALMOST_INFINITE_CLARK2DT = 4
 SPATIALLY_EXPLICIT = 3
+WRAPPING_NOISE = 5
 
 ERRORS = {
     -1: "invalid argument", -2: "CUDA error", -3: "out of memory", -4: "device bound check",
     -5: "device wait timeout", -6: "dispersal map contract violated", -7: "empty habitat map",
     -8: "unsupported", -9: "reporter stopped delivery", -10: "too large",
+    -11: "dispersal target rejected too often",
 }
 
 
@@ -56,6 +58,11 @@ class CScenario(ctypes.Structure):
         ("dispersal", ctypes.POINTER(ctypes.c_double)),
         ("shape_u", ctypes.c_double), ("tail_p", ctypes.c_double),
         ("turnover_map", ctypes.POINTER(ctypes.c_double)),
+        ("noise_seed", ctypes.c_int64), ("coverage", ctypes.c_double),
+        ("scale", ctypes.c_double), ("persistence", ctypes.c_double),
+        ("octaves", ctypes.c_uint64),
+        ("sample_x", ctypes.c_uint32), ("sample_y", ctypes.c_uint32),
+        ("sample_width", ctypes.c_uint64), ("sample_height", ctypes.c_uint64),
     ]
 
 
@@ -269,8 +276,9 @@ class Clark2Dt:
 
 @dataclass
 class AlmostInfinite:
-    """`AlmostInfinite(sample: Circle(..), dispersal: Normal(..) | Clark2Dt(..))`."""
-    sample: Circle
+    """`AlmostInfinite(sample: Circle(..) | Rectangle(..), dispersal: Normal(..) | Clark2Dt(..))`
+    (almost_infinite/mod.rs:92-122)."""
+    sample: object
     dispersal: object
 
 
@@ -283,6 +291,31 @@ class SpatiallyExplicit:
     habitat: np.ndarray
     dispersal: np.ndarray
     turnover: Union[float, np.ndarray] = 0.5
+
+
+@dataclass
+class Rectangle:
+    """`Rectangle(origin: (x, y), width: w, height: h)` sample
+    (LandscapeExtent, necsim/core/src/landscape/extent.rs; wrapping_noise.rs:51-55)."""
+    origin: Tuple[int, int]
+    width: int
+    height: int
+
+
+@dataclass
+class WrappingNoise:
+    """`WrappingNoise(seed, coverage, scale, persistence, octaves, sample, sigma)`
+    (rustcoalescence/scenarios/src/wrapping_noise.rs): the almost-infinite
+    plane, habitable where OpenSimplex octave noise is at most its coverage
+    quantile, approximate Normal dispersal of width sigma, origins the
+    habitable locations of the Rectangle sample."""
+    seed: int
+    coverage: float
+    scale: float
+    persistence: float
+    octaves: int
+    sample: Rectangle
+    sigma: float
 
 
 MAP_LOADING_MODES = {"OffByOne": 0, "FixMe": 1, "Strict": 2}
@@ -455,8 +488,22 @@ def _scenario_struct(scenario, speciation: float):
         else:
             c.kind = ALMOST_INFINITE_NORMAL
             c.sigma = scenario.dispersal.sigma
-        c.centre_x, c.centre_y = scenario.sample.centre
-        c.radius = scenario.sample.radius
+        if isinstance(scenario.sample, Rectangle):
+            c.sample_x, c.sample_y = scenario.sample.origin
+            c.sample_width, c.sample_height = scenario.sample.width, scenario.sample.height
+        else:
+            c.centre_x, c.centre_y = scenario.sample.centre
+            c.radius = scenario.sample.radius
+    elif isinstance(scenario, WrappingNoise):
+        c.kind = WRAPPING_NOISE
+        c.noise_seed = scenario.seed
+        c.coverage = scenario.coverage
+        c.scale = scenario.scale
+        c.persistence = scenario.persistence
+        c.octaves = scenario.octaves
+        c.sigma = scenario.sigma
+        c.sample_x, c.sample_y = scenario.sample.origin
+        c.sample_width, c.sample_height = scenario.sample.width, scenario.sample.height
     elif isinstance(scenario, SpatiallyExplicit):
         c.kind = SPATIALLY_EXPLICIT
         h = np.ascontiguousarray(scenario.habitat, dtype=np.uint32)

@@ -13,8 +13,8 @@
 // Supported: speciation; sample (percentage, origin Habitat | List,
 // mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
 // which writes the configuration that resumes the run; rng Seed | Entropy;
-// the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle; Normal or Clark2Dt) and
-// SpatiallyExplicit (habitat, dispersal and turnover maps as (Geo)TIFF files
+// the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle or Rectangle; Normal or
+// Clark2Dt), WrappingNoise and SpatiallyExplicit (habitat, dispersal and turnover maps as (Geo)TIFF files
 // or .npy arrays, Uniform(rate) or Map(path) turnover, loading mode FixMe |
 // OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
 // or CUDA(...) (exponential event times, the reference CUDA algorithm's
@@ -158,6 +158,22 @@ std::vector<T> load_map(const std::string &path, int32_t mode, std::vector<uint6
     return out;
 }
 
+// `Rectangle(origin: (x: .., y: ..), width: .., height: ..)` (or its
+// `Extent` alias, or the LandscapeExtent wrapped in parentheses): the sample
+// extent (necsim/core/src/landscape/extent.rs; width and height 1..=2^32)
+void parse_rectangle(const Value &sample, necsim_scenario &sc) {
+    const Value *e = &sample;
+    if (e->fields.empty() && e->items.size() == 1 && e->items[0].kind == Value::Struct) e = &e->items[0];
+    const Value &origin = need(*e, "origin");
+    sc.sample_x = as_u32(need(origin, "x"), "origin.x");
+    sc.sample_y = as_u32(need(origin, "y"), "origin.y");
+    sc.sample_width = need(*e, "width").as_u64();
+    sc.sample_height = need(*e, "height").as_u64();
+    if (sc.sample_width == 0 || sc.sample_height == 0 || sc.sample_width > (1ULL << 32) ||
+        sc.sample_height > (1ULL << 32))
+        fail("the sample's width and height must be in 1..=2^32");
+}
+
 void parse_scenario(const Value &s, Run &r) {
     const std::string &k = s.variant();
     necsim_scenario &sc = r.sc;
@@ -188,21 +204,30 @@ void parse_scenario(const Value &s, Run &r) {
     } else if (k == "AlmostInfinite") {
         const Value &sample = need(s, "sample");
         const Value &disp = need(s, "dispersal");
-        if (sample.variant() != "Circle") fail("AlmostInfinite: only the Circle sample is supported");
+        // almost_infinite/mod.rs:92-122: Circle or Rectangle (alias Extent)
+        const bool rectangle = sample.variant() == "Rectangle" || sample.variant() == "Extent";
+        if (sample.variant() != "Circle" && !rectangle)
+            fail("AlmostInfinite: the sample must be Circle or Rectangle");
         if (disp.variant() != "Normal" && disp.variant() != "Clark2Dt")
             fail("AlmostInfinite: dispersal must be Normal or Clark2Dt");
         sc.kind = disp.variant() == "Normal" ? NECSIM_ALMOST_INFINITE_NORMAL : NECSIM_ALMOST_INFINITE_CLARK2DT;
-        // almost_infinite/mod.rs:103-107: the default centre
-        sc.centre_x = sc.centre_y = 0x7fffffffu;
-        if (const Value *c = sample.field("centre")) {
-            sc.centre_x = as_u32(need(*c, "x"), "centre.x");
-            sc.centre_y = as_u32(need(*c, "y"), "centre.y");
+        if (rectangle) {
+            parse_rectangle(sample, sc);
+            o << "AlmostInfinite(Rectangle(origin: (" << sc.sample_x << ", " << sc.sample_y
+              << "), width: " << sc.sample_width << ", height: " << sc.sample_height << "), ";
+        } else {
+            // almost_infinite/mod.rs:103-107: the default centre
+            sc.centre_x = sc.centre_y = 0x7fffffffu;
+            if (const Value *c = sample.field("centre")) {
+                sc.centre_x = as_u32(need(*c, "x"), "centre.x");
+                sc.centre_y = as_u32(need(*c, "y"), "centre.y");
+            }
+            const uint64_t radius = need(sample, "radius").as_u64();
+            if (radius > 0xffff) fail("AlmostInfinite: the radius is a u16");
+            sc.radius = (uint32_t)radius;
+            o << "AlmostInfinite(Circle(centre: (" << sc.centre_x << ", " << sc.centre_y << "), radius: " << radius
+              << "), ";
         }
-        const uint64_t radius = need(sample, "radius").as_u64();
-        if (radius > 0xffff) fail("AlmostInfinite: the radius is a u16");
-        sc.radius = (uint32_t)radius;
-        o << "AlmostInfinite(Circle(centre: (" << sc.centre_x << ", " << sc.centre_y << "), radius: " << radius
-          << "), ";
         if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL) {
             sc.sigma = need(disp, "sigma").as_f64();
             o << "Normal(sigma: " << sc.sigma << "))";
@@ -211,6 +236,23 @@ void parse_scenario(const Value &s, Run &r) {
             sc.tail_p = need(disp, "tail_p").as_f64();
             o << "Clark2Dt(shape_u: " << sc.shape_u << ", tail_p: " << sc.tail_p << "))";
         }
+    } else if (k == "WrappingNoise") {
+        // WrappingNoiseArguments (rustcoalescence/scenarios/src/wrapping_noise.rs:36-56)
+        sc.kind = NECSIM_WRAPPING_NOISE;
+        sc.noise_seed = need(s, "seed").as_i64();
+        sc.coverage = need(s, "coverage").as_f64();
+        sc.scale = need(s, "scale").as_f64();
+        sc.persistence = need(s, "persistence").as_f64();
+        sc.octaves = need(s, "octaves").as_u64();
+        const Value &sample = need(s, "sample");
+        if (sample.variant() != "Rectangle" && sample.variant() != "Extent")
+            fail("WrappingNoise: the sample must be a Rectangle");
+        parse_rectangle(sample, sc);
+        sc.sigma = need(s, "sigma").as_f64();
+        o << "WrappingNoise(seed: " << sc.noise_seed << ", coverage: " << sc.coverage << ", scale: " << sc.scale
+          << ", persistence: " << sc.persistence << ", octaves: " << sc.octaves << ", Rectangle(origin: ("
+          << sc.sample_x << ", " << sc.sample_y << "), width: " << sc.sample_width << ", height: " << sc.sample_height
+          << "), sigma: " << sc.sigma << ")";
     } else if (k == "SpatiallyExplicit") {
         // spatially_explicit/turnover/mod.rs:13-30 (field names and aliases),
         // uniform.rs:131-175 (try_load: the dispersal map first, then the

@@ -8,9 +8,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <random>
+#include <tuple>
 #include <unordered_map>
 #include <string>
 #include <thread>
@@ -20,6 +23,7 @@
 #include "kernels.h"
 #include "layout.h"
 #include "tables.h"
+#include "wrapping_noise.h"
 
 using namespace necsim;
 
@@ -89,6 +93,142 @@ uint64_t seed_from_u64(uint64_t state) {
     return seed;
 }
 
+// ---- WrappingNoise habitat (habitat/wrapping_noise/mod.rs) ----
+
+// WyHash::sample_u64 (wyhash.rs:53-63) on the host, for the threshold sample
+struct HostWyHash {
+    uint64_t state;
+    static uint64_t diffuse(uint64_t x) {  // wyhash.rs:99-119
+        x *= 0x6eed0e9da4d94a4fULL;
+        x ^= (x >> 32) >> (x >> 60);
+        return x * 0x6eed0e9da4d94a4fULL;
+    }
+    uint64_t next() {
+        state += 0xa0761d6478bd642fULL;
+        const uint64_t a = state ^ 0xe7037ed1a0b428dbULL, b = state;
+        const unsigned __int128 r = (unsigned __int128)a * b;  // wyhash.rs:85-96
+        return diffuse((a ^ (uint64_t)r) ^ (b ^ (uint64_t)(r >> 64)));
+    }
+};
+
+// generate_perm_array (opensimplex_noise/mod.rs:76-96): a shuffle of 0..2048
+// whose i128 seed is never advanced, so each swap index is the same value
+// modulo (i + 1), made non-negative; kept as the low bytes of perm[0..256)
+void opensimplex_perm_low_bytes(int64_t seed, uint8_t out[256]) {
+    std::vector<int64_t> source(2048), perm(2048);
+    for (int64_t i = 0; i < 2048; ++i) source[i] = i;
+    const __int128 a = (__int128)seed * 6364136223846793005LL + 1442695040888963407LL + 31;
+    for (int64_t i = 2047; i >= 0; --i) {
+        int64_t r = (int64_t)(a % (__int128)(i + 1));  // truncating, like Rust's %
+        if (r < 0) r += i + 1;
+        perm[i] = source[r];
+        source[r] = source[i];
+    }
+    for (int i = 0; i < 256; ++i) out[i] = (uint8_t)(perm[i] & 0xff);
+}
+
+// Evaluates f(c) for c in [0, n) on all host threads (chunks in order).
+template <typename F>
+void parallel_for(uint64_t n, F &&f) {
+    const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+    if (n < 4096 || threads == 1) {
+        for (uint64_t c = 0; c < n; ++c) f(c);
+        return;
+    }
+    std::vector<std::thread> pool;
+    const uint64_t per = (n + threads - 1) / threads;
+    for (unsigned t = 0; t < threads; ++t) {
+        const uint64_t c0 = t * per, c1 = std::min(n, c0 + per);
+        if (c0 >= c1) break;
+        pool.emplace_back([&f, c0, c1] {
+            for (uint64_t c = c0; c < c1; ++c) f(c);
+        });
+    }
+    for (auto &th : pool) th.join();
+}
+
+// WrappingNoiseHabitat::new (habitat/wrapping_noise/mod.rs:47-99): the noise
+// at 2^16 locations drawn by WyHash::from_seed(seed.to_le_bytes()) (seed and
+// state the i64's bits), sorted by f64::total_cmp, read at
+// min(floor(2^16 * coverage), 2^16 - 1); and the approximate Normal
+// dispersal's self-dispersal probability (dispersal_sampler/wrapping_noise.rs:
+// 89-110, almost_infinite_normal.rs:22-37 with the C library's erf):
+// ps / (ps + (1 - ps) * coverage), ps = erf(0.5 / (sigma * sqrt 2))^2.
+NoiseHabitat make_noise_habitat(const necsim_scenario &sc) {
+    NoiseHabitat h;
+    std::memset(&h, 0, sizeof(h));
+    opensimplex_perm_low_bytes(sc.noise_seed, h.perm);
+    h.scale = sc.scale;
+    h.persistence = sc.persistence;
+    h.coverage = sc.coverage;
+    h.octaves = sc.octaves;
+    if (sc.coverage > 0.0 && sc.coverage < 1.0) {  // otherwise the threshold is never read
+        constexpr uint64_t kSamples = 1u << 16;
+        std::vector<uint64_t> locs(kSamples);
+        HostWyHash g{(uint64_t)sc.noise_seed};
+        for (auto &l : locs) l = g.next();
+        std::vector<double> v(kSamples);
+        parallel_for(kSamples, [&](uint64_t c) { v[c] = noise::octave_sum(h, (uint32_t)locs[c], (uint32_t)(locs[c] >> 32)); });
+        auto key = [](double d) {
+            int64_t b;
+            std::memcpy(&b, &d, 8);
+            return b ^ (int64_t)((uint64_t)(b >> 63) >> 1);
+        };
+        std::sort(v.begin(), v.end(), [&](double a, double b) { return key(a) < key(b); });
+        const double k = std::floor((double)kSamples * sc.coverage);
+        h.threshold = v[k >= (double)(kSamples - 1) ? kSamples - 1 : (uint64_t)k];
+    }
+    const double p1 = sc.sigma > 0.0 ? std::erf(0.5 / (sc.sigma * 1.41421356237309504880168872420969808)) : 1.0;
+    const double ps = p1 * p1;
+    const double p_self = ps / (ps + (1.0 - ps) * sc.coverage);
+    // u < p  <=>  X < ceil(p * 2^53); NaN (0 / 0) never self-disperses
+    h.self_threshold = p_self > 0.0 ? (uint64_t)std::ceil(std::ldexp(std::min(p_self, 1.0), 53)) : 0;
+    return h;
+}
+
+// The noise habitat of a scenario, built once per parameter set (building
+// evaluates the noise 2^16 times).
+const NoiseHabitat &noise_habitat(const necsim_scenario &sc) {
+    static std::mutex mu;
+    static std::map<std::tuple<int64_t, double, double, double, uint64_t, double>, std::unique_ptr<NoiseHabitat>> cache;
+    const auto key = std::make_tuple(sc.noise_seed, sc.coverage, sc.scale, sc.persistence, sc.octaves, sc.sigma);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it == cache.end()) it = cache.emplace(key, std::make_unique<NoiseHabitat>(make_noise_habitat(sc))).first;
+    return *it->second;
+}
+
+// Calls visit(x, y) for every habitable location of the WrappingNoise
+// Rectangle sample in its row-major order (singleton_demes/rectangle.rs:
+// 93-120 over landscape/extent.rs:80-100, coordinates wrapping at 2^32);
+// the habitat of each block of locations is evaluated on all host threads.
+template <typename F>
+void for_each_noise_origin(const necsim_scenario &sc, F &&visit) {
+    const NoiseHabitat &h = noise_habitat(sc);
+    const uint64_t w = sc.sample_width, n = sc.sample_width * sc.sample_height;
+    constexpr uint64_t kBlock = 1u << 20;
+    std::vector<uint8_t> mask;
+    for (uint64_t c0 = 0; c0 < n; c0 += kBlock) {
+        const uint64_t m = std::min(kBlock, n - c0);
+        mask.assign(m, 0);
+        auto at = [&](uint64_t c, uint32_t &x, uint32_t &y) {
+            x = sc.sample_x + (uint32_t)(c % w);
+            y = sc.sample_y + (uint32_t)(c / w);
+        };
+        parallel_for(m, [&](uint64_t j) {
+            uint32_t x, y;
+            at(c0 + j, x, y);
+            mask[j] = (uint8_t)noise::habitat_at(h, x, y);
+        });
+        for (uint64_t j = 0; j < m; ++j)
+            if (mask[j]) {
+                uint32_t x, y;
+                at(c0 + j, x, y);
+                visit(x, y);
+            }
+    }
+}
+
 // One simulation's host-side description.
 struct SimHost {
     necsim_scenario sc;
@@ -99,6 +239,17 @@ struct SimHost {
     double start_max;         // max last event time of its lineages
     SimParams params;
 };
+
+// The Rectangle sample extent (LandscapeExtent: width and height 1..=2^32);
+// optional for AlmostInfinite (sample_width 0: the Circle sample)
+void validate_rectangle(const necsim_scenario &sc, bool required) {
+    if (!required && sc.sample_width == 0) return;
+    if (sc.sample_width == 0 || sc.sample_height == 0 || sc.sample_width > (1ULL << 32) ||
+        sc.sample_height > (1ULL << 32))
+        fail(NECSIM_E_INVALID_ARGUMENT, "the sample extent's width and height must be in 1..=2^32");
+    if (sc.sample_width * sc.sample_height > (1ULL << 40))
+        fail(NECSIM_E_TOO_LARGE, "the sample extent exceeds 2^40 locations");
+}
 
 void validate(const necsim_scenario &sc) {
     if (!(sc.speciation_probability > 0.0) || !(sc.speciation_probability <= 1.0))
@@ -122,11 +273,23 @@ void validate(const necsim_scenario &sc) {
     case NECSIM_ALMOST_INFINITE_NORMAL:
         if (!(sc.sigma >= 0.0) || !std::isfinite(sc.sigma)) fail(NECSIM_E_INVALID_ARGUMENT, "sigma must be >= 0");
         if (sc.radius > 65535) fail(NECSIM_E_INVALID_ARGUMENT, "circle radius is a u16");
+        validate_rectangle(sc, false);
         break;
     case NECSIM_ALMOST_INFINITE_CLARK2DT:
         if (!(sc.shape_u > 0.0) || !std::isfinite(sc.shape_u) || !(sc.tail_p > 0.0) || !std::isfinite(sc.tail_p))
             fail(NECSIM_E_INVALID_ARGUMENT, "Clark2Dt shape_u and tail_p must be positive");
         if (sc.radius > 65535) fail(NECSIM_E_INVALID_ARGUMENT, "circle radius is a u16");
+        validate_rectangle(sc, false);
+        break;
+    case NECSIM_WRAPPING_NOISE:
+        // WrappingNoiseArguments (wrapping_noise.rs:36-48) and their bond types
+        if (!(sc.coverage >= 0.0) || !(sc.coverage <= 1.0))
+            fail(NECSIM_E_INVALID_ARGUMENT, "WrappingNoise coverage must be in [0, 1]");
+        if (!(sc.scale > 0.0) || !(sc.scale <= 1.0) || !(sc.persistence > 0.0) || !(sc.persistence <= 1.0))
+            fail(NECSIM_E_INVALID_ARGUMENT, "WrappingNoise scale and persistence must be in (0, 1]");
+        if (sc.octaves == 0) fail(NECSIM_E_INVALID_ARGUMENT, "WrappingNoise octaves must be >= 1");
+        if (!(sc.sigma >= 0.0) || !std::isfinite(sc.sigma)) fail(NECSIM_E_INVALID_ARGUMENT, "sigma must be >= 0");
+        validate_rectangle(sc, true);
         break;
     case NECSIM_SPATIALLY_EXPLICIT:
         if (!sc.width || !sc.height || !sc.habitat || !sc.dispersal)
@@ -157,11 +320,17 @@ uint64_t count_origins(const necsim_scenario &sc) {
         return (uint64_t)sc.width * sc.height * sc.deme;
     case NECSIM_ALMOST_INFINITE_NORMAL:
     case NECSIM_ALMOST_INFINITE_CLARK2DT: {
+        if (sc.sample_width) return sc.sample_width * sc.sample_height;  // Rectangle: every location
         const int64_t r = sc.radius;
         uint64_t n = 0;
         for (int64_t dy = -r; dy <= r; ++dy)
             for (int64_t dx = -r; dx <= r; ++dx)
                 if ((uint64_t)(dx * dx + dy * dy) <= (uint64_t)(r * r)) ++n;
+        return n;
+    }
+    case NECSIM_WRAPPING_NOISE: {
+        uint64_t n = 0;
+        for_each_noise_origin(sc, [&](uint32_t, uint32_t) { ++n; });
         return n;
     }
     default: {
@@ -257,6 +426,7 @@ SimParams base_params(const necsim_scenario &sc, const necsim_args &args, uint64
         p.clark_shape_u = sc.shape_u;
         p.clark_exponent = 1.0 / sc.tail_p;
     }
+    if (sc.kind == NECSIM_WRAPPING_NOISE) p.noise = noise_habitat(sc);
     p.pause_before = -1.0;
     return p;
 }
@@ -571,6 +741,15 @@ void for_each_origin(const necsim_scenario &sc, F &&push) {
         for (uint32_t yy = 0; yy < sc.height; ++yy)
             for (uint32_t xx = 0; xx < sc.width; ++xx)
                 for (uint32_t ii = 0; ii < sc.deme; ++ii) push(xx, yy, ii, g++);
+    } else if ((sc.kind == NECSIM_ALMOST_INFINITE_NORMAL || sc.kind == NECSIM_ALMOST_INFINITE_CLARK2DT) &&
+               sc.sample_width) {
+        // origin_sampler/singleton_demes/rectangle.rs:93-120: every location of
+        // the extent is habitable, row-major, wrapping at 2^32
+        for (uint64_t yy = 0; yy < sc.sample_height; ++yy)
+            for (uint64_t xx = 0; xx < sc.sample_width; ++xx) {
+                const uint32_t px = sc.sample_x + (uint32_t)xx, py = sc.sample_y + (uint32_t)yy;
+                push(px, py, 0u, ((uint64_t)py << 32) | px);
+            }
     } else if (sc.kind == NECSIM_ALMOST_INFINITE_NORMAL || sc.kind == NECSIM_ALMOST_INFINITE_CLARK2DT) {
         // origin_sampler/singleton_demes/circle.rs:36-70, 100-140
         const uint32_t r = sc.radius;
@@ -584,6 +763,10 @@ void for_each_origin(const necsim_scenario &sc, F &&push) {
                 const uint64_t dy = std::min<uint32_t>(py - sc.centre_y, sc.centre_y - py);
                 if (dx * dx + dy * dy <= r2) push(px, py, 0u, ((uint64_t)py << 32) | px);
             }
+    } else if (sc.kind == NECSIM_WRAPPING_NOISE) {
+        // Lineage::new: the global reference is the AlmostInfinite injection
+        // (habitat/wrapping_noise/mod.rs:170-175)
+        for_each_noise_origin(sc, [&](uint32_t x, uint32_t y) { push(x, y, 0u, ((uint64_t)y << 32) | x); });
     } else {
         // origin_sampler/in_memory.rs:89-119; global reference = prefix(cell) + index
         uint64_t g = 0;
@@ -1096,6 +1279,9 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
     CK(cudaMemcpy(cs.data(), E.d_counters, ns * sizeof(SimCounters), cudaMemcpyDeviceToHost));
     Control c;
     CK(cudaMemcpy(&c, E.d_ctl, sizeof(c), cudaMemcpyDeviceToHost));
+    if (c.status & kErrDispersalRejections)
+        fail(NECSIM_E_DISPERSAL_REJECTED, "a WrappingNoise dispersal rejected " + std::to_string(kMaxDispersalRejections) +
+                                              " targets in a row");
     if (c.status & (kErrCellIndex | kErrAtomIndex | kErrEventOverflow | kErrDispersalOverflow | kErrResident))
         fail(NECSIM_E_DEVICE_CHECK, "device bound check failed (status " + std::to_string(c.status) + ")");
     // surviving lineages live in A after an even number of rounds
@@ -1494,6 +1680,9 @@ static int simulate_impl(necsim_ctx *ctx, const necsim_lineage *lineages, uint64
                 case NECSIM_ALMOST_INFINITE_NORMAL:
                 case NECSIM_ALMOST_INFINITE_CLARK2DT:
                     h = 1;
+                    break;
+                case NECSIM_WRAPPING_NOISE:
+                    h = noise::habitat_at(noise_habitat(sc), l.x, l.y);
                     break;
                 default:
                     h = (l.x < sc.width && l.y < sc.height) ? ctx->habitat[(uint64_t)l.y * sc.width + l.x] : 0;

@@ -18,6 +18,7 @@
 
 #include "device_core.cuh"
 #include "kernels.h"
+#include "wrapping_noise.h"
 
 namespace necsim {
 
@@ -59,7 +60,8 @@ __device__ __forceinline__ uint64_t lane_injection(const Lane &l, const SimParam
         if (in_local(p, l.x, l.y)) return non_spatial_injection(0, 0, p.width, p.deme, l.x, l.y, l.i);
         return non_spatial_injection(p.meta_ox, p.meta_oy, p.meta_width, p.meta_deme, l.x, l.y, l.i);
     }
-    if (KIND == kAlmostInfiniteNormal) return ((uint64_t)l.y << 32) | (uint64_t)l.x;  // almost_infinite.rs:66-70
+    // almost_infinite.rs:66-70 (WrappingNoise defers to it, habitat/wrapping_noise/mod.rs:170-175)
+    if (KIND == kAlmostInfiniteNormal || KIND == kWrappingNoise) return ((uint64_t)l.y << 32) | (uint64_t)l.x;
     return l.rec.injection + (uint64_t)l.i;                                          // in_memory.rs:70-80
 }
 
@@ -224,6 +226,27 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
             clark2dt_dispersal_draw(e2, e3, p.clark_shape_u, p.clark_exponent, l.x, l.y, tx, ty);
         else
             normal_dispersal_draw(e2, e3, p.sigma, l.x, l.y, tx, ty);
+        ti = 0;
+    } else if (KIND == kWrappingNoise) {
+        // dispersal_sampler/wrapping_noise.rs:42-87: self-dispersal iff
+        // sample 2 is below p_self; otherwise Normal targets from samples
+        // (3 + 2c, 4 + 2c) until one is habitable and not the origin.  The
+        // coalescence sample then reads habitat 1 at the target: index 0.
+        tx = l.x;
+        ty = l.y;
+        if ((e2 >> 11) >= p.noise.self_threshold) {
+            uint64_t d0 = e3, d1 = EAGER ? e4 : draw_at(rs, 4);
+            for (uint32_t c = 0;; ++c) {
+                normal_dispersal_draw(d0, d1, p.sigma, l.x, l.y, tx, ty);
+                if ((tx != l.x || ty != l.y) && noise::habitat_at(p.noise, tx, ty) != 0) break;
+                if (c + 1 == kMaxDispersalRejections) {
+                    set_status(k.status, kErrDispersalRejections);
+                    return kStepDropped;
+                }
+                d0 = draw_at(rs, 5 + 2 * (uint64_t)c);
+                d1 = draw_at(rs, 6 + 2 * (uint64_t)c);
+            }
+        }
         ti = 0;
     } else {
         uint64_t d_coal;
@@ -1213,6 +1236,7 @@ cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned blo
     case kSpatiallyImplicit: return launch_step_t<kSpatiallyImplicit>(a, grid, block, st);
     case kAlmostInfiniteNormal: return launch_step_t<kAlmostInfiniteNormal>(a, grid, block, st);
     case kSpatiallyExplicit: return launch_step_t<kSpatiallyExplicit>(a, grid, block, st);
+    case kWrappingNoise: return launch_step_t<kWrappingNoise>(a, grid, block, st);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1230,6 +1254,7 @@ cudaError_t step_kernel_occupancy(int kind, bool exp_sampler, int block, int *bl
     case kSpatiallyImplicit: return step_occupancy_t<kSpatiallyImplicit>(exp_sampler, block, blocks_per_sm);
     case kAlmostInfiniteNormal: return step_occupancy_t<kAlmostInfiniteNormal>(exp_sampler, block, blocks_per_sm);
     case kSpatiallyExplicit: return step_occupancy_t<kSpatiallyExplicit>(exp_sampler, block, blocks_per_sm);
+    case kWrappingNoise: return step_occupancy_t<kWrappingNoise>(exp_sampler, block, blocks_per_sm);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1297,6 +1322,7 @@ cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cuda
     case kSpatiallyImplicit: launch_resident_t<kSpatiallyImplicit>(a, grid, st); break;
     case kAlmostInfiniteNormal: launch_resident_t<kAlmostInfiniteNormal>(a, grid, st); break;
     case kSpatiallyExplicit: launch_resident_t<kSpatiallyExplicit>(a, grid, st); break;
+    case kWrappingNoise: launch_resident_t<kWrappingNoise>(a, grid, st); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

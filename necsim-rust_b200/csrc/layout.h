@@ -20,7 +20,27 @@ enum Kind : int32_t {
     kSpatiallyImplicit = 1,
     kAlmostInfiniteNormal = 2,
     kSpatiallyExplicit = 3,
+    kWrappingNoise = 5,
 };
+
+// A WrappingNoise dispersal that rejects this many Normal targets in a row
+// fails (kErrDispersalRejections) where the reference keeps drawing: it
+// bounds the time one event can take on the device.
+constexpr uint32_t kMaxDispersalRejections = 1u << 20;
+
+// The WrappingNoise habitat (habitat/wrapping_noise/mod.rs) and its
+// approximate Normal dispersal (dispersal_sampler/wrapping_noise.rs).
+struct alignas(16) NoiseHabitat {
+    // low bytes of the OpenSimplex permutation's first 256 entries
+    // (opensimplex_noise/mod.rs:76-96): the lattice hash reads no others
+    uint8_t perm[256];
+    double threshold;         // habitable iff the octave noise <= threshold
+    double scale, persistence;
+    double coverage;          // <= 0: nothing habitable; >= 1: everything
+    uint64_t octaves;
+    uint64_t self_threshold;  // ceil(p_self * 2^53): self-dispersal iff X < this
+};
+static_assert(sizeof(NoiseHabitat) % 16 == 0, "NoiseHabitat must be whole 16-byte words");
 
 // One habitat cell of a SpatiallyExplicit map, 32 bytes (one DRAM sector).
 // Restates InMemoryHabitat's u64 injection prefix (habitat/in_memory.rs:143-163),
@@ -106,6 +126,7 @@ struct alignas(16) SimParams {
     double clark_exponent;
     uint32_t clark;
     uint32_t pad3[3];
+    NoiseHabitat noise;       // WrappingNoise
     uint64_t n_cells;
     uint64_t n_atoms;
     uint64_t step_slice;
@@ -175,6 +196,7 @@ enum : uint32_t {
     kErrDedupFull = 1u << 3,     // dedup probe sequence exhausted
     kErrDispersalOverflow = 1u << 4,
     kErrResident = 1u << 5,      // a resident simulation exceeded the block's capacity
+    kErrDispersalRejections = 1u << 6,  // a WrappingNoise dispersal hit kMaxDispersalRejections
 };
 
 }  // namespace necsim

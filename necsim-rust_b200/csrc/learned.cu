@@ -58,6 +58,10 @@ __device__ void lineage_features(int kind, const SimParams &p, const SimCounters
         // Clark2Dt kernel of scale sqrt(u) (sigma 0: none)
         const float scale2 = p.clark ? (float)p.clark_shape_u : (float)p.sigma * (float)p.sigma;
         ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2, 1.0f));
+    } else if (kind == kWrappingNoise) {
+        // the Normal kernel's entropy, restricted to the habitable share
+        const float scale2 = (float)p.sigma * (float)p.sigma;
+        ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2 * (float)p.noise.coverage, 1.0f));
     } else {
         fx = (float)x / (float)p.width;
         fy = (float)y / (float)p.height;

@@ -1,6 +1,8 @@
 // ron.cpp -- see ron.h.
 #include "ron.h"
 
+#include <cerrno>
+
 #include <cctype>
 #include <cstdlib>
 #include <sstream>
@@ -169,6 +171,15 @@ uint64_t Value::as_u64() const {
     const unsigned long long u = std::strtoull(text.c_str(), &end, 10);
     if (!end || *end || text.empty() || text[0] == '-') throw ParseError{"malformed integer " + text, 0};
     return u;
+}
+
+int64_t Value::as_i64() const {
+    if (kind != Number) throw ParseError{"expected an integer, found " + text, 0};
+    char *end = nullptr;
+    errno = 0;
+    const long long v = std::strtoll(text.c_str(), &end, 10);
+    if (!end || *end || text.empty() || errno == ERANGE) throw ParseError{"malformed i64 " + text, 0};
+    return v;
 }
 
 const Value *Value::field(const std::string &name) const {

@@ -24,6 +24,7 @@ struct Value {
     bool is_number() const { return kind == Number; }
     double as_f64() const;
     uint64_t as_u64() const;
+    int64_t as_i64() const;
     // Struct field by name (nullptr when absent)
     const Value *field(const std::string &name) const;
     // `Name` or `Name(...)`: the variant name of an enum value

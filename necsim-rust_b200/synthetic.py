@@ -124,12 +124,19 @@ def to_scenario(desc):
         return nb.SpatiallyImplicit((desc["width"], desc["height"]), desc["deme"],
                                     (desc["meta_width"], desc["meta_height"]), desc["meta_deme"],
                                     desc["migration_probability"])
-    if k == 2:
-        return nb.AlmostInfinite(nb.Circle(desc["radius"], (desc["centre_x"], desc["centre_y"])),
-                                 nb.Normal(desc["sigma"]))
-    if k == 4:
-        return nb.AlmostInfinite(nb.Circle(desc["radius"], (desc["centre_x"], desc["centre_y"])),
-                                 nb.Clark2Dt(desc["shape_u"], desc["tail_p"]))
+    if k in (2, 4):
+        if "sample" in desc:  # the Rectangle sample (x, y, width, height)
+            x, y, w, h = desc["sample"]
+            sample = nb.Rectangle((x, y), w, h)
+        else:
+            sample = nb.Circle(desc["radius"], (desc["centre_x"], desc["centre_y"]))
+        if k == 2:
+            return nb.AlmostInfinite(sample, nb.Normal(desc["sigma"]))
+        return nb.AlmostInfinite(sample, nb.Clark2Dt(desc["shape_u"], desc["tail_p"]))
+    if k == 5:
+        x, y, w, h = desc["sample"]
+        return nb.WrappingNoise(desc["noise_seed"], desc["coverage"], desc["scale"], desc["persistence"],
+                                desc["octaves"], nb.Rectangle((x, y), w, h), desc["sigma"])
     turnover = desc.get("turnover_map")
     return nb.SpatiallyExplicit(desc["habitat"], desc["dispersal"],
                                 turnover if turnover is not None else desc.get("turnover_rate", 0.5))

@@ -1057,6 +1057,23 @@ static int64_t enumerate_origins(const oracle_scenario *sc, const sim_t *s, line
         break;
     case ORACLE_ALMOST_INFINITE_NORMAL:
     case ORACLE_ALMOST_INFINITE_CLARK2DT: {
+        if (sc->sample_width) {
+            /* almost_infinite/mod.rs:98, 118-120: the Rectangle sample,
+             * singleton_demes/rectangle.rs:93-120 (every location habitable) */
+            for (uint64_t yy = 0; yy < sc->sample_height; ++yy)
+                for (uint64_t xx = 0; xx < sc->sample_width; ++xx) {
+                    uint32_t x = sc->sample_x + (uint32_t)xx, y = sc->sample_y + (uint32_t)yy;
+                    if (out && n < cap) {
+                        out[n].x = x;
+                        out[n].y = y;
+                        out[n].i = 0;
+                        out[n].last = 0.0;
+                        out[n].gref = ((uint64_t)y << 32) | x;
+                    }
+                    n++;
+                }
+            break;
+        }
         /* singleton_demes/circle.rs:36-70, 100-140 */
         uint32_t r = sc->radius;
         uint64_t d = (uint64_t)r * 2 + 1;

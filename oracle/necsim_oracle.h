@@ -50,7 +50,8 @@ typedef struct oracle_scenario {
     double shape_u, tail_p;                   /* AlmostInfinite Clark2Dt dispersal */
     const double *turnover;                   /* SE turnover map, width*height row-major (NULL: uniform) */
     /* WrappingNoise (rustcoalescence/scenarios/src/wrapping_noise.rs); `sigma` is its
-     * Normal dispersal */
+     * Normal dispersal.  The sample fields also serve AlmostInfinite, where
+     * sample_width > 0 selects the Rectangle sample over the Circle */
     int64_t noise_seed;
     double coverage;                          /* [0, 1] */
     double scale, persistence;                /* (0, 1] */

@@ -296,10 +296,12 @@ class AlmostInfiniteLandscape:
     + clamp_round_dispersal); the singleton demes still draw the coalescence
     sample (index 0)."""
 
-    def __init__(self, cx, cy, r, sigma):
-        self.cx, self.cy, self.r, self.sigma = cx, cy, r, sigma
+    def __init__(self, cx, cy, r, sigma, rectangle=None):
+        self.cx, self.cy, self.r, self.sigma, self.rectangle = cx, cy, r, sigma, rectangle
 
     def origins(self):
+        if self.rectangle:  # almost_infinite/mod.rs:98: every location of the extent
+            return [[(y << 32) | x, 0.0, x, y, 0] for (x, y) in extent_iter(*self.rectangle)]
         return [[(y << 32) | x, 0.0, x, y, 0] for (x, y) in circle_origins(self.cx, self.cy, self.r)]
 
     def injection(self, x, y, i):
@@ -926,6 +928,11 @@ def main():
         r = reference_run(AlmostInfiniteLandscape(cx, cy, rad, sigma), nu, seed)
         r.update({"centre": [cx, cy], "radius": rad, "sigma": sigma, "speciation": nu, "seed": seed})
         kat["almost_infinite_runs"].append(r)
+    kat["almost_infinite_rectangle_runs"] = []
+    for (rect, sigma, nu, seed) in [((0xFFFFFFFF - 1, 7, 4, 3), 2.0, 0.05, 31), ((100, 0xFFFFFFFF, 3, 2), 0.0, 0.1, 32)]:
+        r = reference_run(AlmostInfiniteLandscape(0, 0, 0, sigma, rect), nu, seed)
+        r.update({"sample": list(rect), "sigma": sigma, "speciation": nu, "seed": seed})
+        kat["almost_infinite_rectangle_runs"].append(r)
     kat["clark2dt_runs"] = []
     for (cx, cy, rad, shape_u, tail_p, nu, seed) in [(2 ** 31, 2 ** 31, 2, 4.0, 0.5, 0.05, 21),
                                                      (0, 3, 2, 1.0, 1.0, 0.05, 22)]:

@@ -59,3 +59,28 @@ def test_invalid_arguments_fail_cleanly(nb):
         nb.Simulation(nb.NonSpatial((5, 5), 1), 0.0)
     with pytest.raises(nb.NecsimError):
         nb.Simulation(nb.SpatiallyImplicit((5, 1), 1, (10, 1), 1, 0.0), 0.1)
+
+
+def test_scenario_layout_matches_ctypes_mirrors(nb, oracle, tmp_path):
+    """necsim_scenario (include/necsim_b200.h) and oracle_scenario have the
+    field offsets of the package's and the oracle's ctypes structures."""
+    import ctypes
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    fields = [f[0] for f in nb.CScenario._fields_]
+    ofields = [f[0] for f in oracle.OracleScenario._fields_]
+    src = ['#include <stdio.h>', '#include <stddef.h>', '#include "include/necsim_b200.h"',
+           '#include "oracle/necsim_oracle.h"', 'int main(void) {',
+           '  printf("%zu %zu\\n", sizeof(necsim_scenario), sizeof(oracle_scenario));']
+    src += ['  printf("%%zu\\n", offsetof(necsim_scenario, %s));' % f for f in fields]
+    src += ['  printf("%%zu\\n", offsetof(oracle_scenario, %s));' % f for f in ofields]
+    src += ['  return 0;', '}']
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(src) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", root, "-o", str(exe), str(c)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    assert [int(v) for v in out[:2]] == [ctypes.sizeof(nb.CScenario), ctypes.sizeof(oracle.OracleScenario)]
+    got = [int(v) for v in out[2:]]
+    assert got[:len(fields)] == [getattr(nb.CScenario, f).offset for f in fields]
+    assert got[len(fields):] == [getattr(oracle.OracleScenario, f).offset for f in ofields]

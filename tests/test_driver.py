@@ -73,7 +73,13 @@ def test_check_parses_a_configuration(nb, tmp_path):
 @pytest.mark.parametrize("bad,msg", [
     ("speciation: 0.01,", "missing field `scenario`"),
     ("speciation: 0.01, scenario: NonSpatial(area: (3, 3), deme: 1), algorithm: Gillespie(),", "not the Independent"),
-    ("speciation: 0.01, scenario: WrappingNoise(seed: 1),", "not supported"),
+    ("speciation: 0.01, scenario: WrappingNoise(seed: 1),", "missing field `coverage`"),
+    ("speciation: 0.01, scenario: Torus(size: 1),", "not supported"),
+    ("speciation: 0.01, scenario: WrappingNoise(seed: 99999999999999999999, coverage: 0.5, scale: 0.1, "
+     "persistence: 0.5, octaves: 1, sample: Rectangle(origin: (x: 0, y: 0), width: 2, height: 2), sigma: 1.0),",
+     "malformed i64"),
+    ("speciation: 0.01, scenario: AlmostInfinite(sample: Rectangle(origin: (x: 0, y: 0), width: 0, height: 2), "
+     "dispersal: Normal(sigma: 1.0)),", "width and height must be in 1..=2^32"),
     ("speciation: 0.01 scenario: NonSpatial(area: (3, 3), deme: 1),", "expected ')'"),
     ("/* unterminated", "unterminated block comment"),
 ])
@@ -252,3 +258,30 @@ def test_driver_tiff_maps_match_the_package(nb, syn, oracle, tmp_path):
                 dispersal=sc.dispersal)
     ref = oracle.simulate(desc, 7, mode=oracle.MODE_REFERENCE)
     assert ref.biodiversity == o.biodiversity
+
+
+WN_SCENARIO = ("WrappingNoise(seed: -7, coverage: 0.25, scale: 1.0, persistence: 1.0, octaves: 3, "
+               "sample: Rectangle(origin: (x: 4294967276, y: 5), width: 40, height: 30), sigma: 1.0)")
+
+
+def test_check_wrapping_noise(nb, tmp_path, kat):
+    """WrappingNoise in the reference's RON spelling (docs/simulate.ron):
+    the lineages are the habitable cells of the Rectangle sample."""
+    case = kat["wrapping_noise_origins"][0]
+    assert (case["seed"], case["sample"]) == (-7, [4294967276, 5, 40, 30])
+    r = run_driver(nb, "check", CONFIG.replace("NonSpatial(area: (30, 20), deme: 2)", WN_SCENARIO), tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "WrappingNoise(seed: -7, coverage: 0.25" in r.stdout
+    assert int(re.search(r"(\d+) lineages", r.stdout).group(1)) == len(case["origins"])
+
+
+@pytest.mark.parametrize("sample", ["Rectangle(origin: (x: 4294967294, y: 7), width: 4, height: 3)",
+                                    "Rectangle((origin: (x: 1, y: 2), width: 3, height: 4))",
+                                    "Extent(origin: (x: 0, y: 0), width: 6, height: 2)"])
+def test_check_almost_infinite_rectangle_sample(nb, tmp_path, sample):
+    """AlmostInfinite's Rectangle sample (almost_infinite/mod.rs:92-122),
+    also as a wrapped LandscapeExtent and by its Extent alias."""
+    scen = "AlmostInfinite(sample: %s, dispersal: Normal(sigma: 2.0))" % sample
+    r = run_driver(nb, "check", CONFIG.replace("NonSpatial(area: (30, 20), deme: 2)", scen), tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "AlmostInfinite(Rectangle(origin:" in r.stdout and "12 lineages" in r.stdout

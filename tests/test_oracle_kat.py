@@ -329,3 +329,13 @@ def test_wrapping_noise_reference_runs(oracle, kat):
     for case in kat["wrapping_noise_runs"]:
         assert case["rejections"] > 0
         check_run(oracle, wn_desc(oracle, case), case)
+
+
+def test_almost_infinite_rectangle_reference_runs(oracle, kat):
+    """AlmostInfinite with the Rectangle sample (every location of the
+    extent, one wrapping across the plane's edge; sigma 0 keeps every
+    lineage in place)."""
+    for case in kat["almost_infinite_rectangle_runs"]:
+        desc = dict(kind=oracle.ALMOST_INFINITE_NORMAL, speciation_probability=case["speciation"],
+                    sigma=case["sigma"], sample=tuple(case["sample"]))
+        check_run(oracle, desc, case)
