@@ -76,6 +76,8 @@ GPU_CASES = {
     "wrapping_sample": (0.05, -2, 0.7, 0.2, 0.7, 3, (M32 - 5, M32 - 4, 12, 10), 1.5, 12),
     "near_self_dispersal": (0.05, 9, 0.6, 0.05, 0.5, 2, (0, 0, 16, 16), 0.2, 13),
     "full_coverage": (0.03, 1, 1.0, 0.07, 0.5, 3, (7, 7, 20, 20), 4.0, 14),
+    # ~38k lineages: the many-lineages-per-lane passes, then the sparse regimes
+    "throughput": (0.1, 5, 0.5, 0.05, 0.5, 3, (0, 0, 300, 250), 2.0, 15),
 }
 
 
@@ -86,6 +88,16 @@ def test_gpu_matches_oracle(nb, syn, oracle, name):
     desc = wn_desc(oracle, nu, ns, cov, scale, pers, octv, sample, sigma)
     g = check(nb, syn, oracle, desc, seed)
     assert g.steps > 0
+
+
+@pytest.mark.gpu
+def test_gpu_short_rounds_merge_duplicates_like_oracle(nb, syn, oracle):
+    """Rounds of at most 10 events per lineage: lineages that met on a cell
+    share their next event time there and merge (85 merges in the oracle)."""
+    nu, ns, cov, scale, pers, octv, sample, sigma, seed = GPU_CASES["sparse_habitat"]
+    desc = wn_desc(oracle, nu, ns, cov, scale, pers, octv, sample, sigma)
+    g = check(nb, syn, oracle, desc, seed, algo=nb.CUDA(step_slice_max=10))
+    assert g.n_dedup > 0 and g.n_rounds > 1
 
 
 @pytest.mark.gpu
