@@ -334,6 +334,17 @@ int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cel
 int necsim_enumerate_origins(const necsim_scenario *scenario, necsim_lineage *out, uint64_t cap,
                              uint64_t *n_out);
 
+/* IsolatedLandscape parallelism (rustcoalescence/algorithms/independent/src/launch.rs:101-110,
+ * algorithms/cuda/src/launch.rs:135-140): the subdomain rank of each lineage's location under the
+ * scenario's decomposition into `size` subdomains; origin_sampler/decomposition.rs keeps an origin iff
+ * its rank is the partition's.  The decompositions are the scenarios' `decompose`:
+ * ModuloDecomposition (NonSpatial, SpatiallyImplicit), RadialDecomposition (AlmostInfinite,
+ * WrappingNoise) and EqualDecomposition::weight (SpatiallyExplicit), decomposition/{modulo,radial,
+ * equal/{mod,weight}}.rs.  `exact` (may be NULL) receives 0 when the weight decomposition could not
+ * split the habitat into `size` parts (the reference warns and uses the ranks it found), else 1. */
+int necsim_subdomain_ranks(const necsim_scenario *scenario, uint32_t size, const necsim_lineage *lineages,
+                           uint64_t n, uint32_t *ranks, int32_t *exact);
+
 /* Origin pre-sampling: positions, in the order of necsim_enumerate_origins,
  * of the origins that OriginPreSampler::all().percentage(percentage)
  * .partition(rank, size) selects among the first n

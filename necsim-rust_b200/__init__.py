@@ -121,7 +121,7 @@ SYMBOLS = [
     "necsim_abi_version", "necsim_seed_from_u64", "necsim_gpu_create", "necsim_gpu_simulate",
     "necsim_gpu_simulate_lineages", "necsim_gpu_remaining_lineages",
     "necsim_gpu_simulate_batch", "necsim_gpu_last_error", "necsim_gpu_destroy",
-    "necsim_build_tables", "necsim_enumerate_origins", "necsim_gpu_batch_create",
+    "necsim_build_tables", "necsim_enumerate_origins", "necsim_subdomain_ranks", "necsim_gpu_batch_create",
     "necsim_gpu_batch_run", "necsim_gpu_batch_last_error", "necsim_gpu_batch_destroy",
     "necsim_model_create", "necsim_model_destroy", "necsim_model_last_error",
     "necsim_model_get_weights", "necsim_model_set_weights", "necsim_model_predict",
@@ -170,6 +170,8 @@ def lib():
     L.necsim_build_tables.restype = ctypes.c_int
     L.necsim_enumerate_origins.argtypes = [P(CScenario), vp, u64, P(u64)]
     L.necsim_enumerate_origins.restype = ctypes.c_int
+    L.necsim_subdomain_ranks.argtypes = [P(CScenario), ctypes.c_uint32, vp, u64, vp, P(ctypes.c_int32)]
+    L.necsim_subdomain_ranks.restype = ctypes.c_int
     L.necsim_gpu_batch_create.argtypes = [P(CScenario), P(u64), ctypes.c_uint32, P(CArgs),
                                           ctypes.c_double, P(vp)]
     L.necsim_gpu_batch_create.restype = ctypes.c_int
@@ -811,6 +813,22 @@ def enumerate_origins(scenario, speciation: float = 0.5) -> np.ndarray:
     if rc != 0:
         raise NecsimError(rc, "origin enumeration failed")
     return out[:n.value]
+
+
+def subdomain_ranks(scenario, size: int, lineages: np.ndarray, speciation: float = 0.5):
+    """IsolatedLandscape: each lineage's subdomain rank under the scenario's
+    decomposition into `size` parts (decomposition/{modulo,radial,equal}.rs);
+    returns (ranks, exact), exact False when SpatiallyExplicit's weight
+    decomposition found fewer parts."""
+    c = _scenario_struct(scenario, speciation)
+    lins = np.ascontiguousarray(lineages, dtype=LINEAGE_DTYPE)
+    ranks = np.zeros(max(len(lins), 1), dtype=np.uint32)
+    exact = ctypes.c_int32(1)
+    rc = lib().necsim_subdomain_ranks(ctypes.byref(c), size, lins.ctypes.data, len(lins), ranks.ctypes.data,
+                                      ctypes.byref(exact))
+    if rc != 0:
+        raise NecsimError(rc, "subdomain ranks failed")
+    return ranks[:len(lins)], bool(exact.value)
 
 
 def distinct_speciation_set(events: np.ndarray) -> np.ndarray:

@@ -18,7 +18,7 @@
 // or .npy arrays, Uniform(rate) or Map(path) turnover, loading mode FixMe |
 // OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
 // or CUDA(...) (exponential event times, the reference CUDA algorithm's
-// defaults) with Monolithic or IsolatedIndividuals parallelism; reporters Biodiversity,
+// defaults) with Monolithic, IsolatedIndividuals or IsolatedLandscape parallelism; reporters Biodiversity,
 // Counter, Execution (others are ignored with a notice); log EventLog(directory,
 // capacity) writes the reference's event log.
 #include <glob.h>
@@ -119,6 +119,7 @@ struct Run {
     bool entropy = false;
     double percentage = 1.0;
     uint32_t rank = 0, size = 1;
+    bool landscape = false;  // IsolatedLandscape: partition by subdomain, not by origin index
     std::vector<necsim_lineage> list;  // sample origin List
     bool resume = false;
     double pause_before = -1.0;
@@ -334,12 +335,15 @@ void parse_algorithm(const Value &a, Run &r) {
     // reference's lossy cache capacity has no counterpart
     if (const Value *p = a.field("parallelism_mode")) {
         const std::string &m = p->variant();
-        if (m == "IsolatedIndividuals") {
+        if (m == "IsolatedIndividuals" || m == "IsolatedLandscape") {
             const Value &part = need(*p, "partition");
             r.rank = as_u32(need(part, "rank"), "rank");
             r.size = as_u32(need(part, "size"), "size");
+            if (r.size == 0 || r.rank >= r.size) fail("the partition rank must be below its size");
+            r.landscape = m == "IsolatedLandscape";
         } else if (m != "Monolithic") {
-            fail("parallelism mode " + m + " is not supported (Monolithic, IsolatedIndividuals)");
+            fail("parallelism mode " + m +
+                 " is not supported (Monolithic, IsolatedIndividuals, IsolatedLandscape)");
         }
     }
 }
@@ -646,16 +650,34 @@ int simulate(const std::string &path, bool run) {
         std::vector<necsim_lineage> all(n);
         rc = necsim_enumerate_origins(&r.sc, all.data(), n, &n);
         if (rc) fail("origin enumeration failed (status " + std::to_string(rc) + ")");
+        // IsolatedLandscape samples every origin, then keeps its subdomain's
+        // (independent/src/launch.rs:101-110, origin_sampler/decomposition.rs)
+        const uint32_t prank = r.landscape ? 0 : r.rank, psize = r.landscape ? 1 : r.size;
         uint64_t k = 0;
-        necsim_presample_origins(n, r.percentage, r.rank, r.size, nullptr, 0, &k);
+        necsim_presample_origins(n, r.percentage, prank, psize, nullptr, 0, &k);
         std::vector<uint64_t> pos(k);
-        rc = necsim_presample_origins(n, r.percentage, r.rank, r.size, pos.data(), k, &k);
+        rc = necsim_presample_origins(n, r.percentage, prank, psize, pos.data(), k, &k);
         if (rc) fail("invalid sample percentage or partition");
         lineages.reserve(k);
         for (uint64_t p : pos) lineages.push_back(all[p]);
-    } else {
+    } else if (!r.landscape) {
         // a resumed sample is partitioned like fresh origins
         for (size_t j = r.rank; j < r.list.size(); j += r.size) lineages.push_back(r.list[j]);
+    } else {
+        lineages = r.list;
+    }
+    if (r.landscape) {
+        std::vector<uint32_t> ranks(lineages.size());
+        int32_t exact = 1;
+        const int rc = necsim_subdomain_ranks(&r.sc, r.size, lineages.data(), lineages.size(), ranks.data(), &exact);
+        if (rc) fail("landscape decomposition failed (status " + std::to_string(rc) + ")");
+        if (!exact)
+            std::fprintf(stderr, "necsim-b200: warning: the habitat could not be partitioned into %u partition(s)\n",
+                         r.size);
+        size_t m = 0;
+        for (size_t j = 0; j < lineages.size(); ++j)
+            if (ranks[j] == r.rank) lineages[m++] = lineages[j];
+        lineages.resize(m);
     }
     std::printf("necsim-b200: %s, speciation %g, seed %" PRIu64 ", %zu lineages%s\n", r.summary.c_str(),
                 r.speciation, r.seed, lineages.size(), r.resume ? " (resumed)" : "");

@@ -229,6 +229,116 @@ void for_each_noise_origin(const necsim_scenario &sc, F &&visit) {
     }
 }
 
+// ---- landscape decompositions (necsim/impls/no-std/src/decomposition) ----
+
+// Decomposition::map_location_to_subdomain_rank of a scenario's decomposition
+// into `size` subdomains; every extent has its origin at (0, 0).
+struct SubdomainMap {
+    enum { Modulo, Radial, Equal } how = Modulo;
+    uint32_t size = 1;
+    uint64_t width = 1, height = 1;   // the habitat's extent (OffByOneU32 values)
+    uint8_t morton_x = 0, morton_y = 0;
+    std::vector<uint64_t> indices;    // Equal: first Morton index of ranks 1..
+    bool exact = true;
+
+    // equal/mod.rs:75-99
+    static uint64_t morton(uint8_t mx, uint8_t my, uint32_t dx, uint32_t dy) {
+        uint64_t m = 0;
+        const uint8_t both = std::min(mx, my);
+        for (uint32_t b = 0; b < both; ++b) {
+            m |= (uint64_t)(dx & 1u) << (b * 2);
+            dx >>= 1;
+            m |= (uint64_t)(dy & 1u) << (b * 2 + 1);
+            dy >>= 1;
+        }
+        mx -= both;
+        my -= both;
+        if (mx > 0) m |= (uint64_t)dx << (both * 2);
+        if (my > 0) m |= (uint64_t)dy << (both * 2 + mx);
+        return m;
+    }
+
+    // equal/mod.rs:66-73: ceil(ln(n) / ln 2) with the C library's ln, like
+    // the reference's IntrinsicsMathsCore
+    static uint8_t next_log2(uint64_t n) {
+        return n > 1 ? (uint8_t)std::ceil(std::log((double)n) / 0.693147180559945309417232121458176568) : 0;
+    }
+
+    uint32_t rank(uint32_t x, uint32_t y) const {
+        switch (how) {
+        case Modulo:  // modulo.rs:32-45
+            return (uint32_t)(((uint64_t)y * width + (uint64_t)x) % size);
+        case Radial: {  // radial.rs:38-57, atan2 from the C library (libm's in the reference)
+            const double fraction =
+                std::atan2((double)((int64_t)y - (int64_t)height / 2), (double)((int64_t)x - (int64_t)width / 2)) *
+                    0.318309886183790671537767526745028724 * 0.5 +
+                0.5;
+            const double r = std::floor((double)size * fraction);
+            const uint32_t ri = r >= 4294967295.0 ? 0xffffffffu : (r > 0.0 ? (uint32_t)r : 0u);
+            return std::min(ri, size - 1);
+        }
+        default: {  // equal/mod.rs:50-62
+            const uint64_t m = morton(morton_x, morton_y, x, y);
+            const auto it = std::lower_bound(indices.begin(), indices.end(), m);
+            const uint32_t at = (uint32_t)(it - indices.begin());
+            return (it != indices.end() && *it == m) ? at + 1 : at;
+        }
+        }
+    }
+};
+
+// rustcoalescence/scenarios/src/*.rs `decompose`
+SubdomainMap make_subdomain_map(const necsim_scenario &sc, uint32_t size) {
+    SubdomainMap d;
+    d.size = size;
+    switch (sc.kind) {
+    case NECSIM_NON_SPATIAL:  // habitat/non_spatial.rs: the area is the extent
+        d.width = sc.width;
+        d.height = sc.height;
+        break;
+    case NECSIM_SPATIALLY_IMPLICIT:  // SPATIALLY_IMPLICIT_EXTENT, the whole plane
+        d.width = d.height = 1ULL << 32;
+        break;
+    case NECSIM_ALMOST_INFINITE_NORMAL:
+    case NECSIM_ALMOST_INFINITE_CLARK2DT:
+    case NECSIM_WRAPPING_NOISE:
+        d.how = SubdomainMap::Radial;
+        d.width = d.height = 1ULL << 32;
+        break;
+    default: {
+        // equal/weight.rs:12-70 EqualDecomposition::weight
+        d.how = SubdomainMap::Equal;
+        d.width = sc.width;
+        d.height = sc.height;
+        d.morton_x = SubdomainMap::next_log2(d.width);
+        d.morton_y = SubdomainMap::next_log2(d.height);
+        std::vector<std::pair<uint64_t, uint32_t>> cells;
+        uint64_t total = 0;
+        for (uint32_t y = 0; y < sc.height; ++y)
+            for (uint32_t x = 0; x < sc.width; ++x) {
+                const uint32_t h = sc.habitat[(uint64_t)y * sc.width + x];
+                if (h == 0) continue;
+                total += h;
+                cells.emplace_back(SubdomainMap::morton(d.morton_x, d.morton_y, x, y), h);
+            }
+        std::sort(cells.begin(), cells.end());
+        uint64_t cumulative = 0;
+        uint32_t last = 0;
+        for (const auto &c : cells) {
+            const uint32_t next = (uint32_t)((unsigned __int128)cumulative * size / total);
+            cumulative += c.second;
+            if (next != last) {
+                last = next;
+                d.indices.push_back(c.first);
+            }
+        }
+        d.exact = d.indices.size() + 1 == size;
+        break;
+    }
+    }
+    return d;
+}
+
 // One simulation's host-side description.
 struct SimHost {
     necsim_scenario sc;
@@ -1935,6 +2045,17 @@ int necsim_build_tables(const necsim_scenario *scenario, necsim_cell_record *cel
         static_assert(sizeof(necsim_alias_atom) == sizeof(AliasAtom), "alias atom layout");
         if (cells) std::memcpy(cells, t.cells.data(), t.cells.size() * sizeof(CellRecord));
         if (atoms) std::memcpy(atoms, t.atoms.data(), std::min<uint64_t>(atom_cap, t.atoms.size()) * sizeof(AliasAtom));
+    });
+}
+
+int necsim_subdomain_ranks(const necsim_scenario *scenario, uint32_t size, const necsim_lineage *lineages,
+                           uint64_t n, uint32_t *ranks, int32_t *exact) {
+    if (!scenario || size == 0 || (n && (!lineages || !ranks))) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, nullptr, 0, [&] {
+        validate(*scenario);
+        const SubdomainMap d = make_subdomain_map(*scenario, size);
+        for (uint64_t j = 0; j < n; ++j) ranks[j] = d.rank(lineages[j].x, lineages[j].y);
+        if (exact) *exact = d.exact ? 1 : 0;
     });
 }
 

@@ -285,3 +285,28 @@ def test_check_almost_infinite_rectangle_sample(nb, tmp_path, sample):
     r = run_driver(nb, "check", CONFIG.replace("NonSpatial(area: (30, 20), deme: 2)", scen), tmp_path)
     assert r.returncode == 0, r.stderr
     assert "AlmostInfinite(Rectangle(origin:" in r.stdout and "12 lineages" in r.stdout
+
+
+@pytest.mark.parametrize("scenario", ["NonSpatial(area: (30, 20), deme: 2)", WN_SCENARIO,
+                                      "AlmostInfinite(sample: Circle(radius: 12), dispersal: Normal(sigma: 2.0))"])
+def test_check_isolated_landscape_partitions(nb, tmp_path, scenario):
+    """IsolatedLandscape (independent/src/launch.rs:101-110): each rank keeps
+    the sampled origins of its subdomain; the ranks split the sample."""
+    base = CONFIG.replace("NonSpatial(area: (30, 20), deme: 2)", scenario).replace("percentage: 1.0", "percentage: 0.7")
+    counts = []
+    for rank in range(3):
+        cfg = base.replace("Monolithic(event_slice: Relative(factor: 2.0))",
+                           "IsolatedLandscape(partition: Partition(rank: %d, size: 3), "
+                           "event_slice: Relative(factor: 2.0))" % rank)
+        r = run_driver(nb, "check", cfg, tmp_path)
+        assert r.returncode == 0, r.stderr
+        counts.append(int(re.search(r"(\d+) lineages", r.stdout).group(1)))
+    r = run_driver(nb, "check", base, tmp_path)
+    total = int(re.search(r"(\d+) lineages", r.stdout).group(1))
+    # a real split (the wrapping WrappingNoise sample lies at two angles of
+    # the radial decomposition, so one of its ranks is empty)
+    assert sum(counts) == total and max(counts) < total
+    bad = base.replace("Monolithic(event_slice: Relative(factor: 2.0))",
+                       "IsolatedLandscape(partition: Partition(rank: 3, size: 3))")
+    r = run_driver(nb, "check", bad, tmp_path)
+    assert r.returncode == 1 and "rank must be below" in r.stderr
