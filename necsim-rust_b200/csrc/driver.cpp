@@ -19,12 +19,14 @@
 // OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
 // or CUDA(...) (exponential event times, the reference CUDA algorithm's
 // defaults) with Monolithic, IsolatedIndividuals or IsolatedLandscape parallelism; reporters Biodiversity,
-// Counter, Execution (others are ignored with a notice); log EventLog(directory,
+// Counter, Execution, Csv(output) (others are ignored with a notice); log EventLog(directory,
 // capacity) writes the reference's event log.
 #include <glob.h>
 #include <sys/stat.h>
 
+#include <algorithm>
 #include <cctype>
+#include <charconv>
 #include <chrono>
 #include <cinttypes>
 #include <cmath>
@@ -120,6 +122,7 @@ struct Run {
     double percentage = 1.0;
     uint32_t rank = 0, size = 1;
     bool landscape = false;  // IsolatedLandscape: partition by subdomain, not by origin index
+    std::string csv_output;  // the Csv reporter's file (empty: none)
     std::vector<necsim_lineage> list;  // sample origin List
     bool resume = false;
     double pause_before = -1.0;
@@ -416,7 +419,7 @@ Run parse_config(const std::string &text) {
     r.sc.speciation_probability = r.speciation;
     if (const Value *a = root.field("algorithm")) parse_algorithm(*a, r);
     parse_reporters(root, r);
-    r.args.report_dispersal = r.rep_counter ? 1 : 0;
+    r.args.report_dispersal = (r.rep_counter || !r.csv_output.empty()) ? 1 : 0;
     return r;
 }
 
@@ -440,6 +443,8 @@ void parse_reporters(const Value &root, Run &r) {
                 r.rep_counter = true;
             else if (v == "Execution")
                 r.rep_execution = true;
+            else if (v == "Csv")
+                r.csv_output = need(*n, "output").text;
             else
                 std::fprintf(stderr, "necsim-b200: reporter %s is not provided here and is ignored\n", v.c_str());
         }
@@ -579,14 +584,73 @@ struct EventCounter {
     }
 };
 
+// The Csv reporter (necsim/plugins/csv/src/lib.rs): the header, then one
+// line per event in delivery order, `reference,time,x,y,index,type` with the
+// event's origin and type 's' (speciation) or 'd' (dispersal).  Times print
+// as Rust's Display for f64 does: the shortest digits that read back to the
+// same value, without an exponent.
+struct CsvWriter {
+    FILE *f = nullptr;
+    explicit CsvWriter(const std::string &path) {
+        if (path.empty()) return;
+        f = std::fopen(path.c_str(), "w");  // initialise(): create + truncate
+        if (!f) fail("cannot write the Csv reporter's output " + path);
+        std::fputs("reference,time,x,y,index,type\n", f);
+    }
+    ~CsvWriter() {
+        if (f) std::fclose(f);
+    }
+    CsvWriter(const CsvWriter &) = delete;
+    CsvWriter &operator=(const CsvWriter &) = delete;
+    // Rust's Display for a finite f64: the shortest round-trip digits
+    // (std::to_chars' scientific form), written out in fixed notation with
+    // zeros filling any place beyond them
+    static std::string display(double v) {
+        char t[64];
+        const auto end = std::to_chars(t, t + sizeof(t), v, std::chars_format::scientific).ptr;
+        std::string sci(t, end), out;
+        if (!sci.empty() && sci[0] == '-') {
+            out = "-";
+            sci.erase(0, 1);
+        }
+        const size_t e = sci.find('e');
+        std::string digits = sci.substr(0, e);
+        digits.erase(std::remove(digits.begin(), digits.end(), '.'), digits.end());
+        const long x = std::strtol(sci.c_str() + e + 1, nullptr, 10);  // value = 0.d1d2.. * 10^(x + 1)
+        const long n = (long)digits.size();
+        if (x >= n - 1) {
+            out += digits + std::string((size_t)(x - (n - 1)), '0');
+        } else if (x >= 0) {
+            out += digits.substr(0, (size_t)x + 1) + "." + digits.substr((size_t)x + 1);
+        } else {
+            out += "0." + std::string((size_t)(-x - 1), '0') + digits;
+        }
+        return out;
+    }
+    void row(uint64_t gref, double time, uint32_t x, uint32_t y, uint32_t index, char type) {
+        if (!f) return;
+        std::fprintf(f, "%" PRIu64 ",%s,%u,%u,%u,%c\n", gref, display(time).c_str(), x, y, index, type);
+    }
+    void speciation(const necsim_speciation_event *ev, uint64_t n) {
+        for (uint64_t i = 0; f && i < n; ++i)
+            row(ev[i].global_lineage_reference, ev[i].event_time, ev[i].x, ev[i].y, ev[i].index, 's');
+    }
+    void dispersal(const necsim_dispersal_event *ev, uint64_t n) {
+        for (uint64_t i = 0; f && i < n; ++i)
+            row(ev[i].global_lineage_reference, ev[i].event_time, ev[i].x, ev[i].y, ev[i].index, 'd');
+    }
+};
+
 struct Counts {
     EventCounter counter;
     necsim_reporter log{};  // the event log's reporter, when one is written
+    CsvWriter *csv = nullptr;
 };
 
 int on_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
     Counts &c = *static_cast<Counts *>(user);
     for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
+    if (c.csv) c.csv->speciation(ev, n);
     if (c.log.report_speciation) return c.log.report_speciation(c.log.user, ev, n);
     return 0;
 }
@@ -595,6 +659,7 @@ int on_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     Counts &c = *static_cast<Counts *>(user);
     if (c.log.report_dispersal && c.log.report_dispersal(c.log.user, ev, n) != 0) return 1;
     for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
+    if (c.csv) c.csv->dispersal(ev, n);
     return 0;
 }
 
@@ -697,6 +762,8 @@ int simulate(const std::string &path, bool run) {
         fail("set-up failed (status " + std::to_string(rc) + "): " + m);
     }
     Counts counts;
+    CsvWriter csv(r.csv_output);
+    counts.csv = &csv;
     necsim_event_log *log = nullptr;
     if (!r.log_directory.empty()) {
         rc = necsim_event_log_create(r.log_directory.c_str(), r.log_capacity, 1, r.args.report_dispersal, &log);
@@ -758,10 +825,12 @@ struct ReplayCounts {
     bool have_last = false;
     necsim_speciation_event last{};
     EventCounter counter;
+    CsvWriter *csv = nullptr;
 };
 
 int replay_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
     ReplayCounts &c = *static_cast<ReplayCounts *>(user);
+    if (c.csv) c.csv->speciation(ev, n);
     for (uint64_t i = 0; i < n; ++i) {
         c.counter.on(ev[i]);
         const necsim_speciation_event &e = ev[i];
@@ -778,6 +847,7 @@ int replay_speciation(void *user, const necsim_speciation_event *ev, uint64_t n)
 int replay_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     ReplayCounts &c = *static_cast<ReplayCounts *>(user);
     for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
+    if (c.csv) c.csv->dispersal(ev, n);
     return 0;
 }
 
@@ -823,12 +893,16 @@ int replay(const std::string &path) {
     std::vector<const char *> ptrs;
     for (const std::string &s : segs) ptrs.push_back(s.c_str());
     ReplayCounts counts;
+    CsvWriter csv(r.csv_output);
+    counts.csv = &csv;
     necsim_reporter rep{&counts, replay_speciation, replay_dispersal};
     char err[512];
     uint64_t n = 0;
     const auto t0 = std::chrono::steady_clock::now();
-    const int rc = necsim_event_log_replay(ptrs.data(), ptrs.size(), capacity, r.rep_biodiversity ? 1 : 0,
-                                           r.rep_counter ? 1 : 0, strict ? 1 : 0, &rep, &n, err, sizeof(err));
+    const bool csv_out = !r.csv_output.empty();
+    const int rc = necsim_event_log_replay(ptrs.data(), ptrs.size(), capacity, (r.rep_biodiversity || csv_out) ? 1 : 0,
+                                           (r.rep_counter || csv_out) ? 1 : 0, strict ? 1 : 0, &rep, &n, err,
+                                           sizeof(err));
     const auto t1 = std::chrono::steady_clock::now();
     if (rc) fail(std::string("replay failed: ") + err);
     if (err[0]) std::fprintf(stderr, "necsim-b200: warning: %s\n", err);

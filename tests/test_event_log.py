@@ -272,3 +272,47 @@ def counter_summary(out):
             "   - new location, no coalescence:\n     0\n   - new location, with coalescence:\n     0\n"
             "   - detected late, no coalescence:\n     %d\n   - detected late, with coalescence:\n     %d\n"
             % (spec + late, raw, spec + late_disp, spec, (late_disp - late) % (1 << 64), late))
+
+
+def rust_display(v):
+    """Rust's Display for a finite f64: the shortest round-trip digits in
+    fixed notation (no exponent, no trailing `.0`)."""
+    from decimal import Decimal
+    t = format(Decimal(repr(float(v))), "f")
+    if "." in t:
+        t = t.rstrip("0").rstrip(".")
+    return t
+
+
+def test_driver_csv_reporter(nb, tmp_path):
+    """The Csv reporter (necsim/plugins/csv/src/lib.rs) during a replay: a
+    header, then `reference,time,x,y,index,type` per event in delivery order,
+    with the origin of dispersal events and Rust's f64 Display."""
+    import subprocess
+    spec, disp = random_events(nb, 120, 5)
+    spec["event_time"][:4] = [3.0, 1e-7, 0.30000000000000004, 123456789.125]
+    disp["event_time"][:2] = [2.0 ** 60, 5e-324]
+    write(nb, str(tmp_path / "log"), spec, disp, capacity=50)
+    csv = tmp_path / "events.csv"
+    cfg = """(
+        log: EventLog(segments: ["%s/*"]),
+        reporters: [Plugin(library: "libnecsim_plugins_csv.so", reporters: [Csv(output: "%s")])],
+    )""" % (tmp_path / "log", csv)
+    (tmp_path / "r.ron").write_text(cfg)
+    r = subprocess.run([nb.DRIVER, "replay", str(tmp_path / "r.ron")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = nb.replay_event_log(str(tmp_path / "log/*"), need_speciation=True, need_dispersal=True)
+    rows, s, d = ["reference,time,x,y,index,type"], 0, 0
+    for kind, n in out.delivery:
+        src = out.speciation[s:s + n] if kind == "s" else out.dispersal[d:d + n]
+        for e in src:
+            rows.append("%d,%s,%d,%d,%d,%s" % (e["gref"], rust_display(e["event_time"]), e["x"], e["y"], e["index"],
+                                               kind))
+        if kind == "s":
+            s += n
+        else:
+            d += n
+    assert s == 120 and d == 120
+    assert csv.read_text() == "\n".join(rows) + "\n"
+    assert {"3", "0.0000001", "0.30000000000000004", "123456789.125", "1152921504606847000"} <= \
+        {row.split(",")[1] for row in rows[1:]}
