@@ -19,7 +19,8 @@
 // OffByOne | Strict) scenarios; algorithm Independent(...) (Poisson event times)
 // or CUDA(...) (exponential event times, the reference CUDA algorithm's
 // defaults) with Monolithic, IsolatedIndividuals or IsolatedLandscape parallelism; reporters Biodiversity,
-// Counter, Execution, Csv(output) (others are ignored with a notice); log EventLog(directory,
+// Counter, Execution, Csv(output), GlobalSpeciation / GlobalTurnover / GlobalCoverage(output)
+// (others are ignored with a notice); log EventLog(directory,
 // capacity) writes the reference's event log.
 #include <glob.h>
 #include <sys/stat.h>
@@ -123,6 +124,12 @@ struct Run {
     uint32_t rank = 0, size = 1;
     bool landscape = false;  // IsolatedLandscape: partition by subdomain, not by origin index
     std::string csv_output;  // the Csv reporter's file (empty: none)
+    // the statistics plugin's GlobalSpeciation, GlobalTurnover and GlobalCoverage files (empty: none)
+    std::string speciation_output, turnover_output, coverage_output;
+    bool needs_dispersal() const { return rep_counter || !csv_output.empty() || !turnover_output.empty() ||
+                                          !coverage_output.empty(); }
+    bool needs_speciation() const { return rep_biodiversity || !csv_output.empty() || !speciation_output.empty() ||
+                                           !turnover_output.empty(); }
     std::vector<necsim_lineage> list;  // sample origin List
     bool resume = false;
     double pause_before = -1.0;
@@ -419,7 +426,7 @@ Run parse_config(const std::string &text) {
     r.sc.speciation_probability = r.speciation;
     if (const Value *a = root.field("algorithm")) parse_algorithm(*a, r);
     parse_reporters(root, r);
-    r.args.report_dispersal = (r.rep_counter || !r.csv_output.empty()) ? 1 : 0;
+    r.args.report_dispersal = r.needs_dispersal() ? 1 : 0;
     return r;
 }
 
@@ -445,6 +452,12 @@ void parse_reporters(const Value &root, Run &r) {
                 r.rep_execution = true;
             else if (v == "Csv")
                 r.csv_output = need(*n, "output").text;
+            else if (v == "GlobalSpeciation")
+                r.speciation_output = need(*n, "output").text;
+            else if (v == "GlobalTurnover")
+                r.turnover_output = need(*n, "output").text;
+            else if (v == "GlobalCoverage")
+                r.coverage_output = need(*n, "output").text;
             else
                 std::fprintf(stderr, "necsim-b200: reporter %s is not provided here and is ignored\n", v.c_str());
         }
@@ -584,6 +597,91 @@ struct EventCounter {
     }
 };
 
+// Rust's Display for a finite f64: the shortest round-trip digits
+// (std::to_chars' scientific form), written out in fixed notation with zeros
+// filling any place beyond them (2^60 prints as 1152921504606847000)
+std::string rust_f64_display(double v) {
+    char t[64];
+    const auto end = std::to_chars(t, t + sizeof(t), v, std::chars_format::scientific).ptr;
+    std::string sci(t, end), out;
+    if (!sci.empty() && sci[0] == '-') {
+        out = "-";
+        sci.erase(0, 1);
+    }
+    const size_t e = sci.find('e');
+    std::string digits = sci.substr(0, e);
+    digits.erase(std::remove(digits.begin(), digits.end(), '.'), digits.end());
+    const long x = std::strtol(sci.c_str() + e + 1, nullptr, 10);  // value = d1.d2.. * 10^x
+    const long n = (long)digits.size();
+    if (x >= n - 1) {
+        out += digits + std::string((size_t)(x - (n - 1)), '0');
+    } else if (x >= 0) {
+        out += digits.substr(0, (size_t)x + 1) + "." + digits.substr((size_t)x + 1);
+    } else {
+        out += "0." + std::string((size_t)(-x - 1), '0') + digits;
+    }
+    return out;
+}
+
+// A reporter's output file: created and truncated, with its header line.
+FILE *open_output(const std::string &path, const char *header) {
+    if (path.empty()) return nullptr;
+    FILE *f = std::fopen(path.c_str(), "w");  // initialise(): create + truncate
+    if (!f) fail("cannot write the reporter output " + path);
+    std::fprintf(f, "%s\n", header);
+    return f;
+}
+
+// The statistics plugin (necsim/plugins/statistics/src/{speciation,turnover,
+// coverage}.rs): GlobalSpeciation writes each speciation's event time,
+// GlobalTurnover the time since the lineage's previous event for every
+// speciation and dispersal, GlobalCoverage each dispersal's origin and
+// target.  Each skips an event equal to the previous one of its kind
+// (event.rs:299-318: the same origin and event time, and target).
+struct StatisticsWriters {
+    FILE *speciation = nullptr, *turnover = nullptr, *coverage = nullptr;
+    bool have_spec = false, have_disp = false;
+    necsim_speciation_event last_spec{};
+    necsim_dispersal_event last_disp{};
+    explicit StatisticsWriters(const Run &r)
+        : speciation(open_output(r.speciation_output, "speciation")),
+          turnover(open_output(r.turnover_output, "turnover")),
+          coverage(open_output(r.coverage_output, "x-from,y-from,index-from,x-to,y-to,index-to")) {}
+    ~StatisticsWriters() {
+        for (FILE *f : {speciation, turnover, coverage})
+            if (f) std::fclose(f);
+    }
+    StatisticsWriters(const StatisticsWriters &) = delete;
+    StatisticsWriters &operator=(const StatisticsWriters &) = delete;
+    void on(const necsim_speciation_event *ev, uint64_t n) {
+        for (uint64_t i = 0; i < n; ++i) {
+            const necsim_speciation_event &e = ev[i];
+            if (have_spec && e.x == last_spec.x && e.y == last_spec.y && e.index == last_spec.index &&
+                e.event_time == last_spec.event_time)
+                continue;
+            have_spec = true;
+            last_spec = e;
+            if (speciation) std::fprintf(speciation, "%s\n", rust_f64_display(e.event_time).c_str());
+            if (turnover) std::fprintf(turnover, "%s\n", rust_f64_display(e.event_time - e.prior_time).c_str());
+        }
+    }
+    void on(const necsim_dispersal_event *ev, uint64_t n) {
+        for (uint64_t i = 0; i < n; ++i) {
+            const necsim_dispersal_event &e = ev[i];
+            if (have_disp && e.x == last_disp.x && e.y == last_disp.y && e.index == last_disp.index &&
+                e.event_time == last_disp.event_time && e.target_x == last_disp.target_x &&
+                e.target_y == last_disp.target_y && e.target_index == last_disp.target_index)
+                continue;
+            have_disp = true;
+            last_disp = e;
+            if (turnover) std::fprintf(turnover, "%s\n", rust_f64_display(e.event_time - e.prior_time).c_str());
+            if (coverage)
+                std::fprintf(coverage, "%u,%u,%u,%u,%u,%u\n", e.x, e.y, e.index, e.target_x, e.target_y,
+                             e.target_index);
+        }
+    }
+};
+
 // The Csv reporter (necsim/plugins/csv/src/lib.rs): the header, then one
 // line per event in delivery order, `reference,time,x,y,index,type` with the
 // event's origin and type 's' (speciation) or 'd' (dispersal).  Times print
@@ -591,45 +689,15 @@ struct EventCounter {
 // same value, without an exponent.
 struct CsvWriter {
     FILE *f = nullptr;
-    explicit CsvWriter(const std::string &path) {
-        if (path.empty()) return;
-        f = std::fopen(path.c_str(), "w");  // initialise(): create + truncate
-        if (!f) fail("cannot write the Csv reporter's output " + path);
-        std::fputs("reference,time,x,y,index,type\n", f);
-    }
+    explicit CsvWriter(const std::string &path) : f(open_output(path, "reference,time,x,y,index,type")) {}
     ~CsvWriter() {
         if (f) std::fclose(f);
     }
     CsvWriter(const CsvWriter &) = delete;
     CsvWriter &operator=(const CsvWriter &) = delete;
-    // Rust's Display for a finite f64: the shortest round-trip digits
-    // (std::to_chars' scientific form), written out in fixed notation with
-    // zeros filling any place beyond them
-    static std::string display(double v) {
-        char t[64];
-        const auto end = std::to_chars(t, t + sizeof(t), v, std::chars_format::scientific).ptr;
-        std::string sci(t, end), out;
-        if (!sci.empty() && sci[0] == '-') {
-            out = "-";
-            sci.erase(0, 1);
-        }
-        const size_t e = sci.find('e');
-        std::string digits = sci.substr(0, e);
-        digits.erase(std::remove(digits.begin(), digits.end(), '.'), digits.end());
-        const long x = std::strtol(sci.c_str() + e + 1, nullptr, 10);  // value = 0.d1d2.. * 10^(x + 1)
-        const long n = (long)digits.size();
-        if (x >= n - 1) {
-            out += digits + std::string((size_t)(x - (n - 1)), '0');
-        } else if (x >= 0) {
-            out += digits.substr(0, (size_t)x + 1) + "." + digits.substr((size_t)x + 1);
-        } else {
-            out += "0." + std::string((size_t)(-x - 1), '0') + digits;
-        }
-        return out;
-    }
     void row(uint64_t gref, double time, uint32_t x, uint32_t y, uint32_t index, char type) {
         if (!f) return;
-        std::fprintf(f, "%" PRIu64 ",%s,%u,%u,%u,%c\n", gref, display(time).c_str(), x, y, index, type);
+        std::fprintf(f, "%" PRIu64 ",%s,%u,%u,%u,%c\n", gref, rust_f64_display(time).c_str(), x, y, index, type);
     }
     void speciation(const necsim_speciation_event *ev, uint64_t n) {
         for (uint64_t i = 0; f && i < n; ++i)
@@ -645,12 +713,14 @@ struct Counts {
     EventCounter counter;
     necsim_reporter log{};  // the event log's reporter, when one is written
     CsvWriter *csv = nullptr;
+    StatisticsWriters *stats = nullptr;
 };
 
 int on_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
     Counts &c = *static_cast<Counts *>(user);
     for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
     if (c.csv) c.csv->speciation(ev, n);
+    if (c.stats) c.stats->on(ev, n);
     if (c.log.report_speciation) return c.log.report_speciation(c.log.user, ev, n);
     return 0;
 }
@@ -660,6 +730,7 @@ int on_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     if (c.log.report_dispersal && c.log.report_dispersal(c.log.user, ev, n) != 0) return 1;
     for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
     if (c.csv) c.csv->dispersal(ev, n);
+    if (c.stats) c.stats->on(ev, n);
     return 0;
 }
 
@@ -764,6 +835,8 @@ int simulate(const std::string &path, bool run) {
     Counts counts;
     CsvWriter csv(r.csv_output);
     counts.csv = &csv;
+    StatisticsWriters stats(r);
+    counts.stats = &stats;
     necsim_event_log *log = nullptr;
     if (!r.log_directory.empty()) {
         rc = necsim_event_log_create(r.log_directory.c_str(), r.log_capacity, 1, r.args.report_dispersal, &log);
@@ -826,11 +899,13 @@ struct ReplayCounts {
     necsim_speciation_event last{};
     EventCounter counter;
     CsvWriter *csv = nullptr;
+    StatisticsWriters *stats = nullptr;
 };
 
 int replay_speciation(void *user, const necsim_speciation_event *ev, uint64_t n) {
     ReplayCounts &c = *static_cast<ReplayCounts *>(user);
     if (c.csv) c.csv->speciation(ev, n);
+    if (c.stats) c.stats->on(ev, n);
     for (uint64_t i = 0; i < n; ++i) {
         c.counter.on(ev[i]);
         const necsim_speciation_event &e = ev[i];
@@ -848,6 +923,7 @@ int replay_dispersal(void *user, const necsim_dispersal_event *ev, uint64_t n) {
     ReplayCounts &c = *static_cast<ReplayCounts *>(user);
     for (uint64_t i = 0; i < n; ++i) c.counter.on(ev[i]);
     if (c.csv) c.csv->dispersal(ev, n);
+    if (c.stats) c.stats->on(ev, n);
     return 0;
 }
 
@@ -895,14 +971,14 @@ int replay(const std::string &path) {
     ReplayCounts counts;
     CsvWriter csv(r.csv_output);
     counts.csv = &csv;
+    StatisticsWriters stats(r);
+    counts.stats = &stats;
     necsim_reporter rep{&counts, replay_speciation, replay_dispersal};
     char err[512];
     uint64_t n = 0;
     const auto t0 = std::chrono::steady_clock::now();
-    const bool csv_out = !r.csv_output.empty();
-    const int rc = necsim_event_log_replay(ptrs.data(), ptrs.size(), capacity, (r.rep_biodiversity || csv_out) ? 1 : 0,
-                                           (r.rep_counter || csv_out) ? 1 : 0, strict ? 1 : 0, &rep, &n, err,
-                                           sizeof(err));
+    const int rc = necsim_event_log_replay(ptrs.data(), ptrs.size(), capacity, r.needs_speciation() ? 1 : 0,
+                                           r.needs_dispersal() ? 1 : 0, strict ? 1 : 0, &rep, &n, err, sizeof(err));
     const auto t1 = std::chrono::steady_clock::now();
     if (rc) fail(std::string("replay failed: ") + err);
     if (err[0]) std::fprintf(stderr, "necsim-b200: warning: %s\n", err);

@@ -316,3 +316,49 @@ def test_driver_csv_reporter(nb, tmp_path):
     assert csv.read_text() == "\n".join(rows) + "\n"
     assert {"3", "0.0000001", "0.30000000000000004", "123456789.125", "1152921504606847000"} <= \
         {row.split(",")[1] for row in rows[1:]}
+
+
+def test_driver_statistics_reporters(nb, tmp_path):
+    """GlobalSpeciation, GlobalTurnover and GlobalCoverage (necsim/plugins/
+    statistics/src/*.rs) during a replay: each skips an event equal to the
+    previous one of its kind (same origin and event time, and target)."""
+    import subprocess
+    spec, disp = random_events(nb, 150, 9)
+    spec[3::25] = spec[2::25][: len(spec[3::25])]  # repeats: skipped
+    spec["prior_time"][3::50] -= 1e-3              # equal all the same (prior time is ignored)
+    disp[5::20] = disp[4::20][: len(disp[5::20])]
+    write(nb, str(tmp_path / "log"), spec, disp, capacity=40)
+    outs = {k: tmp_path / ("%s.csv" % k) for k in ("GlobalSpeciation", "GlobalTurnover", "GlobalCoverage")}
+    reps = ", ".join('%s(output: "%s")' % (k, v) for k, v in outs.items())
+    cfg = """(
+        log: EventLog(segments: ["%s/*"]),
+        reporters: [Plugin(library: "libnecsim_plugins_statistics.so", reporters: [%s])],
+    )""" % (tmp_path / "log", reps)
+    (tmp_path / "r.ron").write_text(cfg)
+    r = subprocess.run([nb.DRIVER, "replay", str(tmp_path / "r.ron")], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    out = nb.replay_event_log(str(tmp_path / "log/*"), need_speciation=True, need_dispersal=True)
+    sp, tu, co = ["speciation"], ["turnover"], ["x-from,y-from,index-from,x-to,y-to,index-to"]
+    s = d = 0
+    last_s = last_d = None
+    for kind, n in out.delivery:
+        if kind == "s":
+            for e in out.speciation[s:s + n]:
+                key = (int(e["x"]), int(e["y"]), int(e["index"]), float(e["event_time"]))
+                if key != last_s:
+                    last_s = key
+                    sp.append(rust_display(e["event_time"]))
+                    tu.append(rust_display(float(e["event_time"]) - float(e["prior_time"])))
+            s += n
+        else:
+            for e in out.dispersal[d:d + n]:
+                key = tuple(int(e[f]) for f in ("x", "y", "index", "tx", "ty", "tindex")) + (float(e["event_time"]),)
+                if key != last_d:
+                    last_d = key
+                    tu.append(rust_display(float(e["event_time"]) - float(e["prior_time"])))
+                    co.append("%d,%d,%d,%d,%d,%d" % key[:6])
+            d += n
+    assert 1 < len(sp) - 1 < 150 and 1 < len(co) - 1 < 150
+    assert outs["GlobalSpeciation"].read_text() == "\n".join(sp) + "\n"
+    assert outs["GlobalTurnover"].read_text() == "\n".join(tu) + "\n"
+    assert outs["GlobalCoverage"].read_text() == "\n".join(co) + "\n"
