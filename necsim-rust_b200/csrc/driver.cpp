@@ -601,6 +601,8 @@ struct EventCounter {
 // (std::to_chars' scientific form), written out in fixed notation with zeros
 // filling any place beyond them (2^60 prints as 1152921504606847000)
 std::string rust_f64_display(double v) {
+    if (std::isnan(v)) return "NaN";
+    if (std::isinf(v)) return v > 0 ? "inf" : "-inf";
     char t[64];
     const auto end = std::to_chars(t, t + sizeof(t), v, std::chars_format::scientific).ptr;
     std::string sci(t, end), out;
