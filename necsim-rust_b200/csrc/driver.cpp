@@ -11,7 +11,7 @@
 //                                       reporters (no GPU)
 //
 // Supported: speciation; sample (percentage, origin Habitat | List,
-// mode Genesis | Resume); pause (before, config, destiny List, mode Resume),
+// mode Genesis | Resume | Restart(after)); pause (before, config, destiny List, mode Resume | Restart),
 // which writes the configuration that resumes the run; rng Seed | Entropy;
 // the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle or Rectangle; Normal or
 // Clark2Dt), WrappingNoise and SpatiallyExplicit (habitat, dispersal and turnover maps as (Geo)TIFF files
@@ -133,6 +133,9 @@ struct Run {
     std::vector<necsim_lineage> list;  // sample origin List
     bool resume = false;
     double pause_before = -1.0;
+    double restart_after = 0.0;   // sample mode Restart(after): the resume's minimum event time
+    bool restart = false;
+    bool pause_restart = false;   // pause mode Restart: the written configuration restarts
     std::string pause_config;
     std::string algorithm = "Independent";
     bool rep_biodiversity = false, rep_counter = false, rep_execution = false;
@@ -384,10 +387,18 @@ Run parse_config(const std::string &text) {
             }
         }
         if (const Value *m = s->field("mode")) {
-            if (m->variant() == "Resume")
+            // rustcoalescence/src/cli/simulate/dispatch/valid/launch.rs:60-92: Resume
+            // continues with no minimum event time, Restart(after) from `after` on
+            if (m->variant() == "Resume") {
                 r.resume = true;
-            else if (m->variant() != "Genesis")
-                fail("sample mode " + m->variant() + " is not supported (Genesis, Resume)");
+            } else if (m->variant() == "Restart") {
+                r.resume = r.restart = true;
+                r.restart_after = need(*m, "after").as_f64();
+                if (!(r.restart_after >= 0.0) || !std::isfinite(r.restart_after))
+                    fail("Restart(after) must be a finite time >= 0");
+            } else if (m->variant() != "Genesis") {
+                fail("sample mode " + m->variant() + " is not supported (Genesis, Resume, Restart)");
+            }
         }
     }
     if (r.resume != !r.list.empty()) fail("Resume needs a List origin and a List origin needs Resume");
@@ -397,8 +408,12 @@ Run parse_config(const std::string &text) {
             r.pause_config = need(*p, "config").text;
             if (const Value *d = p->field("destiny"))
                 if (d->variant() != "List") fail("pause destiny " + d->variant() + " is not supported (List)");
-            if (const Value *m = p->field("mode"))
-                if (m->variant() != "Resume") fail("pause mode " + m->variant() + " is not supported (Resume)");
+            if (const Value *m = p->field("mode")) {
+                if (m->variant() == "Restart")
+                    r.pause_restart = true;
+                else if (m->variant() != "Resume")
+                    fail("pause mode " + m->variant() + " is not supported (Resume, Restart)");
+            }
         } else if (p->variant() != "None") {
             fail("pause must be None or Pause(...)");
         }
@@ -466,7 +481,10 @@ void parse_reporters(const Value &root, Run &r) {
 
 // the configuration with the remaining lineages as a List sample in Resume
 // mode and no pause (rustcoalescence/src/cli/simulate/pause.rs:20-60)
-std::string resume_config(const std::string &text, uint64_t seed, const std::vector<necsim_lineage> &rem) {
+// (pause.rs:20-61: mode Resume, or Restart(after: the pause time) for the
+// Restart pause mode)
+std::string resume_config(const std::string &text, uint64_t seed, const std::vector<necsim_lineage> &rem,
+                          bool restart, double after) {
     Value root = necsim::ron::parse(text);
     Value sample;
     sample.kind = Value::Struct;
@@ -509,6 +527,16 @@ std::string resume_config(const std::string &text, uint64_t seed, const std::vec
     Value mode;
     mode.kind = Value::Ident;
     mode.text = "Resume";
+    if (restart) {
+        mode.kind = Value::Struct;
+        mode.text = "Restart";
+        Value a;
+        a.kind = Value::Number;
+        std::snprintf(buf, sizeof(buf), "%.17g", after);
+        a.text = buf;
+        if (a.text.find_first_of(".eEn") == std::string::npos) a.text += ".0";
+        mode.fields.emplace_back("after", a);
+    }
     sample.fields.emplace_back("mode", mode);
     Value none;
     none.kind = Value::Ident;
@@ -818,7 +846,8 @@ int simulate(const std::string &path, bool run) {
         lineages.resize(m);
     }
     std::printf("necsim-b200: %s, speciation %g, seed %" PRIu64 ", %zu lineages%s\n", r.summary.c_str(),
-                r.speciation, r.seed, lineages.size(), r.resume ? " (resumed)" : "");
+                r.speciation, r.seed, lineages.size(), r.restart ? " (restarted)" : (r.resume ? " (resumed)" : ""));
+    if (r.restart) std::printf("necsim-b200: restart after t = %.17g\n", r.restart_after);
     std::printf("necsim-b200: algorithm %s, %s event times, delta_t %g, step_slice %" PRIu64 "\n",
                 r.algorithm.c_str(), r.args.event_time_sampler == NECSIM_SAMPLER_EXP ? "exponential" : "Poisson",
                 r.args.delta_t > 0.0 ? r.args.delta_t : 2.0, r.args.step_slice ? r.args.step_slice : (uint64_t)10);
@@ -851,7 +880,7 @@ int simulate(const std::string &path, bool run) {
     necsim_reporter rep{&counts, on_speciation, on_dispersal};
     necsim_outcome out{};
     const auto t1 = std::chrono::steady_clock::now();
-    rc = necsim_gpu_simulate_lineages(ctx, lineages.data(), lineages.size(), 0.0, necsim_seed_from_u64(r.seed),
+    rc = necsim_gpu_simulate_lineages(ctx, lineages.data(), lineages.size(), r.restart_after, necsim_seed_from_u64(r.seed),
                                       r.pause_before, &rep, &out);
     const auto t2 = std::chrono::steady_clock::now();
     if (rc) {
@@ -884,7 +913,7 @@ int simulate(const std::string &path, bool run) {
     if (out.paused && !r.pause_config.empty()) {
         std::ofstream f(r.pause_config);
         if (!f) fail("cannot write " + r.pause_config);
-        f << resume_config(text, r.seed, rem);
+        f << resume_config(text, r.seed, rem, r.pause_restart, r.pause_before);
         std::printf("necsim-b200: %zu remaining lineages written to %s\n", rem.size(), r.pause_config.c_str());
     }
     return 0;

@@ -310,3 +310,38 @@ def test_check_isolated_landscape_partitions(nb, tmp_path, scenario):
                        "IsolatedLandscape(partition: Partition(rank: 3, size: 3))")
     r = run_driver(nb, "check", bad, tmp_path)
     assert r.returncode == 1 and "rank must be below" in r.stderr
+
+
+RESTART_SAMPLE = ("sample: Sample(percentage: 1.0, origin: List([(ref: 7, time: 1.5, loc: (x: 3, y: 4, i: 1)), "
+                  "(ref: 9, time: 0.25, loc: (x: 0, y: 0, i: 0))]), mode: Restart(after: 150.0)),")
+
+
+def test_check_restart_sample_mode(nb, tmp_path):
+    """Sample mode Restart(after) (dispatch/valid/launch.rs:82-92): the listed
+    lineages restart with `after` as the minimum event time."""
+    cfg = CONFIG.replace("sample: Sample(percentage: 1.0, origin: Habitat, mode: Genesis),", RESTART_SAMPLE)
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "2 lineages (restarted)" in r.stdout and "restart after t = 150" in r.stdout
+    r = run_driver(nb, "check", cfg.replace("after: 150.0", "after: -1.0"), tmp_path)
+    assert r.returncode == 1 and "Restart(after)" in r.stderr
+    r = run_driver(nb, "check", cfg.replace("mode: Restart(after: 150.0)", "mode: FixUp()"), tmp_path)
+    assert r.returncode == 1 and "not supported (Genesis, Resume, Restart)" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_restart_pause_mode(nb, tmp_path):
+    """Pause mode Restart (pause.rs:41-53) writes `mode: Restart(after: <before>)`;
+    no lineage has an event between its last one and the pause, so the
+    restart completes the straight run's species."""
+    resume = tmp_path / "restart.ron"
+    cfg = CONFIG.replace("pause: None",
+                         'pause: Pause(before: 150.0, config: "%s", destiny: List, mode: Restart)' % resume)
+    r = run_driver(nb, "simulate", cfg, tmp_path, "p.ron")
+    assert r.returncode == 0, r.stderr
+    assert re.search(r"mode:\s*Restart\(\s*after:\s*150\.0,?\s*\)", resume.read_text())
+    r2 = subprocess.run([nb.DRIVER, "simulate", str(resume)], capture_output=True, text=True, timeout=600)
+    assert r2.returncode == 0, r2.stderr
+    assert "(restarted)" in r2.stdout
+    straight = nb.simulate(0.01, nb.NonSpatial((30, 20), 2), 42)
+    assert species(r.stdout) + species(r2.stdout) == straight.biodiversity
