@@ -11,7 +11,8 @@
 //                                       reporters (no GPU)
 //
 // Supported: speciation; sample (percentage, origin Habitat | List,
-// mode Genesis | Resume | Restart(after)); pause (before, config, destiny List, mode Resume | Restart),
+// origin Bincode(file), mode Genesis | Resume | Restart(after)); pause (before, config,
+// destiny List | Bincode(file), mode Resume | Restart),
 // which writes the configuration that resumes the run; rng Seed | Entropy;
 // the NonSpatial, SpatiallyImplicit, AlmostInfinite (Circle or Rectangle; Normal or
 // Clark2Dt), WrappingNoise and SpatiallyExplicit (habitat, dispersal and turnover maps as (Geo)TIFF files
@@ -136,6 +137,8 @@ struct Run {
     double restart_after = 0.0;   // sample mode Restart(after): the resume's minimum event time
     bool restart = false;
     bool pause_restart = false;   // pause mode Restart: the written configuration restarts
+    bool listed = false;          // the sample origin lists lineages (List or Bincode)
+    std::string pause_bincode;    // pause destiny Bincode(file): the remaining lineages' file
     std::string pause_config;
     std::string algorithm = "Independent";
     bool rep_biodiversity = false, rep_counter = false, rep_execution = false;
@@ -361,6 +364,80 @@ void parse_algorithm(const Value &a, Run &r) {
     }
 }
 
+// ---- lineage files (necsim/impls/std/src/lineage_file/{loader,saver}.rs):
+// a Vec<Lineage> in bincode 1.3.3's DefaultOptions (`bincode::options()`):
+// varint integers (< 251 in one byte, else a 251 / 252 / 253 tag and a u16 /
+// u32 / u64, little-endian), f64 as 8 little-endian bytes; a Lineage is
+// (global reference u64, last event time f64, x u32, y u32, index u32) ----
+void put_varint(std::string &o, uint64_t v) {
+    int bytes = 0;
+    if (v < 251) {
+        o.push_back((char)v);
+        return;
+    } else if (v <= 0xffffULL) {
+        o.push_back((char)251);
+        bytes = 2;
+    } else if (v <= 0xffffffffULL) {
+        o.push_back((char)252);
+        bytes = 4;
+    } else {
+        o.push_back((char)253);
+        bytes = 8;
+    }
+    for (int b = 0; b < bytes; ++b) o.push_back((char)((v >> (8 * b)) & 0xff));
+}
+
+uint64_t get_varint(const std::string &in, size_t &at, const std::string &path) {
+    if (at >= in.size()) fail(path + ": truncated lineage file");
+    const unsigned char tag = (unsigned char)in[at++];
+    if (tag < 251) return tag;
+    const int bytes = tag == 251 ? 2 : tag == 252 ? 4 : tag == 253 ? 8 : 0;
+    if (bytes == 0 || at + bytes > in.size()) fail(path + ": malformed lineage file");
+    uint64_t v = 0;
+    for (int b = 0; b < bytes; ++b) v |= (uint64_t)(unsigned char)in[at + b] << (8 * b);
+    at += bytes;
+    return v;
+}
+
+std::vector<necsim_lineage> read_lineage_file(const std::string &path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) fail("cannot read the lineage file " + path);
+    const std::string in((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+    size_t at = 0;
+    const uint64_t n = get_varint(in, at, path);
+    if (n > in.size()) fail(path + ": malformed lineage file");
+    std::vector<necsim_lineage> out(n);
+    for (auto &l : out) {
+        l.global_reference = get_varint(in, at, path);
+        if (at + 8 > in.size()) fail(path + ": truncated lineage file");
+        std::memcpy(&l.last_event_time, in.data() + at, 8);
+        at += 8;
+        const uint64_t x = get_varint(in, at, path), y = get_varint(in, at, path), i = get_varint(in, at, path);
+        if ((x | y | i) > 0xffffffffULL) fail(path + ": malformed lineage file");
+        l.x = (uint32_t)x;
+        l.y = (uint32_t)y;
+        l.index = (uint32_t)i;
+    }
+    if (at != in.size()) fail(path + ": trailing bytes in the lineage file");
+    return out;
+}
+
+void write_lineage_file(const std::string &path, const std::vector<necsim_lineage> &lins) {
+    std::string o;
+    put_varint(o, lins.size());
+    for (const auto &l : lins) {
+        put_varint(o, l.global_reference);
+        char t[8];
+        std::memcpy(t, &l.last_event_time, 8);
+        o.append(t, 8);
+        put_varint(o, l.x);
+        put_varint(o, l.y);
+        put_varint(o, l.index);
+    }
+    std::ofstream f(path, std::ios::binary | std::ios::trunc);
+    if (!f || !f.write(o.data(), (std::streamsize)o.size())) fail("cannot write the lineage file " + path);
+}
+
 void parse_reporters(const Value &root, Run &r);
 
 Run parse_config(const std::string &text) {
@@ -370,7 +447,11 @@ Run parse_config(const std::string &text) {
     if (const Value *s = root.field("sample")) {
         if (const Value *p = s->field("percentage")) r.percentage = p->as_f64();
         if (const Value *o = s->field("origin")) {
-            if (o->variant() == "List") {
+            if (o->variant() == "Bincode") {
+                r.listed = true;
+                r.list = read_lineage_file(need(*o, "file").text);
+            } else if (o->variant() == "List") {
+                r.listed = true;
                 if (o->items.size() != 1 || o->items[0].kind != Value::List) fail("List([...]) expected");
                 for (const Value &l : o->items[0].items) {
                     necsim_lineage x{};
@@ -383,7 +464,7 @@ Run parse_config(const std::string &text) {
                     r.list.push_back(x);
                 }
             } else if (o->variant() != "Habitat") {
-                fail("sample origin " + o->variant() + " is not supported (Habitat, List)");
+                fail("sample origin " + o->variant() + " is not supported (Habitat, List, Bincode)");
             }
         }
         if (const Value *m = s->field("mode")) {
@@ -401,13 +482,17 @@ Run parse_config(const std::string &text) {
             }
         }
     }
-    if (r.resume != !r.list.empty()) fail("Resume needs a List origin and a List origin needs Resume");
+    if (r.resume != r.listed) fail("Resume needs a List origin and a List origin needs Resume");
     if (const Value *p = root.field("pause")) {
         if (p->variant() == "Pause") {
             r.pause_before = need(*p, "before").as_f64();
             r.pause_config = need(*p, "config").text;
-            if (const Value *d = p->field("destiny"))
-                if (d->variant() != "List") fail("pause destiny " + d->variant() + " is not supported (List)");
+            if (const Value *d = p->field("destiny")) {
+                if (d->variant() == "Bincode")
+                    r.pause_bincode = need(*d, "file").text;
+                else if (d->variant() != "List")
+                    fail("pause destiny " + d->variant() + " is not supported (List, Bincode)");
+            }
             if (const Value *m = p->field("mode")) {
                 if (m->variant() == "Restart")
                     r.pause_restart = true;
@@ -484,7 +569,7 @@ void parse_reporters(const Value &root, Run &r) {
 // (pause.rs:20-61: mode Resume, or Restart(after: the pause time) for the
 // Restart pause mode)
 std::string resume_config(const std::string &text, uint64_t seed, const std::vector<necsim_lineage> &rem,
-                          bool restart, double after) {
+                          bool restart, double after, const std::string &bincode_file) {
     Value root = necsim::ron::parse(text);
     Value sample;
     sample.kind = Value::Struct;
@@ -523,6 +608,17 @@ std::string resume_config(const std::string &text, uint64_t seed, const std::vec
         list.items.push_back(lin);
     }
     origin.items.push_back(list);
+    if (!bincode_file.empty()) {
+        // destiny Bincode(file) (pause.rs:29-39): the lineages go to the file
+        write_lineage_file(bincode_file, rem);
+        origin = Value{};
+        origin.kind = Value::Struct;
+        origin.text = "Bincode";
+        Value file;
+        file.kind = Value::String;
+        file.text = bincode_file;
+        origin.fields.emplace_back("file", file);
+    }
     sample.fields.emplace_back("origin", origin);
     Value mode;
     mode.kind = Value::Ident;
@@ -913,7 +1009,7 @@ int simulate(const std::string &path, bool run) {
     if (out.paused && !r.pause_config.empty()) {
         std::ofstream f(r.pause_config);
         if (!f) fail("cannot write " + r.pause_config);
-        f << resume_config(text, r.seed, rem, r.pause_restart, r.pause_before);
+        f << resume_config(text, r.seed, rem, r.pause_restart, r.pause_before, r.pause_bincode);
         std::printf("necsim-b200: %zu remaining lineages written to %s\n", rem.size(), r.pause_config.c_str());
     }
     return 0;

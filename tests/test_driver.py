@@ -345,3 +345,56 @@ def test_driver_restart_pause_mode(nb, tmp_path):
     assert "(restarted)" in r2.stdout
     straight = nb.simulate(0.01, nb.NonSpatial((30, 20), 2), 42)
     assert species(r.stdout) + species(r2.stdout) == straight.biodiversity
+
+
+def lineage_file(lineages):
+    """Vec<Lineage> in bincode 1.3.3's DefaultOptions (varint integers, f64 as
+    8 little-endian bytes), as lineage_file/saver.rs writes it."""
+    import struct
+
+    def varint(v):
+        if v < 251:
+            return bytes([v])
+        if v < 1 << 16:
+            return b"\xfb" + struct.pack("<H", v)
+        if v < 1 << 32:
+            return b"\xfc" + struct.pack("<I", v)
+        return b"\xfd" + struct.pack("<Q", v)
+    out = varint(len(lineages))
+    for ref, time, x, y, i in lineages:
+        out += varint(ref) + struct.pack("<d", time) + varint(x) + varint(y) + varint(i)
+    return out
+
+
+def test_check_bincode_lineage_file(nb, tmp_path):
+    """Sample origin Bincode(file) (lineage_file/loader.rs) with values in
+    every varint width."""
+    f = tmp_path / "lineages.bin"
+    f.write_bytes(lineage_file([(7, 1.5, 3, 4, 1), (1 << 40, 0.25, 70000, 250, 0), (300, 2.0, 1 << 31, 0, 1)]))
+    sample = 'sample: Sample(percentage: 1.0, origin: Bincode(file: "%s"), mode: Resume),' % f
+    cfg = CONFIG.replace("sample: Sample(percentage: 1.0, origin: Habitat, mode: Genesis),", sample)
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert "3 lineages (resumed)" in r.stdout
+    f.write_bytes(lineage_file([(7, 1.5, 3, 4, 1)])[:-2])
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 1 and "truncated lineage file" in r.stderr
+    f.write_bytes(lineage_file([(7, 1.5, 3, 4, 1)]) + b"\0")
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 1 and "trailing bytes" in r.stderr
+
+
+@pytest.mark.gpu
+def test_driver_pause_to_a_bincode_file(nb, tmp_path):
+    """Pause destiny Bincode(file) (pause.rs:29-39): the remaining lineages go
+    to the file, and the written configuration resumes from it."""
+    resume, lins = tmp_path / "resume.ron", tmp_path / "rest.bin"
+    cfg = CONFIG.replace("pause: None", 'pause: Pause(before: 150.0, config: "%s", destiny: Bincode(file: "%s"))'
+                         % (resume, lins))
+    r = run_driver(nb, "simulate", cfg, tmp_path, "p.ron")
+    assert r.returncode == 0, r.stderr
+    assert lins.exists() and "Bincode" in resume.read_text()
+    r2 = subprocess.run([nb.DRIVER, "simulate", str(resume)], capture_output=True, text=True, timeout=600)
+    assert r2.returncode == 0, r2.stderr
+    straight = nb.simulate(0.01, nb.NonSpatial((30, 20), 2), 42)
+    assert species(r.stdout) + species(r2.stdout) == straight.biodiversity
