@@ -23,11 +23,14 @@
 // Counter, Execution, Csv(output), GlobalSpeciation / GlobalTurnover / GlobalCoverage(output)
 // (others are ignored with a notice); log EventLog(directory,
 // capacity) writes the reference's event log.
+#include <fcntl.h>
 #include <glob.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cctype>
+#include <cerrno>
 #include <charconv>
 #include <chrono>
 #include <cinttypes>
@@ -35,6 +38,7 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <memory>
 #include <random>
 #include <sstream>
 #include <string>
@@ -139,6 +143,7 @@ struct Run {
     bool pause_restart = false;   // pause mode Restart: the written configuration restarts
     bool listed = false;          // the sample origin lists lineages (List or Bincode)
     std::string pause_bincode;    // pause destiny Bincode(file): the remaining lineages' file
+    std::shared_ptr<struct LineageFileSaver> pause_saver;  // that file, created when the config is read
     std::string pause_config;
     std::string algorithm = "Independent";
     bool rep_biodiversity = false, rep_counter = false, rep_execution = false;
@@ -412,33 +417,65 @@ std::vector<necsim_lineage> read_lineage_file(const std::string &path) {
         if (at + 8 > in.size()) fail(path + ": truncated lineage file");
         std::memcpy(&l.last_event_time, in.data() + at, 8);
         at += 8;
+        // Lineage::last_event_time is a NonNegativeF64 (lineage.rs:91-106)
+        if (!(l.last_event_time >= 0.0)) fail(path + ": a lineage's last event time is negative or NaN");
         const uint64_t x = get_varint(in, at, path), y = get_varint(in, at, path), i = get_varint(in, at, path);
         if ((x | y | i) > 0xffffffffULL) fail(path + ": malformed lineage file");
         l.x = (uint32_t)x;
         l.y = (uint32_t)y;
         l.index = (uint32_t)i;
     }
-    if (at != in.size()) fail(path + ": trailing bytes in the lineage file");
+    // bytes after the list are not read, as bincode::Deserializer::with_reader
+    // does not (lineage_file/loader.rs:37-44)
     return out;
 }
 
-void write_lineage_file(const std::string &path, const std::vector<necsim_lineage> &lins) {
-    std::string o;
-    put_varint(o, lins.size());
-    for (const auto &l : lins) {
-        put_varint(o, l.global_reference);
-        char t[8];
-        std::memcpy(t, &l.last_event_time, 8);
-        o.append(t, 8);
-        put_varint(o, l.x);
-        put_varint(o, l.y);
-        put_varint(o, l.index);
+// LineageFileSaver (necsim/impls/std/src/lineage_file/saver.rs): the file is
+// created exclusively when the configuration is read, so an existing file
+// fails the run before it simulates, and it is removed again unless the
+// lineages are written to it.
+struct LineageFileSaver {
+    std::string path;
+    int fd = -1;
+    bool temp = true;
+
+    explicit LineageFileSaver(const std::string &p) : path(p) {
+        fd = ::open(p.c_str(), O_WRONLY | O_CREAT | O_EXCL, 0644);
+        if (fd < 0) fail("cannot create the lineage file " + p + ": " + std::strerror(errno));
     }
-    std::ofstream f(path, std::ios::binary | std::ios::trunc);
-    if (!f || !f.write(o.data(), (std::streamsize)o.size())) fail("cannot write the lineage file " + path);
-}
+    LineageFileSaver(const LineageFileSaver &) = delete;
+    LineageFileSaver &operator=(const LineageFileSaver &) = delete;
+    ~LineageFileSaver() {
+        if (fd >= 0) ::close(fd);
+        if (temp) ::unlink(path.c_str());
+    }
+
+    // bincode 1.3.3 DefaultOptions: a varint length, then per lineage the
+    // varint global reference, the f64 time as 8 bytes and the varint location
+    void write(const std::vector<necsim_lineage> &lins) {
+        std::string o;
+        put_varint(o, lins.size());
+        for (const auto &l : lins) {
+            put_varint(o, l.global_reference);
+            char t[8];
+            std::memcpy(t, &l.last_event_time, 8);
+            o.append(t, 8);
+            put_varint(o, l.x);
+            put_varint(o, l.y);
+            put_varint(o, l.index);
+        }
+        size_t done = 0;
+        while (done < o.size()) {
+            const ssize_t w = ::write(fd, o.data() + done, o.size() - done);
+            if (w <= 0) fail("cannot write the lineage file " + path);
+            done += (size_t)w;
+        }
+        temp = false;
+    }
+};
 
 void parse_reporters(const Value &root, Run &r);
+std::string rust_f64_display(double v);
 
 Run parse_config(const std::string &text) {
     Run r;
@@ -457,6 +494,8 @@ Run parse_config(const std::string &text) {
                     necsim_lineage x{};
                     x.global_reference = need(l, "ref").as_u64();
                     x.last_event_time = need(l, "time").as_f64();
+                    if (!(x.last_event_time >= 0.0))
+                        fail("a listed lineage's time is negative or NaN (NonNegativeF64)");
                     const Value &loc = need(l, "loc");
                     x.x = as_u32(need(loc, "x"), "x");
                     x.y = as_u32(need(loc, "y"), "y");
@@ -483,13 +522,25 @@ Run parse_config(const std::string &text) {
         }
     }
     if (r.resume != r.listed) fail("Resume needs a List origin and a List origin needs Resume");
+    if (r.restart) {
+        // args/config/sample/mod.rs:118-137: every listed lineage lies before
+        // the resume point PositiveF64::max_after(after, after)
+        const double bound = std::isinf(r.restart_after) ? r.restart_after
+                                                          : std::nextafter(r.restart_after, HUGE_VAL);
+        for (const necsim_lineage &l : r.list)
+            if (l.last_event_time >= bound)
+                fail("Lineage #" + std::to_string(l.global_reference) + " at time " +
+                     rust_f64_display(l.last_event_time) + " is not before the resume point");
+    }
     if (const Value *p = root.field("pause")) {
         if (p->variant() == "Pause") {
             r.pause_before = need(*p, "before").as_f64();
             r.pause_config = need(*p, "config").text;
             if (const Value *d = p->field("destiny")) {
-                if (d->variant() == "Bincode")
+                if (d->variant() == "Bincode") {
                     r.pause_bincode = need(*d, "file").text;
+                    r.pause_saver = std::make_shared<LineageFileSaver>(r.pause_bincode);
+                }
                 else if (d->variant() != "List")
                     fail("pause destiny " + d->variant() + " is not supported (List, Bincode)");
             }
@@ -569,7 +620,7 @@ void parse_reporters(const Value &root, Run &r) {
 // (pause.rs:20-61: mode Resume, or Restart(after: the pause time) for the
 // Restart pause mode)
 std::string resume_config(const std::string &text, uint64_t seed, const std::vector<necsim_lineage> &rem,
-                          bool restart, double after, const std::string &bincode_file) {
+                          bool restart, double after, const std::string &bincode_file, LineageFileSaver *saver) {
     Value root = necsim::ron::parse(text);
     Value sample;
     sample.kind = Value::Struct;
@@ -610,7 +661,9 @@ std::string resume_config(const std::string &text, uint64_t seed, const std::vec
     origin.items.push_back(list);
     if (!bincode_file.empty()) {
         // destiny Bincode(file) (pause.rs:29-39): the lineages go to the file
-        write_lineage_file(bincode_file, rem);
+        // created when the configuration was read
+        if (!saver) fail("no lineage file was created for " + bincode_file);
+        saver->write(rem);
         origin = Value{};
         origin.kind = Value::Struct;
         origin.text = "Bincode";
@@ -1009,7 +1062,7 @@ int simulate(const std::string &path, bool run) {
     if (out.paused && !r.pause_config.empty()) {
         std::ofstream f(r.pause_config);
         if (!f) fail("cannot write " + r.pause_config);
-        f << resume_config(text, r.seed, rem, r.pause_restart, r.pause_before, r.pause_bincode);
+        f << resume_config(text, r.seed, rem, r.pause_restart, r.pause_before, r.pause_bincode, r.pause_saver.get());
         std::printf("necsim-b200: %zu remaining lineages written to %s\n", rem.size(), r.pause_config.c_str());
     }
     return 0;

@@ -327,6 +327,45 @@ def test_check_restart_sample_mode(nb, tmp_path):
     assert r.returncode == 1 and "Restart(after)" in r.stderr
     r = run_driver(nb, "check", cfg.replace("mode: Restart(after: 150.0)", "mode: FixUp()"), tmp_path)
     assert r.returncode == 1 and "not supported (Genesis, Resume, Restart)" in r.stderr
+    # every listed lineage must lie before the resume point max_after(after, after),
+    # the next double above `after` (args/config/sample/mod.rs:118-137): a
+    # lineage at `after` itself restarts, one a double later does not
+    r = run_driver(nb, "check", cfg.replace("after: 150.0", "after: 1.5"), tmp_path)
+    assert r.returncode == 0, r.stderr
+    r = run_driver(nb, "check", cfg.replace("after: 150.0", "after: 1.4999999999999998"), tmp_path)
+    assert r.returncode == 1 and "Lineage #7 at time 1.5 is not before the resume point" in r.stderr
+
+
+def test_check_rejects_negative_lineage_times(nb, tmp_path):
+    """Lineage::last_event_time is a NonNegativeF64: a negative or NaN time
+    does not load, from a List or from a lineage file."""
+    cfg = CONFIG.replace("sample: Sample(percentage: 1.0, origin: Habitat, mode: Genesis),",
+                         RESTART_SAMPLE.replace("time: 0.25", "time: -0.25"))
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 1 and "negative or NaN" in r.stderr
+    f = tmp_path / "neg.bin"
+    sample = 'sample: Sample(percentage: 1.0, origin: Bincode(file: "%s"), mode: Resume),' % f
+    cfg = CONFIG.replace("sample: Sample(percentage: 1.0, origin: Habitat, mode: Genesis),", sample)
+    for bad in (-1.0, float("nan")):
+        f.write_bytes(lineage_file([(7, 1.5, 3, 4, 1), (8, bad, 3, 4, 0)]))
+        r = run_driver(nb, "check", cfg, tmp_path)
+        assert r.returncode == 1 and "negative or NaN" in r.stderr
+
+
+def test_check_bincode_destiny_must_not_exist(nb, tmp_path):
+    """LineageFileSaver::try_new opens the destiny with create_new when the
+    configuration is read: an existing file fails before anything runs, and a
+    file the run created but never wrote is removed again."""
+    lins = tmp_path / "rest.bin"
+    cfg = CONFIG.replace("pause: None", 'pause: Pause(before: 150.0, config: "%s", destiny: Bincode(file: "%s"))'
+                         % (tmp_path / "resume.ron", lins))
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 0, r.stderr
+    assert not lins.exists()
+    lins.write_bytes(b"keep")
+    r = run_driver(nb, "check", cfg, tmp_path)
+    assert r.returncode == 1 and "cannot create the lineage file" in r.stderr
+    assert lins.read_bytes() == b"keep"
 
 
 @pytest.mark.gpu
@@ -379,9 +418,10 @@ def test_check_bincode_lineage_file(nb, tmp_path):
     f.write_bytes(lineage_file([(7, 1.5, 3, 4, 1)])[:-2])
     r = run_driver(nb, "check", cfg, tmp_path)
     assert r.returncode == 1 and "truncated lineage file" in r.stderr
+    # bytes after the list are not read (bincode::Deserializer::with_reader)
     f.write_bytes(lineage_file([(7, 1.5, 3, 4, 1)]) + b"\0")
     r = run_driver(nb, "check", cfg, tmp_path)
-    assert r.returncode == 1 and "trailing bytes" in r.stderr
+    assert r.returncode == 0 and "1 lineages (resumed)" in r.stdout, r.stderr
 
 
 @pytest.mark.gpu
