@@ -16,10 +16,18 @@ to completion in one batched launch per round.  One step = one full batch.
   e2e        the same metric through the public C ABI call
              necsim_gpu_simulate_batch with host buffers: scenario set-up,
              host->device origin upload, simulation, device->host events
-  roofline   the step kernel's algorithmic bytes per launch / its average
-             launch time, against the measured HBM copy bandwidth
+  roofline   the round kernels (cooperative + step kernel) against their
+             integer-issue bound: algorithmic wymum work per event on the
+             canonical schedule (counted by the oracle) x events / kernel
+             time, over the measured hash-issue peak; hbm_roofline gives
+             their algorithmic bytes against the measured HBM bandwidth
   cpu_baseline  the CPU restatement of the reference's Independent
-             algorithm on a bounded sample of the same workload
+             algorithm on a bounded sample of the same workload (all
+             simulations to t = 400), with the host CPU model
+  same_slice the GPU's rate on exactly that sample (like for like with the
+             CPU baseline and the reference arm)
+  secondary  C3 in full and C5 to t = 400: the plain kernel's device rate
+             beside the CPU restatement on the same horizon
 
 `--impl reference` times that CPU restatement alone (all host cores) and
 prints its line.  Multi-GPU (`--gpus N` under torchrun) runs N independent
@@ -62,6 +70,8 @@ def parse():
                    help="pause_before of the trace runs that train the lifetime model")
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-secondary", action="store_true",
+                   help="skip the secondary workloads (C3 in full, C5 to t=400) beside the sweep")
     p.add_argument("--pause", type=float, default=None,
                    help="pause_before of every simulation (default: run to completion)")
     p.add_argument("--event-time-sampler", default="poisson", choices=["poisson", "exp"],
@@ -161,12 +171,13 @@ class Clocks:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_rank%d.csv" % gpu_index)
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix="necsim_clocks_%d_" % self.gpu, suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.QUERY,
                  "--format=csv,noheader,nounits", "-lms", "200"],
@@ -183,9 +194,15 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.f.close()
+        with open(self.path) as f:
+            lines = f.readlines()
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -313,31 +330,97 @@ def train_lifetime_model(nb, syn, device, pause):
     return model, info
 
 
-def issue_roofline(nb, sims, args, device, counts, events, kernel_ms):
-    """The step kernel against its integer-issue bound: algorithmic WyHash
-    mixing work (wymum, the 64x64 -> 128-bit multiply-fold) per event, from
-    the reference restatement's prime and draw counts on a sample of the
-    workload (a prime costs 2 wymum, a draw 1), times the events, over the
-    step kernel's CUDA-event time, against the measured rate of independent
-    wymum chains on this GPU."""
+def canonical_work(sims, algo, pause, threads, sampler):
+    """WyHash primes and draws per event of the canonical schedule -- the one
+    the kernels execute -- counted by the oracle on every k-th simulation of
+    the workload (at most 32) up to time `pause`, with the run's step_slice."""
+    import oracle
+    code = oracle.SAMPLER_EXP if sampler == "exp" else oracle.SAMPLER_POISSON
+    pick = sims[:: max(1, len(sims) // 32)]
+
+    def one(item):
+        d, seed = item
+        o = oracle.simulate(d, seed, mode=oracle.MODE_CANONICAL, pause_before=pause, event_time_sampler=code,
+                            step_slice=algo.step_slice, min_round_events=algo.min_round_events,
+                            step_slice_max=algo.step_slice_max)
+        return o.steps, o.n_primes, o.n_draws
+
+    oracle.lib()
+    with concurrent.futures.ThreadPoolExecutor(max_workers=threads) as ex:
+        res = list(ex.map(one, pick))
+    return {"steps": sum(r[0] for r in res), "primes": sum(r[1] for r in res), "draws": sum(r[2] for r in res),
+            "sample": "%d of %d simulation(s) to t=%g" % (len(pick), len(sims), pause)}
+
+
+# DRAM bytes (read + write) per executed event of the round kernels, from the
+# ncu capture summarised in profiles/ (dram__bytes_read.sum +
+# dram__bytes_write.sum over every launch of the capture / its events)
+DRAM_BYTES_PER_EVENT = {}
+
+
+def issue_roofline(nb, device, work, events, kernel_ms, launches, workload_name):
+    """The round kernels (the cooperative kernel and the step kernel, timed
+    together by CUDA events around each round's launches) against their
+    integer-issue bound: algorithmic WyHash mixing work per event -- wymum,
+    the 64x64 -> 128-bit multiply-fold; a prime costs 2, a draw 1 -- on the
+    canonical schedule, times the events, over the kernels' time, against
+    the measured rate of independent wymum chains on this GPU."""
+    per_event = (2.0 * work["primes"] + work["draws"]) / max(work["steps"], 1)
+    achieved = per_event * events / (kernel_ms / 1e3) if kernel_ms > 0 else 0.0
+    peak = nb.hash_peak(device)
+    bpe = DRAM_BYTES_PER_EVENT.get(workload_name)
+    return {"bound": "integer-issue", "achieved": achieved, "peak": peak, "unit": "wymum/s",
+            "frac": achieved / peak,
+            "traffic": (bpe * events / max(launches, 1)) if bpe else None,
+            "traffic_unit": "DRAM bytes per launch (ncu per-event figure x events per launch)",
+            "kernel": "coop_kernel + step_kernel", "avg_launch_ms": kernel_ms / max(launches, 1),
+            "launches": launches, "wymum_per_event": per_event,
+            "primes_per_event": work["primes"] / max(work["steps"], 1),
+            "draws_per_event": work["draws"] / max(work["steps"], 1),
+            "peak_source": "measured: 8 independent wymum chains per thread on every SM "
+                           "(necsim_gpu_hash_peak)",
+            "work_source": "canonical-schedule oracle, " + work["sample"]}
+
+
+def host_cpu_model():
     try:
-        if not counts:
-            # no CPU leg: the ratios from a small sample of the same workload
-            cpu_sample(sims[:: max(1, len(sims) // 4)][:4], 50.0, 4, args.event_time_sampler, counts)
-        per_event = (2.0 * counts["primes"] + counts["draws"]) / max(counts["steps"], 1)
-        achieved = per_event * events / (kernel_ms / 1e3) if kernel_ms > 0 else 0.0
-        peak = nb.hash_peak(device)
-        return {"bound": "integer-issue", "achieved": achieved, "peak": peak, "unit": "wymum/s",
-                "frac": achieved / peak, "kernel": "step_kernel",
-                "wymum_per_event": per_event,
-                "primes_per_event": counts["primes"] / max(counts["steps"], 1),
-                "draws_per_event": counts["draws"] / max(counts["steps"], 1),
-                "peak_source": "measured: 8 independent wymum chains per thread on every SM "
-                               "(necsim_gpu_hash_peak)",
-                "work_source": "reference-schedule restatement on the CPU sample (%d events)"
-                               % counts["steps"]}
-    except Exception as e:  # reported, never fatal to the benchmark line
-        return {"error": "%s: %s" % (type(e).__name__, e)}
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def secondary(nb, name, pause, device, threads, sampler, note):
+    """One secondary workload: the plain kernel's device time on the GPU
+    (one warm-up run, one timed) beside the CPU restatement of the reference
+    on the same horizon, `threads` at a time."""
+    desc, sims = workload(name)
+    syn = importlib.import_module("necsim-rust_b200.synthetic")
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    algo = nb.CUDA(device=device, event_time_sampler=sampler)
+    with nb.Batch(scen, [d["speciation_probability"] for d, _ in sims], [s for _, s in sims], algo,
+                  pause_before=pause) as batch:
+        batch.run()
+        outs = batch.run()
+    ev = sum(o.steps for o in outs)
+    ms = outs[0].total_ms
+    cev, csec = cpu_sample(sims, pause, threads, sampler)
+    # the oracle builds its alias tables inside every run (the GPU time above
+    # excludes the library's build): time one build alone and take it out
+    import oracle
+    t0 = time.perf_counter()
+    oracle.build_alias(sims[0][0])
+    build = time.perf_counter() - t0
+    csec = max(csec - build, 1e-9)
+    return {"workload": desc, "pause_before": pause, "value": ev / (ms / 1e3), "unit": UNIT,
+            "ms": ms, "events": ev, "species": int(sum(o.biodiversity for o in outs)),
+            "cpu_baseline": {"value": cev / csec, "unit": UNIT, "cores": threads, "kind": "port",
+                             "seconds": csec, "table_build_seconds_excluded": build, "events": cev,
+                             "cpu_model": host_cpu_model(),
+                             "sample": cpu_sample_desc(name, pause, len(sims), threads) + note}}
 
 
 def time_arm(nb, scen, nus, seeds, algo, args, dist):
@@ -420,25 +503,17 @@ def main():
     steps, visits, n_spec = head["steps"], head["visits"], head["n_spec"]
     outs = head["outs"]
 
-    # roofline of the step kernel: algorithmic bytes = lineage state read and
-    # written per visit (4 u32 + 5 u64/f64 + 1 flag, 57 B each way), speciation
-    # events written (40 B) and, for SpatiallyExplicit, one 32-B cell record
-    # and one 32-B atom sector per event
+    # the round kernels against HBM (a secondary view: they are issue- and
+    # latency-bound): algorithmic bytes = lineage state read and written per
+    # visit (4 u32 + 5 u64/f64 + 1 flag, 57 B each way), speciation events
+    # written (40 B) and, for SpatiallyExplicit, one 32-B cell record and one
+    # 32-B atom sector per event
     state_bytes = 2 * 57
     alg_bytes = visits * state_bytes + n_spec * 40 + (steps * 64 if se else 0)
     avg_launch_ms = head["kernel_ms"] / max(head["step_launches"], 1)
     per_launch_bytes = alg_bytes / max(head["step_launches"], 1)
     achieved = per_launch_bytes / (avg_launch_ms / 1e3) / 1e9 if avg_launch_ms > 0 else 0.0
     peak, peak_kind = load_peaks()
-    traffic = None
-    prof = os.path.join(ROOT, "profiles", "step_kernel_%s_traffic.json" % args.workload)
-    if os.path.exists(prof):
-        try:
-            with open(prof) as f:
-                t = json.load(f)
-            traffic = t["dram_bytes_per_lineage_visit"] * visits / max(head["step_launches"], 1)
-        except Exception:
-            traffic = None
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world,
@@ -456,12 +531,12 @@ def main():
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                 "d2h_bytes_per_step": d2h / args.steps},
         "gpu_launches": head["launches"],
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
-                     "kernel": "step_kernel", "avg_launch_ms": avg_launch_ms,
-                     "launches": head["step_launches"],
-                     "step_kernel_ms_per_step": head["kernel_ms"] / args.steps},
+        "hbm_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
+                         "kernel": "coop_kernel + step_kernel", "avg_launch_ms": avg_launch_ms,
+                         "launches": head["step_launches"],
+                         "round_kernels_ms_per_step": head["kernel_ms"] / args.steps},
         # the per-simulation resident kernel runs the small simulations' rounds
         # on a second stream: a latency-bound chain of dependent 64-bit hash
         # multiplies per lineage, not a bandwidth roofline
@@ -482,14 +557,34 @@ def main():
         line["model"] = model_info
     if tune_info is not None:
         line["autotune"] = tune_info
-    counts = {}
+    threads = os.cpu_count() or 1
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler, counts)
+        ev, sec = cpu_sample(sims, args.cpu_sample_pause, threads, args.event_time_sampler)
         line["cpu_baseline"] = {"value": ev / sec, "unit": UNIT, "cores": threads, "kind": "port",
+                                "cpu_model": host_cpu_model(),
                                 "sample": cpu_sample_desc(args.workload, args.cpu_sample_pause,
                                                           len(sims), threads)}
-    line["issue_roofline"] = issue_roofline(nb, sims, args, device, counts, steps, head["kernel_ms"])
+    # the same slice the CPU baseline and the reference arm time: every
+    # simulation advanced to t = cpu_sample_pause, on the GPU (device time)
+    if dist.world == 1 and args.pause is None:
+        with nb.Batch(scen, nus, seeds, plain_algo, pause_before=args.cpu_sample_pause) as b:
+            b.run()
+            so = b.run()
+        line["same_slice"] = {"value": sum(o.steps for o in so) / (so[0].total_ms / 1e3), "unit": UNIT,
+                              "pause_before": args.cpu_sample_pause, "events": sum(o.steps for o in so),
+                              "ms": so[0].total_ms, "schedule": "plain"}
+    try:
+        work = canonical_work(sims, plain_algo, args.cpu_sample_pause, threads, args.event_time_sampler)
+        line["roofline"] = issue_roofline(nb, device, work, steps, head["kernel_ms"], head["step_launches"],
+                                          args.workload)
+    except Exception as e:  # reported, never fatal to the benchmark line
+        line["roofline"] = {"error": "%s: %s" % (type(e).__name__, e)}
+    if dist.rank == 0 and dist.world == 1 and args.workload == "c4" and not args.no_secondary:
+        line["secondary"] = {
+            "c3": secondary(nb, "c3", None, device, threads, args.event_time_sampler, ""),
+            # one thread: every oracle partition would build its own 5 GB alias table
+            "c5_t400": secondary(nb, "c5", 400.0, device, 1, args.event_time_sampler, ""),
+        }
     if model is not None:
         model.close()
     if dist.rank == 0:

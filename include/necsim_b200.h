@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define NECSIM_B200_ABI_VERSION 1
+#define NECSIM_B200_ABI_VERSION 2
 
 /* ---- error codes ---- */
 #define NECSIM_OK 0
@@ -87,6 +87,16 @@ typedef struct necsim_scenario {
     uint64_t octaves;                /* >= 1 */
     uint32_t sample_x, sample_y;     /* Rectangle sample: LandscapeExtent origin */
     uint64_t sample_width, sample_height; /* 1 ..= 2^32 (OffByOneU32) */
+    /* SpatiallyExplicit: device tables built before (necsim_build_tables), used instead of
+       building them from `dispersal` (which may then be NULL; the learned model's dispersal
+       entropy feature is 0 without it): width*height cell records and n_atoms alias atoms,
+       read during the call only.  The host does not check the ranges they hold: the kernels
+       bound-check every cell and atom index before reading it, and a record or atom that
+       points outside the tables fails the run with NECSIM_E_DEVICE_CHECK.  NULL: build
+       the tables from the maps. */
+    const struct necsim_cell_record *cells;
+    const struct necsim_alias_atom *atoms;
+    uint64_t n_atoms;
 } necsim_scenario;
 
 /* necsim_args.event_time_sampler: which EventTimeSampler
@@ -130,6 +140,10 @@ typedef struct necsim_args {
                                     per event with a correctly rounded f64 ln */
     struct necsim_model *model; /* schedule == 1: the lifetime model ordering the step queue
                                    (must stay alive during the call; same device) */
+    uint64_t max_rounds;       /* watchdog: a run that needs more rounds fails with
+                                  NECSIM_E_TIMEOUT; 0 = default 2^26.  Every round advances each
+                                  live lineage by >= step_slice expected events, so a valid run
+                                  only meets a limit chosen below its round count */
 } necsim_args;
 
 /* ---- events and lineages (reference layouts) ---- */
@@ -275,13 +289,17 @@ void necsim_gpu_batch_destroy(necsim_batch *batch);
  * NECSIM_NOALLOC_MAX_LINEAGES (NECSIM_E_TOO_LARGE otherwise).  Scenario
  * kinds without tables only (NonSpatial, SpatiallyImplicit, AlmostInfinite);
  * SpatiallyExplicit returns NECSIM_E_UNSUPPORTED.  resume_time is the
- * min_event_time of the lineages.  Surviving lineages and speciation events
- * are written in no particular order; *n_out, *n_events and *steps (events
- * executed) are set on return.  Work is queued on `stream` (a cudaStream_t,
- * NULL = default stream) and the call waits for it.
+ * min_event_time of the lineages.  `args` (NULL: defaults) selects the
+ * event-time sampler (event_time_sampler; other values are
+ * NECSIM_E_INVALID_ARGUMENT) and delta_t; the launch shape follows the
+ * device's SM count.  Surviving lineages and speciation events are written
+ * in no particular order; *n_out, *n_events and *steps (events executed)
+ * are set on return.  Work is queued on `stream` (a cudaStream_t, NULL =
+ * default stream) and the call waits for it.
  *
  * The first call on a device looks up the device address of the working
- * area; make that first call before capturing any stream into a CUDA graph.
+ * area and the device's SM count; make that first call before capturing any
+ * stream into a CUDA graph.
  * Every call shares the one working area and clears it before use, so calls
  * whose GPU work overlaps (other streams or host threads) race. */
 #define NECSIM_NOALLOC_MAX_LINEAGES 65536
@@ -424,6 +442,19 @@ int necsim_event_log_replay(const char *const *segments, uint64_t n_segments, ui
  * wyhash.rs:85-96) over independent chains filling every SM.  No reference
  * counterpart: the denominator of the benchmark's integer-issue roofline. */
 int necsim_gpu_hash_peak(int32_t device, double *wymum_per_second);
+
+/* The AlmostInfinite dispersal displacements (dx, dy), before
+ * clamp_round_dispersal (habitat/almost_infinite.rs:100-114) rounds them onto
+ * the plane, that the kernels compute for n pairs of WyHash samples
+ * (draws[2j], draws[2j + 1]): Normal (kind NECSIM_ALMOST_INFINITE_NORMAL, a =
+ * sigma; Box-Muller of rng.rs:180-197 scaled as almost_infinite_normal.rs:58-68)
+ * or Clark2Dt (NECSIM_ALMOST_INFINITE_CLARK2DT, a = shape u, b = tail p;
+ * almost_infinite_clark2dt.rs:96-107).  The device evaluates ln/sin/cos/pow
+ * with CUDA's f64 library where the reference calls the system libm; this
+ * entry point lets a caller measure where the two disagree.  No reference
+ * counterpart. */
+int necsim_gpu_displacements(int32_t device, int32_t kind, const uint64_t *draws, uint64_t n, double a, double b,
+                             double *dx, double *dy);
 
 /* ---- launch autotuner ----
  * Times a bounded sample of a batch -- every k-th simulation so that the

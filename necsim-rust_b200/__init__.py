@@ -63,6 +63,7 @@ class CScenario(ctypes.Structure):
         ("octaves", ctypes.c_uint64),
         ("sample_x", ctypes.c_uint32), ("sample_y", ctypes.c_uint32),
         ("sample_width", ctypes.c_uint64), ("sample_height", ctypes.c_uint64),
+        ("cells", ctypes.c_void_p), ("atoms", ctypes.c_void_p), ("n_atoms", ctypes.c_uint64),
     ]
 
 
@@ -75,7 +76,7 @@ class CArgs(ctypes.Structure):
         ("schedule", ctypes.c_uint32), ("report_dispersal", ctypes.c_int32),
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
         ("resident", ctypes.c_uint32), ("event_time_sampler", ctypes.c_uint32),
-        ("model", ctypes.c_void_p),
+        ("model", ctypes.c_void_p), ("max_rounds", ctypes.c_uint64),
     ]
 
 
@@ -128,7 +129,7 @@ SYMBOLS = [
     "necsim_model_gradients", "necsim_model_train", "necsim_gpu_trace_batch",
     "necsim_presample_origins", "necsim_gpu_autotune", "necsim_event_log_create",
     "necsim_event_log_reporter", "necsim_event_log_close", "necsim_event_log_replay", "necsim_map_load",
-    "necsim_map_free", "necsim_maps_fix", "necsim_gpu_hash_peak",
+    "necsim_map_free", "necsim_maps_fix", "necsim_gpu_hash_peak", "necsim_gpu_displacements",
 ]
 
 _lib = None
@@ -207,6 +208,9 @@ def lib():
     L.necsim_event_log_replay.restype = ctypes.c_int
     L.necsim_gpu_hash_peak.argtypes = [ctypes.c_int32, P(ctypes.c_double)]
     L.necsim_gpu_hash_peak.restype = ctypes.c_int
+    L.necsim_gpu_displacements.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
+    L.necsim_gpu_displacements.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
     L.necsim_model_create.restype = ctypes.c_int
     L.necsim_model_destroy.argtypes = [vp]
@@ -228,7 +232,7 @@ def lib():
                                          ctypes.c_uint32, u64, fp, fp, P(u64), ctypes.c_char_p,
                                          ctypes.c_size_t]
     L.necsim_gpu_trace_batch.restype = ctypes.c_int
-    if L.necsim_abi_version() != 1:
+    if L.necsim_abi_version() != 2:
         raise ImportError("libnecsim_b200.so ABI version mismatch")
     _lib = L
     return L
@@ -291,8 +295,11 @@ class SpatiallyExplicit:
     (spatially_explicit/turnover/uniform.rs) or an f64 [h, w] turnover map
     (turnover/map.rs: every habitable cell's rate > 0)."""
     habitat: np.ndarray
-    dispersal: np.ndarray
+    dispersal: Optional[np.ndarray]
     turnover: Union[float, np.ndarray] = 0.5
+    # device tables built before (build_tables: CELL_DTYPE records, ATOM_DTYPE
+    # atoms), used instead of building them from `dispersal` (then optional)
+    tables: Optional[Tuple[np.ndarray, np.ndarray]] = None
 
 
 @dataclass
@@ -409,6 +416,9 @@ class CUDA:
     # (event_time_sampler/poisson.rs); "exp": ExpEventTimeSampler, the CUDA
     # algorithm's (event_time_sampler/exp.rs), -ln(U(0,1]) / lambda per event
     event_time_sampler: str = "poisson"
+    # watchdog: a run still active after this many rounds fails with
+    # NECSIM_E_TIMEOUT (checked between graph launches); 0: 2^26
+    max_rounds: int = 0
 
 
 Independent = CUDA
@@ -509,13 +519,28 @@ def _scenario_struct(scenario, speciation: float):
     elif isinstance(scenario, SpatiallyExplicit):
         c.kind = SPATIALLY_EXPLICIT
         h = np.ascontiguousarray(scenario.habitat, dtype=np.uint32)
-        d = np.ascontiguousarray(scenario.dispersal, dtype=np.float64)
-        if h.ndim != 2 or d.shape != (h.size, h.size):
-            raise ValueError("habitat must be [h, w] and dispersal [h*w, h*w]")
+        if h.ndim != 2:
+            raise ValueError("habitat must be [h, w]")
         c.height, c.width = h.shape
         c.habitat = h.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
-        c.dispersal = d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        keep += [h, d]
+        keep.append(h)
+        if scenario.dispersal is not None:
+            d = np.ascontiguousarray(scenario.dispersal, dtype=np.float64)
+            if d.shape != (h.size, h.size):
+                raise ValueError("dispersal must be [h*w, h*w]")
+            c.dispersal = d.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+            keep.append(d)
+        if scenario.tables is not None:
+            cells = np.ascontiguousarray(scenario.tables[0], dtype=CELL_DTYPE)
+            atoms = np.ascontiguousarray(scenario.tables[1], dtype=ATOM_DTYPE)
+            if cells.shape != (h.size,):
+                raise ValueError("tables need one cell record per habitat cell")
+            c.cells = cells.ctypes.data
+            c.atoms = atoms.ctypes.data if atoms.size else None
+            c.n_atoms = atoms.size
+            keep += [cells, atoms]
+        elif scenario.dispersal is None:
+            raise ValueError("SpatiallyExplicit needs a dispersal map or tables")
         if np.ndim(scenario.turnover) == 0:
             c.turnover_rate = float(scenario.turnover)
         else:  # a turnover map (spatially_explicit/turnover/map.rs)
@@ -553,6 +578,7 @@ def _args_struct(algorithm: CUDA):
     if algorithm.event_time_sampler not in EVENT_TIME_SAMPLERS:
         raise ValueError("event_time_sampler must be 'poisson' or 'exp'")
     a.event_time_sampler = EVENT_TIME_SAMPLERS[algorithm.event_time_sampler]
+    a.max_rounds = algorithm.max_rounds
     return a
 
 
@@ -1024,6 +1050,26 @@ def hash_peak(device: int = 0) -> float:
     if rc != 0:
         raise NecsimError(rc, "hash peak measurement failed")
     return v.value
+
+
+def displacements(draws: np.ndarray, dispersal, device: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """The AlmostInfinite displacements (dx, dy) before rounding that the
+    kernels compute from sample pairs draws[:, 0], draws[:, 1] (u64) for a
+    Normal or Clark2Dt dispersal."""
+    d = np.ascontiguousarray(draws, dtype=np.uint64)
+    if d.ndim != 2 or d.shape[1] != 2:
+        raise ValueError("draws must be [n, 2]")
+    n = d.shape[0]
+    dx = np.empty(n, dtype=np.float64)
+    dy = np.empty(n, dtype=np.float64)
+    if isinstance(dispersal, Clark2Dt):
+        kind, a, b = ALMOST_INFINITE_CLARK2DT, dispersal.shape_u, dispersal.tail_p
+    else:
+        kind, a, b = ALMOST_INFINITE_NORMAL, dispersal.sigma, 0.0
+    rc = lib().necsim_gpu_displacements(device, kind, d.ctypes.data, n, a, b, dx.ctypes.data, dy.ctypes.data)
+    if rc != 0:
+        raise NecsimError(rc, "displacement evaluation failed")
+    return dx, dy
 
 
 @dataclass

@@ -372,40 +372,52 @@ __device__ __forceinline__ void clamp_round_dispersal(uint32_t x, uint32_t y, do
 
 // almost_infinite_clark2dt.rs:96-107 with clark2dt::cdf_inverse and
 // pow_fast_one (:167-189) from samples 2 (u01, [0, 1)) and 3 (angle, (0, 1]):
-// jump = sqrt(u * (pow(1 / (1 - u01), 1 / p) - 1)), theta = u2 * 2 * pi.  The
-// transcendental calls are CUDA's f64 pow/cos/sin; their results only pass
-// through round(), like the Normal sampler's.
-__device__ __forceinline__ void clark2dt_dispersal_draw(uint64_t d0, uint64_t d1, double shape_u,
-                                                        double exponent, uint32_t x, uint32_t y, uint32_t &tx,
-                                                        uint32_t &ty) {
+// jump = sqrt(u * (pow(1 / (1 - u01), 1 / p) - 1)), theta = u2 * 2 * pi,
+// displacement (cos(theta) * jump, sin(theta) * jump).  The transcendental
+// calls are CUDA's f64 pow/cos/sin; their results only pass through
+// round(), like the Normal sampler's.
+__device__ __forceinline__ void clark2dt_displacement(uint64_t d0, uint64_t d1, double shape_u, double exponent,
+                                                      double &dx, double &dy) {
     const double u01 = unit_closed_open(d0);
     const double u2 = unit_open_closed(d1);
     const double base = __ddiv_rn(1.0, __dsub_rn(1.0, u01));
     const double powed = exponent == 1.0 ? base : pow(base, exponent);
     const double jump = __dsqrt_rn(__dmul_rn(shape_u, __dsub_rn(powed, 1.0)));
     const double theta = __dmul_rn(__dmul_rn(u2, 2.0), 3.141592653589793);
-    const double dx = __dmul_rn(cos(theta), jump);
-    const double dy = __dmul_rn(sin(theta), jump);
+    dx = __dmul_rn(cos(theta), jump);
+    dy = __dmul_rn(sin(theta), jump);
+}
+
+__device__ __forceinline__ void clark2dt_dispersal_draw(uint64_t d0, uint64_t d1, double shape_u,
+                                                        double exponent, uint32_t x, uint32_t y, uint32_t &tx,
+                                                        uint32_t &ty) {
+    double dx, dy;
+    clark2dt_displacement(d0, d1, shape_u, exponent, dx, dy);
     clamp_round_dispersal(x, y, dx, dy, tx, ty);
 }
 
-// rng.rs:180-197 + almost_infinite.rs:100-114 from the two Box-Muller samples
-__device__ __forceinline__ void normal_dispersal_draw(uint64_t d0, uint64_t d1, double sigma,
-                                                      uint32_t x, uint32_t y, uint32_t &tx,
-                                                      uint32_t &ty) {
+// rng.rs:180-197 sample_2d_normal (Box-Muller) scaled by sigma
+// (almost_infinite_normal.rs:58-68) from the two samples, with CUDA's f64
+// log/sin/cos
+__device__ __forceinline__ void normal_displacement(uint64_t d0, uint64_t d1, double sigma, double &dx,
+                                                    double &dy) {
     const double u0 = unit_open_closed(d0);
     const double u1 = unit_closed_open(d1);
     const double r = __dsqrt_rn(__dmul_rn(-2.0, log(u0)));
     const double theta = __dmul_rn(-kTau, u1);
     const double z0 = __dmul_rn(r, sin(theta));
     const double z1 = __dmul_rn(r, cos(theta));
-    const double dx = __dadd_rn(__dmul_rn(z0, sigma), 0.0);
-    const double dy = __dadd_rn(__dmul_rn(z1, sigma), 0.0);
-    const int64_t wrap = (int64_t)1 << 32;
-    const int64_t nx = ((int64_t)x + f64_to_i64(round(dx))) % wrap;
-    const int64_t ny = ((int64_t)y + f64_to_i64(round(dy))) % wrap;
-    tx = (uint32_t)((nx + wrap) % wrap);
-    ty = (uint32_t)((ny + wrap) % wrap);
+    dx = __dadd_rn(__dmul_rn(z0, sigma), 0.0);
+    dy = __dadd_rn(__dmul_rn(z1, sigma), 0.0);
+}
+
+// the Normal displacement rounded onto the plane (almost_infinite.rs:100-114)
+__device__ __forceinline__ void normal_dispersal_draw(uint64_t d0, uint64_t d1, double sigma,
+                                                      uint32_t x, uint32_t y, uint32_t &tx,
+                                                      uint32_t &ty) {
+    double dx, dy;
+    normal_displacement(d0, d1, sigma, dx, dy);
+    clamp_round_dispersal(x, y, dx, dy, tx, ty);
 }
 
 // landscape/extent.rs:44-49 LandscapeExtent::contains for the SI local

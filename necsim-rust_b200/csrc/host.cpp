@@ -402,8 +402,10 @@ void validate(const necsim_scenario &sc) {
         validate_rectangle(sc, true);
         break;
     case NECSIM_SPATIALLY_EXPLICIT:
-        if (!sc.width || !sc.height || !sc.habitat || !sc.dispersal)
-            fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyExplicit needs habitat and dispersal maps");
+        if (!sc.width || !sc.height || !sc.habitat || (!sc.dispersal && !sc.cells))
+            fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyExplicit needs a habitat map and a dispersal map or tables");
+        if (sc.cells && sc.n_atoms && !sc.atoms)
+            fail(NECSIM_E_INVALID_ARGUMENT, "SpatiallyExplicit tables: n_atoms > 0 without atoms");
         if (sc.turnover_map) {
             // maps/mod.rs:34-53 (non-negative rates) and turnover_rate/in_memory.rs:50-72
             // (InMemoryTurnoverRateError::ZeroTurnoverHabitat)
@@ -638,6 +640,8 @@ struct Engine {
     Control *h_ctl = nullptr;  // pinned
 
     unsigned step_grid = 0, step_block = 0;
+    unsigned coop_grid = 0;   // cooperative kernel (Poisson sampler), kCoopBlock threads per block
+    uint64_t coop_max = 0;    // rounds with at most this many live lineages run there
     unsigned aux_grid = 0, aux_block = 256;
 
     // learned schedule (schedule == 1): model weights (owned by the model)
@@ -732,11 +736,25 @@ struct Engine {
 // ---- SpatiallyExplicit tables ----
 void upload_tables(Engine &E, SimHost &s) {
     HostTables t;
-    int rc = build_spatially_explicit_tables(s.sc, t);
-    if (rc == 1) fail(NECSIM_E_EMPTY_HABITAT, "habitat map has no habitable cell");
-    if (rc == 2) fail(NECSIM_E_DISPERSAL_MAP, "dispersal map violates the in-memory dispersal contract");
-    if (rc == 3) fail(NECSIM_E_TOO_LARGE, "more than 2^32 alias atoms");
-    if (rc) fail(NECSIM_E_INVALID_ARGUMENT, "table build failed");
+    if (s.sc.cells) {
+        // tables built before by the caller: used as given (the kernels
+        // bound-check every index they read from them)
+        const uint64_t n_cells = (uint64_t)s.sc.width * s.sc.height;
+        const CellRecord *c = reinterpret_cast<const CellRecord *>(s.sc.cells);
+        t.cells.assign(c, c + n_cells);
+        if (s.sc.n_atoms) {
+            if (s.sc.n_atoms > 0xffffffffULL) fail(NECSIM_E_TOO_LARGE, "more than 2^32 alias atoms");
+            const AliasAtom *a = reinterpret_cast<const AliasAtom *>(s.sc.atoms);
+            t.atoms.assign(a, a + s.sc.n_atoms);
+        }
+        t.entropy.assign(n_cells, 0.0f);
+    } else {
+        int rc = build_spatially_explicit_tables(s.sc, t);
+        if (rc == 1) fail(NECSIM_E_EMPTY_HABITAT, "habitat map has no habitable cell");
+        if (rc == 2) fail(NECSIM_E_DISPERSAL_MAP, "dispersal map violates the in-memory dispersal contract");
+        if (rc == 3) fail(NECSIM_E_TOO_LARGE, "more than 2^32 alias atoms");
+        if (rc) fail(NECSIM_E_INVALID_ARGUMENT, "table build failed");
+    }
     CellRecord *dc = dev_alloc<CellRecord>(t.cells.size());
     AliasAtom *da = dev_alloc<AliasAtom>(t.atoms.size());
     E.d_cells.push_back(dc);
@@ -794,6 +812,14 @@ void choose_launch(Engine &E) {
     if (per_sm < 1) per_sm = 1;
     E.step_block = block;
     E.step_grid = E.args.grid_size ? E.args.grid_size : (unsigned)(per_sm * E.n_sms);
+    if (E.args.event_time_sampler != NECSIM_SAMPLER_EXP) {
+        // one warp per lineage, all of them resident at once
+        int coop_per_sm = 0;
+        CK(coop_kernel_occupancy(E.kind, &coop_per_sm));
+        if (coop_per_sm < 1) coop_per_sm = 1;
+        E.coop_grid = (unsigned)(coop_per_sm * E.n_sms);
+        E.coop_max = (uint64_t)E.coop_grid * (kCoopBlock / 32);
+    }
     E.aux_block = 256;
     E.aux_grid = (unsigned)(E.n_sms * 8);
 }
@@ -980,6 +1006,7 @@ StepArgs make_step_args(Engine &E, DeviceLineages &in) {
     a.n_sims = (uint32_t)E.sims.size();
     a.order = E.learned ? E.order : nullptr;
     a.exp_sampler = E.args.event_time_sampler == NECSIM_SAMPLER_EXP ? 1u : 0u;
+    a.coop_max = E.coop_max;
     if (E.tracing) {
         a.trace.deaths = E.trace_deaths;
         a.trace.n_deaths = E.trace_counts + 1;
@@ -995,8 +1022,9 @@ FeatureArgs make_feature_args(Engine &E, DeviceLineages &in) {
     f.params = E.d_params;
     f.counters = E.d_counters;
     f.kind = E.kind;
-    // the step kernel's cooperative regime (one warp per lineage)
-    f.skip_at_most = (uint64_t)E.step_grid * (E.step_block / 32);
+    // rounds stepped one warp per lineage (the cooperative kernel, or the
+    // exponential sampler's step kernel when it has a warp per lineage)
+    f.skip_at_most = E.coop_max ? E.coop_max : (uint64_t)E.step_grid * (E.step_block / 32);
     return f;
 }
 
@@ -1079,7 +1107,7 @@ void enqueue_round(Engine &E, unsigned r, bool events, bool external) {
         else
             CK(cudaEventRecord(E.ev_start[r], E.stream));
     }
-    CK(launch_step(E.kind, make_step_args(E, in), E.step_grid, E.step_block, E.stream));
+    CK(launch_step(E.kind, make_step_args(E, in), E.step_grid, E.step_block, E.coop_grid, E.stream));
     if (events) {
         if (external)
             CK(cudaEventRecordWithFlags(E.ev_end[r], E.stream, cudaEventRecordExternal));
@@ -1164,13 +1192,15 @@ RunResult run_rounds(Engine &E) {
     // one block per resident simulation, at most two per SM
     // at most one block per SM beside the global rounds (room for their
     // kernels), two per SM when only resident simulations are left
+    const uint64_t max_rounds = E.args.max_rounds ? E.args.max_rounds : (1ULL << 26);
     const unsigned grid_beside = (unsigned)std::min<size_t>(E.sims.size(), (size_t)E.n_sms);
     const unsigned grid_alone = (unsigned)std::min<size_t>(E.sims.size(), (size_t)E.n_sms * 2);
     while (E.h_ctl->n_active > 0 || E.h_ctl->n_resident > 0) {
         // every round advances each active simulation's horizon by at least
         // step_slice / lambda, so each live lineage expects >= step_slice
         // events per round: a valid run never reaches these bounds
-        if (++graph_launches > (1ULL << 26) / rounds) fail(NECSIM_E_TIMEOUT, "round limit reached");
+        if (++graph_launches > max_rounds / rounds + (max_rounds % rounds ? 1 : 0))
+            fail(NECSIM_E_TIMEOUT, "round limit reached (necsim_args.max_rounds)");
         if (E.h_ctl->steps_total == last_steps && E.h_ctl->n_cur == last_live) {
             if (++stalled >= 64) fail(NECSIM_E_TIMEOUT, "no progress over 64 graph launches");
         } else {
@@ -1211,7 +1241,7 @@ RunResult run_rounds(Engine &E) {
                 enqueue_rounds(E, rounds, true, false);
             }
             CK(cudaMemsetAsync(&E.d_ctl->graph_done, 1, sizeof(int), E.stream));
-            rr.launches += (uint64_t)rounds * (E.learned ? 9 : 5);
+            rr.launches += (uint64_t)rounds * ((E.learned ? 9 : 5) + (E.coop_max ? 1 : 0));
             // after an even number of rounds the live lineages are in A
             if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_rows, E.trace_counts,
                                                     E.trace_rows_cap, E.stream));
@@ -1717,6 +1747,8 @@ int necsim_gpu_create(const necsim_scenario *scenario, const necsim_args *args, 
             ctx->tables_ready = true;
             ctx->scenario.habitat = ctx->habitat.data();
             ctx->scenario.dispersal = nullptr;  // consumed by the table build
+            ctx->scenario.cells = nullptr;
+            ctx->scenario.atoms = nullptr;
         }
     });
     if (rc != NECSIM_OK) {
@@ -1889,6 +1921,39 @@ static std::vector<SimHost> batch_sims(const necsim_scenario *scenarios, const u
         sh.n_origins = count_origins(scenarios[s]);
     }
     return sims;
+}
+
+int necsim_gpu_displacements(int32_t device, int32_t kind, const uint64_t *draws, uint64_t n, double a, double b,
+                             double *dx, double *dy) {
+    if (kind != NECSIM_ALMOST_INFINITE_NORMAL && kind != NECSIM_ALMOST_INFINITE_CLARK2DT)
+        return NECSIM_E_INVALID_ARGUMENT;
+    if (n && (!draws || !dx || !dy)) return NECSIM_E_INVALID_ARGUMENT;
+    if (kind == NECSIM_ALMOST_INFINITE_CLARK2DT && !(b > 0.0)) return NECSIM_E_INVALID_ARGUMENT;
+    return guarded(nullptr, nullptr, 0, [&] {
+        if (n == 0) return;
+        CK(cudaSetDevice(device));
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, device));
+        struct Res {
+            uint64_t *d = nullptr;
+            double *x = nullptr, *y = nullptr;
+            ~Res() {
+                if (d) cudaFree(d);
+                if (x) cudaFree(x);
+                if (y) cudaFree(y);
+            }
+        } r;
+        r.d = dev_alloc<uint64_t>(2 * n);
+        r.x = dev_alloc<double>(n);
+        r.y = dev_alloc<double>(n);
+        CK(cudaMemcpy(r.d, draws, 2 * n * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        // the step kernels take the Clark2Dt exponent 1 / p computed on the host
+        const double bb = kind == NECSIM_ALMOST_INFINITE_CLARK2DT ? 1.0 / b : 0.0;
+        const int32_t dev_kind = kind == NECSIM_ALMOST_INFINITE_NORMAL ? (int32_t)kAlmostInfiniteNormal : -1;
+        CK(launch_displacements(dev_kind, r.d, n, a, bb, r.x, r.y, (unsigned)prop.multiProcessorCount * 8, 0));
+        CK(cudaMemcpy(dx, r.x, n * sizeof(double), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(dy, r.y, n * sizeof(double), cudaMemcpyDeviceToHost));
+    });
 }
 
 int necsim_gpu_hash_peak(int32_t device, double *wymum_per_second) {

@@ -52,19 +52,6 @@ struct Lane {
     CellRecord rec;  // SpatiallyExplicit: record of the current cell
 };
 
-template <int KIND>
-__device__ __forceinline__ uint64_t lane_injection(const Lane &l, const SimParams &p) {
-    if (KIND == kNonSpatial) return non_spatial_injection(0, 0, p.width, p.deme, l.x, l.y, l.i);
-    if (KIND == kSpatiallyImplicit) {
-        // habitat/spatially_implicit.rs:106-120
-        if (in_local(p, l.x, l.y)) return non_spatial_injection(0, 0, p.width, p.deme, l.x, l.y, l.i);
-        return non_spatial_injection(p.meta_ox, p.meta_oy, p.meta_width, p.meta_deme, l.x, l.y, l.i);
-    }
-    // almost_infinite.rs:66-70 (WrappingNoise defers to it, habitat/wrapping_noise/mod.rs:170-175)
-    if (KIND == kAlmostInfiniteNormal || KIND == kWrappingNoise) return ((uint64_t)l.y << 32) | (uint64_t)l.x;
-    return l.rec.injection + (uint64_t)l.i;                                          // in_memory.rs:70-80
-}
-
 // The event-time samplers' constants at the lineage's location: per cell
 // under a SpatiallyExplicit turnover map (turnover_rate/in_memory.rs:22-40,
 // the cell of a loaded lineage is in range), else the simulation's.
@@ -74,24 +61,30 @@ __device__ __forceinline__ const PoissonConsts &poisson_consts(const Lane &l, co
     return p.pois;
 }
 
-__device__ __forceinline__ bool load_cell(const SimParams &p, uint32_t x, uint32_t y, CellRecord &rec,
-                                          uint32_t *status) {
+// The record of cell (x, y); false (and no read) when it lies outside the table.
+__device__ __forceinline__ bool fetch_cell(const SimParams &p, uint32_t x, uint32_t y, CellRecord &rec) {
     const uint64_t cell = (uint64_t)y * p.width + (uint64_t)x;
-    if (cell >= p.n_cells) {
-        set_status(status, kErrCellIndex);
-        return false;
-    }
+    if (cell >= p.n_cells) return false;
     rec = p.cells[cell];
     return true;
+}
+
+__device__ __forceinline__ bool load_cell(const SimParams &p, uint32_t x, uint32_t y, CellRecord &rec,
+                                          uint32_t *status) {
+    if (fetch_cell(p, x, y, rec)) return true;
+    set_status(status, kErrCellIndex);
+    return false;
 }
 
 // packed_separable_alias/dispersal.rs:16-77 and alias/packed.rs:135-163, fed
 // with the event's samples 2..4: the self-dispersal test (when taken) uses
 // the first, the alias draw the next; `d_coal` receives the sample after them.
+// A failed bound check returns false with its status bit in `err` (nothing
+// is read out of range).
 template <bool EAGER>
 __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
     uint64_t e2, uint64_t e3, uint64_t e4, uint64_t rs, const SimParams &p, uint32_t x, uint32_t y,
-    const CellRecord &rec, uint32_t &tx, uint32_t &ty, uint64_t &d_coal, uint32_t *status) {
+    const CellRecord &rec, uint32_t &tx, uint32_t &ty, uint64_t &d_coal, uint32_t &err) {
     const uint64_t cell = (uint64_t)y * p.width + (uint64_t)x;
     uint64_t target;
     const double sd = rec.self_dispersal;
@@ -119,7 +112,7 @@ __device__ __forceinline__ bool spatially_explicit_dispersal_draw(
         const double frac = __dsub_rn(f, __ull2double_rn(i));
         const uint64_t at = (uint64_t)rec.atom_start + i;
         if (i >= len || at >= p.n_atoms) {
-            set_status(status, kErrAtomIndex);
+            err |= kErrAtomIndex;
             return false;
         }
         const AliasAtom atom = p.atoms[at];
@@ -165,45 +158,84 @@ __device__ __forceinline__ void record_death(const TraceSink &t, uint64_t gref, 
     }
 }
 
-// The event at l.next (event_sampler/independent.rs:112-222) from the
-// re-primed state rs: speciation, or dispersal + coalescence index.  The
-// event's first DRAWN samples arrive drawn (e1..e4); later ones are drawn
-// here only when the branch consumes them.  Only a lane with `emit` writes
-// events and counters (all lanes of a cooperative warp hold the same
-// lineage).
-template <int KIND, int DRAWN>
-__device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const EventSink &k, uint64_t rs,
-                                             uint64_t e1, uint64_t e2, uint64_t e3, uint64_t e4, bool emit) {
-    constexpr bool EAGER = DRAWN >= 4;
-    l.steps += 1;
-    // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
-    if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
-        if (emit) {
-            const unsigned long long e = atomicAdd(k.n_spec_total, 1ULL);
-            if (e < k.spec_cap) {
-                DevSpeciationEvent ev;
-                ev.gref = l.gref;
-                ev.prior_time = l.last;
-                ev.event_time = l.next;
-                ev.x = l.x;
-                ev.y = l.y;
-                ev.idx = l.i;
-                ev.sim = l.s;
-                k.spec[e] = ev;
-            } else {
-                set_status(k.status, kErrEventOverflow);
-            }
-            SimCounters &c = k.counters[l.s];
-            atomicAdd(&c.steps, (unsigned long long)l.steps);
-            atomicMax(&c.max_time_bits, f64_bits(l.next));
-            atomicAdd(&c.n_speciation, 1ULL);
-            record_death(k.trace, l.gref, l.steps, l.s);
-        }
-        return kStepSpeciated;
+// The location injection of (x, y, i) (habitat/*: map_indexed_location_to_u64_injective);
+// `rec` is the record of (x, y) for SpatiallyExplicit.
+template <int KIND>
+__device__ __forceinline__ uint64_t injection_at(const SimParams &p, uint32_t x, uint32_t y, uint32_t i,
+                                                 const CellRecord &rec) {
+    if (KIND == kNonSpatial) return non_spatial_injection(0, 0, p.width, p.deme, x, y, i);
+    if (KIND == kSpatiallyImplicit) {
+        // habitat/spatially_implicit.rs:106-120
+        if (in_local(p, x, y)) return non_spatial_injection(0, 0, p.width, p.deme, x, y, i);
+        return non_spatial_injection(p.meta_ox, p.meta_oy, p.meta_width, p.meta_deme, x, y, i);
     }
-    if (DRAWN < 2) e2 = draw_at(rs, 2);
-    if (DRAWN < 3) e3 = draw_at(rs, 3);
-    uint32_t tx, ty, ti;
+    if (KIND == kAlmostInfiniteNormal || KIND == kWrappingNoise) return ((uint64_t)y << 32) | (uint64_t)x;
+    return rec.injection + (uint64_t)i;
+}
+
+template <int KIND>
+__device__ __forceinline__ uint64_t lane_injection(const Lane &l, const SimParams &p) {
+    return injection_at<KIND>(p, l.x, l.y, l.i, l.rec);
+}
+
+// Writes the speciation event of the lineage (event time l.next) and hands
+// its step count to the simulation's counters.
+__device__ __forceinline__ void emit_speciation(const Lane &l, const EventSink &k) {
+    const unsigned long long e = atomicAdd(k.n_spec_total, 1ULL);
+    if (e < k.spec_cap) {
+        DevSpeciationEvent ev;
+        ev.gref = l.gref;
+        ev.prior_time = l.last;
+        ev.event_time = l.next;
+        ev.x = l.x;
+        ev.y = l.y;
+        ev.idx = l.i;
+        ev.sim = l.s;
+        k.spec[e] = ev;
+    } else {
+        set_status(k.status, kErrEventOverflow);
+    }
+    SimCounters &c = k.counters[l.s];
+    atomicAdd(&c.steps, (unsigned long long)l.steps);
+    atomicMax(&c.max_time_bits, f64_bits(l.next));
+    atomicAdd(&c.n_speciation, 1ULL);
+    record_death(k.trace, l.gref, l.steps, l.s);
+}
+
+// Writes the dispersal event of the lineage (event time l.next) to (tx, ty, ti).
+__device__ __forceinline__ void emit_dispersal(const Lane &l, const EventSink &k, uint32_t tx, uint32_t ty,
+                                               uint32_t ti) {
+    const unsigned long long e = atomicAdd(k.n_disp_total, 1ULL);
+    if (e < k.disp_cap) {
+        DevDispersalEvent ev;
+        ev.gref = l.gref;
+        ev.prior_time = l.last;
+        ev.event_time = l.next;
+        ev.x = l.x;
+        ev.y = l.y;
+        ev.idx = l.i;
+        ev.tx = tx;
+        ev.ty = ty;
+        ev.tidx = ti;
+        ev.sim = l.s;
+        ev.pad = 0;
+        k.disp[e] = ev;
+    } else {
+        set_status(k.status, kErrDispersalOverflow);
+    }
+}
+
+// Dispersal target and coalescence index of an event that is not a
+// speciation (event_sampler/independent.rs:160-204), from the re-primed
+// state rs and its samples 2..4 (samples DRAWN + 1.. are drawn here only
+// when the branch consumes them).  No side effects: `rec` receives the
+// target's record (SpatiallyExplicit); a failed bound check or a
+// WrappingNoise rejection limit returns false with its status bit in `err`.
+template <int KIND, int DRAWN>
+__device__ __forceinline__ bool event_target(const Lane &l, const SimParams &p, uint64_t rs, uint64_t e2,
+                                             uint64_t e3, uint64_t e4, uint32_t &tx, uint32_t &ty, uint32_t &ti,
+                                             CellRecord &rec, uint32_t &err) {
+    constexpr bool EAGER = DRAWN >= 4;
     if (KIND == kNonSpatial) {
         non_spatial_dispersal_draw(e2, 0, 0, p.width, p.height, p.width_magic, tx, ty);
         ti = coalescence_index(e3, p.deme);
@@ -213,11 +245,11 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
         const bool to_meta = !local || (e2 >> 11) < p.migration_threshold;
         const uint64_t d_index = local ? e3 : e2;
         const uint64_t d_coal = local ? (EAGER ? e4 : draw_at(rs, 4)) : e3;
-        if (to_meta)
-            non_spatial_dispersal_draw(d_index, p.meta_ox, p.meta_oy, p.meta_width, p.meta_height,
-                                       p.meta_width_magic, tx, ty);
-        else
-            non_spatial_dispersal_draw(d_index, 0, 0, p.width, p.height, p.width_magic, tx, ty);
+        // one draw from the chosen community's extent (selects, not branches)
+        const uint32_t ox = to_meta ? p.meta_ox : 0u, oy = to_meta ? p.meta_oy : 0u;
+        const uint64_t w = to_meta ? p.meta_width : p.width, h = to_meta ? p.meta_height : p.height;
+        const uint64_t magic = to_meta ? p.meta_width_magic : p.width_magic;
+        non_spatial_dispersal_draw(d_index, ox, oy, w, h, magic, tx, ty);
         // habitat/spatially_implicit.rs:95-103: local extent first
         ti = coalescence_index(d_coal, in_local(p, tx, ty) ? p.deme : p.meta_deme);
     } else if (KIND == kAlmostInfiniteNormal) {
@@ -240,8 +272,8 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
                 normal_dispersal_draw(d0, d1, p.sigma, l.x, l.y, tx, ty);
                 if ((tx != l.x || ty != l.y) && noise::habitat_at(p.noise, tx, ty) != 0) break;
                 if (c + 1 == kMaxDispersalRejections) {
-                    set_status(k.status, kErrDispersalRejections);
-                    return kStepDropped;
+                    err |= kErrDispersalRejections;
+                    return false;
                 }
                 d0 = draw_at(rs, 5 + 2 * (uint64_t)c);
                 d1 = draw_at(rs, 6 + 2 * (uint64_t)c);
@@ -250,32 +282,42 @@ __device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const 
         ti = 0;
     } else {
         uint64_t d_coal;
-        if (!spatially_explicit_dispersal_draw<EAGER>(e2, e3, e4, rs, p, l.x, l.y, l.rec, tx, ty, d_coal,
-                                                      k.status) ||
-            !load_cell(p, tx, ty, l.rec, k.status))
-            return kStepDropped;
-        ti = coalescence_index(d_coal, l.rec.habitat);
-    }
-    if (emit && k.report_dispersal) {
-        const unsigned long long e = atomicAdd(k.n_disp_total, 1ULL);
-        if (e < k.disp_cap) {
-            DevDispersalEvent ev;
-            ev.gref = l.gref;
-            ev.prior_time = l.last;
-            ev.event_time = l.next;
-            ev.x = l.x;
-            ev.y = l.y;
-            ev.idx = l.i;
-            ev.tx = tx;
-            ev.ty = ty;
-            ev.tidx = ti;
-            ev.sim = l.s;
-            ev.pad = 0;
-            k.disp[e] = ev;
-        } else {
-            set_status(k.status, kErrDispersalOverflow);
+        if (!spatially_explicit_dispersal_draw<EAGER>(e2, e3, e4, rs, p, l.x, l.y, l.rec, tx, ty, d_coal, err))
+            return false;
+        if (!fetch_cell(p, tx, ty, rec)) {
+            err |= kErrCellIndex;
+            return false;
         }
+        ti = coalescence_index(d_coal, rec.habitat);
     }
+    return true;
+}
+
+// The event at l.next (event_sampler/independent.rs:112-222) from the
+// re-primed state rs: speciation, or dispersal + coalescence index.  The
+// event's first DRAWN samples arrive drawn (e1..e4); later ones are drawn
+// here only when the branch consumes them.  Only a lane with `emit` writes
+// events and counters (all lanes of a cooperative warp hold the same
+// lineage).
+template <int KIND, int DRAWN>
+__device__ __forceinline__ int lineage_event(Lane &l, const SimParams &p, const EventSink &k, uint64_t rs,
+                                             uint64_t e1, uint64_t e2, uint64_t e3, uint64_t e4, bool emit) {
+    l.steps += 1;
+    // speciation iff U[0,1) < nu  <=>  (e1 >> 11) < ceil(nu * 2^53)
+    if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
+        if (emit) emit_speciation(l, k);
+        return kStepSpeciated;
+    }
+    if (DRAWN < 2) e2 = draw_at(rs, 2);
+    if (DRAWN < 3) e3 = draw_at(rs, 3);
+    uint32_t tx, ty, ti, err = 0;
+    CellRecord rec;
+    if (!event_target<KIND, DRAWN>(l, p, rs, e2, e3, e4, tx, ty, ti, rec, err)) {
+        set_status(k.status, err);
+        return kStepDropped;
+    }
+    if (emit && k.report_dispersal) emit_dispersal(l, k, tx, ty, ti);
+    if (KIND == kSpatiallyExplicit) l.rec = rec;
     l.x = tx;
     l.y = ty;
     l.i = ti;
@@ -531,6 +573,223 @@ __device__ __forceinline__ int lineage_step_coop(Lane &l, const SimParams &p, co
     return lineage_event<KIND, 4>(l, p, k, rs, e1, e2, e3, e4, lane == 0);
 }
 
+// ---- the cooperative step, speculative form (Poisson sampler) ----
+//
+// One lineage held by all 32 lanes of a warp, stepped event after event.
+// Every lane primes one WyHash state and draws its samples 1..4 per pass:
+//   lanes 0..7  (bucket lanes): bucket base + b, b = lane, of the search of
+//               poisson.rs:48-100: the Devroye count and the times of
+//               events 0..2 (further events draw their samples here);
+//   lanes 8..31 (candidate lanes): one (bucket b, event k) pair each,
+//               re-primed as if that event came next (time index
+//               base + b + INV_PHI (k + 1), poisson.rs:102-106), computing
+//               the whole event from its samples: speciation, dispersal
+//               target, coalescence index and the target's location term.
+// The first bucket with an event after `before` selects (b, k); the
+// candidate lane holding that pair hands its event to the warp, so the next
+// event's primes start right after the selection.  The pairs are the 24
+// likeliest selections for lambda * delta_t = 1 (the reference's defaults,
+// 99.7% of events); any other selection is computed after it.  Every
+// outcome is a pure function of the lineage and the samples, so the
+// speculation changes no result.
+
+constexpr unsigned kCoopBuckets = 8;
+// SpatiallyExplicit candidates read an alias atom and the target's record:
+// only the likeliest pairs speculate (the others are computed on selection)
+constexpr unsigned kCoopSpecLoads = 8;
+
+struct CoopPair {
+    uint8_t b, k;
+};
+// decreasing probability of being the selected (bucket, event) pair
+constexpr CoopPair kCoopPairList[32 - kCoopBuckets] = {
+    {1, 0}, {0, 0}, {2, 0}, {0, 1}, {1, 1}, {3, 0}, {2, 1}, {0, 2}, {1, 2}, {4, 0}, {3, 1}, {2, 2},
+    {5, 0}, {0, 3}, {4, 1}, {1, 3}, {3, 2}, {6, 0}, {5, 1}, {2, 3}, {4, 2}, {7, 0}, {0, 4}, {6, 1}};
+// the list as bytes b | k << 4, eight per word, so a lane finds its pair in registers
+constexpr uint64_t coop_pair_word(int first) {
+    uint64_t w = 0;
+    for (int j = 0; j < 8; ++j)
+        w |= (uint64_t)(kCoopPairList[first + j].b | (kCoopPairList[first + j].k << 4)) << (8 * j);
+    return w;
+}
+constexpr uint64_t kCoopPairWord0 = coop_pair_word(0), kCoopPairWord1 = coop_pair_word(8),
+                   kCoopPairWord2 = coop_pair_word(16);
+
+// An event computed from its samples: what happened and where the lineage went.
+struct CoopOutcome {
+    uint32_t code;      // kStepMoved, kStepSpeciated or kStepDropped, status bits << 8
+    uint32_t tx, ty, ti;
+    uint64_t loc_next;  // location term of the target (kStepMoved)
+    CellRecord rec;     // record of the target cell (SpatiallyExplicit)
+};
+
+// The event of lineage l from the re-primed state rs and its samples 1..4
+// (event_sampler/independent.rs:112-222), without side effects.  An inactive
+// lane computes nothing (code kStepDropped with no status bits).
+template <int KIND>
+__device__ __forceinline__ void coop_outcome(const Lane &l, const SimParams &p, uint64_t seed, uint64_t rs,
+                                             uint64_t e1, uint64_t e2, uint64_t e3, uint64_t e4, bool active,
+                                             CoopOutcome &o) {
+    o.code = kStepDropped;
+    if (!active) return;
+    if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
+        o.code = kStepSpeciated;
+        return;
+    }
+    uint32_t err = 0;
+    if (!event_target<KIND, 4>(l, p, rs, e2, e3, e4, o.tx, o.ty, o.ti, o.rec, err)) {
+        o.code = kStepDropped | (err << 8);
+        return;
+    }
+    o.code = kStepMoved;
+    o.loc_next = location_term(seed, injection_at<KIND>(p, o.tx, o.ty, o.ti, o.rec));
+}
+
+template <int KIND>
+__device__ __forceinline__ void shfl_outcome(CoopOutcome &o, int src) {
+    o.code = __shfl_sync(kFull, o.code, src);
+    o.tx = __shfl_sync(kFull, o.tx, src);
+    o.ty = __shfl_sync(kFull, o.ty, src);
+    o.ti = __shfl_sync(kFull, o.ti, src);
+    o.loc_next = __shfl_sync(kFull, o.loc_next, src);
+    if (KIND == kSpatiallyExplicit) {
+        o.rec.injection = __shfl_sync(kFull, o.rec.injection, src);
+        o.rec.self_dispersal = __shfl_sync(kFull, o.rec.self_dispersal, src);
+        o.rec.atom_start = __shfl_sync(kFull, o.rec.atom_start, src);
+        o.rec.atom_count = __shfl_sync(kFull, o.rec.atom_count, src);
+        o.rec.habitat = __shfl_sync(kFull, o.rec.habitat, src);
+        o.rec.non_self_event = __shfl_sync(kFull, o.rec.non_self_event, src);
+    }
+}
+
+// Steps lineage l (identical on every lane of the warp) until its next event
+// is at or beyond l.horizon (kStepStop, the peek kept in l), it speciates
+// (kStepSpeciated) or a bound check fails (kStepDropped).  `events` counts
+// the executed events; side effects happen on lane 0 only.
+template <int KIND>
+__device__ __forceinline__ int coop_run(Lane &l, const SimParams &p, const EventSink &k, uint64_t &events) {
+    const unsigned lane = threadIdx.x & 31u;
+    const bool bucket_lane = lane < kCoopBuckets;
+    uint32_t my_b = lane, my_k = 0xffu;
+    if (!bucket_lane) {
+        const unsigned j = lane - kCoopBuckets;
+        const uint64_t w = j < 8u ? kCoopPairWord0 : (j < 16u ? kCoopPairWord1 : kCoopPairWord2);
+        const uint32_t pr = (uint32_t)(w >> (8u * (j & 7u))) & 0xffu;
+        my_b = pr & 15u;
+        my_k = pr >> 4;
+    }
+    const uint64_t my_tadd = (uint64_t)my_b + (bucket_lane ? 0ULL : kInvPhi * (uint64_t)(my_k + 1u));
+    const bool speculate =
+        !bucket_lane && (KIND != kSpatiallyExplicit || lane < kCoopBuckets + kCoopSpecLoads);
+    const uint64_t seed = p.seed;
+    const double delta_t = p.delta_t;
+    const long long horizon_bits = __double_as_longlong(l.horizon);
+    uint64_t loc_term = location_term(seed, lane_injection<KIND>(l, p));
+    const PoissonConsts *pc = &poisson_consts<KIND>(l, p);
+    for (;;) {
+        CoopOutcome o;
+        bool have = false;
+        if (l.has_next) {
+            // a peek kept from the previous round
+            if (__double_as_longlong(l.next) >= horizon_bits) return kStepStop;
+        } else {
+            // IndependentActiveLineageSampler::pop_active_lineage_and_event_time
+            // (active_lineage_sampler/independent/sampler.rs:69-116)
+            const double before = l.last > p.min_event_time ? l.last : p.min_event_time;
+            const long long before_bits = __double_as_longlong(before);
+            uint64_t base = time_bucket(p, before);
+            uint32_t b_sel, k_sel;
+            long long t_bits;
+            for (;;) {
+                const uint64_t s = primed_state(loc_term, base + my_tadd);
+                const uint64_t d1 = draw_at(s, 1), d2 = draw_at(s, 2), d3 = draw_at(s, 3), d4 = draw_at(s, 4);
+                // bucket view: the earliest event of bucket base + b after
+                // `before` (ties: lowest index), poisson.rs:50-95
+                const uint32_t n_ev = poisson_count(d1, *pc);
+                const double step_start = __ull2double_rn(base + my_b);
+                const long long t0 = event_time_bits(step_start, d2, delta_t);
+                const long long t1 = event_time_bits(step_start, d3, delta_t);
+                const long long t2 = event_time_bits(step_start, d4, delta_t);
+                long long mine = kNoEvent;
+                uint32_t mine_k = 0;
+                if (n_ev > 0u && t0 > before_bits) {
+                    mine = t0;
+                    mine_k = 0;
+                }
+                if (n_ev > 1u && t1 > before_bits && t1 < mine) {
+                    mine = t1;
+                    mine_k = 1;
+                }
+                if (n_ev > 2u && t2 > before_bits && t2 < mine) {
+                    mine = t2;
+                    mine_k = 2;
+                }
+                if (bucket_lane && n_ev > 3u) {
+                    for (uint32_t kk = 3; kk < n_ev; ++kk) {
+                        const long long eb = event_time_bits(step_start, draw_at(s, kk + 2u), delta_t);
+                        if (eb > before_bits && eb < mine) {
+                            mine = eb;
+                            mine_k = kk;
+                        }
+                    }
+                }
+                // candidate view: the event this lane's pair would be
+                coop_outcome<KIND>(l, p, seed, s, d1, d2, d3, d4, speculate, o);
+                const unsigned found = __ballot_sync(kFull, bucket_lane && mine != kNoEvent);
+                if (found) {
+                    b_sel = (uint32_t)(__ffs(found) - 1);
+                    k_sel = __shfl_sync(kFull, mine_k, (int)b_sel);
+                    t_bits = __shfl_sync(kFull, mine, (int)b_sel);
+                    break;
+                }
+                base += kCoopBuckets;  // eight empty buckets: the next eight
+            }
+            l.reprime = base + (uint64_t)b_sel + kInvPhi * (uint64_t)(k_sel + 1u);
+            l.next = max_after(before, __longlong_as_double(t_bits));
+            l.has_next = true;
+            // the reference's early stop `next_event_time >= level_time`
+            // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
+            if (__double_as_longlong(l.next) >= horizon_bits) return kStepStop;
+            const unsigned hit = __ballot_sync(kFull, speculate && my_b == b_sel && my_k == k_sel);
+            if (hit) {
+                shfl_outcome<KIND>(o, __ffs(hit) - 1);
+                have = true;
+            }
+        }
+        if (!have) {
+            // re-prime for the event; lanes 0..3 draw samples 1..4
+            const uint64_t rs = primed_state(loc_term, l.reprime);
+            const uint64_t dk = draw_at(rs, (lane & 3u) + 1u);
+            const uint64_t e1 = __shfl_sync(kFull, dk, 0), e2 = __shfl_sync(kFull, dk, 1);
+            const uint64_t e3 = __shfl_sync(kFull, dk, 2), e4 = __shfl_sync(kFull, dk, 3);
+            coop_outcome<KIND>(l, p, seed, rs, e1, e2, e3, e4, true, o);
+        }
+        l.steps += 1;
+        const uint32_t code = o.code & 0xffu;
+        if (code == kStepSpeciated) {
+            events += 1;
+            if (lane == 0) emit_speciation(l, k);
+            return kStepSpeciated;
+        }
+        if (code != kStepMoved) {
+            if (lane == 0) set_status(k.status, o.code >> 8);
+            return kStepDropped;
+        }
+        events += 1;
+        if (lane == 0 && k.report_dispersal) emit_dispersal(l, k, o.tx, o.ty, o.ti);
+        l.x = o.tx;
+        l.y = o.ty;
+        l.i = o.ti;
+        l.last = l.next;
+        l.has_next = false;
+        if (KIND == kSpatiallyExplicit) {
+            l.rec = o.rec;
+            pc = &poisson_consts<KIND>(l, p);
+        }
+        loc_term = o.loc_next;
+    }
+}
+
 __device__ __forceinline__ EventSink sink_of(const StepArgs &a) {
     EventSink k;
     k.spec = a.spec;
@@ -662,52 +921,68 @@ __device__ __forceinline__ int pass_run(Lane &l, const SimParams &p, const Event
 // event and the refill.  With few lineages per lane (latency) each lane
 // runs lineage_step's latency form.  EXP: the exponential event-time
 // sampler, one event at a time per lane (no converged-pass form).
+// Copies one simulation's parameters to shared memory (single-simulation
+// launches); returns the parameters the kernel reads.
+template <bool SINGLE>
+__device__ __forceinline__ const SimParams *stage_params(const StepArgs &a, unsigned char *smem) {
+    if (!SINGLE) return a.params;
+    const uint4 *src = reinterpret_cast<const uint4 *>(a.params);
+    uint4 *dst = reinterpret_cast<uint4 *>(smem);
+    for (unsigned w = threadIdx.x; w < sizeof(SimParams) / 16; w += blockDim.x) dst[w] = src[w];
+    __syncthreads();
+    return reinterpret_cast<const SimParams *>(smem);
+}
+
+// At most one lineage per warp: each warp takes lineages from the queue and
+// steps each one with all its lanes (a lineage's events at warp latency,
+// lineages on all SMs).  Every lineage gets a warp at once, so the queue
+// order is moot (and not computed for such rounds).
+template <int KIND, bool SINGLE, bool EXP>
+__device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P, uint64_t n) {
+    const EventSink sink = sink_of(a);
+    const unsigned lane_id = threadIdx.x & 31u;
+    uint64_t warp_steps = 0;
+    for (;;) {
+        unsigned long long k = 0;
+        if (lane_id == 0) k = atomicAdd(a.work, 1ULL);
+        k = __shfl_sync(kFull, k, 0);
+        if (k >= n) break;
+        Lane c;
+        if (!take_lineage<KIND, SINGLE>(a, P, k, c, false)) continue;
+        const SimParams &p = P[SINGLE ? 0 : c.s];
+        int r;
+        if constexpr (EXP) {
+            for (;;) {
+                r = lineage_step_coop<KIND, true>(c, p, sink);
+                if (r != kStepMoved) break;
+                warp_steps += 1;
+            }
+            if (r == kStepSpeciated) warp_steps += 1;
+        } else {
+            r = coop_run<KIND>(c, p, sink, warp_steps);
+        }
+        if (lane_id == 0) {
+            if (r == kStepStop)
+                store_stopped(a, c);
+            else
+                a.state[c.slot] = (r == kStepSpeciated) ? 1 : 2;
+        }
+    }
+    if (a.steps_total && lane_id == 0 && warp_steps) atomicAdd(a.steps_total, (unsigned long long)warp_steps);
+}
+
 template <int KIND, bool SINGLE, bool EXP>
 __device__ __forceinline__ void step_body(const StepArgs &a) {
     // one simulation: its parameters live in shared memory for the launch
     __shared__ __align__(16) unsigned char params_smem[SINGLE ? sizeof(SimParams) : 16];
-    if (SINGLE) {
-        const uint4 *src = reinterpret_cast<const uint4 *>(a.params);
-        uint4 *dst = reinterpret_cast<uint4 *>(params_smem);
-        for (unsigned w = threadIdx.x; w < sizeof(SimParams) / 16; w += blockDim.x) dst[w] = src[w];
-        __syncthreads();
-    }
-    const SimParams *P = SINGLE ? reinterpret_cast<const SimParams *>(params_smem) : a.params;
-    const EventSink sink = sink_of(a);
     const uint64_t n = *a.n_cur;
+    // the Poisson sampler's cooperative rounds run in coop_kernel
+    if (!EXP && n <= a.coop_max) return;
+    const SimParams *P = stage_params<SINGLE>(a, params_smem);
+    const EventSink sink = sink_of(a);
     const unsigned lane_id = threadIdx.x & 31u;
-    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32u);
-    if (n <= warps) {
-        // at most one lineage per warp: each warp steps its lineages
-        // cooperatively (a lineage's events at warp latency, lineages on
-        // all SMs)
-        uint64_t warp_steps = 0;
-        for (;;) {
-            unsigned long long k = 0;
-            if (lane_id == 0) k = atomicAdd(a.work, 1ULL);
-            k = __shfl_sync(kFull, k, 0);
-            if (k >= n) break;
-            Lane c;
-            // every lineage gets a warp at once: the queue order is moot
-            // (and not computed for such rounds)
-            if (!take_lineage<KIND, SINGLE>(a, P, k, c, false)) continue;
-            const SimParams &p = P[SINGLE ? 0 : c.s];
-            int r;
-            for (;;) {
-                r = lineage_step_coop<KIND, EXP>(c, p, sink);
-                if (r != kStepMoved) break;
-                warp_steps += 1;
-            }
-            if (lane_id == 0) {
-                if (r == kStepStop) {
-                    store_stopped(a, c);
-                } else {
-                    if (r == kStepSpeciated) warp_steps += 1;
-                    a.state[c.slot] = (r == kStepSpeciated) ? 1 : 2;
-                }
-            }
-        }
-        if (a.steps_total && lane_id == 0 && warp_steps) atomicAdd(a.steps_total, (unsigned long long)warp_steps);
+    if (EXP && n <= (uint64_t)gridDim.x * (blockDim.x / 32u)) {
+        coop_body<KIND, SINGLE, true>(a, P, n);
         return;
     }
     const bool lat = n * 4 <= (uint64_t)gridDim.x * blockDim.x;
@@ -779,6 +1054,19 @@ __global__ void __launch_bounds__(kStepBlockMax) step_kernel(StepArgs a) {
 template <int KIND, bool SINGLE>
 __global__ void __launch_bounds__(kStepBlockMax, 1) step_kernel_exp(StepArgs a) {
     step_body<KIND, SINGLE, true>(a);
+}
+
+// The Poisson sampler's rounds with at most coop_max live lineages, one warp
+// per lineage (coop_run); the step kernel takes the other rounds.  Its own
+// kernel, so that the speculative form's registers do not lower the step
+// kernel's occupancy.
+template <int KIND, bool SINGLE>
+__global__ void __launch_bounds__(kCoopBlock) coop_kernel(StepArgs a) {
+    __shared__ __align__(16) unsigned char params_smem[SINGLE ? sizeof(SimParams) : 16];
+    const uint64_t n = *a.n_cur;
+    if (n > a.coop_max) return;
+    const SimParams *P = stage_params<SINGLE>(a, params_smem);
+    coop_body<KIND, SINGLE, false>(a, P, n);
 }
 
 // Per-simulation horizon rule (canonical schedule):
@@ -891,19 +1179,25 @@ __global__ void __launch_bounds__(THREADS) resident_kernel(ResidentArgs a) {
                 const bool c_alive = __shfl_sync(kFull, alive ? 1 : 0, 0) != 0;
                 if (c_alive) {
                     bool c_live = true;
-                    for (;;) {
-                        const int r = lineage_step_coop<KIND, EXP>(c, p, sink);
-                        if (r == kStepMoved) {
-                            ++my_events;
-                            continue;
+                    if constexpr (EXP) {
+                        for (;;) {
+                            const int r = lineage_step_coop<KIND, true>(c, p, sink);
+                            if (r == kStepMoved) {
+                                ++my_events;
+                                continue;
+                            }
+                            if (r == kStepSpeciated) {
+                                ++my_events;
+                                c_live = false;
+                            } else if (r == kStepDropped) {
+                                c_live = false;
+                            }
+                            break;
                         }
-                        if (r == kStepSpeciated) {
-                            ++my_events;
-                            c_live = false;
-                        } else if (r == kStepDropped) {
-                            c_live = false;
-                        }
-                        break;
+                    } else {
+                        uint64_t ev = 0;
+                        c_live = coop_run<KIND>(c, p, sink, ev) == kStepStop;
+                        my_events += ev;
                     }
                     if ((t & 31u) == 0) {
                         l = c;
@@ -1216,27 +1510,53 @@ __global__ void schedule_kernel(ScheduleArgs a) {
 
 // ---- host-side launchers ----
 template <int KIND>
-static cudaError_t launch_step_t(const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st) {
+static cudaError_t launch_step_t(const StepArgs &a, unsigned grid, unsigned block, unsigned coop_grid,
+                                 cudaStream_t st) {
     if (a.exp_sampler) {
         if (a.n_sims == 1)
             step_kernel_exp<KIND, true><<<grid, block, 0, st>>>(a);
         else
             step_kernel_exp<KIND, false><<<grid, block, 0, st>>>(a);
-    } else if (a.n_sims == 1) {
-        step_kernel<KIND, true><<<grid, block, 0, st>>>(a);
-    } else {
-        step_kernel<KIND, false><<<grid, block, 0, st>>>(a);
+        return cudaGetLastError();
     }
+    if (a.coop_max) {
+        if (a.n_sims == 1)
+            coop_kernel<KIND, true><<<coop_grid, kCoopBlock, 0, st>>>(a);
+        else
+            coop_kernel<KIND, false><<<coop_grid, kCoopBlock, 0, st>>>(a);
+    }
+    if (a.n_sims == 1)
+        step_kernel<KIND, true><<<grid, block, 0, st>>>(a);
+    else
+        step_kernel<KIND, false><<<grid, block, 0, st>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st) {
+cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, unsigned coop_grid,
+                        cudaStream_t st) {
+    if (!a.exp_sampler && a.coop_max > (uint64_t)coop_grid * (kCoopBlock / 32)) return cudaErrorInvalidValue;
     switch (kind) {
-    case kNonSpatial: return launch_step_t<kNonSpatial>(a, grid, block, st);
-    case kSpatiallyImplicit: return launch_step_t<kSpatiallyImplicit>(a, grid, block, st);
-    case kAlmostInfiniteNormal: return launch_step_t<kAlmostInfiniteNormal>(a, grid, block, st);
-    case kSpatiallyExplicit: return launch_step_t<kSpatiallyExplicit>(a, grid, block, st);
-    case kWrappingNoise: return launch_step_t<kWrappingNoise>(a, grid, block, st);
+    case kNonSpatial: return launch_step_t<kNonSpatial>(a, grid, block, coop_grid, st);
+    case kSpatiallyImplicit: return launch_step_t<kSpatiallyImplicit>(a, grid, block, coop_grid, st);
+    case kAlmostInfiniteNormal: return launch_step_t<kAlmostInfiniteNormal>(a, grid, block, coop_grid, st);
+    case kSpatiallyExplicit: return launch_step_t<kSpatiallyExplicit>(a, grid, block, coop_grid, st);
+    case kWrappingNoise: return launch_step_t<kWrappingNoise>(a, grid, block, coop_grid, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+template <int KIND>
+static cudaError_t coop_occupancy_t(int *blocks_per_sm) {
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, coop_kernel<KIND, false>, kCoopBlock, 0);
+}
+
+cudaError_t coop_kernel_occupancy(int kind, int *blocks_per_sm) {
+    switch (kind) {
+    case kNonSpatial: return coop_occupancy_t<kNonSpatial>(blocks_per_sm);
+    case kSpatiallyImplicit: return coop_occupancy_t<kSpatiallyImplicit>(blocks_per_sm);
+    case kAlmostInfiniteNormal: return coop_occupancy_t<kAlmostInfiniteNormal>(blocks_per_sm);
+    case kSpatiallyExplicit: return coop_occupancy_t<kSpatiallyExplicit>(blocks_per_sm);
+    case kWrappingNoise: return coop_occupancy_t<kWrappingNoise>(blocks_per_sm);
     default: return cudaErrorInvalidValue;
     }
 }
@@ -1300,6 +1620,29 @@ __global__ void __launch_bounds__(256) hash_peak_kernel(uint64_t seed, uint32_t 
 cudaError_t launch_hash_peak(unsigned grid, uint64_t seed, uint32_t iters, unsigned long long *sink,
                              cudaStream_t st) {
     hash_peak_kernel<<<grid, 256, 0, st>>>(seed, iters, sink);
+    return cudaGetLastError();
+}
+
+// The AlmostInfinite displacements (dx, dy) before rounding for n pairs of
+// samples: Normal (kind kAlmostInfiniteNormal, a = sigma) or Clark2Dt (any
+// other kind, a = shape u, b = 1 / p), exactly as the step kernels compute them.
+__global__ void displacement_kernel(int32_t kind, const uint64_t *draws, uint64_t n, double a, double b,
+                                    double *dx, double *dy) {
+    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+         j += (uint64_t)gridDim.x * blockDim.x) {
+        double x, y;
+        if (kind == kAlmostInfiniteNormal)
+            normal_displacement(draws[2 * j], draws[2 * j + 1], a, x, y);
+        else
+            clark2dt_displacement(draws[2 * j], draws[2 * j + 1], a, b, x, y);
+        dx[j] = x;
+        dy[j] = y;
+    }
+}
+
+cudaError_t launch_displacements(int32_t kind, const uint64_t *draws, uint64_t n, double a, double b, double *dx,
+                                 double *dy, unsigned grid, cudaStream_t st) {
+    displacement_kernel<<<grid, 256, 0, st>>>(kind, draws, n, a, b, dx, dy);
     return cudaGetLastError();
 }
 

@@ -11,6 +11,8 @@
 namespace necsim {
 
 constexpr int kStepBlockMax = 256;
+// block size of the cooperative kernel (one lineage per warp)
+constexpr int kCoopBlock = 128;
 // simulations with at most this many live lineages run in the resident kernel
 constexpr int kResidentMax = 256;
 
@@ -34,6 +36,10 @@ struct StepArgs {
     uint32_t n_sims;                     // simulations in `params`
     TraceSink trace;                     // death records of speciated lineages (tracing only)
     uint32_t exp_sampler;                // 1: exponential event-time sampler (exp.rs), else Poisson
+    // Poisson sampler: rounds with at most this many live lineages run in
+    // the cooperative kernel (one warp per lineage, at most its resident
+    // warps); 0: the step kernel takes every round
+    uint64_t coop_max;
 };
 
 struct DedupArgs {
@@ -69,8 +75,14 @@ struct ScheduleArgs {
     unsigned int *n_resident;            // active simulations owned by the resident kernel
 };
 
-cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, cudaStream_t st);
+// the step kernel on grid x block and, for the Poisson sampler with
+// a.coop_max > 0, the cooperative kernel on coop_grid x kCoopBlock before it
+// (a.coop_max at most coop_grid's warps); each returns at once in the
+// other's rounds
+cudaError_t launch_step(int kind, const StepArgs &a, unsigned grid, unsigned block, unsigned coop_grid,
+                        cudaStream_t st);
 cudaError_t step_kernel_occupancy(int kind, bool exp_sampler, int block, int *blocks_per_sm);
+cudaError_t coop_kernel_occupancy(int kind, int *blocks_per_sm);
 cudaError_t launch_dedup(const DedupArgs &a, unsigned grid, unsigned block, cudaStream_t st);
 cudaError_t launch_schedule(const ScheduleArgs &a, cudaStream_t st);
 
@@ -93,6 +105,10 @@ struct ResidentArgs {
 
 cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st);
 cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st);
+// AlmostInfinite displacements before rounding (kind kAlmostInfiniteNormal: a =
+// sigma; else Clark2Dt: a = shape u, b = 1 / p) of n sample pairs
+cudaError_t launch_displacements(int32_t kind, const uint64_t *draws, uint64_t n, double a, double b, double *dx,
+                                 double *dy, unsigned grid, cudaStream_t st);
 // 8 * 256 * grid * iters wymum in independent chains (the hash-issue ceiling)
 cudaError_t launch_hash_peak(unsigned grid, uint64_t seed, uint32_t iters, unsigned long long *sink,
                              cudaStream_t st);

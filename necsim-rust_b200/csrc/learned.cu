@@ -9,6 +9,8 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <cstdint>
 
 #include "device_core.cuh"
@@ -413,16 +415,31 @@ __global__ void order_scatter_kernel(const unsigned long long *n_cur, uint64_t s
     }
 }
 
+// The current device's SM count, queried once per device; launch grids are
+// multiples of it.
+unsigned current_sm_count() {
+    constexpr int kMaxDevices = 64;
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 1;
+    int v = cache[dev].load();
+    if (v == 0) {
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v < 1) v = 1;
+        cache[dev].store(v);
+    }
+    return (unsigned)v;
+}
+
 }  // namespace
 
 cudaError_t launch_trace_snapshot(const FeatureArgs &f, TraceRow *rows, unsigned long long *n_rows, uint64_t cap,
                                   cudaStream_t st) {
-    trace_snapshot_kernel<<<148 * 4, 256, 0, st>>>(f, rows, n_rows, cap);
+    trace_snapshot_kernel<<<current_sm_count() * 4, 256, 0, st>>>(f, rows, n_rows, cap);
     return cudaGetLastError();
 }
 
 cudaError_t launch_lineage_predict(const FeatureArgs &f, const __nv_bfloat16 *w, float *pred_end, cudaStream_t st) {
-    lineage_predict_kernel<<<148 * 4, 256, 0, st>>>(f, w, pred_end);
+    lineage_predict_kernel<<<current_sm_count() * 4, 256, 0, st>>>(f, w, pred_end);
     return cudaGetLastError();
 }
 
@@ -437,7 +454,7 @@ cudaError_t launch_order(const FeatureArgs &f, const float *pred_end, uint8_t *k
 cudaError_t launch_mlp_predict(const __nv_bfloat16 *w, const float *X, uint64_t n, float *y, cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     uint64_t blocks = (n + 255) / 256;
-    if (blocks > 148 * 8) blocks = 148 * 8;
+    if (blocks > current_sm_count() * 8ULL) blocks = current_sm_count() * 8ULL;
     mlp_predict_kernel<<<(unsigned)blocks, 256, 0, st>>>(w, X, n, y);
     return cudaGetLastError();
 }
@@ -449,7 +466,7 @@ cudaError_t launch_mlp_grad(const __nv_bfloat16 *w, const float *X, const float 
     cudaError_t e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     uint64_t tiles = (n + kTile - 1) / kTile;
-    if (tiles > 148) tiles = 148;
+    if (tiles > current_sm_count()) tiles = current_sm_count();
     mlp_grad_kernel<<<(unsigned)tiles, kGradThreads, smem, st>>>(w, X, T, perm, offset, n, inv_n, grads, loss);
     return cudaGetLastError();
 }

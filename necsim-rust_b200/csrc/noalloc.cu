@@ -11,12 +11,13 @@
 // device array, sized for at most NECSIM_NOALLOC_MAX_LINEAGES lineages; the
 // caller passes device buffers for the input lineages and for the outputs.
 //
-// Every GPU that loads this library holds the array (about 8 MB) until the
+// Every GPU that loads this library holds the array (about 9.5 MB) until the
 // process exits.  All calls share it: the call clears what must start empty
 // (dedup table, counters) and two calls whose work overlaps on the GPU (on
 // different streams, or from different host threads) race on it.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 
@@ -54,10 +55,14 @@ constexpr uint64_t kScratchBytes = align256(kOffSlot + kMax * 4);
 // The working memory of every call of necsim_gpu_round_noalloc.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-// device address of g_noalloc_scratch per device, looked up on a device's
-// first call (cudaGetSymbolAddress; host code must not use the symbol itself)
+static_assert(kScratchBytes < 10u * 1024 * 1024, "the scratch array is documented as about 9.5 MB");
+
+// Per device, looked up on its first call: the device address of
+// g_noalloc_scratch (cudaGetSymbolAddress; host code must not use the
+// symbol itself) and the SM count the launch grids are sized by.
 constexpr int kMaxDevices = 64;
-unsigned char *g_scratch_ptr[kMaxDevices] = {nullptr};
+std::atomic<unsigned char *> g_scratch_ptr[kMaxDevices];
+std::atomic<int> g_sm_count[kMaxDevices];
 
 struct Carved {
     SimParams *params;
@@ -176,16 +181,26 @@ extern "C" int necsim_gpu_round_noalloc(const necsim_scenario *scenario, const n
     *steps = 0;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 
+    const uint32_t sampler = args ? args->event_time_sampler : NECSIM_SAMPLER_POISSON;
+    if (sampler != NECSIM_SAMPLER_POISSON && sampler != NECSIM_SAMPLER_EXP) return NECSIM_E_INVALID_ARGUMENT;
+    const bool exp_sampler = sampler == NECSIM_SAMPLER_EXP;
+
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return NECSIM_E_CUDA;
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev].load()) {
         // first call on this device: the device address of the scratch array
+        // and the device's SM count
         void *p = nullptr;
+        int sms = 0;
         if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return NECSIM_E_CUDA;
-        g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1)
+            return NECSIM_E_CUDA;
+        g_sm_count[dev].store(sms);
+        g_scratch_ptr[dev].store(static_cast<unsigned char *>(p));
     }
     if (n == 0) return NECSIM_OK;
-    const Carved c = carve(g_scratch_ptr[dev]);
+    const Carved c = carve(g_scratch_ptr[dev].load());
+    const unsigned sms = (unsigned)g_sm_count[dev].load();
 
     SimParams p = host_sim_params(*scenario, args, wyhash_seed);
     if (!(p.p0 > 0.0)) return NECSIM_E_UNSUPPORTED;
@@ -202,6 +217,16 @@ extern "C" int necsim_gpu_round_noalloc(const necsim_scenario *scenario, const n
     SimCounters counters;
     std::memset(&counters, 0, sizeof(counters));
 
+    // launch shapes from the kernels' occupancy on this device's SMs (host
+    // queries, no allocation)
+    constexpr unsigned kBlock = 128;
+    int step_per_sm = 0, coop_per_sm = 0;
+    if (step_kernel_occupancy(scenario->kind, exp_sampler, (int)kBlock, &step_per_sm) != cudaSuccess)
+        return NECSIM_E_CUDA;
+    if (!exp_sampler && coop_kernel_occupancy(scenario->kind, &coop_per_sm) != cudaSuccess) return NECSIM_E_CUDA;
+    const unsigned step_grid = sms * (unsigned)(step_per_sm > 0 ? step_per_sm : 1);
+    const unsigned coop_grid = sms * (unsigned)(coop_per_sm > 0 ? coop_per_sm : 1);
+
     // the array keeps the previous call's contents: reset what must start
     // empty (dedup table, counters, control words) on the caller's stream
     if (cudaMemcpyAsync(c.params, &p, sizeof(p), cudaMemcpyHostToDevice, st) != cudaSuccess ||
@@ -211,7 +236,7 @@ extern "C" int necsim_gpu_round_noalloc(const necsim_scenario *scenario, const n
         cudaMemsetAsync(c.min_gref, 0xff, mask * sizeof(unsigned long long), st) != cudaSuccess)
         return NECSIM_E_CUDA;
 
-    load_lineages_kernel<<<256, 256, 0, st>>>(d_lineages, n, c.a, c.state_a);
+    load_lineages_kernel<<<sms * 2, 256, 0, st>>>(d_lineages, n, c.a, c.state_a);
 
     StepArgs sa;
     std::memset(&sa, 0, sizeof(sa));
@@ -228,7 +253,9 @@ extern "C" int necsim_gpu_round_noalloc(const necsim_scenario *scenario, const n
     sa.status = reinterpret_cast<uint32_t *>(&c.ctl[kCtlStatus]);
     sa.steps_total = &c.ctl[kCtlSteps];
     sa.n_sims = 1;
-    if (launch_step(scenario->kind, sa, 148 * 4, 128, st) != cudaSuccess) return NECSIM_E_CUDA;
+    sa.exp_sampler = exp_sampler ? 1u : 0u;
+    sa.coop_max = exp_sampler ? 0 : (uint64_t)coop_grid * (kCoopBlock / 32);
+    if (launch_step(scenario->kind, sa, step_grid, kBlock, coop_grid, st) != cudaSuccess) return NECSIM_E_CUDA;
 
     DedupArgs da;
     std::memset(&da, 0, sizeof(da));
@@ -244,9 +271,9 @@ extern "C" int necsim_gpu_round_noalloc(const necsim_scenario *scenario, const n
     da.out_count = &c.ctl[kCtlOut];
     da.counters = c.counters;
     da.status = reinterpret_cast<uint32_t *>(&c.ctl[kCtlStatus]);
-    if (launch_dedup(da, 148 * 2, 256, st) != cudaSuccess) return NECSIM_E_CUDA;
+    if (launch_dedup(da, sms * 2, 256, st) != cudaSuccess) return NECSIM_E_CUDA;
 
-    store_lineages_kernel<<<256, 256, 0, st>>>(c.b, &c.ctl[kCtlOut], d_out, &c.counters->steps);
+    store_lineages_kernel<<<sms * 2, 256, 0, st>>>(c.b, &c.ctl[kCtlOut], d_out, &c.counters->steps);
     if (cudaGetLastError() != cudaSuccess) return NECSIM_E_CUDA;
 
     unsigned long long back[kControlWords];

@@ -394,24 +394,29 @@ static inline void clamp_round_dispersal(uint32_t x, uint32_t y, double dx, doub
 }
 
 /* rng.rs:180-197 sample_2d_normal via Box-Muller; almost_infinite_normal.rs:58-68 */
-static inline void normal_disperse_from_draws(uint64_t d0, uint64_t d1, double sigma, uint32_t x,
-                                              uint32_t y, uint32_t *tx, uint32_t *ty) {
+static inline void normal_displacement(uint64_t d0, uint64_t d1, double sigma, double *dx, double *dy) {
     double u0 = (double)((d0 >> 11) + 1) * 0x1.0p-53;
     double u1 = (double)(d1 >> 11) * 0x1.0p-53;
     double r = sqrt(-2.0 * log(u0));
     double theta = -6.283185307179586 * u1;
     double z0 = r * sin(theta);
     double z1 = r * cos(theta);
-    double dx = z0 * sigma + 0.0;
-    double dy = z1 * sigma + 0.0;
+    *dx = z0 * sigma + 0.0;
+    *dy = z1 * sigma + 0.0;
+}
+
+static inline void normal_disperse_from_draws(uint64_t d0, uint64_t d1, double sigma, uint32_t x,
+                                              uint32_t y, uint32_t *tx, uint32_t *ty) {
+    double dx, dy;
+    normal_displacement(d0, d1, sigma, &dx, &dy);
     clamp_round_dispersal(x, y, dx, dy, tx, ty);
 }
 
 /* almost_infinite_clark2dt.rs:96-107 with clark2dt::cdf_inverse and
  * pow_fast_one (:167-189): jump = sqrt(u * (pow(1 / (1 - u01), 1 / p) - 1)),
  * theta = u2 * 2 * pi, (dx, dy) = (cos(theta) * jump, sin(theta) * jump) */
-static inline void clark2dt_disperse_from_draws(uint64_t d0, uint64_t d1, double shape_u, double tail_p,
-                                                uint32_t x, uint32_t y, uint32_t *tx, uint32_t *ty) {
+static inline void clark2dt_displacement(uint64_t d0, uint64_t d1, double shape_u, double tail_p, double *dx,
+                                         double *dy) {
     double u01 = (double)(d0 >> 11) * 0x1.0p-53;
     double u2 = (double)((d1 >> 11) + 1) * 0x1.0p-53;
     double expo = 1.0 / tail_p;
@@ -419,8 +424,14 @@ static inline void clark2dt_disperse_from_draws(uint64_t d0, uint64_t d1, double
     double powed = (expo == 1.0) ? base : pow(base, expo);
     double jump = sqrt(shape_u * (powed - 1.0));
     double theta = u2 * 2.0 * 3.141592653589793;
-    double dx = cos(theta) * jump;
-    double dy = sin(theta) * jump;
+    *dx = cos(theta) * jump;
+    *dy = sin(theta) * jump;
+}
+
+static inline void clark2dt_disperse_from_draws(uint64_t d0, uint64_t d1, double shape_u, double tail_p,
+                                                uint32_t x, uint32_t y, uint32_t *tx, uint32_t *ty) {
+    double dx, dy;
+    clark2dt_displacement(d0, d1, shape_u, tail_p, &dx, &dy);
     clamp_round_dispersal(x, y, dx, dy, tx, ty);
 }
 
@@ -432,6 +443,16 @@ void oracle_clark2dt_dispersal(uint64_t draw0, uint64_t draw1, double shape_u, d
 void oracle_normal_dispersal(uint64_t draw0, uint64_t draw1, double sigma, uint32_t x, uint32_t y,
                              uint32_t *tx, uint32_t *ty) {
     normal_disperse_from_draws(draw0, draw1, sigma, x, y, tx, ty);
+}
+
+void oracle_displacements(int32_t kind, const uint64_t *draws, uint64_t n, double a, double b, double *dx,
+                          double *dy) {
+    for (uint64_t j = 0; j < n; ++j) {
+        if (kind == ORACLE_ALMOST_INFINITE_CLARK2DT)
+            clark2dt_displacement(draws[2 * j], draws[2 * j + 1], a, b, &dx[j], &dy[j]);
+        else
+            normal_displacement(draws[2 * j], draws[2 * j + 1], a, &dx[j], &dy[j]);
+    }
 }
 
 /* ------------------------------------------------------------------------ */

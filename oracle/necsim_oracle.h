@@ -183,6 +183,11 @@ void oracle_clark2dt_dispersal(uint64_t draw0, uint64_t draw1, double shape_u, d
                                uint32_t y, uint32_t *tx, uint32_t *ty);
 void oracle_normal_dispersal(uint64_t draw0, uint64_t draw1, double sigma, uint32_t x, uint32_t y,
                              uint32_t *tx, uint32_t *ty);
+/* The raw displacements (dx, dy) before rounding, from n draw pairs: kind
+ * ORACLE_ALMOST_INFINITE_NORMAL (a = sigma) or ORACLE_ALMOST_INFINITE_CLARK2DT
+ * (a = shape u, b = tail p), with the C library's log/sin/cos/pow. */
+void oracle_displacements(int32_t kind, const uint64_t *draws, uint64_t n, double a, double b, double *dx,
+                          double *dy);
 
 /* WrappingNoise: the octave noise at (x, y) (sum_noise_octaves), the
  * habitat threshold of WrappingNoiseHabitat::new, and the self-dispersal

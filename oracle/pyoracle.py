@@ -182,6 +182,8 @@ def lib():
                                               ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                               ctypes.POINTER(ctypes.c_uint32)]
         L.oracle_normal_dispersal.restype = None
+        L.oracle_displacements.argtypes = [ctypes.c_int32, vp, u64, ctypes.c_double, ctypes.c_double, vp, vp]
+        L.oracle_displacements.restype = None
         L.oracle_clark2dt_dispersal.argtypes = [u64, u64, ctypes.c_double, ctypes.c_double, ctypes.c_uint32,
                                                 ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                                 ctypes.POINTER(ctypes.c_uint32)]
@@ -385,6 +387,18 @@ def normal_dispersal(d0, d1, sigma, x, y):
     ty = ctypes.c_uint32(0)
     lib().oracle_normal_dispersal(d0, d1, sigma, x, y, ctypes.byref(tx), ctypes.byref(ty))
     return tx.value, ty.value
+
+
+def displacements(kind, draws, a, b=0.0):
+    """Raw AlmostInfinite displacements (dx, dy) with the C library's
+    log/sin/cos/pow: kind ALMOST_INFINITE_NORMAL (a = sigma) or
+    ALMOST_INFINITE_CLARK2DT (a = shape u, b = tail p); draws is [n, 2] u64."""
+    d = np.ascontiguousarray(draws, dtype=np.uint64)
+    n = d.shape[0]
+    dx = np.empty(n, dtype=np.float64)
+    dy = np.empty(n, dtype=np.float64)
+    lib().oracle_displacements(kind, d.ctypes.data, n, a, b, dx.ctypes.data, dy.ctypes.data)
+    return dx, dy
 
 
 def distinct_speciation_set(events):

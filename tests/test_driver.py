@@ -235,9 +235,13 @@ def test_check_reads_tiff_maps(nb, syn, tmp_path):
     assert r.returncode == 1 and "bitwidth" in r.stderr
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference/maps/test"), reason="reference map fixtures not present")
+REF_MAPS = os.environ.get("NECSIM_REFERENCE_MAPS", "")
+
+
+@pytest.mark.skipif(not REF_MAPS or not os.path.isdir(os.path.join(REF_MAPS, "test")),
+                    reason="set NECSIM_REFERENCE_MAPS to the reference's maps/ folder")
 def test_check_reads_the_reference_fixture(nb, tmp_path):
-    cfg = (SE_CONFIG % ("/root/reference/maps/test/habitat.tif", "/root/reference/maps/test/dispersal.tif", "")
+    cfg = (SE_CONFIG % (os.path.join(REF_MAPS, "test", "habitat.tif"), os.path.join(REF_MAPS, "test", "dispersal.tif"), "")
            ).replace("percentage: 1.0", "percentage: 0.01")
     r = run_driver(nb, "check", cfg, tmp_path)
     assert r.returncode == 0, r.stderr

@@ -14,8 +14,9 @@ import numpy as np
 import pytest
 import tiff_util
 
-REF_MAPS = "/root/reference/maps"
-needs_fixtures = pytest.mark.skipif(not os.path.isdir(REF_MAPS), reason="reference map fixtures not present")
+REF_MAPS = os.environ.get("NECSIM_REFERENCE_MAPS", "")
+needs_fixtures = pytest.mark.skipif(not REF_MAPS or not os.path.isdir(REF_MAPS),
+                                    reason="set NECSIM_REFERENCE_MAPS to the reference's maps/ folder")
 
 
 @needs_fixtures

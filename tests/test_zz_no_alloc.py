@@ -8,8 +8,11 @@ one round and merges duplicates, using a working area that lives in the
 library.  The existing necsim_gpu_simulate_lineages reaches the same horizon
 in several rounds; both must leave the same surviving lineages (state and
 smallest global reference) and the same distinct speciation events, bit for
-bit.  Two calls in a row check that the shared working area is reset between
-calls.  This file sorts last so a failure here does not hide other results.
+bit.  The oracle's canonical schedule run to the same horizon in one round
+pins the round itself: the same surviving lineages, the same speciation
+events and exactly the same number of executed events.  Two calls in a row
+check that the shared working area is reset between calls.  This file sorts
+last so a failure here does not hide other results.
 """
 import ctypes
 
@@ -35,7 +38,7 @@ def _bind(nb):
     return L
 
 
-def _round(nb, torch, scenario_struct, seed_word, lineages, resume_time, horizon):
+def _round(nb, torch, scenario_struct, seed_word, lineages, resume_time, horizon, sampler="poisson"):
     L = _bind(nb)
     n = len(lineages)
     d_in = _device_bytes(torch, np.ascontiguousarray(lineages, dtype=nb.LINEAGE_DTYPE))
@@ -44,7 +47,7 @@ def _round(nb, torch, scenario_struct, seed_word, lineages, resume_time, horizon
     n_out = ctypes.c_uint64(0)
     n_ev = ctypes.c_uint64(0)
     steps = ctypes.c_uint64(0)
-    args = nb.CArgs()
+    args = nb._args_struct(nb.CUDA(event_time_sampler=sampler))
     torch.cuda.synchronize()
     rc = L.necsim_gpu_round_noalloc(ctypes.byref(scenario_struct), ctypes.byref(args), seed_word,
                                     d_in.data_ptr(), n, resume_time, horizon, d_out.data_ptr(),
@@ -67,35 +70,78 @@ def _same_lineages(a, b):
                                b["last_event_time"].view(np.uint64)))
 
 
-@pytest.mark.parametrize("scenario", ["non_spatial", "almost_infinite"])
-def test_round_noalloc_matches_existing_entry_point(nb, scenario):
+SCENARIOS = {
+    "non_spatial": (dict(kind=0, speciation_probability=2e-3, width=40, height=40, deme=4), 11),
+    "spatially_implicit": (dict(kind=1, speciation_probability=1e-3, width=3000, height=1, deme=1,
+                                meta_width=100000, meta_height=1, meta_deme=1, migration_probability=0.1), 5),
+    "almost_infinite": (dict(kind=2, speciation_probability=2e-3, sigma=5.0, radius=30, centre_x=1 << 31,
+                             centre_y=1 << 31), 11),
+}
+
+
+def _one_round_oracle(oracle, desc, seed, sampler, lineages, resume_time, horizon):
+    """The canonical schedule with a round that reaches `horizon` at once."""
+    code = oracle.SAMPLER_EXP if sampler == "exp" else oracle.SAMPLER_POISSON
+    return oracle.simulate(desc, seed, mode=oracle.MODE_CANONICAL, lineages=lineages, resume_time=resume_time,
+                           pause_before=horizon, step_slice=1000, step_slice_max=1000, min_round_events=1,
+                           event_time_sampler=code)
+
+
+def _same_events(a, b):
+    key = ["gref", "x", "y", "index"]
+    a = np.sort(a, order=key)
+    b = np.sort(b, order=key)
+    return len(a) == len(b) and all(np.array_equal(a[f], b[f]) for f in key) and all(
+        np.array_equal(a[f].view(np.uint64), b[f].view(np.uint64)) for f in ("prior_time", "event_time"))
+
+
+@pytest.mark.parametrize("sampler", ["poisson", "exp"])
+@pytest.mark.parametrize("scenario", sorted(SCENARIOS))
+def test_round_noalloc_matches_existing_entry_point(nb, syn, oracle, scenario, sampler):
     torch = pytest.importorskip("torch")
-    if scenario == "non_spatial":
-        sc, nu = nb.NonSpatial((40, 40), 4), 2e-3
-    else:
-        sc, nu = nb.AlmostInfinite(nb.Circle(30, (1 << 31, 1 << 31)), nb.Normal(5.0)), 2e-3
-    seed = 11
+    desc, seed = SCENARIOS[scenario]
+    sc, nu = syn.to_scenario(desc), desc["speciation_probability"]
     word = nb.seed_from_u64(seed)
     struct = nb._scenario_struct(sc, nu)
     origins = nb.enumerate_origins(sc, nu)
     assert 0 < len(origins) <= 65536
+    algo = nb.CUDA(event_time_sampler=sampler)
 
     # first call: origins -> horizon 60
-    out1, ev1, steps1 = _round(nb, torch, struct, word, origins, 0.0, 60.0)
-    with nb.Simulation(sc, nu) as sim:
+    out1, ev1, steps1 = _round(nb, torch, struct, word, origins, 0.0, 60.0, sampler)
+    with nb.Simulation(sc, nu, algo) as sim:
         ref1 = sim.resume(origins, 0.0, seed, pause_before=60.0)
     assert _same_lineages(out1, ref1.remaining)
     assert np.array_equal(nb.distinct_speciation_set(ev1),
                           nb.distinct_speciation_set(ref1.speciation))
-    assert steps1 >= ref1.steps > 0
+    c1 = _one_round_oracle(oracle, desc, seed, sampler, origins, 0.0, 60.0)
+    assert c1.n_rounds == 1 and steps1 == c1.steps > 0
+    assert _same_lineages(out1, c1.remaining) and _same_events(ev1, c1.speciation)
 
     # second call in a row reuses the working area: survivors -> horizon 150
-    out2, ev2, _ = _round(nb, torch, struct, word, out1, 60.0, 150.0)
-    with nb.Simulation(sc, nu) as sim:
+    out2, ev2, steps2 = _round(nb, torch, struct, word, out1, 60.0, 150.0, sampler)
+    with nb.Simulation(sc, nu, algo) as sim:
         ref2 = sim.resume(ref1.remaining, 60.0, seed, pause_before=150.0)
     assert _same_lineages(out2, ref2.remaining)
     assert np.array_equal(nb.distinct_speciation_set(ev2),
                           nb.distinct_speciation_set(ref2.speciation))
+    c2 = _one_round_oracle(oracle, desc, seed, sampler, out1, 60.0, 150.0)
+    assert c2.n_rounds == 1 and steps2 == c2.steps > 0
+    assert _same_lineages(out2, c2.remaining) and _same_events(ev2, c2.speciation)
+
+
+def test_round_noalloc_rejects_an_unknown_sampler(nb):
+    torch = pytest.importorskip("torch")
+    L = _bind(nb)
+    struct = nb._scenario_struct(nb.NonSpatial((10, 10), 1), 0.01)
+    args = nb.CArgs()
+    args.event_time_sampler = 7
+    n_out, n_ev, steps = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint64(0)
+    buf = torch.zeros(64 * 40, dtype=torch.uint8, device="cuda")
+    p = buf.data_ptr()
+    rc = L.necsim_gpu_round_noalloc(ctypes.byref(struct), ctypes.byref(args), 1, p, 1, 0.0, 10.0, p,
+                                    ctypes.byref(n_out), p, 1, ctypes.byref(n_ev), ctypes.byref(steps), None)
+    assert rc == -1  # NECSIM_E_INVALID_ARGUMENT
 
 
 def test_round_noalloc_rejects_too_many_lineages(nb):
