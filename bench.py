@@ -382,6 +382,17 @@ def issue_roofline(nb, device, work, events, kernel_ms, launches, workload_name)
             "work_source": "canonical-schedule oracle, " + work["sample"]}
 
 
+def roofline_entry(nb, device, sims, algo, pause, threads, sampler, events, kernel_ms, launches, name):
+    """The `roofline` key: the canonical-schedule work count and the
+    integer-issue roofline, or the error that prevented them (never fatal to
+    the benchmark line)."""
+    try:
+        work = canonical_work(sims, algo, pause, threads, sampler)
+        return issue_roofline(nb, device, work, events, kernel_ms, launches, name)
+    except Exception as e:
+        return {"error": "%s: %s" % (type(e).__name__, e)}
+
+
 def host_cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -573,12 +584,9 @@ def main():
         line["same_slice"] = {"value": sum(o.steps for o in so) / (so[0].total_ms / 1e3), "unit": UNIT,
                               "pause_before": args.cpu_sample_pause, "events": sum(o.steps for o in so),
                               "ms": so[0].total_ms, "schedule": "plain"}
-    try:
-        work = canonical_work(sims, plain_algo, args.cpu_sample_pause, threads, args.event_time_sampler)
-        line["roofline"] = issue_roofline(nb, device, work, steps, head["kernel_ms"], head["step_launches"],
-                                          args.workload)
-    except Exception as e:  # reported, never fatal to the benchmark line
-        line["roofline"] = {"error": "%s: %s" % (type(e).__name__, e)}
+    line["roofline"] = roofline_entry(nb, device, sims, plain_algo, args.cpu_sample_pause, threads,
+                                      args.event_time_sampler, steps, head["kernel_ms"], head["step_launches"],
+                                      args.workload)
     if dist.rank == 0 and dist.world == 1 and args.workload == "c4" and not args.no_secondary:
         line["secondary"] = {
             "c3": secondary(nb, "c3", None, device, threads, args.event_time_sampler, ""),

@@ -1097,7 +1097,7 @@ __device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long l
 // lineages gets one lineage per warp, so lineages never share (and diverge
 // within) a warp until there are more than eight of them.
 template <int KIND, int THREADS, bool EXP>
-__global__ void __launch_bounds__(THREADS) resident_kernel(ResidentArgs a) {
+__global__ void __launch_bounds__(THREADS, 1) resident_kernel(ResidentArgs a) {
     constexpr unsigned kWarps = THREADS / 32;
     constexpr unsigned kSlots = THREADS;  // lineage slots (>= kResidentMax)
     __shared__ uint32_t sx[kSlots], sy[kSlots], si[kSlots];

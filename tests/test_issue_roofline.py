@@ -1,6 +1,7 @@
-"""The benchmark's integer-issue roofline: the step kernel's algorithmic
-WyHash mixing work (wymum per event, from the reference restatement's prime
-and draw counts) against the measured rate of independent wymum chains."""
+"""The benchmark's integer-issue roofline: the round kernels' algorithmic
+WyHash mixing work (wymum per event, from the oracle's prime and draw counts
+on the canonical schedule the kernels run) against the measured rate of
+independent wymum chains."""
 import types
 
 import pytest
@@ -18,12 +19,19 @@ def test_counts_per_event_from_the_reference_sample():
     assert 2.0 < primes < 5.0 and 4.0 < draws < 10.0
 
 
+def test_canonical_work_counts(nb):
+    import bench
+    _, sims = bench.workload("c1")
+    w = bench.canonical_work(sims, nb.CUDA(), 30.0, 2, "poisson")
+    assert w["steps"] > 0 and 2.0 < w["primes"] / w["steps"] < 5.0 and 4.0 < w["draws"] / w["steps"] < 10.0
+    assert "1 of 1 simulation(s) to t=30" in w["sample"]
+
+
 def test_roofline_entry_is_never_fatal(nb):
     import bench
     _, sims = bench.workload("c1")
-    args = types.SimpleNamespace(event_time_sampler="poisson")
     broken = types.SimpleNamespace(hash_peak=lambda device: (_ for _ in ()).throw(RuntimeError("no GPU")))
-    out = bench.issue_roofline(broken, sims, args, 0, {}, 1000, 1.0)
+    out = bench.roofline_entry(broken, 0, sims, nb.CUDA(), 20.0, 2, "poisson", 1000, 1.0, 10, "c1")
     assert set(out) == {"error"} and "no GPU" in out["error"]
 
 
@@ -33,8 +41,7 @@ def test_hash_peak_and_roofline(nb):
     peak = nb.hash_peak(0)
     assert 1e10 < peak < 1e14
     _, sims = bench.workload("c1")
-    args = types.SimpleNamespace(event_time_sampler="poisson")
-    out = bench.issue_roofline(nb, sims, args, 0, {}, 2_500_000, 10.0)
+    out = bench.roofline_entry(nb, 0, sims, nb.CUDA(), 30.0, 2, "poisson", 2_500_000, 10.0, 100, "c1")
     assert out["bound"] == "integer-issue" and 0.0 < out["frac"] < 1.5
     assert 10.0 < out["wymum_per_event"] < 20.0
 
