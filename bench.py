@@ -70,6 +70,9 @@ def parse():
                    help="pause_before of the trace runs that train the lifetime model")
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--once", action="store_true",
+                   help="profiling aid: one run of the workload's batch (plain schedule), then print its "
+                        "events and device time; no timing arms, baselines or training")
     p.add_argument("--no-secondary", action="store_true",
                    help="skip the secondary workloads (C3 in full, C5 to t=400) beside the sweep")
     p.add_argument("--pause", type=float, default=None,
@@ -472,6 +475,15 @@ def main():
     nus = [d["speciation_probability"] for d, _ in sims]
     seeds = [s for _, s in sims]
     device = dist.local_rank if dist.world > 1 else 0
+    if args.once:
+        with nb.Batch(scen, nus, seeds, nb.CUDA(device=device, event_time_sampler=args.event_time_sampler),
+                      pause_before=args.pause) as b:
+            outs = b.run()
+        print(json.dumps({"workload": args.workload, "pause_before": args.pause,
+                          "events": sum(o.steps for o in outs), "ms": outs[0].total_ms,
+                          "rounds": outs[0].n_step_launches}), flush=True)
+        dist.close()
+        return
     se = sims[0][0]["kind"] == 3
     kind = sims[0][0]["kind"]
 

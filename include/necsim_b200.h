@@ -127,12 +127,13 @@ typedef struct necsim_args {
                                   would exceed the buffer (2x the round's expected events) */
     int32_t device;            /* CUDA device ordinal; default 0 */
     uint32_t rounds_per_graph; /* rounds captured per CUDA graph launch; 0 = default (16) */
-    uint32_t resident;         /* 1: in a batch, simulations with at most 256 live lineages leave
-                                  the global rounds for the per-simulation resident kernel (one
-                                  block each, its own rounds); default 0: every simulation stays
-                                  in the global rounds, whose sparse rounds step each lineage with
-                                  a whole warp (faster on every measured workload); same results
-                                  either way; a run of one simulation always stays global */
+    uint32_t resident;         /* in a batch, simulations that start a round with few live lineages
+                                  leave the global rounds for the per-simulation resident kernel (one
+                                  block each, running its own rounds beside the global ones): 1 routes
+                                  at 8 lineages (one warp of the block per lineage, each stepped
+                                  cooperatively), 2..256 at that many; default 0: every simulation
+                                  stays in the global rounds; same results either way; a run of one
+                                  simulation always stays global */
     uint32_t event_time_sampler; /* NECSIM_SAMPLER_POISSON (0, default): PoissonEventTimeSampler,
                                     the Independent algorithm's (event_time_sampler/poisson.rs);
                                     NECSIM_SAMPLER_EXP (1): ExpEventTimeSampler, the CUDA

@@ -407,7 +407,9 @@ class CUDA:
     schedule: str = "plain"   # or "learned" (needs `model`)
     device: int = 0
     rounds_per_graph: int = 16
-    resident: bool = False    # batches: small simulations move to the per-simulation resident kernel
+    # batches: simulations with few live lineages move to the per-simulation
+    # resident kernel (True: at 8 lineages; an int 2..256: at that many)
+    resident: Union[bool, int] = False
     model: Optional["LifetimeModel"] = None
     # reporters consume dispersal events (ReportDispersal): the events leave
     # the device after every round (global rounds only, no CUDA graphs)
@@ -574,7 +576,7 @@ def _args_struct(algorithm: CUDA):
     a.report_dispersal = 1 if algorithm.report_dispersal else 0
     a.device = algorithm.device
     a.rounds_per_graph = algorithm.rounds_per_graph
-    a.resident = 1 if algorithm.resident else 0
+    a.resident = int(algorithm.resident) if algorithm.resident is not True else 1
     if algorithm.event_time_sampler not in EVENT_TIME_SAMPLERS:
         raise ValueError("event_time_sampler must be 'poisson' or 'exp'")
     a.event_time_sampler = EVENT_TIME_SAMPLERS[algorithm.event_time_sampler]

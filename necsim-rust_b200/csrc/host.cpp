@@ -914,6 +914,60 @@ void for_each_origin(const necsim_scenario &sc, F &&push) {
     }
 }
 
+// ---- per-simulation priority of the learned schedule ----
+
+// The lifetime model's score of each simulation: the largest predicted
+// remaining event count (expm1 of the model's output) over up to 32 of its
+// origin lineages, evenly spaced in origin order, at the start of the run
+// (no event executed, the simulation's origin count live).  The features are
+// the kernels' (lineage_features_of), with a SpatiallyExplicit cell's
+// habitat and dispersal entropy read from the maps.
+std::vector<float> score_simulations(necsim_model *m, const std::vector<SimHost> &sims) {
+    constexpr uint64_t kSample = 32;
+    std::vector<float> X;
+    std::vector<uint32_t> owner;
+    for (size_t s = 0; s < sims.size(); ++s) {
+        const SimHost &sh = sims[s];
+        const int kind = sh.sc.kind == NECSIM_ALMOST_INFINITE_CLARK2DT ? NECSIM_ALMOST_INFINITE_NORMAL : sh.sc.kind;
+        const uint64_t stride = std::max<uint64_t>(1, sh.n_origins / kSample);
+        uint64_t k = 0;
+        for_each_origin(sh.sc, [&](uint32_t x, uint32_t y, uint32_t, uint64_t) {
+            if (k++ % stride) return;
+            float hab = 1.f, ent = 0.f;
+            if (kind == NECSIM_SPATIALLY_EXPLICIT) {
+                const uint64_t cell = (uint64_t)y * sh.sc.width + x;
+                hab = (float)sh.sc.habitat[cell];
+                ent = dispersal_entropy(sh.sc, cell);
+            }
+            float f[kFeat];
+            lineage_features_of(kind, sh.params, sh.n_origins, x, y, 0.0, 0, hab, ent, f);
+            X.insert(X.end(), f, f + kFeat);
+            owner.push_back((uint32_t)s);
+        });
+    }
+    std::vector<float> score(sims.size(), 0.f);
+    const uint64_t n = owner.size();
+    if (n == 0) return score;
+    CK(cudaSetDevice(m->device));
+    struct Res {
+        float *x = nullptr, *y = nullptr;
+        ~Res() {
+            if (x) cudaFree(x);
+            if (y) cudaFree(y);
+        }
+    } r;
+    r.x = dev_alloc<float>(n * kFeat);
+    r.y = dev_alloc<float>(n);
+    CK(cudaMemcpyAsync(r.x, X.data(), n * kFeat * sizeof(float), cudaMemcpyHostToDevice, m->stream));
+    CK(launch_mlp_predict(m->w, r.x, n, r.y, m->stream));
+    std::vector<float> y(n);
+    CK(cudaMemcpyAsync(y.data(), r.y, n * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    for (uint64_t j = 0; j < n; ++j)
+        score[owner[j]] = std::max(score[owner[j]], std::expm1(std::min(std::max(y[j], 0.f), 40.f)));
+    return score;
+}
+
 // Builds the origin lineages of every simulation on the host, in the
 // reference's origin-sampler order, and uploads them as structure of arrays.
 void upload_origins(Engine &E, const std::vector<std::vector<necsim_lineage>> *given) {
@@ -1042,7 +1096,14 @@ DedupArgs make_dedup_args(Engine &E, DeviceLineages &in, DeviceLineages &out) {
     a.out_count = &E.d_ctl->out_count;
     a.counters = E.d_counters;
     a.status = &E.d_ctl->status;
-    if (E.args.resident) a.arena = E.R.soa;  // route small simulations to the arena
+    if (E.args.resident) {
+        // route small simulations to the arena: resident == 1 routes at one
+        // lineage per warp of the resident block (every routed lineage is
+        // stepped cooperatively), larger values at that many lineages
+        a.arena = E.R.soa;
+        a.resident_max = E.args.resident == 1 ? (uint64_t)(kResidentMax / 32)
+                                              : std::min<uint64_t>(E.args.resident, kResidentMax);
+    }
     a.params = E.d_params;
     if (E.tracing) {
         a.trace.deaths = E.trace_deaths;

@@ -1395,7 +1395,7 @@ __global__ void dedup_compact_kernel(DedupArgs a) {
         // kResidentMax lineages move to its segment of the resident arena
         // (the resident kernel owns the simulation from the next round on)
         const bool to_arena = survivor && a.arena.x != nullptr &&
-                              a.counters[s].n_live <= (unsigned long long)kResidentMax;
+                              a.counters[s].n_live <= (unsigned long long)a.resident_max;
         const bool to_out = survivor && !to_arena;
         const unsigned sv = __ballot_sync(kFull, to_out);
         unsigned long long dst_base = 0;

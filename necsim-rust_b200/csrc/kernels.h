@@ -44,6 +44,7 @@ struct StepArgs {
 
 struct DedupArgs {
     LineageSoA arena;                    // resident arena (x == nullptr: no routing)
+    uint64_t resident_max;               // route simulations that start a round with at most this many (<= kResidentMax)
     const SimParams *params;             // lineage_offset of each simulation
     LineageSoA in;
     LineageSoA out;

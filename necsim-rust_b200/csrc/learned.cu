@@ -22,65 +22,19 @@ namespace {
 
 constexpr unsigned kFullMask = 0xffffffffu;
 
-// The eight features of a lineage, each scaled to about [0, 1]:
-//   0, 1  position in the scenario's extent (x / width, y / height; the
-//         metacommunity's own extent for an SI lineage outside the local
-//         community; 0 on the unbounded AlmostInfinite plane)
-//   2     log(1 + habitat at the location) / 8 (deme size)
-//   3     entropy (nats) of the location's dispersal distribution / 16
-//   4     log(1 + time of the lineage's last event) / 20
-//   5     -log10(speciation probability per event at the location) / 15
-//         (SI local community: speciation happens after migration, nu * m)
-//   6     log(1 + live lineages of the simulation) / 16 (crowding)
-//   7     log(1 + events the lineage has executed) / 20 (age)
+// The features of a lineage (lineage_features_of, learned.h), reading the
+// SpatiallyExplicit cell's habitat and dispersal entropy from the tables.
 __device__ void lineage_features(int kind, const SimParams &p, const SimCounters &c, uint32_t x, uint32_t y,
                                  double last, uint64_t steps, float f[kFeat]) {
-    float fx = 0.f, fy = 0.f, hab = 1.f, ent = 0.f;
-    float nu = (float)p.nu;
-    if (kind == kNonSpatial) {
-        fx = (float)x / (float)p.width;
-        fy = (float)y / (float)p.height;
-        hab = (float)p.deme;
-        ent = logf((float)p.width * (float)p.height);
-    } else if (kind == kSpatiallyImplicit) {
-        if (in_local(p, x, y)) {
-            fx = (float)x / (float)p.width;
-            fy = (float)y / (float)p.height;
-            hab = (float)p.deme;
-            ent = logf((float)p.width * (float)p.height);
-            nu *= (float)p.migration;
-        } else {
-            fx = (float)(x - p.meta_ox) / (float)p.meta_width;
-            fy = (float)(y - p.meta_oy) / (float)p.meta_height;
-            hab = (float)p.meta_deme;
-            ent = logf((float)p.meta_width * (float)p.meta_height);
-        }
-    } else if (kind == kAlmostInfiniteNormal) {
-        // differential entropy of the 2D dispersal kernel: normal, or a
-        // Clark2Dt kernel of scale sqrt(u) (sigma 0: none)
-        const float scale2 = p.clark ? (float)p.clark_shape_u : (float)p.sigma * (float)p.sigma;
-        ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2, 1.0f));
-    } else if (kind == kWrappingNoise) {
-        // the Normal kernel's entropy, restricted to the habitable share
-        const float scale2 = (float)p.sigma * (float)p.sigma;
-        ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2 * (float)p.noise.coverage, 1.0f));
-    } else {
-        fx = (float)x / (float)p.width;
-        fy = (float)y / (float)p.height;
+    float hab = 1.f, ent = 0.f;
+    if (kind == kSpatiallyExplicit) {
         const uint64_t cell = (uint64_t)y * p.width + x;
         if (cell < p.n_cells) {
             hab = (float)p.cells[cell].habitat;
             ent = p.cell_entropy ? p.cell_entropy[cell] : 0.f;
         }
     }
-    f[0] = fx;
-    f[1] = fy;
-    f[2] = log1pf(hab) * 0.125f;
-    f[3] = ent * 0.0625f;
-    f[4] = log1pf((float)last) * 0.05f;
-    f[5] = -log10f(fmaxf(nu, 1e-15f)) * (1.0f / 15.0f);
-    f[6] = log1pf((float)c.n_live) * 0.0625f;
-    f[7] = log1pf((float)steps) * 0.05f;
+    lineage_features_of(kind, p, c.n_live, x, y, last, steps, hab, ent, f);
 }
 
 __device__ __forceinline__ void stage_weights(const __nv_bfloat16 *w, float *Ws) {

@@ -8,6 +8,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 
 #include "layout.h"
@@ -63,6 +64,68 @@ struct FeatureArgs {
     int kind;
     uint64_t skip_at_most;  // rounds with at most this many live lineages need no order
 };
+
+// The eight features of a lineage, each scaled to about [0, 1]:
+//   0, 1  position in the scenario's extent (x / width, y / height; the
+//         metacommunity's own extent for an SI lineage outside the local
+//         community; 0 on the unbounded AlmostInfinite plane)
+//   2     log(1 + habitat at the location) / 8 (deme size)
+//   3     entropy (nats) of the location's dispersal distribution / 16
+//   4     log(1 + time of the lineage's last event) / 20
+//   5     -log10(speciation probability per event at the location) / 15
+//         (SI local community: speciation happens after migration, nu * m)
+//   6     log(1 + live lineages of the simulation) / 16 (crowding)
+//   7     log(1 + events the lineage has executed) / 20 (age)
+// `se_habitat` and `se_entropy` are the SpatiallyExplicit cell's habitat and
+// dispersal entropy (read from the device tables by the kernels, from the
+// maps by the host).  The same source serves the kernels and the host.
+__host__ __device__ inline void lineage_features_of(int kind, const SimParams &p, uint64_t n_live, uint32_t x,
+                                                    uint32_t y, double last, uint64_t steps, float se_habitat,
+                                                    float se_entropy, float f[kFeat]) {
+    float fx = 0.f, fy = 0.f, hab = 1.f, ent = 0.f;
+    float nu = (float)p.nu;
+    if (kind == kNonSpatial) {
+        fx = (float)x / (float)p.width;
+        fy = (float)y / (float)p.height;
+        hab = (float)p.deme;
+        ent = logf((float)p.width * (float)p.height);
+    } else if (kind == kSpatiallyImplicit) {
+        if (x <= p.width - 1 && y <= p.height - 1) {  // the local community (extent at (0, 0))
+            fx = (float)x / (float)p.width;
+            fy = (float)y / (float)p.height;
+            hab = (float)p.deme;
+            ent = logf((float)p.width * (float)p.height);
+            nu *= (float)p.migration;
+        } else {
+            fx = (float)(x - p.meta_ox) / (float)p.meta_width;
+            fy = (float)(y - p.meta_oy) / (float)p.meta_height;
+            hab = (float)p.meta_deme;
+            ent = logf((float)p.meta_width * (float)p.meta_height);
+        }
+    } else if (kind == kAlmostInfiniteNormal) {
+        // differential entropy of the 2D dispersal kernel: normal, or a
+        // Clark2Dt kernel of scale sqrt(u) (sigma 0: none)
+        const float scale2 = p.clark ? (float)p.clark_shape_u : (float)p.sigma * (float)p.sigma;
+        ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2, 1.0f));
+    } else if (kind == kWrappingNoise) {
+        // the Normal kernel's entropy, restricted to the habitable share
+        const float scale2 = (float)p.sigma * (float)p.sigma;
+        ent = logf(fmaxf(2.0f * 3.14159265f * 2.71828183f * scale2 * (float)p.noise.coverage, 1.0f));
+    } else {
+        fx = (float)x / (float)p.width;
+        fy = (float)y / (float)p.height;
+        hab = se_habitat;
+        ent = se_entropy;
+    }
+    f[0] = fx;
+    f[1] = fy;
+    f[2] = log1pf(hab) * 0.125f;
+    f[3] = ent * 0.0625f;
+    f[4] = log1pf((float)last) * 0.05f;
+    f[5] = -log10f(fmaxf(nu, 1e-15f)) * (1.0f / 15.0f);
+    f[6] = log1pf((float)n_live) * 0.0625f;
+    f[7] = log1pf((float)steps) * 0.05f;
+}
 
 // Appends a snapshot row for every live lineage of `f.in` (rows beyond `cap`
 // are counted but not written).

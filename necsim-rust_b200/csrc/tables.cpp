@@ -124,6 +124,22 @@ bool dispersal_contract_holds(const necsim_scenario &sc) {
     return ok.load();
 }
 
+float dispersal_entropy(const necsim_scenario &sc, uint64_t r) {
+    if (!sc.dispersal) return 0.0f;
+    RowScratch s;
+    double self_w;
+    row_weights(sc, r, s, self_w);
+    if (s.ev.empty()) return 0.0f;
+    double total = 0.0;
+    for (double w : s.w) total = total + w;
+    double h = 0.0;
+    for (double w : s.w) {
+        const double q = w / total;
+        h -= q * std::log(q);
+    }
+    return (float)h;
+}
+
 int build_spatially_explicit_tables(const necsim_scenario &sc, HostTables &out, unsigned threads) {
     const uint64_t n = (uint64_t)sc.width * sc.height;
     out.cells.assign(n, CellRecord{});

@@ -26,6 +26,10 @@ struct HostTables {
 // Returns 0, or 1 empty habitat, 2 dispersal contract violated, 3 too many atoms.
 int build_spatially_explicit_tables(const necsim_scenario &sc, HostTables &out, unsigned threads = 0);
 
+// The Shannon entropy (nats) of cell r's dispersal distribution, as the
+// table build records it (0 without a dispersal map or from a non-habitat cell).
+float dispersal_entropy(const necsim_scenario &sc, uint64_t r);
+
 // check_in_memory_dispersal_contract (dispersal_sampler/in_memory/contract.rs:13-69).
 bool dispersal_contract_holds(const necsim_scenario &sc);
 

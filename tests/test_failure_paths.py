@@ -44,7 +44,9 @@ def test_scenario_needs_a_dispersal_map_or_tables(nb, syn):
 def test_round_watchdog_times_out(nb, syn):
     desc, seed = syn.config1()
     with pytest.raises(nb.NecsimError) as e:
-        nb.simulate(desc["speciation_probability"], syn.to_scenario(desc), seed, nb.CUDA(max_rounds=4))
+        # checked between graph launches: two rounds per graph, so at most 4 rounds run
+        nb.simulate(desc["speciation_probability"], syn.to_scenario(desc), seed,
+                    nb.CUDA(max_rounds=4, rounds_per_graph=2))
     assert e.value.code == E_TIMEOUT
     # the same run within its round count completes
     ok = nb.simulate(desc["speciation_probability"], syn.to_scenario(desc), seed)
