@@ -322,6 +322,15 @@ def train_lifetime_model(nb, syn, device, pause):
                                    max_rows=1 << 17)
         X.append(xs)
         y.append(ys)
+    # SpatiallyImplicit traces from a sweep of the same family with other
+    # parameters (sweep seed 99, local communities of at most 2e4 cells,
+    # speciation raised 100-fold so lineages end within the trace horizon)
+    si = syn.config4(n_sims=16, sweep_seed=99, max_local=20000)
+    xs, ys = nb.collect_traces([syn.to_scenario(d) for d, _ in si],
+                               [d["speciation_probability"] * 100 for d, _ in si], [1000 + s for _, s in si],
+                               nb.CUDA(device=device), pause_before=pause, snapshot_rounds=16, max_rows=1 << 17)
+    X.append(xs)
+    y.append(ys)
     X = np.concatenate(X)
     y = np.concatenate(y)
     model = nb.LifetimeModel(seed=1, device=device)
@@ -329,7 +338,8 @@ def train_lifetime_model(nb, syn, device, pause):
     info = {"trace_rows": int(X.shape[0]), "epochs": 8, "final_loss": float(losses[-1]),
             "label_variance": float(np.var(y)), "seconds": time.perf_counter() - t0,
             "traces": "AlmostInfinite r=100 sigma=10 and SpatiallyExplicit 64x64, speciation "
-                      "{1e-2,1e-3,1e-4}, paused at t=%g" % pause}
+                      "{1e-2,1e-3,1e-4}, and 16 SpatiallyImplicit simulations of another sweep (seed 99, "
+                      "J <= 2e4, speciation x100), paused at t=%g" % pause}
     return model, info
 
 

@@ -145,6 +145,14 @@ typedef struct necsim_args {
                                   NECSIM_E_TIMEOUT; 0 = default 2^26.  Every round advances each
                                   live lineage by >= step_slice expected events, so a valid run
                                   only meets a limit chosen below its round count */
+    uint32_t priority_sims;    /* batches: this many simulations run in engines of their own (own
+                                  rounds, stream and host thread) beside the others, so the others'
+                                  rounds never hold them back: those in priority_list, else (schedule
+                                  1) the ones the lifetime model scores as longest-lived; 0 = none,
+                                  or 2 with schedule 1.  Results are identical either way */
+    uint32_t pad_priority;
+    const uint32_t *priority_list; /* batch indices of the priority simulations (NULL: the model's
+                                      choice); at most priority_sims are used */
 } necsim_args;
 
 /* ---- events and lineages (reference layouts) ---- */

@@ -77,6 +77,8 @@ class CArgs(ctypes.Structure):
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
         ("resident", ctypes.c_uint32), ("event_time_sampler", ctypes.c_uint32),
         ("model", ctypes.c_void_p), ("max_rounds", ctypes.c_uint64),
+        ("priority_sims", ctypes.c_uint32), ("pad_priority", ctypes.c_uint32),
+        ("priority_list", ctypes.c_void_p),
     ]
 
 
@@ -421,6 +423,11 @@ class CUDA:
     # watchdog: a run still active after this many rounds fails with
     # NECSIM_E_TIMEOUT (checked between graph launches); 0: 2^26
     max_rounds: int = 0
+    # batches: simulations run in engines of their own beside the others
+    # (their own rounds); `priority_list` names them (batch indices), else the
+    # learned schedule's model picks `priority_sims` of them (default 2)
+    priority_sims: int = 0
+    priority_list: Optional[Sequence[int]] = None
 
 
 Independent = CUDA
@@ -581,6 +588,13 @@ def _args_struct(algorithm: CUDA):
         raise ValueError("event_time_sampler must be 'poisson' or 'exp'")
     a.event_time_sampler = EVENT_TIME_SAMPLERS[algorithm.event_time_sampler]
     a.max_rounds = algorithm.max_rounds
+    a.priority_sims = algorithm.priority_sims
+    if algorithm.priority_list is not None:
+        lst = (ctypes.c_uint32 * max(1, len(algorithm.priority_list)))(*algorithm.priority_list)
+        a._priority_keep = lst
+        a.priority_list = ctypes.cast(lst, ctypes.c_void_p)
+        if not a.priority_sims:
+            a.priority_sims = len(algorithm.priority_list)
     return a
 
 

@@ -1772,6 +1772,151 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
     if (E.n_total > 0) build_graph(E);
 }
 
+// ---- a batch split into engines: priority simulations each run alone ----
+//
+// The rounds of a batch are synchronised: every round waits for the slowest
+// lineage of every simulation, so a long-lived simulation advances at the
+// pace of the whole batch.  A priority simulation gets an engine of its own
+// (its own rounds, stream and host thread) and runs beside the others.  The
+// canonical schedule of every simulation depends only on that simulation,
+// so the split changes no result.
+struct BatchRun {
+    std::vector<std::unique_ptr<Engine>> engines;  // engines[0]: the others (empty: none); then one per priority simulation
+    std::vector<std::vector<uint32_t>> members;    // batch indices of each engine's simulations
+    std::vector<Remaining> rem;
+};
+
+// The priority simulations of a batch: priority_list's first priority_sims
+// entries, else with the learned schedule the model's longest-lived
+// priority_sims (default 2), at most all but one simulation.
+std::vector<uint32_t> choose_priority(const std::vector<SimHost> &sims, const necsim_args &args) {
+    const uint32_t n = (uint32_t)sims.size();
+    std::vector<uint32_t> out;
+    if (n < 2 || args.report_dispersal) return out;
+    if (args.priority_list && args.priority_sims) {
+        std::vector<uint8_t> seen(n, 0);
+        for (uint32_t k = 0; k < args.priority_sims; ++k) {
+            const uint32_t j = args.priority_list[k];
+            if (j >= n) fail(NECSIM_E_INVALID_ARGUMENT, "priority_list names a simulation outside the batch");
+            if (!seen[j]) out.push_back(j);
+            seen[j] = 1;
+        }
+        if (out.size() >= n) out.pop_back();  // keep one simulation for the shared engine
+        return out;
+    }
+    if (args.schedule != 1 || !args.model) return out;
+    const uint32_t k = std::min<uint32_t>(args.priority_sims ? args.priority_sims : 2, n - 1);
+    const std::vector<float> score = score_simulations(args.model, sims);
+    std::vector<uint32_t> order(n);
+    for (uint32_t j = 0; j < n; ++j) order[j] = j;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return score[a] > score[b]; });
+    out.assign(order.begin(), order.begin() + k);
+    return out;
+}
+
+void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &args) {
+    const std::vector<uint32_t> prio = choose_priority(sims, args);
+    std::vector<uint8_t> is_prio(sims.size(), 0);
+    for (uint32_t j : prio) is_prio[j] = 1;
+    std::vector<SimHost> rest;
+    std::vector<uint32_t> rest_ids;
+    for (uint32_t j = 0; j < sims.size(); ++j)
+        if (!is_prio[j]) {
+            rest.push_back(sims[j]);
+            rest_ids.push_back(j);
+        }
+    b.engines.clear();
+    b.members.clear();
+    auto add = [&](std::vector<SimHost> part, std::vector<uint32_t> ids) {
+        b.engines.emplace_back(new Engine());
+        Engine &E = *b.engines.back();
+        setup_engine(E, args);
+        prepare_engine(E, std::move(part), args, nullptr, nullptr);
+        b.members.push_back(std::move(ids));
+    };
+    add(std::move(rest), std::move(rest_ids));
+    for (uint32_t j : prio) add({sims[j]}, {j});
+    b.rem.assign(b.engines.size(), Remaining{});
+}
+
+// One run of every engine of the batch, the priority engines on their own
+// host threads; outcomes in batch order.  The device time of the batch is
+// the span from a common start to the last engine's end; kernel times,
+// launches and traffic are summed over the engines.
+void run_batch(BatchRun &b, const necsim_reporter *reporters, necsim_outcome *outcomes) {
+    const size_t ne = b.engines.size();
+    if (ne == 1) {
+        Engine &E = *b.engines[0];
+        E.h2d_bytes = E.d2h_bytes = 0;
+        execute_engine(E, reporters, false, outcomes, b.rem[0]);
+        return;
+    }
+    Engine &E0 = *b.engines[0];
+    CK(cudaSetDevice(E0.device));
+    cudaEvent_t start = nullptr;
+    CK(cudaEventCreate(&start));
+    struct EventFree {
+        cudaEvent_t e;
+        ~EventFree() { cudaEventDestroy(e); }
+    } start_free{start};
+    CK(cudaEventRecord(start, E0.stream));
+    CK(cudaEventSynchronize(start));
+    std::vector<std::vector<necsim_outcome>> outs(ne);
+    std::vector<std::vector<necsim_reporter>> reps(ne);
+    std::vector<std::exception_ptr> errs(ne);
+    for (size_t e = 0; e < ne; ++e) {
+        outs[e].resize(b.members[e].size());
+        if (reporters)
+            for (uint32_t j : b.members[e]) reps[e].push_back(reporters[j]);
+    }
+    auto work = [&](size_t e) {
+        try {
+            Engine &E = *b.engines[e];
+            CK(cudaSetDevice(E.device));
+            E.h2d_bytes = E.d2h_bytes = 0;
+            if (!b.members[e].empty())
+                execute_engine(E, reporters ? reps[e].data() : nullptr, false, outs[e].data(), b.rem[e]);
+        } catch (...) {
+            errs[e] = std::current_exception();
+        }
+    };
+    std::vector<std::thread> threads;
+    for (size_t e = 1; e < ne; ++e) threads.emplace_back(work, e);
+    work(0);
+    for (auto &t : threads) t.join();
+    for (auto &err : errs)
+        if (err) std::rethrow_exception(err);
+    double span = 0.0, kernel = 0.0, resident = 0.0;
+    uint64_t launches = 0, steps_l = 0, visits = 0, h2d = 0, d2h = 0;
+    for (size_t e = 0; e < ne; ++e) {
+        if (b.members[e].empty()) continue;
+        float ms = 0.f;
+        if (b.engines[e]->n_total > 0 && cudaEventElapsedTime(&ms, start, b.engines[e]->ev_total1) == cudaSuccess)
+            span = std::max(span, (double)ms);
+        const necsim_outcome &o = outs[e][0];
+        kernel += o.kernel_ms;
+        resident += o.resident_ms;
+        launches += o.n_launches;
+        steps_l += o.n_step_launches;
+        visits += o.lineage_visits;
+        h2d += o.h2d_bytes;
+        d2h += o.d2h_bytes;
+    }
+    for (size_t e = 0; e < ne; ++e)
+        for (size_t k = 0; k < b.members[e].size(); ++k) {
+            necsim_outcome o = outs[e][k];
+            o.total_ms = span;
+            o.kernel_ms = kernel;
+            o.resident_ms = resident;
+            o.n_launches = launches;
+            o.n_step_launches = steps_l;
+            o.lineage_visits = visits;
+            o.h2d_bytes = h2d;
+            o.d2h_bytes = d2h;
+            outcomes[b.members[e][k]] = o;
+        }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1955,17 +2100,15 @@ int necsim_gpu_simulate_batch(const necsim_scenario *scenarios, const uint64_t *
             sh.params.pause_before = pause_before >= 0.0 ? pause_before : -1.0;
             sh.n_origins = count_origins(scenarios[s]);
         }
-        Engine E;
-        setup_engine(E, args);
-        Remaining rem;
-        run_simulations(E, sims, args, nullptr, reporters, false, outcomes, rem, nullptr);
+        BatchRun b;
+        prepare_batch(b, std::move(sims), args);
+        run_batch(b, reporters, outcomes);
     });
 }
 
 struct necsim_batch {
-    Engine engine;
+    BatchRun run;
     std::string error;
-    Remaining rem;
 };
 
 static std::vector<SimHost> batch_sims(const necsim_scenario *scenarios, const uint64_t *wyhash_seeds,
@@ -2131,9 +2274,7 @@ int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wy
     char msg[512] = {0};
     const int rc = guarded(nullptr, msg, sizeof(msg), [&] {
         const necsim_args args = with_defaults(args_in);
-        setup_engine(b->engine, args);
-        prepare_engine(b->engine, batch_sims(scenarios, wyhash_seeds, n_sims, args, pause_before), args,
-                       nullptr, nullptr);
+        prepare_batch(b->run, batch_sims(scenarios, wyhash_seeds, n_sims, args, pause_before), args);
     });
     b->error = msg;
     *out = b;
@@ -2143,11 +2284,7 @@ int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wy
 int necsim_gpu_batch_run(necsim_batch *b, const necsim_reporter *reporters, necsim_outcome *outcomes) {
     if (!b || !outcomes) return NECSIM_E_INVALID_ARGUMENT;
     char msg[512] = {0};
-    const int rc = guarded(nullptr, msg, sizeof(msg), [&] {
-        b->engine.h2d_bytes = 0;
-        b->engine.d2h_bytes = 0;
-        execute_engine(b->engine, reporters, false, outcomes, b->rem);
-    });
+    const int rc = guarded(nullptr, msg, sizeof(msg), [&] { run_batch(b->run, reporters, outcomes); });
     b->error = msg;
     return rc;
 }

@@ -267,3 +267,25 @@ def test_dispersal_events_batch_and_pause(nb, syn, oracle):
         assert same_disp_stream(g.dispersal, c.dispersal)
         assert same_stream(g.speciation, c.speciation)
         assert g.biodiversity == c.biodiversity and g.n_remaining == c.n_remaining
+
+
+def test_priority_split_is_bit_identical(nb, syn):
+    """Simulations run in engines of their own (priority_list) give the same
+    per-simulation results as the unsplit batch: every simulation's
+    canonical schedule depends on that simulation only."""
+    sims = syn.config4(n_sims=6, max_local=3000)
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] * 50 for d, _ in sims]
+    seeds = [s for _, s in sims]
+    whole = nb.simulate_batch(scen, nus, seeds, collect=True)
+    split = nb.simulate_batch(scen, nus, seeds, nb.CUDA(priority_list=[4, 1]), collect=True)
+    with nb.Batch(scen, nus, seeds, nb.CUDA(priority_list=[0, 5, 2])) as b:
+        b.run()
+        again = b.run(collect=True)
+    for x, y, z in zip(whole, split, again):
+        for o in (y, z):
+            assert same_stream(x.speciation, o.speciation)
+            assert (x.steps, x.n_rounds, x.n_dedup, x.biodiversity, x.time) == (
+                o.steps, o.n_rounds, o.n_dedup, o.biodiversity, o.time)
+    # the batch's device time spans its engines
+    assert split[0].total_ms > 0 and split[0].n_launches > whole[0].n_launches
