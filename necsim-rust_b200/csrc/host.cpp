@@ -593,6 +593,7 @@ struct Control {  // small device scalars
     uint32_t status;
     unsigned int n_resident;  // active simulations owned by the resident kernel
     int graph_done;           // set when the global rounds beside a resident launch end
+    unsigned int busy;        // warps of the cooperative kernel holding a lineage
 };
 
 // Events delivered round by round (dispersal reporting): per simulation the
@@ -1061,6 +1062,10 @@ StepArgs make_step_args(Engine &E, DeviceLineages &in) {
     a.order = E.learned ? E.order : nullptr;
     a.exp_sampler = E.args.event_time_sampler == NECSIM_SAMPLER_EXP ? 1u : 0u;
     a.coop_max = E.coop_max;
+    // free rounds of single-lineage simulations (not when dispersal events
+    // are drained round by round)
+    a.free_rounds = E.args.report_dispersal ? 0u : 64u;
+    a.busy = &E.d_ctl->busy;
     if (E.tracing) {
         a.trace.deaths = E.trace_deaths;
         a.trace.n_deaths = E.trace_counts + 1;

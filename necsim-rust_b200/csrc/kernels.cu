@@ -933,6 +933,21 @@ __device__ __forceinline__ const SimParams *stage_params(const StepArgs &a, unsi
     return reinterpret_cast<const SimParams *>(smem);
 }
 
+// Per-simulation horizon rule (canonical schedule):
+// H' = min(H + clamp(ceil(min_round_events / n), step_slice, step_slice_max) / lambda, pause),
+// or no further round when n == 0 or H has reached pause_before.
+__device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long long live, double &h) {
+    const bool paused = p.pause_before >= 0.0 && !(p.horizon < p.pause_before);
+    if (live == 0 || paused) return false;
+    const unsigned long long step_slice = p.step_slice ? p.step_slice : 1ULL;
+    unsigned long long per = (p.min_round_events + live - 1) / live;
+    if (p.step_slice_max && per > p.step_slice_max) per = p.step_slice_max;
+    if (per < step_slice) per = step_slice;
+    h = __dadd_rn(p.horizon, __ddiv_rn(__ull2double_rn(per), p.lambda));
+    if (p.pause_before >= 0.0 && p.pause_before < h) h = p.pause_before;
+    return true;
+}
+
 // At most one lineage per warp: each warp takes lineages from the queue and
 // steps each one with all its lanes (a lineage's events at warp latency,
 // lineages on all SMs).  Every lineage gets a warp at once, so the queue
@@ -944,11 +959,17 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
     uint64_t warp_steps = 0;
     for (;;) {
         unsigned long long k = 0;
-        if (lane_id == 0) k = atomicAdd(a.work, 1ULL);
+        if (lane_id == 0) {
+            k = atomicAdd(a.work, 1ULL);
+            if (a.busy && k < n) atomicAdd(a.busy, 1u);
+        }
         k = __shfl_sync(kFull, k, 0);
         if (k >= n) break;
         Lane c;
-        if (!take_lineage<KIND, SINGLE>(a, P, k, c, false)) continue;
+        if (!take_lineage<KIND, SINGLE>(a, P, k, c, false)) {
+            if (a.busy && lane_id == 0) atomicSub(a.busy, 1u);
+            continue;
+        }
         const SimParams &p = P[SINGLE ? 0 : c.s];
         int r;
         if constexpr (EXP) {
@@ -960,7 +981,31 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
             if (r == kStepSpeciated) warp_steps += 1;
         } else {
             r = coop_run<KIND>(c, p, sink, warp_steps);
+            // A simulation that started the round with one live lineage has
+            // nothing to merge: while other lineages of the launch are still
+            // stepping (or the launch has this simulation alone), its warp
+            // runs the simulation's next rounds itself, each to the horizon
+            // the scheduler would set (next_horizon) and counted as a round.
+            if (a.free_rounds && r == kStepStop && a.counters[c.s].n_live == 1) {
+                SimParams &pg = const_cast<SimParams *>(a.params)[SINGLE ? 0 : c.s];
+                for (uint32_t extra = 0; extra < a.free_rounds; ++extra) {
+                    const bool others = SINGLE || *(volatile const unsigned *)a.busy > 1u;
+                    if (!__shfl_sync(kFull, others ? 1 : 0, 0)) break;
+                    double h;
+                    if (!next_horizon(pg, 1, h)) break;  // paused
+                    __syncwarp();
+                    if (lane_id == 0) {
+                        pg.horizon = h;
+                        a.counters[c.s].n_rounds += 1;
+                    }
+                    __syncwarp();
+                    c.horizon = h;
+                    r = coop_run<KIND>(c, p, sink, warp_steps);
+                    if (r != kStepStop) break;
+                }
+            }
         }
+        if (a.busy && lane_id == 0) atomicSub(a.busy, 1u);
         if (lane_id == 0) {
             if (r == kStepStop)
                 store_stopped(a, c);
@@ -1067,21 +1112,6 @@ __global__ void __launch_bounds__(kCoopBlock) coop_kernel(StepArgs a) {
     if (n > a.coop_max) return;
     const SimParams *P = stage_params<SINGLE>(a, params_smem);
     coop_body<KIND, SINGLE, false>(a, P, n);
-}
-
-// Per-simulation horizon rule (canonical schedule):
-// H' = min(H + clamp(ceil(min_round_events / n), step_slice, step_slice_max) / lambda, pause),
-// or no further round when n == 0 or H has reached pause_before.
-__device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long long live, double &h) {
-    const bool paused = p.pause_before >= 0.0 && !(p.horizon < p.pause_before);
-    if (live == 0 || paused) return false;
-    const unsigned long long step_slice = p.step_slice ? p.step_slice : 1ULL;
-    unsigned long long per = (p.min_round_events + live - 1) / live;
-    if (p.step_slice_max && per > p.step_slice_max) per = p.step_slice_max;
-    if (per < step_slice) per = step_slice;
-    h = __dadd_rn(p.horizon, __ddiv_rn(__ull2double_rn(per), p.lambda));
-    if (p.pause_before >= 0.0 && p.pause_before < h) h = p.pause_before;
-    return true;
 }
 
 // A simulation with at most kResidentMax live lineages is advanced by one

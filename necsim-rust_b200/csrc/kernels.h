@@ -40,6 +40,12 @@ struct StepArgs {
     // the cooperative kernel (one warp per lineage, at most its resident
     // warps); 0: the step kernel takes every round
     uint64_t coop_max;
+    // cooperative kernel: a simulation with one live lineage runs up to this
+    // many of its next rounds in the same launch while other warps are busy
+    // (or it is the launch's only simulation); 0: off.  `busy` counts the
+    // warps holding a lineage (zero between launches)
+    uint32_t free_rounds;
+    unsigned int *busy;
 };
 
 struct DedupArgs {
