@@ -454,7 +454,7 @@ def time_arm(nb, scen, nus, seeds, algo, args, dist):
         batch.run()
     dist.barrier()
     r = {"steps": 0, "dev_ms": 0.0, "kernel_ms": 0.0, "resident_ms": 0.0, "step_launches": 0, "visits": 0,
-         "launches": 0, "n_spec": 0, "outs": None}
+         "launches": 0, "n_spec": 0, "outs": None, "priority": batch.priority}
     for _ in range(args.steps):
         outs = batch.run()
         o0 = outs[0]
@@ -585,6 +585,7 @@ def main():
         line["plain"] = {"value": p_value, "unit": UNIT, "ms_per_step": p_ms / args.steps,
                          "gpu_launches": plain["launches"]}
         line["learned_over_plain"] = value / p_value
+        line["priority_sims"] = head["priority"]
         line["outcomes_identical"] = bool(same)
     if model_info is not None:
         line["model"] = model_info

@@ -280,6 +280,10 @@ int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wy
                             necsim_batch **out);
 int necsim_gpu_batch_run(necsim_batch *batch, const necsim_reporter *reporters,
                          necsim_outcome *outcomes);
+/* The batch indices of the simulations that run in engines of their own
+ * (necsim_args.priority_sims): up to `cap` into `ids`, their count in *n.
+ * No reference counterpart. */
+int necsim_gpu_batch_priority(const necsim_batch *batch, uint32_t *ids, uint32_t cap, uint32_t *n);
 const char *necsim_gpu_batch_last_error(const necsim_batch *batch);
 void necsim_gpu_batch_destroy(necsim_batch *batch);
 

@@ -132,6 +132,7 @@ SYMBOLS = [
     "necsim_presample_origins", "necsim_gpu_autotune", "necsim_event_log_create",
     "necsim_event_log_reporter", "necsim_event_log_close", "necsim_event_log_replay", "necsim_map_load",
     "necsim_map_free", "necsim_maps_fix", "necsim_gpu_hash_peak", "necsim_gpu_displacements",
+    "necsim_gpu_batch_priority",
 ]
 
 _lib = None
@@ -213,6 +214,9 @@ def lib():
     L.necsim_gpu_displacements.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_uint64,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p]
     L.necsim_gpu_displacements.restype = ctypes.c_int
+    L.necsim_gpu_batch_priority.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                            ctypes.POINTER(ctypes.c_uint32)]
+    L.necsim_gpu_batch_priority.restype = ctypes.c_int
     L.necsim_model_create.argtypes = [ctypes.c_int32, u64, P(vp)]
     L.necsim_model_create.restype = ctypes.c_int
     L.necsim_model_destroy.argtypes = [vp]
@@ -806,6 +810,16 @@ class Batch:
             raise NecsimError(rc, L.necsim_gpu_batch_last_error(self._b).decode())
         return [_outcome(outs[j], cols[j].events() if cols else None, None, cols[j] if cols else None)
                 for j in range(self.n)]
+
+    @property
+    def priority(self) -> List[int]:
+        """Batch indices of the simulations running in engines of their own."""
+        n = ctypes.c_uint32(0)
+        ids = (ctypes.c_uint32 * max(1, self.n))()
+        rc = lib().necsim_gpu_batch_priority(self._b, ids, self.n, ctypes.byref(n))
+        if rc != 0:
+            raise NecsimError(rc, "priority query failed")
+        return [int(ids[k]) for k in range(n.value)]
 
     def close(self):
         if getattr(self, "_b", None) is not None and self._b.value:

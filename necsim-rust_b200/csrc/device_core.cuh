@@ -28,26 +28,19 @@ constexpr uint64_t kInvPhi = 0x9e3779b97f4a7c15ULL;
 // core::f64::consts::TAU
 constexpr double kTau = 6.283185307179586;
 
-// wyhash.rs:85-96: 64x64 -> 128 multiply, low and high halves xor-folded.
-// The 128-bit product is formed once from four 32x32 -> 64 partial products
-// (each accumulating into a 64-bit sum that cannot overflow), so the low and
-// high halves share them instead of being multiplied out separately.
+// wyhash.rs:85-96: 64x64 -> 128 multiply, low and high halves xor-folded
 __device__ __forceinline__ uint64_t wymum(uint64_t a, uint64_t b) {
-    const uint32_t a0 = (uint32_t)a, a1 = (uint32_t)(a >> 32), b0 = (uint32_t)b, b1 = (uint32_t)(b >> 32);
-    const uint64_t p00 = (uint64_t)a0 * b0;
-    const uint64_t t = (uint64_t)a0 * b1 + (p00 >> 32);
-    const uint64_t u = (uint64_t)a1 * b0 + (uint32_t)t;
-    const uint64_t lo = (u << 32) | (uint32_t)p00;
-    const uint64_t hi = (uint64_t)a1 * b1 + (t >> 32) + (u >> 32);
+    const uint64_t lo = a * b;
+    const uint64_t hi = __umul64hi(a, b);
     return (a ^ lo) ^ (b ^ hi);
 }
 
-// wyhash.rs:99-119.  The shifted value x >> 32 is below 2^32 and the shift
-// count x >> 60 below 16, so the xor only touches the low word: a 32-bit shift.
+// wyhash.rs:99-119
 __device__ __forceinline__ uint64_t seahash_diffuse(uint64_t x) {
     x *= kSeaHashK;
-    const uint32_t hi = (uint32_t)(x >> 32);
-    x ^= (uint64_t)(hi >> (hi >> 28));
+    const uint64_t a = x >> 32;
+    const uint64_t b = x >> 60;
+    x ^= a >> b;
     x *= kSeaHashK;
     return x;
 }

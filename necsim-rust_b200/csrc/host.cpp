@@ -2294,6 +2294,18 @@ int necsim_gpu_batch_run(necsim_batch *b, const necsim_reporter *reporters, necs
     return rc;
 }
 
+int necsim_gpu_batch_priority(const necsim_batch *b, uint32_t *ids, uint32_t cap, uint32_t *n) {
+    if (!b || !n || (cap && !ids)) return NECSIM_E_INVALID_ARGUMENT;
+    uint32_t k = 0;
+    for (size_t e = 1; e < b->run.members.size(); ++e)
+        for (uint32_t j : b->run.members[e]) {
+            if (k < cap) ids[k] = j;
+            ++k;
+        }
+    *n = k;
+    return NECSIM_OK;
+}
+
 const char *necsim_gpu_batch_last_error(const necsim_batch *b) { return b ? b->error.c_str() : "null batch"; }
 
 void necsim_gpu_batch_destroy(necsim_batch *b) { delete b; }

@@ -981,15 +981,18 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
             if (r == kStepSpeciated) warp_steps += 1;
         } else {
             r = coop_run<KIND>(c, p, sink, warp_steps);
+            // the lineage's own round is done: it no longer holds the launch
+            if (a.busy && lane_id == 0) atomicSub(a.busy, 1u);
             // A simulation that started the round with one live lineage has
             // nothing to merge: while other lineages of the launch are still
-            // stepping (or the launch has this simulation alone), its warp
-            // runs the simulation's next rounds itself, each to the horizon
-            // the scheduler would set (next_horizon) and counted as a round.
+            // in their own round (or the launch has this simulation alone),
+            // its warp runs the simulation's next rounds itself, each to the
+            // horizon the scheduler would set (next_horizon) and counted as a
+            // round.  Free-running warps do not keep one another going.
             if (a.free_rounds && r == kStepStop && a.counters[c.s].n_live == 1) {
                 SimParams &pg = const_cast<SimParams *>(a.params)[SINGLE ? 0 : c.s];
                 for (uint32_t extra = 0; extra < a.free_rounds; ++extra) {
-                    const bool others = SINGLE || *(volatile const unsigned *)a.busy > 1u;
+                    const bool others = SINGLE || *(volatile const unsigned *)a.busy > 0u;
                     if (!__shfl_sync(kFull, others ? 1 : 0, 0)) break;
                     double h;
                     if (!next_horizon(pg, 1, h)) break;  // paused
@@ -1005,7 +1008,7 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
                 }
             }
         }
-        if (a.busy && lane_id == 0) atomicSub(a.busy, 1u);
+        if (EXP && a.busy && lane_id == 0) atomicSub(a.busy, 1u);
         if (lane_id == 0) {
             if (r == kStepStop)
                 store_stopped(a, c);
