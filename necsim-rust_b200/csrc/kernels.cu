@@ -666,8 +666,13 @@ __device__ __forceinline__ void shfl_outcome(CoopOutcome &o, int src) {
 // is at or beyond l.horizon (kStepStop, the peek kept in l), it speciates
 // (kStepSpeciated) or a bound check fails (kStepDropped).  `events` counts
 // the executed events; side effects happen on lane 0 only.
+// `stop`, when given, interrupts the run at a peek below the horizon once it
+// reads zero (checked every 32 events): the lineage keeps that peek and
+// continues in a later launch.  Only a simulation with a single lineage may
+// be interrupted mid-round (its rounds merge nothing).
 template <int KIND>
-__device__ __forceinline__ int coop_run(Lane &l, const SimParams &p, const EventSink &k, uint64_t &events) {
+__device__ __forceinline__ int coop_run(Lane &l, const SimParams &p, const EventSink &k, uint64_t &events,
+                                        const volatile unsigned *stop = nullptr) {
     const unsigned lane = threadIdx.x & 31u;
     const bool bucket_lane = lane < kCoopBuckets;
     uint32_t my_b = lane, my_k = 0xffu;
@@ -750,6 +755,8 @@ __device__ __forceinline__ int coop_run(Lane &l, const SimParams &p, const Event
             // the reference's early stop `next_event_time >= level_time`
             // (monolithic/mod.rs:228-239); non-negative doubles order like their bits
             if (__double_as_longlong(l.next) >= horizon_bits) return kStepStop;
+            if (stop && (events & 31u) == 0u && __shfl_sync(kFull, lane == 0 ? *stop : 1u, 0) == 0u)
+                return kStepStop;  // interrupted with the peek kept
             const unsigned hit = __ballot_sync(kFull, speculate && my_b == b_sel && my_k == k_sel);
             if (hit) {
                 shfl_outcome<KIND>(o, __ffs(hit) - 1);
@@ -980,7 +987,18 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
             }
             if (r == kStepSpeciated) warp_steps += 1;
         } else {
-            r = coop_run<KIND>(c, p, sink, warp_steps);
+            if constexpr (KIND == kSpatiallyExplicit) {
+                // the speculative candidates' alias and record reads cost more
+                // than they save here: select first, then read (measured)
+                for (;;) {
+                    r = lineage_step_coop<KIND, false>(c, p, sink);
+                    if (r != kStepMoved) break;
+                    warp_steps += 1;
+                }
+                if (r == kStepSpeciated) warp_steps += 1;
+            } else {
+                r = coop_run<KIND>(c, p, sink, warp_steps);
+            }
             // the lineage's own round is done: it no longer holds the launch
             if (a.busy && lane_id == 0) atomicSub(a.busy, 1u);
             // A simulation that started the round with one live lineage has
@@ -989,7 +1007,7 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
             // its warp runs the simulation's next rounds itself, each to the
             // horizon the scheduler would set (next_horizon) and counted as a
             // round.  Free-running warps do not keep one another going.
-            if (a.free_rounds && r == kStepStop && a.counters[c.s].n_live == 1) {
+            if (KIND != kSpatiallyExplicit && a.free_rounds && r == kStepStop && a.counters[c.s].n_live == 1) {
                 SimParams &pg = const_cast<SimParams *>(a.params)[SINGLE ? 0 : c.s];
                 for (uint32_t extra = 0; extra < a.free_rounds; ++extra) {
                     const bool others = SINGLE || *(volatile const unsigned *)a.busy > 0u;
@@ -1003,8 +1021,9 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
                     }
                     __syncwarp();
                     c.horizon = h;
-                    r = coop_run<KIND>(c, p, sink, warp_steps);
-                    if (r != kStepStop) break;
+                    // interrupted at a peek once the launch's regular work is done
+                    r = coop_run<KIND>(c, p, sink, warp_steps, SINGLE ? nullptr : a.busy);
+                    if (r != kStepStop || __double_as_longlong(c.next) < __double_as_longlong(h)) break;
                 }
             }
         }
