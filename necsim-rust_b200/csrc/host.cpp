@@ -917,10 +917,13 @@ void for_each_origin(const necsim_scenario &sc, F &&push) {
 
 // ---- per-simulation priority of the learned schedule ----
 
-// The lifetime model's score of each simulation: the largest predicted
-// remaining event count (expm1 of the model's output) over up to 32 of its
-// origin lineages, evenly spaced in origin order, at the start of the run
-// (no event executed, the simulation's origin count live).  The features are
+// The lifetime model's score of each simulation, its expected time to end:
+// a simulation ends with its longest-lived lineage, and the expected largest
+// of n independent exponential lifetimes of mean m is m * H(n) (H the
+// harmonic number).  m is the largest predicted remaining event count
+// (expm1 of the model's output) over up to 32 of its origin lineages, evenly
+// spaced in origin order, at the start of the run (no event executed, the
+// simulation's origin count live); n is its origin count.  The features are
 // the kernels' (lineage_features_of), with a SpatiallyExplicit cell's
 // habitat and dispersal entropy read from the maps.
 std::vector<float> score_simulations(necsim_model *m, const std::vector<SimHost> &sims) {
@@ -966,6 +969,16 @@ std::vector<float> score_simulations(necsim_model *m, const std::vector<SimHost>
     CK(cudaStreamSynchronize(m->stream));
     for (uint64_t j = 0; j < n; ++j)
         score[owner[j]] = std::max(score[owner[j]], std::expm1(std::min(std::max(y[j], 0.f), 40.f)));
+    for (size_t s = 0; s < sims.size(); ++s) {
+        // H(n): summed below 64, else ln n + Euler's gamma + 1 / 2n
+        const uint64_t no = sims[s].n_origins;
+        double harmonic = 0.0;
+        if (no < 64)
+            for (uint64_t i = 1; i <= no; ++i) harmonic += 1.0 / (double)i;
+        else
+            harmonic = std::log((double)no) + 0.5772156649 + 0.5 / (double)no;
+        score[s] = (float)(score[s] * harmonic);
+    }
     return score;
 }
 

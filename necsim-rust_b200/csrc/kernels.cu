@@ -1014,6 +1014,7 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
                     if (!__shfl_sync(kFull, others ? 1 : 0, 0)) break;
                     double h;
                     if (!next_horizon(pg, 1, h)) break;  // paused
+                    const double h_prev = pg.horizon;
                     __syncwarp();
                     if (lane_id == 0) {
                         pg.horizon = h;
@@ -1023,7 +1024,18 @@ __device__ __forceinline__ void coop_body(const StepArgs &a, const SimParams *P,
                     c.horizon = h;
                     // interrupted at a peek once the launch's regular work is done
                     r = coop_run<KIND>(c, p, sink, warp_steps, SINGLE ? nullptr : a.busy);
-                    if (r != kStepStop || __double_as_longlong(c.next) < __double_as_longlong(h)) break;
+                    if (r == kStepStop && __double_as_longlong(c.next) < __double_as_longlong(h)) {
+                        // the round is not finished: give it back, so the
+                        // scheduler sets (and counts) the same horizon again
+                        __syncwarp();
+                        if (lane_id == 0) {
+                            pg.horizon = h_prev;
+                            a.counters[c.s].n_rounds -= 1;
+                        }
+                        __syncwarp();
+                        break;
+                    }
+                    if (r != kStepStop) break;
                 }
             }
         }
