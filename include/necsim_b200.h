@@ -150,7 +150,12 @@ typedef struct necsim_args {
                                   rounds never hold them back: those in priority_list, else (schedule
                                   1) the ones the lifetime model scores as longest-lived; 0 = none,
                                   or 2 with schedule 1.  Results are identical either way */
-    uint32_t pad_priority;
+    uint32_t priority_groups;  /* batches: the simulations that do not run alone split into this
+                                  many engines (0 or 1: one), contiguous runs of the priority order
+                                  (schedule 1: the lifetime model's longest-lived first, else batch
+                                  order) whose streams have decreasing CUDA stream priority, so the
+                                  first groups' rounds go first and their tails start early.
+                                  Results are identical either way */
     const uint32_t *priority_list; /* batch indices of the priority simulations (NULL: the model's
                                       choice); at most priority_sims are used */
 } necsim_args;

@@ -77,7 +77,7 @@ class CArgs(ctypes.Structure):
         ("device", ctypes.c_int32), ("rounds_per_graph", ctypes.c_uint32),
         ("resident", ctypes.c_uint32), ("event_time_sampler", ctypes.c_uint32),
         ("model", ctypes.c_void_p), ("max_rounds", ctypes.c_uint64),
-        ("priority_sims", ctypes.c_uint32), ("pad_priority", ctypes.c_uint32),
+        ("priority_sims", ctypes.c_uint32), ("priority_groups", ctypes.c_uint32),
         ("priority_list", ctypes.c_void_p),
     ]
 
@@ -432,6 +432,9 @@ class CUDA:
     # learned schedule's model picks `priority_sims` of them (default 2)
     priority_sims: int = 0
     priority_list: Optional[Sequence[int]] = None
+    # batches: the other simulations in this many engines of decreasing CUDA
+    # stream priority (the learned model's longest-lived first, else batch order)
+    priority_groups: int = 0
 
 
 Independent = CUDA
@@ -593,6 +596,7 @@ def _args_struct(algorithm: CUDA):
     a.event_time_sampler = EVENT_TIME_SAMPLERS[algorithm.event_time_sampler]
     a.max_rounds = algorithm.max_rounds
     a.priority_sims = algorithm.priority_sims
+    a.priority_groups = algorithm.priority_groups
     if algorithm.priority_list is not None:
         lst = (ctypes.c_uint32 * max(1, len(algorithm.priority_list)))(*algorithm.priority_list)
         a._priority_keep = lst

@@ -592,7 +592,6 @@ struct Control {  // small device scalars
     unsigned int n_active;    // active simulations in the global rounds
     uint32_t status;
     unsigned int n_resident;  // active simulations owned by the resident kernel
-    int graph_done;           // set when the global rounds beside a resident launch end
     unsigned int busy;        // warps of the cooperative kernel holding a lineage
 };
 
@@ -787,15 +786,17 @@ void upload_tables(Engine &E, SimHost &s) {
     }
 }
 
-void setup_engine(Engine &E, const necsim_args &args) {
+// `stream_priority`: the CUDA stream priority of the engine's streams (0:
+// the default, the least).
+void setup_engine(Engine &E, const necsim_args &args, int stream_priority = 0) {
     E.args = args;
     E.device = args.device;
     CK(cudaSetDevice(E.device));
     cudaDeviceProp prop;
     CK(cudaGetDeviceProperties(&prop, E.device));
     E.n_sms = prop.multiProcessorCount;
-    CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&E.stream_t, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&E.stream, cudaStreamNonBlocking, stream_priority));
+    CK(cudaStreamCreateWithPriority(&E.stream_t, cudaStreamNonBlocking, stream_priority));
     CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
     CK(cudaEventCreate(&E.ev_total0));
     CK(cudaEventCreate(&E.ev_total1));
@@ -1274,13 +1275,19 @@ RunResult run_rounds(Engine &E) {
     const uint64_t max_rounds = E.args.max_rounds ? E.args.max_rounds : (1ULL << 26);
     const unsigned grid_beside = (unsigned)std::min<size_t>(E.sims.size(), (size_t)E.n_sms);
     const unsigned grid_alone = (unsigned)std::min<size_t>(E.sims.size(), (size_t)E.n_sms * 2);
-    while (E.h_ctl->n_active > 0 || E.h_ctl->n_resident > 0) {
+    // The resident kernel runs on its own stream, decoupled from the global
+    // rounds: the main stream never waits for it.  A finished launch is
+    // relaunched at the next graph boundary; routed simulations are handed
+    // over (promote) on the main stream, between graphs, only while no
+    // resident launch is in flight.
+    bool res_inflight = false;
+    while (E.h_ctl->n_active > 0 || E.h_ctl->n_resident > 0 || res_inflight) {
         // every round advances each active simulation's horizon by at least
         // step_slice / lambda, so each live lineage expects >= step_slice
         // events per round: a valid run never reaches these bounds
         if (++graph_launches > max_rounds / rounds + (max_rounds % rounds ? 1 : 0))
             fail(NECSIM_E_TIMEOUT, "round limit reached (necsim_args.max_rounds)");
-        if (E.h_ctl->steps_total == last_steps && E.h_ctl->n_cur == last_live) {
+        if (E.h_ctl->steps_total == last_steps && E.h_ctl->n_cur == last_live && !res_inflight) {
             if (++stalled >= 64) fail(NECSIM_E_TIMEOUT, "no progress over 64 graph launches");
         } else {
             stalled = 0;
@@ -1289,22 +1296,30 @@ RunResult run_rounds(Engine &E) {
         last_live = E.h_ctl->n_cur;
         const bool global = E.h_ctl->n_active > 0;
         if (E.args.resident) {
-            // both streams are idle here: hand routed simulations to the
-            // resident kernel, then run it on its own stream beside the
-            // global rounds
-            CK(launch_promote(E.d_params, (uint32_t)E.sims.size(), E.stream));
-            CK(cudaMemsetAsync(&E.d_ctl->graph_done, 0, sizeof(int), E.stream));
-            CK(cudaEventRecord(E.ev_fork, E.stream));
-            CK(cudaStreamWaitEvent(E.stream_t, E.ev_fork, 0));
-            // beside global rounds: until they end (at most 64 rounds, so the
-            // global kernels never wait long for SM space); alone: long stretches
-            const uint32_t budget = global ? 64 : 256;
-            CK(cudaEventRecord(E.ev_res0, E.stream_t));
-            CK(launch_resident(E.kind, make_resident_args(E, budget, global ? &E.d_ctl->graph_done : nullptr),
-                               global ? grid_beside : grid_alone, E.stream_t));
-            CK(cudaEventRecord(E.ev_res1, E.stream_t));
-            rr.launches += 2;
-            rr.rounds_launched += 1;
+            if (res_inflight && cudaEventQuery(E.ev_res1) == cudaSuccess) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, E.ev_res0, E.ev_res1) == cudaSuccess) rr.resident_ms += ms;
+                res_inflight = false;
+            }
+            // n_resident counts the routed simulations too
+            if (!res_inflight && E.h_ctl->n_resident > 0) {
+                // hand routed simulations over, then run the resident kernel
+                // on its own stream beside the global rounds (short stretches
+                // while they run, so newly routed simulations wait little;
+                // long ones when only resident simulations are left)
+                CK(cudaStreamWaitEvent(E.stream, E.ev_res1, 0));  // the last resident launch has ended
+                CK(launch_promote(E.d_params, (uint32_t)E.sims.size(), E.stream));
+                CK(cudaEventRecord(E.ev_fork, E.stream));
+                CK(cudaStreamWaitEvent(E.stream_t, E.ev_fork, 0));
+                const uint32_t budget = global ? 32 : 256;
+                CK(cudaEventRecord(E.ev_res0, E.stream_t));
+                CK(launch_resident(E.kind, make_resident_args(E, budget, nullptr), global ? grid_beside : grid_alone,
+                                   E.stream_t));
+                CK(cudaEventRecord(E.ev_res1, E.stream_t));
+                res_inflight = true;
+                rr.launches += 2;
+                rr.rounds_launched += 1;
+            }
         }
         if (global) {
             if (E.delivery) {
@@ -1319,14 +1334,15 @@ RunResult run_rounds(Engine &E) {
             } else {
                 enqueue_rounds(E, rounds, true, false);
             }
-            CK(cudaMemsetAsync(&E.d_ctl->graph_done, 1, sizeof(int), E.stream));
             rr.launches += (uint64_t)rounds * ((E.learned ? 9 : 5) + (E.coop_max ? 1 : 0));
             // after an even number of rounds the live lineages are in A
             if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_rows, E.trace_counts,
                                                     E.trace_rows_cap, E.stream));
             rr.rounds_launched += rounds;
+        } else if (res_inflight) {
+            // only resident simulations are left: wait for their launch
+            CK(cudaEventSynchronize(E.ev_res1));
         }
-        if (E.args.resident) CK(cudaStreamWaitEvent(E.stream, E.ev_res1, 0));
         CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
         E.d2h_bytes += sizeof(Control);
         CK(cudaStreamSynchronize(E.stream));
@@ -1336,11 +1352,13 @@ RunResult run_rounds(Engine &E) {
                 if (cudaEventElapsedTime(&ms, E.ev_start[r], E.ev_end[r]) == cudaSuccess) rr.kernel_ms += ms;
             }
         }
-        if (E.args.resident) {
-            float ms = 0.f;
-            if (cudaEventElapsedTime(&ms, E.ev_res0, E.ev_res1) == cudaSuccess) rr.resident_ms += ms;
-        }
         if (E.h_ctl->status & ~kErrDedupFull) break;
+    }
+    if (res_inflight) CK(cudaEventSynchronize(E.ev_res1));
+    // the resident stream's work is part of the run
+    if (E.args.resident) {
+        CK(cudaEventRecord(E.ev_fork, E.stream_t));
+        CK(cudaStreamWaitEvent(E.stream, E.ev_fork, 0));
     }
     CK(cudaEventRecord(E.ev_total1, E.stream));
     CK(cudaEventSynchronize(E.ev_total1));
@@ -1799,61 +1817,91 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
 // canonical schedule of every simulation depends only on that simulation,
 // so the split changes no result.
 struct BatchRun {
-    std::vector<std::unique_ptr<Engine>> engines;  // engines[0]: the others (empty: none); then one per priority simulation
-    std::vector<std::vector<uint32_t>> members;    // batch indices of each engine's simulations
+    // engines[0 .. n_groups): the priority groups of the simulations that do
+    // not run alone, in decreasing stream priority (engines[0] may be empty);
+    // then one engine per priority simulation
+    std::vector<std::unique_ptr<Engine>> engines;
+    std::vector<std::vector<uint32_t>> members;  // batch indices of each engine's simulations
     std::vector<Remaining> rem;
+    size_t n_groups = 1;
 };
 
-// The priority simulations of a batch: priority_list's first priority_sims
-// entries, else with the learned schedule the model's longest-lived
-// priority_sims (default 2), at most all but one simulation.
-std::vector<uint32_t> choose_priority(const std::vector<SimHost> &sims, const necsim_args &args) {
+// The batch's simulations in priority order: with the learned schedule the
+// lifetime model's longest-lived first, else batch order; then the priority
+// simulations are priority_list's first priority_sims entries, else with the
+// learned schedule the order's first priority_sims (default 2), at most all
+// but one simulation.
+void choose_priority(const std::vector<SimHost> &sims, const necsim_args &args, std::vector<uint32_t> &order,
+                     std::vector<uint32_t> &prio) {
     const uint32_t n = (uint32_t)sims.size();
-    std::vector<uint32_t> out;
-    if (n < 2 || args.report_dispersal) return out;
+    order.resize(n);
+    for (uint32_t j = 0; j < n; ++j) order[j] = j;
+    prio.clear();
+    const bool learned = args.schedule == 1 && args.model;
+    if (learned && n > 1) {
+        const std::vector<float> score = score_simulations(args.model, sims);
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return score[a] > score[b]; });
+    }
+    if (n < 2 || args.report_dispersal) return;
     if (args.priority_list && args.priority_sims) {
         std::vector<uint8_t> seen(n, 0);
         for (uint32_t k = 0; k < args.priority_sims; ++k) {
             const uint32_t j = args.priority_list[k];
             if (j >= n) fail(NECSIM_E_INVALID_ARGUMENT, "priority_list names a simulation outside the batch");
-            if (!seen[j]) out.push_back(j);
+            if (!seen[j]) prio.push_back(j);
             seen[j] = 1;
         }
-        if (out.size() >= n) out.pop_back();  // keep one simulation for the shared engine
-        return out;
+        if (prio.size() >= n) prio.pop_back();  // keep one simulation for the shared engines
+        return;
     }
-    if (args.schedule != 1 || !args.model) return out;
+    if (!learned) return;
     const uint32_t k = std::min<uint32_t>(args.priority_sims ? args.priority_sims : 2, n - 1);
-    const std::vector<float> score = score_simulations(args.model, sims);
-    std::vector<uint32_t> order(n);
-    for (uint32_t j = 0; j < n; ++j) order[j] = j;
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return score[a] > score[b]; });
-    out.assign(order.begin(), order.begin() + k);
-    return out;
+    prio.assign(order.begin(), order.begin() + k);
+}
+
+// Stream priority of priority level g (0: the device's greatest); levels
+// beyond the device's range share its least priority.
+int stream_priority_level(int device, size_t g) {
+    int least = 0, greatest = 0;
+    CK(cudaSetDevice(device));
+    CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    return (int)std::min<long long>((long long)greatest + (long long)g, (long long)least);
 }
 
 void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &args) {
-    const std::vector<uint32_t> prio = choose_priority(sims, args);
+    std::vector<uint32_t> order, prio;
+    choose_priority(sims, args, order, prio);
     std::vector<uint8_t> is_prio(sims.size(), 0);
     for (uint32_t j : prio) is_prio[j] = 1;
-    std::vector<SimHost> rest;
     std::vector<uint32_t> rest_ids;
-    for (uint32_t j = 0; j < sims.size(); ++j)
-        if (!is_prio[j]) {
-            rest.push_back(sims[j]);
-            rest_ids.push_back(j);
-        }
+    for (uint32_t j : order)
+        if (!is_prio[j]) rest_ids.push_back(j);
+    // the others in priority groups: contiguous runs of the order, sizes
+    // differing by at most one
+    const size_t groups = std::max<size_t>(1, std::min<size_t>(args.priority_groups, rest_ids.size()));
     b.engines.clear();
     b.members.clear();
-    auto add = [&](std::vector<SimHost> part, std::vector<uint32_t> ids) {
+    b.n_groups = groups;
+    const bool staggered = groups > 1;
+    auto add = [&](std::vector<uint32_t> ids, int level) {
+        std::vector<SimHost> part;
+        // an engine's simulations in batch order
+        std::sort(ids.begin(), ids.end());
+        for (uint32_t j : ids) part.push_back(sims[j]);
         b.engines.emplace_back(new Engine());
         Engine &E = *b.engines.back();
-        setup_engine(E, args);
+        setup_engine(E, args, level);
         prepare_engine(E, std::move(part), args, nullptr, nullptr);
         b.members.push_back(std::move(ids));
     };
-    add(std::move(rest), std::move(rest_ids));
-    for (uint32_t j : prio) add({sims[j]}, {j});
+    size_t at = 0;
+    for (size_t g = 0; g < groups; ++g) {
+        const size_t len = rest_ids.size() / groups + (g < rest_ids.size() % groups ? 1 : 0);
+        std::vector<uint32_t> ids(rest_ids.begin() + at, rest_ids.begin() + at + len);
+        at += len;
+        add(std::move(ids), staggered ? stream_priority_level(args.device, g) : 0);
+    }
+    for (uint32_t j : prio) add({j}, staggered ? stream_priority_level(args.device, 0) : 0);
     b.rem.assign(b.engines.size(), Remaining{});
 }
 
@@ -2310,7 +2358,7 @@ int necsim_gpu_batch_run(necsim_batch *b, const necsim_reporter *reporters, necs
 int necsim_gpu_batch_priority(const necsim_batch *b, uint32_t *ids, uint32_t cap, uint32_t *n) {
     if (!b || !n || (cap && !ids)) return NECSIM_E_INVALID_ARGUMENT;
     uint32_t k = 0;
-    for (size_t e = 1; e < b->run.members.size(); ++e)
+    for (size_t e = b->run.n_groups; e < b->run.members.size(); ++e)
         for (uint32_t j : b->run.members[e]) {
             if (k < cap) ids[k] = j;
             ++k;

@@ -631,6 +631,17 @@ __device__ __forceinline__ void coop_outcome(const Lane &l, const SimParams &p, 
                                              uint64_t e1, uint64_t e2, uint64_t e3, uint64_t e4, bool active,
                                              CoopOutcome &o) {
     o.code = kStepDropped;
+    if (KIND == kNonSpatial || KIND == kSpatiallyImplicit || KIND == kAlmostInfiniteNormal) {
+        // no loads and no rejection loop: every lane computes both outcomes
+        // without branching, so the warp's instruction stream stays one
+        // block that interleaves with the bucket view's
+        const bool spec = (e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y);
+        uint32_t err = 0;
+        event_target<KIND, 4>(l, p, rs, e2, e3, e4, o.tx, o.ty, o.ti, o.rec, err);
+        o.loc_next = location_term(seed, injection_at<KIND>(p, o.tx, o.ty, o.ti, o.rec));
+        o.code = !active ? kStepDropped : (spec ? kStepSpeciated : kStepMoved);
+        return;
+    }
     if (!active) return;
     if ((e1 >> 11) < speciation_threshold<KIND>(p, l.x, l.y)) {
         o.code = kStepSpeciated;
@@ -729,6 +740,9 @@ __device__ __forceinline__ int coop_run(Lane &l, const SimParams &p, const Event
                     mine = t2;
                     mine_k = 2;
                 }
+                // candidate view: the event this lane's pair would be
+                coop_outcome<KIND>(l, p, seed, s, d1, d2, d3, d4, speculate, o);
+                // rare: a bucket with more than three events
                 if (bucket_lane && n_ev > 3u) {
                     for (uint32_t kk = 3; kk < n_ev; ++kk) {
                         const long long eb = event_time_bits(step_start, draw_at(s, kk + 2u), delta_t);
@@ -738,8 +752,6 @@ __device__ __forceinline__ int coop_run(Lane &l, const SimParams &p, const Event
                         }
                     }
                 }
-                // candidate view: the event this lane's pair would be
-                coop_outcome<KIND>(l, p, seed, s, d1, d2, d3, d4, speculate, o);
                 const unsigned found = __ballot_sync(kFull, bucket_lane && mine != kNoEvent);
                 if (found) {
                     b_sel = (uint32_t)(__ffs(found) - 1);

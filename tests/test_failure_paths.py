@@ -30,7 +30,7 @@ def test_tables_argument_mirrors_header(nb):
     """The ctypes mirror carries the new trailing fields in the header's order."""
     names = [f for f, _ in nb.CScenario._fields_]
     assert names[-3:] == ["cells", "atoms", "n_atoms"]
-    assert [f for f, _ in nb.CArgs._fields_][-4:] == ["max_rounds", "priority_sims", "pad_priority", "priority_list"]
+    assert [f for f, _ in nb.CArgs._fields_][-4:] == ["max_rounds", "priority_sims", "priority_groups", "priority_list"]
     assert nb.lib().necsim_abi_version() == 2
 
 
