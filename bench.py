@@ -7,9 +7,12 @@ to completion in one batched launch per round.  One step = one full batch.
 
   value      events/sec of the learned-scheduled kernel (the step queue
              ordered by the lifetime model, trained first on traces the
-             backend generates) with the origins resident in HBM (device time
-             of the whole batch measured with CUDA events by the library, max
-             over ranks), events = executed lineage steps
+             backend generates, and the model's longest-lived simulations in
+             engines of their own) with the origins resident in HBM (device
+             time of the whole batch measured with CUDA events by the
+             library, max over ranks), events = executed lineage steps;
+             simulations down to 8 lineages continue in the per-simulation
+             resident kernel on a stream of their own (both arms)
   plain      the same for the plain (unordered) kernel on the same workload,
              with `learned_over_plain` and `outcomes_identical` (the two arms'
              steps, species, speciation and duplicate counts, times)
@@ -71,8 +74,9 @@ def parse():
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--once", action="store_true",
-                   help="profiling aid: one run of the workload's batch (plain schedule), then print its "
-                        "events and device time; no timing arms, baselines or training")
+                   help="profiling aid: one run of the workload's batch (plain schedule, the resident "
+                        "kernel as in the timed arm), then print its events and device time; no timing "
+                        "arms, baselines or training")
     p.add_argument("--no-secondary", action="store_true",
                    help="skip the secondary workloads (C3 in full, C5 to t=400) beside the sweep")
     p.add_argument("--pause", type=float, default=None,
@@ -262,8 +266,8 @@ def cpu_sample(sims, pause, threads, sampler="poisson", counts=None):
 def cpu_sample_desc(name, pause, n, threads=1):
     parts = cpu_partitions(n, threads)
     split = (", each in %d IsolatedIndividuals partitions" % parts) if parts > 1 else ""
-    return "%s: all %d simulation(s) advanced to t=%g (pause_before) with the reference schedule%s" % (
-        name, n, pause, split)
+    horizon = "to completion" if pause is None else "advanced to t=%g (pause_before)" % pause
+    return "%s: all %d simulation(s) %s with the reference schedule%s" % (name, n, horizon, split)
 
 
 def reference_arm(args, dist):
@@ -365,10 +369,12 @@ def canonical_work(sims, algo, pause, threads, sampler):
             "sample": "%d of %d simulation(s) to t=%g" % (len(pick), len(sims), pause)}
 
 
-# DRAM bytes (read + write) per executed event of the round kernels, from the
-# ncu capture summarised in profiles/ (dram__bytes_read.sum +
-# dram__bytes_write.sum over every launch of the capture / its events)
-DRAM_BYTES_PER_EVENT = {}
+# DRAM bytes (read + write) per executed event of the round kernels (the
+# cooperative kernel and the step kernel), from ncu captures of every launch
+# of `bench.py --workload <w> --once` (dram__bytes_read.sum +
+# dram__bytes_write.sum of those kernels / the run's events): the sweep's
+# figure is the 16-simulation sweep's to t = 3000, scaled by events
+DRAM_BYTES_PER_EVENT = {"c4": 1.95, "c4-small": 1.95, "c3": 36.5}
 
 
 def issue_roofline(nb, device, work, events, kernel_ms, launches, workload_name):
@@ -485,11 +491,15 @@ def main():
     nus = [d["speciation_probability"] for d, _ in sims]
     seeds = [s for _, s in sims]
     device = dist.local_rank if dist.world > 1 else 0
+    # batches: simulations down to 8 lineages (one per warp of a resident
+    # block) continue in the resident kernel on a stream of their own,
+    # decoupled from the global rounds
+    resident = True if len(sims) > 1 else False
     if args.once:
-        with nb.Batch(scen, nus, seeds, nb.CUDA(device=device, event_time_sampler=args.event_time_sampler),
-                      pause_before=args.pause) as b:
+        with nb.Batch(scen, nus, seeds, nb.CUDA(device=device, event_time_sampler=args.event_time_sampler,
+                                                resident=resident), pause_before=args.pause) as b:
             outs = b.run()
-        print(json.dumps({"workload": args.workload, "pause_before": args.pause,
+        print(json.dumps({"workload": args.workload, "pause_before": args.pause, "resident": resident,
                           "events": sum(o.steps for o in outs), "ms": outs[0].total_ms,
                           "rounds": outs[0].n_step_launches}), flush=True)
         dist.close()
@@ -500,7 +510,7 @@ def main():
     model, model_info = None, None
     if args.schedule in ("learned", "both"):
         model, model_info = train_lifetime_model(nb, syn, device, args.train_pause)
-    plain_algo = nb.CUDA(device=device, event_time_sampler=args.event_time_sampler)
+    plain_algo = nb.CUDA(device=device, event_time_sampler=args.event_time_sampler, resident=resident)
     tune_info = None
     if args.autotune == "on" or (args.autotune == "auto" and args.workload.startswith("c4")):
         t0 = time.perf_counter()
@@ -541,10 +551,23 @@ def main():
     # visit (4 u32 + 5 u64/f64 + 1 flag, 57 B each way), speciation events
     # written (40 B) and, for SpatiallyExplicit, one 32-B cell record and one
     # 32-B atom sector per event
+    # The round kernels' rooflines need every event to run in them: with the
+    # resident kernel on they come from one more run with it off.
+    r_steps, r_visits, r_spec = steps, visits, n_spec
+    r_kernel_ms, r_launches = head["kernel_ms"], head["step_launches"]
+    roof_note = "the timed runs"
+    if resident:
+        with nb.Batch(scen, nus, seeds, nb.CUDA(**{**plain_algo.__dict__, "resident": False}),
+                      pause_before=args.pause) as b:
+            b.run()
+            ro = b.run()
+        r_steps, r_spec = sum(o.steps for o in ro), sum(o.n_speciation for o in ro)
+        r_visits, r_kernel_ms, r_launches = ro[0].lineage_visits, ro[0].kernel_ms, ro[0].n_step_launches
+        roof_note = "one run with the resident kernel off (every event in the round kernels)"
     state_bytes = 2 * 57
-    alg_bytes = visits * state_bytes + n_spec * 40 + (steps * 64 if se else 0)
-    avg_launch_ms = head["kernel_ms"] / max(head["step_launches"], 1)
-    per_launch_bytes = alg_bytes / max(head["step_launches"], 1)
+    alg_bytes = r_visits * state_bytes + r_spec * 40 + (r_steps * 64 if se else 0)
+    avg_launch_ms = r_kernel_ms / max(r_launches, 1)
+    per_launch_bytes = alg_bytes / max(r_launches, 1)
     achieved = per_launch_bytes / (avg_launch_ms / 1e3) / 1e9 if avg_launch_ms > 0 else 0.0
     peak, peak_kind = load_peaks()
 
@@ -553,7 +576,8 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+u64",
         "data": "synthetic",
-        "config": {"workload": desc, "schedule": "learned" if model else "plain", "kind": kind,
+        "config": {"workload": desc, "schedule": "learned" if model else "plain",
+                   "resident": resident, "kind": kind,
                    "pause_before": args.pause, "event_time_sampler": args.event_time_sampler,
                    "simulations": len(sims), "lineages": int(sum(o.n_initial for o in outs)),
                    "l2": "inputs larger than L2 (lineage state %.2f GB)" % (
@@ -568,8 +592,7 @@ def main():
                          "frac": achieved / peak,
                          "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)",
                          "kernel": "coop_kernel + step_kernel", "avg_launch_ms": avg_launch_ms,
-                         "launches": head["step_launches"],
-                         "round_kernels_ms_per_step": head["kernel_ms"] / args.steps},
+                         "launches": r_launches, "round_kernels_ms": r_kernel_ms, "timed": roof_note},
         # the per-simulation resident kernel runs the small simulations' rounds
         # on a second stream: a latency-bound chain of dependent 64-bit hash
         # multiplies per lineage, not a bandwidth roofline
@@ -608,13 +631,19 @@ def main():
                               "pause_before": args.cpu_sample_pause, "events": sum(o.steps for o in so),
                               "ms": so[0].total_ms, "schedule": "plain"}
     line["roofline"] = roofline_entry(nb, device, sims, plain_algo, args.cpu_sample_pause, threads,
-                                      args.event_time_sampler, steps, head["kernel_ms"], head["step_launches"],
+                                      args.event_time_sampler, r_steps, r_kernel_ms, r_launches,
                                       args.workload)
+    line["roofline"]["timed"] = roof_note
     if dist.rank == 0 and dist.world == 1 and args.workload == "c4" and not args.no_secondary:
+        def guarded(*a):
+            try:
+                return secondary(*a)
+            except Exception as e:  # a secondary never costs the headline line
+                return {"error": "%s: %s" % (type(e).__name__, e)}
         line["secondary"] = {
-            "c3": secondary(nb, "c3", None, device, threads, args.event_time_sampler, ""),
+            "c3": guarded(nb, "c3", None, device, threads, args.event_time_sampler, ""),
             # one thread: every oracle partition would build its own 5 GB alias table
-            "c5_t400": secondary(nb, "c5", 400.0, device, 1, args.event_time_sampler, ""),
+            "c5_t400": guarded(nb, "c5", 400.0, device, 1, args.event_time_sampler, ""),
         }
     if model is not None:
         model.close()
