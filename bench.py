@@ -69,8 +69,9 @@ def parse():
     p.add_argument("--autotune", default="auto", choices=["auto", "on", "off"],
                    help="pick block size, step_slice and dedup factor by timing a paused sample first "
                         "(auto: on for the batched sweeps)")
-    p.add_argument("--train-pause", type=float, default=3000.0,
-                   help="pause_before of the trace runs that train the lifetime model")
+    p.add_argument("--train-pause", type=float, default=None,
+                   help="pause_before of the trace runs that train the lifetime model (default: to "
+                        "completion, so that every snapshotted lineage has its remaining events as label)")
     p.add_argument("--cpu-sample-pause", type=float, default=400.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--once", action="store_true",
@@ -314,7 +315,9 @@ def train_lifetime_model(nb, syn, device, pause):
     """The learned scheduler's model, trained before anything is timed on
     traces the backend generates from the AlmostInfinite circle (r = 100,
     sigma = 10) and the SpatiallyExplicit 64x64 landscape, each over a
-    sweep of speciation probabilities, every run paused at `pause`."""
+    sweep of speciation probabilities, and a SpatiallyImplicit sweep, every
+    run paused at `pause` (None: to completion; a paused run labels only the
+    lineages that end before the pause, so long lives go unseen)."""
     ai, _ = syn.config2()
     se, _ = syn.config3()
     X, y = [], []
@@ -326,15 +329,17 @@ def train_lifetime_model(nb, syn, device, pause):
                                    max_rows=1 << 17)
         X.append(xs)
         y.append(ys)
-    # SpatiallyImplicit traces from a sweep of the same family with other
-    # parameters (sweep seed 99, local communities of at most 2e4 cells,
-    # speciation raised 100-fold so lineages end within the trace horizon)
-    si = syn.config4(n_sims=16, sweep_seed=99, max_local=20000)
-    xs, ys = nb.collect_traces([syn.to_scenario(d) for d, _ in si],
-                               [d["speciation_probability"] * 100 for d, _ in si], [1000 + s for _, s in si],
-                               nb.CUDA(device=device), pause_before=pause, snapshot_rounds=16, max_rows=1 << 17)
-    X.append(xs)
-    y.append(ys)
+    # SpatiallyImplicit traces from two sweeps of the same family with other
+    # parameters (sweep seeds 99 and 98, speciation raised 100- and 10-fold
+    # so that the runs end quickly)
+    for sweep_seed, factor in ((99, 100.0), (98, 10.0)):
+        si = syn.config4(n_sims=64, sweep_seed=sweep_seed)
+        xs, ys = nb.collect_traces([syn.to_scenario(d) for d, _ in si],
+                                   [d["speciation_probability"] * factor for d, _ in si],
+                                   [1000 + s for _, s in si], nb.CUDA(device=device), pause_before=pause,
+                                   snapshot_rounds=4, max_rows=1 << 17)
+        X.append(xs)
+        y.append(ys)
     X = np.concatenate(X)
     y = np.concatenate(y)
     model = nb.LifetimeModel(seed=1, device=device)
@@ -342,8 +347,9 @@ def train_lifetime_model(nb, syn, device, pause):
     info = {"trace_rows": int(X.shape[0]), "epochs": 8, "final_loss": float(losses[-1]),
             "label_variance": float(np.var(y)), "seconds": time.perf_counter() - t0,
             "traces": "AlmostInfinite r=100 sigma=10 and SpatiallyExplicit 64x64, speciation "
-                      "{1e-2,1e-3,1e-4}, and 16 SpatiallyImplicit simulations of another sweep (seed 99, "
-                      "J <= 2e4, speciation x100), paused at t=%g" % pause}
+                      "{1e-2,1e-3,1e-4}, and two SpatiallyImplicit sweeps of 64 simulations (seeds 99 and "
+                      "98, speciation x100 and x10), " + ("to completion" if pause is None else
+                                                         "paused at t=%g" % pause)}
     return model, info
 
 

@@ -145,13 +145,13 @@ typedef struct necsim_args {
                                   NECSIM_E_TIMEOUT; 0 = default 2^26.  Every round advances each
                                   live lineage by >= step_slice expected events, so a valid run
                                   only meets a limit chosen below its round count */
-    uint32_t priority_sims;    /* batches: this many simulations run in engines of their own (own
+    uint32_t priority_sims;    /* batches: this many simulations run in one priority engine (own
                                   rounds, stream and host thread) beside the others, so the others'
                                   rounds never hold them back: those in priority_list, else (schedule
                                   1) the ones the lifetime model scores as longest-lived; 0 = none,
-                                  or 2 with schedule 1.  Results are identical either way */
-    uint32_t priority_groups;  /* batches: the simulations that do not run alone split into this
-                                  many engines (0 or 1: one), contiguous runs of the priority order
+                                  or 8 with schedule 1.  Results are identical either way */
+    uint32_t priority_groups;  /* batches: the simulations outside the priority engine split into
+                                  this many engines (0 or 1: one), contiguous runs of the priority order
                                   (schedule 1: the lifetime model's longest-lived first, else batch
                                   order) whose streams have decreasing CUDA stream priority, so the
                                   first groups' rounds go first and their tails start early.
@@ -285,9 +285,9 @@ int necsim_gpu_batch_create(const necsim_scenario *scenarios, const uint64_t *wy
                             necsim_batch **out);
 int necsim_gpu_batch_run(necsim_batch *batch, const necsim_reporter *reporters,
                          necsim_outcome *outcomes);
-/* The batch indices of the simulations that run in engines of their own
- * (necsim_args.priority_sims): up to `cap` into `ids`, their count in *n.
- * No reference counterpart. */
+/* The batch indices of the simulations in the priority engine
+ * (necsim_args.priority_sims), in priority order: up to `cap` into `ids`,
+ * their count in *n.  No reference counterpart. */
 int necsim_gpu_batch_priority(const necsim_batch *batch, uint32_t *ids, uint32_t cap, uint32_t *n);
 const char *necsim_gpu_batch_last_error(const necsim_batch *batch);
 void necsim_gpu_batch_destroy(necsim_batch *batch);
@@ -500,14 +500,17 @@ int necsim_gpu_autotune(const necsim_scenario *scenarios, const uint64_t *wyhash
 
 /* ---- learned lifetime scheduler ----
  * A small MLP (8 -> 64 -> 64 -> 1, ReLU, bf16 weights, fp32 accumulation)
- * predicting log(1 + remaining events) of a lineage from 8 features
- * (position in the extent, habitat, dispersal entropy, time, speciation
- * probability, live lineages of its simulation, events executed).  With
- * necsim_args.schedule = 1 and .model set, every round's step queue is
- * bucketed by expected work (min(events per round, predicted remaining)),
- * largest first.  The model only reorders work: events, species counts and
- * step counts are the same as with schedule = 0.  There is no reference
- * interface for this part (it is new in this backend). */
+ * predicting, from one lineage's 8 features (position in the extent,
+ * habitat, dispersal entropy, time, speciation probability, live lineages of
+ * its simulation, events executed), log(1 + remaining events) of its
+ * simulation's longest-lived lineage: the simulation's remaining life.  With
+ * necsim_args.schedule = 1 and .model set, a batch's simulations with the
+ * longest predicted lives run in a priority engine of their own
+ * (necsim_args.priority_sims) and every round's step queue is bucketed by
+ * expected work (min(events per round, prediction)), largest first.  The
+ * model only reorders work: events, species counts and step counts are the
+ * same as with schedule = 0.  There is no reference interface for this part
+ * (it is new in this backend). */
 #define NECSIM_MODEL_FEATURES 8
 #define NECSIM_MODEL_PARAMS 4801 /* W1[64][8], b1[64], W2[64][64], b2[64], W3[64], b3 */
 

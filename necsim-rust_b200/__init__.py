@@ -427,9 +427,9 @@ class CUDA:
     # watchdog: a run still active after this many rounds fails with
     # NECSIM_E_TIMEOUT (checked between graph launches); 0: 2^26
     max_rounds: int = 0
-    # batches: simulations run in engines of their own beside the others
+    # batches: simulations run in one priority engine beside the others
     # (their own rounds); `priority_list` names them (batch indices), else the
-    # learned schedule's model picks `priority_sims` of them (default 2)
+    # learned schedule's model picks `priority_sims` of them (default 8)
     priority_sims: int = 0
     priority_list: Optional[Sequence[int]] = None
     # batches: the other simulations in this many engines of decreasing CUDA
@@ -817,7 +817,7 @@ class Batch:
 
     @property
     def priority(self) -> List[int]:
-        """Batch indices of the simulations running in engines of their own."""
+        """Batch indices of the simulations in the priority engine, in priority order."""
         n = ctypes.c_uint32(0)
         ids = (ctypes.c_uint32 * max(1, self.n))()
         rc = lib().necsim_gpu_batch_priority(self._b, ids, self.n, ctypes.byref(n))
@@ -918,8 +918,9 @@ def _f32(a, shape_tail=None):
 
 class LifetimeModel:
     """The MLP (8 -> 64 -> 64 -> 1, bf16 weights, fp32 accumulation) that
-    predicts log(1 + remaining events) of a lineage; trained and evaluated
-    by the backend's own CUDA kernels on `device`."""
+    predicts, from a lineage's features, log(1 + remaining events) of its
+    simulation's longest-lived lineage; trained and evaluated by the
+    backend's own CUDA kernels on `device`."""
 
     def __init__(self, seed: int = 0, device: int = 0):
         L = lib()
@@ -1001,7 +1002,8 @@ def collect_traces(scenarios: Sequence, speciations: Sequence[float], seeds: Seq
                    algorithm: Optional[CUDA] = None, pause_before: Optional[float] = None,
                    snapshot_rounds: int = 32, max_rows: int = 1 << 18):
     """Training traces generated by the backend itself: (features [n, 8],
-    labels [n] = log(1 + remaining events)) of lineages snapshotted every
+    labels [n] = log(1 + remaining events of the simulation's longest-lived
+    lineage at that snapshot)) of lineages snapshotted every
     `snapshot_rounds` rounds of a batch run."""
     L = lib()
     n = len(scenarios)

@@ -663,6 +663,7 @@ struct Engine {
     TraceDeath *trace_deaths = nullptr;
     unsigned long long *trace_counts = nullptr;  // [0] rows, [1] deaths
     uint64_t trace_rows_cap = 0, trace_deaths_cap = 0;
+    uint32_t trace_snap = 0;  // index of the next snapshot
 
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<cudaEvent_t> ev_start, ev_end;
@@ -918,15 +919,14 @@ void for_each_origin(const necsim_scenario &sc, F &&push) {
 
 // ---- per-simulation priority of the learned schedule ----
 
-// The lifetime model's score of each simulation, its expected time to end:
-// a simulation ends with its longest-lived lineage, and the expected largest
-// of n independent exponential lifetimes of mean m is m * H(n) (H the
-// harmonic number).  m is the largest predicted remaining event count
-// (expm1 of the model's output) over up to 32 of its origin lineages, evenly
-// spaced in origin order, at the start of the run (no event executed, the
-// simulation's origin count live); n is its origin count.  The features are
-// the kernels' (lineage_features_of), with a SpatiallyExplicit cell's
-// habitat and dispersal entropy read from the maps.
+// The lifetime model's score of each simulation, its expected remaining
+// life: the model is trained to predict, from one lineage's features, the
+// log remaining events of that lineage's simulation (of its longest-lived
+// lineage, with which the simulation ends).  The score is the mean
+// prediction over up to 32 of its origin lineages, evenly spaced in origin
+// order, at the start of the run (no event executed, the simulation's origin
+// count live).  The features are the kernels' (lineage_features_of), with a
+// SpatiallyExplicit cell's habitat and dispersal entropy read from the maps.
 std::vector<float> score_simulations(necsim_model *m, const std::vector<SimHost> &sims) {
     constexpr uint64_t kSample = 32;
     std::vector<float> X;
@@ -968,18 +968,15 @@ std::vector<float> score_simulations(necsim_model *m, const std::vector<SimHost>
     std::vector<float> y(n);
     CK(cudaMemcpyAsync(y.data(), r.y, n * sizeof(float), cudaMemcpyDeviceToHost, m->stream));
     CK(cudaStreamSynchronize(m->stream));
-    for (uint64_t j = 0; j < n; ++j)
-        score[owner[j]] = std::max(score[owner[j]], std::expm1(std::min(std::max(y[j], 0.f), 40.f)));
-    for (size_t s = 0; s < sims.size(); ++s) {
-        // H(n): summed below 64, else ln n + Euler's gamma + 1 / 2n
-        const uint64_t no = sims[s].n_origins;
-        double harmonic = 0.0;
-        if (no < 64)
-            for (uint64_t i = 1; i <= no; ++i) harmonic += 1.0 / (double)i;
-        else
-            harmonic = std::log((double)no) + 0.5772156649 + 0.5 / (double)no;
-        score[s] = (float)(score[s] * harmonic);
+    // the model predicts the simulation's remaining life (log events) from
+    // each lineage: the score is the mean over the sampled origins
+    std::vector<uint32_t> count(sims.size(), 0);
+    for (uint64_t j = 0; j < n; ++j) {
+        score[owner[j]] += y[j];
+        count[owner[j]] += 1;
     }
+    for (size_t s = 0; s < sims.size(); ++s)
+        if (count[s]) score[s] /= (float)count[s];
     return score;
 }
 
@@ -1262,8 +1259,8 @@ RunResult run_rounds(Engine &E) {
     CK(cudaMemcpyAsync(E.d_counters, cs.data(), cs.size() * sizeof(SimCounters), cudaMemcpyHostToDevice, E.stream));
     CK(launch_schedule(make_schedule_args(E), E.stream));
     rr.launches += 1;
-    if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_rows, E.trace_counts,
-                                            E.trace_rows_cap, E.stream));
+    if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_snap++, E.trace_rows,
+                                            E.trace_counts, E.trace_rows_cap, E.stream));
     CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
     uint64_t graph_launches = 0;
@@ -1336,8 +1333,8 @@ RunResult run_rounds(Engine &E) {
             }
             rr.launches += (uint64_t)rounds * ((E.learned ? 9 : 5) + (E.coop_max ? 1 : 0));
             // after an even number of rounds the live lineages are in A
-            if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_rows, E.trace_counts,
-                                                    E.trace_rows_cap, E.stream));
+            if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_snap++, E.trace_rows,
+                                                    E.trace_counts, E.trace_rows_cap, E.stream));
             rr.rounds_launched += rounds;
         } else if (res_inflight) {
             // only resident simulations are left: wait for their launch
@@ -1817,19 +1814,20 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
 // canonical schedule of every simulation depends only on that simulation,
 // so the split changes no result.
 struct BatchRun {
-    // engines[0 .. n_groups): the priority groups of the simulations that do
-    // not run alone, in decreasing stream priority (engines[0] may be empty);
-    // then one engine per priority simulation
+    // engines[0 .. n_groups): the priority groups of the simulations outside
+    // the priority engine, in decreasing stream priority (engines[0] may be
+    // empty); then the priority engine, when there are priority simulations
     std::vector<std::unique_ptr<Engine>> engines;
     std::vector<std::vector<uint32_t>> members;  // batch indices of each engine's simulations
     std::vector<Remaining> rem;
     size_t n_groups = 1;
+    std::vector<uint32_t> priority;  // the priority simulations, in priority order
 };
 
 // The batch's simulations in priority order: with the learned schedule the
 // lifetime model's longest-lived first, else batch order; then the priority
 // simulations are priority_list's first priority_sims entries, else with the
-// learned schedule the order's first priority_sims (default 2), at most all
+// learned schedule the order's first priority_sims (default 8), at most all
 // but one simulation.
 void choose_priority(const std::vector<SimHost> &sims, const necsim_args &args, std::vector<uint32_t> &order,
                      std::vector<uint32_t> &prio) {
@@ -1855,7 +1853,7 @@ void choose_priority(const std::vector<SimHost> &sims, const necsim_args &args, 
         return;
     }
     if (!learned) return;
-    const uint32_t k = std::min<uint32_t>(args.priority_sims ? args.priority_sims : 2, n - 1);
+    const uint32_t k = std::min<uint32_t>(args.priority_sims ? args.priority_sims : 8, n - 1);
     prio.assign(order.begin(), order.begin() + k);
 }
 
@@ -1901,7 +1899,10 @@ void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &ar
         at += len;
         add(std::move(ids), staggered ? stream_priority_level(args.device, g) : 0);
     }
-    for (uint32_t j : prio) add({j}, staggered ? stream_priority_level(args.device, 0) : 0);
+    // the priority simulations share one engine: their rounds wait for none
+    // of the others' (and the others' for none of theirs)
+    if (!prio.empty()) add(prio, staggered ? stream_priority_level(args.device, 0) : 0);
+    b.priority = prio;
     b.rem.assign(b.engines.size(), Remaining{});
 }
 
@@ -2358,11 +2359,10 @@ int necsim_gpu_batch_run(necsim_batch *b, const necsim_reporter *reporters, necs
 int necsim_gpu_batch_priority(const necsim_batch *b, uint32_t *ids, uint32_t cap, uint32_t *n) {
     if (!b || !n || (cap && !ids)) return NECSIM_E_INVALID_ARGUMENT;
     uint32_t k = 0;
-    for (size_t e = b->run.n_groups; e < b->run.members.size(); ++e)
-        for (uint32_t j : b->run.members[e]) {
-            if (k < cap) ids[k] = j;
-            ++k;
-        }
+    for (uint32_t j : b->run.priority) {
+        if (k < cap) ids[k] = j;
+        ++k;
+    }
     *n = k;
     return NECSIM_OK;
 }
@@ -2662,32 +2662,26 @@ int necsim_gpu_trace_batch(const necsim_scenario *scenarios, const uint64_t *wyh
         unsigned long long counts[2] = {0, 0};
         CK(cudaMemcpy(counts, E.trace_counts, sizeof(counts), cudaMemcpyDeviceToHost));
         const uint64_t nr = std::min<uint64_t>(counts[0], E.trace_rows_cap);
-        const uint64_t nd = std::min<uint64_t>(counts[1], E.trace_deaths_cap);
         std::vector<TraceRow> rows(nr);
-        std::vector<TraceDeath> deaths(nd);
         if (nr) CK(cudaMemcpy(rows.data(), E.trace_rows, nr * sizeof(TraceRow), cudaMemcpyDeviceToHost));
-        if (nd) CK(cudaMemcpy(deaths.data(), E.trace_deaths, nd * sizeof(TraceDeath), cudaMemcpyDeviceToHost));
-        // (simulation, global reference) -> step count at death
-        struct KeyHash {
-            size_t operator()(const std::pair<uint32_t, uint64_t> &k) const {
-                return std::hash<uint64_t>()(k.second * 0x9e3779b97f4a7c15ULL ^ (uint64_t)k.first);
-            }
-        };
-        std::unordered_map<std::pair<uint32_t, uint64_t>, uint64_t, KeyHash> death_steps;
-        death_steps.reserve(nd * 2 + 1);
-        for (const TraceDeath &d : deaths) death_steps[{d.sim, d.gref}] = d.steps;
-        std::vector<uint64_t> labelled;
-        labelled.reserve(nr);
-        for (uint64_t i = 0; i < nr; ++i) {
-            auto it = death_steps.find({rows[i].sim, rows[i].gref});
-            if (it != death_steps.end() && it->second >= rows[i].steps) labelled.push_back(i);
-        }
-        const uint64_t take = std::min<uint64_t>(max_rows, labelled.size());
+        // The label of a snapshotted lineage is the remaining life of its
+        // simulation: the simulation ends with its longest-lived lineage, at
+        // its largest event time t_end, so the label is log(1 + lambda
+        // (t_end - t)), the expected events of one lineage over the rest of
+        // the run from the lineage's time t.  (A paused run ends at its last
+        // event before the pause: its labels are censored there.)
+        std::vector<SimCounters> cs(E.sims.size());
+        CK(cudaMemcpy(cs.data(), E.d_counters, cs.size() * sizeof(SimCounters), cudaMemcpyDeviceToHost));
+        const uint64_t take = std::min<uint64_t>(max_rows, nr);
         for (uint64_t k = 0; k < take; ++k) {
-            // evenly spaced over the labelled rows (all snapshots, all sims)
-            const TraceRow &r = rows[labelled[(uint64_t)((double)k * (double)labelled.size() / (double)take)]];
+            // evenly spaced over the rows (all snapshots, all sims)
+            const TraceRow &r = rows[(uint64_t)((double)k * (double)nr / (double)take)];
             for (int j = 0; j < kFeat; ++j) features[k * kFeat + j] = r.f[j];
-            labels[k] = (float)std::log1p((double)(death_steps[{r.sim, r.gref}] - r.steps));
+            double t_end;
+            const unsigned long long bits = cs[r.sim].max_time_bits;
+            std::memcpy(&t_end, &bits, sizeof(double));
+            const double rest = std::max(0.0, t_end - r.time) * E.sims[r.sim].params.lambda;
+            labels[k] = (float)std::log1p(rest);
         }
         *n_rows = take;
     });

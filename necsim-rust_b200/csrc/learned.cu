@@ -114,17 +114,25 @@ __global__ void __launch_bounds__(256) lineage_predict_kernel(FeatureArgs a, con
     }
 }
 
-__global__ void trace_snapshot_kernel(FeatureArgs a, TraceRow *rows, unsigned long long *n_rows, uint64_t cap) {
+__global__ void trace_snapshot_kernel(FeatureArgs a, uint32_t snap, TraceRow *rows, unsigned long long *n_rows,
+                                      uint64_t cap) {
     const uint64_t n = *a.n_cur;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n; j += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t s = a.in.sim[j];
         if (!a.params[s].active) continue;
+        // about kTraceRowsPerSim rows per simulation and snapshot, so that
+        // large simulations do not crowd out the others
+        const uint64_t live = a.counters[s].n_live;
+        const uint64_t stride = live > kTraceRowsPerSim ? live / kTraceRowsPerSim : 1;
+        const uint64_t gref = a.in.gref[j];
+        if (stride > 1 && seahash_diffuse(gref ^ ((uint64_t)snap << 40)) % stride != 0) continue;
         TraceRow r;
         lineage_features(a.kind, a.params[s], a.counters[s], a.in.x[j], a.in.y[j], a.in.last[j], a.in.steps[j], r.f);
-        r.gref = a.in.gref[j];
+        r.gref = gref;
         r.steps = a.in.steps[j];
         r.sim = s;
-        r.pad = 0;
+        r.snap = snap;
+        r.time = a.in.last[j];
         const unsigned long long i = atomicAdd(n_rows, 1ULL);
         if (i < cap) rows[i] = r;
     }
@@ -386,9 +394,9 @@ unsigned current_sm_count() {
 
 }  // namespace
 
-cudaError_t launch_trace_snapshot(const FeatureArgs &f, TraceRow *rows, unsigned long long *n_rows, uint64_t cap,
-                                  cudaStream_t st) {
-    trace_snapshot_kernel<<<current_sm_count() * 4, 256, 0, st>>>(f, rows, n_rows, cap);
+cudaError_t launch_trace_snapshot(const FeatureArgs &f, uint32_t snap, TraceRow *rows, unsigned long long *n_rows,
+                                  uint64_t cap, cudaStream_t st) {
+    trace_snapshot_kernel<<<current_sm_count() * 4, 256, 0, st>>>(f, snap, rows, n_rows, cap);
     return cudaGetLastError();
 }
 

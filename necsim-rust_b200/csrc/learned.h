@@ -15,8 +15,9 @@
 
 namespace necsim {
 
-// MLP 8 -> 64 -> 64 -> 1 with ReLU hidden layers, predicting
-// log(1 + remaining events).  Parameters are one flat array:
+// MLP 8 -> 64 -> 64 -> 1 with ReLU hidden layers, predicting from a
+// lineage's features log(1 + remaining events) of its simulation's
+// longest-lived lineage.  Parameters are one flat array:
 constexpr int kFeat = 8;
 constexpr int kHidden = 64;
 constexpr int kW1 = 0;                        // [64][8]  layer 1 weights (row = output)
@@ -30,14 +31,17 @@ constexpr int kOrderBuckets = 32;
 
 // One trace snapshot of a live lineage: its features and the step count at
 // the snapshot, keyed by (simulation, global reference).
+constexpr uint64_t kTraceRowsPerSim = 256;
+
 struct TraceRow {
     float f[kFeat];
     uint64_t gref;
     uint64_t steps;
     uint32_t sim;
-    uint32_t pad;
+    uint32_t snap;   // the snapshot's index in the run
+    double time;     // the lineage's time (its last event) at the snapshot
 };
-static_assert(sizeof(TraceRow) == 56, "TraceRow layout");
+static_assert(sizeof(TraceRow) == 64, "TraceRow layout");
 
 // Where a lineage left the simulation (speciation or duplicate removal) and
 // its step count there.
@@ -94,8 +98,14 @@ __host__ __device__ inline void lineage_features_of(int kind, const SimParams &p
             fx = (float)x / (float)p.width;
             fy = (float)y / (float)p.height;
             hab = (float)p.deme;
-            ent = logf((float)p.width * (float)p.height);
-            nu *= (float)p.migration;
+            // entropy of one dispersal: uniform over the local community with
+            // probability 1 - m, over the metacommunity with probability m;
+            // the speciation probability is the metacommunity's, where the
+            // lineage must migrate to speciate
+            const float m = fminf(fmaxf((float)p.migration, 0.f), 1.f);
+            const float h = (m > 0.f ? -m * logf(m) : 0.f) + (m < 1.f ? -(1.f - m) * logf(1.f - m) : 0.f);
+            ent = (1.f - m) * logf((float)p.width * (float)p.height) +
+                  m * logf((float)p.meta_width * (float)p.meta_height) + h;
         } else {
             fx = (float)(x - p.meta_ox) / (float)p.meta_width;
             fy = (float)(y - p.meta_oy) / (float)p.meta_height;
@@ -127,9 +137,10 @@ __host__ __device__ inline void lineage_features_of(int kind, const SimParams &p
     f[7] = log1pf((float)steps) * 0.05f;
 }
 
-// Appends a snapshot row for every live lineage of `f.in` (rows beyond `cap`
-// are counted but not written).
-cudaError_t launch_trace_snapshot(const FeatureArgs &f, TraceRow *rows, unsigned long long *n_rows,
+// Appends a snapshot row for about kTraceRowsPerSim live lineages of every
+// active simulation of `f.in`, chosen by a hash of (global reference,
+// snapshot) (rows beyond `cap` are counted but not written).
+cudaError_t launch_trace_snapshot(const FeatureArgs &f, uint32_t snap, TraceRow *rows, unsigned long long *n_rows,
                                   uint64_t cap, cudaStream_t st);
 // Fills pred_end (= steps + predicted remaining events) of every live lineage
 // whose prediction is unset (0) or used up.

@@ -270,9 +270,10 @@ def test_dispersal_events_batch_and_pause(nb, syn, oracle):
 
 
 def test_priority_split_is_bit_identical(nb, syn):
-    """Simulations run in engines of their own (priority_list) give the same
-    per-simulation results as the unsplit batch: every simulation's
-    canonical schedule depends on that simulation only."""
+    """Simulations in a priority engine of their own (priority_list), and
+    the others in priority groups, give the same per-simulation results as
+    the unsplit batch: every simulation's canonical schedule depends on that
+    simulation only."""
     sims = syn.config4(n_sims=6, max_local=3000)
     scen = [syn.to_scenario(d) for d, _ in sims]
     nus = [d["speciation_probability"] * 50 for d, _ in sims]
@@ -280,10 +281,13 @@ def test_priority_split_is_bit_identical(nb, syn):
     whole = nb.simulate_batch(scen, nus, seeds, collect=True)
     split = nb.simulate_batch(scen, nus, seeds, nb.CUDA(priority_list=[4, 1]), collect=True)
     with nb.Batch(scen, nus, seeds, nb.CUDA(priority_list=[0, 5, 2])) as b:
+        assert b.priority == [0, 5, 2]
         b.run()
         again = b.run(collect=True)
-    for x, y, z in zip(whole, split, again):
-        for o in (y, z):
+    grouped = nb.simulate_batch(scen, nus, seeds, nb.CUDA(priority_list=[3], priority_groups=2, resident=True),
+                                collect=True)
+    for x, y, z, w in zip(whole, split, again, grouped):
+        for o in (y, z, w):
             assert same_stream(x.speciation, o.speciation)
             assert (x.steps, x.n_rounds, x.n_dedup, x.biodiversity, x.time) == (
                 o.steps, o.n_rounds, o.n_dedup, o.biodiversity, o.time)

@@ -82,24 +82,23 @@ def _trace_workloads(syn):
 
 @pytest.mark.gpu
 def test_traces_train_a_model_that_beats_the_mean(nb, syn):
-    # a sweep over the speciation probability (as in the batched sweeps):
-    # within one simulation a lineage's remaining life is memoryless
-    # speciation plus coalescence decided by reference order, so most of the
-    # learnable signal is across simulations and over time
+    # a sweep over the speciation probability (as in the batched sweeps),
+    # each run to completion: a row's label is the remaining life of its
+    # simulation, set mostly by the speciation probability and the time
     ai, se = _trace_workloads(syn)
     nus = [1e-2, 1e-3, 1e-4] * 2
     X, y = nb.collect_traces([syn.to_scenario(se)] * len(nus), nus, list(range(1, len(nus) + 1)),
-                             snapshot_rounds=8, max_rows=60000)
-    assert X.shape[0] > 5000 and X.shape[1] == mo.N_FEATURES
+                             snapshot_rounds=2, max_rows=60000)
+    assert X.shape[0] > 1000 and X.shape[1] == mo.N_FEATURES
     assert np.all(np.isfinite(X)) and np.all(np.isfinite(y)) and np.all(y >= 0.0)
     rng = np.random.default_rng(0)
     idx = rng.permutation(X.shape[0])
     cut = int(0.8 * len(idx))
     tr, te = idx[:cut], idx[cut:]
     with nb.LifetimeModel(seed=7) as m:
-        m.train(X[tr], y[tr], epochs=10, batch=1024, lr=2e-3, seed=1)
+        m.train(X[tr], y[tr], epochs=60, batch=256, lr=2e-3, seed=1)
         mse = float(np.mean((m.predict(X[te]) - y[te]) ** 2))
-    # the gain over predicting every lineage's remaining events by the mean
+    # the gain over predicting every row's label by the mean
     var = float(np.var(y[te]))
     print(f"held-out MSE {mse:.4f} vs constant predictor {var:.4f} ({var / mse:.2f}x)")
     assert mse < 0.7 * var
@@ -135,3 +134,57 @@ def test_learned_schedule_requires_a_model(nb):
         nb._args_struct(nb.CUDA(schedule="learned"))
     with pytest.raises(ValueError):
         nb._args_struct(nb.CUDA(schedule="sorted"))
+
+
+@pytest.mark.gpu
+def test_priority_engine_model_against_unsorted_and_heuristics(nb, syn):
+    """A 64-simulation sweep (every 4th of the benchmark's 256) ends when its
+    longest-lived simulation does.  The learned schedule puts the model's 8
+    longest-lived simulations in a priority engine whose rounds wait for no
+    other simulation; the arms compared are no priority engine (unsorted) and
+    priority engines chosen by two closed-form estimates: nu / ln J (the
+    expected longest tail of ln J lineages that each speciate at rate nu) and
+    nu * J.  Outcomes are identical in every arm.  A priority engine costs
+    little when it misses the longest-lived simulation and shortens the sweep
+    when it holds it."""
+    import math
+
+    import bench
+    sims = syn.config4()[::4]
+    n = len(sims)
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] for d, _ in sims]
+    seeds = [s for _, s in sims]
+    J = [d["width"] * d["height"] for d, _ in sims]
+    k = 8
+    model, _ = bench.train_lifetime_model(nb, syn, 0, None)
+    try:
+        arms = {
+            "unsorted": nb.CUDA(resident=True),
+            "model": nb.CUDA(resident=True, schedule="learned", model=model, priority_sims=k),
+            "nu/lnJ": nb.CUDA(resident=True, priority_list=sorted(range(n), key=lambda j: nus[j] / math.log(J[j]))[:k]),
+            "nu*J": nb.CUDA(resident=True, priority_list=sorted(range(n), key=lambda j: nus[j] * J[j])[:k]),
+        }
+        res = {}
+        for name, algo in arms.items():
+            with nb.Batch(scen, nus, seeds, algo) as b:
+                b.run()
+                ms = b.run()[0].total_ms
+                res[name] = (ms, b.priority, b.run(collect=True))
+    finally:
+        model.close()
+    base = res["unsorted"][2]
+    for name, (_, _, outs) in res.items():
+        for a, b in zip(base, outs):
+            assert (a.steps, a.biodiversity, a.n_speciation, a.n_dedup, a.time, a.n_rounds) == \
+                   (b.steps, b.biodiversity, b.n_speciation, b.n_dedup, b.time, b.n_rounds), name
+            assert np.array_equal(np.sort(a.speciation), np.sort(b.speciation)), name
+    longest = max(range(n), key=lambda j: base[j].time)
+    t0 = res["unsorted"][0]
+    for name, (ms, prio, _) in res.items():
+        print("%-9s %8.1f ms (%.3f of unsorted)  priority engine %s  holds the longest-lived (#%d): %s" % (
+            name, ms, ms / t0, prio, longest, longest in prio))
+    for name, (ms, prio, _) in res.items():
+        assert ms <= 1.05 * t0, name  # a priority engine that misses costs little
+        if longest in prio:
+            assert ms < t0, name       # one that holds the longest-lived simulation gains
