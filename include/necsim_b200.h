@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define NECSIM_B200_ABI_VERSION 2
+#define NECSIM_B200_ABI_VERSION 3
 
 /* ---- error codes ---- */
 #define NECSIM_OK 0
@@ -158,6 +158,13 @@ typedef struct necsim_args {
                                   Results are identical either way */
     const uint32_t *priority_list; /* batch indices of the priority simulations (NULL: the model's
                                       choice); at most priority_sims are used */
+    uint32_t reserve_sms;      /* batches with a priority engine: once the priority engine's live
+                                  lineages fit this many SMs (its cooperative kernel's warps there),
+                                  its kernels run on these SMs alone and the other engines' kernels
+                                  leave them, so the priority tails' dependent event chains do not
+                                  share issue slots with bulk warps; at most half the SMs; 0 = off.
+                                  Results are identical either way */
+    uint32_t pad_args;
 } necsim_args;
 
 /* ---- events and lineages (reference layouts) ---- */

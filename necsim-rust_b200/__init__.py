@@ -79,6 +79,7 @@ class CArgs(ctypes.Structure):
         ("model", ctypes.c_void_p), ("max_rounds", ctypes.c_uint64),
         ("priority_sims", ctypes.c_uint32), ("priority_groups", ctypes.c_uint32),
         ("priority_list", ctypes.c_void_p),
+        ("reserve_sms", ctypes.c_uint32), ("pad_args", ctypes.c_uint32),
     ]
 
 
@@ -238,7 +239,7 @@ def lib():
                                          ctypes.c_uint32, u64, fp, fp, P(u64), ctypes.c_char_p,
                                          ctypes.c_size_t]
     L.necsim_gpu_trace_batch.restype = ctypes.c_int
-    if L.necsim_abi_version() != 2:
+    if L.necsim_abi_version() != 3:
         raise ImportError("libnecsim_b200.so ABI version mismatch")
     _lib = L
     return L
@@ -435,6 +436,9 @@ class CUDA:
     # batches: the other simulations in this many engines of decreasing CUDA
     # stream priority (the learned model's longest-lived first, else batch order)
     priority_groups: int = 0
+    # batches with a priority engine: this many SMs run the priority engine's
+    # tails alone once its live lineages fit them (0: off)
+    reserve_sms: int = 0
 
 
 Independent = CUDA
@@ -597,6 +601,7 @@ def _args_struct(algorithm: CUDA):
     a.max_rounds = algorithm.max_rounds
     a.priority_sims = algorithm.priority_sims
     a.priority_groups = algorithm.priority_groups
+    a.reserve_sms = algorithm.reserve_sms
     if algorithm.priority_list is not None:
         lst = (ctypes.c_uint32 * max(1, len(algorithm.priority_list)))(*algorithm.priority_list)
         a._priority_keep = lst

@@ -593,6 +593,10 @@ struct Control {  // small device scalars
     uint32_t status;
     unsigned int n_resident;  // active simulations owned by the resident kernel
     unsigned int busy;        // warps of the cooperative kernel holding a lineage
+    unsigned int blocks_done; // blocks of the round's step or cooperative kernel that finished or left
+    unsigned int res_claim;   // the resident launch's next simulation (SM gate only)
+    unsigned int res_done;    // the resident launch's blocks that finished or left (SM gate only)
+    unsigned int pad;
 };
 
 // Events delivered round by round (dispersal reporting): per simulation the
@@ -643,6 +647,14 @@ struct Engine {
     unsigned coop_grid = 0;   // cooperative kernel (Poisson sampler), kCoopBlock threads per block
     uint64_t coop_max = 0;    // rounds with at most this many live lineages run there
     unsigned aux_grid = 0, aux_block = 256;
+
+    // SM reservation between the engines of a batch (owned by the batch):
+    // kGateOnly for the priority engine, which turns it on once its live
+    // lineages fit the reserved SMs (gate_lineages); kGateAvoid for the others
+    SmGate *gate = nullptr;
+    uint32_t gate_role = kGateNone;
+    uint64_t gate_lineages = 0;
+    bool gate_on = false;
 
     // learned schedule (schedule == 1): model weights (owned by the model)
     // and the round's queue order
@@ -1077,6 +1089,9 @@ StepArgs make_step_args(Engine &E, DeviceLineages &in) {
     // are drained round by round)
     a.free_rounds = E.args.report_dispersal ? 0u : 64u;
     a.busy = &E.d_ctl->busy;
+    a.gate = E.gate;
+    a.gate_role = E.gate ? E.gate_role : kGateNone;
+    a.blocks_done = &E.d_ctl->blocks_done;
     if (E.tracing) {
         a.trace.deaths = E.trace_deaths;
         a.trace.n_deaths = E.trace_counts + 1;
@@ -1145,6 +1160,10 @@ ResidentArgs make_resident_args(Engine &E, uint32_t budget, const int *stop_flag
     a.n_resident = &E.d_ctl->n_resident;
     a.stop_flag = stop_flag;
     a.exp_sampler = E.args.event_time_sampler == NECSIM_SAMPLER_EXP ? 1u : 0u;
+    a.gate = E.gate;
+    a.gate_role = E.gate ? E.gate_role : kGateNone;
+    a.claim = &E.d_ctl->res_claim;
+    a.blocks_done = &E.d_ctl->res_done;
     return a;
 }
 
@@ -1163,6 +1182,7 @@ ScheduleArgs make_schedule_args(Engine &E) {
     a.n_active = &E.d_ctl->n_active;
     a.visits = &E.d_ctl->visits;
     a.n_resident = &E.d_ctl->n_resident;
+    a.blocks_done = &E.d_ctl->blocks_done;
     return a;
 }
 
@@ -1261,6 +1281,11 @@ RunResult run_rounds(Engine &E) {
     rr.launches += 1;
     if (E.tracing) CK(launch_trace_snapshot(make_feature_args(E, E.A), E.trace_snap++, E.trace_rows,
                                             E.trace_counts, E.trace_rows_cap, E.stream));
+    const bool gate_owner = E.gate && E.gate_role == kGateOnly;
+    if (gate_owner) {
+        CK(cudaMemsetAsync(&E.gate->on, 0, sizeof(uint32_t), E.stream));
+        E.gate_on = false;
+    }
     CK(cudaMemcpyAsync(E.h_ctl, E.d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
     uint64_t graph_launches = 0;
@@ -1309,9 +1334,16 @@ RunResult run_rounds(Engine &E) {
                 CK(cudaEventRecord(E.ev_fork, E.stream));
                 CK(cudaStreamWaitEvent(E.stream_t, E.ev_fork, 0));
                 const uint32_t budget = global ? 32 : 256;
+                unsigned grid = global ? grid_beside : grid_alone;
+                if (E.gate) {
+                    // claims and arrivals of the launch start at zero; the
+                    // priority engine's blocks, confined to the reserved SMs,
+                    // come in a grid large enough to reach all of them
+                    CK(cudaMemsetAsync(&E.d_ctl->res_claim, 0, 2 * sizeof(unsigned int), E.stream_t));
+                    if (gate_owner && E.gate_on) grid = (unsigned)E.n_sms * 2;
+                }
                 CK(cudaEventRecord(E.ev_res0, E.stream_t));
-                CK(launch_resident(E.kind, make_resident_args(E, budget, nullptr), global ? grid_beside : grid_alone,
-                                   E.stream_t));
+                CK(launch_resident(E.kind, make_resident_args(E, budget, nullptr), grid, E.stream_t));
                 CK(cudaEventRecord(E.ev_res1, E.stream_t));
                 res_inflight = true;
                 rr.launches += 2;
@@ -1350,8 +1382,19 @@ RunResult run_rounds(Engine &E) {
             }
         }
         if (E.h_ctl->status & ~kErrDedupFull) break;
+        if (gate_owner && !E.gate_on && E.h_ctl->n_cur <= E.gate_lineages) {
+            // the priority engine's bulk is over: its tails take the reserved
+            // SMs, the other engines leave them
+            CK(cudaMemsetAsync(&E.gate->on, 1, sizeof(uint32_t), E.stream));
+            E.gate_on = true;
+        }
     }
     if (res_inflight) CK(cudaEventSynchronize(E.ev_res1));
+    if (gate_owner) {
+        // the other engines get every SM back
+        CK(cudaMemsetAsync(&E.gate->on, 0, sizeof(uint32_t), E.stream));
+        E.gate_on = false;
+    }
     // the resident stream's work is part of the run
     if (E.args.resident) {
         CK(cudaEventRecord(E.ev_fork, E.stream_t));
@@ -1822,7 +1865,44 @@ struct BatchRun {
     std::vector<Remaining> rem;
     size_t n_groups = 1;
     std::vector<uint32_t> priority;  // the priority simulations, in priority order
+    // the SM reservation shared by the engines (args.reserve_sms > 0 and a
+    // priority engine), freed after the engines are released
+    struct GateMem {
+        SmGate *p = nullptr;
+        ~GateMem() {
+            if (p) cudaFree(p);
+        }
+    };
+    GateMem gate;
 };
+
+// Sets aside `count` of the device's SMs for the priority engine: the SM ids
+// present (a census kernel), every (present / count)-th of them, so the
+// reserved SMs spread over the dies.  Returns the number reserved.
+uint32_t reserve_sms(SmGate *gate, int device, int n_sms, uint32_t count) {
+    CK(cudaSetDevice(device));
+    SmGate g;
+    std::memset(&g, 0, sizeof(g));
+    CK(cudaMemset(gate, 0, sizeof(SmGate)));
+    CK(launch_sm_census(gate->mask, (unsigned)n_sms * 16u, 0));
+    CK(cudaMemcpy(g.mask, gate->mask, sizeof(g.mask), cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> present;
+    for (uint32_t id = 0; id < 256; ++id)
+        if ((g.mask[id >> 5] >> (id & 31)) & 1u) present.push_back(id);
+    std::memset(g.mask, 0, sizeof(g.mask));
+    uint32_t n = 0;
+    if (!present.empty() && count < present.size()) {
+        const double stride = (double)present.size() / (double)count;
+        for (uint32_t k = 0; k < count; ++k) {
+            const uint32_t id = present[(size_t)((double)k * stride)];
+            g.mask[id >> 5] |= 1u << (id & 31);
+            ++n;
+        }
+    }
+    g.on = 0;
+    CK(cudaMemcpy(gate, &g, sizeof(g), cudaMemcpyHostToDevice));
+    return n;
+}
 
 // The batch's simulations in priority order: with the learned schedule the
 // lifetime model's longest-lived first, else batch order; then the priority
@@ -1881,7 +1961,16 @@ void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &ar
     b.members.clear();
     b.n_groups = groups;
     const bool staggered = groups > 1;
-    auto add = [&](std::vector<uint32_t> ids, int level) {
+    // SMs set aside for the priority engine's tails
+    uint32_t reserved = 0;
+    if (args.reserve_sms && !prio.empty() && !rest_ids.empty()) {
+        cudaDeviceProp prop;
+        CK(cudaGetDeviceProperties(&prop, args.device));
+        if (!b.gate.p) b.gate.p = dev_alloc<SmGate>(1);
+        reserved = reserve_sms(b.gate.p, args.device, prop.multiProcessorCount,
+                               std::min<uint32_t>(args.reserve_sms, (uint32_t)prop.multiProcessorCount / 2));
+    }
+    auto add = [&](std::vector<uint32_t> ids, int level, uint32_t role) {
         std::vector<SimHost> part;
         // an engine's simulations in batch order
         std::sort(ids.begin(), ids.end());
@@ -1889,7 +1978,18 @@ void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &ar
         b.engines.emplace_back(new Engine());
         Engine &E = *b.engines.back();
         setup_engine(E, args, level);
+        if (reserved) {
+            E.gate = b.gate.p;
+            E.gate_role = role;
+        }
         prepare_engine(E, std::move(part), args, nullptr, nullptr);
+        // the reservation starts when the priority engine's live lineages
+        // fit its cooperative kernel's warps on the reserved SMs
+        if (reserved && role == kGateOnly) {
+            int coop_per_sm = 0;
+            CK(coop_kernel_occupancy(E.kind, &coop_per_sm));
+            E.gate_lineages = (uint64_t)reserved * (uint64_t)std::max(coop_per_sm, 1) * (kCoopBlock / 32);
+        }
         b.members.push_back(std::move(ids));
     };
     size_t at = 0;
@@ -1897,11 +1997,11 @@ void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &ar
         const size_t len = rest_ids.size() / groups + (g < rest_ids.size() % groups ? 1 : 0);
         std::vector<uint32_t> ids(rest_ids.begin() + at, rest_ids.begin() + at + len);
         at += len;
-        add(std::move(ids), staggered ? stream_priority_level(args.device, g) : 0);
+        add(std::move(ids), staggered ? stream_priority_level(args.device, g) : 0, kGateAvoid);
     }
     // the priority simulations share one engine: their rounds wait for none
     // of the others' (and the others' for none of theirs)
-    if (!prio.empty()) add(prio, staggered ? stream_priority_level(args.device, 0) : 0);
+    if (!prio.empty()) add(prio, staggered ? stream_priority_level(args.device, 0) : 0, kGateOnly);
     b.priority = prio;
     b.rem.assign(b.engines.size(), Remaining{});
 }

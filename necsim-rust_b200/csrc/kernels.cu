@@ -967,6 +967,37 @@ __device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long l
     return true;
 }
 
+// The SM reservation (SmGate): true when the calling block's SM is one its
+// engine must leave while the reservation is on.
+__device__ __forceinline__ bool gate_leaves(const SmGate *g, uint32_t role) {
+    if (*(volatile const uint32_t *)&g->on == 0u) return false;
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    const bool reserved = smid < 256u && ((g->mask[smid >> 5] >> (smid & 31u)) & 1u) != 0u;
+    return role == kGateAvoid ? reserved : !reserved;
+}
+
+// Block-uniform.  Every block of a gated launch arrives once at `done`: a
+// block that leaves arrives at once, one that works arrives when its first
+// warp has found the queue empty.  A leaving block that arrives last stays
+// and takes whatever is left, so the launch's work is done wherever its
+// blocks landed (when any working block arrives, every item is claimed).
+__device__ __forceinline__ bool block_leaves(const SmGate *g, uint32_t role, unsigned int *done) {
+    if (g == nullptr || role == kGateNone) return false;
+    __shared__ int s_leave;
+    if (threadIdx.x == 0) {
+        int leave = gate_leaves(g, role) ? 1 : 0;
+        if (leave) leave = (atomicAdd(done, 1u) + 1u < gridDim.x) ? 1 : 0;
+        s_leave = leave;
+    }
+    __syncthreads();
+    return s_leave != 0;
+}
+
+__device__ __forceinline__ void block_arrives(const SmGate *g, uint32_t role, unsigned int *done) {
+    if (g != nullptr && role != kGateNone && threadIdx.x == 0) atomicAdd(done, 1u);
+}
+
 // At most one lineage per warp: each warp takes lineages from the queue and
 // steps each one with all its lanes (a lineage's events at warp latency,
 // lineages on all SMs).  Every lineage gets a warp at once, so the queue
@@ -1069,11 +1100,13 @@ __device__ __forceinline__ void step_body(const StepArgs &a) {
     const uint64_t n = *a.n_cur;
     // the Poisson sampler's cooperative rounds run in coop_kernel
     if (!EXP && n <= a.coop_max) return;
+    if (block_leaves(a.gate, a.gate_role, a.blocks_done)) return;
     const SimParams *P = stage_params<SINGLE>(a, params_smem);
     const EventSink sink = sink_of(a);
     const unsigned lane_id = threadIdx.x & 31u;
     if (EXP && n <= (uint64_t)gridDim.x * (blockDim.x / 32u)) {
         coop_body<KIND, SINGLE, true>(a, P, n);
+        block_arrives(a.gate, a.gate_role, a.blocks_done);
         return;
     }
     const bool lat = n * 4 <= (uint64_t)gridDim.x * blockDim.x;
@@ -1104,7 +1137,10 @@ __device__ __forceinline__ void step_body(const StepArgs &a) {
                 }
             }
         }
-        if (!__any_sync(kFull, have)) break;
+        // a warp leaves only when the queue is empty for all its lanes (a
+        // lineage of an inactive simulation, or one with nothing to do before
+        // the horizon, leaves its lane free to take the next)
+        if (!__any_sync(kFull, have || !exhausted)) break;
         if (!have) continue;
         const SimParams &p = P[SINGLE ? 0 : l.s];
 
@@ -1132,6 +1168,7 @@ __device__ __forceinline__ void step_body(const StepArgs &a) {
         for (int off = 16; off > 0; off >>= 1) w += __shfl_down_sync(kFull, w, off);
         if (lane_id == 0 && w) atomicAdd(a.steps_total, w);
     }
+    block_arrives(a.gate, a.gate_role, a.blocks_done);
 }
 
 // The step kernel with the Poisson sampler, and with the exponential one:
@@ -1156,8 +1193,10 @@ __global__ void __launch_bounds__(kCoopBlock) coop_kernel(StepArgs a) {
     __shared__ __align__(16) unsigned char params_smem[SINGLE ? sizeof(SimParams) : 16];
     const uint64_t n = *a.n_cur;
     if (n > a.coop_max) return;
+    if (block_leaves(a.gate, a.gate_role, a.blocks_done)) return;
     const SimParams *P = stage_params<SINGLE>(a, params_smem);
     coop_body<KIND, SINGLE, false>(a, P, n);
+    block_arrives(a.gate, a.gate_role, a.blocks_done);
 }
 
 // A simulation with at most kResidentMax live lineages is advanced by one
@@ -1205,7 +1244,19 @@ __global__ void __launch_bounds__(THREADS, 1) resident_kernel(ResidentArgs a) {
     sink.trace.n_deaths = nullptr;
     sink.trace.cap = 0;
 
-    for (uint32_t s = blockIdx.x; s < a.n_sims; s += gridDim.x) {
+    // with an SM gate the blocks claim simulations one at a time (a block
+    // may leave its SM), else block b takes simulations b, b + grid, ...
+    const bool claiming = a.gate != nullptr && a.gate_role != kGateNone;
+    if (block_leaves(a.gate, a.gate_role, a.blocks_done)) return;
+    __shared__ uint32_t s_claim;
+    auto next_sim = [&](uint32_t prev) -> uint32_t {
+        if (!claiming) return prev + gridDim.x;
+        __syncthreads();  // every thread has read the previous claim
+        if (t == 0) s_claim = atomicAdd(a.claim, 1u);
+        __syncthreads();
+        return s_claim;
+    };
+    for (uint32_t s = claiming ? next_sim(0) : blockIdx.x; s < a.n_sims; s = next_sim(s)) {
         SimParams &pm = a.params[s];
         if (t == 0) {
             // resident == 2: owned by this kernel (1: routed, handed over at
@@ -1407,6 +1458,7 @@ __global__ void __launch_bounds__(THREADS, 1) resident_kernel(ResidentArgs a) {
         }
         __syncthreads();
     }
+    block_arrives(a.gate, a.gate_role, a.blocks_done);
 }
 
 namespace {
@@ -1575,6 +1627,7 @@ __global__ void schedule_kernel(ScheduleArgs a) {
         *a.n_cur = n;
         *a.out_count = 0;
         *a.work = 0;
+        if (a.blocks_done) *a.blocks_done = 0;
         unsigned long long want = (n * (unsigned long long)a.dedup_pct + 99ULL) / 100ULL;
         if (want < 2) want = 2;
         unsigned long long size = 1;
@@ -1664,6 +1717,18 @@ cudaError_t launch_dedup(const DedupArgs &a, unsigned grid, unsigned block, cuda
 
 cudaError_t launch_schedule(const ScheduleArgs &a, cudaStream_t st) {
     schedule_kernel<<<1, 256, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+__global__ void sm_census_kernel(uint32_t *mask) {
+    if (threadIdx.x != 0) return;
+    uint32_t smid;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+    if (smid < 256u) atomicOr(&mask[smid >> 5], 1u << (smid & 31u));
+}
+
+cudaError_t launch_sm_census(uint32_t *mask, unsigned grid, cudaStream_t st) {
+    sm_census_kernel<<<grid, 32, 0, st>>>(mask);
     return cudaGetLastError();
 }
 

@@ -16,6 +16,19 @@ constexpr int kCoopBlock = 128;
 // simulations with at most this many live lineages run in the resident kernel
 constexpr int kResidentMax = 256;
 
+// SMs set aside for the priority engine's tails.  While `on` is nonzero the
+// persistent kernels of an engine with role kGateAvoid leave the SMs whose
+// id (%smid) has its bit set in `mask`, and those of an engine with role
+// kGateOnly run only there, so a tail's dependent event chain does not share
+// its issue slots with bulk warps.  Which blocks do the work never changes
+// what is computed: the work is claimed dynamically, and the last block of a
+// launch to leave takes whatever is still unclaimed.
+struct SmGate {
+    uint32_t on;
+    uint32_t mask[8];  // SM ids 0..255
+};
+constexpr uint32_t kGateNone = 0, kGateAvoid = 1, kGateOnly = 2;
+
 struct StepArgs {
     LineageSoA in;                       // lineages of this round (updated in place)
     uint8_t *state;                      // per slot: 0 alive, 1 speciated, 2 dropped
@@ -46,6 +59,10 @@ struct StepArgs {
     // warps holding a lineage (zero between launches)
     uint32_t free_rounds;
     unsigned int *busy;
+    const SmGate *gate;                  // SM reservation (nullable) and this engine's role in it
+    uint32_t gate_role;
+    unsigned int *blocks_done;           // blocks of the round's kernel that have finished or left
+                                         // (reset by the scheduler)
 };
 
 struct DedupArgs {
@@ -80,6 +97,7 @@ struct ScheduleArgs {
     unsigned int *n_active;
     unsigned long long *visits;          // lineages the scheduled rounds process
     unsigned int *n_resident;            // active simulations owned by the resident kernel
+    unsigned int *blocks_done;           // the next round's kernel arrivals (reset here)
 };
 
 // the step kernel on grid x block and, for the Poisson sampler with
@@ -108,7 +126,15 @@ struct ResidentArgs {
     unsigned int *n_resident;
     const int *stop_flag;                // set when the concurrent global rounds end (nullable)
     uint32_t exp_sampler;                // 1: exponential event-time sampler (exp.rs), else Poisson
+    const SmGate *gate;                  // SM reservation (nullable) and this engine's role in it
+    uint32_t gate_role;
+    unsigned int *claim;                 // with a gate: next simulation to claim, and the blocks
+    unsigned int *blocks_done;           // that have finished or left (both zero at launch)
 };
+
+// The SM ids present on the device: bit smid of mask[smid / 32] is set by a
+// block that ran there (grid blocks of 32 threads; mask zeroed before).
+cudaError_t launch_sm_census(uint32_t *mask, unsigned grid, cudaStream_t st);
 
 cudaError_t launch_resident(int kind, const ResidentArgs &a, unsigned grid, cudaStream_t st);
 cudaError_t launch_promote(SimParams *params, uint32_t n_sims, cudaStream_t st);

@@ -30,8 +30,11 @@ def test_tables_argument_mirrors_header(nb):
     """The ctypes mirror carries the new trailing fields in the header's order."""
     names = [f for f, _ in nb.CScenario._fields_]
     assert names[-3:] == ["cells", "atoms", "n_atoms"]
-    assert [f for f, _ in nb.CArgs._fields_][-4:] == ["max_rounds", "priority_sims", "priority_groups", "priority_list"]
-    assert nb.lib().necsim_abi_version() == 2
+    assert [f for f, _ in nb.CArgs._fields_][-6:] == ["max_rounds", "priority_sims", "priority_groups",
+                                                      "priority_list", "reserve_sms", "pad_args"]
+    assert nb.lib().necsim_abi_version() == 3
+    assert nb._args_struct(nb.CUDA(reserve_sms=8)).reserve_sms == 8
+    assert nb._args_struct(nb.CUDA()).reserve_sms == 0
 
 
 def test_scenario_needs_a_dispersal_map_or_tables(nb, syn):

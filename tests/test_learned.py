@@ -164,6 +164,8 @@ def test_priority_engine_model_against_unsorted_and_heuristics(nb, syn):
             "model": nb.CUDA(resident=True, schedule="learned", model=model, priority_sims=k),
             "nu*J": nb.CUDA(resident=True, priority_list=sorted(range(n), key=lambda j: nus[j] * J[j])[:k]),
             "nu/lnJ": nb.CUDA(resident=True, priority_list=sorted(range(n), key=lambda j: nus[j] / math.log(J[j]))[:k]),
+            # the model's priority engine with its tails on 8 SMs of their own
+            "model+sms": nb.CUDA(resident=True, schedule="learned", model=model, priority_sims=k, reserve_sms=8),
         }
         res = {}
         for name, algo in arms.items():
@@ -193,3 +195,29 @@ def test_priority_engine_model_against_unsorted_and_heuristics(nb, syn):
     if longest not in res["nu*J"][1]:
         assert res["model"][0] < res["nu*J"][0]
 
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("reserve", [4, 16])
+def test_reserved_sms_change_no_result(nb, syn, reserve):
+    """A priority engine whose tails run on SMs of their own (the other
+    engine's kernels leave those SMs, its own leave the rest, and the last
+    block of a launch to leave takes the unclaimed work) gives the outcomes
+    and speciation events of the run without the reservation, for both
+    event-time samplers."""
+    sims = syn.config4()[::16]
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] * 10 for d, _ in sims]
+    seeds = [s for _, s in sims]
+    longest = sorted(range(len(sims)), key=lambda j: nus[j])[:3]
+    for sampler in ("poisson", "exp"):
+        outs = {}
+        for r in (0, reserve):
+            algo = nb.CUDA(resident=True, priority_list=longest, reserve_sms=r, event_time_sampler=sampler)
+            with nb.Batch(scen, nus, seeds, algo) as b:
+                assert sorted(b.priority) == sorted(longest)
+                outs[r] = b.run(collect=True)
+        for a, b in zip(outs[0], outs[reserve]):
+            assert (a.steps, a.biodiversity, a.n_speciation, a.n_dedup, a.time, a.n_rounds) == \
+                   (b.steps, b.biodiversity, b.n_speciation, b.n_dedup, b.time, b.n_rounds), sampler
+            assert np.array_equal(np.sort(a.speciation), np.sort(b.speciation)), sampler
