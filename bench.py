@@ -616,6 +616,20 @@ def main():
         line["learned_over_plain"] = value / p_value
         line["priority_sims"] = head["priority"]
         line["outcomes_identical"] = bool(same)
+    # when each simulation ended on the device clock (from the batch's first
+    # round): the priority engine's simulations against the others'
+    prio = set(head["priority"])
+    ends = [(o.end_ms, j) for j, o in enumerate(outs)]
+    longest = max(ends)[1]
+    line["timeline"] = {
+        "batch_ms": outs[0].total_ms,
+        "priority_last_end_ms": max((e for e, j in ends if j in prio), default=None),
+        "others_last_end_ms": max((e for e, j in ends if j not in prio), default=None),
+        "last_simulation": {"sim": longest, "end_ms": outs[longest].end_ms,
+                            "routed_ms": outs[longest].routed_ms, "in_priority_engine": longest in prio},
+        "priority_simulations": [{"sim": j, "routed_ms": outs[j].routed_ms, "end_ms": outs[j].end_ms}
+                                 for j in head["priority"]],
+    }
     if model_info is not None:
         line["model"] = model_info
     if tune_info is not None:

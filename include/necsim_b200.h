@@ -162,9 +162,13 @@ typedef struct necsim_args {
                                   lineages fit this many SMs (its cooperative kernel's warps there),
                                   its kernels run on these SMs alone and the other engines' kernels
                                   leave them, so the priority tails' dependent event chains do not
-                                  share issue slots with bulk warps; at most half the SMs; 0 = off.
-                                  Results are identical either way */
-    uint32_t pad_args;
+                                  share issue slots with bulk warps; at most half the SMs; 0 = off;
+                                  only with one priority engine.  Results are identical either way */
+    uint32_t priority_engines; /* batches: the priority simulations split into this many engines,
+                                  contiguous runs of the priority order, so that a long tail waits in
+                                  lockstep rounds for fewer other priority simulations' bulk; 0 = one
+                                  engine.  An engine of one simulation runs it without the resident
+                                  kernel.  Results are identical either way */
 } necsim_args;
 
 /* ---- events and lineages (reference layouts) ---- */
@@ -228,6 +232,10 @@ typedef struct necsim_outcome {
     uint64_t lineage_visits;   /* lineage slots the step kernels processed */
     double resident_ms;        /* device time of the per-simulation resident kernel (CUDA
                                   events; overlaps the global rounds) */
+    double end_ms;             /* when this simulation ended (or paused), in ms of the device
+                                  clock after the run (batch: the batch) began its rounds */
+    double routed_ms;          /* batches: when the resident kernel took the simulation over
+                                  (same clock), -1 if it stayed in the global rounds */
 } necsim_outcome;
 
 typedef struct necsim_ctx necsim_ctx;

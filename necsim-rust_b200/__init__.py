@@ -79,7 +79,7 @@ class CArgs(ctypes.Structure):
         ("model", ctypes.c_void_p), ("max_rounds", ctypes.c_uint64),
         ("priority_sims", ctypes.c_uint32), ("priority_groups", ctypes.c_uint32),
         ("priority_list", ctypes.c_void_p),
-        ("reserve_sms", ctypes.c_uint32), ("pad_args", ctypes.c_uint32),
+        ("reserve_sms", ctypes.c_uint32), ("priority_engines", ctypes.c_uint32),
     ]
 
 
@@ -94,6 +94,7 @@ class COutcome(ctypes.Structure):
         ("total_ms", ctypes.c_double), ("h2d_bytes", ctypes.c_uint64),
         ("d2h_bytes", ctypes.c_uint64), ("n_step_launches", ctypes.c_uint64),
         ("lineage_visits", ctypes.c_uint64), ("resident_ms", ctypes.c_double),
+        ("end_ms", ctypes.c_double), ("routed_ms", ctypes.c_double),
     ]
 
 
@@ -439,6 +440,9 @@ class CUDA:
     # batches with a priority engine: this many SMs run the priority engine's
     # tails alone once its live lineages fit them (0: off)
     reserve_sms: int = 0
+    # batches: the priority simulations split into this many engines (0: one
+    # engine), so a long tail waits for fewer other ones' bulk
+    priority_engines: int = 0
 
 
 Independent = CUDA
@@ -470,6 +474,11 @@ class Outcome:
     n_dispersal: int = 0
     dispersal: Optional[np.ndarray] = None   # with CUDA(report_dispersal=True), collect=True
     delivery: Optional[list] = None          # reporter calls in order: ("s" | "d", count)
+    # device-clock ms after the run's (a batch's) first round began: when the
+    # simulation ended or paused, and when the resident kernel took it over
+    # (-1: never)
+    end_ms: float = 0.0
+    routed_ms: float = -1.0
 
 
 def presample_origins(n: int, percentage: float = 1.0, rank: int = 0, size: int = 1) -> np.ndarray:
@@ -602,6 +611,7 @@ def _args_struct(algorithm: CUDA):
     a.priority_sims = algorithm.priority_sims
     a.priority_groups = algorithm.priority_groups
     a.reserve_sms = algorithm.reserve_sms
+    a.priority_engines = algorithm.priority_engines
     if algorithm.priority_list is not None:
         lst = (ctypes.c_uint32 * max(1, len(algorithm.priority_list)))(*algorithm.priority_list)
         a._priority_keep = lst
@@ -653,6 +663,7 @@ def _outcome(o: COutcome, spec=None, remaining=None, col=None) -> Outcome:
                   o.h2d_bytes, o.d2h_bytes, o.n_step_launches, o.lineage_visits, o.resident_ms,
                   spec, remaining)
     out.n_dispersal = o.n_dispersal
+    out.end_ms, out.routed_ms = o.end_ms, o.routed_ms
     if col is not None and col.disp_chunks:
         out.dispersal = col.dispersal_events()
         out.delivery = list(col.kinds)

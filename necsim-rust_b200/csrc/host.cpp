@@ -676,6 +676,7 @@ struct Engine {
     unsigned long long *trace_counts = nullptr;  // [0] rows, [1] deaths
     uint64_t trace_rows_cap = 0, trace_deaths_cap = 0;
     uint32_t trace_snap = 0;  // index of the next snapshot
+    uint64_t first_start_ns = 0;  // device clock of the last run's first schedule (outcomes' end_ms base)
 
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<cudaEvent_t> ev_start, ev_end;
@@ -1630,10 +1631,18 @@ void finish(Engine &E, const RunResult &rr, const necsim_reporter *reporters, bo
     E.d2h_bytes += ns * sizeof(SimCounters) + sizeof(Control) + n * (4 * 4 + 8 * 3) +
                    n_spec * sizeof(DevSpeciationEvent);
 
+    // the simulations' timeline on the device clock, from the run's first schedule
+    uint64_t base = 0;
+    for (size_t s = 0; s < ns; ++s)
+        if (cs[s].start_ns && (base == 0 || cs[s].start_ns < base)) base = cs[s].start_ns;
+    E.first_start_ns = base;
+    auto since = [base](unsigned long long t) { return t > base ? (double)(t - base) / 1e6 : 0.0; };
     size_t pos = 0;
     for (size_t s = 0; s < ns; ++s) {
         necsim_outcome &o = outcomes[s];
         std::memset(&o, 0, sizeof(o));
+        o.end_ms = since(cs[s].end_ns);
+        o.routed_ms = cs[s].routed_ns ? since(cs[s].routed_ns) : -1.0;
         double t;
         uint64_t tb = cs[s].max_time_bits;
         std::memcpy(&t, &tb, 8);
@@ -1858,8 +1867,8 @@ void prepare_engine(Engine &E, std::vector<SimHost> sims, const necsim_args &arg
 // so the split changes no result.
 struct BatchRun {
     // engines[0 .. n_groups): the priority groups of the simulations outside
-    // the priority engine, in decreasing stream priority (engines[0] may be
-    // empty); then the priority engine, when there are priority simulations
+    // the priority engines, in decreasing stream priority (engines[0] may be
+    // empty); then the priority engines, when there are priority simulations
     std::vector<std::unique_ptr<Engine>> engines;
     std::vector<std::vector<uint32_t>> members;  // batch indices of each engine's simulations
     std::vector<Remaining> rem;
@@ -1961,9 +1970,13 @@ void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &ar
     b.members.clear();
     b.n_groups = groups;
     const bool staggered = groups > 1;
-    // SMs set aside for the priority engine's tails
+    // the priority simulations' engines: contiguous runs of the priority
+    // order, one engine by default
+    const size_t n_prio_engines =
+        prio.empty() ? 0 : (args.priority_engines ? std::min<size_t>(args.priority_engines, prio.size()) : 1);
+    // SMs set aside for the priority engine's tails (one priority engine)
     uint32_t reserved = 0;
-    if (args.reserve_sms && !prio.empty() && !rest_ids.empty()) {
+    if (args.reserve_sms && n_prio_engines == 1 && !rest_ids.empty()) {
         cudaDeviceProp prop;
         CK(cudaGetDeviceProperties(&prop, args.device));
         if (!b.gate.p) b.gate.p = dev_alloc<SmGate>(1);
@@ -1999,9 +2012,14 @@ void prepare_batch(BatchRun &b, std::vector<SimHost> sims, const necsim_args &ar
         at += len;
         add(std::move(ids), staggered ? stream_priority_level(args.device, g) : 0, kGateAvoid);
     }
-    // the priority simulations share one engine: their rounds wait for none
-    // of the others' (and the others' for none of theirs)
-    if (!prio.empty()) add(prio, staggered ? stream_priority_level(args.device, 0) : 0, kGateOnly);
+    // the priority engines: their rounds wait for none of the others' (and
+    // the others' for none of theirs)
+    for (size_t g = 0, pat = 0; g < n_prio_engines; ++g) {
+        const size_t len = prio.size() / n_prio_engines + (g < prio.size() % n_prio_engines ? 1 : 0);
+        std::vector<uint32_t> ids(prio.begin() + pat, prio.begin() + pat + len);
+        pat += len;
+        add(std::move(ids), staggered ? stream_priority_level(args.device, 0) : 0, kGateOnly);
+    }
     b.priority = prio;
     b.rem.assign(b.engines.size(), Remaining{});
 }
@@ -2055,6 +2073,12 @@ void run_batch(BatchRun &b, const necsim_reporter *reporters, necsim_outcome *ou
         if (err) std::rethrow_exception(err);
     double span = 0.0, kernel = 0.0, resident = 0.0;
     uint64_t launches = 0, steps_l = 0, visits = 0, h2d = 0, d2h = 0;
+    // the engines' timelines share the earliest engine's start
+    uint64_t base = 0;
+    for (size_t e = 0; e < ne; ++e) {
+        const uint64_t t = b.engines[e]->first_start_ns;
+        if (!b.members[e].empty() && t && (base == 0 || t < base)) base = t;
+    }
     for (size_t e = 0; e < ne; ++e) {
         if (b.members[e].empty()) continue;
         float ms = 0.f;
@@ -2069,9 +2093,13 @@ void run_batch(BatchRun &b, const necsim_reporter *reporters, necsim_outcome *ou
         h2d += o.h2d_bytes;
         d2h += o.d2h_bytes;
     }
-    for (size_t e = 0; e < ne; ++e)
+    for (size_t e = 0; e < ne; ++e) {
+        const uint64_t t = b.engines[e]->first_start_ns;
+        const double shift = (t > base) ? (double)(t - base) / 1e6 : 0.0;
         for (size_t k = 0; k < b.members[e].size(); ++k) {
             necsim_outcome o = outs[e][k];
+            o.end_ms += shift;
+            if (o.routed_ms >= 0.0) o.routed_ms += shift;
             o.total_ms = span;
             o.kernel_ms = kernel;
             o.resident_ms = resident;
@@ -2082,6 +2110,7 @@ void run_batch(BatchRun &b, const necsim_reporter *reporters, necsim_outcome *ou
             o.d2h_bytes = d2h;
             outcomes[b.members[e][k]] = o;
         }
+    }
 }
 
 }  // namespace

@@ -967,6 +967,12 @@ __device__ __forceinline__ bool next_horizon(const SimParams &p, unsigned long l
     return true;
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 // The SM reservation (SmGate): true when the calling block's SM is one its
 // engine must leave while the reservation is on.
 __device__ __forceinline__ bool gate_leaves(const SmGate *g, uint32_t role) {
@@ -1436,6 +1442,7 @@ __global__ void __launch_bounds__(THREADS, 1) resident_kernel(ResidentArgs a) {
                     if (a.stop_flag && *(volatile const int *)a.stop_flag) s_go = 2;
                 } else {
                     pm.active = 0;
+                    c.end_ns = global_ns();
                     atomicSub(a.n_resident, 1u);
                     s_go = 0;
                 }
@@ -1605,6 +1612,10 @@ __global__ void schedule_kernel(ScheduleArgs a) {
         c.n_live_next = 0;
         double h;
         const bool more = next_horizon(p, live, h);
+        const unsigned long long now = global_ns();
+        if (c.start_ns == 0) c.start_ns = now;
+        // the end: the round in which it stops (or, never started, now)
+        if (!more && (p.active || c.end_ns == 0)) c.end_ns = now;
         if (more) {
             p.horizon = h;
             c.n_rounds += 1;
@@ -1612,6 +1623,7 @@ __global__ void schedule_kernel(ScheduleArgs a) {
         p.active = more ? 1 : 0;
         if (c.routed) {
             // its survivors are in the resident arena
+            if (c.routed_ns == 0) c.routed_ns = now;
             p.resident = 1;
             if (more) atomicAdd(a.n_resident, 1u);
         } else if (more) {

@@ -153,6 +153,9 @@ struct SimCounters {
     unsigned long long n_live_next;    // survivors of the current round
     unsigned long long n_dispersal;
     unsigned long long routed;         // survivors were moved to the resident arena
+    // device clock (%globaltimer, ns): the simulation's first schedule, its
+    // hand-over to the resident kernel (0: never) and its end or pause
+    unsigned long long start_ns, routed_ns, end_ns;
 };
 
 // Lineage state, structure of arrays.

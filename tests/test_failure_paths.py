@@ -31,10 +31,11 @@ def test_tables_argument_mirrors_header(nb):
     names = [f for f, _ in nb.CScenario._fields_]
     assert names[-3:] == ["cells", "atoms", "n_atoms"]
     assert [f for f, _ in nb.CArgs._fields_][-6:] == ["max_rounds", "priority_sims", "priority_groups",
-                                                      "priority_list", "reserve_sms", "pad_args"]
+                                                      "priority_list", "reserve_sms", "priority_engines"]
     assert nb.lib().necsim_abi_version() == 3
     assert nb._args_struct(nb.CUDA(reserve_sms=8)).reserve_sms == 8
     assert nb._args_struct(nb.CUDA()).reserve_sms == 0
+    assert nb._args_struct(nb.CUDA(priority_engines=2)).priority_engines == 2
 
 
 def test_scenario_needs_a_dispersal_map_or_tables(nb, syn):
@@ -95,3 +96,17 @@ def test_atom_target_outside_the_map_is_a_device_check(nb, syn):
     with pytest.raises(nb.NecsimError) as e:
         nb.simulate(2e-3, nb.SpatiallyExplicit(hab, None, tables=(cells, bad)), 5)
     assert e.value.code == E_DEVICE_CHECK
+
+
+def test_outcome_conversion_keeps_every_field(nb):
+    """The ctypes outcome converts field by field: events and lineages stay
+    in their own attributes beside the timeline fields."""
+    o = nb.COutcome()
+    o.paused, o.time, o.steps, o.n_initial, o.n_remaining = 1, 2.5, 7, 9, 3
+    o.resident_ms, o.end_ms, o.routed_ms = 1.5, 4.25, -1.0
+    spec = np.zeros(2, dtype=nb.SPECIATION_DTYPE)
+    rem = np.zeros(3)
+    out = nb._outcome(o, spec, rem)
+    assert out.speciation is spec and out.remaining is rem
+    assert (out.paused, out.time, out.steps, out.n_initial, out.n_remaining) == (True, 2.5, 7, 9, 3)
+    assert (out.resident_ms, out.end_ms, out.routed_ms) == (1.5, 4.25, -1.0)

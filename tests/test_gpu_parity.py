@@ -293,3 +293,28 @@ def test_priority_split_is_bit_identical(nb, syn):
                 o.steps, o.n_rounds, o.n_dedup, o.biodiversity, o.time)
     # the batch's device time spans its engines
     assert split[0].total_ms > 0 and split[0].n_launches > whole[0].n_launches
+
+
+@pytest.mark.gpu
+def test_batch_timeline_on_the_device_clock(nb, syn):
+    """Every simulation of a batch reports when it ended (and when the
+    resident kernel took it over) on the device clock, from the batch's first
+    round: within the batch's span, hand-over before the end, the last end
+    at the batch's end."""
+    sims = syn.config4()[::16]
+    scen = [syn.to_scenario(d) for d, _ in sims]
+    nus = [d["speciation_probability"] * 10 for d, _ in sims]
+    seeds = [s for _, s in sims]
+    algo = nb.CUDA(resident=True, priority_list=[0, 1])
+    with nb.Batch(scen, nus, seeds, algo) as b:
+        b.run()
+        outs = b.run()
+    total = outs[0].total_ms
+    for o in outs:
+        assert 0.0 < o.end_ms <= total + 0.5
+        assert o.routed_ms == -1.0 or 0.0 <= o.routed_ms <= o.end_ms
+    assert any(o.routed_ms >= 0.0 for o in outs)
+    assert max(o.end_ms for o in outs) >= 0.8 * total
+    with nb.Simulation(scen[0], nus[0], nb.CUDA()) as sim:
+        one = sim.simulate(seeds[0])
+    assert 0.0 < one.end_ms <= one.total_ms + 0.5 and one.routed_ms == -1.0
