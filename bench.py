@@ -18,7 +18,10 @@ to completion in one batched launch per round.  One step = one full batch.
              steps, species, speciation and duplicate counts, times)
   e2e        the same metric through the public C ABI call
              necsim_gpu_simulate_batch with host buffers: scenario set-up,
-             host->device origin upload, simulation, device->host events
+             host->device origin upload, simulation, device->host events;
+             `parts` times a resident batch's set-up, run and release once
+  timeline   when the last priority and other simulations ended, on the
+             device clock from the batch's first round
   roofline   the round kernels (cooperative + step kernel) against their
              integer-issue bound: algorithmic wymum work per event on the
              canonical schedule (counted by the oracle) x events / kernel
@@ -545,6 +548,18 @@ def main():
         h2d += outs[0].h2d_bytes
         d2h += outs[0].d2h_bytes
 
+    # where the end-to-end call's host time goes: the same batch set up
+    # (engines, buffers, origins, CUDA graphs, model scores), run (device time
+    # inside) and released, each timed on the host once
+    t0 = time.perf_counter()
+    bb = nb.Batch(scen, nus, seeds, head_algo, pause_before=args.pause)
+    t1 = time.perf_counter()
+    bo = bb.run()
+    t2 = time.perf_counter()
+    bb.close()
+    t3 = time.perf_counter()
+    e2e_parts = {"prepare_s": t1 - t0, "run_s": t2 - t1, "device_ms": bo[0].total_ms, "release_s": t3 - t2}
+
     max_ms = dist.max(head["dev_ms"])
     total_steps = dist.sum(head["steps"])
     value = total_steps / (max_ms / 1e3)
@@ -592,7 +607,7 @@ def main():
         "events_per_step": steps / args.steps,
         "clocks": clk,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-                "d2h_bytes_per_step": d2h / args.steps},
+                "d2h_bytes_per_step": d2h / args.steps, "parts": e2e_parts},
         "gpu_launches": head["launches"],
         "hbm_roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,
