@@ -362,3 +362,28 @@ def test_driver_statistics_reporters(nb, tmp_path):
     assert outs["GlobalSpeciation"].read_text() == "\n".join(sp) + "\n"
     assert outs["GlobalTurnover"].read_text() == "\n".join(tu) + "\n"
     assert outs["GlobalCoverage"].read_text() == "\n".join(co) + "\n"
+
+
+def test_sign_encoding_follows_the_reference_kats(nb, tmp_path):
+    """The event kind lives in the time sign bits (event.rs:105-160), set and
+    cleared bit-wise like the reference's make_negative / make_positive,
+    whose own tests (event.rs:337-353) pin -0.0 <-> 0.0, 42.0 <-> -42.0 and
+    24.0 / -24.0: a speciation event at prior time 0.0 is stored with the
+    sign bit alone, and replay gives back +0.0."""
+    spec = np.zeros(1, dtype=nb.SPECIATION_DTYPE)
+    spec[0] = (3, 0.0, 42.0, 1, 1, 0, 0)
+    disp = np.zeros(1, dtype=nb.DISPERSAL_DTYPE)
+    disp[0] = (4, 24.0, 42.0, 1, 1, 0, 2, 2, 0, 0, 0)
+    d = str(tmp_path / "log")
+    write(nb, d, spec, disp, capacity=10)
+    seg = np.frombuffer(open(os.path.join(d, "0"), "rb").read()[26:], dtype=nb.PACKED_EVENT_DTYPE)
+    bits = {int(g): (int(p), int(e)) for g, p, e in zip(seg["gref"], seg["prior_time"].view(np.uint64),
+                                                           seg["event_time"].view(np.uint64))}
+    f64 = lambda v: struct.unpack("<Q", struct.pack("<d", v))[0]  # noqa: E731
+    assert bits[3] == (0x8000000000000000, f64(42.0))      # make_negative(0.0), make_positive(42.0)
+    assert bits[4] == (f64(24.0), f64(-42.0))              # make_positive(24.0), make_negative(42.0)
+    _, ev = nb.read_event_log(d)
+    s = ev[ev["kind"] == 0][0]
+    assert s["prior_time"] == 0.0 and not np.signbit(s["prior_time"]) and s["event_time"] == 42.0
+    g = ev[ev["kind"] == 2][0]
+    assert (g["prior_time"], g["event_time"]) == (24.0, 42.0)
