@@ -412,17 +412,27 @@ static inline void normal_disperse_from_draws(uint64_t d0, uint64_t d1, double s
     clamp_round_dispersal(x, y, dx, dy, tx, ty);
 }
 
-/* almost_infinite_clark2dt.rs:96-107 with clark2dt::cdf_inverse and
- * pow_fast_one (:167-189): jump = sqrt(u * (pow(1 / (1 - u01), 1 / p) - 1)),
+/* clark2dt::cdf_inverse with pow_fast_one (almost_infinite_clark2dt.rs:167-189):
+ * jump = sqrt(u * (pow(1 / (1 - u01), 1 / p) - 1)), the power skipped for an
+ * exponent of exactly 1 */
+static inline double clark2dt_cdf_inverse(double u01, double shape_u, double tail_p) {
+    double expo = 1.0 / tail_p;
+    double base = 1.0 / (1.0 - u01);
+    double powed = (expo == 1.0) ? base : pow(base, expo);
+    return sqrt(shape_u * (powed - 1.0));
+}
+
+double oracle_clark2dt_cdf_inverse(double u01, double shape_u, double tail_p) {
+    return clark2dt_cdf_inverse(u01, shape_u, tail_p);
+}
+
+/* almost_infinite_clark2dt.rs:96-107: the jump from cdf_inverse,
  * theta = u2 * 2 * pi, (dx, dy) = (cos(theta) * jump, sin(theta) * jump) */
 static inline void clark2dt_displacement(uint64_t d0, uint64_t d1, double shape_u, double tail_p, double *dx,
                                          double *dy) {
     double u01 = (double)(d0 >> 11) * 0x1.0p-53;
     double u2 = (double)((d1 >> 11) + 1) * 0x1.0p-53;
-    double expo = 1.0 / tail_p;
-    double base = 1.0 / (1.0 - u01);
-    double powed = (expo == 1.0) ? base : pow(base, expo);
-    double jump = sqrt(shape_u * (powed - 1.0));
+    double jump = clark2dt_cdf_inverse(u01, shape_u, tail_p);
     double theta = u2 * 2.0 * 3.141592653589793;
     *dx = cos(theta) * jump;
     *dy = sin(theta) * jump;

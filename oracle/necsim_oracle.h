@@ -178,6 +178,8 @@ void oracle_free_alias(oracle_alias_tables *t);
 int oracle_check_dispersal_contract(const oracle_scenario *sc);
 
 /* Box-Muller + clamp_round_dispersal for given raw u64 draws (AlmostInfinite). */
+/* clark2dt::cdf_inverse(u01, shape_u, tail_p): the Clark2Dt jump distance. */
+double oracle_clark2dt_cdf_inverse(double u01, double shape_u, double tail_p);
 /* Clark2Dt cdf_inverse + clamp_round_dispersal for given raw u64 draws. */
 void oracle_clark2dt_dispersal(uint64_t draw0, uint64_t draw1, double shape_u, double tail_p, uint32_t x,
                                uint32_t y, uint32_t *tx, uint32_t *ty);

@@ -188,6 +188,8 @@ def lib():
                                                 ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
                                                 ctypes.POINTER(ctypes.c_uint32)]
         L.oracle_clark2dt_dispersal.restype = None
+        L.oracle_clark2dt_cdf_inverse.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.oracle_clark2dt_cdf_inverse.restype = ctypes.c_double
         f64 = ctypes.c_double
         L.oracle_wrapping_noise.argtypes = [ctypes.c_int64, f64, f64, u64, ctypes.c_uint32, ctypes.c_uint32]
         L.oracle_wrapping_noise.restype = f64
@@ -408,6 +410,11 @@ def distinct_speciation_set(events):
     k = np.stack([events["event_time"].view(np.uint64), events["x"].astype(np.uint64),
                   events["y"].astype(np.uint64), events["index"].astype(np.uint64)], axis=1)
     return np.unique(k, axis=0)
+
+
+def clark2dt_cdf_inverse(u01, shape_u, tail_p):
+    """clark2dt::cdf_inverse: the Clark2Dt jump distance for a uniform u01."""
+    return lib().oracle_clark2dt_cdf_inverse(u01, shape_u, tail_p)
 
 
 def clark2dt_dispersal(d0, d1, shape_u, tail_p, x, y):

@@ -101,6 +101,29 @@ def test_box_muller_device_vs_libm(nb, syn, oracle, dispersal):
     assert np.all(np.abs(gx - cx) <= 1e-12 * np.abs(cx)) and np.all(np.abs(gy - cy) <= 1e-12 * np.abs(cy))
 
 
+def test_clark2dt_device_jump_against_the_reference_test(nb):
+    """The reference's golden bits for clark2dt::cdf_inverse
+    (almost_infinite_clark2dt.rs test_cdf_inverse; tests/golden) through the
+    device's displacement arithmetic: draws giving each case's u01 and an
+    angle of 2 pi, so dx is the jump.  CUDA's pow and cos may round the last
+    bit differently from the C library the reference calls; the number of
+    bit-exact cases is printed and every value is within 1e-12 relative."""
+    import json
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "clark2dt_cdf_inverse.json")) as f:
+        cases = json.load(f)["cases"]
+    exact = 0
+    for c in cases:
+        d0 = int(c["u01"] * 2.0 ** 53) << 11
+        draws = np.array([[d0, (1 << 64) - 1]], dtype=np.uint64)
+        dx, dy = nb.displacements(draws, nb.Clark2Dt(c["shape_u"], c["tail_p"]))
+        want = c["expected"]
+        exact += int(dx.view(np.uint64)[0] == int(c["expected_bits"], 16))
+        assert abs(dx[0] - want) <= 1e-12 * abs(want), c
+        assert abs(dy[0]) <= 1e-12 * max(1.0, abs(want)), c
+    print("device jump bit-exact with the reference's test in %d of %d cases" % (exact, len(cases)))
+
+
 def rust_round(v):
     """f64::round: to the nearest integer, halves away from zero (exact:
     the fraction v - trunc(v) is computed without rounding)."""

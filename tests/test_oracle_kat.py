@@ -339,3 +339,32 @@ def test_almost_infinite_rectangle_reference_runs(oracle, kat):
         desc = dict(kind=oracle.ALMOST_INFINITE_NORMAL, speciation_probability=case["speciation"],
                     sigma=case["sigma"], sample=tuple(case["sample"]))
         check_run(oracle, desc, case)
+
+
+def _clark2dt_reference_cases():
+    import json
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "clark2dt_cdf_inverse.json")) as f:
+        return json.load(f)["cases"]
+
+
+def test_clark2dt_cdf_inverse_matches_the_reference_test(oracle):
+    """The reference's own golden bits for clark2dt::cdf_inverse
+    (almost_infinite_clark2dt.rs test_cdf_inverse, extracted by
+    golden/make_clark2dt_kat.py): the oracle's jump distance equals every one,
+    and so does its dispersal displacement for draws that give the same u01
+    and an angle of 2 pi (cos = 1, so dx is the jump itself)."""
+    import struct
+    cases = _clark2dt_reference_cases()
+    assert len(cases) == 27
+    for c in cases:
+        want = int(c["expected_bits"], 16)
+        got = oracle.clark2dt_cdf_inverse(c["u01"], c["shape_u"], c["tail_p"])
+        assert struct.unpack("<Q", struct.pack("<d", got))[0] == want, c
+        # u01 = (d0 >> 11) * 2^-53 exactly (every case's u01 is a multiple of 2^-53)
+        d0 = int(c["u01"] * 2.0 ** 53) << 11
+        draws = np.array([[d0, (1 << 64) - 1]], dtype=np.uint64)
+        dx, dy = oracle.displacements(oracle.ALMOST_INFINITE_CLARK2DT, draws, c["shape_u"], c["tail_p"])
+        assert dx.view(np.uint64)[0] == want, c
+        assert abs(dy[0]) <= 1e-15 * max(1.0, got)
