@@ -2298,7 +2298,18 @@ int necsim_gpu_simulate_batch(const necsim_scenario *scenarios, const uint64_t *
         }
         BatchRun b;
         prepare_batch(b, std::move(sims), args);
+        // the call's traffic includes the set-up's (tables, origins), which
+        // run_batch does not count (a prepared batch's runs report their own)
+        uint64_t setup_h2d = 0, setup_d2h = 0;
+        for (const auto &e : b.engines) {
+            setup_h2d += e->h2d_bytes;
+            setup_d2h += e->d2h_bytes;
+        }
         run_batch(b, reporters, outcomes);
+        for (uint32_t s = 0; s < n_sims; ++s) {
+            outcomes[s].h2d_bytes += setup_h2d;
+            outcomes[s].d2h_bytes += setup_d2h;
+        }
     });
 }
 
